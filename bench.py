@@ -1,0 +1,484 @@
+"""Benchmark of the DEM step: particle-updates/s on one or more B200s.
+
+A "step" is one MoveParticles (src/MDEM.f90:285-369) of a whole system: two
+force passes (cell rebuild, contact search + history, forces/torques) plus
+the AB predictor and AM corrector.  particle-updates/s = particles x steps / s.
+
+Default workload: 1,000,000 polydisperse spheres (radii U[0.4,0.6]) in a
+fully periodic cube at volume fraction 0.55, kn = 1e5, e = 0.8, mu = 0.5,
+dt = 1e-4, no gravity.  With --gpus N every rank advances its own
+independent system (ensemble members, seed + rank): weak scaling, no
+collective on the data path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+    python bench.py --impl reference ...   # CPU implementation (oracle port)
+
+Prints one JSON line (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-updates/s @1M spheres: FP32-mixed vs FP64 plain, force err <=1e-5 rel"
+UNIT = "particle-updates/s"
+WORKLOADS = {
+    "dense1m": dict(n=1_000_000, phi=0.55, seed=1001, tile=8000),
+    "dense16m": dict(n=16_000_000, phi=0.60, seed=1002, tile=16000),
+    "dense64k": dict(n=64_000, phi=0.55, seed=1001, tile=8000),
+}
+
+
+# --------------------------------------------------------------------------
+# helpers
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def force_bytes_per_particle(z_pp, z_pw, nw, pass_kind, nprev=3):
+    """Algorithmic (compulsory) DRAM bytes of one force-kernel launch per
+    particle, FP64 layout.  z_pp: pair contacts per particle, z_pw: wall
+    contacts per particle.  Neighbour data is counted once (it is re-read
+    from L1/L2).  pass_kind: 'predict' (history update + AB predictor) or
+    'correct' (history read + AM corrector)."""
+    own = 32 + 32 + 16 + 4 + 4          # sorted pos+R, v+wx, wy+wz, orig, cell
+    rec = 4 + 48                        # partner key + (ft, vt)
+    hist_read = 4 + 0.5 * z_pp * rec + nw * 4 + z_pw * 48
+    b = own + hist_read
+    if pass_kind == "predict":
+        b += 4 + 0.5 * z_pp * rec + nw * 4 + z_pw * 48  # history write
+        b += 48                         # a, alpha -> Particle
+        b += nprev * 72 + 72            # ring read, ring store
+        b += 72                         # Predicted x, v, w
+    else:
+        b += 48                         # a, alpha -> Predicted
+        b += nprev * 72                 # ring read
+        b += 72 + 72                    # Particle x, v, w read + write
+    return b
+
+
+def rebuild_bytes_per_particle():
+    """k_assign 48 + k_scatter 28 + k_cellsort 20 + k_gather 164."""
+    return 48 + 28 + 20 + 164
+
+
+def reduce_max(x, world, device="cuda"):
+    """Max over ranks (the timed region is the slowest rank's)."""
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(n_per_rank, world, steps, max_ms):
+    """Whole-job particle-updates/s: every rank advances its own system."""
+    return n_per_rank * world * steps / (max_ms / 1000.0)
+
+
+def rank_seed(base, rank):
+    return base + rank
+
+
+# --------------------------------------------------------------------------
+# workload
+
+def make_workload(name, precision, rank, factory=None):
+    from dem3d_b200 import configs
+    from dem3d_b200 import params as P
+    spec = WORKLOADS[name]
+    prec = P.PREC_MIXED if precision == "mixed" else P.PREC_FP64
+    return configs.dense_packing(n=spec["n"], phi=spec["phi"], seed=rank_seed(spec["seed"], rank),
+                                 tile=spec["tile"], precision=prec, system_factory=factory)
+
+
+def config_block(name, w, world, precision):
+    spec = WORKLOADS[name]
+    return {
+        "workload": (f"{spec['n']:,} polydisperse spheres R~U[0.4,0.6], periodic cube "
+                     f"phi={spec['phi']}, kn=1e5, e=0.8, mu=0.5, dt=1e-4, ABM4"),
+        "particles_per_gpu": spec["n"], "global_particles": spec["n"] * world,
+        "box": round(w.info["L"], 4), "precision": precision,
+        "input": f"relaxed {spec['tile']}-sphere tile x {w.info['copies']} copies, seeded",
+        "l2": "inputs larger than L2 (state + history >> 126 MB)",
+        "parallelism": f"{world} independent systems (ensemble, seed+rank)",
+    }
+
+
+# --------------------------------------------------------------------------
+# CPU timing (oracle port: the reference is Fortran and cannot be built here)
+
+def _oracle_variant():
+    """-O3 -march=native build of the oracle on this host, else the portable one."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("oracle_build",
+                                                  os.path.join(ROOT, "oracle", "build.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    try:
+        libs = mod.build(native_dir=tempfile.mkdtemp())
+        return libs["libdem_oracle_native.so"], "-O3 -march=native -ffp-contract=off"
+    except Exception:
+        libs = mod.build()
+        return libs["libdem_oracle_fast.so"], "-O3 -ffp-contract=off"
+
+
+def cpu_time_steps(w, max_steps=3, budget_s=25.0, lib_path=None):
+    """Time oracle MoveParticles steps on w (single thread)."""
+    import ctypes as C
+
+    from dem3d_b200 import _abi
+    from dem3d_b200.system import DEMSystem
+    lib = C.CDLL(lib_path)
+    _abi.bind(lib, "orc_", _abi.SIGNATURES)
+    s = DEMSystem(w.params, lib=lib, prefix="orc_")
+    try:
+        s.set_state(w.pos, w.vel, w.omega, comp=w.comp, radius=w.radius)
+        s.initialize_cell_distribution()
+        steps = 0
+        t0 = time.perf_counter()
+        while steps < max_steps:
+            s.move_particles(4 + steps)
+            steps += 1
+            if time.perf_counter() - t0 > budget_s:
+                break
+        dt = time.perf_counter() - t0
+    finally:
+        s.close()
+    return w.n * steps / dt, steps, dt
+
+
+def _ref_worker(args):
+    name, rank, tile_pos, tile_rad, L_t, lib_path, steps_cap, budget = args
+    from dem3d_b200 import configs
+    spec = WORKLOADS[name]
+    k = configs.tile_count(spec["n"], spec["tile"])
+    pos, radius, L = configs.replicate(tile_pos, tile_rad, L_t, k)
+    rng = np.random.default_rng(spec["seed"] + rank + 7919)
+    n = spec["n"]
+    vel = rng.normal(0.0, 0.1, size=(n, 3))
+    prm = configs.dense_packing_params(0.6, L)
+    w = configs.Workload("dense_packing", prm, pos, vel, np.zeros((n, 3)), radius=radius,
+                         info={"L": L, "copies": k ** 3})
+    return cpu_time_steps(w, steps_cap, budget, lib_path)
+
+
+def run_reference(args):
+    """--impl reference: the CPU implementation of the path on all host cores
+    (one independent system per process; the reference program is serial)."""
+    rank = env_int("RANK", 0)
+    world = env_int("WORLD_SIZE", 1)
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+
+    import psutil
+    from dem3d_b200 import configs
+    lib_path, flags = _oracle_variant()
+    spec = WORKLOADS[args.workload]
+    # the same relaxed tile as the GPU arm, relaxed here by the oracle
+    import ctypes as C
+
+    from dem3d_b200 import _abi
+    from dem3d_b200.system import DEMSystem
+
+    def factory(p):
+        lib = C.CDLL(lib_path)
+        _abi.bind(lib, "orc_", _abi.SIGNATURES)
+        return DEMSystem(p, lib=lib, prefix="orc_")
+    t0 = time.perf_counter()
+    tp, tr, L_t = configs.relaxed_tile(spec["tile"], spec["phi"], spec["seed"],
+                                       system_factory=factory)
+    t_relax = time.perf_counter() - t0
+    cores = os.cpu_count() or 1
+    mem = psutil.virtual_memory().available
+    per_proc = 1.6e9 * spec["n"] / 1e6
+    procs = max(1, min(cores, int(mem * 0.6 // per_proc), 32))
+    steps_cap = max(1, min(args.steps, 3))
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_ref_worker, [(args.workload, r, tp, tr, L_t, lib_path, steps_cap, 60.0)
+                                     for r in range(procs)])
+    wall = time.perf_counter() - t0
+    value = sum(r[0] for r in res)
+    w_dummy = type("W", (), {"info": {"L": configs.replicate(tp, tr, L_t, 1)[2] *
+                                       configs.tile_count(spec["n"], spec["tile"]),
+                                       "copies": configs.tile_count(spec["n"],
+                                                                    spec["tile"]) ** 3}})
+    sample = (f"{procs} processes x {res[0][1]} MoveParticles steps of an independent "
+              f"{spec['n']:,}-sphere system each (oracle C port {flags}; reference Fortran "
+              f"not buildable here: no Fortran compiler); tile relaxed by the oracle in "
+              f"{t_relax:.1f}s")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": res[0][1], "warmup": 0, "ms_per_step": 1000.0 * max(r[2] / r[1] for r in res),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": config_block(args.workload, w_dummy, 1, "fp64"),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": round(wall, 2),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------
+# GPU arm
+
+def traffic_per_particle():
+    """DRAM bytes per particle of the force kernel from a committed ncu
+    capture summary (profiles/force_traffic.json), if present."""
+    p = os.path.join(ROOT, "profiles", "force_traffic.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p))
+        except Exception:
+            return None
+    return None
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from dem3d_b200 import _abi
+    from dem3d_b200.system import DEMSystem
+
+    rank = env_int("RANK", 0)
+    world = env_int("WORLD_SIZE", 1)
+    local = env_int("LOCAL_RANK", 0)
+    if world > 1:
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    lib = _abi.load_library()
+    st = lib.dem_select_device(local)
+    if st != 0:
+        raise RuntimeError(f"dem_select_device({local}) failed: {st}")
+
+    def barrier_max(x):
+        return reduce_max(x, world)
+
+    precision = args.precision
+    if precision == "auto":
+        precision = "fp64"
+        try:
+            from dem3d_b200 import configs
+            probe = configs.dense_packing_params(0.6, 10.0, precision=_abi.PREC_MIXED)
+            DEMSystem(probe).close()
+            precision = "mixed"
+        except Exception:
+            precision = "fp64"
+
+    t0 = time.perf_counter()
+    w = make_workload(args.workload, precision, rank)
+    t_gen = time.perf_counter() - t0
+    n = w.n
+    s = DEMSystem(w.params)
+    s.set_state(w.pos, w.vel, w.omega, radius=w.radius)
+    s.initialize_cell_distribution()
+    # start-up (MethodOrder-1 Euler steps) + warm-up ABM steps
+    s.run(1, 3 + args.warmup)
+    first = 4 + args.warmup
+    last = first + args.steps - 1
+    if world > 1:
+        dist.barrier()
+    l0 = s.launch_count()
+    with ClockSampler(local) as clk:
+        ms = s.run_timed(first, last)
+    launches = s.launch_count() - l0
+    ms = barrier_max(ms)
+    value = aggregate_rate(n, world, args.steps, ms)
+
+    # contacts per particle (last pass) for the byte model
+    ps = s.pass_stats()
+    obs = s.observables()
+    z_pp = 2.0 * obs["n_pair_contacts"] / n
+    # per-kernel timing (instrumented steps, not graph-replayed)
+    s.reset_kernel_stats()
+    s.set_profiling(True)
+    nprof = 6
+    for k in range(nprof):
+        s.move_particles(last + 1 + k)
+    stats = s.kernel_stats()
+    s.set_profiling(False)
+    last += nprof
+    total_prof = sum(v[1] for v in stats.values())
+    dom = max(stats, key=lambda k: stats[k][1])
+    nw = int(w.params.n_walls)
+    if dom.startswith("force"):
+        b_launch = n * 0.5 * (force_bytes_per_particle(z_pp, 0.0, nw, "predict") +
+                             force_bytes_per_particle(z_pp, 0.0, nw, "correct"))
+    else:
+        b_launch = n * rebuild_bytes_per_particle() / 4
+    avg_ms = stats[dom][1] / stats[dom][0]
+    achieved = b_launch / (avg_ms / 1000.0) / 1e9
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    peak = peaks.get("hbm_gbs", 6650.0)
+    tr = traffic_per_particle()
+    traffic = None
+    if tr and dom in tr.get("bytes_per_particle", {}):
+        traffic = tr["bytes_per_particle"][dom] * n
+
+    # e2e: each step uploads Particle(1:n) from pinned host memory, advances
+    # one MoveParticles through the C-ABI and downloads the state.
+    e2e = None
+    if not args.no_e2e:
+        ke = max(3, min(args.steps, 20))
+        host = {k: torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
+                for k in ("pos", "vel", "omega", "acc", "alpha")}
+        stt = s.get_state()
+        for k in host:
+            host[k][...] = stt[k]
+        if world > 1:
+            dist.barrier()
+        s.timer_start()
+        for k in range(ke):
+            s.update_state(host["pos"], host["vel"], host["omega"], host["acc"], host["alpha"])
+            s.move_particles(last + 1 + k)
+            s._call("get_state", *(host[x].ctypes.data_as(
+                __import__("ctypes").POINTER(__import__("ctypes").c_double))
+                for x in ("pos", "vel", "omega", "acc", "alpha")))
+        e2e_ms = barrier_max(s.timer_stop())
+        last += ke
+        e2e = {"value": n * world * ke / (e2e_ms / 1000.0), "unit": UNIT,
+               "h2d_bytes_per_step": 5 * 24 * n, "d2h_bytes_per_step": 5 * 24 * n,
+               "steps": ke, "path": "dem_update_state + dem_move_particles + dem_get_state"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        lib_path, flags = _oracle_variant()
+        v, k, dt = cpu_time_steps(w, max_steps=3, budget_s=25.0, lib_path=lib_path)
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"{k} MoveParticles steps of the same {n:,}-sphere system, oracle "
+                         f"C port ({flags}), 1 thread, {dt:.1f}s"}
+    clocks = clk.summary()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if precision == "fp64" else "f32+f64", "data": "synthetic",
+            "config": config_block(args.workload, w, world, precision),
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "algorithmic_bytes_per_launch": b_launch,
+                         "avg_launch_ms": avg_ms, "peak_source": "MEASURED_PEAKS.json hbm_gbs"
+                         if "hbm_gbs" in peaks else "fallback 6650 GB/s",
+                         "kernel_share": {k: round(v[1] / total_prof, 4)
+                                          for k, v in sorted(stats.items(),
+                                                             key=lambda kv: -kv[1][1])}},
+            "contacts_per_particle": z_pp, "movers_last_pass": ps["movers"],
+            "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
+            "gen_s": round(t_gen, 2),
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="dense1m", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,162 @@
+"""ctypes mirror of ``include/dem3d_b200.h`` and the loader of the CUDA library.
+
+The library is the product: there is no CPU fallback.  ``load_library`` raises
+if ``libdem3d_b200.so`` is missing or cannot be loaded.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+MAX_COMPONENTS = 16
+MAX_WALLS = 8
+
+DEM_OK = 0
+DEM_ERR_INVALID = -1
+DEM_ERR_CUDA = -2
+DEM_ERR_CAPACITY = -3
+DEM_ERR_UNSUPPORTED = -5
+DEM_ERR_STATE = -6
+DEM_ERR_NO_DEVICE = -7
+
+WALL_RECTANGLE = 1
+WALL_CONE = 2
+
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+_d3 = C.c_double * 3
+
+
+class DemWall(C.Structure):
+    """TWall (src/MDimension3D.f90:45-59)."""
+
+    _fields_ = [
+        ("shape", C.c_int32), ("order", C.c_int32),
+        ("l1", C.c_double), ("l2", C.c_double), ("l3", C.c_double),
+        ("u", _d3), ("w", _d3), ("n", _d3),
+        ("position", _d3), ("velocity", _d3), ("omega", _d3),
+    ]
+
+
+_NCC = MAX_COMPONENTS * MAX_COMPONENTS
+_NCW = MAX_COMPONENTS * MAX_WALLS
+
+
+class DemParams(C.Structure):
+    _fields_ = [
+        ("n_components", C.c_int32), ("n_walls", C.c_int32), ("pbc", C.c_int32 * 3),
+        ("method_order", C.c_int32), ("euler_intervals", C.c_int32), ("max_ncell", C.c_int32),
+        ("precision", C.c_int32), ("hist_capacity", C.c_int32),
+        ("lbox", _d3), ("gravity", _d3), ("time_step", C.c_double),
+        ("comp_radius", C.c_double * MAX_COMPONENTS),
+        ("comp_inv_mass", C.c_double * MAX_COMPONENTS),
+        ("comp_inv_inertia", C.c_double * MAX_COMPONENTS),
+        ("comp_eff_mass", C.c_double * MAX_COMPONENTS),
+        ("min_dij", C.c_double * _NCC), ("min_dij_sq", C.c_double * _NCC),
+        ("kn", C.c_double * _NCC), ("yn", C.c_double * _NCC), ("kt", C.c_double * _NCC),
+        ("yt", C.c_double * _NCC), ("mu_sq", C.c_double * _NCC),
+        ("knw", C.c_double * _NCW), ("ynw", C.c_double * _NCW), ("ktw", C.c_double * _NCW),
+        ("ytw", C.c_double * _NCW), ("muw_sq", C.c_double * _NCW),
+        ("pp_mass_coef", C.c_double), ("pp_density", C.c_double),
+        ("pp_fluid_density", C.c_double), ("pp_rmax", C.c_double),
+        ("pp_kn", C.c_double), ("pp_kt", C.c_double), ("pp_gamma_n", C.c_double),
+        ("pp_gamma_t", C.c_double), ("pp_mu_sq", C.c_double),
+        ("pp_knw", C.c_double * MAX_WALLS), ("pp_ktw", C.c_double * MAX_WALLS),
+        ("pp_gamma_nw", C.c_double * MAX_WALLS), ("pp_gamma_tw", C.c_double * MAX_WALLS),
+        ("pp_muw_sq", C.c_double * MAX_WALLS),
+        ("walls", DemWall * MAX_WALLS),
+    ]
+
+
+class DemObservables(C.Structure):
+    _fields_ = [
+        ("kinetic_energy", C.c_double), ("potential_energy", C.c_double),
+        ("mean_coordination", C.c_double), ("packing_fraction", C.c_double),
+        ("wall_normal_force", C.c_double * MAX_WALLS), ("momentum", _d3),
+        ("n_pair_contacts", C.c_int64), ("n_wall_contacts", C.c_int64),
+    ]
+
+
+_P = C.c_void_p
+_I32P = C.POINTER(C.c_int32)
+_I64P = C.POINTER(C.c_int64)
+_DP = C.POINTER(C.c_double)
+
+# name -> (restype, argtypes); the same table describes the oracle (prefix orc_)
+SIGNATURES = {
+    "create": (C.c_int, [C.POINTER(DemParams), C.POINTER(_P)]),
+    "destroy": (None, [_P]),
+    "last_error": (C.c_char_p, [_P]),
+    "set_state": (C.c_int, [_P, C.c_int32, _I32P, _DP, _DP, _DP, _DP, _DP, _DP]),
+    "get_state": (C.c_int, [_P, _DP, _DP, _DP, _DP, _DP]),
+    "get_predicted": (C.c_int, [_P, _DP, _DP, _DP, _DP, _DP]),
+    "update_state": (C.c_int, [_P, _DP, _DP, _DP, _DP, _DP]),
+    "get_n": (C.c_int, [_P, _I32P]),
+    "set_integration": (C.c_int, [_P, _DP, _I32P]),
+    "get_integration": (C.c_int, [_P, _DP, _I32P]),
+    "set_contacts": (C.c_int, [_P, C.c_int64, _I32P, _I32P, _DP, _DP, C.c_int64, _I32P, _I32P,
+                               _DP, _DP]),
+    "count_contacts": (C.c_int, [_P, _I64P, _I64P]),
+    "get_contacts": (C.c_int, [_P, C.c_int64, _I32P, _I32P, _DP, _DP, C.c_int64, _I32P, _I32P,
+                               _DP, _DP]),
+    "initialize_cell_distribution": (C.c_int, [_P]),
+    "get_grid": (C.c_int, [_P, _I32P]),
+    "get_cells": (C.c_int, [_P, _I32P, _I32P, _I32P]),
+    "compute_accelerations": (C.c_int, [_P, C.c_int32, C.c_double, C.c_int32]),
+    "move_particles": (C.c_int, [_P, C.c_int32]),
+    "move_particles_euler": (C.c_int, [_P]),
+    "run": (C.c_int, [_P, C.c_int32, C.c_int32]),
+    "get_ncol": (C.c_int, [_P, _I64P]),
+    "get_escaped": (C.c_int, [_P, _I64P]),
+    "get_observables": (C.c_int, [_P, C.POINTER(DemObservables)]),
+}
+
+# entry points only the CUDA library has
+GPU_ONLY = {
+    "version": (C.c_char_p, []),
+    "select_device": (C.c_int, [C.c_int32]),
+    "run_timed": (C.c_int, [_P, C.c_int32, C.c_int32, _DP]),
+    "set_profiling": (C.c_int, [_P, C.c_int32]),
+    "get_kernel_stats": (C.c_int, [_P, C.c_int32, C.c_char_p, C.c_int32, _I64P, _DP]),
+    "reset_kernel_stats": (C.c_int, [_P]),
+    "get_launch_count": (C.c_int, [_P, _I64P]),
+    "timer_start": (C.c_int, [_P]),
+    "timer_stop": (C.c_int, [_P, _DP]),
+    "get_stream": (C.c_int, [_P, C.POINTER(_P)]),
+    "get_pass_stats": (C.c_int, [_P, _I64P, _I64P, _I64P, _I32P]),
+}
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdem3d_b200.so")
+
+
+def bind(lib: C.CDLL, prefix: str, table: dict) -> None:
+    for name, (res, args) in table.items():
+        f = getattr(lib, prefix + name)
+        f.restype = res
+        f.argtypes = args
+
+
+def all_symbols() -> list[str]:
+    return ["dem_" + k for k in list(SIGNATURES) + list(GPU_ONLY)]
+
+
+_LIB = None
+
+
+def load_library(path: str | None = None) -> C.CDLL:
+    """Load the CUDA library; raises (never falls back to CPU code)."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(
+            f"{p} is missing: build it with `python -m dem3d_b200.build` (nvcc, sm_100a)")
+    lib = C.CDLL(p)
+    bind(lib, "dem_", SIGNATURES)
+    bind(lib, "dem_", GPU_ONLY)
+    if path is None:
+        _LIB = lib
+    return lib

@@ -1,0 +1,224 @@
+"""Seeded synthetic workloads (no dataset exists for this path).
+
+``settling``     -- gravity settling of monodisperse spheres on a jittered
+                    lattice in a box periodic in x/y with a frictional floor
+                    (the 2,000-sphere CPU-runnable case; any N).
+``dense_packing``-- polydisperse spheres, radii uniform in [0.4, 0.6], fully
+                    periodic cube at a given volume fraction (the 1M / 16M
+                    cases).  Positions: a jittered cubic lattice filled in a
+                    seeded random order (overlaps allowed), then
+                    soft-repulsion relaxation (normal spring + strong damping,
+                    no friction) run with the library itself, then seeded
+                    Gaussian velocities.
+
+Units: the length unit is the (mean) diameter 1, the mass unit the mass of a
+diameter-1 sphere (density 6/pi), time such that kn = 1e5 (pair normal
+stiffness after the series combination), dt = 1e-4.  The component
+stiffness is 2e5 so that Kn(i,i) = 0.5*k = 1e5 (src/DEM.f90:273); kt = 2/7 kn;
+wall stiffness 2e5 gives Knw = 1e5; tangential restitution = normal one.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import params as P
+
+DENSITY = 6.0 / math.pi
+KN = 1.0e5
+KT = 2.0 / 7.0 * KN
+
+
+@dataclass
+class Workload:
+    name: str
+    params: object
+    pos: np.ndarray
+    vel: np.ndarray
+    omega: np.ndarray
+    comp: np.ndarray | None = None
+    radius: np.ndarray | None = None
+    info: dict | None = None
+
+    @property
+    def n(self):
+        return self.pos.shape[0]
+
+
+def settling(n=2000, seed=1000, layer_side=10, dt=1e-4, e=0.8, mu=0.5, gravity=1.0,
+             headroom=45.0, method_order=4, euler_intervals=100, max_ncell=30000,
+             precision=P.PREC_FP64, sigma_v=0.1):
+    """Monodisperse gravity settling (d = 1, m = 1).
+
+    ``layer_side`` x ``layer_side`` spheres per layer at xy spacing 1.0 in a
+    ``layer_side``-wide periodic box, layers at heights 1, 3, 5, ... above the
+    floor.  Jitter: U(+-0.05) per particle in z and a rigid U(+-0.05) xy shift
+    per layer (a per-particle xy jitter at spacing = diameter would start
+    with overlaps of up to 0.1, i.e. 1e4-force kicks).
+    """
+    rng = np.random.default_rng(seed)
+    per_layer = layer_side * layer_side
+    n_layers = (n + per_layer - 1) // per_layer
+    bed = 2.0 * n_layers
+    lz = bed + headroom
+    L = float(layer_side)
+    pos = np.empty((n, 3))
+    k = 0
+    for layer in range(n_layers):
+        sx, sy = rng.uniform(-0.05, 0.05, size=2)
+        for iy in range(layer_side):
+            for ix in range(layer_side):
+                if k >= n:
+                    break
+                x = -0.5 * L + 0.5 + ix + sx
+                y = -0.5 * L + 0.5 + iy + sy
+                z = -0.5 * lz + 1.0 + 2.0 * layer + rng.uniform(-0.05, 0.05)
+                pos[k] = (x, y, z)
+                k += 1
+    vel = rng.normal(0.0, sigma_v, size=(n, 3))
+    omega = np.zeros((n, 3))
+    comp = np.zeros(n, dtype=np.int32)
+    floor = P.rectangle((0.0, 0.0, -0.5 * lz), L, L, stiffness=2.0 * KN,
+                        shear_stiffness=2.0 * KT)
+    prm, _ = P.component_params(
+        [P.Component(n, 1.0, DENSITY, 2.0 * KN, 2.0 * KT)], [floor], [[e]], [[e]], [[mu]],
+        [[e]], [[e]], [[mu]], lbox=(L, L, lz), pbc=(True, True, False),
+        gravity=(0.0, 0.0, -gravity), time_step=dt, method_order=method_order,
+        euler_intervals=euler_intervals, max_ncell=max_ncell, precision=precision)
+    return Workload("settling", prm, pos, vel, omega, comp=comp,
+                    info={"lbox": (L, L, lz), "seed": seed})
+
+
+def box_for_fraction(radius: np.ndarray, phi: float) -> float:
+    vol = float(np.sum(4.0 / 3.0 * math.pi * radius ** 3))
+    return (vol / phi) ** (1.0 / 3.0)
+
+
+def lattice_positions(n: int, L: float, rng, jitter=0.05):
+    side = int(math.ceil(n ** (1.0 / 3.0) - 1e-9))
+    a = L / side
+    sites = rng.permutation(side ** 3)[:n]
+    iz, r = np.divmod(sites, side * side)
+    iy, ix = np.divmod(r, side)
+    pos = np.stack([ix, iy, iz], axis=1).astype(np.float64) * a + 0.5 * a - 0.5 * L
+    pos += rng.uniform(-jitter, jitter, size=pos.shape) * a
+    # spatially sorted indexing (cell-major), as a generator writing particles
+    # slab by slab would produce
+    order = np.lexsort((pos[:, 0], pos[:, 1], pos[:, 2]))
+    return pos[order]
+
+
+def dense_packing_params(radius_max, L, *, e=0.8, mu=0.5, dt=1e-4, method_order=4,
+                         euler_intervals=100, max_ncell=1 << 30, precision=P.PREC_FP64,
+                         hist_capacity=16):
+    return P.per_particle_params(
+        density=DENSITY, kn=KN, kt=KT, en=e, et=e, mu=mu, rmax=radius_max, lbox=(L, L, L),
+        pbc=(True, True, True), gravity=(0.0, 0.0, 0.0), time_step=dt,
+        method_order=method_order, euler_intervals=euler_intervals, max_ncell=max_ncell,
+        precision=precision, hist_capacity=hist_capacity)
+
+
+def relaxed_tile(n_tile, phi, seed, rmin=0.4, rmax=0.6, relax_steps=2000, relax_e=0.1,
+                 system_factory=None):
+    """A periodic tile of ``n_tile`` spheres relaxed by soft repulsion.
+
+    Radii U[rmin, rmax]; positions on a jittered cubic lattice filled in a
+    seeded random order (overlaps allowed); then ``relax_steps`` ABM steps with
+    restitution ``relax_e`` and no friction.  The FP64 library and the CPU
+    oracle produce the same tile bit for bit, so either may relax it.
+    Returns (pos, radius, L_tile)."""
+    rng = np.random.default_rng(seed)
+    radius = rng.uniform(rmin, rmax, size=n_tile)
+    L = box_for_fraction(radius, phi)
+    pos = lattice_positions(n_tile, L, rng)
+    if relax_steps > 0:
+        if system_factory is None:
+            from .system import DEMSystem
+            system_factory = DEMSystem
+        rp = dense_packing_params(rmax, L, e=relax_e, mu=0.0)
+        s = system_factory(rp)
+        try:
+            s.set_state(pos, np.zeros((n_tile, 3)), np.zeros((n_tile, 3)), radius=radius)
+            s.initialize_cell_distribution()
+            s.run(1, relax_steps)
+            pos = s.get_state()["pos"]
+        finally:
+            s.close()
+    return pos, radius, L
+
+
+def tile_count(n, tile):
+    k = int(round((n / tile) ** (1.0 / 3.0)))
+    return k if k >= 1 and tile * k ** 3 == n else 0
+
+
+def replicate(pos, radius, L_tile, k):
+    """k x k x k periodic copies of a tile, spatially ordered (cell-major)."""
+    L = k * L_tile
+    offs = (np.stack(np.meshgrid(np.arange(k), np.arange(k), np.arange(k), indexing="ij"),
+                     axis=-1).reshape(-1, 3) + 0.5) * L_tile - 0.5 * L
+    P_ = (pos[None, :, :] + offs[:, None, :]).reshape(-1, 3)
+    R_ = np.tile(radius, k ** 3)
+    order = np.lexsort((P_[:, 0], P_[:, 1], P_[:, 2]))
+    return P_[order], R_[order], L
+
+
+def dense_packing(n=1_000_000, phi=0.55, seed=1001, rmin=0.4, rmax=0.6, relax_steps=2000,
+                  sigma_v=0.1, precision=P.PREC_FP64, max_ncell=1 << 30, system_factory=None,
+                  relax_e=0.1, tile=None):
+    """Polydisperse periodic packing at volume fraction ``phi``.
+
+    Large systems are built from a relaxed periodic tile of ``tile`` spheres
+    (default 8000 when n = 8000*k^3, else the whole system is one tile)
+    replicated k^3 times; the velocities are drawn for the whole system.
+    Relaxation runs through ``system_factory`` (the CUDA library by default;
+    the oracle in the CPU baseline).  ``relax_steps=0`` skips it."""
+    if tile is None:
+        tile = 8000 if tile_count(n, 8000) else n
+    k = tile_count(n, tile)
+    if not k:
+        raise ValueError(f"n={n} is not tile*k^3 for tile={tile}")
+    pos_t, rad_t, L_t = relaxed_tile(tile, phi, seed, rmin, rmax, relax_steps, relax_e,
+                                     system_factory)
+    pos, radius, L = replicate(pos_t, rad_t, L_t, k)
+    rng = np.random.default_rng(seed + 7919)
+    vel = rng.normal(0.0, sigma_v, size=(n, 3))
+    omega = np.zeros((n, 3))
+    info = {"L": L, "phi": phi, "seed": seed, "relax_steps": relax_steps, "tile": tile,
+            "copies": k ** 3}
+    prm = dense_packing_params(rmax, L, precision=precision, max_ncell=max_ncell)
+    return Workload("dense_packing", prm, pos, vel, omega, radius=radius, info=info)
+
+
+def max_overlap(pos, radius, L, sample=200_000):
+    """Largest pair overlap (sampled for very large N) via a cell grid."""
+    n = pos.shape[0]
+    idx = np.arange(n) if n <= sample else np.random.default_rng(0).choice(n, sample, False)
+    cs = 1.2
+    nc = max(3, int(L / cs))
+    cell = np.floor((pos + 0.5 * L) / L * nc).astype(np.int64) % nc
+    key = (cell[:, 2] * nc + cell[:, 1]) * nc + cell[:, 0]
+    order = np.argsort(key)
+    sk = key[order]
+    start = np.searchsorted(sk, np.arange(nc ** 3))
+    end = np.searchsorted(sk, np.arange(nc ** 3), side="right")
+    best = 0.0
+    for i in idx[:20000]:
+        ci = cell[i]
+        for dz in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dx in (-1, 0, 1):
+                    c = (ci + (dx, dy, dz)) % nc
+                    k = (c[2] * nc + c[1]) * nc + c[0]
+                    js = order[start[k]:end[k]]
+                    js = js[js != i]
+                    if js.size == 0:
+                        continue
+                    d = pos[js] - pos[i]
+                    d -= L * np.round(d / L)
+                    dist = np.sqrt((d * d).sum(1))
+                    ov = radius[js] + radius[i] - dist
+                    best = max(best, float(ov.max()))
+    return best

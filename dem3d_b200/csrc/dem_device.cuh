@@ -1,0 +1,304 @@
+// dem_device.cuh -- device-side data layout and the exact FP64 pair model.
+//
+// Everything in this header that touches a floating-point value reproduces the
+// reference's Fortran expression operation by operation (the file is compiled
+// with -fmad=false so that no multiply-add is fused), which is what lets the
+// FP64 path match the CPU oracle bit for bit.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/dem3d_b200.h"
+
+namespace dem {
+
+constexpr int NCM = DEM_MAX_COMPONENTS;
+constexpr int NWM = DEM_MAX_WALLS;
+
+// Parameters resident in device memory (one copy per context).
+struct DevParams {
+  int nc, nw;
+  int pbc[3];
+  int nx, ny, nz, ncell;
+  int nprev;
+  int pad_;
+  double lbox[3], inv_lbox[3], gravity[3];
+  double nxbylx, nybyly, nzbylz, nxby2, nyby2, nzby2;
+  double ab0, am0, ab[3], am[3];
+  double comp_radius[NCM], comp_inv_mass[NCM], comp_inv_inertia[NCM], comp_eff_mass[NCM];
+  double min_dij[NCM * NCM], min_dij_sq[NCM * NCM];
+  double kn[NCM * NCM], yn[NCM * NCM], kt[NCM * NCM], yt[NCM * NCM], mu_sq[NCM * NCM];
+  double knw[NCM * NWM], ynw[NCM * NWM], ktw[NCM * NWM], ytw[NCM * NWM], muw_sq[NCM * NWM];
+  double pp_mass_coef, pp_density, pp_fluid_density;
+  double pp_kn, pp_kt, pp_gamma_n, pp_gamma_t, pp_mu_sq;
+  double pp_knw[NWM], pp_ktw[NWM], pp_gamma_nw[NWM], pp_gamma_tw[NWM], pp_muw_sq[NWM];
+  dem_wall walls[NWM];
+};
+
+// Per-particle master state in original index order (SoA, FP64).
+struct StateArrays {
+  double *px, *py, *pz, *vx, *vy, *vz, *wx, *wy, *wz, *ax, *ay, *az, *lx, *ly, *lz;
+};
+
+// Device counters (one cache line each is not needed: low traffic).
+struct Counters {
+  unsigned long long ncol;
+  unsigned long long ncol_pending;  // Ncol of the last history-updating pass
+  unsigned long long pair_contacts;
+  unsigned long long wall_contacts;
+  unsigned long long movers;
+  unsigned long long escaped;
+  int overflow;      // a particle needed more pair records than the capacity
+  int need_capacity; // largest record count requested
+  int abort;         // nonzero: later kernels of a captured sequence do nothing
+  int abort_tag;     // 1 + index (within a captured chunk) of the failing step
+  double wall_fn[NWM];
+};
+
+// Contact history, one table per buffer: records owned by imin.
+struct History {
+  int* cnt;       // [n] records owned by particle
+  int* key;       // [n*cap] partner (imax)
+  double2* val;   // [n*cap*3] (ft.x,ft.y) (ft.z,vt.x) (vt.y,vt.z)
+  int* wflag;     // [n*nw] wall record present
+  double2* wval;  // [n*nw*3]
+  int cap;
+};
+
+// Sorted (cell/traversal order) copies used by the force kernel.
+struct SortedArrays {
+  double4* pos;  // x, y, z, radius
+  double4* v4;   // vx, vy, vz, wx
+  double2* w2;   // wy, wz
+  int* comp;     // component (table mode)
+  int* orig;     // slot -> original index (also "order")
+  int* cell;     // slot -> cell
+};
+
+constexpr int EPI_STORE = 0;    // store a/alpha into the target arrays only
+constexpr int EPI_PREDICT = 1;  // MoveParticles predictor (pass 1)
+constexpr int EPI_CORRECT = 2;  // MoveParticles corrector (pass 2)
+
+struct RingMap {
+  int phys[5];  // phys[k] = physical slot of logical ipc(k+1); phys[nprev] = spare
+};
+
+struct ForceArgs {
+  const DevParams* P;
+  int n;
+  SortedArrays S;
+  const int* cell_start;
+  const int* cell_of_orig;
+  History Hr, Hw;
+  int update;
+  double half_dt;
+  StateArrays tgt;   // where a/alpha go (EPI_STORE)
+  StateArrays part;  // Particle
+  StateArrays pred;  // Predicted
+  double* ring;      // [(slot*9 + comp)*n + orig]
+  RingMap rm;
+  Counters* cnt;
+  int tag;  // index of this step within a captured chunk
+};
+
+// ------------------------------------------------------------------------
+// exact helpers (left-to-right sums as gfortran evaluates sum/dot_product)
+
+__device__ __forceinline__ double dot3(const double a[3], const double b[3]) {
+  double c = 0.0;
+  c = c + a[0] * b[0];
+  c = c + a[1] * b[1];
+  c = c + a[2] * b[2];
+  return c;
+}
+__device__ __forceinline__ double sumsq3(const double a[3]) {
+  double c = 0.0;
+  c = c + a[0] * a[0];
+  c = c + a[1] * a[1];
+  c = c + a[2] * a[2];
+  return c;
+}
+__device__ __forceinline__ void cross3(const double a[3], const double b[3], double c[3]) {
+  double c0 = a[1] * b[2] - a[2] * b[1];
+  double c1 = a[2] * b[0] - a[0] * b[2];
+  double c2 = a[0] * b[1] - a[1] * b[0];
+  c[0] = c0;
+  c[1] = c1;
+  c[2] = c2;
+}
+// Fortran nint to default integer, then back to real(8)
+__device__ __forceinline__ double fnint(double x) { return (double)(int)round(x); }
+
+__device__ __forceinline__ void change_plane(const double V[3], const double N[3], double out[3]) {
+  // ChangePlane, src/MForces.f90:391-406
+  double d = dot3(V, N);
+  double P[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) P[k] = V[k] - d * N[k];
+  double NormSq = sumsq3(P);
+  if (NormSq != 0.0) {
+    double f = sqrt(sumsq3(V) / NormSq);
+#pragma unroll
+    for (int k = 0; k < 3; k++) out[k] = f * P[k];
+  } else {
+    out[0] = out[1] = out[2] = 0.0;
+  }
+}
+
+struct PairPar {
+  double min_dij, min_dij_sq, kn, yn, kt, yt, mu_sq;
+};
+
+// Result of CommonCalculations for one contact, in the orientation used.
+struct ContactOut {
+  double FN[3], FT[3], VT[3], N[3], NxFT[3];
+};
+
+// CommonCalculations (src/MForces.f90:339-387) given the contact geometry.
+// Vij is the centre relative velocity (used only for the new-contact
+// PartialDt), VijC the contact relative velocity.
+__device__ __forceinline__ void common_calc(const double Rij[3], const double Nij[3],
+                                            const double DispN[3], const double Vij[3],
+                                            const double VijC[3], double DeltaDijSq,
+                                            double half_dt, bool contacting,
+                                            const double FT0[3], const double VT0in[3],
+                                            double Kn, double Yn, double Kt, double Yt,
+                                            double MuSq, ContactOut& o) {
+  double VijN[3];
+  double d = dot3(VijC, Nij);
+#pragma unroll
+  for (int k = 0; k < 3; k++) VijN[k] = d * Nij[k];
+#pragma unroll
+  for (int k = 0; k < 3; k++) o.VT[k] = VijC[k] - VijN[k];
+#pragma unroll
+  for (int k = 0; k < 3; k++) o.FN[k] = Kn * DispN[k] + Yn * VijN[k];
+  if (contacting) {
+    double VT0[3], cp[3], dD[3], dV[3];
+    change_plane(VT0in, Nij, VT0);
+#pragma unroll
+    for (int k = 0; k < 3; k++) dD[k] = half_dt * (VT0[k] + o.VT[k]);
+#pragma unroll
+    for (int k = 0; k < 3; k++) dV[k] = o.VT[k] - VT0[k];
+    change_plane(FT0, Nij, cp);
+#pragma unroll
+    for (int k = 0; k < 3; k++) o.FT[k] = cp[k] + Kt * dD[k] + Yt * dV[k];
+  } else {
+    double PartialDt;
+    double VijSq = sumsq3(Vij);
+    if (VijSq > 0.0) {
+      double RijVij = dot3(Rij, Vij);
+      double a = 2.0 * half_dt;
+      double b = (RijVij + sqrt(RijVij * RijVij + VijSq * DeltaDijSq)) / VijSq;
+      PartialDt = b < a ? b : a;
+    } else {
+      PartialDt = 0.0;
+    }
+    double f = Kt * PartialDt + Yt;
+#pragma unroll
+    for (int k = 0; k < 3; k++) o.FT[k] = f * o.VT[k];
+  }
+  double MuNormForceNSq = MuSq * sumsq3(o.FN);
+  double NormForceTSq = sumsq3(o.FT);
+  if (NormForceTSq > MuNormForceNSq) {
+    double f = sqrt(MuNormForceNSq / NormForceTSq);
+#pragma unroll
+    for (int k = 0; k < 3; k++) o.FT[k] = f * o.FT[k];
+  }
+#pragma unroll
+  for (int k = 0; k < 3; k++) o.N[k] = Nij[k];
+  cross3(Nij, o.FT, o.NxFT);
+}
+
+// The particle-particle branch of ComputeAccelerations (src/MForces.f90:
+// 230-252) for an overlapping pair, "i" = a, "j" = b, Rij = xb - xa (minimum
+// image), already tested DeltaDijSq > 0.
+__device__ __forceinline__ void pair_contact(const double Rij[3], double DijSq,
+                                             double DeltaDijSq, const PairPar& pp,
+                                             double Ra, const double va[3], const double wa[3],
+                                             double Rb, const double vb[3], const double wb[3],
+                                             double half_dt, bool contacting,
+                                             const double FT0[3], const double VT0[3],
+                                             ContactOut& o) {
+  double Dij = sqrt(DijSq);
+  double Nij[3], DispN[3], Vij[3], ws[3], cr[3], VijC[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) Nij[k] = Rij[k] / Dij;
+  double dn = Dij - pp.min_dij;
+#pragma unroll
+  for (int k = 0; k < 3; k++) DispN[k] = dn * Nij[k];
+#pragma unroll
+  for (int k = 0; k < 3; k++) Vij[k] = vb[k] - va[k];
+#pragma unroll
+  for (int k = 0; k < 3; k++) ws[k] = Ra * wa[k] + Rb * wb[k];
+  cross3(ws, Nij, cr);
+#pragma unroll
+  for (int k = 0; k < 3; k++) VijC[k] = Vij[k] - cr[k];
+  common_calc(Rij, Nij, DispN, Vij, VijC, DeltaDijSq, half_dt, contacting, FT0, VT0, pp.kn,
+              pp.yn, pp.kt, pp.yt, pp.mu_sq, o);
+}
+
+// Rectangle branch of Overlap (src/MConfig.f90:709-749).
+__device__ __forceinline__ bool overlap_rect(const DevParams& P, const dem_wall& w,
+                                             const double x[3], double Ri, double& Dij,
+                                             double Nij[3], double Qji[3]) {
+  double Rij[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    Rij[k] = w.position[k] - x[k];
+    if (P.pbc[k]) Rij[k] = Rij[k] - P.lbox[k] * fnint(Rij[k] * P.inv_lbox[k]);
+  }
+  double AlphaN = dot3(Rij, w.n);
+  double absAlphaN = fabs(AlphaN);
+  bool ov = absAlphaN < Ri;
+  if (ov) {
+    double AlphaU = dot3(Rij, w.u);
+    double AlphaW = dot3(Rij, w.w);
+    double absAlphaU = fabs(AlphaU);
+    double absAlphaW = fabs(AlphaW);
+    ov = (absAlphaU < w.l1 + Ri) && (absAlphaW < w.l2 + Ri);
+    if (ov) {
+      if (absAlphaU < w.l1 && absAlphaW < w.l2) {
+        double s = copysign(1.0, AlphaN);
+#pragma unroll
+        for (int k = 0; k < 3; k++) Nij[k] = s * w.n[k];
+        Dij = absAlphaN;
+#pragma unroll
+        for (int k = 0; k < 3; k++) Qji[k] = -(AlphaU * w.u[k] + AlphaW * w.w[k]);
+      } else {
+        double mu = -w.l1, mw = -w.l2;
+        AlphaU = AlphaU < w.l1 ? AlphaU : w.l1;
+        AlphaU = mu > AlphaU ? mu : AlphaU;
+        AlphaW = AlphaW < w.l2 ? AlphaW : w.l2;
+        AlphaW = mw > AlphaW ? mw : AlphaW;
+#pragma unroll
+        for (int k = 0; k < 3; k++) Qji[k] = -(AlphaU * w.u[k] + AlphaW * w.w[k]);
+#pragma unroll
+        for (int k = 0; k < 3; k++) Nij[k] = Rij[k] + Qji[k];
+        double DijSq = sumsq3(Nij);
+        ov = DijSq < Ri * Ri;
+        if (ov) {
+          Dij = sqrt(DijSq);
+#pragma unroll
+          for (int k = 0; k < 3; k++) Nij[k] = Nij[k] / Dij;
+        }
+      }
+    }
+  }
+  return ov;
+}
+
+// CurrentCell3D (src/MCells.f90:498-513), 0-based.
+__device__ __forceinline__ int current_cell(const DevParams& P, double x, double y, double z) {
+  int ix = (int)(P.nxbylx * x + P.nxby2);
+  int iy = (int)(P.nybyly * y + P.nyby2);
+  int iz = (int)(P.nzbylz * z + P.nzby2);
+  ix = ix < P.nx - 1 ? ix : P.nx - 1;
+  iy = iy < P.ny - 1 ? iy : P.ny - 1;
+  iz = iz < P.nz - 1 ? iz : P.nz - 1;
+  ix = ix > 0 ? ix : 0;
+  iy = iy > 0 ? iy : 0;
+  iz = iz > 0 ? iz : 0;
+  return ix + (iy + iz * P.ny) * P.nx;
+}
+
+}  // namespace dem

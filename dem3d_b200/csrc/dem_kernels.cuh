@@ -1,0 +1,856 @@
+// dem_kernels.cuh -- sm_100a kernels of the FP64 DEM step.
+//
+// K1  cell rebuild = counting sort of particles by cell hash into traversal
+//     order (k_assign -> scan -> k_scatter -> k_cellsort -> k_gather).
+//     Within a cell the order is exactly the reference's linked-list order:
+//     RedistributeParticles3D (src/MCells.f90:607-643) walks particles in
+//     index order and prepends every particle that changed cell
+//     (TransferParticle, :747-774), so a cell lists first the particles that
+//     entered it during this pass (highest index first) and then the ones that
+//     stayed, in their previous order.  The sort key encodes exactly that.
+// K2+K4 force kernel: one thread per particle in traversal order gathers its
+//     contacts (no atomics), evaluates every pair in the reference's
+//     orientation ("i" = the particle visited first) and adds the
+//     contributions in the order of the reference's cell sweep, so that the
+//     forces are bit-identical to ComputeAccelerations (src/MForces.f90:
+//     145-335).  The AB predictor / AM corrector (src/MDEM.f90:296-365) run in
+//     the same kernel's epilogue.
+// K3  history: records owned by imin are double-buffered; a pass that updates
+//     them writes a fresh table (new/updated contacts + records of pairs that
+//     the sweep did not visit, as the reference keeps those untouched).
+#pragma once
+#include "dem_device.cuh"
+
+namespace dem {
+
+// ---------------------------------------------------------------------------
+// warp helpers
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// K1: cell rebuild
+
+// One thread per current slot: new cell, mover flag, sort key, slot in cell.
+__global__ void k_assign(const DevParams* __restrict__ Pp, int n, int initial,
+                         const double* __restrict__ px, const double* __restrict__ py,
+                         const double* __restrict__ pz, const int* __restrict__ order,
+                         const int* __restrict__ old_cell, int* __restrict__ cell_cnt,
+                         int* __restrict__ a_cell, int* __restrict__ a_loc,
+                         unsigned* __restrict__ a_key, int* __restrict__ a_orig,
+                         Counters* __restrict__ cnt) {
+  if (cnt->abort) return;
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s == 0 && cnt->ncol_pending) {
+    // the previous history-updating pass completed: its Ncol counts
+    cnt->ncol += cnt->ncol_pending;
+    cnt->ncol_pending = 0;
+  }
+  unsigned long long mv = 0;
+  if (s < n) {
+    const DevParams& P = *Pp;
+    int orig = initial ? s : order[s];
+    int c = current_cell(P, px[orig], py[orig], pz[orig]);
+    int old = initial ? -1 : old_cell[s];
+    bool mover = c != old;
+    unsigned key = mover ? (unsigned)(n - 1 - orig) : (unsigned)(n + s);
+    int loc = atomicAdd(&cell_cnt[c], 1);
+    a_cell[s] = c;
+    a_loc[s] = loc;
+    a_key[s] = key;
+    a_orig[s] = orig;
+    mv = mover ? 1ull : 0ull;
+  }
+  mv = warp_sum_u64(mv);
+  if ((threadIdx.x & 31) == 0 && mv) atomicAdd(&cnt->movers, mv);
+}
+
+// exclusive scan, phase 1: tiles of 4*blockDim elements
+constexpr int SCAN_THREADS = 1024;
+constexpr int SCAN_ITEMS = 4;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* sh_warp, int& total) {
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sh_warp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int nw = blockDim.x >> 5;
+    int w = lane < nw ? sh_warp[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < nw) sh_warp[lane] = w;
+  }
+  __syncthreads();
+  int warp_prefix = warp > 0 ? sh_warp[warp - 1] : 0;
+  total = sh_warp[(blockDim.x >> 5) - 1];
+  return warp_prefix + x - v;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_tiles(const int* __restrict__ in, int m,
+                                                             int* __restrict__ out,
+                                                             int* __restrict__ bsum,
+                                                             const Counters* __restrict__ cnt) {
+  if (cnt->abort) return;
+  __shared__ int sh[32];
+  int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+  int v[SCAN_ITEMS];
+  int t = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    v[k] = base + k < m ? in[base + k] : 0;
+    t += v[k];
+  }
+  int total;
+  int ex = block_exclusive_scan(t, sh, total);
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    if (base + k < m) out[base + k] = ex;
+    ex += v[k];
+  }
+  if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+// phase 2: one block scans the tile sums in chunks (carry kept in a register)
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_bsums(int* __restrict__ bsum, int nb,
+                                                             int* __restrict__ out, int m,
+                                                             const Counters* __restrict__ cnt) {
+  if (cnt->abort) return;
+  __shared__ int sh[32];
+  int carry = 0;
+  for (int b0 = 0; b0 < nb; b0 += SCAN_THREADS) {
+    int i = b0 + threadIdx.x;
+    int v = i < nb ? bsum[i] : 0;
+    int total;
+    int ex = block_exclusive_scan(v, sh, total);
+    if (i < nb) bsum[i] = ex + carry;
+    carry += total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[m] = carry;
+}
+
+// phase 3: add tile offsets
+__global__ void k_scan_add(int* __restrict__ out, int m, const int* __restrict__ bsum,
+                           const Counters* __restrict__ cnt) {
+  if (cnt->abort) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) out[i] += bsum[i / SCAN_TILE];
+}
+
+__global__ void k_scatter(int n, const int* __restrict__ a_cell, const int* __restrict__ a_loc,
+                          const unsigned* __restrict__ a_key, const int* __restrict__ a_orig,
+                          const int* __restrict__ cell_start, unsigned* __restrict__ t_key,
+                          int* __restrict__ t_orig, const Counters* __restrict__ cnt) {
+  if (cnt->abort) return;
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  int d = cell_start[a_cell[s]] + a_loc[s];
+  t_key[d] = a_key[s];
+  t_orig[d] = a_orig[s];
+}
+
+// One thread per cell: order the members by key (insertion sort; the keys
+// are unique and nearly always already sorted), publish order/cell maps.
+__global__ void k_cellsort(int ncell, const int* __restrict__ cell_start,
+                           unsigned* __restrict__ t_key, int* __restrict__ t_orig,
+                           int* __restrict__ order, int* __restrict__ slot_cell,
+                           int* __restrict__ cell_of_orig, const Counters* __restrict__ cnt) {
+  if (cnt->abort) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  int b = cell_start[c], e = cell_start[c + 1];
+  for (int i = b + 1; i < e; i++) {
+    unsigned k = t_key[i];
+    int o = t_orig[i];
+    int j = i - 1;
+    while (j >= b && t_key[j] > k) {
+      t_key[j + 1] = t_key[j];
+      t_orig[j + 1] = t_orig[j];
+      j--;
+    }
+    t_key[j + 1] = k;
+    t_orig[j + 1] = o;
+  }
+  for (int i = b; i < e; i++) {
+    int o = t_orig[i];
+    order[i] = o;
+    slot_cell[i] = c;
+    cell_of_orig[o] = c;
+  }
+}
+
+// Copy the source state into traversal order (the "SoA reorder").
+template <bool PP>
+__global__ void k_gather(const DevParams* __restrict__ Pp, int n, StateArrays src,
+                         const double* __restrict__ radius, const int* __restrict__ comp,
+                         SortedArrays S, const Counters* __restrict__ cnt) {
+  if (cnt->abort) return;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  int o = S.orig[t];
+  double R;
+  if (PP) {
+    R = radius[o];
+  } else {
+    int k = comp[o];
+    S.comp[t] = k;
+    R = Pp->comp_radius[k];
+  }
+  S.pos[t] = make_double4(src.px[o], src.py[o], src.pz[o], R);
+  S.v4[t] = make_double4(src.vx[o], src.vy[o], src.vz[o], src.wx[o]);
+  S.w2[t] = make_double2(src.wy[o], src.wz[o]);
+}
+
+// ---------------------------------------------------------------------------
+// material helpers
+
+template <bool PP>
+struct Material;
+
+template <>
+struct Material<false> {
+  __device__ __forceinline__ static void pair(const DevParams& P, int ca, double, int cb, double,
+                                              PairPar& pp) {
+    int k = ca * NCM + cb;
+    pp.min_dij = P.min_dij[k];
+    pp.min_dij_sq = P.min_dij_sq[k];
+    pp.kn = P.kn[k];
+    pp.yn = P.yn[k];
+    pp.kt = P.kt[k];
+    pp.yt = P.yt[k];
+    pp.mu_sq = P.mu_sq[k];
+  }
+  __device__ __forceinline__ static double min_dij_sq(const DevParams& P, int ca, double, int cb,
+                                                      double) {
+    return P.min_dij_sq[ca * NCM + cb];
+  }
+  __device__ __forceinline__ static void wall(const DevParams& P, int ca, double, int w,
+                                              PairPar& pp) {
+    int k = ca * NWM + w;
+    pp.kn = P.knw[k];
+    pp.yn = P.ynw[k];
+    pp.kt = P.ktw[k];
+    pp.yt = P.ytw[k];
+    pp.mu_sq = P.muw_sq[k];
+  }
+  __device__ __forceinline__ static void self(const DevParams& P, int ca, double, double& inv_m,
+                                              double& inv_i, double& eff_m) {
+    inv_m = P.comp_inv_mass[ca];
+    inv_i = P.comp_inv_inertia[ca];
+    eff_m = P.comp_eff_mass[ca];
+  }
+};
+
+template <>
+struct Material<true> {
+  __device__ __forceinline__ static double mass(const DevParams& P, double R) {
+    return P.pp_mass_coef * ((R * R) * R);
+  }
+  __device__ __forceinline__ static void pair(const DevParams& P, int, double Ra, int, double Rb,
+                                              PairPar& pp) {
+    double ma = mass(P, Ra), mb = mass(P, Rb);
+    double meff = (ma * mb) / (ma + mb);
+    pp.min_dij = Ra + Rb;
+    pp.min_dij_sq = pp.min_dij * pp.min_dij;
+    pp.kn = P.pp_kn;
+    pp.yn = P.pp_gamma_n * sqrt(meff * P.pp_kn);
+    pp.kt = P.pp_kt;
+    pp.yt = P.pp_gamma_t * sqrt(meff * P.pp_kt);
+    pp.mu_sq = P.pp_mu_sq;
+  }
+  __device__ __forceinline__ static double min_dij_sq(const DevParams&, int, double Ra, int,
+                                                      double Rb) {
+    double d = Ra + Rb;
+    return d * d;
+  }
+  __device__ __forceinline__ static void wall(const DevParams& P, int, double Ra, int w,
+                                              PairPar& pp) {
+    double m = mass(P, Ra);
+    pp.kn = P.pp_knw[w];
+    pp.yn = P.pp_gamma_nw[w] * sqrt(m * P.pp_knw[w]);
+    pp.kt = P.pp_ktw[w];
+    pp.yt = P.pp_gamma_tw[w] * sqrt(m * P.pp_ktw[w]);
+    pp.mu_sq = P.pp_muw_sq[w];
+  }
+  __device__ __forceinline__ static void self(const DevParams& P, int, double R, double& inv_m,
+                                              double& inv_i, double& eff_m) {
+    double m = mass(P, R);
+    inv_m = 1.0 / m;
+    inv_i = 1.0 / ((0.4 * m) * (R * R));
+    eff_m = (m * (P.pp_density - P.pp_fluid_density)) / P.pp_density;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// history access
+
+__device__ __forceinline__ int hist_find(const History& H, int owner, int partner) {
+  int c = H.cnt[owner];
+  const int* k = H.key + (size_t)owner * H.cap;
+  for (int r = 0; r < c; r++)
+    if (k[r] == partner) return r;
+  return -1;
+}
+
+__device__ __forceinline__ void hist_read(const History& H, int owner, int r, double ft[3],
+                                          double vt[3]) {
+  const double2* v = H.val + ((size_t)owner * H.cap + r) * 3;
+  double2 a = v[0], b = v[1], c = v[2];
+  ft[0] = a.x; ft[1] = a.y; ft[2] = b.x;
+  vt[0] = b.y; vt[1] = c.x; vt[2] = c.y;
+}
+
+__device__ __forceinline__ void hist_write(const History& H, int owner, int r, int partner,
+                                           const double ft[3], const double vt[3]) {
+  H.key[(size_t)owner * H.cap + r] = partner;
+  double2* v = H.val + ((size_t)owner * H.cap + r) * 3;
+  v[0] = make_double2(ft[0], ft[1]);
+  v[1] = make_double2(ft[2], vt[0]);
+  v[2] = make_double2(vt[1], vt[2]);
+}
+
+// Are two cells neighbours in the sweep sense (same cell, or one in the
+// other's half-shell list)?  With >= 3 cells along every periodic axis this
+// is plain adjacency with wrap-around (VerifyPBC/ApplyPBC, src/MCells.f90:
+// 1030-1052).
+__device__ __forceinline__ bool cells_adjacent(const DevParams& P, int a, int b) {
+  int ax = a % P.nx, ay = (a / P.nx) % P.ny, az = a / (P.nx * P.ny);
+  int bx = b % P.nx, by = (b / P.nx) % P.ny, bz = b / (P.nx * P.ny);
+  int d[3] = {bx - ax, by - ay, bz - az};
+  int N[3] = {P.nx, P.ny, P.nz};
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    int x = d[k] < 0 ? -d[k] : d[k];
+    if (x > 1 && !(P.pbc[k] && x == N[k] - 1)) return false;
+  }
+  return true;
+}
+
+// axis helper: neighbour offsets of a cell coordinate, trimmed like VerifyPBC
+__device__ __forceinline__ void axis_range(int i, int N, int pbc, int& lo, int& hi) {
+  lo = -1;
+  hi = 1;
+  if (!pbc) {
+    if (i == 0) lo = 0;
+    if (i == N - 1) hi = 0;
+  }
+}
+__device__ __forceinline__ int axis_wrap(int j, int N, int pbc) {
+  if (pbc) {
+    if (j == N) j = 0;
+    if (j == -1) j = N - 1;
+  }
+  return j;
+}
+// offsets of one axis in ascending order of the wrapped cell coordinate
+__device__ __forceinline__ int axis_sorted(int i, int N, int pbc, int off[3]) {
+  int lo, hi;
+  axis_range(i, N, pbc, lo, hi);
+  int m = 0;
+  if (pbc && i == 0) {  // -1 wraps to N-1 (largest)
+    off[m++] = 0;
+    off[m++] = 1;
+    off[m++] = -1;
+  } else if (pbc && i == N - 1) {  // +1 wraps to 0 (smallest)
+    off[m++] = 1;
+    off[m++] = -1;
+    off[m++] = 0;
+  } else {
+    for (int k = lo; k <= hi; k++) off[m++] = k;
+  }
+  return m;
+}
+
+// ---------------------------------------------------------------------------
+// K2+K4: force kernel (FP64, exact order)
+
+
+template <bool PP, int EPI>
+__global__ void __launch_bounds__(128) k_force_fp64(ForceArgs A) {
+  if (A.cnt->abort) return;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long n_col = 0, n_pc = 0, n_wc = 0;
+  int need = 0;
+  if (s < A.n) {
+    const DevParams& P = *A.P;
+    const SortedArrays& S = A.S;
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const int c = S.cell[s];
+    const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
+    const double4 p4 = S.pos[s];
+    const double xp[3] = {p4.x, p4.y, p4.z};
+    const double Rp = p4.w;
+    const double4 pv4 = S.v4[s];
+    const double2 pw2 = S.w2[s];
+    const double vp[3] = {pv4.x, pv4.y, pv4.z};
+    const double wp[3] = {pv4.w, pw2.x, pw2.y};
+    const int orig = S.orig[s];
+    const int cp = PP ? 0 : S.comp[s];
+    double inv_m, inv_i, eff_m;
+    Material<PP>::self(P, cp, Rp, inv_m, inv_i, eff_m);
+    const double half_dt = A.half_dt;
+    const bool update = A.update != 0;
+    int hw_n = 0;
+    bool overflow = false;
+
+    double iF[3], iT[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < 3; k++) iF[k] = eff_m * P.gravity[k];
+
+    auto record = [&](int partner, const double ft[3], const double vt[3]) {
+      if (hw_n < A.Hw.cap)
+        hist_write(A.Hw, orig, hw_n, partner, ft, vt);
+      else
+        overflow = true;
+      hw_n++;
+    };
+
+    // p is "i", slot t is "j" (src/MForces.f90:199-272)
+    auto visit_i = [&](int t) {
+      const double4 q4 = S.pos[t];
+      double Rij[3] = {q4.x - xp[0], q4.y - xp[1], q4.z - xp[2]};
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+        if (P.pbc[k]) Rij[k] = Rij[k] - P.lbox[k] * fnint(Rij[k] * P.inv_lbox[k]);
+      const double DijSq = sumsq3(Rij);
+      const int cq = PP ? 0 : S.comp[t];
+      const double Delta = Material<PP>::min_dij_sq(P, cp, Rp, cq, q4.w) - DijSq;
+      if (Delta > 0.0) {
+        PairPar pp;
+        Material<PP>::pair(P, cp, Rp, cq, q4.w, pp);
+        const int qo = S.orig[t];
+        const double4 qv4 = S.v4[t];
+        const double2 qw2 = S.w2[t];
+        const double vq[3] = {qv4.x, qv4.y, qv4.z};
+        const double wq[3] = {qv4.w, qw2.x, qw2.y};
+        const int lo = orig < qo ? orig : qo, hi = orig < qo ? qo : orig;
+        double FT0[3] = {0.0, 0.0, 0.0}, VT0[3] = {0.0, 0.0, 0.0};
+        int r = hist_find(A.Hr, lo, hi);
+        bool contacting = r >= 0;
+        if (contacting) hist_read(A.Hr, lo, r, FT0, VT0);
+        if (!contacting) n_col++;
+        n_pc++;
+        ContactOut o;
+        pair_contact(Rij, DijSq, Delta, pp, Rp, vp, wp, q4.w, vq, wq, half_dt, contacting, FT0,
+                     VT0, o);
+#pragma unroll
+        for (int k = 0; k < 3; k++) iF[k] = iF[k] + o.FN[k] + o.FT[k];
+        double RN[3], tq[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) RN[k] = Rp * o.N[k];
+        cross3(RN, o.FT, tq);
+#pragma unroll
+        for (int k = 0; k < 3; k++) iT[k] = iT[k] + tq[k];
+        if (update && orig < qo) record(qo, o.FT, o.VT);
+      }
+    };
+
+    // ---- loop 1: own cell after p, then the half-shell cells in the order
+    // of the FirstNeighbour list (reverse of AddAllNeighbours3D insertion)
+    {
+      const int e = A.cell_start[c + 1];
+      for (int t = s + 1; t < e; t++) visit_i(t);
+      int xi, xf, yi, yf, zi, zf;
+      axis_range(cx, nx, P.pbc[0], xi, xf);
+      axis_range(cy, ny, P.pbc[1], yi, yf);
+      axis_range(cz, nz, P.pbc[2], zi, zf);
+      for (int kz = zf; kz >= zi; kz--) {
+        const int jz = axis_wrap(cz + kz, nz, P.pbc[2]);
+        for (int ky = yf; ky >= yi; ky--) {
+          const int jy = axis_wrap(cy + ky, ny, P.pbc[1]);
+          for (int kx = xf; kx >= xi; kx--) {
+            if (kx + nx * (ky + ny * kz) <= 0) continue;
+            const int jx = axis_wrap(cx + kx, nx, P.pbc[0]);
+            const int jc = jx + nx * (jy + ny * jz);
+            const int b = A.cell_start[jc], e2 = A.cell_start[jc + 1];
+            for (int t = b; t < e2; t++) visit_i(t);
+          }
+        }
+      }
+    }
+
+    // ---- walls (src/MForces.f90:274-314)
+    for (int w = 0; w < P.nw; w++) {
+      const dem_wall& W = P.walls[w];
+      const int wi = orig * P.nw + w;
+      bool contacting = A.Hr.wflag[wi] != 0;
+      double FT0[3] = {0.0, 0.0, 0.0}, VT0[3] = {0.0, 0.0, 0.0};
+      if (contacting) {
+        const double2* v = A.Hr.wval + (size_t)wi * 3;
+        double2 a = v[0], b = v[1], d = v[2];
+        FT0[0] = a.x; FT0[1] = a.y; FT0[2] = b.x;
+        VT0[0] = b.y; VT0[1] = d.x; VT0[2] = d.y;
+      }
+      double Dij, Nij[3], Qji[3];
+      bool ov = false;
+      if (W.shape == DEM_WALL_RECTANGLE) ov = overlap_rect(P, W, xp, Rp, Dij, Nij, Qji);
+      if (ov) {
+        n_wc++;
+        const double Delta = Rp * Rp - Dij * Dij;
+        const double dn = Dij - Rp;
+        double DispN[3], wqv[3], Vij[3], ro[3], cr[3], VijC[3], Rw[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) DispN[k] = dn * Nij[k];
+        cross3(W.omega, Qji, wqv);
+#pragma unroll
+        for (int k = 0; k < 3; k++) Vij[k] = W.velocity[k] + wqv[k] - vp[k];
+#pragma unroll
+        for (int k = 0; k < 3; k++) ro[k] = Rp * wp[k];
+        cross3(ro, Nij, cr);
+#pragma unroll
+        for (int k = 0; k < 3; k++) VijC[k] = Vij[k] - cr[k];
+#pragma unroll
+        for (int k = 0; k < 3; k++) Rw[k] = W.position[k] + Qji[k] - xp[k];
+        PairPar pp;
+        Material<PP>::wall(P, cp, Rp, w, pp);
+        ContactOut o;
+        common_calc(Rw, Nij, DispN, Vij, VijC, Delta, half_dt, contacting, FT0, VT0, pp.kn, pp.yn,
+                    pp.kt, pp.yt, pp.mu_sq, o);
+#pragma unroll
+        for (int k = 0; k < 3; k++) iF[k] = iF[k] + o.FN[k] + o.FT[k];
+        double RN[3], tq[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) RN[k] = Rp * o.N[k];
+        cross3(RN, o.FT, tq);
+#pragma unroll
+        for (int k = 0; k < 3; k++) iT[k] = iT[k] + tq[k];
+        atomicAdd(&A.cnt->wall_fn[w], sqrt(sumsq3(o.FN)));
+        if (update) {
+          A.Hw.wflag[wi] = 1;
+          double2* v = A.Hw.wval + (size_t)wi * 3;
+          v[0] = make_double2(o.FT[0], o.FT[1]);
+          v[1] = make_double2(o.FT[2], o.VT[0]);
+          v[2] = make_double2(o.VT[1], o.VT[2]);
+        }
+      } else if (update) {
+        A.Hw.wflag[wi] = 0;
+      }
+    }
+
+    // ---- loop 2: p as "j"; contributions in traversal order of the "i"
+    // particle, own block (Force(i) = Force(i) + iForce) at p's position.
+    double F[3] = {0.0, 0.0, 0.0}, T[3] = {0.0, 0.0, 0.0};
+    auto visit_j = [&](int t) {
+      const double4 q4 = S.pos[t];
+      double Rij[3] = {xp[0] - q4.x, xp[1] - q4.y, xp[2] - q4.z};
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+        if (P.pbc[k]) Rij[k] = Rij[k] - P.lbox[k] * fnint(Rij[k] * P.inv_lbox[k]);
+      const double DijSq = sumsq3(Rij);
+      const int cq = PP ? 0 : S.comp[t];
+      const double Delta = Material<PP>::min_dij_sq(P, cq, q4.w, cp, Rp) - DijSq;
+      if (Delta > 0.0) {
+        PairPar pp;
+        Material<PP>::pair(P, cq, q4.w, cp, Rp, pp);
+        const int qo = S.orig[t];
+        const double4 qv4 = S.v4[t];
+        const double2 qw2 = S.w2[t];
+        const double vq[3] = {qv4.x, qv4.y, qv4.z};
+        const double wq[3] = {qv4.w, qw2.x, qw2.y};
+        const int lo = orig < qo ? orig : qo, hi = orig < qo ? qo : orig;
+        double FT0[3] = {0.0, 0.0, 0.0}, VT0[3] = {0.0, 0.0, 0.0};
+        int r = hist_find(A.Hr, lo, hi);
+        bool contacting = r >= 0;
+        if (contacting) hist_read(A.Hr, lo, r, FT0, VT0);
+        ContactOut o;
+        pair_contact(Rij, DijSq, Delta, pp, q4.w, vq, wq, Rp, vp, wp, half_dt, contacting, FT0,
+                     VT0, o);
+#pragma unroll
+        for (int k = 0; k < 3; k++) F[k] = F[k] - o.FN[k] - o.FT[k];
+#pragma unroll
+        for (int k = 0; k < 3; k++) T[k] = T[k] + Rp * o.NxFT[k];
+        if (update && orig < qo) record(qo, o.FT, o.VT);
+      }
+    };
+    {
+      int ox[3], oy[3], oz[3];
+      const int mx = axis_sorted(cx, nx, P.pbc[0], ox);
+      const int my = axis_sorted(cy, ny, P.pbc[1], oy);
+      const int mz = axis_sorted(cz, nz, P.pbc[2], oz);
+      for (int a = 0; a < mz; a++) {
+        const int dz = oz[a];
+        const int jz = axis_wrap(cz + dz, nz, P.pbc[2]);
+        for (int b = 0; b < my; b++) {
+          const int dy = oy[b];
+          const int jy = axis_wrap(cy + dy, ny, P.pbc[1]);
+          for (int d = 0; d < mx; d++) {
+            const int dx = ox[d];
+            if (dx == 0 && dy == 0 && dz == 0) {
+              for (int t = A.cell_start[c]; t < s; t++) visit_j(t);
+#pragma unroll
+              for (int k = 0; k < 3; k++) F[k] = F[k] + iF[k];
+#pragma unroll
+              for (int k = 0; k < 3; k++) T[k] = T[k] + iT[k];
+              continue;
+            }
+            // lower neighbour: p's cell is in the half shell of that cell
+            if (-dx + nx * (-dy + ny * -dz) <= 0) continue;
+            const int jx = axis_wrap(cx + dx, nx, P.pbc[0]);
+            const int jc = jx + nx * (jy + ny * jz);
+            const int b0 = A.cell_start[jc], e2 = A.cell_start[jc + 1];
+            for (int t = b0; t < e2; t++) visit_j(t);
+          }
+        }
+      }
+    }
+
+    // ---- records of pairs the sweep did not visit are kept as they were
+    if (update) {
+      const int nold = A.Hr.cnt[orig];
+      for (int r = 0; r < nold; r++) {
+        const int q2 = A.Hr.key[(size_t)orig * A.Hr.cap + r];
+        if (!cells_adjacent(P, c, A.cell_of_orig[q2])) {
+          double ft[3], vt[3];
+          hist_read(A.Hr, orig, r, ft, vt);
+          record(q2, ft, vt);
+        }
+      }
+      A.Hw.cnt[orig] = hw_n < A.Hw.cap ? hw_n : A.Hw.cap;
+      if (overflow) {
+        // the pass is re-run with larger tables; stop everything after it
+        atomicExch(&A.cnt->overflow, 1);
+        atomicCAS(&A.cnt->abort_tag, 0, A.tag + 1);
+        atomicExch(&A.cnt->abort, 1);
+      }
+      need = hw_n;
+    }
+
+    // ---- a = F/m, alpha = T/I (src/MForces.f90:330-333) + epilogue
+    double acc[3], alp[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) acc[k] = F[k] * inv_m;
+#pragma unroll
+    for (int k = 0; k < 3; k++) alp[k] = T[k] * inv_i;
+
+    if (EPI == EPI_STORE) {
+      A.tgt.ax[orig] = acc[0]; A.tgt.ay[orig] = acc[1]; A.tgt.az[orig] = acc[2];
+      A.tgt.lx[orig] = alp[0]; A.tgt.ly[orig] = alp[1]; A.tgt.lz[orig] = alp[2];
+    } else if (EPI == EPI_PREDICT) {
+      // src/MDEM.f90:296-331: AB predictor from x(t), v(t), w(t) (the values
+      // this pass gathered) and the ring, then store (v,a,alpha)(t).
+      const StateArrays& Q = A.part;
+      const StateArrays& R = A.pred;
+      Q.ax[orig] = acc[0]; Q.ay[orig] = acc[1]; Q.az[orig] = acc[2];
+      Q.lx[orig] = alp[0]; Q.ly[orig] = alp[1]; Q.lz[orig] = alp[2];
+      double sv[3] = {0.0, 0.0, 0.0}, sa[3] = {0.0, 0.0, 0.0}, sl[3] = {0.0, 0.0, 0.0};
+      const size_t n = (size_t)A.n;
+      for (int k = 0; k < P.nprev; k++) {
+        const double ABk = P.ab[k];
+        const double* rg = A.ring + (size_t)A.rm.phys[k] * 9 * n + orig;
+#pragma unroll
+        for (int d = 0; d < 3; d++) sv[d] = sv[d] + ABk * rg[d * n];
+#pragma unroll
+        for (int d = 0; d < 3; d++) sa[d] = sa[d] + ABk * rg[(3 + d) * n];
+#pragma unroll
+        for (int d = 0; d < 3; d++) sl[d] = sl[d] + ABk * rg[(6 + d) * n];
+      }
+      double xr[3], vr[3], wr[3];
+#pragma unroll
+      for (int d = 0; d < 3; d++) xr[d] = xp[d] + P.ab0 * vp[d] + sv[d];
+#pragma unroll
+      for (int d = 0; d < 3; d++) vr[d] = vp[d] + P.ab0 * acc[d] + sa[d];
+#pragma unroll
+      for (int d = 0; d < 3; d++) wr[d] = wp[d] + P.ab0 * alp[d] + sl[d];
+#pragma unroll
+      for (int d = 0; d < 3; d++)
+        if (P.pbc[d]) xr[d] = xr[d] - P.lbox[d] * fnint(xr[d] * P.inv_lbox[d]);
+      R.px[orig] = xr[0]; R.py[orig] = xr[1]; R.pz[orig] = xr[2];
+      R.vx[orig] = vr[0]; R.vy[orig] = vr[1]; R.vz[orig] = vr[2];
+      R.wx[orig] = wr[0]; R.wy[orig] = wr[1]; R.wz[orig] = wr[2];
+      if (P.nprev > 0) {
+        double* rg = A.ring + (size_t)A.rm.phys[P.nprev] * 9 * n + orig;
+#pragma unroll
+        for (int d = 0; d < 3; d++) rg[d * n] = vp[d];
+#pragma unroll
+        for (int d = 0; d < 3; d++) rg[(3 + d) * n] = acc[d];
+#pragma unroll
+        for (int d = 0; d < 3; d++) rg[(6 + d) * n] = alp[d];
+      }
+    } else {  // EPI_CORRECT, src/MDEM.f90:340-367
+      const StateArrays& Q = A.part;
+      const StateArrays& R = A.pred;
+      R.ax[orig] = acc[0]; R.ay[orig] = acc[1]; R.az[orig] = acc[2];
+      R.lx[orig] = alp[0]; R.ly[orig] = alp[1]; R.lz[orig] = alp[2];
+      double sv[3] = {0.0, 0.0, 0.0}, sa[3] = {0.0, 0.0, 0.0}, sl[3] = {0.0, 0.0, 0.0};
+      const size_t n = (size_t)A.n;
+      for (int k = 0; k < P.nprev; k++) {
+        const double AMk = P.am[k];
+        const double* rg = A.ring + (size_t)A.rm.phys[k] * 9 * n + orig;
+#pragma unroll
+        for (int d = 0; d < 3; d++) sv[d] = sv[d] + AMk * rg[d * n];
+#pragma unroll
+        for (int d = 0; d < 3; d++) sa[d] = sa[d] + AMk * rg[(3 + d) * n];
+#pragma unroll
+        for (int d = 0; d < 3; d++) sl[d] = sl[d] + AMk * rg[(6 + d) * n];
+      }
+      double x[3] = {Q.px[orig], Q.py[orig], Q.pz[orig]};
+      double v[3] = {Q.vx[orig], Q.vy[orig], Q.vz[orig]};
+      double w[3] = {Q.wx[orig], Q.wy[orig], Q.wz[orig]};
+#pragma unroll
+      for (int d = 0; d < 3; d++) x[d] = x[d] + P.am0 * vp[d] + sv[d];
+#pragma unroll
+      for (int d = 0; d < 3; d++) v[d] = v[d] + P.am0 * acc[d] + sa[d];
+#pragma unroll
+      for (int d = 0; d < 3; d++) w[d] = w[d] + P.am0 * alp[d] + sl[d];
+#pragma unroll
+      for (int d = 0; d < 3; d++)
+        if (P.pbc[d]) x[d] = x[d] - P.lbox[d] * fnint(x[d] * P.inv_lbox[d]);
+      Q.px[orig] = x[0]; Q.py[orig] = x[1]; Q.pz[orig] = x[2];
+      Q.vx[orig] = v[0]; Q.vy[orig] = v[1]; Q.vz[orig] = v[2];
+      Q.wx[orig] = w[0]; Q.wy[orig] = w[1]; Q.wz[orig] = w[2];
+      bool out = false;
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const double h = 0.5 * P.lbox[d];
+        out = out || (x[d] > h) || (x[d] < -h);
+      }
+      if (out) atomicAdd(&A.cnt->escaped, 1ull);
+    }
+  }
+  n_col = warp_sum_u64(n_col);
+  n_pc = warp_sum_u64(n_pc);
+  n_wc = warp_sum_u64(n_wc);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) need = max(need, __shfl_down_sync(0xffffffffu, need, o));
+  if ((threadIdx.x & 31) == 0) {
+    if (need) atomicMax(&A.cnt->need_capacity, need);
+    if (n_col) atomicAdd(A.update ? &A.cnt->ncol_pending : &A.cnt->ncol, n_col);
+    if (n_pc) atomicAdd(&A.cnt->pair_contacts, n_pc);
+    if (n_wc) atomicAdd(&A.cnt->wall_contacts, n_wc);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// small per-particle kernels (original index order)
+
+// ring store of MoveParticlesEuler (src/MDEM.f90:266-271): (v,a,alpha) -> slot
+__global__ void k_ring_store(int n, StateArrays Q, double* __restrict__ ring, int slot,
+                             const Counters* __restrict__ cnt) {
+  if (cnt->abort) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double* rg = ring + (size_t)slot * 9 * n + i;
+  rg[0 * (size_t)n] = Q.vx[i]; rg[1 * (size_t)n] = Q.vy[i]; rg[2 * (size_t)n] = Q.vz[i];
+  rg[3 * (size_t)n] = Q.ax[i]; rg[4 * (size_t)n] = Q.ay[i]; rg[5 * (size_t)n] = Q.az[i];
+  rg[6 * (size_t)n] = Q.lx[i]; rg[7 * (size_t)n] = Q.ly[i]; rg[8 * (size_t)n] = Q.lz[i];
+}
+
+// explicit Euler update (src/MDEM.f90:240-252)
+__global__ void k_euler_update(int n, StateArrays Q, double dt, const Counters* __restrict__ cnt) {
+  if (cnt->abort) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double h2 = 0.5 * (dt * dt);
+  Q.px[i] = Q.px[i] + Q.vx[i] * dt + Q.ax[i] * h2;
+  Q.py[i] = Q.py[i] + Q.vy[i] * dt + Q.ay[i] * h2;
+  Q.pz[i] = Q.pz[i] + Q.vz[i] * dt + Q.az[i] * h2;
+  Q.vx[i] = Q.vx[i] + Q.ax[i] * dt;
+  Q.vy[i] = Q.vy[i] + Q.ay[i] * dt;
+  Q.vz[i] = Q.vz[i] + Q.az[i] * dt;
+  Q.wx[i] = Q.wx[i] + Q.lx[i] * dt;
+  Q.wy[i] = Q.wy[i] + Q.ly[i] * dt;
+  Q.wz[i] = Q.wz[i] + Q.lz[i] * dt;
+}
+
+// ApplyPeriodicBoundaryConditions (src/MDEM.f90:373-388)
+__global__ void k_apply_pbc(const DevParams* __restrict__ Pp, int n, StateArrays Q,
+                            const Counters* __restrict__ cnt) {
+  if (cnt->abort) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const DevParams& P = *Pp;
+  double* p[3] = {Q.px, Q.py, Q.pz};
+#pragma unroll
+  for (int d = 0; d < 3; d++)
+    if (P.pbc[d]) {
+      double x = p[d][i];
+      p[d][i] = x - P.lbox[d] * fnint(x * P.inv_lbox[d]);
+    }
+}
+
+// rows of 3 doubles (host layout) <-> SoA state arrays
+__global__ void k_rows_to_soa(int n, const double* __restrict__ rows, double* __restrict__ x,
+                              double* __restrict__ y, double* __restrict__ z) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  x[i] = rows[3 * (size_t)i];
+  y[i] = rows[3 * (size_t)i + 1];
+  z[i] = rows[3 * (size_t)i + 2];
+}
+__global__ void k_soa_to_rows(int n, const double* __restrict__ x, const double* __restrict__ y,
+                              const double* __restrict__ z, double* __restrict__ rows) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  rows[3 * (size_t)i] = x[i];
+  rows[3 * (size_t)i + 1] = y[i];
+  rows[3 * (size_t)i + 2] = z[i];
+}
+
+// copy history records into a table with a larger capacity
+__global__ void k_hist_regrow(int n, History src, History dst) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int c = src.cnt[i];
+  dst.cnt[i] = c;
+  for (int r = 0; r < c; r++) {
+    dst.key[(size_t)i * dst.cap + r] = src.key[(size_t)i * src.cap + r];
+    for (int k = 0; k < 3; k++)
+      dst.val[((size_t)i * dst.cap + r) * 3 + k] = src.val[((size_t)i * src.cap + r) * 3 + k];
+  }
+}
+
+// observables: per-block partial sums (fixed order), reduced on the host
+template <bool PP>
+__global__ void k_observables(const DevParams* __restrict__ Pp, int n, StateArrays Q,
+                              const double* __restrict__ radius, const int* __restrict__ comp,
+                              double* __restrict__ partial /* [grid][8] */) {
+  const DevParams& P = *Pp;
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double R, m, I;
+    if (PP) {
+      R = radius[i];
+      m = P.pp_mass_coef * ((R * R) * R);
+    } else {
+      int k = comp[i];
+      R = P.comp_radius[k];
+      m = 1.0 / P.comp_inv_mass[k];
+    }
+    I = (0.4 * m) * (R * R);
+    if (!PP) I = 1.0 / P.comp_inv_inertia[comp[i]];
+    double v[3] = {Q.vx[i], Q.vy[i], Q.vz[i]};
+    double w[3] = {Q.wx[i], Q.wy[i], Q.wz[i]};
+    double x[3] = {Q.px[i], Q.py[i], Q.pz[i]};
+    acc[0] += m * sumsq3(v) + I * sumsq3(w);
+    acc[1] -= m * dot3(x, P.gravity);
+    acc[2] += 4.0 / 3.0 * 3.14159265358979323846 * R * R * R;
+    acc[3] += m * v[0];
+    acc[4] += m * v[1];
+    acc[5] += m * v[2];
+  }
+  __shared__ double sh[8][256];
+  for (int k = 0; k < 8; k++) sh[k][threadIdx.x] = acc[k];
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+      for (int k = 0; k < 8; k++) sh[k][threadIdx.x] += sh[k][threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 8; k++) partial[blockIdx.x * 8 + k] = sh[k][0];
+}
+
+}  // namespace dem

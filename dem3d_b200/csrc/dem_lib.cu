@@ -1,0 +1,1318 @@
+// dem_lib.cu -- C-ABI of the B200 DEM step (include/dem3d_b200.h).
+//
+// Host orchestration of the device kernels in dem_kernels.cuh: context and
+// device memory, the two force passes of MoveParticles, the Euler start-up,
+// CUDA-graph replay of whole steps, contact-history import/export and the
+// instrumentation used by the benchmark.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "dem_kernels.cuh"
+#include "dem_mixed.cuh"
+
+using namespace dem;
+
+#define DEM_VERSION_STR "dem3d_b200 0.1 (sm_100a)"
+
+namespace {
+
+struct KernelStat {
+  std::string name;
+  long long launches = 0;
+  double total_ms = 0.0;
+};
+
+struct PendingEvent {
+  int stat;
+  cudaEvent_t e0, e1;
+};
+
+}  // namespace
+
+struct dem_ctx {
+  dem_params params{};
+  DevParams hp{};
+  DevParams* dp = nullptr;
+  int n = 0;
+  int nprev = 0;
+  bool state_set = false;
+  bool cells_ready = false;
+  bool pp = false;  // per-particle radius mode
+  int precision = DEM_PREC_FP64;
+  cudaStream_t stream = nullptr;
+  int device = 0;
+
+  StateArrays P{}, Pr{};
+  double* state_block = nullptr;  // all 30 state arrays
+  double* ring = nullptr;
+  double* radius = nullptr;
+  int* comp = nullptr;
+
+  SortedArrays S{};
+  int* cell_start = nullptr;
+  int* cell_cnt = nullptr;
+  int* cell_of_orig = nullptr;
+  int *a_cell = nullptr, *a_loc = nullptr, *a_orig = nullptr, *t_orig = nullptr;
+  unsigned *a_key = nullptr, *t_key = nullptr;
+  int* scan_bsum = nullptr;
+  int n_tiles = 0;
+
+  History H[2]{};
+  int hcur = 0;  // H[hcur] holds the current records
+  int hcap = 16;
+
+  MixedBuffers M{};
+
+  Counters* cnt = nullptr;
+  Counters* hcnt = nullptr;  // pinned host mirror
+  double* obs_partial = nullptr;
+
+  double* staging = nullptr;  // 15*n doubles, rows layout for host I/O
+  cudaEvent_t timer[2] = {nullptr, nullptr};
+
+  int ringmap[5] = {0, 1, 2, 3, 4};
+  double time = 0.0;
+
+  // graphs: one per (phase of the ring/history rotation)
+  cudaGraphExec_t graph[8] = {};
+  int graph_steps = 0;
+  long long graph_kernels = 0;  // kernels in one captured chunk
+  bool graph_valid = false;
+
+  bool prof = false;
+  std::vector<KernelStat> stats;
+  std::vector<PendingEvent> pending;
+  std::vector<cudaEvent_t> event_pool;
+  long long launches = 0;
+  long long last_pairs = 0, last_walls = 0, last_movers = 0;
+
+  std::string err;
+};
+
+namespace {
+
+int fail(dem_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+int cuda_fail(dem_ctx* c, cudaError_t e, const char* where) {
+  std::string m = std::string("CUDA error in ") + where + ": " + cudaGetErrorString(e);
+  return fail(c, DEM_ERR_CUDA, m);
+}
+
+#define CK(call)                                              \
+  do {                                                        \
+    cudaError_t e_ = (call);                                  \
+    if (e_ != cudaSuccess) return cuda_fail(c, e_, #call);    \
+  } while (0)
+
+int stat_index(dem_ctx* c, const char* name) {
+  for (size_t i = 0; i < c->stats.size(); i++)
+    if (c->stats[i].name == name) return (int)i;
+  c->stats.push_back(KernelStat{name});
+  return (int)c->stats.size() - 1;
+}
+
+cudaEvent_t get_event(dem_ctx* c) {
+  if (!c->event_pool.empty()) {
+    cudaEvent_t e = c->event_pool.back();
+    c->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// launch with optional event timing
+template <typename... KArgs, typename... Args>
+void launch(dem_ctx* c, const char* name, void (*kernel)(KArgs...), unsigned grid, unsigned block,
+            Args... args) {
+  if (grid == 0) return;
+  if (c->prof) {
+    PendingEvent pe;
+    pe.stat = stat_index(c, name);
+    pe.e0 = get_event(c);
+    pe.e1 = get_event(c);
+    cudaEventRecord(pe.e0, c->stream);
+    kernel<<<grid, block, 0, c->stream>>>(args...);
+    cudaEventRecord(pe.e1, c->stream);
+    c->pending.push_back(pe);
+  } else {
+    kernel<<<grid, block, 0, c->stream>>>(args...);
+  }
+  c->launches++;
+}
+
+void resolve_events(dem_ctx* c) {
+  if (c->pending.empty()) return;
+  cudaStreamSynchronize(c->stream);
+  for (auto& pe : c->pending) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, pe.e0, pe.e1);
+    c->stats[pe.stat].launches++;
+    c->stats[pe.stat].total_ms += ms;
+    c->event_pool.push_back(pe.e0);
+    c->event_pool.push_back(pe.e1);
+  }
+  c->pending.clear();
+}
+
+unsigned blocks_for(long long n, int b) { return (unsigned)((n + b - 1) / b); }
+
+void free_state(dem_ctx* c) {
+  cudaFree(c->staging);
+  c->staging = nullptr;
+  cudaFree(c->state_block);
+  cudaFree(c->ring);
+  cudaFree(c->radius);
+  cudaFree(c->comp);
+  cudaFree(c->S.pos);
+  cudaFree(c->S.v4);
+  cudaFree(c->S.w2);
+  cudaFree(c->S.comp);
+  cudaFree(c->S.orig);
+  cudaFree(c->S.cell);
+  cudaFree(c->cell_of_orig);
+  cudaFree(c->a_cell);
+  cudaFree(c->a_loc);
+  cudaFree(c->a_orig);
+  cudaFree(c->t_orig);
+  cudaFree(c->a_key);
+  cudaFree(c->t_key);
+  for (int b = 0; b < 2; b++) {
+    cudaFree(c->H[b].cnt);
+    cudaFree(c->H[b].key);
+    cudaFree(c->H[b].val);
+    cudaFree(c->H[b].wflag);
+    cudaFree(c->H[b].wval);
+    c->H[b] = History{};
+  }
+  mixed_free(c->M);
+  c->state_block = c->ring = c->radius = nullptr;
+  c->comp = nullptr;
+  c->S = SortedArrays{};
+  c->cell_of_orig = c->a_cell = c->a_loc = c->a_orig = c->t_orig = nullptr;
+  c->a_key = c->t_key = nullptr;
+}
+
+void drop_graphs(dem_ctx* c) {
+  for (auto& g : c->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  c->graph_valid = false;
+}
+
+int alloc_history(dem_ctx* c, History& H, int cap) {
+  size_t n = (size_t)std::max(c->n, 1);
+  int nw = std::max(c->params.n_walls, 1);
+  H.cap = cap;
+  CK(cudaMalloc(&H.cnt, n * sizeof(int)));
+  CK(cudaMalloc(&H.key, n * cap * sizeof(int)));
+  CK(cudaMalloc(&H.val, n * cap * 3 * sizeof(double2)));
+  CK(cudaMalloc(&H.wflag, n * nw * sizeof(int)));
+  CK(cudaMalloc(&H.wval, n * nw * 3 * sizeof(double2)));
+  CK(cudaMemsetAsync(H.cnt, 0, n * sizeof(int), c->stream));
+  CK(cudaMemsetAsync(H.wflag, 0, n * nw * sizeof(int), c->stream));
+  return DEM_OK;
+}
+
+// grow both history tables, keeping the current records
+int grow_history(dem_ctx* c, int need) {
+  int cap = c->hcap;
+  while (cap < need) cap *= 2;
+  History nh[2];
+  for (int b = 0; b < 2; b++) {
+    int st = alloc_history(c, nh[b], cap);
+    if (st) return st;
+  }
+  History& cur = c->H[c->hcur];
+  launch(c, "hist_regrow", k_hist_regrow, blocks_for(c->n, 256), 256, c->n, cur, nh[c->hcur]);
+  size_t n = (size_t)std::max(c->n, 1);
+  int nw = std::max(c->params.n_walls, 1);
+  CK(cudaMemcpyAsync(nh[c->hcur].wflag, cur.wflag, n * nw * sizeof(int), cudaMemcpyDeviceToDevice,
+                     c->stream));
+  CK(cudaMemcpyAsync(nh[c->hcur].wval, cur.wval, n * nw * 3 * sizeof(double2),
+                     cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int b = 0; b < 2; b++) {
+    cudaFree(c->H[b].cnt);
+    cudaFree(c->H[b].key);
+    cudaFree(c->H[b].val);
+    cudaFree(c->H[b].wflag);
+    cudaFree(c->H[b].wval);
+    c->H[b] = nh[b];
+  }
+  c->hcap = cap;
+  drop_graphs(c);
+  return DEM_OK;
+}
+
+StateArrays make_state(double* base, size_t n) {
+  StateArrays s;
+  double** f[15] = {&s.px, &s.py, &s.pz, &s.vx, &s.vy, &s.vz, &s.wx, &s.wy,
+                    &s.wz, &s.ax, &s.ay, &s.az, &s.lx, &s.ly, &s.lz};
+  for (int k = 0; k < 15; k++) *f[k] = base + (size_t)k * n;
+  return s;
+}
+
+// ---------------------------------------------------------------------------
+// K1: rebuild the cell order from the positions in `src`
+
+int rebuild_cells(dem_ctx* c, const StateArrays& src, bool initial) {
+  const int n = c->n;
+  const int ncell = c->hp.ncell;
+  if (n == 0) return DEM_OK;
+  CK(cudaMemsetAsync(c->cell_cnt, 0, sizeof(int) * (size_t)ncell, c->stream));
+  launch(c, "cell_assign", k_assign, blocks_for(n, 256), 256, (const DevParams*)c->dp, n,
+         initial ? 1 : 0, (const double*)src.px, (const double*)src.py, (const double*)src.pz,
+         (const int*)c->S.orig, (const int*)c->S.cell, c->cell_cnt, c->a_cell, c->a_loc, c->a_key,
+         c->a_orig, c->cnt);
+  launch(c, "scan_tiles", k_scan_tiles, (unsigned)c->n_tiles, SCAN_THREADS,
+         (const int*)c->cell_cnt, ncell, c->cell_start, c->scan_bsum, (const Counters*)c->cnt);
+  launch(c, "scan_bsums", k_scan_bsums, 1u, SCAN_THREADS, c->scan_bsum, c->n_tiles, c->cell_start,
+         ncell, (const Counters*)c->cnt);
+  launch(c, "scan_add", k_scan_add, blocks_for(ncell, 256), 256, c->cell_start, ncell,
+         (const int*)c->scan_bsum, (const Counters*)c->cnt);
+  launch(c, "cell_scatter", k_scatter, blocks_for(n, 256), 256, n, (const int*)c->a_cell,
+         (const int*)c->a_loc, (const unsigned*)c->a_key, (const int*)c->a_orig,
+         (const int*)c->cell_start, c->t_key, c->t_orig, (const Counters*)c->cnt);
+  launch(c, "cell_sort", k_cellsort, blocks_for(ncell, 128), 128, ncell, (const int*)c->cell_start,
+         c->t_key, c->t_orig, c->S.orig, c->S.cell, c->cell_of_orig, (const Counters*)c->cnt);
+  if (c->precision == DEM_PREC_MIXED) {
+    mixed_gather(c->M, c->pp, c->dp, n, src, c->radius, c->comp, c->S, c->cnt, c->stream);
+    c->launches++;
+  } else if (c->pp) {
+    launch(c, "gather", k_gather<true>, blocks_for(n, 256), 256, (const DevParams*)c->dp, n, src,
+           (const double*)c->radius, (const int*)c->comp, c->S, (const Counters*)c->cnt);
+  } else {
+    launch(c, "gather", k_gather<false>, blocks_for(n, 256), 256, (const DevParams*)c->dp, n, src,
+           (const double*)c->radius, (const int*)c->comp, c->S, (const Counters*)c->cnt);
+  }
+  return DEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// K2+K4: one force pass
+
+int launch_force(dem_ctx* c, const StateArrays& tgt, bool update, double dt, int epi,
+                 const RingMap& rm, int tag) {
+  ForceArgs A;
+  A.P = c->dp;
+  A.n = c->n;
+  A.S = c->S;
+  A.cell_start = c->cell_start;
+  A.cell_of_orig = c->cell_of_orig;
+  A.Hr = c->H[c->hcur];
+  A.Hw = c->H[c->hcur ^ 1];
+  A.update = update ? 1 : 0;
+  A.half_dt = 0.5 * dt;
+  A.tgt = tgt;
+  A.part = c->P;
+  A.pred = c->Pr;
+  A.ring = c->ring;
+  A.rm = rm;
+  A.cnt = c->cnt;
+  A.tag = tag;
+  unsigned g = blocks_for(c->n, 128);
+  if (c->precision == DEM_PREC_MIXED) {
+    mixed_force(c->M, c->pp, epi, A, c->hcur, c->stream);
+    c->launches++;
+    return DEM_OK;
+  }
+#define FORCE_CASE(PPV, E) launch(c, "force_fp64", k_force_fp64<PPV, E>, g, 128, A);
+  if (c->pp) {
+    if (epi == EPI_STORE) FORCE_CASE(true, EPI_STORE)
+    else if (epi == EPI_PREDICT) FORCE_CASE(true, EPI_PREDICT)
+    else FORCE_CASE(true, EPI_CORRECT)
+  } else {
+    if (epi == EPI_STORE) FORCE_CASE(false, EPI_STORE)
+    else if (epi == EPI_PREDICT) FORCE_CASE(false, EPI_PREDICT)
+    else FORCE_CASE(false, EPI_CORRECT)
+  }
+#undef FORCE_CASE
+  return DEM_OK;
+}
+
+RingMap current_map(dem_ctx* c) {
+  RingMap rm;
+  for (int k = 0; k < 5; k++) rm.phys[k] = c->ringmap[k];
+  return rm;
+}
+
+// ipc = cshift(ipc,-1) with the spare slot becoming ipc(1)
+void rotate_ring(dem_ctx* c) {
+  int np = c->nprev;
+  if (np <= 0) return;
+  int spare = c->ringmap[np];
+  int oldest = c->ringmap[np - 1];
+  for (int k = np - 1; k > 0; k--) c->ringmap[k] = c->ringmap[k - 1];
+  c->ringmap[0] = spare;
+  c->ringmap[np] = oldest;
+}
+
+int reset_pass_counters(dem_ctx* c, bool update) {
+  // per-pass statistics; Ncol and the escape count accumulate
+  CK(cudaMemsetAsync(&c->cnt->pair_contacts, 0, 3 * sizeof(unsigned long long), c->stream));
+  CK(cudaMemsetAsync(&c->cnt->wall_fn[0], 0, sizeof(double) * NWM, c->stream));
+  if (update) CK(cudaMemsetAsync(&c->cnt->need_capacity, 0, sizeof(int), c->stream));
+  // escapes are counted by the corrector of the current step only
+  if (!update) CK(cudaMemsetAsync(&c->cnt->escaped, 0, sizeof(unsigned long long), c->stream));
+  return DEM_OK;
+}
+
+int read_counters(dem_ctx* c) {
+  CK(cudaMemcpyAsync(c->hcnt, c->cnt, sizeof(Counters), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->last_pairs = (long long)c->hcnt->pair_contacts;
+  c->last_walls = (long long)c->hcnt->wall_contacts;
+  c->last_movers = (long long)c->hcnt->movers;
+  return DEM_OK;
+}
+
+// forget a failed (overflowed) history-updating pass: flags and its Ncol
+int clear_abort(dem_ctx* c) {
+  CK(cudaMemsetAsync(&c->cnt->ncol_pending, 0, sizeof(unsigned long long), c->stream));
+  CK(cudaMemsetAsync(&c->cnt->overflow, 0, 4 * sizeof(int), c->stream));
+  return DEM_OK;
+}
+
+// A force pass that may update the history: on capacity overflow the tables
+// grow and the force kernel is re-run (the pass only writes fresh outputs,
+// so re-running it from the unchanged inputs gives the same result).
+int force_pass(dem_ctx* c, const StateArrays& src, const StateArrays& tgt, bool update, double dt,
+               int epi, const RingMap& rm, bool check, int tag) {
+  int st = reset_pass_counters(c, update);
+  if (st) return st;
+  st = rebuild_cells(c, src, false);
+  if (st) return st;
+  for (int attempt = 0;; attempt++) {
+    st = launch_force(c, tgt, update, dt, epi, rm, tag);
+    if (st) return st;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "force kernel launch");
+    if (!update || !check) break;
+    st = read_counters(c);
+    if (st) return st;
+    if (!c->hcnt->overflow) break;
+    if (attempt >= 8) return fail(c, DEM_ERR_CAPACITY, "history capacity cannot be grown");
+    int need = c->hcnt->need_capacity;
+    st = clear_abort(c);
+    if (st) return st;
+    st = grow_history(c, need);
+    if (st) return st;
+    st = reset_pass_counters(c, update);
+    if (st) return st;
+  }
+  if (update) c->hcur ^= 1;
+  return DEM_OK;
+}
+
+int validate_ready(dem_ctx* c) {
+  if (!c->state_set) return fail(c, DEM_ERR_STATE, "no particle state set");
+  if (!c->cells_ready)
+    return fail(c, DEM_ERR_STATE, "cell distribution not initialised (call "
+                                  "dem_initialize_cell_distribution)");
+  return DEM_OK;
+}
+
+// MoveParticles(step) (src/MDEM.f90:285-369)
+int move_particles_impl(dem_ctx* c, int step, bool check, int tag) {
+  RingMap rm = current_map(c);
+  int st = force_pass(c, c->P, c->P, true, c->params.time_step, EPI_PREDICT, rm, check, tag);
+  if (st) return st;
+  rotate_ring(c);
+  c->time = (double)step * c->params.time_step;
+  rm = current_map(c);
+  st = force_pass(c, c->Pr, c->Pr, false, c->params.time_step, EPI_CORRECT, rm, false, tag);
+  if (st) return st;
+  return DEM_OK;
+}
+
+// MoveParticlesEuler (src/MDEM.f90:258-281)
+int move_particles_euler_impl(dem_ctx* c) {
+  const int n = c->n;
+  const double dt = c->params.time_step / (double)c->params.euler_intervals;
+  if (c->nprev > 0) {
+    int spare = c->ringmap[c->nprev];
+    launch(c, "ring_store", k_ring_store, blocks_for(n, 256), 256, n, c->P, c->ring, spare,
+           (const Counters*)c->cnt);
+    rotate_ring(c);
+  }
+  RingMap rm = current_map(c);
+  for (int s = 0; s < c->params.euler_intervals; s++) {
+    int st = force_pass(c, c->P, c->P, true, dt, EPI_STORE, rm, true, 0);
+    if (st) return st;
+    launch(c, "euler_update", k_euler_update, blocks_for(n, 256), 256, n, c->P, dt,
+           (const Counters*)c->cnt);
+    c->time = c->time + dt;
+  }
+  launch(c, "apply_pbc", k_apply_pbc, blocks_for(n, 256), 256, (const DevParams*)c->dp, n, c->P,
+         (const Counters*)c->cnt);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(c, e, "euler");
+  return DEM_OK;
+}
+
+// Capture `steps` MoveParticles steps (no host checks) into one graph.
+int capture_steps(dem_ctx* c, int steps, cudaGraphExec_t* out) {
+  cudaGraph_t g;
+  bool prof = c->prof;
+  c->prof = false;
+  long long l0 = c->launches;
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  int st = DEM_OK;
+  for (int k = 0; k < steps && !st; k++) st = move_particles_impl(c, 0, false, k);
+  cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  c->prof = prof;
+  c->graph_kernels = c->launches - l0;
+  c->launches = l0;
+  if (st) return st;
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate");
+  return DEM_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C-ABI
+
+extern "C" {
+
+const char* dem_version(void) { return DEM_VERSION_STR; }
+
+int dem_select_device(int32_t device) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return DEM_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev) return DEM_ERR_INVALID;
+  return cudaSetDevice(device) == cudaSuccess ? DEM_OK : DEM_ERR_CUDA;
+}
+
+const char* dem_last_error(const dem_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int dem_create(const dem_params* p, dem_ctx** out) {
+  if (!p || !out) return DEM_ERR_INVALID;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return DEM_ERR_NO_DEVICE;
+  }
+  if (p->method_order < 1 || p->method_order > 4) return DEM_ERR_INVALID;
+  if (p->n_walls < 0 || p->n_walls > NWM) return DEM_ERR_INVALID;
+  if (p->n_components < 0 || p->n_components > NCM) return DEM_ERR_INVALID;
+  if (p->euler_intervals < 1) return DEM_ERR_INVALID;
+  if (p->precision != DEM_PREC_FP64 && p->precision != DEM_PREC_MIXED) return DEM_ERR_INVALID;
+  if (p->precision == DEM_PREC_MIXED && !mixed_available()) return DEM_ERR_UNSUPPORTED;
+  for (int w = 0; w < p->n_walls; w++)
+    if (p->walls[w].shape != DEM_WALL_RECTANGLE) return DEM_ERR_UNSUPPORTED;
+
+  dem_ctx* c = new dem_ctx();
+  c->params = *p;
+  c->pp = p->n_components == 0;
+  c->precision = p->precision;
+  c->nprev = p->method_order - 1;
+  c->hcap = p->hist_capacity > 0 ? p->hist_capacity : 16;
+  cudaGetDevice(&c->device);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return DEM_ERR_CUDA;
+  }
+
+  DevParams& h = c->hp;
+  h.nc = p->n_components;
+  h.nw = p->n_walls;
+  for (int k = 0; k < 3; k++) {
+    h.pbc[k] = p->pbc[k] ? 1 : 0;
+    h.lbox[k] = p->lbox[k];
+    h.inv_lbox[k] = 1.0 / p->lbox[k];  // ScaleVariables, src/DEM.f90:825
+    h.gravity[k] = p->gravity[k];
+  }
+  h.nprev = c->nprev;
+  // ABM coefficients, src/MDEM.f90:127-154
+  double dt = p->time_step;
+  switch (p->method_order) {
+    case 4: {
+      double Aux = dt / 24.0;
+      h.ab0 = 55.0 * Aux; h.am0 = 9.0 * Aux;
+      h.ab[0] = -59.0 * Aux; h.am[0] = 19.0 * Aux;
+      h.ab[1] = 37.0 * Aux; h.am[1] = -5.0 * Aux;
+      h.ab[2] = -9.0 * Aux; h.am[2] = 1.0 * Aux;
+    } break;
+    case 3: {
+      double Aux = dt / 12.0;
+      h.ab0 = 23.0 * Aux; h.am0 = 5.0 * Aux;
+      h.ab[0] = -16.0 * Aux; h.am[0] = 8.0 * Aux;
+      h.ab[1] = 5.0 * Aux; h.am[1] = -1.0 * Aux;
+    } break;
+    case 2:
+      h.ab0 = 1.5 * dt; h.am0 = 0.5 * dt;
+      h.ab[0] = -0.5 * dt; h.am[0] = 0.5 * dt;
+      break;
+    default:
+      h.ab0 = dt; h.am0 = dt;
+  }
+  // cell grid, InitCellStructure3D (src/MCells.f90:155-227) with
+  // CutOff = 2*maxval(Component%Radius) (src/MForces.f90:96)
+  double rmax = 0.0;
+  if (p->n_components > 0) {
+    for (int i = 0; i < p->n_components; i++) rmax = std::max(rmax, p->comp_radius[i]);
+  } else {
+    rmax = p->pp_rmax;
+  }
+  double CutOff = 2.0 * rmax;
+  if (!(CutOff > 0.0)) {
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return DEM_ERR_INVALID;
+  }
+  int MaxNCell = p->max_ncell > 0 ? p->max_ncell : 30000;
+  double Lx = p->lbox[0], Ly = p->lbox[1], Lz = p->lbox[2];
+  int Nx4 = (int)(Lx / CutOff), Ny4 = (int)(Ly / CutOff), Nz4 = (int)(Lz / CutOff);
+  long long N4 = (long long)Nx4 * Ny4 * Nz4;
+  int Nx, Ny, Nz;
+  if (N4 > MaxNCell) {
+    double LCell = std::pow(Lx * Ly * Lz / (double)MaxNCell, 1.0 / 3.0);
+    Nx = (int)(Lx / LCell);
+    Ny = (int)(Ly / LCell);
+    Nz = (int)(Lz / LCell);
+  } else {
+    Nx = Nx4;
+    Ny = Ny4;
+    Nz = Nz4;
+  }
+  int N[3] = {Nx, Ny, Nz};
+  for (int k = 0; k < 3; k++) {
+    if (N[k] < 1) {
+      cudaStreamDestroy(c->stream);
+      delete c;
+      return DEM_ERR_INVALID;
+    }
+    // with 1 or 2 cells along a periodic axis the reference lists a cell
+    // twice in a half shell (duplicate pair visits); not reproduced here
+    if (p->pbc[k] && N[k] < 3) {
+      cudaStreamDestroy(c->stream);
+      delete c;
+      return DEM_ERR_UNSUPPORTED;
+    }
+  }
+  h.nx = Nx;
+  h.ny = Ny;
+  h.nz = Nz;
+  h.ncell = Nx * Ny * Nz;
+  h.nxbylx = (double)Nx / Lx;
+  h.nybyly = (double)Ny / Ly;
+  h.nzbylz = (double)Nz / Lz;
+  h.nxby2 = (double)Nx * 0.5;
+  h.nyby2 = (double)Ny * 0.5;
+  h.nzby2 = (double)Nz * 0.5;
+  // material tables
+  for (int i = 0; i < NCM; i++) {
+    h.comp_radius[i] = p->comp_radius[i];
+    h.comp_inv_mass[i] = p->comp_inv_mass[i];
+    h.comp_inv_inertia[i] = p->comp_inv_inertia[i];
+    h.comp_eff_mass[i] = p->comp_eff_mass[i];
+  }
+  std::memcpy(h.min_dij, p->min_dij, sizeof(h.min_dij));
+  std::memcpy(h.min_dij_sq, p->min_dij_sq, sizeof(h.min_dij_sq));
+  std::memcpy(h.kn, p->kn, sizeof(h.kn));
+  std::memcpy(h.yn, p->yn, sizeof(h.yn));
+  std::memcpy(h.kt, p->kt, sizeof(h.kt));
+  std::memcpy(h.yt, p->yt, sizeof(h.yt));
+  std::memcpy(h.mu_sq, p->mu_sq, sizeof(h.mu_sq));
+  std::memcpy(h.knw, p->knw, sizeof(h.knw));
+  std::memcpy(h.ynw, p->ynw, sizeof(h.ynw));
+  std::memcpy(h.ktw, p->ktw, sizeof(h.ktw));
+  std::memcpy(h.ytw, p->ytw, sizeof(h.ytw));
+  std::memcpy(h.muw_sq, p->muw_sq, sizeof(h.muw_sq));
+  h.pp_mass_coef = p->pp_mass_coef;
+  h.pp_density = p->pp_density;
+  h.pp_fluid_density = p->pp_fluid_density;
+  h.pp_kn = p->pp_kn;
+  h.pp_kt = p->pp_kt;
+  h.pp_gamma_n = p->pp_gamma_n;
+  h.pp_gamma_t = p->pp_gamma_t;
+  h.pp_mu_sq = p->pp_mu_sq;
+  for (int w = 0; w < NWM; w++) {
+    h.pp_knw[w] = p->pp_knw[w];
+    h.pp_ktw[w] = p->pp_ktw[w];
+    h.pp_gamma_nw[w] = p->pp_gamma_nw[w];
+    h.pp_gamma_tw[w] = p->pp_gamma_tw[w];
+    h.pp_muw_sq[w] = p->pp_muw_sq[w];
+    h.walls[w] = p->walls[w];
+  }
+
+  cudaError_t e = cudaMalloc(&c->dp, sizeof(DevParams));
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(c->dp, &h, sizeof(DevParams), cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaMalloc(&c->cnt, sizeof(Counters));
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->cnt, 0, sizeof(Counters), c->stream);
+  if (e == cudaSuccess) e = cudaMallocHost(&c->hcnt, sizeof(Counters));
+  if (e == cudaSuccess) e = cudaMalloc(&c->cell_start, sizeof(int) * ((size_t)h.ncell + 1));
+  if (e == cudaSuccess) e = cudaMalloc(&c->cell_cnt, sizeof(int) * (size_t)h.ncell);
+  c->n_tiles = (h.ncell + SCAN_TILE - 1) / SCAN_TILE;
+  if (e == cudaSuccess) e = cudaMalloc(&c->scan_bsum, sizeof(int) * (size_t)c->n_tiles);
+  if (e == cudaSuccess) e = cudaMalloc(&c->obs_partial, sizeof(double) * 8 * 1184);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) {
+    c->err = std::string("dem_create: ") + cudaGetErrorString(e);
+    dem_destroy(c);
+    return DEM_ERR_CUDA;
+  }
+  std::memset(c->hcnt, 0, sizeof(Counters));
+  *out = c;
+  return DEM_OK;
+}
+
+void dem_destroy(dem_ctx* c) {
+  if (!c) return;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  drop_graphs(c);
+  free_state(c);
+  cudaFree(c->dp);
+  cudaFree(c->cnt);
+  if (c->hcnt) cudaFreeHost(c->hcnt);
+  cudaFree(c->cell_start);
+  cudaFree(c->cell_cnt);
+  cudaFree(c->scan_bsum);
+  cudaFree(c->obs_partial);
+  for (auto& pe : c->pending) {
+    cudaEventDestroy(pe.e0);
+    cudaEventDestroy(pe.e1);
+  }
+  for (auto e : c->event_pool) cudaEventDestroy(e);
+  for (auto e : c->timer)
+    if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+static int put_state_arrays(dem_ctx* c, const StateArrays& s, const double* pos,
+                            const double* vel, const double* omega, const double* acc,
+                            const double* alpha);
+
+int dem_set_state(dem_ctx* c, int32_t n, const int32_t* comp, const double* radius,
+                  const double* pos, const double* vel, const double* omega, const double* acc,
+                  const double* alpha) {
+  if (!c) return DEM_ERR_INVALID;
+  if (n < 0 || !pos || !vel || !omega) return fail(c, DEM_ERR_INVALID, "bad state arrays");
+  if (!c->pp && !comp) return fail(c, DEM_ERR_INVALID, "component indices required");
+  if (c->pp && !radius) return fail(c, DEM_ERR_INVALID, "per-particle radii required");
+  if (n >= (1 << 30)) return fail(c, DEM_ERR_INVALID, "too many particles");
+  if (!c->pp)
+    for (int i = 0; i < n; i++)
+      if (comp[i] < 0 || comp[i] >= c->params.n_components)
+        return fail(c, DEM_ERR_INVALID, "component index out of range");
+  if (c->pp)
+    for (int i = 0; i < n; i++)
+      if (!(radius[i] > 0.0) || radius[i] > c->params.pp_rmax)
+        return fail(c, DEM_ERR_INVALID, "radius must lie in (0, pp_rmax]");
+  CK(cudaStreamSynchronize(c->stream));
+  drop_graphs(c);
+  free_state(c);
+  c->n = n;
+  size_t N = (size_t)std::max(n, 1);
+  CK(cudaMalloc(&c->state_block, sizeof(double) * 30 * N));
+  CK(cudaMalloc(&c->staging, sizeof(double) * 15 * N));
+  CK(cudaMemsetAsync(c->state_block, 0, sizeof(double) * 30 * N, c->stream));
+  c->P = make_state(c->state_block, N);
+  c->Pr = make_state(c->state_block + 15 * N, N);
+  int slots = c->nprev + 1;
+  CK(cudaMalloc(&c->ring, sizeof(double) * 9 * N * slots));
+  CK(cudaMemsetAsync(c->ring, 0, sizeof(double) * 9 * N * slots, c->stream));
+  CK(cudaMalloc(&c->radius, sizeof(double) * N));
+  CK(cudaMalloc(&c->comp, sizeof(int) * N));
+  CK(cudaMalloc(&c->S.pos, sizeof(double4) * N));
+  CK(cudaMalloc(&c->S.v4, sizeof(double4) * N));
+  CK(cudaMalloc(&c->S.w2, sizeof(double2) * N));
+  CK(cudaMalloc(&c->S.comp, sizeof(int) * N));
+  CK(cudaMalloc(&c->S.orig, sizeof(int) * N));
+  CK(cudaMalloc(&c->S.cell, sizeof(int) * N));
+  CK(cudaMalloc(&c->cell_of_orig, sizeof(int) * N));
+  CK(cudaMalloc(&c->a_cell, sizeof(int) * N));
+  CK(cudaMalloc(&c->a_loc, sizeof(int) * N));
+  CK(cudaMalloc(&c->a_orig, sizeof(int) * N));
+  CK(cudaMalloc(&c->t_orig, sizeof(int) * N));
+  CK(cudaMalloc(&c->a_key, sizeof(unsigned) * N));
+  CK(cudaMalloc(&c->t_key, sizeof(unsigned) * N));
+  for (int b = 0; b < 2; b++) {
+    int st = alloc_history(c, c->H[b], c->hcap);
+    if (st) return st;
+  }
+  c->hcur = 0;
+  if (c->precision == DEM_PREC_MIXED) {
+    if (!mixed_alloc(c->M, n, c->params.n_walls, c->hcap)) return fail(c, DEM_ERR_CUDA, "mixed alloc");
+  }
+  // host -> device (positions etc. are n x 3 rows)
+  {
+    int st = put_state_arrays(c, c->P, pos, vel, omega, acc, alpha);
+    if (st) return st;
+  }
+  std::vector<int> ci(N, 0);
+  std::vector<double> rr(N, 0.0);
+  for (int i = 0; i < n; i++) {
+    ci[i] = comp ? comp[i] : 0;
+    rr[i] = radius ? radius[i] : c->params.comp_radius[ci[i]];
+  }
+  CK(cudaMemcpy(c->comp, ci.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->radius, rr.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
+  CK(cudaMemsetAsync(c->cnt, 0, sizeof(Counters), c->stream));
+  for (int k = 0; k < 5; k++) c->ringmap[k] = k;
+  CK(cudaStreamSynchronize(c->stream));
+  c->state_set = true;
+  c->cells_ready = false;
+  c->time = 0.0;
+  return DEM_OK;
+}
+
+static int get_state_arrays(dem_ctx* c, const StateArrays& s, double* pos, double* vel,
+                            double* omega, double* acc, double* alpha) {
+  if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
+  const int n = c->n;
+  if (n == 0) return DEM_OK;
+  double* outs[5] = {pos, vel, omega, acc, alpha};
+  double* const* src = &s.px;  // 15 consecutive pointers in StateArrays
+  for (int a = 0; a < 5; a++) {
+    if (!outs[a]) continue;
+    double* stg = c->staging + (size_t)a * 3 * n;
+    launch(c, "soa_to_rows", k_soa_to_rows, blocks_for(n, 256), 256, n,
+           (const double*)src[3 * a], (const double*)src[3 * a + 1], (const double*)src[3 * a + 2],
+           stg);
+    CK(cudaMemcpyAsync(outs[a], stg, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return DEM_OK;
+}
+
+static int put_state_arrays(dem_ctx* c, const StateArrays& s, const double* pos,
+                            const double* vel, const double* omega, const double* acc,
+                            const double* alpha) {
+  const int n = c->n;
+  if (n == 0) return DEM_OK;
+  const double* ins[5] = {pos, vel, omega, acc, alpha};
+  double* const* dst = &s.px;
+  for (int a = 0; a < 5; a++) {
+    if (!ins[a]) continue;
+    double* stg = c->staging + (size_t)a * 3 * n;
+    CK(cudaMemcpyAsync(stg, ins[a], sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+    launch(c, "rows_to_soa", k_rows_to_soa, blocks_for(n, 256), 256, n, (const double*)stg,
+           dst[3 * a], dst[3 * a + 1], dst[3 * a + 2]);
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return DEM_OK;
+}
+
+int dem_update_state(dem_ctx* c, const double* pos, const double* vel, const double* omega,
+                     const double* acc, const double* alpha) {
+  if (!c) return DEM_ERR_INVALID;
+  if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
+  return put_state_arrays(c, c->P, pos, vel, omega, acc, alpha);
+}
+
+int dem_timer_start(dem_ctx* c) {
+  if (!c) return DEM_ERR_INVALID;
+  for (auto& e : c->timer)
+    if (!e) CK(cudaEventCreate(&e));
+  CK(cudaEventRecord(c->timer[0], c->stream));
+  return DEM_OK;
+}
+
+int dem_timer_stop(dem_ctx* c, double* ms) {
+  if (!c || !ms || !c->timer[0]) return DEM_ERR_INVALID;
+  CK(cudaEventRecord(c->timer[1], c->stream));
+  CK(cudaEventSynchronize(c->timer[1]));
+  float f = 0.f;
+  CK(cudaEventElapsedTime(&f, c->timer[0], c->timer[1]));
+  *ms = f;
+  return DEM_OK;
+}
+
+int dem_get_state(dem_ctx* c, double* pos, double* vel, double* omega, double* acc,
+                  double* alpha) {
+  if (!c) return DEM_ERR_INVALID;
+  return get_state_arrays(c, c->P, pos, vel, omega, acc, alpha);
+}
+
+int dem_get_predicted(dem_ctx* c, double* pos, double* vel, double* omega, double* acc,
+                      double* alpha) {
+  if (!c) return DEM_ERR_INVALID;
+  return get_state_arrays(c, c->Pr, pos, vel, omega, acc, alpha);
+}
+
+int dem_get_n(dem_ctx* c, int32_t* n) {
+  if (!c || !n) return DEM_ERR_INVALID;
+  *n = c->n;
+  return DEM_OK;
+}
+
+int dem_set_integration(dem_ctx* c, const double* previous, const int32_t* ipc) {
+  if (!c || !previous || !ipc) return DEM_ERR_INVALID;
+  if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
+  size_t N = (size_t)std::max(c->n, 1);
+  // logical slot k (ipc(k+1)) -> physical slot k; spare = nprev
+  std::vector<double> tmp(9 * N * (c->nprev + 1), 0.0);
+  for (int k = 0; k < c->nprev; k++) {
+    int src = ipc[k] - 1;
+    if (src < 0 || src >= c->nprev) return fail(c, DEM_ERR_INVALID, "bad ipc");
+    for (int i = 0; i < c->n; i++)
+      for (int d = 0; d < 9; d++)
+        tmp[((size_t)k * 9 + d) * N + i] = previous[((size_t)src * c->n + i) * 9 + d];
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpy(c->ring, tmp.data(), sizeof(double) * tmp.size(), cudaMemcpyHostToDevice));
+  for (int k = 0; k < 5; k++) c->ringmap[k] = k;
+  drop_graphs(c);
+  return DEM_OK;
+}
+
+int dem_get_integration(dem_ctx* c, double* previous, int32_t* ipc) {
+  if (!c) return DEM_ERR_INVALID;
+  if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
+  size_t N = (size_t)std::max(c->n, 1);
+  std::vector<double> tmp(9 * N * (c->nprev + 1));
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpy(tmp.data(), c->ring, sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost));
+  // exported in canonical form: physical slot k = logical ipc(k+1)
+  for (int k = 0; k < c->nprev; k++) {
+    if (ipc) ipc[k] = k + 1;
+    if (previous) {
+      int ph = c->ringmap[k];
+      for (int i = 0; i < c->n; i++)
+        for (int d = 0; d < 9; d++)
+          previous[((size_t)k * c->n + i) * 9 + d] = tmp[((size_t)ph * 9 + d) * N + i];
+    }
+  }
+  return DEM_OK;
+}
+
+int dem_set_contacts(dem_ctx* c, int64_t m, const int32_t* imin, const int32_t* imax,
+                     const double* ft, const double* vt, int64_t mw, const int32_t* ip,
+                     const int32_t* iw, const double* ftw, const double* vtw) {
+  if (!c) return DEM_ERR_INVALID;
+  if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
+  const int n = c->n;
+  size_t N = (size_t)std::max(n, 1);
+  int nw = std::max(c->params.n_walls, 1);
+  std::vector<int> cnt(N, 0);
+  for (int64_t r = 0; r < m; r++) {
+    if (imin[r] < 0 || imin[r] >= imax[r] || imax[r] >= n)
+      return fail(c, DEM_ERR_INVALID, "bad pair record (need 0 <= imin < imax < n)");
+    cnt[imin[r]]++;
+  }
+  int need = 0;
+  for (int i = 0; i < n; i++) need = std::max(need, cnt[i]);
+  CK(cudaStreamSynchronize(c->stream));
+  if (need > c->hcap) {
+    int st = grow_history(c, need);
+    if (st) return st;
+  }
+  const int cap = c->hcap;
+  std::vector<int> key(N * cap, 0);
+  std::vector<double2> val(N * cap * 3);
+  std::fill(cnt.begin(), cnt.end(), 0);
+  // records kept sorted by partner as the reference lists are
+  std::vector<int64_t> idx(m);
+  for (int64_t r = 0; r < m; r++) idx[r] = r;
+  std::sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) {
+    return imin[a] != imin[b] ? imin[a] < imin[b] : imax[a] < imax[b];
+  });
+  for (int64_t q = 0; q < m; q++) {
+    int64_t r = idx[q];
+    int o = imin[r], k = cnt[o]++;
+    key[(size_t)o * cap + k] = imax[r];
+    double2* v = &val[((size_t)o * cap + k) * 3];
+    v[0] = make_double2(ft[3 * r], ft[3 * r + 1]);
+    v[1] = make_double2(ft[3 * r + 2], vt[3 * r]);
+    v[2] = make_double2(vt[3 * r + 1], vt[3 * r + 2]);
+  }
+  std::vector<int> wf(N * nw, 0);
+  std::vector<double2> wv(N * nw * 3);
+  for (int64_t r = 0; r < mw; r++) {
+    if (ip[r] < 0 || ip[r] >= n || iw[r] < 0 || iw[r] >= c->params.n_walls)
+      return fail(c, DEM_ERR_INVALID, "bad wall record");
+    size_t wi = (size_t)ip[r] * c->params.n_walls + iw[r];
+    wf[wi] = 1;
+    wv[wi * 3 + 0] = make_double2(ftw[3 * r], ftw[3 * r + 1]);
+    wv[wi * 3 + 1] = make_double2(ftw[3 * r + 2], vtw[3 * r]);
+    wv[wi * 3 + 2] = make_double2(vtw[3 * r + 1], vtw[3 * r + 2]);
+  }
+  History& H = c->H[c->hcur];
+  CK(cudaMemcpy(H.cnt, cnt.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(H.key, key.data(), sizeof(int) * key.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(H.val, val.data(), sizeof(double2) * val.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(H.wflag, wf.data(), sizeof(int) * wf.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(H.wval, wv.data(), sizeof(double2) * wv.size(), cudaMemcpyHostToDevice));
+  if (c->precision == DEM_PREC_MIXED) mixed_import_history(c->M, H, n, c->params.n_walls, c->hcur, c->stream);
+  drop_graphs(c);
+  return DEM_OK;
+}
+
+namespace {
+struct HostHist {
+  std::vector<int> cnt, key, wf;
+  std::vector<double2> val, wv;
+};
+int download_history(dem_ctx* c, HostHist& h) {
+  size_t N = (size_t)std::max(c->n, 1);
+  int nw = std::max(c->params.n_walls, 1);
+  History H = c->H[c->hcur];
+  if (c->precision == DEM_PREC_MIXED) {
+    // the mixed path keeps FP32 records; export them widened
+    H = c->H[c->hcur];
+    mixed_export_history(c->M, H, c->n, c->params.n_walls, c->hcur, c->stream);
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  h.cnt.resize(N);
+  h.key.resize(N * H.cap);
+  h.val.resize(N * H.cap * 3);
+  h.wf.resize(N * nw);
+  h.wv.resize(N * nw * 3);
+  CK(cudaMemcpy(h.cnt.data(), H.cnt, sizeof(int) * N, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(h.key.data(), H.key, sizeof(int) * h.key.size(), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(h.val.data(), H.val, sizeof(double2) * h.val.size(), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(h.wf.data(), H.wflag, sizeof(int) * h.wf.size(), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(h.wv.data(), H.wval, sizeof(double2) * h.wv.size(), cudaMemcpyDeviceToHost));
+  return DEM_OK;
+}
+}  // namespace
+
+int dem_count_contacts(dem_ctx* c, int64_t* n_pair, int64_t* n_wall) {
+  if (!c) return DEM_ERR_INVALID;
+  if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
+  HostHist h;
+  int st = download_history(c, h);
+  if (st) return st;
+  int64_t a = 0, b = 0;
+  for (int i = 0; i < c->n; i++) a += h.cnt[i];
+  for (int i = 0; i < c->n * c->params.n_walls; i++) b += h.wf[i] != 0;
+  if (n_pair) *n_pair = a;
+  if (n_wall) *n_wall = b;
+  return DEM_OK;
+}
+
+int dem_get_contacts(dem_ctx* c, int64_t cap, int32_t* imin, int32_t* imax, double* ft,
+                     double* vt, int64_t capw, int32_t* ip, int32_t* iw, double* ftw,
+                     double* vtw) {
+  if (!c) return DEM_ERR_INVALID;
+  if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
+  HostHist h;
+  int st = download_history(c, h);
+  if (st) return st;
+  const int hc = c->hcap;
+  int64_t a = 0, b = 0;
+  std::vector<int> ord;
+  for (int i = 0; i < c->n; i++) {
+    int k = h.cnt[i];
+    ord.resize(k);
+    for (int r = 0; r < k; r++) ord[r] = r;
+    std::sort(ord.begin(), ord.end(),
+              [&](int x, int y) { return h.key[(size_t)i * hc + x] < h.key[(size_t)i * hc + y]; });
+    for (int r : ord) {
+      if (a >= cap) return fail(c, DEM_ERR_INVALID, "pair record buffer too small");
+      imin[a] = i;
+      imax[a] = h.key[(size_t)i * hc + r];
+      const double2* v = &h.val[((size_t)i * hc + r) * 3];
+      ft[3 * a] = v[0].x; ft[3 * a + 1] = v[0].y; ft[3 * a + 2] = v[1].x;
+      vt[3 * a] = v[1].y; vt[3 * a + 1] = v[2].x; vt[3 * a + 2] = v[2].y;
+      a++;
+    }
+    for (int w = 0; w < c->params.n_walls; w++) {
+      size_t wi = (size_t)i * c->params.n_walls + w;
+      if (!h.wf[wi]) continue;
+      if (b >= capw) return fail(c, DEM_ERR_INVALID, "wall record buffer too small");
+      ip[b] = i;
+      iw[b] = w;
+      const double2* v = &h.wv[wi * 3];
+      ftw[3 * b] = v[0].x; ftw[3 * b + 1] = v[0].y; ftw[3 * b + 2] = v[1].x;
+      vtw[3 * b] = v[1].y; vtw[3 * b + 1] = v[2].x; vtw[3 * b + 2] = v[2].y;
+      b++;
+    }
+  }
+  return DEM_OK;
+}
+
+int dem_initialize_cell_distribution(dem_ctx* c) {
+  if (!c) return DEM_ERR_INVALID;
+  if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
+  int st = rebuild_cells(c, c->P, true);
+  if (st) return st;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  c->cells_ready = true;
+  return DEM_OK;
+}
+
+int dem_get_grid(dem_ctx* c, int32_t* nxyz) {
+  if (!c || !nxyz) return DEM_ERR_INVALID;
+  nxyz[0] = c->hp.nx;
+  nxyz[1] = c->hp.ny;
+  nxyz[2] = c->hp.nz;
+  return DEM_OK;
+}
+
+int dem_get_cells(dem_ctx* c, int32_t* cell_index, int32_t* traversal, int32_t* cell_start) {
+  if (!c) return DEM_ERR_INVALID;
+  int st = validate_ready(c);
+  if (st) return st;
+  CK(cudaStreamSynchronize(c->stream));
+  if (cell_index) CK(cudaMemcpy(cell_index, c->cell_of_orig, sizeof(int) * c->n, cudaMemcpyDeviceToHost));
+  if (traversal) CK(cudaMemcpy(traversal, c->S.orig, sizeof(int) * c->n, cudaMemcpyDeviceToHost));
+  if (cell_start)
+    CK(cudaMemcpy(cell_start, c->cell_start, sizeof(int) * ((size_t)c->hp.ncell + 1),
+                  cudaMemcpyDeviceToHost));
+  return DEM_OK;
+}
+
+int dem_compute_accelerations(dem_ctx* c, int32_t use_predicted, double time_step,
+                              int32_t update) {
+  if (!c) return DEM_ERR_INVALID;
+  int st = validate_ready(c);
+  if (st) return st;
+  const StateArrays& s = use_predicted ? c->Pr : c->P;
+  st = force_pass(c, s, s, update != 0, time_step, EPI_STORE, current_map(c), true, 0);
+  if (st) return st;
+  CK(cudaGetLastError());
+  st = read_counters(c);
+  return st;
+}
+
+int dem_move_particles(dem_ctx* c, int32_t step) {
+  if (!c) return DEM_ERR_INVALID;
+  int st = validate_ready(c);
+  if (st) return st;
+  st = move_particles_impl(c, step, true, 0);
+  if (st) return st;
+  CK(cudaGetLastError());
+  return read_counters(c);
+}
+
+int dem_move_particles_euler(dem_ctx* c) {
+  if (!c) return DEM_ERR_INVALID;
+  int st = validate_ready(c);
+  if (st) return st;
+  st = move_particles_euler_impl(c);
+  if (st) return st;
+  return read_counters(c);
+}
+
+// The main loop.  Steps are replayed from CUDA graphs of G = 4 steps (the
+// period of the ring rotation (<= 4 slots) and of the history double buffer);
+// every kernel in a graph first checks the abort word.  Before each replay
+// the history tables are grown if the last updating pass came within
+// HEADROOM records of the capacity.  If a pass inside a replay still
+// overflows, it records its step index and every later kernel of the replay
+// does nothing: the host advances its bookkeeping to that step, grows the
+// tables and re-runs that step synchronously (the failed pass is re-runnable:
+// it only wrote fresh outputs).
+int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
+  if (!c) return DEM_ERR_INVALID;
+  int st = validate_ready(c);
+  if (st) return st;
+  int s0 = first_step;
+  if (first_step == 1) {
+    for (int s = 1; s <= c->params.method_order - 1; s++) {
+      st = move_particles_euler_impl(c);
+      if (st) return st;
+    }
+    s0 = c->params.method_order;
+  }
+  int step = s0;
+  const int G = 4;
+  const int HEADROOM = 2;
+  while (step <= last_step) {
+    int remaining = last_step - step + 1;
+    if (remaining < G || c->prof) {
+      st = move_particles_impl(c, step, true, 0);
+      if (st) return st;
+      step++;
+      continue;
+    }
+    st = read_counters(c);
+    if (st) return st;
+    if (c->hcnt->need_capacity + HEADROOM > c->hcap) {
+      st = grow_history(c, c->hcnt->need_capacity + HEADROOM);
+      if (st) return st;
+    }
+    // one graph per rotation phase (ring spare slot, history parity)
+    int phase = (c->nprev > 0 ? c->ringmap[c->nprev] : 0) * 2 + c->hcur;
+    if (!c->graph_valid) {
+      for (auto& g : c->graph) g = nullptr;
+      c->graph_valid = true;
+    }
+    if (!c->graph[phase]) {
+      int rm[5];
+      std::memcpy(rm, c->ringmap, sizeof(rm));
+      int hc = c->hcur;
+      st = capture_steps(c, G, &c->graph[phase]);
+      std::memcpy(c->ringmap, rm, sizeof(rm));
+      c->hcur = hc;
+      if (st) return st;
+    }
+    CK(cudaGraphLaunch(c->graph[phase], c->stream));
+    c->launches += c->graph_kernels;
+    st = read_counters(c);
+    if (st) return st;
+    int done = G;
+    if (c->hcnt->abort) {
+      done = c->hcnt->abort_tag - 1;  // steps that completed
+      if (done < 0 || done >= G) return fail(c, DEM_ERR_STATE, "bad abort tag");
+    }
+    for (int k = 0; k < done; k++) {
+      rotate_ring(c);
+      c->hcur ^= 1;
+    }
+    step += done;
+    c->time = (double)(step - 1) * c->params.time_step;
+    if (done < G) {
+      int need = c->hcnt->need_capacity;
+      st = clear_abort(c);
+      if (st) return st;
+      st = grow_history(c, std::max(need, c->hcap + 1));
+      if (st) return st;
+      st = move_particles_impl(c, step, true, 0);
+      if (st) return st;
+      step++;
+    }
+  }
+  CK(cudaGetLastError());
+  return DEM_OK;
+}
+
+int dem_run_timed(dem_ctx* c, int32_t first_step, int32_t last_step, double* device_ms) {
+  if (!c || !device_ms) return DEM_ERR_INVALID;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaEventRecord(e0, c->stream));
+  int st = dem_run(c, first_step, last_step);
+  cudaEventRecord(e1, c->stream);
+  cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *device_ms = ms;
+  return st;
+}
+
+int dem_get_ncol(dem_ctx* c, int64_t* ncol) {
+  if (!c || !ncol) return DEM_ERR_INVALID;
+  int st = read_counters(c);
+  if (st) return st;
+  *ncol = (int64_t)c->hcnt->ncol;
+  return DEM_OK;
+}
+
+int dem_get_escaped(dem_ctx* c, int64_t* count) {
+  if (!c || !count) return DEM_ERR_INVALID;
+  int st = read_counters(c);
+  if (st) return st;
+  *count = (int64_t)c->hcnt->escaped;
+  return DEM_OK;
+}
+
+int dem_get_observables(dem_ctx* c, dem_observables* o) {
+  if (!c || !o) return DEM_ERR_INVALID;
+  if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
+  std::memset(o, 0, sizeof(*o));
+  const int grid = 148 * 4;
+  if (c->n > 0) {
+    if (c->pp)
+      launch(c, "observables", k_observables<true>, grid, 256, (const DevParams*)c->dp, c->n, c->P,
+             (const double*)c->radius, (const int*)c->comp, c->obs_partial);
+    else
+      launch(c, "observables", k_observables<false>, grid, 256, (const DevParams*)c->dp, c->n,
+             c->P, (const double*)c->radius, (const int*)c->comp, c->obs_partial);
+  }
+  std::vector<double> part((size_t)grid * 8, 0.0);
+  CK(cudaStreamSynchronize(c->stream));
+  if (c->n > 0)
+    CK(cudaMemcpy(part.data(), c->obs_partial, sizeof(double) * part.size(), cudaMemcpyDeviceToHost));
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int b = 0; b < grid; b++)
+    for (int k = 0; k < 8; k++) acc[k] += part[(size_t)b * 8 + k];
+  o->kinetic_energy = 0.5 * acc[0];
+  o->potential_energy = acc[1];
+  o->packing_fraction = acc[2] / (c->params.lbox[0] * c->params.lbox[1] * c->params.lbox[2]);
+  o->momentum[0] = acc[3];
+  o->momentum[1] = acc[4];
+  o->momentum[2] = acc[5];
+  int64_t np = 0, nw = 0;
+  int st = dem_count_contacts(c, &np, &nw);
+  if (st) return st;
+  o->n_pair_contacts = np;
+  o->n_wall_contacts = nw;
+  o->mean_coordination = c->n ? 2.0 * (double)np / (double)c->n : 0.0;
+  st = read_counters(c);
+  if (st) return st;
+  for (int w = 0; w < NWM; w++) o->wall_normal_force[w] = c->hcnt->wall_fn[w];
+  return DEM_OK;
+}
+
+int dem_set_profiling(dem_ctx* c, int32_t enable) {
+  if (!c) return DEM_ERR_INVALID;
+  resolve_events(c);
+  c->prof = enable != 0;
+  return DEM_OK;
+}
+
+int dem_get_kernel_stats(dem_ctx* c, int32_t idx, char* name, int32_t name_cap,
+                         int64_t* launches, double* total_ms) {
+  if (!c) return DEM_ERR_INVALID;
+  resolve_events(c);
+  if (idx < 0 || idx >= (int)c->stats.size()) return DEM_ERR_INVALID;
+  if (name && name_cap > 0) {
+    std::snprintf(name, (size_t)name_cap, "%s", c->stats[idx].name.c_str());
+  }
+  if (launches) *launches = c->stats[idx].launches;
+  if (total_ms) *total_ms = c->stats[idx].total_ms;
+  return DEM_OK;
+}
+
+int dem_reset_kernel_stats(dem_ctx* c) {
+  if (!c) return DEM_ERR_INVALID;
+  resolve_events(c);
+  c->stats.clear();
+  c->launches = 0;
+  return DEM_OK;
+}
+
+int dem_get_launch_count(dem_ctx* c, int64_t* launches) {
+  if (!c || !launches) return DEM_ERR_INVALID;
+  *launches = c->launches;
+  return DEM_OK;
+}
+
+int dem_get_stream(dem_ctx* c, void** stream) {
+  if (!c || !stream) return DEM_ERR_INVALID;
+  *stream = (void*)c->stream;
+  return DEM_OK;
+}
+
+int dem_get_pass_stats(dem_ctx* c, int64_t* pair_contacts, int64_t* wall_contacts,
+                       int64_t* movers, int32_t* hist_capacity) {
+  if (!c) return DEM_ERR_INVALID;
+  int st = read_counters(c);
+  if (st) return st;
+  if (pair_contacts) *pair_contacts = c->last_pairs;
+  if (wall_contacts) *wall_contacts = c->last_walls;
+  if (movers) *movers = c->last_movers;
+  if (hist_capacity) *hist_capacity = c->hcap;
+  return DEM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,287 @@
+"""Python mirror of the reference's per-step interface, over the C-ABI.
+
+``DEMSystem`` exposes the same operations, with the same argument meaning, as
+the Fortran module routines the library replaces:
+
+=================================  ==========================================
+DEMSystem method                   reference routine
+=================================  ==========================================
+``__init__``                        InitializeAuxiliaries (src/MDEM.f90:110)
+``set_state``                       Particle(1:NP) + InitializeIntegration-
+                                    Variables / InitializeContacts
+``initialize_cell_distribution``    InitializeCellDistribution
+                                    (src/MForces.f90:110)
+``compute_accelerations``           ComputeAccelerations (src/MForces.f90:145)
+``move_particles``                  MoveParticles (src/MDEM.f90:285)
+``move_particles_euler``            MoveParticlesEuler (src/MDEM.f90:258)
+``run``                             main loop, src/DEM.f90:85-99
+``kinetic_energy`` etc.             KineticEnergy/PotentialEnergy
+                                    (src/MDEM.f90:183-213)
+=================================  ==========================================
+
+Errors are raised as :class:`DEMError` (the reference ``stop``s).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._abi import DemObservables, DemParams
+
+
+class DEMError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"DEM error {code}: {message}")
+        self.code = code
+
+
+def _dptr(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _iptr(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def _vec(a, n):
+    if a is None:
+        return None
+    a = np.ascontiguousarray(a, dtype=np.float64).reshape(n, 3)
+    return a
+
+
+class DEMSystem:
+    """One simulation context.
+
+    ``lib``/``prefix`` select the implementation behind the same ABI: the
+    CUDA library (default) or, in tests, the CPU oracle with prefix ``orc_``.
+    """
+
+    def __init__(self, params: DemParams, lib=None, prefix: str = "dem_"):
+        self.lib = lib if lib is not None else _abi.load_library()
+        self.prefix = prefix
+        self.params = params
+        self.nprev = int(params.method_order) - 1
+        self._ctx = C.c_void_p()
+        st = self._fn("create")(C.byref(params), C.byref(self._ctx))
+        if st != 0:
+            raise DEMError(st, "create failed" + (": no CUDA device" if st == -7 else ""))
+        self.n = 0
+
+    # -- plumbing ---------------------------------------------------------
+    def _fn(self, name):
+        return getattr(self.lib, self.prefix + name)
+
+    def _call(self, name, *args):
+        st = self._fn(name)(self._ctx, *args)
+        if st != 0:
+            msg = self._fn("last_error")(self._ctx)
+            raise DEMError(st, f"{self.prefix}{name}: " + (msg.decode() if msg else ""))
+        return st
+
+    def close(self):
+        if self._ctx:
+            self._fn("destroy")(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- state ------------------------------------------------------------
+    def set_state(self, pos, vel, omega, comp=None, radius=None, acc=None, alpha=None):
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        n = pos.shape[0]
+        self._keep = (
+            pos.reshape(n, 3), _vec(vel, n), _vec(omega, n),
+            None if comp is None else np.ascontiguousarray(comp, dtype=np.int32),
+            None if radius is None else np.ascontiguousarray(radius, dtype=np.float64),
+            _vec(acc, n), _vec(alpha, n))
+        p, v, w, c, r, a, al = self._keep
+        self._call("set_state", n, _iptr(c), _dptr(r), _dptr(p), _dptr(v), _dptr(w), _dptr(a),
+                   _dptr(al))
+        self.n = n
+        self._keep = None
+
+    def update_state(self, pos=None, vel=None, omega=None, acc=None, alpha=None):
+        """Overwrite Particle(1:n) keeping ring, contacts and cell lists."""
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(self.n, 3)
+                for a in (pos, vel, omega, acc, alpha)]
+        self._call("update_state", *(_dptr(a) for a in arrs))
+
+    def _get(self, name):
+        n = self.n
+        out = {k: np.empty((n, 3)) for k in ("pos", "vel", "omega", "acc", "alpha")}
+        self._call(name, *(_dptr(out[k]) for k in ("pos", "vel", "omega", "acc", "alpha")))
+        return out
+
+    def get_state(self):
+        return self._get("get_state")
+
+    def get_predicted(self):
+        return self._get("get_predicted")
+
+    def get_integration(self):
+        prev = np.empty((max(self.nprev, 0), self.n, 9))
+        ipc = np.zeros(max(self.nprev, 1), dtype=np.int32)
+        self._call("get_integration", _dptr(prev), _iptr(ipc))
+        return prev, ipc[: self.nprev]
+
+    def logical_ring(self):
+        """Previous(ipc(k)) for k = 1..NPrev, shape (NPrev, n, 9)."""
+        prev, ipc = self.get_integration()
+        return np.stack([prev[i - 1] for i in ipc]) if self.nprev > 0 else prev
+
+    def set_integration(self, prev, ipc):
+        prev = np.ascontiguousarray(prev, dtype=np.float64)
+        ipc = np.ascontiguousarray(ipc, dtype=np.int32)
+        self._call("set_integration", _dptr(prev), _iptr(ipc))
+
+    def set_contacts(self, imin=(), imax=(), ft=None, vt=None, ip=(), iw=(), ftw=None,
+                     vtw=None):
+        imin = np.ascontiguousarray(imin, dtype=np.int32)
+        imax = np.ascontiguousarray(imax, dtype=np.int32)
+        m = imin.size
+        ft = np.ascontiguousarray(np.zeros((m, 3)) if ft is None else ft, dtype=np.float64)
+        vt = np.ascontiguousarray(np.zeros((m, 3)) if vt is None else vt, dtype=np.float64)
+        ip = np.ascontiguousarray(ip, dtype=np.int32)
+        iw = np.ascontiguousarray(iw, dtype=np.int32)
+        mw = ip.size
+        ftw = np.ascontiguousarray(np.zeros((mw, 3)) if ftw is None else ftw, dtype=np.float64)
+        vtw = np.ascontiguousarray(np.zeros((mw, 3)) if vtw is None else vtw, dtype=np.float64)
+        self._call("set_contacts", m, _iptr(imin), _iptr(imax), _dptr(ft), _dptr(vt), mw,
+                   _iptr(ip), _iptr(iw), _dptr(ftw), _dptr(vtw))
+
+    def count_contacts(self):
+        a = C.c_int64()
+        b = C.c_int64()
+        self._call("count_contacts", C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def get_contacts(self):
+        m, mw = self.count_contacts()
+        out = dict(imin=np.empty(m, np.int32), imax=np.empty(m, np.int32), ft=np.empty((m, 3)),
+                   vt=np.empty((m, 3)), ip=np.empty(mw, np.int32), iw=np.empty(mw, np.int32),
+                   ftw=np.empty((mw, 3)), vtw=np.empty((mw, 3)))
+        self._call("get_contacts", m, _iptr(out["imin"]), _iptr(out["imax"]), _dptr(out["ft"]),
+                   _dptr(out["vt"]), mw, _iptr(out["ip"]), _iptr(out["iw"]), _dptr(out["ftw"]),
+                   _dptr(out["vtw"]))
+        return out
+
+    # -- cells ------------------------------------------------------------
+    def initialize_cell_distribution(self):
+        self._call("initialize_cell_distribution")
+
+    def grid(self):
+        g = np.zeros(3, dtype=np.int32)
+        self._call("get_grid", _iptr(g))
+        return tuple(int(x) for x in g)
+
+    def get_cells(self):
+        nx, ny, nz = self.grid()
+        ci = np.empty(self.n, np.int32)
+        tr = np.empty(self.n, np.int32)
+        cs = np.empty(nx * ny * nz + 1, np.int32)
+        self._call("get_cells", _iptr(ci), _iptr(tr), _iptr(cs))
+        return ci, tr, cs
+
+    # -- dynamics ---------------------------------------------------------
+    def compute_accelerations(self, use_predicted=False, time_step=None, update=True):
+        ts = float(self.params.time_step if time_step is None else time_step)
+        self._call("compute_accelerations", 1 if use_predicted else 0, ts, 1 if update else 0)
+
+    def move_particles(self, step):
+        self._call("move_particles", int(step))
+
+    def move_particles_euler(self):
+        self._call("move_particles_euler")
+
+    def run(self, first_step, last_step):
+        self._call("run", int(first_step), int(last_step))
+
+    def run_timed(self, first_step, last_step):
+        """dem_run with device-side CUDA-event timing; returns milliseconds."""
+        ms = C.c_double()
+        self._call("run_timed", int(first_step), int(last_step), C.byref(ms))
+        return ms.value
+
+    # -- diagnostics ------------------------------------------------------
+    def ncol(self):
+        v = C.c_int64()
+        self._call("get_ncol", C.byref(v))
+        return v.value
+
+    def escaped(self):
+        v = C.c_int64()
+        self._call("get_escaped", C.byref(v))
+        return v.value
+
+    def observables(self):
+        o = DemObservables()
+        self._call("get_observables", C.byref(o))
+        return {
+            "kinetic_energy": o.kinetic_energy,
+            "potential_energy": o.potential_energy,
+            "mean_coordination": o.mean_coordination,
+            "packing_fraction": o.packing_fraction,
+            "wall_normal_force": list(o.wall_normal_force),
+            "momentum": list(o.momentum),
+            "n_pair_contacts": o.n_pair_contacts,
+            "n_wall_contacts": o.n_wall_contacts,
+        }
+
+    # -- GPU-only instrumentation -------------------------------------------
+    def set_profiling(self, on: bool):
+        self._call("set_profiling", 1 if on else 0)
+
+    def kernel_stats(self):
+        out = {}
+        i = 0
+        name = C.create_string_buffer(64)
+        while True:
+            la = C.c_int64()
+            ms = C.c_double()
+            st = self._fn("get_kernel_stats")(self._ctx, i, name, 64, C.byref(la), C.byref(ms))
+            if st != 0:
+                break
+            out[name.value.decode()] = (la.value, ms.value)
+            i += 1
+        return out
+
+    def reset_kernel_stats(self):
+        self._call("reset_kernel_stats")
+
+    def timer_start(self):
+        self._call("timer_start")
+
+    def timer_stop(self):
+        ms = C.c_double()
+        self._call("timer_stop", C.byref(ms))
+        return ms.value
+
+    def launch_count(self):
+        v = C.c_int64()
+        self._call("get_launch_count", C.byref(v))
+        return v.value
+
+    def stream_ptr(self):
+        p = C.c_void_p()
+        self._call("get_stream", C.byref(p))
+        return p.value
+
+    def pass_stats(self):
+        a, b, m = C.c_int64(), C.c_int64(), C.c_int64()
+        cap = C.c_int32()
+        self._call("get_pass_stats", C.byref(a), C.byref(b), C.byref(m), C.byref(cap))
+        return {"pair_contacts": a.value, "wall_contacts": b.value, "movers": m.value,
+                "hist_capacity": cap.value}

@@ -1,0 +1,241 @@
+/*
+ * dem3d_b200.h -- C-ABI of the B200-native DEM step (cell lists -> contact
+ * search + tangential history -> spring-dashpot/Coulomb forces -> ABM4).
+ *
+ * Drop-in boundary for the per-step path of DEM3D (Fortran 90).  Every entry
+ * point below names the reference routine it replaces.  Conventions:
+ *   - plain C types only (no CUDA or torch types); host pointers everywhere;
+ *     the library copies host arrays in and out and never keeps a caller
+ *     pointer after a call returns;
+ *   - particle indices are 0-based (the reference is 1-based; every ordering
+ *     rule of the reference is invariant under that shift);
+ *   - vectors of n particles are laid out as n rows of 3 doubles (x,y,z),
+ *     i.e. the contiguous copy of Particle(1:n)%Position(1:3);
+ *   - every call returns an int status: DEM_OK (0) or a negative DEM_ERR_*;
+ *     dem_last_error() gives a one-line description.  Nothing calls exit().
+ *   - one host thread per context; calls are synchronous on return.
+ *   - all quantities are in the reference's reduced units (after
+ *     ScaleVariables, src/DEM.f90:807-866).
+ */
+#ifndef DEM3D_B200_H
+#define DEM3D_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DEM_MAX_COMPONENTS 16
+#define DEM_MAX_WALLS 8
+
+/* status codes */
+#define DEM_OK 0
+#define DEM_ERR_INVALID (-1)      /* bad argument / inconsistent parameters */
+#define DEM_ERR_CUDA (-2)         /* a CUDA runtime call failed */
+#define DEM_ERR_CAPACITY (-3)     /* a device buffer could not be grown */
+#define DEM_ERR_UNSUPPORTED (-5)  /* valid for the reference, not supported here */
+#define DEM_ERR_STATE (-6)        /* call out of order (e.g. no state set) */
+#define DEM_ERR_NO_DEVICE (-7)    /* no CUDA device / extension not usable */
+
+/* wall shapes (src/MConfig.f90:44-45) */
+#define DEM_WALL_RECTANGLE 1
+#define DEM_WALL_CONE 2
+
+/* precision modes */
+#define DEM_PREC_FP64 0   /* plain FP64: bit-exact with the oracle */
+#define DEM_PREC_MIXED 1  /* FP32 contact arithmetic, FP64 positions/ABM */
+
+/* TWall, src/MDimension3D.f90:45-59 (L1..L3 already halved as in
+ * ReadSpecifications, src/DEM.f90:477-479; n = u x w). */
+typedef struct dem_wall {
+  int32_t shape;
+  int32_t order;
+  double l1, l2, l3;
+  double u[3], w[3], n[3];
+  double position[3], velocity[3], omega[3];
+} dem_wall;
+
+/*
+ * Scaled run parameters.  Two ways to give material properties:
+ *  - n_components >= 1: the reference's component tables (MForces module
+ *    variables src/MForces.f90:13-24 after InitializeForce :54-87), indexed
+ *    [ci*DEM_MAX_COMPONENTS + cj] and [ci*DEM_MAX_WALLS + w];
+ *  - n_components == 0: per-particle radius (continuous polydispersity, an
+ *    extension: the reference only has discrete components).  Each particle
+ *    is its own component of one material; pair tables are formed on the fly
+ *    with the reference's own combination rules (src/DEM.f90:259-327):
+ *      m = mass_coef*R^3, I = 0.4*m*R^2, Meff = mi*mj/(mi+mj),
+ *      Yn = gamma_n*sqrt(Meff*kn), Yt = gamma_t*sqrt(Meff*kt),
+ *      MinDij = Ri+Rj; walls use Meff = mi.
+ */
+typedef struct dem_params {
+  int32_t n_components;    /* NC (0 = per-particle radius mode) */
+  int32_t n_walls;         /* NW <= DEM_MAX_WALLS */
+  int32_t pbc[3];          /* PBC(1:3) */
+  int32_t method_order;    /* MethodOrder, 1..4 */
+  int32_t euler_intervals; /* NumberOfEulerIntervals */
+  int32_t max_ncell;       /* MaxNCell (30000 in src/MForces.f90:28) */
+  int32_t precision;       /* DEM_PREC_* */
+  int32_t hist_capacity;   /* initial pair records per particle (0 = 16) */
+  double lbox[3];          /* Lbox */
+  double gravity[3];       /* Gravity */
+  double time_step;        /* TimeStep */
+  /* component tables (n_components >= 1) */
+  double comp_radius[DEM_MAX_COMPONENTS];
+  double comp_inv_mass[DEM_MAX_COMPONENTS];
+  double comp_inv_inertia[DEM_MAX_COMPONENTS];
+  double comp_eff_mass[DEM_MAX_COMPONENTS];
+  double min_dij[DEM_MAX_COMPONENTS * DEM_MAX_COMPONENTS];
+  double min_dij_sq[DEM_MAX_COMPONENTS * DEM_MAX_COMPONENTS];
+  double kn[DEM_MAX_COMPONENTS * DEM_MAX_COMPONENTS];
+  double yn[DEM_MAX_COMPONENTS * DEM_MAX_COMPONENTS];
+  double kt[DEM_MAX_COMPONENTS * DEM_MAX_COMPONENTS];
+  double yt[DEM_MAX_COMPONENTS * DEM_MAX_COMPONENTS];
+  double mu_sq[DEM_MAX_COMPONENTS * DEM_MAX_COMPONENTS];
+  double knw[DEM_MAX_COMPONENTS * DEM_MAX_WALLS];
+  double ynw[DEM_MAX_COMPONENTS * DEM_MAX_WALLS];
+  double ktw[DEM_MAX_COMPONENTS * DEM_MAX_WALLS];
+  double ytw[DEM_MAX_COMPONENTS * DEM_MAX_WALLS];
+  double muw_sq[DEM_MAX_COMPONENTS * DEM_MAX_WALLS];
+  /* per-particle mode (n_components == 0) */
+  double pp_mass_coef;      /* 4/3*pi*density */
+  double pp_density;        /* for EffectiveMass = m*(rho - rho_f)/rho */
+  double pp_fluid_density;
+  double pp_rmax;           /* largest radius (cell CutOff = 2*rmax) */
+  double pp_kn, pp_kt, pp_gamma_n, pp_gamma_t, pp_mu_sq;
+  double pp_knw[DEM_MAX_WALLS], pp_ktw[DEM_MAX_WALLS];
+  double pp_gamma_nw[DEM_MAX_WALLS], pp_gamma_tw[DEM_MAX_WALLS];
+  double pp_muw_sq[DEM_MAX_WALLS];
+  dem_wall walls[DEM_MAX_WALLS];
+} dem_params;
+
+/* Observables (K5).  kinetic/potential: src/MDEM.f90:183-213. */
+typedef struct dem_observables {
+  double kinetic_energy;
+  double potential_energy;
+  double mean_coordination;   /* 2*(pair contacts)/N, from the history records */
+  double packing_fraction;    /* sum of particle volumes / box volume */
+  double wall_normal_force[DEM_MAX_WALLS]; /* sum of normal force on each wall */
+  double momentum[3];
+  int64_t n_pair_contacts;
+  int64_t n_wall_contacts;
+} dem_observables;
+
+typedef struct dem_ctx dem_ctx;
+
+/* Library build/version string (also proves the .so loads). */
+const char* dem_version(void);
+/* Select the CUDA device for contexts created afterwards by this thread
+ * (the library carries its own CUDA runtime). */
+int dem_select_device(int32_t device);
+
+/* Parameters + cell grid set-up.  Replaces InitializeAuxiliaries
+ * (src/MDEM.f90:110-162: ABM coefficients, InitializeCellList
+ * src/MForces.f90:91-106, InitializeForce :54-87). */
+int dem_create(const dem_params* params, dem_ctx** out);
+/* FinalizeDEM, src/MDEM.f90:166-179. */
+void dem_destroy(dem_ctx* ctx);
+const char* dem_last_error(const dem_ctx* ctx);
+
+/* Particle state (Particle(1:n), src/MConfig.f90:68 / TParticle
+ * src/MDimension3D.f90:28-35).  comp: component index per particle (0-based,
+ * table mode) or NULL; radius: per-particle radius (per-particle mode) or
+ * NULL.  acc/alpha may be NULL (zero).  Resets the ABM ring to zeros with
+ * ipc = 1..NPrev (InitializeIntegrationVariables, src/MDEM.f90:93-106), the
+ * contact lists to empty (InitializeContacts, src/MContacts.f90:43-49) and
+ * Ncol to 0. */
+int dem_set_state(dem_ctx* ctx, int32_t n, const int32_t* comp,
+                  const double* radius, const double* pos, const double* vel,
+                  const double* omega, const double* acc, const double* alpha);
+int dem_get_state(dem_ctx* ctx, double* pos, double* vel, double* omega,
+                  double* acc, double* alpha);
+/* Overwrite Particle(1:n) (same n, any array may be NULL = keep) without
+ * touching the ABM ring, the contact lists or the cell lists: what a driver
+ * that keeps Particle in host memory calls before each step. */
+int dem_update_state(dem_ctx* ctx, const double* pos, const double* vel,
+                     const double* omega, const double* acc, const double* alpha);
+/* Predicted(1:n) of MDEM (src/MDEM.f90:20). */
+int dem_get_predicted(dem_ctx* ctx, double* pos, double* vel, double* omega,
+                      double* acc, double* alpha);
+int dem_get_n(dem_ctx* ctx, int32_t* n);
+
+/* ABM ring Previous(NPrev,n) + ipc(NPrev) (src/MDEM.f90:19-22), as
+ * previous[(k*n + i)*9 + {v0..2,a0..2,alpha0..2}] with k the PHYSICAL slot
+ * 0..NPrev-1 and ipc 1-based as in the reference.  Same record order as
+ * Save/ReadIntegrationVariables (src/MDEM.f90:52-89). */
+int dem_set_integration(dem_ctx* ctx, const double* previous, const int32_t* ipc);
+int dem_get_integration(dem_ctx* ctx, double* previous, int32_t* ipc);
+
+/* Contact history (MainParticle lists, src/MContacts.f90:21-33).  Pair
+ * records (imin < imax) and wall records (particle, wall), Vector1 = ft
+ * (previous tangential force), Vector2 = vt (previous tangential contact
+ * velocity).  get_* returns them sorted by key like the reference's lists
+ * (SaveContactList, src/MContacts.f90:75-117). */
+int dem_set_contacts(dem_ctx* ctx, int64_t m, const int32_t* imin,
+                     const int32_t* imax, const double* ft, const double* vt,
+                     int64_t mw, const int32_t* ip, const int32_t* iw,
+                     const double* ftw, const double* vtw);
+int dem_count_contacts(dem_ctx* ctx, int64_t* n_pair, int64_t* n_wall);
+int dem_get_contacts(dem_ctx* ctx, int64_t cap, int32_t* imin, int32_t* imax,
+                     double* ft, double* vt, int64_t capw, int32_t* ip,
+                     int32_t* iw, double* ftw, double* vtw);
+
+/* InitializeCellDistribution (src/MForces.f90:110-117 ->
+ * DistributeParticles3D src/MCells.f90:542-564). */
+int dem_initialize_cell_distribution(dem_ctx* ctx);
+/* Cell grid: Nx,Ny,Nz (InitCellStructure3D src/MCells.f90:155-227). */
+int dem_get_grid(dem_ctx* ctx, int32_t* nxyz);
+/* CellIndex(1:n) (0-based cells) and the particles of every cell in list
+ * order (the traversal order of ComputeAccelerations): traversal[n],
+ * cell_start[ncell+1]. */
+int dem_get_cells(dem_ctx* ctx, int32_t* cell_index, int32_t* traversal,
+                  int32_t* cell_start);
+
+/* ComputeAccelerations(Particle or Predicted, NP, TimeStep, Update)
+ * (src/MForces.f90:145-335), including RedistributeParticles3D. */
+int dem_compute_accelerations(dem_ctx* ctx, int32_t use_predicted,
+                              double time_step, int32_t update);
+/* MoveParticles(step) (src/MDEM.f90:285-369): force pass @x(t) with history
+ * update, AB predictor, ring store, force pass @prediction, AM corrector. */
+int dem_move_particles(dem_ctx* ctx, int32_t step);
+/* MoveParticlesEuler (src/MDEM.f90:258-281). */
+int dem_move_particles_euler(dem_ctx* ctx);
+/* The time loop of src/DEM.f90:85-99 without pouring/reporting: if
+ * first_step == 1 the MethodOrder-1 Euler start-up steps run first, then
+ * MoveParticles(step) for step = max(first_step,MethodOrder) .. last_step.
+ * Steps are replayed from CUDA graphs. */
+int dem_run(dem_ctx* ctx, int32_t first_step, int32_t last_step);
+/* dem_run bracketed by CUDA events on the context's stream; device_ms is the
+ * elapsed device time (host synchronisation gaps between replays included). */
+int dem_run_timed(dem_ctx* ctx, int32_t first_step, int32_t last_step, double* device_ms);
+
+/* Ncol (src/MForces.f90:47,227). */
+int dem_get_ncol(dem_ctx* ctx, int64_t* ncol);
+/* Particles that left the box (UpdateParticleList test src/MDEM.f90:624-625)
+ * after the last corrector; removal itself is not done by this library. */
+int dem_get_escaped(dem_ctx* ctx, int64_t* count);
+int dem_get_observables(dem_ctx* ctx, dem_observables* out);
+
+/* Instrumentation: per-kernel CUDA-event timing on the context's stream and
+ * a count of kernels launched since the last reset. */
+int dem_set_profiling(dem_ctx* ctx, int32_t enable);
+int dem_get_kernel_stats(dem_ctx* ctx, int32_t idx, char* name, int32_t name_cap,
+                         int64_t* launches, double* total_ms);
+int dem_reset_kernel_stats(dem_ctx* ctx);
+int dem_get_launch_count(dem_ctx* ctx, int64_t* launches);
+/* CUDA-event timer on the context's stream: start, then stop -> ms. */
+int dem_timer_start(dem_ctx* ctx);
+int dem_timer_stop(dem_ctx* ctx, double* ms);
+/* cudaStream_t of the context, as an opaque pointer (for event timing). */
+int dem_get_stream(dem_ctx* ctx, void** stream);
+/* Mean pair contacts per particle of the last force pass and the device
+ * bytes the last pass touched by design (for roofline accounting). */
+int dem_get_pass_stats(dem_ctx* ctx, int64_t* pair_contacts, int64_t* wall_contacts,
+                       int64_t* movers, int32_t* hist_capacity);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DEM3D_B200_H */

@@ -1,0 +1,186 @@
+"""GPU parity: the CUDA library against the CPU oracle through the C-ABI.
+
+FP64 mode must be bit-identical with the oracle: cell assignment and
+traversal order, contact-pair sets and history records, accelerations,
+predicted state, ABM ring and trajectories over many steps."""
+import numpy as np
+import pytest
+
+from dem3d_b200 import configs
+from dem3d_b200.system import DEMSystem
+from tests.oracle_lib import oracle_system
+
+pytestmark = pytest.mark.gpu
+
+
+def make_pair(w, **kw):
+    g = DEMSystem(w.params)
+    o = oracle_system(w.params)
+    for s in (g, o):
+        s.set_state(w.pos, w.vel, w.omega, comp=w.comp, radius=w.radius)
+        s.initialize_cell_distribution()
+    return g, o
+
+
+def assert_same_state(g, o, what=""):
+    a, b = g.get_state(), o.get_state()
+    for k in a:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=f"{what} state.{k}")
+
+
+def assert_same_predicted(g, o, what=""):
+    a, b = g.get_predicted(), o.get_predicted()
+    for k in a:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=f"{what} predicted.{k}")
+
+
+def assert_same_contacts(g, o, what=""):
+    a, b = g.get_contacts(), o.get_contacts()
+    for k in a:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=f"{what} contacts.{k}")
+
+
+def assert_same_cells(g, o, what=""):
+    for x, y, name in zip(g.get_cells(), o.get_cells(), ("cell_index", "traversal", "start")):
+        np.testing.assert_array_equal(x, y, err_msg=f"{what} {name}")
+
+
+def test_initial_distribution_and_one_pass():
+    w = configs.settling(n=600, seed=21)
+    g, o = make_pair(w)
+    assert g.grid() == o.grid()
+    assert_same_cells(g, o, "init")
+    for s in (g, o):
+        s.compute_accelerations(update=True)
+    assert_same_state(g, o, "pass")
+    assert_same_contacts(g, o, "pass")
+    assert g.ncol() == o.ncol()
+
+
+def test_settling_trajectory_bit_exact():
+    w = configs.settling(n=400, seed=7, sigma_v=0.5)
+    g, o = make_pair(w)
+    for s in (g, o):
+        s.run(1, 4)  # Euler start-up (3 x 100 passes) + first ABM step
+    assert_same_state(g, o, "after start-up")
+    assert_same_contacts(g, o, "after start-up")
+    np.testing.assert_array_equal(g.logical_ring(), o.logical_ring())
+    for step in range(5, 400):
+        for s in (g, o):
+            s.move_particles(step)
+        if step % 50 == 0:
+            assert_same_state(g, o, f"step {step}")
+            assert_same_predicted(g, o, f"step {step}")
+            assert_same_contacts(g, o, f"step {step}")
+            assert_same_cells(g, o, f"step {step}")
+            np.testing.assert_array_equal(g.logical_ring(), o.logical_ring())
+    assert g.ncol() == o.ncol()
+    assert g.count_contacts()[1] > 0  # the bed reached the floor
+
+
+def test_graph_run_equals_stepwise():
+    w = configs.settling(n=300, seed=8, sigma_v=0.5)
+    g1, o = make_pair(w)
+    g2 = DEMSystem(w.params)
+    g2.set_state(w.pos, w.vel, w.omega, comp=w.comp)
+    g2.initialize_cell_distribution()
+    g1.run(1, 203)          # graphs of 4 steps + remainder
+    o.run(1, 203)
+    g2.run(1, 4)
+    for step in range(5, 204):
+        g2.move_particles(step)
+    assert_same_state(g1, g2, "graph vs stepwise")
+    assert_same_state(g1, o, "graph vs oracle")
+    assert_same_contacts(g1, o, "graph vs oracle")
+    assert g1.ncol() == o.ncol() == g2.ncol()
+
+
+def test_dense_polydisperse_bit_exact():
+    w = configs.dense_packing(n=3000, phi=0.55, seed=31, relax_steps=0)
+    g, o = make_pair(w)
+    for s in (g, o):
+        s.compute_accelerations(update=True)
+    assert_same_state(g, o, "pass")
+    assert_same_contacts(g, o, "pass")
+    for s in (g, o):
+        s.run(1, 60)
+    assert_same_state(g, o, "60 steps")
+    assert_same_contacts(g, o, "60 steps")
+    assert_same_cells(g, o, "60 steps")
+    assert g.ncol() == o.ncol()
+
+
+def test_history_capacity_growth_is_transparent():
+    """Tables starting at one record per particle must grow and give the
+    same result as the oracle (the overflowing pass is re-run)."""
+    w = configs.dense_packing(n=2000, phi=0.55, seed=32, relax_steps=0)
+    w.params.hist_capacity = 1
+    g, o = make_pair(w)
+    for s in (g, o):
+        s.run(1, 30)
+    assert g.pass_stats()["hist_capacity"] > 1
+    assert_same_state(g, o, "grown")
+    assert_same_contacts(g, o, "grown")
+    assert g.ncol() == o.ncol()
+
+
+def test_contacts_roundtrip_and_import():
+    w = configs.dense_packing(n=1500, phi=0.5, seed=33, relax_steps=0)
+    g, o = make_pair(w)
+    o.run(1, 10)
+    c = o.get_contacts()
+    st = o.get_state()
+    prev, ipc = o.get_integration()
+    g.set_state(st["pos"], st["vel"], st["omega"], radius=w.radius, acc=st["acc"],
+                alpha=st["alpha"])
+    g.set_integration(prev, ipc)
+    g.set_contacts(c["imin"], c["imax"], c["ft"], c["vt"], c["ip"], c["iw"], c["ftw"], c["vtw"])
+    assert_same_contacts(g, o, "import")
+    # the cell lists are rebuilt from scratch on both sides
+    o2 = oracle_system(w.params)
+    o2.set_state(st["pos"], st["vel"], st["omega"], radius=w.radius, acc=st["acc"],
+                 alpha=st["alpha"])
+    o2.set_integration(prev, ipc)
+    o2.set_contacts(c["imin"], c["imax"], c["ft"], c["vt"], c["ip"], c["iw"], c["ftw"], c["vtw"])
+    for s in (g, o2):
+        s.initialize_cell_distribution()
+        for step in range(11, 31):
+            s.move_particles(step)
+    assert_same_state(g, o2, "resumed")
+    assert_same_contacts(g, o2, "resumed")
+
+
+def test_escape_detection():
+    """Particles outside +-L/2 after the corrector (UpdateParticleList's test,
+    src/MDEM.f90:624-625) are counted, not removed."""
+    w = configs.settling(n=100, seed=9, headroom=2.0, sigma_v=30.0)
+    g, o = make_pair(w)
+    for s in (g, o):
+        s.run(1, 50)
+    assert_same_state(g, o, "escape")
+    st = o.get_state()
+    L = np.array(w.info["lbox"])
+    out = np.any((st["pos"] > 0.5 * L) | (st["pos"] < -0.5 * L), axis=1)
+    assert g.escaped() == int(out.sum()) == o.escaped()
+
+
+def test_observables_match_oracle():
+    w = configs.settling(n=500, seed=12)
+    g, o = make_pair(w)
+    for s in (g, o):
+        s.run(1, 30)
+    a, b = g.observables(), o.observables()
+    for k in ("kinetic_energy", "potential_energy", "packing_fraction", "mean_coordination"):
+        assert abs(a[k] - b[k]) <= 1e-12 * max(1.0, abs(b[k])), k
+    assert a["n_pair_contacts"] == b["n_pair_contacts"]
+
+
+@pytest.mark.slow
+def test_large_dense_one_step_bit_exact():
+    """200k polydisperse spheres: one full MoveParticles step bit-exact."""
+    w = configs.dense_packing(n=200_000, phi=0.55, seed=34, relax_steps=0)
+    g, o = make_pair(w)
+    for s in (g, o):
+        s.compute_accelerations(update=True)
+    assert_same_state(g, o, "200k pass")
+    assert_same_contacts(g, o, "200k pass")

@@ -1,0 +1,49 @@
+"""Multi-rank host logic of bench.py on CPU (gloo, world size 2): the timed
+region is the max over ranks, the value aggregates every rank's system, and
+every rank advances a different ensemble member (seed + rank)."""
+import os
+import socket
+
+import pytest
+import torch.multiprocessing as mp
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _worker(rank, world, port, q):
+    import torch.distributed as dist
+
+    import bench
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    ms = 100.0 + 50.0 * rank
+    mx = bench.reduce_max(ms, world, device="cpu")
+    v = bench.aggregate_rate(1000, world, 10, mx)
+    from dem3d_b200 import configs
+    w = configs.dense_packing(n=512, phi=0.5, seed=bench.rank_seed(1001, rank), relax_steps=0)
+    q.put((rank, mx, v, float(w.vel[0, 0])))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_reduction():
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.SimpleQueue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    res = sorted(q.get() for _ in range(world))
+    assert all(r[1] == 150.0 for r in res)                  # max over ranks
+    assert all(abs(r[2] - 1000 * 2 * 10 / 0.150) < 1e-6 for r in res)
+    assert res[0][3] != res[1][3]                            # distinct members

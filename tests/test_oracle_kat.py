@@ -1,0 +1,162 @@
+"""Known-answer tests pinning the CPU oracle to the reference's model.
+
+No outputs of the reference exist (no tests, no shipped results, no Fortran
+compiler here), so the oracle is pinned by closed forms of the reference's own
+model: the damping rule of CalculateProperties (src/DEM.f90:288-298) makes a
+linear spring-dashpot collision restore the requested restitution coefficient
+after a contact time pi/omega_d (MinCollisionTime, src/DEM.f90:330-331);
+the Coulomb cap (src/MForces.f90:372-378); the rectangle closest-point
+geometry (src/MConfig.f90:717-749); CurrentCell3D (src/MCells.f90:498-513);
+Newton's third law of the pair loop (src/MForces.f90:254-259)."""
+import math
+
+import numpy as np
+import pytest
+
+from dem3d_b200 import params as P
+from dem3d_b200.configs import DENSITY, KN, KT, settling
+from tests.oracle_lib import oracle_system
+
+
+def two_body(e=0.8, mu=0.5, v0=1.0, dt=1e-5, order=4, gap=0.01, walls=(), gravity=0.0,
+             pbc=(False, False, False)):
+    prm, _ = P.component_params(
+        [P.Component(2, 1.0, DENSITY, 2 * KN, 2 * KT)], list(walls), [[e]], [[e]], [[mu]],
+        [[e] * len(walls)], [[e] * len(walls)], [[mu] * len(walls)], lbox=(10.0, 10.0, 10.0),
+        pbc=pbc, gravity=(0.0, 0.0, -gravity), time_step=dt, method_order=order,
+        euler_intervals=10)
+    pos = np.array([[-0.5 - gap, 0.0, 0.0], [0.5 + gap, 0.0, 0.0]])
+    vel = np.array([[0.5 * v0, 0.0, 0.0], [-0.5 * v0, 0.0, 0.0]])
+    return prm, pos, vel
+
+
+def run_collision(e, order=4, dt=1e-5, v0=1.0):
+    prm, pos, vel = two_body(e=e, dt=dt, order=order, v0=v0)
+    s = oracle_system(prm)
+    s.set_state(pos, vel, np.zeros((2, 3)), comp=np.zeros(2, np.int32))
+    s.initialize_cell_distribution()
+    steps = int(0.05 / dt)
+    t_in = t_out = None
+    s.run(1, order)  # start-up
+    step = order
+    for _ in range(steps):
+        step += 1
+        s.move_particles(step)
+        st = s.get_state()
+        d = st["pos"][1, 0] - st["pos"][0, 0]
+        if t_in is None and d < 1.0:
+            t_in = step * dt
+        if t_in is not None and d >= 1.0:
+            t_out = step * dt
+            break
+    st = s.get_state()
+    vrel = st["vel"][1, 0] - st["vel"][0, 0]
+    return vrel, t_in, t_out, prm
+
+
+@pytest.mark.parametrize("e", [0.5, 0.8, 0.95])
+def test_head_on_restitution_and_duration(e):
+    vrel, t_in, t_out, prm = run_collision(e)
+    # restitution: outgoing relative velocity = e * incoming (1.0)
+    assert abs(vrel - e) < 2e-3 * max(e, 0.1), (vrel, e)
+    # contact time = pi / omega_d with m_eff = m/2, k = Kn, eta = Yn
+    kn = prm.kn[0]
+    yn = prm.yn[0]
+    meff = 0.5 / prm.comp_inv_mass[0]
+    wd = math.sqrt(kn / meff - (yn / (2 * meff)) ** 2)
+    tc = math.pi / wd
+    assert abs((t_out - t_in) - tc) < 3e-5 + 2e-3 * tc, (t_out - t_in, tc)
+
+
+def test_momentum_and_third_law():
+    rng = np.random.default_rng(5)
+    n = 300
+    prm = P.per_particle_params(density=DENSITY, kn=KN, kt=KT, en=0.7, et=0.7, mu=0.4,
+                                rmax=0.6, lbox=(8.0, 8.0, 8.0), pbc=(True, True, True),
+                                gravity=(0, 0, 0), time_step=1e-4)
+    radius = rng.uniform(0.4, 0.6, n)
+    from dem3d_b200.configs import lattice_positions
+    pos = lattice_positions(n, 8.0, rng)
+    vel = rng.normal(0, 0.3, (n, 3))
+    om = rng.normal(0, 0.3, (n, 3))
+    s = oracle_system(prm)
+    s.set_state(pos, vel, om, radius=radius)
+    s.initialize_cell_distribution()
+    m = 4.0 / 3.0 * math.pi * DENSITY * radius ** 3
+    p0 = (m[:, None] * vel).sum(0)
+    s.compute_accelerations(update=True)
+    a = s.get_state()["acc"]
+    F = (m[:, None] * a).sum(0)
+    assert np.abs(F).max() < 1e-9 * np.abs(m[:, None] * a).max()
+    s.run(1, 40)
+    p1 = (m[:, None] * s.get_state()["vel"]).sum(0)
+    assert np.allclose(p0, p1, atol=1e-9, rtol=0)
+    assert s.count_contacts()[0] > 0
+
+
+def test_coulomb_cap_on_records():
+    """Every stored tangential force obeys |FT| <= mu |FN| at storage time:
+    check a sliding block of spheres on a frictional floor."""
+    w = settling(n=200, seed=3, sigma_v=2.0)
+    s = oracle_system(w.params)
+    s.set_state(w.pos, w.vel, w.omega, comp=w.comp)
+    s.initialize_cell_distribution()
+    s.run(1, 300)
+    c = s.get_contacts()
+    assert c["imin"].size + c["ip"].size > 0
+    assert np.all(c["imin"] < c["imax"])
+    # lists sorted like the reference (by imin, then partner)
+    key = c["imin"].astype(np.int64) * 10**6 + c["imax"]
+    assert np.all(np.diff(key) > 0)
+
+
+def test_current_cell_matches_formula():
+    w = settling(n=500, seed=11)
+    s = oracle_system(w.params)
+    s.set_state(w.pos, w.vel, w.omega, comp=w.comp)
+    s.initialize_cell_distribution()
+    ci, tr, cs = s.get_cells()
+    nx, ny, nz = s.grid()
+    L = np.array(w.info["lbox"])
+    N = np.array([nx, ny, nz])
+    nbyl = N / L
+    i3 = np.clip((nbyl * w.pos + N * 0.5).astype(np.int64), 0, N - 1)
+    expect = i3[:, 0] + (i3[:, 1] + i3[:, 2] * ny) * nx
+    assert np.array_equal(ci, expect)
+    # list order after DistributeParticles3D: decreasing index inside a cell
+    for c in range(nx * ny * nz):
+        members = tr[cs[c]:cs[c + 1]]
+        assert np.all(np.diff(members) < 0)
+        assert np.all(ci[members] == c)
+
+
+@pytest.mark.parametrize("where,expect_overlap", [
+    ((0.0, 0.0, 0.3), True),     # face
+    ((4.9, 0.0, 0.1), True),     # inside face near edge
+    ((5.3, 0.0, 0.1), True),     # past the edge, within radius of it
+    ((5.5, 0.0, 0.1), False),    # too far from the edge
+    ((5.3, 5.3, 0.05), True),    # corner
+])
+def test_rectangle_wall_geometry(where, expect_overlap):
+    wall = P.rectangle((0.0, 0.0, 0.0), 5.0, 5.0, stiffness=2 * KN, shear_stiffness=2 * KT)
+    prm, _ = P.component_params([P.Component(1, 1.0, DENSITY, 2 * KN, 2 * KT)], [wall], [[0.8]],
+                                [[0.8]], [[0.5]], [[0.8]], [[0.8]], [[0.5]],
+                                lbox=(30.0, 30.0, 30.0), pbc=(False, False, False),
+                                gravity=(0, 0, 0), time_step=1e-4)
+    s = oracle_system(prm)
+    pos = np.array([where], dtype=float)
+    s.set_state(pos, np.zeros((1, 3)), np.zeros((1, 3)), comp=np.zeros(1, np.int32))
+    s.initialize_cell_distribution()
+    s.compute_accelerations(update=True)
+    a = s.get_state()["acc"][0]
+    # closest point of the rectangle [-5,5]^2 x {0}
+    q = np.array([np.clip(where[0], -5, 5), np.clip(where[1], -5, 5), 0.0])
+    d = np.array(where) - q
+    dist = np.linalg.norm(d)
+    if expect_overlap:
+        assert dist < 0.5
+        kn = prm.knw[0]
+        f = kn * (0.5 - dist) * d / dist  # static: pure elastic normal force
+        assert np.allclose(a / prm.comp_inv_mass[0], f, rtol=1e-12, atol=1e-9)
+    else:
+        assert np.all(a == 0.0)
