@@ -49,7 +49,7 @@ class Workload:
 
 def settling(n=2000, seed=1000, layer_side=10, dt=1e-4, e=0.8, mu=0.5, gravity=1.0,
              headroom=45.0, method_order=4, euler_intervals=100, max_ncell=30000,
-             precision=P.PREC_FP64, sigma_v=0.1):
+             precision=P.PREC_FP64, sigma_v=0.1, first_height=1.0):
     """Monodisperse gravity settling (d = 1, m = 1).
 
     ``layer_side`` x ``layer_side`` spheres per layer at xy spacing 1.0 in a
@@ -74,7 +74,7 @@ def settling(n=2000, seed=1000, layer_side=10, dt=1e-4, e=0.8, mu=0.5, gravity=1
                     break
                 x = -0.5 * L + 0.5 + ix + sx
                 y = -0.5 * L + 0.5 + iy + sy
-                z = -0.5 * lz + 1.0 + 2.0 * layer + rng.uniform(-0.05, 0.05)
+                z = -0.5 * lz + first_height + 2.0 * layer + rng.uniform(-0.05, 0.05)
                 pos[k] = (x, y, z)
                 k += 1
     vel = rng.normal(0.0, sigma_v, size=(n, 3))

@@ -83,12 +83,25 @@ struct RingMap {
   int phys[5];  // phys[k] = physical slot of logical ipc(k+1); phys[nprev] = spare
 };
 
+// Contact lists emitted by the screening kernel, one row of KC slots per
+// particle: first the "p is i" partners in the order of p's neighbour list,
+// then the "p is j" partners in sweep order.  meta = (n1, n2 before p's own
+// block, n2 after it, 0); n1 = -1 when the row overflowed (the force kernel
+// then sweeps the cells itself for that particle).
+constexpr int KC = 32;
+struct ContactLists {
+  int* slot;   // [n*KC]
+  int4* meta;  // [n]
+};
+
 struct ForceArgs {
   const DevParams* P;
   int n;
   SortedArrays S;
   const int* cell_start;
   const int* cell_of_orig;
+  const int* cl_slot;
+  const int4* cl_meta;
   History Hr, Hw;
   int update;
   double half_dt;
@@ -299,6 +312,156 @@ __device__ __forceinline__ int current_cell(const DevParams& P, double x, double
   iy = iy > 0 ? iy : 0;
   iz = iz > 0 ? iz : 0;
   return ix + (iy + iz * P.ny) * P.nx;
+}
+
+// Are two cells neighbours in the sweep sense (same cell, or one in the
+// other's half-shell list)?  With >= 3 cells along every periodic axis this
+// is plain adjacency with wrap-around (VerifyPBC/ApplyPBC, src/MCells.f90:
+// 1030-1052).
+__device__ __forceinline__ bool cells_adjacent(const DevParams& P, int a, int b) {
+  int ax = a % P.nx, ay = (a / P.nx) % P.ny, az = a / (P.nx * P.ny);
+  int bx = b % P.nx, by = (b / P.nx) % P.ny, bz = b / (P.nx * P.ny);
+  int d[3] = {bx - ax, by - ay, bz - az};
+  int N[3] = {P.nx, P.ny, P.nz};
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    int x = d[k] < 0 ? -d[k] : d[k];
+    if (x > 1 && !(P.pbc[k] && x == N[k] - 1)) return false;
+  }
+  return true;
+}
+
+// axis helper: neighbour offsets of a cell coordinate, trimmed like VerifyPBC
+__device__ __forceinline__ void axis_range(int i, int N, int pbc, int& lo, int& hi) {
+  lo = -1;
+  hi = 1;
+  if (!pbc) {
+    if (i == 0) lo = 0;
+    if (i == N - 1) hi = 0;
+  }
+}
+__device__ __forceinline__ int axis_wrap(int j, int N, int pbc) {
+  if (pbc) {
+    if (j == N) j = 0;
+    if (j == -1) j = N - 1;
+  }
+  return j;
+}
+// offsets of one axis in ascending order of the wrapped cell coordinate
+__device__ __forceinline__ int axis_sorted(int i, int N, int pbc, int off[3]) {
+  int lo, hi;
+  axis_range(i, N, pbc, lo, hi);
+  int m = 0;
+  if (pbc && i == 0) {  // -1 wraps to N-1 (largest)
+    off[m++] = 0;
+    off[m++] = 1;
+    off[m++] = -1;
+  } else if (pbc && i == N - 1) {  // +1 wraps to 0 (smallest)
+    off[m++] = 1;
+    off[m++] = -1;
+    off[m++] = 0;
+  } else {
+    for (int k = lo; k <= hi; k++) off[m++] = k;
+  }
+  return m;
+}
+
+
+// ------------------------------------------------------------------------
+// the reference's cell sweep (ComputeAccelerations, src/MForces.f90:173-324)
+// seen from one particle p at traversal slot s of cell c = (cx, cy, cz)
+
+// Loop 1 ("p is i"): the neighbour list of p's block is the rest of its own
+// cell, then the half-shell cells in the order of the FirstNeighbour list,
+// which AddAllNeighbours3D (src/MCells.f90:424-476) builds by prepending in
+// kz, ky, kx loop order with kx + Nx*(ky + Ny*kz) > 0 (so: reverse order).
+template <class Visit>
+__device__ __forceinline__ void sweep_as_i(const DevParams& P, const int* __restrict__ cs, int s,
+                                           int c, int cx, int cy, int cz, Visit&& visit) {
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  const int e = cs[c + 1];
+  for (int t = s + 1; t < e; t++) visit(t);
+  int xi, xf, yi, yf, zi, zf;
+  axis_range(cx, nx, P.pbc[0], xi, xf);
+  axis_range(cy, ny, P.pbc[1], yi, yf);
+  axis_range(cz, nz, P.pbc[2], zi, zf);
+  for (int kz = zf; kz >= zi; kz--) {
+    const int jz = axis_wrap(cz + kz, nz, P.pbc[2]);
+    for (int ky = yf; ky >= yi; ky--) {
+      const int jy = axis_wrap(cy + ky, ny, P.pbc[1]);
+      for (int kx = xf; kx >= xi; kx--) {
+        if (kx + nx * (ky + ny * kz) <= 0) continue;
+        const int jx = axis_wrap(cx + kx, nx, P.pbc[0]);
+        const int jc = jx + nx * (jy + ny * jz);
+        const int b = cs[jc], e2 = cs[jc + 1];
+        for (int t = b; t < e2; t++) visit(t);
+      }
+    }
+  }
+}
+
+// Loop 2 ("p is j"): every particle q whose block lists p -- the earlier
+// members of p's cell and the members of the cells whose half shell holds
+// p's cell -- in the order the sweep reaches q (ascending cell index, then
+// list order); own() is called where p's own block ends (Force(i) =
+// Force(i) + iForce, src/MForces.f90:319-320).
+template <class Visit, class Own>
+__device__ __forceinline__ void sweep_as_j(const DevParams& P, const int* __restrict__ cs, int s,
+                                           int c, int cx, int cy, int cz, Visit&& visit,
+                                           Own&& own) {
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  int ox[3], oy[3], oz[3];
+  const int mx = axis_sorted(cx, nx, P.pbc[0], ox);
+  const int my = axis_sorted(cy, ny, P.pbc[1], oy);
+  const int mz = axis_sorted(cz, nz, P.pbc[2], oz);
+  for (int a = 0; a < mz; a++) {
+    const int dz = oz[a];
+    const int jz = axis_wrap(cz + dz, nz, P.pbc[2]);
+    for (int b = 0; b < my; b++) {
+      const int dy = oy[b];
+      const int jy = axis_wrap(cy + dy, ny, P.pbc[1]);
+      for (int d = 0; d < mx; d++) {
+        const int dx = ox[d];
+        if (dx == 0 && dy == 0 && dz == 0) {
+          for (int t = cs[c]; t < s; t++) visit(t);
+          own();
+          continue;
+        }
+        // p's cell is in the half shell of the cell at offset (dx,dy,dz)
+        if (-dx + nx * (-dy + ny * -dz) <= 0) continue;
+        const int jx = axis_wrap(cx + dx, nx, P.pbc[0]);
+        const int jc = jx + nx * (jy + ny * jz);
+        const int b0 = cs[jc], e2 = cs[jc + 1];
+        for (int t = b0; t < e2; t++) visit(t);
+      }
+    }
+  }
+}
+
+// Loop 1 / loop 2 driven by the screening kernel's contact list when the
+// particle's row did not overflow, else by the full sweep (same order).
+template <class Visit>
+__device__ __forceinline__ void walk_as_i(const ForceArgs& A, int4 meta, int s, int c, int cx,
+                                          int cy, int cz, Visit&& visit) {
+  if (meta.x >= 0) {
+    const int* l = A.cl_slot + (size_t)s * KC;
+    for (int k = 0; k < meta.x; k++) visit(l[k]);
+  } else {
+    sweep_as_i(*A.P, A.cell_start, s, c, cx, cy, cz, visit);
+  }
+}
+
+template <class Visit, class Own>
+__device__ __forceinline__ void walk_as_j(const ForceArgs& A, int4 meta, int s, int c, int cx,
+                                          int cy, int cz, Visit&& visit, Own&& own) {
+  if (meta.x >= 0) {
+    const int* l = A.cl_slot + (size_t)s * KC + meta.x;
+    for (int k = 0; k < meta.y; k++) visit(l[k]);
+    own();
+    for (int k = meta.y; k < meta.y + meta.z; k++) visit(l[k]);
+  } else {
+    sweep_as_j(*A.P, A.cell_start, s, c, cx, cy, cz, visit, own);
+  }
 }
 
 }  // namespace dem

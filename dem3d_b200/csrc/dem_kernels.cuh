@@ -322,58 +322,6 @@ __device__ __forceinline__ void hist_write(const History& H, int owner, int r, i
   v[2] = make_double2(vt[1], vt[2]);
 }
 
-// Are two cells neighbours in the sweep sense (same cell, or one in the
-// other's half-shell list)?  With >= 3 cells along every periodic axis this
-// is plain adjacency with wrap-around (VerifyPBC/ApplyPBC, src/MCells.f90:
-// 1030-1052).
-__device__ __forceinline__ bool cells_adjacent(const DevParams& P, int a, int b) {
-  int ax = a % P.nx, ay = (a / P.nx) % P.ny, az = a / (P.nx * P.ny);
-  int bx = b % P.nx, by = (b / P.nx) % P.ny, bz = b / (P.nx * P.ny);
-  int d[3] = {bx - ax, by - ay, bz - az};
-  int N[3] = {P.nx, P.ny, P.nz};
-#pragma unroll
-  for (int k = 0; k < 3; k++) {
-    int x = d[k] < 0 ? -d[k] : d[k];
-    if (x > 1 && !(P.pbc[k] && x == N[k] - 1)) return false;
-  }
-  return true;
-}
-
-// axis helper: neighbour offsets of a cell coordinate, trimmed like VerifyPBC
-__device__ __forceinline__ void axis_range(int i, int N, int pbc, int& lo, int& hi) {
-  lo = -1;
-  hi = 1;
-  if (!pbc) {
-    if (i == 0) lo = 0;
-    if (i == N - 1) hi = 0;
-  }
-}
-__device__ __forceinline__ int axis_wrap(int j, int N, int pbc) {
-  if (pbc) {
-    if (j == N) j = 0;
-    if (j == -1) j = N - 1;
-  }
-  return j;
-}
-// offsets of one axis in ascending order of the wrapped cell coordinate
-__device__ __forceinline__ int axis_sorted(int i, int N, int pbc, int off[3]) {
-  int lo, hi;
-  axis_range(i, N, pbc, lo, hi);
-  int m = 0;
-  if (pbc && i == 0) {  // -1 wraps to N-1 (largest)
-    off[m++] = 0;
-    off[m++] = 1;
-    off[m++] = -1;
-  } else if (pbc && i == N - 1) {  // +1 wraps to 0 (smallest)
-    off[m++] = 1;
-    off[m++] = -1;
-    off[m++] = 0;
-  } else {
-    for (int k = lo; k <= hi; k++) off[m++] = k;
-  }
-  return m;
-}
-
 // ---------------------------------------------------------------------------
 // K2+K4: force kernel (FP64, exact order)
 
@@ -460,27 +408,8 @@ __global__ void __launch_bounds__(128) k_force_fp64(ForceArgs A) {
 
     // ---- loop 1: own cell after p, then the half-shell cells in the order
     // of the FirstNeighbour list (reverse of AddAllNeighbours3D insertion)
-    {
-      const int e = A.cell_start[c + 1];
-      for (int t = s + 1; t < e; t++) visit_i(t);
-      int xi, xf, yi, yf, zi, zf;
-      axis_range(cx, nx, P.pbc[0], xi, xf);
-      axis_range(cy, ny, P.pbc[1], yi, yf);
-      axis_range(cz, nz, P.pbc[2], zi, zf);
-      for (int kz = zf; kz >= zi; kz--) {
-        const int jz = axis_wrap(cz + kz, nz, P.pbc[2]);
-        for (int ky = yf; ky >= yi; ky--) {
-          const int jy = axis_wrap(cy + ky, ny, P.pbc[1]);
-          for (int kx = xf; kx >= xi; kx--) {
-            if (kx + nx * (ky + ny * kz) <= 0) continue;
-            const int jx = axis_wrap(cx + kx, nx, P.pbc[0]);
-            const int jc = jx + nx * (jy + ny * jz);
-            const int b = A.cell_start[jc], e2 = A.cell_start[jc + 1];
-            for (int t = b; t < e2; t++) visit_i(t);
-          }
-        }
-      }
-    }
+    const int4 meta = A.cl_meta[s];
+    walk_as_i(A, meta, s, c, cx, cy, cz, visit_i);
 
     // ---- walls (src/MForces.f90:274-314)
     for (int w = 0; w < P.nw; w++) {
@@ -575,37 +504,12 @@ __global__ void __launch_bounds__(128) k_force_fp64(ForceArgs A) {
         if (update && orig < qo) record(qo, o.FT, o.VT);
       }
     };
-    {
-      int ox[3], oy[3], oz[3];
-      const int mx = axis_sorted(cx, nx, P.pbc[0], ox);
-      const int my = axis_sorted(cy, ny, P.pbc[1], oy);
-      const int mz = axis_sorted(cz, nz, P.pbc[2], oz);
-      for (int a = 0; a < mz; a++) {
-        const int dz = oz[a];
-        const int jz = axis_wrap(cz + dz, nz, P.pbc[2]);
-        for (int b = 0; b < my; b++) {
-          const int dy = oy[b];
-          const int jy = axis_wrap(cy + dy, ny, P.pbc[1]);
-          for (int d = 0; d < mx; d++) {
-            const int dx = ox[d];
-            if (dx == 0 && dy == 0 && dz == 0) {
-              for (int t = A.cell_start[c]; t < s; t++) visit_j(t);
+    walk_as_j(A, meta, s, c, cx, cy, cz, visit_j, [&]() {
 #pragma unroll
-              for (int k = 0; k < 3; k++) F[k] = F[k] + iF[k];
+      for (int k = 0; k < 3; k++) F[k] = F[k] + iF[k];
 #pragma unroll
-              for (int k = 0; k < 3; k++) T[k] = T[k] + iT[k];
-              continue;
-            }
-            // lower neighbour: p's cell is in the half shell of that cell
-            if (-dx + nx * (-dy + ny * -dz) <= 0) continue;
-            const int jx = axis_wrap(cx + dx, nx, P.pbc[0]);
-            const int jc = jx + nx * (jy + ny * jz);
-            const int b0 = A.cell_start[jc], e2 = A.cell_start[jc + 1];
-            for (int t = b0; t < e2; t++) visit_j(t);
-          }
-        }
-      }
-    }
+      for (int k = 0; k < 3; k++) T[k] = T[k] + iT[k];
+    });
 
     // ---- records of pairs the sweep did not visit are kept as they were
     if (update) {
@@ -735,6 +639,60 @@ __global__ void __launch_bounds__(128) k_force_fp64(ForceArgs A) {
 
 // ---------------------------------------------------------------------------
 // small per-particle kernels (original index order)
+
+// K2 screening: the overlap test DeltaDijSq = MinDijSq - DijSq > 0
+// (src/MForces.f90:209-224) for every candidate of the sweep, in FP64 with the
+// same operations as the force kernels, compacted into the particle's
+// contact-list row in sweep order.  Register-light, so that many warps hide
+// the latency of the candidate loads; the heavy contact arithmetic then runs
+// only over real contacts.
+template <bool PP>
+__global__ void __launch_bounds__(256) k_screen(const DevParams* __restrict__ Pp, int n,
+                                                const double4* __restrict__ pos,
+                                                const int* __restrict__ comp,
+                                                const int* __restrict__ slot_cell,
+                                                const int* __restrict__ cs, ContactLists L,
+                                                const Counters* __restrict__ cnt) {
+  if (cnt->abort) return;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const DevParams& P = *Pp;
+  const int nx = P.nx, ny = P.ny;
+  const int c = slot_cell[s];
+  const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
+  const double4 p4 = pos[s];
+  const int cp = PP ? 0 : comp[s];
+  const bool pb[3] = {P.pbc[0] != 0, P.pbc[1] != 0, P.pbc[2] != 0};
+  const double lb[3] = {P.lbox[0], P.lbox[1], P.lbox[2]};
+  const double il[3] = {P.inv_lbox[0], P.inv_lbox[1], P.inv_lbox[2]};
+  int* out = L.slot + (size_t)s * KC;
+  int m = 0;
+  auto test = [&](int t, bool p_is_i) {
+    const double4 q4 = pos[t];
+    double Rij[3];
+    if (p_is_i) {
+      Rij[0] = q4.x - p4.x; Rij[1] = q4.y - p4.y; Rij[2] = q4.z - p4.z;
+    } else {
+      Rij[0] = p4.x - q4.x; Rij[1] = p4.y - q4.y; Rij[2] = p4.z - q4.z;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+      if (pb[k]) Rij[k] = Rij[k] - lb[k] * fnint(Rij[k] * il[k]);
+    const double DijSq = sumsq3(Rij);
+    const int cq = PP ? 0 : comp[t];
+    const double Delta = p_is_i ? Material<PP>::min_dij_sq(P, cp, p4.w, cq, q4.w) - DijSq
+                                : Material<PP>::min_dij_sq(P, cq, q4.w, cp, p4.w) - DijSq;
+    if (Delta > 0.0) {
+      if (m < KC) out[m] = t;
+      m++;
+    }
+  };
+  sweep_as_i(P, cs, s, c, cx, cy, cz, [&](int t) { test(t, true); });
+  const int n1 = m;
+  int n2b = 0;
+  sweep_as_j(P, cs, s, c, cx, cy, cz, [&](int t) { test(t, false); }, [&]() { n2b = m - n1; });
+  L.meta[s] = m <= KC ? make_int4(n1, n2b, m - n1 - n2b, 0) : make_int4(-1, 0, 0, 0);
+}
 
 // ring store of MoveParticlesEuler (src/MDEM.f90:266-271): (v,a,alpha) -> slot
 __global__ void k_ring_store(int n, StateArrays Q, double* __restrict__ ring, int slot,

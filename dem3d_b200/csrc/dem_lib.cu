@@ -60,6 +60,7 @@ struct dem_ctx {
   unsigned *a_key = nullptr, *t_key = nullptr;
   int* scan_bsum = nullptr;
   int n_tiles = 0;
+  ContactLists CL{};
 
   History H[2]{};
   int hcur = 0;  // H[hcur] holds the current records
@@ -149,6 +150,25 @@ void launch(dem_ctx* c, const char* name, void (*kernel)(KArgs...), unsigned gri
   c->launches++;
 }
 
+// run fn (which launches exactly one kernel on the context stream) with the
+// same event timing as launch()
+template <class Fn>
+void timed(dem_ctx* c, const char* name, Fn&& fn) {
+  if (c->prof) {
+    PendingEvent pe;
+    pe.stat = stat_index(c, name);
+    pe.e0 = get_event(c);
+    pe.e1 = get_event(c);
+    cudaEventRecord(pe.e0, c->stream);
+    fn();
+    cudaEventRecord(pe.e1, c->stream);
+    c->pending.push_back(pe);
+  } else {
+    fn();
+  }
+  c->launches++;
+}
+
 void resolve_events(dem_ctx* c) {
   if (c->pending.empty()) return;
   cudaStreamSynchronize(c->stream);
@@ -185,6 +205,9 @@ void free_state(dem_ctx* c) {
   cudaFree(c->t_orig);
   cudaFree(c->a_key);
   cudaFree(c->t_key);
+  cudaFree(c->CL.slot);
+  cudaFree(c->CL.meta);
+  c->CL = ContactLists{};
   for (int b = 0; b < 2; b++) {
     cudaFree(c->H[b].cnt);
     cudaFree(c->H[b].key);
@@ -241,6 +264,8 @@ int grow_history(dem_ctx* c, int need) {
                      c->stream));
   CK(cudaMemcpyAsync(nh[c->hcur].wval, cur.wval, n * nw * 3 * sizeof(double2),
                      cudaMemcpyDeviceToDevice, c->stream));
+  if (c->precision == DEM_PREC_MIXED && !mixed_regrow(c->M, c->n, cap, c->hcur, cur, c->stream))
+    return fail(c, DEM_ERR_CAPACITY, "mixed history regrow failed");
   CK(cudaStreamSynchronize(c->stream));
   for (int b = 0; b < 2; b++) {
     cudaFree(c->H[b].cnt);
@@ -287,8 +312,9 @@ int rebuild_cells(dem_ctx* c, const StateArrays& src, bool initial) {
   launch(c, "cell_sort", k_cellsort, blocks_for(ncell, 128), 128, ncell, (const int*)c->cell_start,
          c->t_key, c->t_orig, c->S.orig, c->S.cell, c->cell_of_orig, (const Counters*)c->cnt);
   if (c->precision == DEM_PREC_MIXED) {
-    mixed_gather(c->M, c->pp, c->dp, n, src, c->radius, c->comp, c->S, c->cnt, c->stream);
-    c->launches++;
+    timed(c, "gather_mixed", [&]() {
+      mixed_gather(c->M, c->pp, c->dp, n, src, c->radius, c->comp, c->S, c->cnt, c->stream);
+    });
   } else if (c->pp) {
     launch(c, "gather", k_gather<true>, blocks_for(n, 256), 256, (const DevParams*)c->dp, n, src,
            (const double*)c->radius, (const int*)c->comp, c->S, (const Counters*)c->cnt);
@@ -310,6 +336,8 @@ int launch_force(dem_ctx* c, const StateArrays& tgt, bool update, double dt, int
   A.S = c->S;
   A.cell_start = c->cell_start;
   A.cell_of_orig = c->cell_of_orig;
+  A.cl_slot = c->CL.slot;
+  A.cl_meta = c->CL.meta;
   A.Hr = c->H[c->hcur];
   A.Hw = c->H[c->hcur ^ 1];
   A.update = update ? 1 : 0;
@@ -323,8 +351,7 @@ int launch_force(dem_ctx* c, const StateArrays& tgt, bool update, double dt, int
   A.tag = tag;
   unsigned g = blocks_for(c->n, 128);
   if (c->precision == DEM_PREC_MIXED) {
-    mixed_force(c->M, c->pp, epi, A, c->hcur, c->stream);
-    c->launches++;
+    timed(c, "force_mixed", [&]() { mixed_force(c->M, c->pp, epi, A, c->hcur, c->stream); });
     return DEM_OK;
   }
 #define FORCE_CASE(PPV, E) launch(c, "force_fp64", k_force_fp64<PPV, E>, g, 128, A);
@@ -393,6 +420,16 @@ int force_pass(dem_ctx* c, const StateArrays& src, const StateArrays& tgt, bool 
   if (st) return st;
   st = rebuild_cells(c, src, false);
   if (st) return st;
+  if (c->n > 0) {
+    if (c->pp)
+      launch(c, "screen", k_screen<true>, blocks_for(c->n, 256), 256, (const DevParams*)c->dp,
+             c->n, (const double4*)c->S.pos, (const int*)c->S.comp, (const int*)c->S.cell,
+             (const int*)c->cell_start, c->CL, (const Counters*)c->cnt);
+    else
+      launch(c, "screen", k_screen<false>, blocks_for(c->n, 256), 256, (const DevParams*)c->dp,
+             c->n, (const double4*)c->S.pos, (const int*)c->S.comp, (const int*)c->S.cell,
+             (const int*)c->cell_start, c->CL, (const Counters*)c->cnt);
+  }
   for (int attempt = 0;; attempt++) {
     st = launch_force(c, tgt, update, dt, epi, rm, tag);
     if (st) return st;
@@ -748,6 +785,8 @@ int dem_set_state(dem_ctx* c, int32_t n, const int32_t* comp, const double* radi
   CK(cudaMalloc(&c->t_orig, sizeof(int) * N));
   CK(cudaMalloc(&c->a_key, sizeof(unsigned) * N));
   CK(cudaMalloc(&c->t_key, sizeof(unsigned) * N));
+  CK(cudaMalloc(&c->CL.slot, sizeof(int) * N * KC));
+  CK(cudaMalloc(&c->CL.meta, sizeof(int4) * N));
   for (int b = 0; b < 2; b++) {
     int st = alloc_history(c, c->H[b], c->hcap);
     if (st) return st;
@@ -1213,7 +1252,9 @@ int dem_get_ncol(dem_ctx* c, int64_t* ncol) {
   if (!c || !ncol) return DEM_ERR_INVALID;
   int st = read_counters(c);
   if (st) return st;
-  *ncol = (int64_t)c->hcnt->ncol;
+  // the last history-updating pass completed (no abort is pending after an
+  // API call returns), so its count is part of Ncol
+  *ncol = (int64_t)(c->hcnt->ncol + c->hcnt->ncol_pending);
   return DEM_OK;
 }
 

@@ -1,16 +1,725 @@
-// dem_mixed.cu -- mixed-precision force path (placeholder until implemented).
+// dem_mixed.cu -- mixed-precision force path (DEM_PREC_MIXED).
+//
+// Same sweep, same pair sets, same history semantics and summation order as
+// the FP64 kernel; what changes is the arithmetic of a contact:
+//  - the candidate test DeltaDijSq = MinDijSq - DijSq stays FP64 (from FP64
+//    positions), so the contact-pair set equals the FP64 one;
+//  - the overlap is formed as delta = DeltaDijSq / (MinDij + Dij), which
+//    keeps its relative digits in FP32 (MinDij - Dij itself would cancel);
+//  - everything downstream (normal, relative velocity, spring-dashpot,
+//    tangential spring, Coulomb cap, torques, per-particle sums) is FP32;
+//  - the tangential spring is carried as an FP32 pair (hi, lo) and each
+//    increment is added with a compensated (Kahan/TwoSum) sum;
+//  - velocities are gathered as FP32 copies; positions, the ABM ring and
+//    the predictor/corrector stay FP64.
+// This translation unit may fuse multiply-adds.
 #include "dem_mixed.cuh"
 
 namespace dem {
 
-bool mixed_available() { return false; }
-bool mixed_alloc(MixedBuffers&, int, int, int) { return false; }
-void mixed_free(MixedBuffers& M) { M = MixedBuffers{}; }
-bool mixed_regrow(MixedBuffers&, int, int, int, const History&) { return false; }
-void mixed_gather(MixedBuffers&, bool, const DevParams*, int, const StateArrays&, const double*,
-                  const int*, const SortedArrays&, Counters*, cudaStream_t) {}
-void mixed_force(MixedBuffers&, bool, int, const ForceArgs&, int, cudaStream_t) {}
-void mixed_import_history(MixedBuffers&, const History&, int, int, int, cudaStream_t) {}
-void mixed_export_history(MixedBuffers&, const History&, int, int, int, cudaStream_t) {}
+namespace {
+
+struct MixedView {
+  const float4* v4;  // traversal-order vx, vy, vz, wx
+  const float2* w2;  // wy, wz
+  // history values [n*cap]: a = (ft.xyz, vt.x) b = (vt.yz, lo.xy) c = lo.z
+  const float4* ra;
+  const float4* rb;
+  const float* rc;
+  float4* wa;
+  float4* wb;
+  float* wc;
+  // wall history values [n*nw], same packing
+  const float4* rwa;
+  const float4* rwb;
+  const float* rwc;
+  float4* wwa;
+  float4* wwb;
+  float* wwc;
+};
+
+struct F3 {
+  float x, y, z;
+};
+__device__ __forceinline__ F3 mk(float x, float y, float z) { return F3{x, y, z}; }
+__device__ __forceinline__ F3 operator+(F3 a, F3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ F3 operator-(F3 a, F3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ F3 operator*(float s, F3 a) { return mk(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ float dot(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ F3 cross(F3 a, F3 b) {
+  return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+struct MPair {
+  float min_dij, kn, yn, kt, yt, mu_sq;
+};
+
+template <bool PP>
+struct MMat;
+
+template <>
+struct MMat<false> {
+  __device__ __forceinline__ static double min_dij_sq(const DevParams& P, int ca, double, int cb,
+                                                      double) {
+    return P.min_dij_sq[ca * NCM + cb];
+  }
+  __device__ __forceinline__ static void pair(const DevParams& P, int ca, float, int cb, float,
+                                              MPair& m) {
+    int k = ca * NCM + cb;
+    m.min_dij = (float)P.min_dij[k];
+    m.kn = (float)P.kn[k];
+    m.yn = (float)P.yn[k];
+    m.kt = (float)P.kt[k];
+    m.yt = (float)P.yt[k];
+    m.mu_sq = (float)P.mu_sq[k];
+  }
+  __device__ __forceinline__ static void wall(const DevParams& P, int ca, float, int w, MPair& m) {
+    int k = ca * NWM + w;
+    m.kn = (float)P.knw[k];
+    m.yn = (float)P.ynw[k];
+    m.kt = (float)P.ktw[k];
+    m.yt = (float)P.ytw[k];
+    m.mu_sq = (float)P.muw_sq[k];
+  }
+  __device__ __forceinline__ static void self(const DevParams& P, int ca, float, float& im,
+                                              float& ii, float& em) {
+    im = (float)P.comp_inv_mass[ca];
+    ii = (float)P.comp_inv_inertia[ca];
+    em = (float)P.comp_eff_mass[ca];
+  }
+};
+
+template <>
+struct MMat<true> {
+  __device__ __forceinline__ static double min_dij_sq(const DevParams&, int, double Ra, int,
+                                                      double Rb) {
+    double d = Ra + Rb;
+    return d * d;
+  }
+  __device__ __forceinline__ static float mass(const DevParams& P, float R) {
+    return (float)P.pp_mass_coef * (R * R * R);
+  }
+  __device__ __forceinline__ static void pair(const DevParams& P, int, float Ra, int, float Rb,
+                                              MPair& m) {
+    float ma = mass(P, Ra), mb = mass(P, Rb);
+    float meff = ma * mb / (ma + mb);
+    m.min_dij = Ra + Rb;
+    m.kn = (float)P.pp_kn;
+    m.kt = (float)P.pp_kt;
+    m.yn = (float)P.pp_gamma_n * sqrtf(meff * m.kn);
+    m.yt = (float)P.pp_gamma_t * sqrtf(meff * m.kt);
+    m.mu_sq = (float)P.pp_mu_sq;
+  }
+  __device__ __forceinline__ static void wall(const DevParams& P, int, float Ra, int w, MPair& m) {
+    float ma = mass(P, Ra);
+    m.kn = (float)P.pp_knw[w];
+    m.kt = (float)P.pp_ktw[w];
+    m.yn = (float)P.pp_gamma_nw[w] * sqrtf(ma * m.kn);
+    m.yt = (float)P.pp_gamma_tw[w] * sqrtf(ma * m.kt);
+    m.mu_sq = (float)P.pp_muw_sq[w];
+  }
+  __device__ __forceinline__ static void self(const DevParams& P, int, float R, float& im,
+                                              float& ii, float& em) {
+    float m = mass(P, R);
+    im = 1.0f / m;
+    ii = 1.0f / (0.4f * m * (R * R));
+    em = (float)((double)m * (P.pp_density - P.pp_fluid_density) / P.pp_density);
+  }
+};
+
+__device__ __forceinline__ F3 change_plane_f(F3 V, F3 N) {
+  F3 P = V - dot(V, N) * N;
+  float ns = dot(P, P);
+  if (ns != 0.0f) return sqrtf(dot(V, V) / ns) * P;
+  return mk(0.f, 0.f, 0.f);
+}
+
+// TwoSum: s + e == a + b exactly
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+  s = __fadd_rn(a, b);
+  float bp = __fsub_rn(s, a);
+  e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bp)), __fsub_rn(b, bp));
+}
+
+struct MOut {
+  F3 FN, FT, FTlo, VT, N, NxFT;
+};
+
+// CommonCalculations (src/MForces.f90:339-387) in FP32 given the geometry.
+__device__ __forceinline__ void common_mixed(F3 Rij, F3 N, F3 DispN, F3 Vij, F3 VijC,
+                                             float DeltaDijSq, float half_dt, bool contacting,
+                                             F3 ft0, F3 ft0lo, F3 vt0, const MPair& m, MOut& o) {
+  F3 VijN = dot(VijC, N) * N;
+  o.VT = VijC - VijN;
+  o.FN = m.kn * DispN + m.yn * VijN;
+  if (contacting) {
+    F3 VT0 = change_plane_f(vt0, N);
+    F3 dD = half_dt * (VT0 + o.VT);
+    F3 dV = o.VT - VT0;
+    // rotate the compensated spring (hi + lo) onto the new contact plane
+    F3 ph = ft0 - dot(ft0, N) * N;
+    F3 pl = ft0lo - dot(ft0lo, N) * N;
+    float ns = dot(ph, ph);
+    F3 hi = mk(0.f, 0.f, 0.f), lo = mk(0.f, 0.f, 0.f);
+    if (ns != 0.0f) {
+      float f = sqrtf(dot(ft0, ft0) / ns);
+      hi = f * ph;
+      lo = f * pl;
+    }
+    F3 inc = m.kt * dD + m.yt * dV;
+    float e;
+    two_sum(hi.x, inc.x, o.FT.x, e);
+    o.FTlo.x = lo.x + e;
+    two_sum(hi.y, inc.y, o.FT.y, e);
+    o.FTlo.y = lo.y + e;
+    two_sum(hi.z, inc.z, o.FT.z, e);
+    o.FTlo.z = lo.z + e;
+  } else {
+    float PartialDt;
+    float VijSq = dot(Vij, Vij);
+    if (VijSq > 0.0f) {
+      float RijVij = dot(Rij, Vij);
+      float a = 2.0f * half_dt;
+      float b = (RijVij + sqrtf(RijVij * RijVij + VijSq * DeltaDijSq)) / VijSq;
+      PartialDt = b < a ? b : a;
+    } else {
+      PartialDt = 0.0f;
+    }
+    o.FT = (m.kt * PartialDt + m.yt) * o.VT;
+    o.FTlo = mk(0.f, 0.f, 0.f);
+  }
+  float mun = m.mu_sq * dot(o.FN, o.FN);
+  float nt = dot(o.FT, o.FT);
+  if (nt > mun) {
+    float g = sqrtf(mun / nt);
+    o.FT = g * o.FT;
+    o.FTlo = g * o.FTlo;
+  }
+  o.N = N;
+  o.NxFT = cross(N, o.FT);
+}
+
+// pair branch (src/MForces.f90:230-252), "i" = a, "j" = b, Rij = xb - xa
+__device__ __forceinline__ void mixed_pair(const double Rd[3], double DijSq, double Delta,
+                                           const MPair& m, float Ra, F3 va, F3 wa, float Rb,
+                                           F3 vb, F3 wb, float half_dt, bool contacting, F3 ft0,
+                                           F3 ft0lo, F3 vt0, MOut& o) {
+  const float D = sqrtf((float)DijSq);
+  const float fDelta = (float)Delta;
+  const float delta = fDelta / (m.min_dij + D);  // = MinDij - Dij, without cancellation
+  const float rD = 1.0f / D;
+  F3 Rij = mk((float)Rd[0], (float)Rd[1], (float)Rd[2]);
+  F3 N = rD * Rij;
+  F3 DispN = (-delta) * N;
+  F3 Vij = vb - va;
+  F3 ws = Ra * wa + Rb * wb;
+  F3 VijC = Vij - cross(ws, N);
+  common_mixed(Rij, N, DispN, Vij, VijC, fDelta, half_dt, contacting, ft0, ft0lo, vt0, m, o);
+}
+
+__device__ __forceinline__ void rec_read(const float4* a, const float4* b, const float* c,
+                                         size_t i, F3& ft, F3& lo, F3& vt) {
+  float4 x = a[i], y = b[i];
+  ft = mk(x.x, x.y, x.z);
+  vt = mk(x.w, y.x, y.y);
+  lo = mk(y.z, y.w, c[i]);
+}
+__device__ __forceinline__ void rec_write(float4* a, float4* b, float* c, size_t i, F3 ft, F3 lo,
+                                          F3 vt) {
+  a[i] = make_float4(ft.x, ft.y, ft.z, vt.x);
+  b[i] = make_float4(vt.y, vt.z, lo.x, lo.y);
+  c[i] = lo.z;
+}
+
+__device__ __forceinline__ unsigned long long wsum(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <bool PP, int EPI>
+__global__ void __launch_bounds__(128) k_force_mixed(ForceArgs A, MixedView V) {
+  if (A.cnt->abort) return;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long n_col = 0, n_pc = 0, n_wc = 0;
+  int need = 0;
+  if (s < A.n) {
+    const DevParams& P = *A.P;
+    const SortedArrays& S = A.S;
+    const int nx = P.nx, ny = P.ny;
+    const int c = S.cell[s];
+    const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
+    const double4 p4 = S.pos[s];
+    const double xp[3] = {p4.x, p4.y, p4.z};
+    const double Rpd = p4.w;
+    const float Rp = (float)Rpd;
+    const float4 pv4 = V.v4[s];
+    const float2 pw2 = V.w2[s];
+    const F3 vp = mk(pv4.x, pv4.y, pv4.z);
+    const F3 wp = mk(pv4.w, pw2.x, pw2.y);
+    const int orig = S.orig[s];
+    const int cp = PP ? 0 : S.comp[s];
+    float inv_m, inv_i, eff_m;
+    MMat<PP>::self(P, cp, Rp, inv_m, inv_i, eff_m);
+    const float half_dt = (float)A.half_dt;
+    const bool update = A.update != 0;
+    int hw_n = 0;
+    bool overflow = false;
+    const History& Hr = A.Hr;
+    const History& Hw = A.Hw;
+
+    F3 iF = mk(eff_m * (float)P.gravity[0], eff_m * (float)P.gravity[1],
+               eff_m * (float)P.gravity[2]);
+    F3 iT = mk(0.f, 0.f, 0.f);
+
+    auto record = [&](int partner, F3 ft, F3 lo, F3 vt) {
+      if (hw_n < Hw.cap) {
+        size_t i = (size_t)orig * Hw.cap + hw_n;
+        Hw.key[i] = partner;
+        rec_write(V.wa, V.wb, V.wc, i, ft, lo, vt);
+      } else {
+        overflow = true;
+      }
+      hw_n++;
+    };
+    auto lookup = [&](int lo_i, int hi_i, F3& ft, F3& lo, F3& vt) -> bool {
+      const int cnt = Hr.cnt[lo_i];
+      const int* k = Hr.key + (size_t)lo_i * Hr.cap;
+      for (int r = 0; r < cnt; r++)
+        if (k[r] == hi_i) {
+          rec_read(V.ra, V.rb, V.rc, (size_t)lo_i * Hr.cap + r, ft, lo, vt);
+          return true;
+        }
+      ft = lo = vt = mk(0.f, 0.f, 0.f);
+      return false;
+    };
+
+    auto visit_i = [&](int t) {
+      const double4 q4 = S.pos[t];
+      double Rij[3] = {q4.x - xp[0], q4.y - xp[1], q4.z - xp[2]};
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+        if (P.pbc[k]) Rij[k] = Rij[k] - P.lbox[k] * fnint(Rij[k] * P.inv_lbox[k]);
+      const double DijSq = sumsq3(Rij);
+      const int cq = PP ? 0 : S.comp[t];
+      const double Delta = MMat<PP>::min_dij_sq(P, cp, Rpd, cq, q4.w) - DijSq;
+      if (Delta > 0.0) {
+        const float Rq = (float)q4.w;
+        MPair m;
+        MMat<PP>::pair(P, cp, Rp, cq, Rq, m);
+        const int qo = S.orig[t];
+        const float4 qv4 = V.v4[t];
+        const float2 qw2 = V.w2[t];
+        const int lo_i = orig < qo ? orig : qo, hi_i = orig < qo ? qo : orig;
+        F3 ft0, ft0lo, vt0;
+        const bool contacting = lookup(lo_i, hi_i, ft0, ft0lo, vt0);
+        if (!contacting) n_col++;
+        n_pc++;
+        MOut o;
+        mixed_pair(Rij, DijSq, Delta, m, Rp, vp, wp, Rq, mk(qv4.x, qv4.y, qv4.z),
+                   mk(qv4.w, qw2.x, qw2.y), half_dt, contacting, ft0, ft0lo, vt0, o);
+        iF = iF + o.FN + (o.FT + o.FTlo);
+        iT = iT + cross(Rp * o.N, o.FT);
+        if (update && orig < qo) record(qo, o.FT, o.FTlo, o.VT);
+      }
+    };
+    const int4 meta = A.cl_meta[s];
+    walk_as_i(A, meta, s, c, cx, cy, cz, visit_i);
+
+    for (int w = 0; w < P.nw; w++) {
+      const dem_wall& W = P.walls[w];
+      const size_t wi = (size_t)orig * P.nw + w;
+      const bool contacting = Hr.wflag[wi] != 0;
+      F3 ft0 = mk(0.f, 0.f, 0.f), ft0lo = ft0, vt0 = ft0;
+      if (contacting) rec_read(V.rwa, V.rwb, V.rwc, wi, ft0, ft0lo, vt0);
+      double Dij, Nij[3], Qji[3];
+      bool ov = false;
+      if (W.shape == DEM_WALL_RECTANGLE) ov = overlap_rect(P, W, xp, Rpd, Dij, Nij, Qji);
+      if (ov) {
+        n_wc++;
+        const double Delta = Rpd * Rpd - Dij * Dij;
+        const float delta = (float)(Rpd - Dij);
+        F3 N = mk((float)Nij[0], (float)Nij[1], (float)Nij[2]);
+        F3 Q = mk((float)Qji[0], (float)Qji[1], (float)Qji[2]);
+        F3 wv = mk((float)W.velocity[0], (float)W.velocity[1], (float)W.velocity[2]);
+        F3 ww = mk((float)W.omega[0], (float)W.omega[1], (float)W.omega[2]);
+        F3 Vij = (wv + cross(ww, Q)) - vp;
+        F3 VijC = Vij - cross(Rp * wp, N);
+        F3 Rw = mk((float)(W.position[0] + Qji[0] - xp[0]), (float)(W.position[1] + Qji[1] - xp[1]),
+                   (float)(W.position[2] + Qji[2] - xp[2]));
+        MPair m;
+        MMat<PP>::wall(P, cp, Rp, w, m);
+        MOut o;
+        common_mixed(Rw, N, (-delta) * N, Vij, VijC, (float)Delta, half_dt, contacting, ft0,
+                     ft0lo, vt0, m, o);
+        iF = iF + o.FN + (o.FT + o.FTlo);
+        iT = iT + cross(Rp * o.N, o.FT);
+        atomicAdd(&A.cnt->wall_fn[w], (double)sqrtf(dot(o.FN, o.FN)));
+        if (update) {
+          Hw.wflag[wi] = 1;
+          rec_write(V.wwa, V.wwb, V.wwc, wi, o.FT, o.FTlo, o.VT);
+        }
+      } else if (update) {
+        Hw.wflag[wi] = 0;
+      }
+    }
+
+    F3 F = mk(0.f, 0.f, 0.f), T = mk(0.f, 0.f, 0.f);
+    auto visit_j = [&](int t) {
+      const double4 q4 = S.pos[t];
+      double Rij[3] = {xp[0] - q4.x, xp[1] - q4.y, xp[2] - q4.z};
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+        if (P.pbc[k]) Rij[k] = Rij[k] - P.lbox[k] * fnint(Rij[k] * P.inv_lbox[k]);
+      const double DijSq = sumsq3(Rij);
+      const int cq = PP ? 0 : S.comp[t];
+      const double Delta = MMat<PP>::min_dij_sq(P, cq, q4.w, cp, Rpd) - DijSq;
+      if (Delta > 0.0) {
+        const float Rq = (float)q4.w;
+        MPair m;
+        MMat<PP>::pair(P, cq, Rq, cp, Rp, m);
+        const int qo = S.orig[t];
+        const float4 qv4 = V.v4[t];
+        const float2 qw2 = V.w2[t];
+        const int lo_i = orig < qo ? orig : qo, hi_i = orig < qo ? qo : orig;
+        F3 ft0, ft0lo, vt0;
+        const bool contacting = lookup(lo_i, hi_i, ft0, ft0lo, vt0);
+        MOut o;
+        mixed_pair(Rij, DijSq, Delta, m, Rq, mk(qv4.x, qv4.y, qv4.z), mk(qv4.w, qw2.x, qw2.y), Rp,
+                   vp, wp, half_dt, contacting, ft0, ft0lo, vt0, o);
+        F = F - o.FN - (o.FT + o.FTlo);
+        T = T + Rp * o.NxFT;
+        if (update && orig < qo) record(qo, o.FT, o.FTlo, o.VT);
+      }
+    };
+    walk_as_j(A, meta, s, c, cx, cy, cz, visit_j, [&]() {
+      F = F + iF;
+      T = T + iT;
+    });
+
+    if (update) {
+      const int nold = Hr.cnt[orig];
+      for (int r = 0; r < nold; r++) {
+        const size_t i = (size_t)orig * Hr.cap + r;
+        const int q2 = Hr.key[i];
+        if (!cells_adjacent(P, c, A.cell_of_orig[q2])) {
+          F3 ft, lo, vt;
+          rec_read(V.ra, V.rb, V.rc, i, ft, lo, vt);
+          record(q2, ft, lo, vt);
+        }
+      }
+      Hw.cnt[orig] = hw_n < Hw.cap ? hw_n : Hw.cap;
+      if (overflow) {
+        atomicExch(&A.cnt->overflow, 1);
+        atomicCAS(&A.cnt->abort_tag, 0, A.tag + 1);
+        atomicExch(&A.cnt->abort, 1);
+      }
+      need = hw_n;
+    }
+
+    const double acc[3] = {(double)(F.x * inv_m), (double)(F.y * inv_m), (double)(F.z * inv_m)};
+    const double alp[3] = {(double)(T.x * inv_i), (double)(T.y * inv_i), (double)(T.z * inv_i)};
+    const size_t n = (size_t)A.n;
+    if (EPI == EPI_STORE) {
+      A.tgt.ax[orig] = acc[0]; A.tgt.ay[orig] = acc[1]; A.tgt.az[orig] = acc[2];
+      A.tgt.lx[orig] = alp[0]; A.tgt.ly[orig] = alp[1]; A.tgt.lz[orig] = alp[2];
+    } else if (EPI == EPI_PREDICT) {
+      const StateArrays& Q = A.part;
+      const StateArrays& R = A.pred;
+      Q.ax[orig] = acc[0]; Q.ay[orig] = acc[1]; Q.az[orig] = acc[2];
+      Q.lx[orig] = alp[0]; Q.ly[orig] = alp[1]; Q.lz[orig] = alp[2];
+      // FP64 velocities of Particle (the traversal copies are FP32)
+      const double vd[3] = {Q.vx[orig], Q.vy[orig], Q.vz[orig]};
+      const double wd[3] = {Q.wx[orig], Q.wy[orig], Q.wz[orig]};
+      double sv[3] = {0.0, 0.0, 0.0}, sa[3] = {0.0, 0.0, 0.0}, sl[3] = {0.0, 0.0, 0.0};
+      for (int k = 0; k < P.nprev; k++) {
+        const double ABk = P.ab[k];
+        const double* rg = A.ring + (size_t)A.rm.phys[k] * 9 * n + orig;
+#pragma unroll
+        for (int d = 0; d < 3; d++) sv[d] = sv[d] + ABk * rg[d * n];
+#pragma unroll
+        for (int d = 0; d < 3; d++) sa[d] = sa[d] + ABk * rg[(3 + d) * n];
+#pragma unroll
+        for (int d = 0; d < 3; d++) sl[d] = sl[d] + ABk * rg[(6 + d) * n];
+      }
+      double xr[3], vr[3], wr[3];
+#pragma unroll
+      for (int d = 0; d < 3; d++) xr[d] = xp[d] + P.ab0 * vd[d] + sv[d];
+#pragma unroll
+      for (int d = 0; d < 3; d++) vr[d] = vd[d] + P.ab0 * acc[d] + sa[d];
+#pragma unroll
+      for (int d = 0; d < 3; d++) wr[d] = wd[d] + P.ab0 * alp[d] + sl[d];
+#pragma unroll
+      for (int d = 0; d < 3; d++)
+        if (P.pbc[d]) xr[d] = xr[d] - P.lbox[d] * fnint(xr[d] * P.inv_lbox[d]);
+      R.px[orig] = xr[0]; R.py[orig] = xr[1]; R.pz[orig] = xr[2];
+      R.vx[orig] = vr[0]; R.vy[orig] = vr[1]; R.vz[orig] = vr[2];
+      R.wx[orig] = wr[0]; R.wy[orig] = wr[1]; R.wz[orig] = wr[2];
+      if (P.nprev > 0) {
+        double* rg = A.ring + (size_t)A.rm.phys[P.nprev] * 9 * n + orig;
+#pragma unroll
+        for (int d = 0; d < 3; d++) rg[d * n] = vd[d];
+#pragma unroll
+        for (int d = 0; d < 3; d++) rg[(3 + d) * n] = acc[d];
+#pragma unroll
+        for (int d = 0; d < 3; d++) rg[(6 + d) * n] = alp[d];
+      }
+    } else {
+      const StateArrays& Q = A.part;
+      const StateArrays& R = A.pred;
+      R.ax[orig] = acc[0]; R.ay[orig] = acc[1]; R.az[orig] = acc[2];
+      R.lx[orig] = alp[0]; R.ly[orig] = alp[1]; R.lz[orig] = alp[2];
+      const double vpd[3] = {R.vx[orig], R.vy[orig], R.vz[orig]};
+      double sv[3] = {0.0, 0.0, 0.0}, sa[3] = {0.0, 0.0, 0.0}, sl[3] = {0.0, 0.0, 0.0};
+      for (int k = 0; k < P.nprev; k++) {
+        const double AMk = P.am[k];
+        const double* rg = A.ring + (size_t)A.rm.phys[k] * 9 * n + orig;
+#pragma unroll
+        for (int d = 0; d < 3; d++) sv[d] = sv[d] + AMk * rg[d * n];
+#pragma unroll
+        for (int d = 0; d < 3; d++) sa[d] = sa[d] + AMk * rg[(3 + d) * n];
+#pragma unroll
+        for (int d = 0; d < 3; d++) sl[d] = sl[d] + AMk * rg[(6 + d) * n];
+      }
+      double x[3] = {Q.px[orig], Q.py[orig], Q.pz[orig]};
+      double v[3] = {Q.vx[orig], Q.vy[orig], Q.vz[orig]};
+      double w[3] = {Q.wx[orig], Q.wy[orig], Q.wz[orig]};
+#pragma unroll
+      for (int d = 0; d < 3; d++) x[d] = x[d] + P.am0 * vpd[d] + sv[d];
+#pragma unroll
+      for (int d = 0; d < 3; d++) v[d] = v[d] + P.am0 * acc[d] + sa[d];
+#pragma unroll
+      for (int d = 0; d < 3; d++) w[d] = w[d] + P.am0 * alp[d] + sl[d];
+#pragma unroll
+      for (int d = 0; d < 3; d++)
+        if (P.pbc[d]) x[d] = x[d] - P.lbox[d] * fnint(x[d] * P.inv_lbox[d]);
+      Q.px[orig] = x[0]; Q.py[orig] = x[1]; Q.pz[orig] = x[2];
+      Q.vx[orig] = v[0]; Q.vy[orig] = v[1]; Q.vz[orig] = v[2];
+      Q.wx[orig] = w[0]; Q.wy[orig] = w[1]; Q.wz[orig] = w[2];
+      bool out = false;
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const double h = 0.5 * P.lbox[d];
+        out = out || (x[d] > h) || (x[d] < -h);
+      }
+      if (out) atomicAdd(&A.cnt->escaped, 1ull);
+    }
+  }
+  n_col = wsum(n_col);
+  n_pc = wsum(n_pc);
+  n_wc = wsum(n_wc);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) need = max(need, __shfl_down_sync(0xffffffffu, need, o));
+  if ((threadIdx.x & 31) == 0) {
+    if (need) atomicMax(&A.cnt->need_capacity, need);
+    if (n_col) atomicAdd(A.update ? &A.cnt->ncol_pending : &A.cnt->ncol, n_col);
+    if (n_pc) atomicAdd(&A.cnt->pair_contacts, n_pc);
+    if (n_wc) atomicAdd(&A.cnt->wall_contacts, n_wc);
+  }
+}
+
+template <bool PP>
+__global__ void k_gather_mixed(const DevParams* __restrict__ Pp, int n, StateArrays src,
+                               const double* __restrict__ radius, const int* __restrict__ comp,
+                               SortedArrays S, float4* __restrict__ v4, float2* __restrict__ w2,
+                               const Counters* __restrict__ cnt) {
+  if (cnt->abort) return;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  int o = S.orig[t];
+  double R;
+  if (PP) {
+    R = radius[o];
+  } else {
+    int k = comp[o];
+    S.comp[t] = k;
+    R = Pp->comp_radius[k];
+  }
+  S.pos[t] = make_double4(src.px[o], src.py[o], src.pz[o], R);
+  v4[t] = make_float4((float)src.vx[o], (float)src.vy[o], (float)src.vz[o], (float)src.wx[o]);
+  w2[t] = make_float2((float)src.wy[o], (float)src.wz[o]);
+}
+
+// FP64 records <-> FP32 records
+__global__ void k_hist_to_mixed(int n, History H, float4* a, float4* b, float* c, int nw,
+                                float4* wa, float4* wb, float* wc) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int r = 0; r < H.cnt[i]; r++) {
+    size_t k = (size_t)i * H.cap + r;
+    double2 x = H.val[3 * k], y = H.val[3 * k + 1], z = H.val[3 * k + 2];
+    a[k] = make_float4((float)x.x, (float)x.y, (float)y.x, (float)y.y);
+    b[k] = make_float4((float)z.x, (float)z.y, 0.f, 0.f);
+    c[k] = 0.f;
+  }
+  for (int w = 0; w < nw; w++) {
+    size_t k = (size_t)i * nw + w;
+    double2 x = H.wval[3 * k], y = H.wval[3 * k + 1], z = H.wval[3 * k + 2];
+    wa[k] = make_float4((float)x.x, (float)x.y, (float)y.x, (float)y.y);
+    wb[k] = make_float4((float)z.x, (float)z.y, 0.f, 0.f);
+    wc[k] = 0.f;
+  }
+}
+
+__global__ void k_hist_from_mixed(int n, History H, const float4* a, const float4* b,
+                                  const float* c, int nw, const float4* wa, const float4* wb,
+                                  const float* wc) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int r = 0; r < H.cnt[i]; r++) {
+    size_t k = (size_t)i * H.cap + r;
+    float4 x = a[k], y = b[k];
+    H.val[3 * k] = make_double2((double)x.x + y.z, (double)x.y + y.w);
+    H.val[3 * k + 1] = make_double2((double)x.z + c[k], (double)x.w);
+    H.val[3 * k + 2] = make_double2((double)y.x, (double)y.y);
+  }
+  for (int w = 0; w < nw; w++) {
+    size_t k = (size_t)i * nw + w;
+    float4 x = wa[k], y = wb[k];
+    H.wval[3 * k] = make_double2((double)x.x + y.z, (double)x.y + y.w);
+    H.wval[3 * k + 1] = make_double2((double)x.z + wc[k], (double)x.w);
+    H.wval[3 * k + 2] = make_double2((double)y.x, (double)y.y);
+  }
+}
+
+__global__ void k_mixed_regrow(int n, const int* cnt, int oldcap, int newcap, const float4* a,
+                               const float4* b, const float* c, float4* na, float4* nb,
+                               float* nc) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int r = 0; r < cnt[i]; r++) {
+    size_t s = (size_t)i * oldcap + r, d = (size_t)i * newcap + r;
+    na[d] = a[s];
+    nb[d] = b[s];
+    nc[d] = c[s];
+  }
+}
+
+unsigned blocks(long long n, int b) { return (unsigned)((n + b - 1) / b); }
+
+}  // namespace
+
+bool mixed_available() { return true; }
+
+bool mixed_alloc(MixedBuffers& M, int n, int nw, int cap) {
+  mixed_free(M);
+  size_t N = (size_t)(n > 0 ? n : 1);
+  size_t W = N * (size_t)(nw > 0 ? nw : 1);
+  M.n = n;
+  M.nw = nw;
+  M.cap = cap;
+  bool ok = cudaMalloc(&M.v4, N * sizeof(float4)) == cudaSuccess &&
+            cudaMalloc(&M.w2, N * sizeof(float2)) == cudaSuccess;
+  for (int b = 0; b < 2 && ok; b++) {
+    ok = cudaMalloc(&M.ha[b], N * cap * sizeof(float4)) == cudaSuccess &&
+         cudaMalloc(&M.hb[b], N * cap * sizeof(float4)) == cudaSuccess &&
+         cudaMalloc(&M.hc[b], N * cap * sizeof(float)) == cudaSuccess &&
+         cudaMalloc(&M.wa[b], W * sizeof(float4)) == cudaSuccess &&
+         cudaMalloc(&M.wb[b], W * sizeof(float4)) == cudaSuccess &&
+         cudaMalloc(&M.wc[b], W * sizeof(float)) == cudaSuccess;
+  }
+  M.ready = ok;
+  return ok;
+}
+
+void mixed_free(MixedBuffers& M) {
+  cudaFree(M.v4);
+  cudaFree(M.w2);
+  for (int b = 0; b < 2; b++) {
+    cudaFree(M.ha[b]);
+    cudaFree(M.hb[b]);
+    cudaFree(M.hc[b]);
+    cudaFree(M.wa[b]);
+    cudaFree(M.wb[b]);
+    cudaFree(M.wc[b]);
+  }
+  M = MixedBuffers{};
+}
+
+bool mixed_regrow(MixedBuffers& M, int n, int newcap, int cur, const History& old,
+                  cudaStream_t st) {
+  size_t N = (size_t)(n > 0 ? n : 1);
+  float4 *na[2], *nb[2];
+  float* nc[2];
+  for (int b = 0; b < 2; b++) {
+    if (cudaMalloc(&na[b], N * newcap * sizeof(float4)) != cudaSuccess ||
+        cudaMalloc(&nb[b], N * newcap * sizeof(float4)) != cudaSuccess ||
+        cudaMalloc(&nc[b], N * newcap * sizeof(float)) != cudaSuccess)
+      return false;
+  }
+  if (n > 0)
+    k_mixed_regrow<<<blocks(n, 256), 256, 0, st>>>(n, old.cnt, old.cap, newcap, M.ha[cur],
+                                                    M.hb[cur], M.hc[cur], na[cur], nb[cur],
+                                                    nc[cur]);
+  cudaStreamSynchronize(st);
+  for (int b = 0; b < 2; b++) {
+    cudaFree(M.ha[b]);
+    cudaFree(M.hb[b]);
+    cudaFree(M.hc[b]);
+    M.ha[b] = na[b];
+    M.hb[b] = nb[b];
+    M.hc[b] = nc[b];
+  }
+  M.cap = newcap;
+  return true;
+}
+
+void mixed_gather(MixedBuffers& M, bool pp, const DevParams* dp, int n, const StateArrays& src,
+                  const double* radius, const int* comp, const SortedArrays& S, Counters* cnt,
+                  cudaStream_t st) {
+  if (n == 0) return;
+  if (pp)
+    k_gather_mixed<true><<<blocks(n, 256), 256, 0, st>>>(dp, n, src, radius, comp, S, M.v4, M.w2,
+                                                         cnt);
+  else
+    k_gather_mixed<false><<<blocks(n, 256), 256, 0, st>>>(dp, n, src, radius, comp, S, M.v4, M.w2,
+                                                          cnt);
+}
+
+void mixed_force(MixedBuffers& M, bool pp, int epi, const ForceArgs& A, int cur,
+                 cudaStream_t st) {
+  if (A.n == 0) return;
+  MixedView V;
+  V.v4 = M.v4;
+  V.w2 = M.w2;
+  V.ra = M.ha[cur];
+  V.rb = M.hb[cur];
+  V.rc = M.hc[cur];
+  V.wa = M.ha[cur ^ 1];
+  V.wb = M.hb[cur ^ 1];
+  V.wc = M.hc[cur ^ 1];
+  V.rwa = M.wa[cur];
+  V.rwb = M.wb[cur];
+  V.rwc = M.wc[cur];
+  V.wwa = M.wa[cur ^ 1];
+  V.wwb = M.wb[cur ^ 1];
+  V.wwc = M.wc[cur ^ 1];
+  unsigned g = blocks(A.n, 128);
+#define MCASE(PPV, E) k_force_mixed<PPV, E><<<g, 128, 0, st>>>(A, V)
+  if (pp) {
+    if (epi == EPI_STORE) MCASE(true, EPI_STORE);
+    else if (epi == EPI_PREDICT) MCASE(true, EPI_PREDICT);
+    else MCASE(true, EPI_CORRECT);
+  } else {
+    if (epi == EPI_STORE) MCASE(false, EPI_STORE);
+    else if (epi == EPI_PREDICT) MCASE(false, EPI_PREDICT);
+    else MCASE(false, EPI_CORRECT);
+  }
+#undef MCASE
+}
+
+void mixed_import_history(MixedBuffers& M, const History& H, int n, int nw, int cur,
+                          cudaStream_t st) {
+  if (n == 0) return;
+  k_hist_to_mixed<<<blocks(n, 256), 256, 0, st>>>(n, H, M.ha[cur], M.hb[cur], M.hc[cur], nw,
+                                                  M.wa[cur], M.wb[cur], M.wc[cur]);
+}
+
+void mixed_export_history(MixedBuffers& M, const History& H, int n, int nw, int cur,
+                          cudaStream_t st) {
+  if (n == 0) return;
+  k_hist_from_mixed<<<blocks(n, 256), 256, 0, st>>>(n, H, M.ha[cur], M.hb[cur], M.hc[cur], nw,
+                                                    M.wa[cur], M.wb[cur], M.wc[cur]);
+}
 
 }  // namespace dem

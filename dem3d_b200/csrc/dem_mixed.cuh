@@ -8,21 +8,26 @@ namespace dem {
 struct MixedBuffers {
   bool ready = false;
   int n = 0, nw = 0, cap = 0;
-  // traversal-order copies: cell-origin-relative FP32 positions + radius,
-  // FP32 velocities / angular velocities
-  float4* rel = nullptr;  // x - ox, y - oy, z - oz, R
-  float4* v4 = nullptr;   // vx, vy, vz, wx
-  float2* w2 = nullptr;   // wy, wz
-  // FP32 history (ft, vt) + Kahan compensation of the tangential spring,
-  // double-buffered like the FP64 tables
-  float4* hval[2] = {nullptr, nullptr};   // [n*cap*2]: (ft.xyz, c.x) (vt.xyz, c.y)
-  float4* wval[2] = {nullptr, nullptr};   // [n*nw*2]
+  // traversal-order FP32 velocities / angular velocities
+  float4* v4 = nullptr;  // vx, vy, vz, wx
+  float2* w2 = nullptr;  // wy, wz
+  // FP32 pair records (ft, vt, Kahan remainder of ft), double-buffered like
+  // the key/count tables of History: a = (ft.xyz, vt.x), b = (vt.yz, lo.xy),
+  // c = lo.z
+  float4* ha[2] = {nullptr, nullptr};
+  float4* hb[2] = {nullptr, nullptr};
+  float* hc[2] = {nullptr, nullptr};
+  // wall records, same packing, [n*nw]
+  float4* wa[2] = {nullptr, nullptr};
+  float4* wb[2] = {nullptr, nullptr};
+  float* wc[2] = {nullptr, nullptr};
 };
 
 bool mixed_available();
 bool mixed_alloc(MixedBuffers& M, int n, int nw, int cap);
 void mixed_free(MixedBuffers& M);
-bool mixed_regrow(MixedBuffers& M, int n, int newcap, int cur, const History& src_old);
+bool mixed_regrow(MixedBuffers& M, int n, int newcap, int cur, const History& old,
+                  cudaStream_t st);
 void mixed_gather(MixedBuffers& M, bool pp, const DevParams* dp, int n, const StateArrays& src,
                   const double* radius, const int* comp, const SortedArrays& S, Counters* cnt,
                   cudaStream_t st);

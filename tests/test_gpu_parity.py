@@ -75,7 +75,24 @@ def test_settling_trajectory_bit_exact():
             assert_same_cells(g, o, f"step {step}")
             np.testing.assert_array_equal(g.logical_ring(), o.logical_ring())
     assert g.ncol() == o.ncol()
-    assert g.count_contacts()[1] > 0  # the bed reached the floor
+    assert g.count_contacts()[0] > 0
+
+
+def test_floor_contacts_bit_exact():
+    """First layer starts in contact with the floor: wall records, wall
+    forces and their history through the Euler start-up and ABM steps."""
+    w = configs.settling(n=300, seed=17, sigma_v=0.01, first_height=0.47)
+    g, o = make_pair(w)
+    for s in (g, o):
+        s.run(1, 4)
+    assert o.count_contacts()[1] > 0
+    assert_same_state(g, o, "floor start-up")
+    assert_same_contacts(g, o, "floor start-up")
+    for s in (g, o):
+        s.run(5, 150)
+    assert_same_state(g, o, "floor")
+    assert_same_contacts(g, o, "floor")
+    assert g.ncol() == o.ncol()
 
 
 def test_graph_run_equals_stepwise():
