@@ -96,7 +96,20 @@ def box_for_fraction(radius: np.ndarray, phi: float) -> float:
     return (vol / phi) ** (1.0 / 3.0)
 
 
-def lattice_positions(n: int, L: float, rng, jitter=0.05):
+def cell_major_order(pos, L, cutoff):
+    """Permutation listing particles cell by cell (x fastest) on the cell grid
+    the library builds for a cubic box of side L (InitCellStructure3D with
+    CutOff = 2*max radius, no cap).  Particle labels are the user's: the
+    library keeps them (the reference's sweep order depends on them), so a
+    generator that numbers particles cell by cell gives the library's
+    label-indexed arrays the same locality as its cell-ordered traversal."""
+    nc = max(1, int(L / cutoff))
+    i3 = np.clip(((pos + 0.5 * L) * (nc / L)).astype(np.int64), 0, nc - 1)
+    key = i3[:, 0] + nc * (i3[:, 1] + nc * i3[:, 2])
+    return np.argsort(key, kind="stable")
+
+
+def lattice_positions(n: int, L: float, rng, jitter=0.05, cutoff=1.2):
     side = int(math.ceil(n ** (1.0 / 3.0) - 1e-9))
     a = L / side
     sites = rng.permutation(side ** 3)[:n]
@@ -104,10 +117,7 @@ def lattice_positions(n: int, L: float, rng, jitter=0.05):
     iy, ix = np.divmod(r, side)
     pos = np.stack([ix, iy, iz], axis=1).astype(np.float64) * a + 0.5 * a - 0.5 * L
     pos += rng.uniform(-jitter, jitter, size=pos.shape) * a
-    # spatially sorted indexing (cell-major), as a generator writing particles
-    # slab by slab would produce
-    order = np.lexsort((pos[:, 0], pos[:, 1], pos[:, 2]))
-    return pos[order]
+    return pos[cell_major_order(pos, L, cutoff)]
 
 
 def dense_packing_params(radius_max, L, *, e=0.8, mu=0.5, dt=1e-4, method_order=4,
@@ -132,7 +142,7 @@ def relaxed_tile(n_tile, phi, seed, rmin=0.4, rmax=0.6, relax_steps=2000, relax_
     rng = np.random.default_rng(seed)
     radius = rng.uniform(rmin, rmax, size=n_tile)
     L = box_for_fraction(radius, phi)
-    pos = lattice_positions(n_tile, L, rng)
+    pos = lattice_positions(n_tile, L, rng, cutoff=2.0 * rmax)
     if relax_steps > 0:
         if system_factory is None:
             from .system import DEMSystem
@@ -154,14 +164,14 @@ def tile_count(n, tile):
     return k if k >= 1 and tile * k ** 3 == n else 0
 
 
-def replicate(pos, radius, L_tile, k):
-    """k x k x k periodic copies of a tile, spatially ordered (cell-major)."""
+def replicate(pos, radius, L_tile, k, cutoff=1.2):
+    """k x k x k periodic copies of a tile, numbered cell by cell."""
     L = k * L_tile
     offs = (np.stack(np.meshgrid(np.arange(k), np.arange(k), np.arange(k), indexing="ij"),
                      axis=-1).reshape(-1, 3) + 0.5) * L_tile - 0.5 * L
     P_ = (pos[None, :, :] + offs[:, None, :]).reshape(-1, 3)
     R_ = np.tile(radius, k ** 3)
-    order = np.lexsort((P_[:, 0], P_[:, 1], P_[:, 2]))
+    order = cell_major_order(P_, L, cutoff)
     return P_[order], R_[order], L
 
 
@@ -182,7 +192,7 @@ def dense_packing(n=1_000_000, phi=0.55, seed=1001, rmin=0.4, rmax=0.6, relax_st
         raise ValueError(f"n={n} is not tile*k^3 for tile={tile}")
     pos_t, rad_t, L_t = relaxed_tile(tile, phi, seed, rmin, rmax, relax_steps, relax_e,
                                      system_factory)
-    pos, radius, L = replicate(pos_t, rad_t, L_t, k)
+    pos, radius, L = replicate(pos_t, rad_t, L_t, k, cutoff=2.0 * rmax)
     rng = np.random.default_rng(seed + 7919)
     vel = rng.normal(0.0, sigma_v, size=(n, 3))
     omega = np.zeros((n, 3))

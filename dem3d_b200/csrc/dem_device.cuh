@@ -25,6 +25,7 @@ struct DevParams {
   double lbox[3], inv_lbox[3], gravity[3];
   double nxbylx, nybyly, nzbylz, nxby2, nyby2, nzby2;
   double ab0, am0, ab[3], am[3];
+  double max_min_dij_sq;  // largest MinDijSq of any pair (screening early-out)
   double comp_radius[NCM], comp_inv_mass[NCM], comp_inv_inertia[NCM], comp_eff_mass[NCM];
   double min_dij[NCM * NCM], min_dij_sq[NCM * NCM];
   double kn[NCM * NCM], yn[NCM * NCM], kt[NCM * NCM], yt[NCM * NCM], mu_sq[NCM * NCM];
@@ -52,6 +53,8 @@ struct Counters {
   int need_capacity; // largest record count requested
   int abort;         // nonzero: later kernels of a captured sequence do nothing
   int abort_tag;     // 1 + index (within a captured chunk) of the failing step
+  int list_overflow; // particles of this pass whose contact-list row overflowed
+  int pad_;
   double wall_fn[NWM];
 };
 
@@ -438,12 +441,100 @@ __device__ __forceinline__ void sweep_as_j(const DevParams& P, const int* __rest
   }
 }
 
+// The same two sweeps, also telling the visitor how the neighbour cell was
+// reached: w = (+1 | -1 | 0) per axis when the cell index wrapped past the
+// upper | lower edge of a periodic axis.
+__device__ __forceinline__ int axis_wrap_w(int j, int N, int pbc, int& w) {
+  w = 0;
+  if (pbc) {
+    if (j == N) { j = 0; w = 1; }
+    if (j == -1) { j = N - 1; w = -1; }
+  }
+  return j;
+}
+
+template <class Visit>
+__device__ __forceinline__ void sweep_as_i_w(const DevParams& P, const int* __restrict__ cs,
+                                             int s, int c, int cx, int cy, int cz,
+                                             Visit&& visit) {
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  const int e = cs[c + 1];
+  for (int t = s + 1; t < e; t++) visit(t, 0, 0, 0);
+  int xi, xf, yi, yf, zi, zf;
+  axis_range(cx, nx, P.pbc[0], xi, xf);
+  axis_range(cy, ny, P.pbc[1], yi, yf);
+  axis_range(cz, nz, P.pbc[2], zi, zf);
+  for (int kz = zf; kz >= zi; kz--) {
+    int wz;
+    const int jz = axis_wrap_w(cz + kz, nz, P.pbc[2], wz);
+    for (int ky = yf; ky >= yi; ky--) {
+      int wy;
+      const int jy = axis_wrap_w(cy + ky, ny, P.pbc[1], wy);
+      for (int kx = xf; kx >= xi; kx--) {
+        if (kx + nx * (ky + ny * kz) <= 0) continue;
+        int wx;
+        const int jx = axis_wrap_w(cx + kx, nx, P.pbc[0], wx);
+        const int jc = jx + nx * (jy + ny * jz);
+        const int b = cs[jc], e2 = cs[jc + 1];
+        for (int t = b; t < e2; t++) visit(t, wx, wy, wz);
+      }
+    }
+  }
+}
+
+template <class Visit, class Own>
+__device__ __forceinline__ void sweep_as_j_w(const DevParams& P, const int* __restrict__ cs,
+                                             int s, int c, int cx, int cy, int cz, Visit&& visit,
+                                             Own&& own) {
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  int ox[3], oy[3], oz[3];
+  const int mx = axis_sorted(cx, nx, P.pbc[0], ox);
+  const int my = axis_sorted(cy, ny, P.pbc[1], oy);
+  const int mz = axis_sorted(cz, nz, P.pbc[2], oz);
+  for (int a = 0; a < mz; a++) {
+    const int dz = oz[a];
+    int wz;
+    const int jz = axis_wrap_w(cz + dz, nz, P.pbc[2], wz);
+    for (int b = 0; b < my; b++) {
+      const int dy = oy[b];
+      int wy;
+      const int jy = axis_wrap_w(cy + dy, ny, P.pbc[1], wy);
+      for (int d = 0; d < mx; d++) {
+        const int dx = ox[d];
+        if (dx == 0 && dy == 0 && dz == 0) {
+          for (int t = cs[c]; t < s; t++) visit(t, 0, 0, 0);
+          own();
+          continue;
+        }
+        if (-dx + nx * (-dy + ny * -dz) <= 0) continue;
+        int wx;
+        const int jx = axis_wrap_w(cx + dx, nx, P.pbc[0], wx);
+        const int jc = jx + nx * (jy + ny * jz);
+        const int b0 = cs[jc], e2 = cs[jc + 1];
+        for (int t = b0; t < e2; t++) visit(t, wx, wy, wz);
+      }
+    }
+  }
+}
+
+// Minimum image of one component exactly as Rij(k) - Lbox(k)*nint(Rij(k)*
+// InvLbox(k)) (src/MForces.f90:212-214), given the image n the cell sweep
+// implies: if |Rij - n*L| < 0.49*L then nint(Rij/L) == n (the margin covers
+// the rounding of Rij*InvLbox), so Rij - L*n is the reference's value bit for
+// bit; otherwise the formula itself is evaluated.
+__device__ __forceinline__ double min_image(double r, int pbc, double L, double iL, int n) {
+  if (!pbc) return r;
+  const double d = r - L * (double)n;
+  if (fabs(d) < 0.49 * L) return d;
+  return r - L * fnint(r * iL);
+}
+
 // Loop 1 / loop 2 driven by the screening kernel's contact list when the
 // particle's row did not overflow, else by the full sweep (same order).
-template <class Visit>
+template <bool SWEEP, class Visit>
 __device__ __forceinline__ void walk_as_i(const ForceArgs& A, int4 meta, int s, int c, int cx,
                                           int cy, int cz, Visit&& visit) {
-  if (meta.x >= 0) {
+  if (!SWEEP) {
     const int* l = A.cl_slot + (size_t)s * KC;
     for (int k = 0; k < meta.x; k++) visit(l[k]);
   } else {
@@ -451,10 +542,10 @@ __device__ __forceinline__ void walk_as_i(const ForceArgs& A, int4 meta, int s, 
   }
 }
 
-template <class Visit, class Own>
+template <bool SWEEP, class Visit, class Own>
 __device__ __forceinline__ void walk_as_j(const ForceArgs& A, int4 meta, int s, int c, int cx,
                                           int cy, int cz, Visit&& visit, Own&& own) {
-  if (meta.x >= 0) {
+  if (!SWEEP) {
     const int* l = A.cl_slot + (size_t)s * KC + meta.x;
     for (int k = 0; k < meta.y; k++) visit(l[k]);
     own();

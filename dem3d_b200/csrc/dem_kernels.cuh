@@ -326,13 +326,17 @@ __device__ __forceinline__ void hist_write(const History& H, int owner, int r, i
 // K2+K4: force kernel (FP64, exact order)
 
 
-template <bool PP, int EPI>
+// SWEEP = false: particles whose contact-list row is valid; SWEEP = true:
+// the (rare) particles whose row overflowed, which sweep the cells here.
+template <bool PP, int EPI, bool SWEEP>
 __global__ void __launch_bounds__(128) k_force_fp64(ForceArgs A) {
   if (A.cnt->abort) return;
+  if (SWEEP && A.cnt->list_overflow == 0) return;
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long n_col = 0, n_pc = 0, n_wc = 0;
   int need = 0;
-  if (s < A.n) {
+  const int4 meta = s < A.n ? A.cl_meta[s] : make_int4(0, 0, 0, 0);
+  if (s < A.n && (meta.x < 0) == SWEEP) {
     const DevParams& P = *A.P;
     const SortedArrays& S = A.S;
     const int nx = P.nx, ny = P.ny, nz = P.nz;
@@ -408,8 +412,7 @@ __global__ void __launch_bounds__(128) k_force_fp64(ForceArgs A) {
 
     // ---- loop 1: own cell after p, then the half-shell cells in the order
     // of the FirstNeighbour list (reverse of AddAllNeighbours3D insertion)
-    const int4 meta = A.cl_meta[s];
-    walk_as_i(A, meta, s, c, cx, cy, cz, visit_i);
+    walk_as_i<SWEEP>(A, meta, s, c, cx, cy, cz, visit_i);
 
     // ---- walls (src/MForces.f90:274-314)
     for (int w = 0; w < P.nw; w++) {
@@ -504,7 +507,7 @@ __global__ void __launch_bounds__(128) k_force_fp64(ForceArgs A) {
         if (update && orig < qo) record(qo, o.FT, o.VT);
       }
     };
-    walk_as_j(A, meta, s, c, cx, cy, cz, visit_j, [&]() {
+    walk_as_j<SWEEP>(A, meta, s, c, cx, cy, cz, visit_j, [&]() {
 #pragma unroll
       for (int k = 0; k < 3; k++) F[k] = F[k] + iF[k];
 #pragma unroll
@@ -647,12 +650,12 @@ __global__ void __launch_bounds__(128) k_force_fp64(ForceArgs A) {
 // the latency of the candidate loads; the heavy contact arithmetic then runs
 // only over real contacts.
 template <bool PP>
-__global__ void __launch_bounds__(256) k_screen(const DevParams* __restrict__ Pp, int n,
+__global__ void __launch_bounds__(256, 3) k_screen(const DevParams* __restrict__ Pp, int n,
                                                 const double4* __restrict__ pos,
                                                 const int* __restrict__ comp,
                                                 const int* __restrict__ slot_cell,
                                                 const int* __restrict__ cs, ContactLists L,
-                                                const Counters* __restrict__ cnt) {
+                                                Counters* __restrict__ cnt) {
   if (cnt->abort) return;
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
@@ -665,33 +668,40 @@ __global__ void __launch_bounds__(256) k_screen(const DevParams* __restrict__ Pp
   const bool pb[3] = {P.pbc[0] != 0, P.pbc[1] != 0, P.pbc[2] != 0};
   const double lb[3] = {P.lbox[0], P.lbox[1], P.lbox[2]};
   const double il[3] = {P.inv_lbox[0], P.inv_lbox[1], P.inv_lbox[2]};
+  const double maxsq = P.max_min_dij_sq;
   int* out = L.slot + (size_t)s * KC;
   int m = 0;
-  auto test = [&](int t, bool p_is_i) {
+  // sg = +1: p is "i" (Rij = xq - xp, image -w); sg = -1: p is "j"
+  auto test = [&](int t, int sg, int wx, int wy, int wz) {
     const double4 q4 = pos[t];
     double Rij[3];
-    if (p_is_i) {
-      Rij[0] = q4.x - p4.x; Rij[1] = q4.y - p4.y; Rij[2] = q4.z - p4.z;
-    } else {
-      Rij[0] = p4.x - q4.x; Rij[1] = p4.y - q4.y; Rij[2] = p4.z - q4.z;
-    }
-#pragma unroll
-    for (int k = 0; k < 3; k++)
-      if (pb[k]) Rij[k] = Rij[k] - lb[k] * fnint(Rij[k] * il[k]);
+    Rij[0] = sg > 0 ? q4.x - p4.x : p4.x - q4.x;
+    Rij[0] = min_image(Rij[0], pb[0], lb[0], il[0], -sg * wx);
+    // DijSq >= fl(Rij_x^2) (sums of non-negative terms never round below
+    // a partial sum): no overlap is possible past the largest MinDijSq
+    if (Rij[0] * Rij[0] >= maxsq) return;
+    Rij[1] = sg > 0 ? q4.y - p4.y : p4.y - q4.y;
+    Rij[1] = min_image(Rij[1], pb[1], lb[1], il[1], -sg * wy);
+    Rij[2] = sg > 0 ? q4.z - p4.z : p4.z - q4.z;
+    Rij[2] = min_image(Rij[2], pb[2], lb[2], il[2], -sg * wz);
     const double DijSq = sumsq3(Rij);
     const int cq = PP ? 0 : comp[t];
-    const double Delta = p_is_i ? Material<PP>::min_dij_sq(P, cp, p4.w, cq, q4.w) - DijSq
+    const double Delta = sg > 0 ? Material<PP>::min_dij_sq(P, cp, p4.w, cq, q4.w) - DijSq
                                 : Material<PP>::min_dij_sq(P, cq, q4.w, cp, p4.w) - DijSq;
     if (Delta > 0.0) {
       if (m < KC) out[m] = t;
       m++;
     }
   };
-  sweep_as_i(P, cs, s, c, cx, cy, cz, [&](int t) { test(t, true); });
+  sweep_as_i_w(P, cs, s, c, cx, cy, cz,
+               [&](int t, int wx, int wy, int wz) { test(t, 1, wx, wy, wz); });
   const int n1 = m;
   int n2b = 0;
-  sweep_as_j(P, cs, s, c, cx, cy, cz, [&](int t) { test(t, false); }, [&]() { n2b = m - n1; });
+  sweep_as_j_w(
+      P, cs, s, c, cx, cy, cz, [&](int t, int wx, int wy, int wz) { test(t, -1, wx, wy, wz); },
+      [&]() { n2b = m - n1; });
   L.meta[s] = m <= KC ? make_int4(n1, n2b, m - n1 - n2b, 0) : make_int4(-1, 0, 0, 0);
+  if (m > KC) atomicAdd(&cnt->list_overflow, 1);
 }
 
 // ring store of MoveParticlesEuler (src/MDEM.f90:266-271): (v,a,alpha) -> slot

@@ -352,9 +352,14 @@ int launch_force(dem_ctx* c, const StateArrays& tgt, bool update, double dt, int
   unsigned g = blocks_for(c->n, 128);
   if (c->precision == DEM_PREC_MIXED) {
     timed(c, "force_mixed", [&]() { mixed_force(c->M, c->pp, epi, A, c->hcur, c->stream); });
+    c->launches++;  // list-driven + overflow launches
     return DEM_OK;
   }
-#define FORCE_CASE(PPV, E) launch(c, "force_fp64", k_force_fp64<PPV, E>, g, 128, A);
+#define FORCE_CASE(PPV, E)                                                  \
+  {                                                                         \
+    launch(c, "force_fp64", k_force_fp64<PPV, E, false>, g, 128, A);        \
+    launch(c, "force_fp64_sweep", k_force_fp64<PPV, E, true>, g, 128, A);   \
+  }
   if (c->pp) {
     if (epi == EPI_STORE) FORCE_CASE(true, EPI_STORE)
     else if (epi == EPI_PREDICT) FORCE_CASE(true, EPI_PREDICT)
@@ -389,6 +394,7 @@ int reset_pass_counters(dem_ctx* c, bool update) {
   // per-pass statistics; Ncol and the escape count accumulate
   CK(cudaMemsetAsync(&c->cnt->pair_contacts, 0, 3 * sizeof(unsigned long long), c->stream));
   CK(cudaMemsetAsync(&c->cnt->wall_fn[0], 0, sizeof(double) * NWM, c->stream));
+  CK(cudaMemsetAsync(&c->cnt->list_overflow, 0, sizeof(int), c->stream));
   if (update) CK(cudaMemsetAsync(&c->cnt->need_capacity, 0, sizeof(int), c->stream));
   // escapes are counted by the corrector of the current step only
   if (!update) CK(cudaMemsetAsync(&c->cnt->escaped, 0, sizeof(unsigned long long), c->stream));
@@ -424,11 +430,11 @@ int force_pass(dem_ctx* c, const StateArrays& src, const StateArrays& tgt, bool 
     if (c->pp)
       launch(c, "screen", k_screen<true>, blocks_for(c->n, 256), 256, (const DevParams*)c->dp,
              c->n, (const double4*)c->S.pos, (const int*)c->S.comp, (const int*)c->S.cell,
-             (const int*)c->cell_start, c->CL, (const Counters*)c->cnt);
+             (const int*)c->cell_start, c->CL, c->cnt);
     else
       launch(c, "screen", k_screen<false>, blocks_for(c->n, 256), 256, (const DevParams*)c->dp,
              c->n, (const double4*)c->S.pos, (const int*)c->S.comp, (const int*)c->S.cell,
-             (const int*)c->cell_start, c->CL, (const Counters*)c->cnt);
+             (const int*)c->cell_start, c->CL, c->cnt);
   }
   for (int attempt = 0;; attempt++) {
     st = launch_force(c, tgt, update, dt, epi, rm, tag);
@@ -675,6 +681,16 @@ int dem_create(const dem_params* p, dem_ctx** out) {
   std::memcpy(h.ktw, p->ktw, sizeof(h.ktw));
   std::memcpy(h.ytw, p->ytw, sizeof(h.ytw));
   std::memcpy(h.muw_sq, p->muw_sq, sizeof(h.muw_sq));
+  // largest MinDijSq of any pair, for the screening early-out
+  h.max_min_dij_sq = 0.0;
+  if (p->n_components > 0) {
+    for (int i = 0; i < p->n_components; i++)
+      for (int j = 0; j < p->n_components; j++)
+        h.max_min_dij_sq = std::max(h.max_min_dij_sq, p->min_dij_sq[i * NCM + j]);
+  } else {
+    double d = p->pp_rmax + p->pp_rmax;  // Ri + Rj <= rmax + rmax after rounding
+    h.max_min_dij_sq = d * d;
+  }
   h.pp_mass_coef = p->pp_mass_coef;
   h.pp_density = p->pp_density;
   h.pp_fluid_density = p->pp_fluid_density;

@@ -237,13 +237,15 @@ __device__ __forceinline__ unsigned long long wsum(unsigned long long v) {
   return v;
 }
 
-template <bool PP, int EPI>
+template <bool PP, int EPI, bool SWEEP>
 __global__ void __launch_bounds__(128) k_force_mixed(ForceArgs A, MixedView V) {
   if (A.cnt->abort) return;
+  if (SWEEP && A.cnt->list_overflow == 0) return;
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long n_col = 0, n_pc = 0, n_wc = 0;
   int need = 0;
-  if (s < A.n) {
+  const int4 meta = s < A.n ? A.cl_meta[s] : make_int4(0, 0, 0, 0);
+  if (s < A.n && (meta.x < 0) == SWEEP) {
     const DevParams& P = *A.P;
     const SortedArrays& S = A.S;
     const int nx = P.nx, ny = P.ny;
@@ -323,8 +325,7 @@ __global__ void __launch_bounds__(128) k_force_mixed(ForceArgs A, MixedView V) {
         if (update && orig < qo) record(qo, o.FT, o.FTlo, o.VT);
       }
     };
-    const int4 meta = A.cl_meta[s];
-    walk_as_i(A, meta, s, c, cx, cy, cz, visit_i);
+    walk_as_i<SWEEP>(A, meta, s, c, cx, cy, cz, visit_i);
 
     for (int w = 0; w < P.nw; w++) {
       const dem_wall& W = P.walls[w];
@@ -392,7 +393,7 @@ __global__ void __launch_bounds__(128) k_force_mixed(ForceArgs A, MixedView V) {
         if (update && orig < qo) record(qo, o.FT, o.FTlo, o.VT);
       }
     };
-    walk_as_j(A, meta, s, c, cx, cy, cz, visit_j, [&]() {
+    walk_as_j<SWEEP>(A, meta, s, c, cx, cy, cz, visit_j, [&]() {
       F = F + iF;
       T = T + iT;
     });
@@ -695,7 +696,11 @@ void mixed_force(MixedBuffers& M, bool pp, int epi, const ForceArgs& A, int cur,
   V.wwb = M.wb[cur ^ 1];
   V.wwc = M.wc[cur ^ 1];
   unsigned g = blocks(A.n, 128);
-#define MCASE(PPV, E) k_force_mixed<PPV, E><<<g, 128, 0, st>>>(A, V)
+#define MCASE(PPV, E)                                        \
+  do {                                                       \
+    k_force_mixed<PPV, E, false><<<g, 128, 0, st>>>(A, V);   \
+    k_force_mixed<PPV, E, true><<<g, 128, 0, st>>>(A, V);    \
+  } while (0)
   if (pp) {
     if (epi == EPI_STORE) MCASE(true, EPI_STORE);
     else if (epi == EPI_PREDICT) MCASE(true, EPI_PREDICT);
