@@ -125,7 +125,13 @@ GPU_ONLY = {
     "timer_stop": (C.c_int, [_P, _DP]),
     "get_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "get_pass_stats": (C.c_int, [_P, _I64P, _I64P, _I64P, _I32P]),
+    # device pointers for positions and outputs; see the header
+    "distribute_particles_noalloc": (C.c_int, [C.POINTER(DemParams), C.c_int32, _P, _P, _P, _P,
+                                               _I32P, _P, C.c_char_p, C.c_int32]),
 }
+
+NOALLOC_MAX_PARTICLES = 262144
+NOALLOC_MAX_CELLS = 262144
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libdem3d_b200.so")

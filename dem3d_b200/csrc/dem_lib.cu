@@ -1373,3 +1373,167 @@ int dem_get_pass_stats(dem_ctx* c, int64_t* pair_contacts, int64_t* wall_contact
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free cell distribution (dem_distribute_particles_noalloc).
+//
+// For callers that may not allocate device memory: the working memory of the
+// counting sort lives in one file-scope device array of fixed size instead
+// of per-context buffers.  Host code only ever sees the array's host-side
+// stand-in symbol, which is not a device address; the device address is
+// looked up once per device with cudaGetSymbolAddress.
+
+namespace {
+
+constexpr int NA_MAXN = DEM_NOALLOC_MAX_PARTICLES;
+constexpr int NA_MAXC = DEM_NOALLOC_MAX_CELLS;
+constexpr int NA_TILES = (NA_MAXC + SCAN_TILE - 1) / SCAN_TILE;
+
+struct NoAllocScratch {
+  DevParams params;
+  Counters counters;
+  int cell_cnt[NA_MAXC];
+  int bsum[NA_TILES + 1];
+  int a_cell[NA_MAXN];
+  int a_loc[NA_MAXN];
+  int a_orig[NA_MAXN];
+  int t_orig[NA_MAXN];
+  int slot_cell[NA_MAXN];
+  unsigned a_key[NA_MAXN];
+  unsigned t_key[NA_MAXN];
+  double px[NA_MAXN];
+  double py[NA_MAXN];
+  double pz[NA_MAXN];
+};
+
+constexpr int NA_MAX_DEVICES = 64;
+void* g_na_base[NA_MAX_DEVICES] = {};
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
+
+extern "C" int dem_distribute_particles_noalloc(const dem_params* p, int32_t n,
+                                                const double* d_pos, int32_t* d_cell_index,
+                                                int32_t* d_traversal, int32_t* d_cell_start,
+                                                int32_t* ncell_out, void* stream, char* err,
+                                                int32_t err_cap) {
+  auto say = [&](int code, const char* msg) {
+    if (err && err_cap > 0) std::snprintf(err, (size_t)err_cap, "%s", msg);
+    return code;
+  };
+  if (!p || n < 0) return say(DEM_ERR_INVALID, "null parameters or negative n");
+  if (n > NA_MAXN) {
+    char m[160];
+    std::snprintf(m, sizeof(m),
+                  "n = %d exceeds DEM_NOALLOC_MAX_PARTICLES = %d (use a context instead)", n,
+                  NA_MAXN);
+    return say(DEM_ERR_CAPACITY, m);
+  }
+  if (n > 0 && (!d_pos || !d_cell_index || !d_traversal)) return say(DEM_ERR_INVALID, "null array");
+  if (!d_cell_start) return say(DEM_ERR_INVALID, "null cell_start");
+  // cell grid: InitCellStructure3D (src/MCells.f90:155-227), CutOff = 2*max R
+  double rmax = 0.0;
+  if (p->n_components > 0) {
+    if (p->n_components > NCM) return say(DEM_ERR_INVALID, "too many components");
+    for (int i = 0; i < p->n_components; i++) rmax = std::max(rmax, p->comp_radius[i]);
+  } else {
+    rmax = p->pp_rmax;
+  }
+  const double CutOff = 2.0 * rmax;
+  if (!(CutOff > 0.0)) return say(DEM_ERR_INVALID, "radius must be positive");
+  const int MaxNCell = p->max_ncell > 0 ? p->max_ncell : 30000;
+  const double Lx = p->lbox[0], Ly = p->lbox[1], Lz = p->lbox[2];
+  const int Nx4 = (int)(Lx / CutOff), Ny4 = (int)(Ly / CutOff), Nz4 = (int)(Lz / CutOff);
+  int N[3];
+  if ((long long)Nx4 * Ny4 * Nz4 > MaxNCell) {
+    const double LCell = std::pow(Lx * Ly * Lz / (double)MaxNCell, 1.0 / 3.0);
+    N[0] = (int)(Lx / LCell);
+    N[1] = (int)(Ly / LCell);
+    N[2] = (int)(Lz / LCell);
+  } else {
+    N[0] = Nx4;
+    N[1] = Ny4;
+    N[2] = Nz4;
+  }
+  for (int k = 0; k < 3; k++) {
+    if (N[k] < 1) return say(DEM_ERR_INVALID, "box smaller than one cell");
+    if (p->pbc[k] && N[k] < 3)
+      return say(DEM_ERR_UNSUPPORTED, "fewer than 3 cells along a periodic axis");
+  }
+  const long long ncell_ll = (long long)N[0] * N[1] * N[2];
+  if (ncell_ll > NA_MAXC) {
+    char m[160];
+    std::snprintf(m, sizeof(m),
+                  "%lld cells exceed DEM_NOALLOC_MAX_CELLS = %d (use a context instead)",
+                  ncell_ll, NA_MAXC);
+    return say(DEM_ERR_CAPACITY, m);
+  }
+  const int ncell = (int)ncell_ll;
+  if (ncell_out) *ncell_out = ncell;
+
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NA_MAX_DEVICES) {
+    cudaGetLastError();
+    return say(DEM_ERR_NO_DEVICE, "no usable CUDA device");
+  }
+  // once per device, with that device current: the array's device address
+  if (!g_na_base[dev]) {
+    void* base = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&base, g_noalloc_scratch);
+    if (e != cudaSuccess || !base) {
+      cudaGetLastError();
+      return say(DEM_ERR_CUDA, "cudaGetSymbolAddress of the scratch array failed");
+    }
+    g_na_base[dev] = base;
+  }
+  unsigned char* base = (unsigned char*)g_na_base[dev];
+  NoAllocScratch* S = (NoAllocScratch*)base;  // device addresses only
+  DevParams* dp = &S->params;
+  Counters* cnt = &S->counters;
+  cudaStream_t st = (cudaStream_t)stream;
+
+  DevParams h{};
+  h.nx = N[0];
+  h.ny = N[1];
+  h.nz = N[2];
+  h.ncell = ncell;
+  h.nxbylx = (double)N[0] / Lx;
+  h.nybyly = (double)N[1] / Ly;
+  h.nzbylz = (double)N[2] / Lz;
+  h.nxby2 = (double)N[0] * 0.5;
+  h.nyby2 = (double)N[1] * 0.5;
+  h.nzby2 = (double)N[2] * 0.5;
+  for (int k = 0; k < 3; k++) h.pbc[k] = p->pbc[k] ? 1 : 0;
+
+  // the array keeps the previous call's contents: reset what must start at 0
+  cudaError_t e = cudaMemcpyAsync(dp, &h, sizeof(DevParams), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(cnt, 0, sizeof(Counters), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(S->cell_cnt, 0, sizeof(int) * (size_t)ncell, st);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return say(DEM_ERR_CUDA, cudaGetErrorString(e));
+  }
+  const int ntiles = (ncell + SCAN_TILE - 1) / SCAN_TILE;
+  if (n > 0) {
+    k_rows_to_soa<<<blocks_for(n, 256), 256, 0, st>>>(n, d_pos, S->px, S->py, S->pz);
+    // DistributeParticles3D: every particle enters its cell in index order
+    k_assign<<<blocks_for(n, 256), 256, 0, st>>>(dp, n, 1, S->px, S->py, S->pz, d_traversal,
+                                                   S->slot_cell, S->cell_cnt, S->a_cell, S->a_loc,
+                                                   S->a_key, S->a_orig, cnt);
+  }
+  k_scan_tiles<<<ntiles, SCAN_THREADS, 0, st>>>(S->cell_cnt, ncell, d_cell_start, S->bsum, cnt);
+  k_scan_bsums<<<1, SCAN_THREADS, 0, st>>>(S->bsum, ntiles, d_cell_start, ncell, cnt);
+  k_scan_add<<<blocks_for(ncell, 256), 256, 0, st>>>(d_cell_start, ncell, S->bsum, cnt);
+  if (n > 0) {
+    k_scatter<<<blocks_for(n, 256), 256, 0, st>>>(n, S->a_cell, S->a_loc, S->a_key, S->a_orig,
+                                                   d_cell_start, S->t_key, S->t_orig, cnt);
+    k_cellsort<<<blocks_for(ncell, 128), 128, 0, st>>>(ncell, d_cell_start, S->t_key, S->t_orig,
+                                                        d_traversal, S->slot_cell, d_cell_index,
+                                                        cnt);
+  }
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return say(DEM_ERR_CUDA, cudaGetErrorString(e));
+  return DEM_OK;
+}

@@ -234,6 +234,35 @@ int dem_get_stream(dem_ctx* ctx, void** stream);
 int dem_get_pass_stats(dem_ctx* ctx, int64_t* pair_contacts, int64_t* wall_contacts,
                        int64_t* movers, int32_t* hist_capacity);
 
+/* Allocation-free cell distribution.  No counterpart in the reference: it
+ * serves callers that may not allocate device memory while they run, such
+ * as code recording work into a CUDA graph, a host application whose device
+ * memory is all handed out by its own pool or framework, or a service that
+ * forbids allocation after start-up.  It computes what
+ * dem_initialize_cell_distribution computes (the cell of every particle and
+ * the particles of every cell in list order) for one particle set, without a
+ * context and without calling cudaMalloc/cudaFree or any allocating library:
+ * its working memory is one static device array of about 14 MB that every
+ * GPU which loads the library keeps until the process exits.
+ *  - d_pos: device array of n rows (x,y,z); d_cell_index[n], d_traversal[n]
+ *    and d_cell_start[ncell+1] are device outputs (ncell from
+ *    dem_get_grid's formula, also returned in *ncell_out if not NULL);
+ *  - limits: n <= DEM_NOALLOC_MAX_PARTICLES and
+ *    ncell <= DEM_NOALLOC_MAX_CELLS, else DEM_ERR_CAPACITY (with a message
+ *    in err, if given); the other checks of dem_create apply;
+ *  - stream: a cudaStream_t (NULL = the default stream); the call waits for
+ *    its own work before returning;
+ *  - the first call on a device looks up the array's device address, so on
+ *    each device make that first call before any stream capture;
+ *  - all calls share the one array: calls that overlap on the GPU (other
+ *    threads, other streams) race and must be serialised by the caller. */
+#define DEM_NOALLOC_MAX_PARTICLES 262144
+#define DEM_NOALLOC_MAX_CELLS 262144
+int dem_distribute_particles_noalloc(const dem_params* params, int32_t n, const double* d_pos,
+                                     int32_t* d_cell_index, int32_t* d_traversal,
+                                     int32_t* d_cell_start, int32_t* ncell_out, void* stream,
+                                     char* err, int32_t err_cap);
+
 #ifdef __cplusplus
 }
 #endif
