@@ -517,6 +517,70 @@ __device__ __forceinline__ void sweep_as_j_w(const DevParams& P, const int* __re
   }
 }
 
+// The two sweeps as slot ranges: emit(b, e, wx, wy, wz) per visited cell
+// (own cell: the part after / before p), own() right after p's own range in
+// loop 2.
+template <class Emit>
+__device__ __forceinline__ void sweep_cells_as_i(const DevParams& P, const int* __restrict__ cs,
+                                                 int s, int c, int cx, int cy, int cz,
+                                                 Emit&& emit) {
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  emit(s + 1, cs[c + 1], 0, 0, 0);
+  int xi, xf, yi, yf, zi, zf;
+  axis_range(cx, nx, P.pbc[0], xi, xf);
+  axis_range(cy, ny, P.pbc[1], yi, yf);
+  axis_range(cz, nz, P.pbc[2], zi, zf);
+  for (int kz = zf; kz >= zi; kz--) {
+    int wz;
+    const int jz = axis_wrap_w(cz + kz, nz, P.pbc[2], wz);
+    for (int ky = yf; ky >= yi; ky--) {
+      int wy;
+      const int jy = axis_wrap_w(cy + ky, ny, P.pbc[1], wy);
+      for (int kx = xf; kx >= xi; kx--) {
+        if (kx + nx * (ky + ny * kz) <= 0) continue;
+        int wx;
+        const int jx = axis_wrap_w(cx + kx, nx, P.pbc[0], wx);
+        const int jc = jx + nx * (jy + ny * jz);
+        emit(cs[jc], cs[jc + 1], wx, wy, wz);
+      }
+    }
+  }
+}
+
+template <class Emit, class Own>
+__device__ __forceinline__ void sweep_cells_as_j(const DevParams& P, const int* __restrict__ cs,
+                                                 int s, int c, int cx, int cy, int cz, Emit&& emit,
+                                                 Own&& own) {
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  int ox[3], oy[3], oz[3];
+  const int mx = axis_sorted(cx, nx, P.pbc[0], ox);
+  const int my = axis_sorted(cy, ny, P.pbc[1], oy);
+  const int mz = axis_sorted(cz, nz, P.pbc[2], oz);
+  for (int a = 0; a < mz; a++) {
+    const int dz = oz[a];
+    int wz;
+    const int jz = axis_wrap_w(cz + dz, nz, P.pbc[2], wz);
+    for (int b = 0; b < my; b++) {
+      const int dy = oy[b];
+      int wy;
+      const int jy = axis_wrap_w(cy + dy, ny, P.pbc[1], wy);
+      for (int d = 0; d < mx; d++) {
+        const int dx = ox[d];
+        if (dx == 0 && dy == 0 && dz == 0) {
+          emit(cs[c], s, 0, 0, 0);
+          own();
+          continue;
+        }
+        if (-dx + nx * (-dy + ny * -dz) <= 0) continue;
+        int wx;
+        const int jx = axis_wrap_w(cx + dx, nx, P.pbc[0], wx);
+        const int jc = jx + nx * (jy + ny * jz);
+        emit(cs[jc], cs[jc + 1], wx, wy, wz);
+      }
+    }
+  }
+}
+
 // Minimum image of one component exactly as Rij(k) - Lbox(k)*nint(Rij(k)*
 // InvLbox(k)) (src/MForces.f90:212-214), given the image n the cell sweep
 // implies: if |Rij - n*L| < 0.49*L then nint(Rij/L) == n (the margin covers

@@ -646,16 +646,26 @@ __global__ void __launch_bounds__(128) k_force_fp64(ForceArgs A) {
 // K2 screening: the overlap test DeltaDijSq = MinDijSq - DijSq > 0
 // (src/MForces.f90:209-224) for every candidate of the sweep, in FP64 with the
 // same operations as the force kernels, compacted into the particle's
-// contact-list row in sweep order.  Register-light, so that many warps hide
-// the latency of the candidate loads; the heavy contact arithmetic then runs
-// only over real contacts.
+// contact-list row in sweep order.  The cells of both sweeps are first
+// gathered as up to 29 slot ranges (range, image of the cell, role) and then
+// scanned by one loop with a single copy of the test: the kernel stays small
+// (instruction fetch) and register-light (many warps hide the candidate-load
+// latency).  The heavy contact arithmetic then runs only over real contacts.
+struct ScreenRange {
+  int b, e, code;  // code: bit 0..5 image (2 bits per axis, biased by 1), bit 6: p is "j"
+};
+
+__device__ __forceinline__ int range_code(int wx, int wy, int wz, bool p_is_j) {
+  return (wx + 1) | ((wy + 1) << 2) | ((wz + 1) << 4) | (p_is_j ? 64 : 0);
+}
+
 template <bool PP>
-__global__ void __launch_bounds__(256, 3) k_screen(const DevParams* __restrict__ Pp, int n,
-                                                const double4* __restrict__ pos,
-                                                const int* __restrict__ comp,
-                                                const int* __restrict__ slot_cell,
-                                                const int* __restrict__ cs, ContactLists L,
-                                                Counters* __restrict__ cnt) {
+__global__ void __launch_bounds__(256, 4) k_screen(const DevParams* __restrict__ Pp, int n,
+                                                   const double4* __restrict__ pos,
+                                                   const int* __restrict__ comp,
+                                                   const int* __restrict__ slot_cell,
+                                                   const int* __restrict__ cs, ContactLists L,
+                                                   Counters* __restrict__ cnt) {
   if (cnt->abort) return;
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
@@ -663,45 +673,166 @@ __global__ void __launch_bounds__(256, 3) k_screen(const DevParams* __restrict__
   const int nx = P.nx, ny = P.ny;
   const int c = slot_cell[s];
   const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
+
+  // ---- the ranges, in sweep order: loop 1, then loop 2
+  ScreenRange R[29];
+  int nr = 0, own_j = -1;
+  sweep_cells_as_i(P, cs, s, c, cx, cy, cz, [&](int b, int e, int wx, int wy, int wz) {
+    R[nr++] = ScreenRange{b, e, range_code(wx, wy, wz, false)};
+  });
+  const int nr1 = nr;
+  sweep_cells_as_j(
+      P, cs, s, c, cx, cy, cz,
+      [&](int b, int e, int wx, int wy, int wz) {
+        R[nr++] = ScreenRange{b, e, range_code(wx, wy, wz, true)};
+      },
+      [&]() { own_j = nr - 1; });
+
+  // ---- one loop over all candidates
   const double4 p4 = pos[s];
   const int cp = PP ? 0 : comp[s];
-  const bool pb[3] = {P.pbc[0] != 0, P.pbc[1] != 0, P.pbc[2] != 0};
-  const double lb[3] = {P.lbox[0], P.lbox[1], P.lbox[2]};
-  const double il[3] = {P.inv_lbox[0], P.inv_lbox[1], P.inv_lbox[2]};
   const double maxsq = P.max_min_dij_sq;
   int* out = L.slot + (size_t)s * KC;
-  int m = 0;
-  // sg = +1: p is "i" (Rij = xq - xp, image -w); sg = -1: p is "j"
-  auto test = [&](int t, int sg, int wx, int wy, int wz) {
-    const double4 q4 = pos[t];
-    double Rij[3];
-    Rij[0] = sg > 0 ? q4.x - p4.x : p4.x - q4.x;
-    Rij[0] = min_image(Rij[0], pb[0], lb[0], il[0], -sg * wx);
-    // DijSq >= fl(Rij_x^2) (sums of non-negative terms never round below
-    // a partial sum): no overlap is possible past the largest MinDijSq
-    if (Rij[0] * Rij[0] >= maxsq) return;
-    Rij[1] = sg > 0 ? q4.y - p4.y : p4.y - q4.y;
-    Rij[1] = min_image(Rij[1], pb[1], lb[1], il[1], -sg * wy);
-    Rij[2] = sg > 0 ? q4.z - p4.z : p4.z - q4.z;
-    Rij[2] = min_image(Rij[2], pb[2], lb[2], il[2], -sg * wz);
-    const double DijSq = sumsq3(Rij);
-    const int cq = PP ? 0 : comp[t];
-    const double Delta = sg > 0 ? Material<PP>::min_dij_sq(P, cp, p4.w, cq, q4.w) - DijSq
-                                : Material<PP>::min_dij_sq(P, cq, q4.w, cp, p4.w) - DijSq;
-    if (Delta > 0.0) {
-      if (m < KC) out[m] = t;
-      m++;
+  int m = 0, n1 = 0, n2b = 0;
+  for (int r = 0; r < nr; r++) {
+    const ScreenRange rr = R[r];
+    const bool pj = rr.code & 64;
+    const int sg = pj ? -1 : 1;
+    const int nxi = sg * -(((rr.code) & 3) - 1);
+    const int nyi = sg * -(((rr.code >> 2) & 3) - 1);
+    const int nzi = sg * -(((rr.code >> 4) & 3) - 1);
+    for (int t = rr.b; t < rr.e; t++) {
+      const double4 q4 = pos[t];
+      double Rij[3];
+      Rij[0] = pj ? p4.x - q4.x : q4.x - p4.x;
+      Rij[0] = min_image(Rij[0], P.pbc[0], P.lbox[0], P.inv_lbox[0], nxi);
+      // DijSq >= fl(Rij_x^2): sums of non-negative terms never round below a
+      // partial sum, so no overlap is possible past the largest MinDijSq
+      if (Rij[0] * Rij[0] >= maxsq) continue;
+      Rij[1] = pj ? p4.y - q4.y : q4.y - p4.y;
+      Rij[1] = min_image(Rij[1], P.pbc[1], P.lbox[1], P.inv_lbox[1], nyi);
+      Rij[2] = pj ? p4.z - q4.z : q4.z - p4.z;
+      Rij[2] = min_image(Rij[2], P.pbc[2], P.lbox[2], P.inv_lbox[2], nzi);
+      const double DijSq = sumsq3(Rij);
+      const int cq = PP ? 0 : comp[t];
+      const double Delta = pj ? Material<PP>::min_dij_sq(P, cq, q4.w, cp, p4.w) - DijSq
+                              : Material<PP>::min_dij_sq(P, cp, p4.w, cq, q4.w) - DijSq;
+      if (Delta > 0.0) {
+        if (m < KC) out[m] = t;
+        m++;
+      }
     }
-  };
-  sweep_as_i_w(P, cs, s, c, cx, cy, cz,
-               [&](int t, int wx, int wy, int wz) { test(t, 1, wx, wy, wz); });
-  const int n1 = m;
-  int n2b = 0;
-  sweep_as_j_w(
-      P, cs, s, c, cx, cy, cz, [&](int t, int wx, int wy, int wz) { test(t, -1, wx, wy, wz); },
-      [&]() { n2b = m - n1; });
+    if (r == nr1 - 1) n1 = m;
+    if (r == own_j) n2b = m - n1;
+  }
+  if (nr1 == 0) n1 = 0;
   L.meta[s] = m <= KC ? make_int4(n1, n2b, m - n1 - n2b, 0) : make_int4(-1, 0, 0, 0);
   if (m > KC) atomicAdd(&cnt->list_overflow, 1);
+}
+
+// AB predictor (src/MDEM.f90:297-331) as a streaming pass over particles in
+// index order: Predicted = x(t) + AB0*v + sum_k AB(k)*Previous(ipc(k)), PBC
+// wrap, then (v, a, alpha)(t) into the spare ring slot (the slot the
+// reference's cshift makes ipc(1)).
+__global__ void __launch_bounds__(256) k_predict(const DevParams* __restrict__ Pp, int n,
+                                                 StateArrays Q, StateArrays R,
+                                                 double* __restrict__ ring, RingMap rm,
+                                                 const Counters* __restrict__ cnt) {
+  if (cnt->abort) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const DevParams& P = *Pp;
+  const size_t N = (size_t)n;
+  const double x[3] = {Q.px[i], Q.py[i], Q.pz[i]};
+  const double v[3] = {Q.vx[i], Q.vy[i], Q.vz[i]};
+  const double w[3] = {Q.wx[i], Q.wy[i], Q.wz[i]};
+  const double a[3] = {Q.ax[i], Q.ay[i], Q.az[i]};
+  const double l[3] = {Q.lx[i], Q.ly[i], Q.lz[i]};
+  double sv[3] = {0.0, 0.0, 0.0}, sa[3] = {0.0, 0.0, 0.0}, sl[3] = {0.0, 0.0, 0.0};
+  for (int k = 0; k < P.nprev; k++) {
+    const double ABk = P.ab[k];
+    const double* rg = ring + (size_t)rm.phys[k] * 9 * N + i;
+#pragma unroll
+    for (int d = 0; d < 3; d++) sv[d] = sv[d] + ABk * rg[d * N];
+#pragma unroll
+    for (int d = 0; d < 3; d++) sa[d] = sa[d] + ABk * rg[(3 + d) * N];
+#pragma unroll
+    for (int d = 0; d < 3; d++) sl[d] = sl[d] + ABk * rg[(6 + d) * N];
+  }
+  double xr[3], vr[3], wr[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) xr[d] = x[d] + P.ab0 * v[d] + sv[d];
+#pragma unroll
+  for (int d = 0; d < 3; d++) vr[d] = v[d] + P.ab0 * a[d] + sa[d];
+#pragma unroll
+  for (int d = 0; d < 3; d++) wr[d] = w[d] + P.ab0 * l[d] + sl[d];
+#pragma unroll
+  for (int d = 0; d < 3; d++)
+    if (P.pbc[d]) xr[d] = xr[d] - P.lbox[d] * fnint(xr[d] * P.inv_lbox[d]);
+  R.px[i] = xr[0]; R.py[i] = xr[1]; R.pz[i] = xr[2];
+  R.vx[i] = vr[0]; R.vy[i] = vr[1]; R.vz[i] = vr[2];
+  R.wx[i] = wr[0]; R.wy[i] = wr[1]; R.wz[i] = wr[2];
+  if (P.nprev > 0) {
+    double* rg = ring + (size_t)rm.phys[P.nprev] * 9 * N + i;
+#pragma unroll
+    for (int d = 0; d < 3; d++) rg[d * N] = v[d];
+#pragma unroll
+    for (int d = 0; d < 3; d++) rg[(3 + d) * N] = a[d];
+#pragma unroll
+    for (int d = 0; d < 3; d++) rg[(6 + d) * N] = l[d];
+  }
+}
+
+// AM corrector (src/MDEM.f90:340-367) as a streaming pass: x = x + AM0*v~ +
+// sum_k AM(k)*Previous(ipc(k)) (ipc after the shift), likewise v and omega,
+// PBC wrap; counts the particles that left the box (src/MDEM.f90:624-625).
+__global__ void __launch_bounds__(256) k_correct(const DevParams* __restrict__ Pp, int n,
+                                                 StateArrays Q, StateArrays R,
+                                                 const double* __restrict__ ring, RingMap rm,
+                                                 Counters* __restrict__ cnt) {
+  if (cnt->abort) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool out = false;
+  if (i < n) {
+    const DevParams& P = *Pp;
+    const size_t N = (size_t)n;
+    double sv[3] = {0.0, 0.0, 0.0}, sa[3] = {0.0, 0.0, 0.0}, sl[3] = {0.0, 0.0, 0.0};
+    for (int k = 0; k < P.nprev; k++) {
+      const double AMk = P.am[k];
+      const double* rg = ring + (size_t)rm.phys[k] * 9 * N + i;
+#pragma unroll
+      for (int d = 0; d < 3; d++) sv[d] = sv[d] + AMk * rg[d * N];
+#pragma unroll
+      for (int d = 0; d < 3; d++) sa[d] = sa[d] + AMk * rg[(3 + d) * N];
+#pragma unroll
+      for (int d = 0; d < 3; d++) sl[d] = sl[d] + AMk * rg[(6 + d) * N];
+    }
+    const double vp[3] = {R.vx[i], R.vy[i], R.vz[i]};
+    const double ap[3] = {R.ax[i], R.ay[i], R.az[i]};
+    const double lp[3] = {R.lx[i], R.ly[i], R.lz[i]};
+    double x[3] = {Q.px[i], Q.py[i], Q.pz[i]};
+    double v[3] = {Q.vx[i], Q.vy[i], Q.vz[i]};
+    double w[3] = {Q.wx[i], Q.wy[i], Q.wz[i]};
+#pragma unroll
+    for (int d = 0; d < 3; d++) x[d] = x[d] + P.am0 * vp[d] + sv[d];
+#pragma unroll
+    for (int d = 0; d < 3; d++) v[d] = v[d] + P.am0 * ap[d] + sa[d];
+#pragma unroll
+    for (int d = 0; d < 3; d++) w[d] = w[d] + P.am0 * lp[d] + sl[d];
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+      if (P.pbc[d]) x[d] = x[d] - P.lbox[d] * fnint(x[d] * P.inv_lbox[d]);
+    Q.px[i] = x[0]; Q.py[i] = x[1]; Q.pz[i] = x[2];
+    Q.vx[i] = v[0]; Q.vy[i] = v[1]; Q.vz[i] = v[2];
+    Q.wx[i] = w[0]; Q.wy[i] = w[1]; Q.wz[i] = w[2];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const double h = 0.5 * P.lbox[d];
+      out = out || (x[d] > h) || (x[d] < -h);
+    }
+  }
+  const unsigned long long e = warp_sum_u64(out ? 1ull : 0ull);
+  if ((threadIdx.x & 31) == 0 && e) atomicAdd(&cnt->escaped, e);
 }
 
 // ring store of MoveParticlesEuler (src/MDEM.f90:266-271): (v,a,alpha) -> slot

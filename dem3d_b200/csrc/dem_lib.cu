@@ -468,14 +468,21 @@ int validate_ready(dem_ctx* c) {
 
 // MoveParticles(step) (src/MDEM.f90:285-369)
 int move_particles_impl(dem_ctx* c, int step, bool check, int tag) {
+  const int n = c->n;
   RingMap rm = current_map(c);
-  int st = force_pass(c, c->P, c->P, true, c->params.time_step, EPI_PREDICT, rm, check, tag);
+  // force pass @ x(t) with history update; a(t), alpha(t) -> Particle
+  int st = force_pass(c, c->P, c->P, true, c->params.time_step, EPI_STORE, rm, check, tag);
   if (st) return st;
+  launch(c, "predict", k_predict, blocks_for(n, 256), 256, (const DevParams*)c->dp, n, c->P,
+         c->Pr, c->ring, rm, (const Counters*)c->cnt);
   rotate_ring(c);
   c->time = (double)step * c->params.time_step;
   rm = current_map(c);
-  st = force_pass(c, c->Pr, c->Pr, false, c->params.time_step, EPI_CORRECT, rm, false, tag);
+  // force pass @ prediction, history read only; a~, alpha~ -> Predicted
+  st = force_pass(c, c->Pr, c->Pr, false, c->params.time_step, EPI_STORE, rm, false, tag);
   if (st) return st;
+  launch(c, "correct", k_correct, blocks_for(n, 256), 256, (const DevParams*)c->dp, n, c->P,
+         c->Pr, (const double*)c->ring, rm, c->cnt);
   return DEM_OK;
 }
 
