@@ -106,26 +106,17 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def force_bytes_per_particle(z_pp, z_pw, nw, pass_kind, nprev=3):
+def force_bytes_per_particle(z_pp, z_pw, nw, update):
     """Algorithmic (compulsory) DRAM bytes of one force-kernel launch per
-    particle, FP64 layout.  z_pp: pair contacts per particle, z_pw: wall
-    contacts per particle.  Neighbour data is counted once (it is re-read
-    from L1/L2).  pass_kind: 'predict' (history update + AB predictor) or
-    'correct' (history read + AM corrector)."""
-    own = 32 + 32 + 16 + 4 + 4          # sorted pos+R, v+wx, wy+wz, orig, cell
-    rec = 4 + 48                        # partner key + (ft, vt)
-    hist_read = 4 + 0.5 * z_pp * rec + nw * 4 + z_pw * 48
-    b = own + hist_read
-    if pass_kind == "predict":
-        b += 4 + 0.5 * z_pp * rec + nw * 4 + z_pw * 48  # history write
-        b += 48                         # a, alpha -> Particle
-        b += nprev * 72 + 72            # ring read, ring store
-        b += 72                         # Predicted x, v, w
-    else:
-        b += 48                         # a, alpha -> Predicted
-        b += nprev * 72                 # ring read
-        b += 72 + 72                    # Particle x, v, w read + write
-    return b
+    particle (FP64 layout): own traversal copies (pos+R, v+wx, wy+wz, orig,
+    cell) and contact-list meta, the history records (each pair record read
+    once: Z/2 per particle) and, in the updating pass, the records written,
+    then a and alpha stored.  Neighbour data is counted once (it is re-read
+    from L1/L2).  z_pp: pair contacts per particle, z_pw: wall contacts."""
+    own = 32 + 32 + 16 + 4 + 4 + 16 + 4 * z_pp
+    rec = 4 + 48
+    hist = 4 + 0.5 * z_pp * rec + nw * 4 + z_pw * 48
+    return own + hist * (2 if update else 1) + 48
 
 
 def rebuild_bytes_per_particle():
@@ -314,6 +305,91 @@ def traffic_per_particle():
     return None
 
 
+def screen_bytes_per_particle(z_pp):
+    """k_screen: own position + cell, the staged neighbourhood (each position
+    read once from DRAM), the contact-list row and its meta."""
+    return 32 + 4 + 16 + 4 * z_pp
+
+
+def integrator_bytes_per_particle(kind, nprev=3):
+    """k_predict: x,v,w,a,alpha + ring read, Predicted + ring store written;
+    k_correct: x,v,w + v~,a~,alpha~ + ring read, x,v,w written."""
+    if kind == "predict":
+        return 120 + nprev * 72 + 72 + 72
+    return 72 + 72 + nprev * 72 + 72
+
+
+def step_bytes_per_particle(z_pp, nw=0, nprev=3):
+    """Compulsory bytes of one particle-update (two passes + AB + AM)."""
+    return (2 * rebuild_bytes_per_particle() + 2 * screen_bytes_per_particle(z_pp)
+            + force_bytes_per_particle(z_pp, 0.0, nw, True)
+            + force_bytes_per_particle(z_pp, 0.0, nw, False)
+            + integrator_bytes_per_particle("predict", nprev)
+            + integrator_bytes_per_particle("correct", nprev))
+
+
+def kernel_bytes(name, n, z_pp, nw):
+    """Bytes of one launch (the force kernels: mean of the two passes)."""
+    if name.startswith("force"):
+        return n * 0.5 * (force_bytes_per_particle(z_pp, 0.0, nw, True) +
+                          force_bytes_per_particle(z_pp, 0.0, nw, False))
+    if name == "screen":
+        return n * screen_bytes_per_particle(z_pp)
+    if name == "predict":
+        return n * integrator_bytes_per_particle("predict")
+    if name == "correct":
+        return n * integrator_bytes_per_particle("correct")
+    if name.startswith("gather"):
+        return n * 164
+    return None
+
+
+def measure(s, w, args, world, local, torch, dist):
+    """Warm-up, then the timed region (graph replay of K steps)."""
+    s.run(1, 3 + args.warmup)
+    first = 4 + args.warmup
+    last = first + args.steps - 1
+    if world > 1:
+        dist.barrier()
+    l0 = s.launch_count()
+    with ClockSampler(local) as clk:
+        # NVTX range "dem_timed": lets a profiler select exactly these launches
+        torch.cuda.nvtx.range_push("dem_timed")
+        ms = s.run_timed(first, last)
+        torch.cuda.nvtx.range_pop()
+    launches = s.launch_count() - l0
+    ms = reduce_max(ms, world)
+    return {"ms": ms, "launches": launches, "last": last, "clocks": clk.summary(),
+            "value": aggregate_rate(w.n, world, args.steps, ms)}
+
+
+def force_error(w_fp64, w_mixed, src):
+    """Per-step force error of the mixed path: one force pass from the same
+    state and contact history (taken from ``src``) in both precisions; the
+    error is normed by the largest |a| (net forces cancel in packings)."""
+    from dem3d_b200.system import DEMSystem
+    st = src.get_state()
+    c = src.get_contacts()
+    prev, ipc = src.get_integration()
+    acc = {}
+    for name, w in (("fp64", w_fp64), ("mixed", w_mixed)):
+        t = DEMSystem(w.params)
+        t.set_state(st["pos"], st["vel"], st["omega"], comp=w.comp, radius=w.radius,
+                    acc=st["acc"], alpha=st["alpha"])
+        t.set_integration(prev, ipc)
+        t.set_contacts(c["imin"], c["imax"], c["ft"], c["vt"], c["ip"], c["iw"], c["ftw"],
+                       c["vtw"])
+        t.initialize_cell_distribution()
+        t.compute_accelerations(update=True)
+        acc[name] = t.get_state()
+        t.close()
+    out = {}
+    for k in ("acc", "alpha"):
+        ref = acc["fp64"][k]
+        out[k] = float(np.abs(acc["mixed"][k] - ref).max() / max(np.abs(ref).max(), 1e-300))
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -337,44 +413,52 @@ def run_ours(args):
     def barrier_max(x):
         return reduce_max(x, world)
 
-    precision = args.precision
-    if precision == "auto":
-        precision = "fp64"
-        try:
-            from dem3d_b200 import configs
-            probe = configs.dense_packing_params(0.6, 10.0, precision=_abi.PREC_MIXED)
-            DEMSystem(probe).close()
-            precision = "mixed"
-        except Exception:
-            precision = "fp64"
+    # the metric compares the mixed path with the plain FP64 path: by default
+    # both are timed on the same workload, the headline value is the mixed one
+    precisions = [args.precision] if args.precision != "auto" else ["fp64", "mixed"]
+    headline = precisions[-1]
 
     t0 = time.perf_counter()
-    w = make_workload(args.workload, precision, rank)
+    base = make_workload(args.workload, "fp64", rank)
     t_gen = time.perf_counter() - t0
-    n = w.n
-    s = DEMSystem(w.params)
-    s.set_state(w.pos, w.vel, w.omega, radius=w.radius)
-    s.initialize_cell_distribution()
-    # start-up (MethodOrder-1 Euler steps) + warm-up ABM steps
-    s.run(1, 3 + args.warmup)
-    first = 4 + args.warmup
-    last = first + args.steps - 1
-    if world > 1:
-        dist.barrier()
-    l0 = s.launch_count()
-    with ClockSampler(local) as clk:
-        # NVTX range "dem_timed": lets a profiler select exactly these launches
-        torch.cuda.nvtx.range_push("dem_timed")
-        ms = s.run_timed(first, last)
-        torch.cuda.nvtx.range_pop()
-    launches = s.launch_count() - l0
-    ms = barrier_max(ms)
-    value = aggregate_rate(n, world, args.steps, ms)
+    n = base.n
+    works = {}
+    from dem3d_b200 import params as P
+    import copy
+    for prec in precisions:
+        w = copy.copy(base)
+        w.params = copy.deepcopy(base.params)
+        w.params.precision = P.PREC_MIXED if prec == "mixed" else P.PREC_FP64
+        works[prec] = w
+    res = {}
+    systems = {}
+    for prec in precisions:
+        w = works[prec]
+        s = DEMSystem(w.params)
+        s.set_state(w.pos, w.vel, w.omega, comp=w.comp, radius=w.radius)
+        s.initialize_cell_distribution()
+        res[prec] = measure(s, w, args, world, local, torch, dist)
+        systems[prec] = s
+    s = systems[headline]
+    w = works[headline]
+    ms = res[headline]["ms"]
+    value = res[headline]["value"]
+    launches = res[headline]["launches"]
+    last = res[headline]["last"]
+    clocks = res[headline]["clocks"]
 
-    # contacts per particle (last pass) for the byte model
+    ferr = None
+    if "fp64" in systems and "mixed" in systems:
+        ferr = force_error(works["fp64"], works["mixed"], systems["fp64"])
+    for prec, sy in systems.items():
+        if prec != headline:
+            sy.close()
+
+    # contacts per particle for the byte model
     ps = s.pass_stats()
     obs = s.observables()
     z_pp = 2.0 * obs["n_pair_contacts"] / n
+    nw = int(w.params.n_walls)
     # per-kernel timing (instrumented steps, not graph-replayed)
     s.reset_kernel_stats()
     s.set_profiling(True)
@@ -386,14 +470,9 @@ def run_ours(args):
     last += nprof
     total_prof = sum(v[1] for v in stats.values())
     dom = max(stats, key=lambda k: stats[k][1])
-    nw = int(w.params.n_walls)
-    if dom.startswith("force"):
-        b_launch = n * 0.5 * (force_bytes_per_particle(z_pp, 0.0, nw, "predict") +
-                             force_bytes_per_particle(z_pp, 0.0, nw, "correct"))
-    else:
-        b_launch = n * rebuild_bytes_per_particle() / 4
+    b_launch = kernel_bytes(dom, n, z_pp, nw)
     avg_ms = stats[dom][1] / stats[dom][0]
-    achieved = b_launch / (avg_ms / 1000.0) / 1e9
+    achieved = b_launch / (avg_ms / 1000.0) / 1e9 if b_launch else None
     peaks = {}
     pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pk):
@@ -403,11 +482,14 @@ def run_ours(args):
     traffic = None
     if tr and dom in tr.get("bytes_per_particle", {}):
         traffic = tr["bytes_per_particle"][dom] * n
+    step_b = step_bytes_per_particle(z_pp, nw)
+    step_gbs = step_b * n / (ms / args.steps / 1000.0) / 1e9
 
     # e2e: each step uploads Particle(1:n) from pinned host memory, advances
     # one MoveParticles through the C-ABI and downloads the state.
     e2e = None
     if not args.no_e2e:
+        import ctypes as C
         ke = max(3, min(args.steps, 20))
         host = {k: torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
                 for k in ("pos", "vel", "omega", "acc", "alpha")}
@@ -420,9 +502,8 @@ def run_ours(args):
         for k in range(ke):
             s.update_state(host["pos"], host["vel"], host["omega"], host["acc"], host["alpha"])
             s.move_particles(last + 1 + k)
-            s._call("get_state", *(host[x].ctypes.data_as(
-                __import__("ctypes").POINTER(__import__("ctypes").c_double))
-                for x in ("pos", "vel", "omega", "acc", "alpha")))
+            s._call("get_state", *(host[x].ctypes.data_as(C.POINTER(C.c_double))
+                                   for x in ("pos", "vel", "omega", "acc", "alpha")))
         e2e_ms = barrier_max(s.timer_stop())
         last += ke
         e2e = {"value": n * world * ke / (e2e_ms / 1000.0), "unit": UNIT,
@@ -432,24 +513,30 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         lib_path, flags = _oracle_variant()
-        v, k, dt = cpu_time_steps(w, max_steps=3, budget_s=25.0, lib_path=lib_path)
+        v, k, dt = cpu_time_steps(base, max_steps=3, budget_s=25.0, lib_path=lib_path)
         cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
                "sample": f"{k} MoveParticles steps of the same {n:,}-sphere system, oracle "
                          f"C port ({flags}), 1 thread, {dt:.1f}s"}
-    clocks = clk.summary()
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if precision == "fp64" else "f32+f64", "data": "synthetic",
-            "config": config_block(args.workload, w, world, precision),
+            "dtype": "f64" if headline == "fp64" else "f32+f64", "data": "synthetic",
+            "config": config_block(args.workload, w, world, headline),
             "gpu_launches": int(launches),
+            "precisions": {p: {"value": r["value"], "ms_per_step": r["ms"] / args.steps}
+                           for p, r in res.items()},
+            "mixed_over_fp64": (res["mixed"]["value"] / res["fp64"]["value"]
+                                if "mixed" in res and "fp64" in res else None),
+            "force_err_vs_fp64": ferr,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak,
+                         "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                          "traffic": traffic, "algorithmic_bytes_per_launch": b_launch,
                          "avg_launch_ms": avg_ms, "peak_source": "MEASURED_PEAKS.json hbm_gbs"
                          if "hbm_gbs" in peaks else "fallback 6650 GB/s",
+                         "step_bytes_per_particle_update": step_b,
+                         "step_achieved_gbs": step_gbs, "step_frac": step_gbs / peak,
                          "kernel_share": {k: round(v[1] / total_prof, 4)
                                           for k, v in sorted(stats.items(),
                                                              key=lambda kv: -kv[1][1])}},

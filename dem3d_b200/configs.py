@@ -91,6 +91,89 @@ def settling(n=2000, seed=1000, layer_side=10, dt=1e-4, e=0.8, mu=0.5, gravity=1
                     info={"lbox": (L, L, lz), "seed": seed})
 
 
+def bidisperse_settling(n=4_000_000, seed=1004, width=200.0, ratio=3.0, number_ratio=20,
+                        e=0.7, mu=0.5, dt=5e-5, gravity=1.0, headroom=20.0, method_order=4,
+                        euler_intervals=100, max_ncell=1 << 30, precision=P.PREC_FP64,
+                        sigma_v=0.1):
+    """Wide polydispersity: small (d = 1) and large (d = ``ratio``) spheres,
+    small:large = ``number_ratio``:1, settling under gravity in a
+    ``width`` x ``width`` box closed by a floor and four side walls (five
+    rectangles, no periodic axis).  Two components, as the reference models
+    discrete sizes.  Initial state: sites of a cubic lattice of spacing
+    1.02*``ratio`` filled bottom-up in seeded random order, each site holding
+    one large sphere or a 3x3x3 block of small ones (no overlaps)."""
+    rng = np.random.default_rng(seed)
+    d_l = ratio
+    a = 1.02 * d_l
+    m_side = int(width / a)                       # sites per row
+    n_large = max(1, int(round(n / (number_ratio + 1))))
+    n_small = n - n_large
+    blocks = (n_small + 26) // 27
+    sites = n_large + blocks
+    layers = (sites + m_side * m_side - 1) // (m_side * m_side)
+    lz = layers * a + headroom
+    kind = np.zeros(sites, dtype=np.int8)
+    kind[rng.permutation(sites)[:n_large]] = 1    # 1 = large
+    pos = []
+    comp = []
+    left_small = n_small
+    for k in range(sites):
+        iz, r = divmod(k, m_side * m_side)
+        iy, ix = divmod(r, m_side)
+        cx = -0.5 * width + (ix + 0.5) * a
+        cy = -0.5 * width + (iy + 0.5) * a
+        cz = -0.5 * lz + (iz + 0.5) * a
+        if kind[k] == 1:
+            pos.append((cx, cy, cz))
+            comp.append(1)
+        else:
+            for bz in (-1, 0, 1):
+                for by in (-1, 0, 1):
+                    for bx in (-1, 0, 1):
+                        if left_small == 0:
+                            break
+                        pos.append((cx + 1.01 * bx, cy + 1.01 * by, cz + 1.01 * bz))
+                        comp.append(0)
+                        left_small -= 1
+    pos = np.asarray(pos, dtype=np.float64)
+    comp = np.asarray(comp, dtype=np.int32)
+    nn = pos.shape[0]
+    order = cell_major_order_box(pos, (width, width, lz), d_l)
+    pos, comp = pos[order], comp[order]
+    vel = rng.normal(0.0, sigma_v, size=(nn, 3))
+    half = 0.5 * width
+    zc = 0.0
+    hz = 0.5 * lz
+    k_w, kt_w = 2.0 * KN, 2.0 * KT
+    walls = [
+        P.rectangle((0.0, 0.0, -hz), half + 1.0, half + 1.0, (1, 0, 0), (0, 1, 0), k_w, kt_w),
+        P.rectangle((-half, 0.0, zc), half + 1.0, hz, (0, 1, 0), (0, 0, 1), k_w, kt_w),
+        P.rectangle((half, 0.0, zc), half + 1.0, hz, (0, 1, 0), (0, 0, 1), k_w, kt_w),
+        P.rectangle((0.0, -half, zc), half + 1.0, hz, (1, 0, 0), (0, 0, 1), k_w, kt_w),
+        P.rectangle((0.0, half, zc), half + 1.0, hz, (1, 0, 0), (0, 0, 1), k_w, kt_w),
+    ]
+    comps = [P.Component(n_small, 1.0, DENSITY, 2.0 * KN, 2.0 * KT),
+             P.Component(n_large, d_l, DENSITY, 2.0 * KN, 2.0 * KT)]
+    E = np.full((2, 2), e)
+    M = np.full((2, 2), mu)
+    prm, _ = P.component_params(
+        comps, walls, E, E, M, np.full((2, 5), e), np.full((2, 5), e), np.full((2, 5), mu),
+        lbox=(width, width, lz), pbc=(False, False, False), gravity=(0.0, 0.0, -gravity),
+        time_step=dt, method_order=method_order, euler_intervals=euler_intervals,
+        max_ncell=max_ncell, precision=precision)
+    return Workload("bidisperse_settling", prm, pos, vel, np.zeros((nn, 3)), comp=comp,
+                    info={"lbox": (width, width, lz), "seed": seed, "n_large": n_large})
+
+
+def cell_major_order_box(pos, lbox, cutoff):
+    """cell_major_order for a rectangular box."""
+    L = np.asarray(lbox, dtype=np.float64)
+    nc = np.maximum(1, (L / cutoff).astype(np.int64))
+    i3 = np.clip(((pos + 0.5 * L) * (nc / L)).astype(np.int64), 0, nc - 1)
+    key = i3[:, 0] + nc[0] * (i3[:, 1] + nc[1] * i3[:, 2])
+    return np.argsort(key, kind="stable")
+
+
 def box_for_fraction(radius: np.ndarray, phi: float) -> float:
     vol = float(np.sum(4.0 / 3.0 * math.pi * radius ** 3))
     return (vol / phi) ** (1.0 / 3.0)

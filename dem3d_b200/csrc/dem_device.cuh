@@ -5,6 +5,7 @@
 // with -fmad=false so that no multiply-add is fused), which is what lets the
 // FP64 path match the CPU oracle bit for bit.
 #pragma once
+#include <climits>
 #include <cstdint>
 #include <cuda_runtime.h>
 

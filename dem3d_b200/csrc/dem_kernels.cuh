@@ -329,7 +329,7 @@ __device__ __forceinline__ void hist_write(const History& H, int owner, int r, i
 // SWEEP = false: particles whose contact-list row is valid; SWEEP = true:
 // the (rare) particles whose row overflowed, which sweep the cells here.
 template <bool PP, int EPI, bool SWEEP>
-__global__ void __launch_bounds__(128) k_force_fp64(ForceArgs A) {
+__global__ void __launch_bounds__(128, 4) k_force_fp64(ForceArgs A) {
   if (A.cnt->abort) return;
   if (SWEEP && A.cnt->list_overflow == 0) return;
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -659,18 +659,71 @@ __device__ __forceinline__ int range_code(int wx, int wy, int wz, bool p_is_j) {
   return (wx + 1) | ((wy + 1) << 2) | ((wz + 1) << 4) | (p_is_j ? 64 : 0);
 }
 
+// A CTA takes SCR_THREADS consecutive slots, i.e. a run of consecutive cells.
+// Every candidate of those slots lies in one of three contiguous cell ranges,
+// one per z-plane offset (-1, 0, +1): [first cell - 1 - Nx, last cell + 1 +
+// Nx] shifted by a plane.  Their positions are staged in shared memory with
+// coalesced loads; candidates in cells reached by a y/z wrap (or past the
+// staging capacity) are read from global memory.
+constexpr int SCR_THREADS = 256;
+constexpr int SCR_CAP = 2048;  // staged particles per CTA
+
 template <bool PP>
-__global__ void __launch_bounds__(256, 4) k_screen(const DevParams* __restrict__ Pp, int n,
-                                                   const double4* __restrict__ pos,
-                                                   const int* __restrict__ comp,
-                                                   const int* __restrict__ slot_cell,
-                                                   const int* __restrict__ cs, ContactLists L,
-                                                   Counters* __restrict__ cnt) {
+constexpr int screen_smem_bytes() {
+  return SCR_CAP * (int)sizeof(double4) + (PP ? 0 : SCR_CAP * (int)sizeof(int));
+}
+
+template <bool PP>
+__global__ void __launch_bounds__(SCR_THREADS, 3) k_screen(const DevParams* __restrict__ Pp,
+                                                           int n, const double4* __restrict__ pos,
+                                                           const int* __restrict__ comp,
+                                                           const int* __restrict__ slot_cell,
+                                                           const int* __restrict__ cs,
+                                                           ContactLists L,
+                                                           Counters* __restrict__ cnt) {
+  extern __shared__ __align__(16) unsigned char scr_smem[];
+  double4* sp = reinterpret_cast<double4*>(scr_smem);
+  int* sc = reinterpret_cast<int*>(sp + SCR_CAP);
+  __shared__ int band_b[3], band_e[3], band_off[3];
   if (cnt->abort) return;
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
   const DevParams& P = *Pp;
   const int nx = P.nx, ny = P.ny;
+  const int s0 = blockIdx.x * SCR_THREADS;
+  if (threadIdx.x == 0) {
+    const int clo = slot_cell[s0];
+    const int chi = slot_cell[min(s0 + SCR_THREADS, n) - 1];
+    const long long plane = (long long)nx * ny;
+    int off = 0;
+    for (int b = 0; b < 3; b++) {
+      long long lo = (long long)clo - 1 - nx + (b - 1) * plane;
+      long long hi = (long long)chi + 1 + nx + (b - 1) * plane;
+      lo = lo < 0 ? 0 : lo;
+      hi = hi > P.ncell - 1 ? P.ncell - 1 : hi;
+      band_off[b] = -1;
+      band_b[b] = band_e[b] = 0;
+      if (lo > hi) continue;
+      const int sb = cs[lo], se = cs[hi + 1];
+      band_b[b] = sb;
+      band_e[b] = se;
+      if (off + (se - sb) <= SCR_CAP) {
+        band_off[b] = off;
+        off += se - sb;
+      }
+    }
+  }
+  __syncthreads();
+  for (int b = 0; b < 3; b++) {
+    const int o = band_off[b];
+    if (o < 0) continue;
+    const int sb = band_b[b], cnt_b = band_e[b] - sb;
+    for (int i = threadIdx.x; i < cnt_b; i += SCR_THREADS) {
+      sp[o + i] = pos[sb + i];
+      if (!PP) sc[o + i] = comp[sb + i];
+    }
+  }
+  __syncthreads();
+  const int s = s0 + threadIdx.x;
+  if (s >= n) return;
   const int c = slot_cell[s];
   const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
 
@@ -701,8 +754,13 @@ __global__ void __launch_bounds__(256, 4) k_screen(const DevParams* __restrict__
     const int nxi = sg * -(((rr.code) & 3) - 1);
     const int nyi = sg * -(((rr.code >> 2) & 3) - 1);
     const int nzi = sg * -(((rr.code >> 4) & 3) - 1);
+    // staged band holding this cell's slot range, if any
+    int base = INT_MIN;
+#pragma unroll
+    for (int b = 0; b < 3; b++)
+      if (band_off[b] >= 0 && band_b[b] <= rr.b && rr.e <= band_e[b]) base = band_off[b] - band_b[b];
     for (int t = rr.b; t < rr.e; t++) {
-      const double4 q4 = pos[t];
+      const double4 q4 = base != INT_MIN ? sp[t + base] : pos[t];
       double Rij[3];
       Rij[0] = pj ? p4.x - q4.x : q4.x - p4.x;
       Rij[0] = min_image(Rij[0], P.pbc[0], P.lbox[0], P.inv_lbox[0], nxi);
@@ -714,7 +772,7 @@ __global__ void __launch_bounds__(256, 4) k_screen(const DevParams* __restrict__
       Rij[2] = pj ? p4.z - q4.z : q4.z - p4.z;
       Rij[2] = min_image(Rij[2], P.pbc[2], P.lbox[2], P.inv_lbox[2], nzi);
       const double DijSq = sumsq3(Rij);
-      const int cq = PP ? 0 : comp[t];
+      const int cq = PP ? 0 : (base != INT_MIN ? sc[t + base] : comp[t]);
       const double Delta = pj ? Material<PP>::min_dij_sq(P, cq, q4.w, cp, p4.w) - DijSq
                               : Material<PP>::min_dij_sq(P, cp, p4.w, cq, q4.w) - DijSq;
       if (Delta > 0.0) {

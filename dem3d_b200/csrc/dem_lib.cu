@@ -150,6 +150,31 @@ void launch(dem_ctx* c, const char* name, void (*kernel)(KArgs...), unsigned gri
   c->launches++;
 }
 
+// launch with dynamic shared memory (opt-in raised once per kernel)
+template <typename... KArgs, typename... Args>
+void launch_sm(dem_ctx* c, const char* name, void (*kernel)(KArgs...), unsigned grid,
+               unsigned block, int smem, Args... args) {
+  if (grid == 0) return;
+  static thread_local std::vector<const void*> raised;
+  if (std::find(raised.begin(), raised.end(), (const void*)kernel) == raised.end()) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    raised.push_back((const void*)kernel);
+  }
+  if (c->prof) {
+    PendingEvent pe;
+    pe.stat = stat_index(c, name);
+    pe.e0 = get_event(c);
+    pe.e1 = get_event(c);
+    cudaEventRecord(pe.e0, c->stream);
+    kernel<<<grid, block, smem, c->stream>>>(args...);
+    cudaEventRecord(pe.e1, c->stream);
+    c->pending.push_back(pe);
+  } else {
+    kernel<<<grid, block, smem, c->stream>>>(args...);
+  }
+  c->launches++;
+}
+
 // run fn (which launches exactly one kernel on the context stream) with the
 // same event timing as launch()
 template <class Fn>
@@ -428,13 +453,15 @@ int force_pass(dem_ctx* c, const StateArrays& src, const StateArrays& tgt, bool 
   if (st) return st;
   if (c->n > 0) {
     if (c->pp)
-      launch(c, "screen", k_screen<true>, blocks_for(c->n, 256), 256, (const DevParams*)c->dp,
-             c->n, (const double4*)c->S.pos, (const int*)c->S.comp, (const int*)c->S.cell,
-             (const int*)c->cell_start, c->CL, c->cnt);
+      launch_sm(c, "screen", k_screen<true>, blocks_for(c->n, SCR_THREADS), SCR_THREADS,
+                screen_smem_bytes<true>(), (const DevParams*)c->dp, c->n,
+                (const double4*)c->S.pos, (const int*)c->S.comp, (const int*)c->S.cell,
+                (const int*)c->cell_start, c->CL, c->cnt);
     else
-      launch(c, "screen", k_screen<false>, blocks_for(c->n, 256), 256, (const DevParams*)c->dp,
-             c->n, (const double4*)c->S.pos, (const int*)c->S.comp, (const int*)c->S.cell,
-             (const int*)c->cell_start, c->CL, c->cnt);
+      launch_sm(c, "screen", k_screen<false>, blocks_for(c->n, SCR_THREADS), SCR_THREADS,
+                screen_smem_bytes<false>(), (const DevParams*)c->dp, c->n,
+                (const double4*)c->S.pos, (const int*)c->S.comp, (const int*)c->S.cell,
+                (const int*)c->cell_start, c->CL, c->cnt);
   }
   for (int attempt = 0;; attempt++) {
     st = launch_force(c, tgt, update, dt, epi, rm, tag);

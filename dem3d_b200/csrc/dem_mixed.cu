@@ -238,7 +238,7 @@ __device__ __forceinline__ unsigned long long wsum(unsigned long long v) {
 }
 
 template <bool PP, int EPI, bool SWEEP>
-__global__ void __launch_bounds__(128) k_force_mixed(ForceArgs A, MixedView V) {
+__global__ void __launch_bounds__(128, 4) k_force_mixed(ForceArgs A, MixedView V) {
   if (A.cnt->abort) return;
   if (SWEEP && A.cnt->list_overflow == 0) return;
   const int s = blockIdx.x * blockDim.x + threadIdx.x;

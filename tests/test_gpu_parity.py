@@ -201,3 +201,17 @@ def test_large_dense_one_step_bit_exact():
         s.compute_accelerations(update=True)
     assert_same_state(g, o, "200k pass")
     assert_same_contacts(g, o, "200k pass")
+
+
+def test_bidisperse_walls_bit_exact():
+    """Two components (d = 1 and 3) in a box closed by a floor and four side
+    walls: component tables, rectangle faces/edges/corners, no periodic axis."""
+    w = configs.bidisperse_settling(n=3000, width=24.0, headroom=6.0, sigma_v=0.5)
+    g, o = make_pair(w)
+    for s in (g, o):
+        s.run(1, 400)
+    assert o.count_contacts()[1] > 0
+    assert_same_state(g, o, "bidisperse")
+    assert_same_contacts(g, o, "bidisperse")
+    assert_same_cells(g, o, "bidisperse")
+    assert g.ncol() == o.ncol()
