@@ -27,6 +27,8 @@ struct DevParams {
   double nxbylx, nybyly, nzbylz, nxby2, nyby2, nzby2;
   double ab0, am0, ab[3], am[3];
   double max_min_dij_sq;  // largest MinDijSq of any pair (screening early-out)
+  double vl_skin;         // candidate-list skin (added to MinDij)
+  double vl_thr2;         // (skin/4)^2: displacement that forces a full rebuild
   double comp_radius[NCM], comp_inv_mass[NCM], comp_inv_inertia[NCM], comp_eff_mass[NCM];
   double min_dij[NCM * NCM], min_dij_sq[NCM * NCM];
   double kn[NCM * NCM], yn[NCM * NCM], kt[NCM * NCM], yt[NCM * NCM], mu_sq[NCM * NCM];
@@ -55,7 +57,9 @@ struct Counters {
   int abort;         // nonzero: later kernels of a captured sequence do nothing
   int abort_tag;     // 1 + index (within a captured chunk) of the failing step
   int list_overflow; // particles of this pass whose contact-list row overflowed
-  int pad_;
+  int force_rebuild; // rebuild every candidate list in the next pass
+  unsigned long long max_disp2;  // bits of the largest squared displacement since
+                                 // the last full candidate-list rebuild
   double wall_fn[NWM];
 };
 
@@ -87,15 +91,27 @@ struct RingMap {
   int phys[5];  // phys[k] = physical slot of logical ipc(k+1); phys[nprev] = spare
 };
 
-// Contact lists emitted by the screening kernel, one row of KC slots per
-// particle: first the "p is i" partners in the order of p's neighbour list,
-// then the "p is j" partners in sweep order.  meta = (n1, n2 before p's own
-// block, n2 after it, 0); n1 = -1 when the row overflowed (the force kernel
-// then sweeps the cells itself for that particle).
+// Candidate lists, one row of KC entries per particle (indexed by original
+// index): the particles within MinDij + skin, as original indices, first the
+// "p is i" partners in the order of p's neighbour list, then the "p is j"
+// partners in sweep order.  meta = (n1, n2 before p's own block, n2 after
+// it, 0); n1 = -1 when the row overflowed or was never built (the force
+// kernel then sweeps the cells itself for that particle).  A row stays valid
+// while no cell of its 27-cell neighbourhood gains or loses a particle (the
+// relative order of the others in the cell lists is unchanged) and no
+// particle has moved skin/4 since the last full rebuild.
 constexpr int KC = 32;
 struct ContactLists {
-  int* slot;   // [n*KC]
-  int4* meta;  // [n]
+  int* slot;          // [n*KC] candidate original indices
+  int4* meta;         // [n]
+  int* slot_of_orig;  // [n] traversal slot of every particle (this pass)
+  double4* ref_pos;   // [n] positions at the last full rebuild
+  unsigned char* dirty;   // [ncell] a particle entered/left the cell this pass
+  unsigned char* repair;  // [ncell] rows of this cell's particles are rebuilt
+  // this pass's exact contacts, filtered from the candidates: rows indexed by
+  // traversal slot holding traversal slots, same order and meta layout
+  int* xslot;   // [n*KC]
+  int4* xmeta;  // [n]
 };
 
 struct ForceArgs {
@@ -106,6 +122,7 @@ struct ForceArgs {
   const int* cell_of_orig;
   const int* cl_slot;
   const int4* cl_meta;
+  const int* slot_of_orig;
   History Hr, Hw;
   int update;
   double half_dt;
@@ -596,9 +613,25 @@ __device__ __forceinline__ double min_image(double r, int pbc, double L, double 
 
 // Loop 1 / loop 2 driven by the screening kernel's contact list when the
 // particle's row did not overflow, else by the full sweep (same order).
+// Full candidate-list rebuild due in this pass: requested by the host (new
+// state or cells) or some particle moved more than skin/4 since the last one.
+__device__ __forceinline__ bool rebuild_due(const DevParams& P, const Counters* cnt) {
+  return cnt->force_rebuild != 0 ||
+         __longlong_as_double((long long)cnt->max_disp2) > P.vl_thr2;
+}
+
+// Called by one thread of the force kernel (after the screening kernel has
+// read the trigger): the rebuild of this pass is done.
+__device__ __forceinline__ void clear_rebuild_trigger(const ForceArgs& A) {
+  if (rebuild_due(*A.P, A.cnt)) {
+    A.cnt->force_rebuild = 0;
+    A.cnt->max_disp2 = 0ull;
+  }
+}
+
 template <bool SWEEP, class Visit>
-__device__ __forceinline__ void walk_as_i(const ForceArgs& A, int4 meta, int s, int c, int cx,
-                                          int cy, int cz, Visit&& visit) {
+__device__ __forceinline__ void walk_as_i(const ForceArgs& A, int4 meta, int s, int orig, int c,
+                                          int cx, int cy, int cz, Visit&& visit) {
   if (!SWEEP) {
     const int* l = A.cl_slot + (size_t)s * KC;
     for (int k = 0; k < meta.x; k++) visit(l[k]);
@@ -608,8 +641,8 @@ __device__ __forceinline__ void walk_as_i(const ForceArgs& A, int4 meta, int s, 
 }
 
 template <bool SWEEP, class Visit, class Own>
-__device__ __forceinline__ void walk_as_j(const ForceArgs& A, int4 meta, int s, int c, int cx,
-                                          int cy, int cz, Visit&& visit, Own&& own) {
+__device__ __forceinline__ void walk_as_j(const ForceArgs& A, int4 meta, int s, int orig, int c,
+                                          int cx, int cy, int cz, Visit&& visit, Own&& own) {
   if (!SWEEP) {
     const int* l = A.cl_slot + (size_t)s * KC + meta.x;
     for (int k = 0; k < meta.y; k++) visit(l[k]);

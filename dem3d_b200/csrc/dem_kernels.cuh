@@ -68,6 +68,57 @@ __global__ void k_assign(const DevParams* __restrict__ Pp, int n, int initial,
   if ((threadIdx.x & 31) == 0 && mv) atomicAdd(&cnt->movers, mv);
 }
 
+// k_assign for the context path: also marks the old and new cell of every
+// particle that changed cell (their neighbourhoods' candidate rows are
+// rebuilt) and tracks the largest squared displacement since the last full
+// candidate-list rebuild.
+__global__ void k_assign_track(const DevParams* __restrict__ Pp, int n,
+                               const double* __restrict__ px, const double* __restrict__ py,
+                               const double* __restrict__ pz, const int* __restrict__ order,
+                               const int* __restrict__ old_cell, int* __restrict__ cell_cnt,
+                               int* __restrict__ a_cell, int* __restrict__ a_loc,
+                               unsigned* __restrict__ a_key, int* __restrict__ a_orig,
+                               ContactLists L, Counters* __restrict__ cnt) {
+  if (cnt->abort) return;
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s == 0 && cnt->ncol_pending) {
+    cnt->ncol += cnt->ncol_pending;
+    cnt->ncol_pending = 0;
+  }
+  unsigned long long mv = 0;
+  double d2 = 0.0;
+  if (s < n) {
+    const DevParams& P = *Pp;
+    const int orig = order[s];
+    const double x = px[orig], y = py[orig], z = pz[orig];
+    const int c = current_cell(P, x, y, z);
+    const int old = old_cell[s];
+    const bool mover = c != old;
+    const unsigned key = mover ? (unsigned)(n - 1 - orig) : (unsigned)(n + s);
+    const int loc = atomicAdd(&cell_cnt[c], 1);
+    a_cell[s] = c;
+    a_loc[s] = loc;
+    a_key[s] = key;
+    a_orig[s] = orig;
+    if (mover) {
+      L.dirty[c] = 1;
+      L.dirty[old] = 1;
+      mv = 1ull;
+    }
+    const double4 r = L.ref_pos[orig];
+    const double dx = x - r.x, dy = y - r.y, dz = z - r.z;
+    d2 = dx * dx + dy * dy + dz * dz;
+    if (!(d2 <= 1e300)) d2 = 1e300;  // NaN-safe: any invalid state forces a rebuild
+  }
+  mv = warp_sum_u64(mv);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) d2 = fmax(d2, __shfl_down_sync(0xffffffffu, d2, o));
+  if ((threadIdx.x & 31) == 0) {
+    if (mv) atomicAdd(&cnt->movers, mv);
+    if (d2 > 0.0) atomicMax(&cnt->max_disp2, (unsigned long long)__double_as_longlong(d2));
+  }
+}
+
 // exclusive scan, phase 1: tiles of 4*blockDim elements
 constexpr int SCAN_THREADS = 1024;
 constexpr int SCAN_ITEMS = 4;
@@ -329,13 +380,14 @@ __device__ __forceinline__ void hist_write(const History& H, int owner, int r, i
 // SWEEP = false: particles whose contact-list row is valid; SWEEP = true:
 // the (rare) particles whose row overflowed, which sweep the cells here.
 template <bool PP, int EPI, bool SWEEP>
-__global__ void __launch_bounds__(128, 4) k_force_fp64(ForceArgs A) {
+__global__ void __launch_bounds__(128, SWEEP ? 1 : 4) k_force_fp64(ForceArgs A) {
   if (A.cnt->abort) return;
   if (SWEEP && A.cnt->list_overflow == 0) return;
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long n_col = 0, n_pc = 0, n_wc = 0;
   int need = 0;
   const int4 meta = s < A.n ? A.cl_meta[s] : make_int4(0, 0, 0, 0);
+  if (!SWEEP && s == 0) clear_rebuild_trigger(A);
   if (s < A.n && (meta.x < 0) == SWEEP) {
     const DevParams& P = *A.P;
     const SortedArrays& S = A.S;
@@ -412,7 +464,7 @@ __global__ void __launch_bounds__(128, 4) k_force_fp64(ForceArgs A) {
 
     // ---- loop 1: own cell after p, then the half-shell cells in the order
     // of the FirstNeighbour list (reverse of AddAllNeighbours3D insertion)
-    walk_as_i<SWEEP>(A, meta, s, c, cx, cy, cz, visit_i);
+    walk_as_i<SWEEP>(A, meta, s, orig, c, cx, cy, cz, visit_i);
 
     // ---- walls (src/MForces.f90:274-314)
     for (int w = 0; w < P.nw; w++) {
@@ -507,7 +559,7 @@ __global__ void __launch_bounds__(128, 4) k_force_fp64(ForceArgs A) {
         if (update && orig < qo) record(qo, o.FT, o.VT);
       }
     };
-    walk_as_j<SWEEP>(A, meta, s, c, cx, cy, cz, visit_j, [&]() {
+    walk_as_j<SWEEP>(A, meta, s, orig, c, cx, cy, cz, visit_j, [&]() {
 #pragma unroll
       for (int k = 0; k < 3; k++) F[k] = F[k] + iF[k];
 #pragma unroll
@@ -643,14 +695,14 @@ __global__ void __launch_bounds__(128, 4) k_force_fp64(ForceArgs A) {
 // ---------------------------------------------------------------------------
 // small per-particle kernels (original index order)
 
-// K2 screening: the overlap test DeltaDijSq = MinDijSq - DijSq > 0
-// (src/MForces.f90:209-224) for every candidate of the sweep, in FP64 with the
-// same operations as the force kernels, compacted into the particle's
-// contact-list row in sweep order.  The cells of both sweeps are first
-// gathered as up to 29 slot ranges (range, image of the cell, role) and then
-// scanned by one loop with a single copy of the test: the kernel stays small
-// (instruction fetch) and register-light (many warps hide the candidate-load
-// latency).  The heavy contact arithmetic then runs only over real contacts.
+// K2 screening: candidate lists.  For every particle whose row must be
+// (re)built -- all particles on a full rebuild, else those whose 27-cell
+// neighbourhood gained or lost a particle in this pass, and rows that
+// overflowed -- sweep the cells exactly as ComputeAccelerations does
+// (src/MForces.f90:173-272) and keep, in sweep order, the particles within
+// MinDij + skin.  The force kernels apply the exact FP64 overlap test to these
+// candidates, so contact sets, orientation and order stay the reference's.
+// Every thread also publishes its particle's slot for the orig -> slot map.
 struct ScreenRange {
   int b, e, code;  // code: bit 0..5 image (2 bits per axis, biased by 1), bit 6: p is "j"
 };
@@ -659,74 +711,26 @@ __device__ __forceinline__ int range_code(int wx, int wy, int wz, bool p_is_j) {
   return (wx + 1) | ((wy + 1) << 2) | ((wz + 1) << 4) | (p_is_j ? 64 : 0);
 }
 
-// A CTA takes SCR_THREADS consecutive slots, i.e. a run of consecutive cells.
-// Every candidate of those slots lies in one of three contiguous cell ranges,
-// one per z-plane offset (-1, 0, +1): [first cell - 1 - Nx, last cell + 1 +
-// Nx] shifted by a plane.  Their positions are staged in shared memory with
-// coalesced loads; candidates in cells reached by a y/z wrap (or past the
-// staging capacity) are read from global memory.
-constexpr int SCR_THREADS = 256;
-constexpr int SCR_CAP = 2048;  // staged particles per CTA
-
 template <bool PP>
-constexpr int screen_smem_bytes() {
-  return SCR_CAP * (int)sizeof(double4) + (PP ? 0 : SCR_CAP * (int)sizeof(int));
-}
-
-template <bool PP>
-__global__ void __launch_bounds__(SCR_THREADS, 3) k_screen(const DevParams* __restrict__ Pp,
-                                                           int n, const double4* __restrict__ pos,
-                                                           const int* __restrict__ comp,
-                                                           const int* __restrict__ slot_cell,
-                                                           const int* __restrict__ cs,
-                                                           ContactLists L,
-                                                           Counters* __restrict__ cnt) {
-  extern __shared__ __align__(16) unsigned char scr_smem[];
-  double4* sp = reinterpret_cast<double4*>(scr_smem);
-  int* sc = reinterpret_cast<int*>(sp + SCR_CAP);
-  __shared__ int band_b[3], band_e[3], band_off[3];
+__global__ void __launch_bounds__(256, 4) k_screen(const DevParams* __restrict__ Pp, int n,
+                                                   const double4* __restrict__ pos,
+                                                   const int* __restrict__ comp,
+                                                   const int* __restrict__ slot_cell,
+                                                   const int* __restrict__ order,
+                                                   const int* __restrict__ cs, ContactLists L,
+                                                   Counters* __restrict__ cnt) {
   if (cnt->abort) return;
-  const DevParams& P = *Pp;
-  const int nx = P.nx, ny = P.ny;
-  const int s0 = blockIdx.x * SCR_THREADS;
-  if (threadIdx.x == 0) {
-    const int clo = slot_cell[s0];
-    const int chi = slot_cell[min(s0 + SCR_THREADS, n) - 1];
-    const long long plane = (long long)nx * ny;
-    int off = 0;
-    for (int b = 0; b < 3; b++) {
-      long long lo = (long long)clo - 1 - nx + (b - 1) * plane;
-      long long hi = (long long)chi + 1 + nx + (b - 1) * plane;
-      lo = lo < 0 ? 0 : lo;
-      hi = hi > P.ncell - 1 ? P.ncell - 1 : hi;
-      band_off[b] = -1;
-      band_b[b] = band_e[b] = 0;
-      if (lo > hi) continue;
-      const int sb = cs[lo], se = cs[hi + 1];
-      band_b[b] = sb;
-      band_e[b] = se;
-      if (off + (se - sb) <= SCR_CAP) {
-        band_off[b] = off;
-        off += se - sb;
-      }
-    }
-  }
-  __syncthreads();
-  for (int b = 0; b < 3; b++) {
-    const int o = band_off[b];
-    if (o < 0) continue;
-    const int sb = band_b[b], cnt_b = band_e[b] - sb;
-    for (int i = threadIdx.x; i < cnt_b; i += SCR_THREADS) {
-      sp[o + i] = pos[sb + i];
-      if (!PP) sc[o + i] = comp[sb + i];
-    }
-  }
-  __syncthreads();
-  const int s = s0 + threadIdx.x;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
+  const DevParams& P = *Pp;
+  const int orig = order[s];
+  L.slot_of_orig[orig] = s;
   const int c = slot_cell[s];
-  const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
+  const bool full = rebuild_due(P, cnt);
+  if (!full && !L.repair[c] && L.meta[orig].x >= 0) return;
 
+  const int nx = P.nx, ny = P.ny;
+  const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
   // ---- the ranges, in sweep order: loop 1, then loop 2
   ScreenRange R[29];
   int nr = 0, own_j = -1;
@@ -743,9 +747,12 @@ __global__ void __launch_bounds__(SCR_THREADS, 3) k_screen(const DevParams* __re
 
   // ---- one loop over all candidates
   const double4 p4 = pos[s];
+  if (full) L.ref_pos[orig] = p4;
   const int cp = PP ? 0 : comp[s];
-  const double maxsq = P.max_min_dij_sq;
-  int* out = L.slot + (size_t)s * KC;
+  const double skin = P.vl_skin;
+  const double maxd = sqrt(P.max_min_dij_sq) + skin;
+  const double maxsq = maxd * maxd;
+  int* out = L.slot + (size_t)orig * KC;
   int m = 0, n1 = 0, n2b = 0;
   for (int r = 0; r < nr; r++) {
     const ScreenRange rr = R[r];
@@ -754,38 +761,103 @@ __global__ void __launch_bounds__(SCR_THREADS, 3) k_screen(const DevParams* __re
     const int nxi = sg * -(((rr.code) & 3) - 1);
     const int nyi = sg * -(((rr.code >> 2) & 3) - 1);
     const int nzi = sg * -(((rr.code >> 4) & 3) - 1);
-    // staged band holding this cell's slot range, if any
-    int base = INT_MIN;
-#pragma unroll
-    for (int b = 0; b < 3; b++)
-      if (band_off[b] >= 0 && band_b[b] <= rr.b && rr.e <= band_e[b]) base = band_off[b] - band_b[b];
     for (int t = rr.b; t < rr.e; t++) {
-      const double4 q4 = base != INT_MIN ? sp[t + base] : pos[t];
+      const double4 q4 = pos[t];
       double Rij[3];
       Rij[0] = pj ? p4.x - q4.x : q4.x - p4.x;
       Rij[0] = min_image(Rij[0], P.pbc[0], P.lbox[0], P.inv_lbox[0], nxi);
-      // DijSq >= fl(Rij_x^2): sums of non-negative terms never round below a
-      // partial sum, so no overlap is possible past the largest MinDijSq
       if (Rij[0] * Rij[0] >= maxsq) continue;
       Rij[1] = pj ? p4.y - q4.y : q4.y - p4.y;
       Rij[1] = min_image(Rij[1], P.pbc[1], P.lbox[1], P.inv_lbox[1], nyi);
       Rij[2] = pj ? p4.z - q4.z : q4.z - p4.z;
       Rij[2] = min_image(Rij[2], P.pbc[2], P.lbox[2], P.inv_lbox[2], nzi);
       const double DijSq = sumsq3(Rij);
-      const int cq = PP ? 0 : (base != INT_MIN ? sc[t + base] : comp[t]);
-      const double Delta = pj ? Material<PP>::min_dij_sq(P, cq, q4.w, cp, p4.w) - DijSq
-                              : Material<PP>::min_dij_sq(P, cp, p4.w, cq, q4.w) - DijSq;
-      if (Delta > 0.0) {
-        if (m < KC) out[m] = t;
+      const int cq = PP ? 0 : comp[t];
+      // candidates: within MinDij + skin (a superset of the exact overlaps)
+      double md = PP ? p4.w + q4.w : sqrt(Material<PP>::min_dij_sq(P, cp, p4.w, cq, q4.w));
+      md = md + skin;
+      if (md * md - DijSq > 0.0) {
+        if (m < KC) out[m] = order[t];
         m++;
       }
     }
     if (r == nr1 - 1) n1 = m;
     if (r == own_j) n2b = m - n1;
   }
-  if (nr1 == 0) n1 = 0;
-  L.meta[s] = m <= KC ? make_int4(n1, n2b, m - n1 - n2b, 0) : make_int4(-1, 0, 0, 0);
+  L.meta[orig] = m <= KC ? make_int4(n1, n2b, m - n1 - n2b, 0) : make_int4(-1, 0, 0, 0);
   if (m > KC) atomicAdd(&cnt->list_overflow, 1);
+}
+
+// This pass's exact contact rows: the candidates of every particle that
+// pass the overlap test DeltaDijSq > 0 of the force kernels (same operations,
+// src/MForces.f90:209-224), in candidate order, as traversal slots.  A light
+// kernel, so that the heavy contact arithmetic only meets real contacts.
+template <bool PP>
+__global__ void __launch_bounds__(256) k_filter(const DevParams* __restrict__ Pp, int n,
+                                                const double4* __restrict__ pos,
+                                                const int* __restrict__ comp,
+                                                const int* __restrict__ order, ContactLists L,
+                                                const Counters* __restrict__ cnt) {
+  if (cnt->abort) return;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const DevParams& P = *Pp;
+  const int orig = order[s];
+  const int4 meta = L.meta[orig];
+  if (meta.x < 0) {
+    L.xmeta[s] = meta;  // overflowed row: the force kernel sweeps the cells
+    return;
+  }
+  const double4 p4 = pos[s];
+  const int cp = PP ? 0 : comp[s];
+  const int* in = L.slot + (size_t)orig * KC;
+  int* out = L.xslot + (size_t)s * KC;
+  const int total = meta.x + meta.y + meta.z;
+  int m = 0, n1 = 0, n2b = 0;
+  for (int k = 0; k < total; k++) {
+    const int t = L.slot_of_orig[in[k]];
+    const double4 q4 = pos[t];
+    const bool pj = k >= meta.x;  // loop 2: p is "j", Rij = xp - xq
+    double Rij[3] = {pj ? p4.x - q4.x : q4.x - p4.x, pj ? p4.y - q4.y : q4.y - p4.y,
+                     pj ? p4.z - q4.z : q4.z - p4.z};
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+      if (P.pbc[d]) Rij[d] = Rij[d] - P.lbox[d] * fnint(Rij[d] * P.inv_lbox[d]);
+    const double DijSq = sumsq3(Rij);
+    const int cq = PP ? 0 : comp[t];
+    const double Delta = pj ? Material<PP>::min_dij_sq(P, cq, q4.w, cp, p4.w) - DijSq
+                            : Material<PP>::min_dij_sq(P, cp, p4.w, cq, q4.w) - DijSq;
+    if (Delta > 0.0) out[m++] = t;
+    if (k == meta.x - 1) n1 = m;
+    if (k == meta.x + meta.y - 1) n2b = m - n1;
+  }
+  if (meta.x == 0) n1 = 0;
+  if (meta.y == 0) n2b = 0;
+  L.xmeta[s] = make_int4(n1, n2b, m - n1 - n2b, 0);
+}
+
+// A particle entered or left each dirty cell: the rows of every particle in
+// its 27-cell neighbourhood are rebuilt in this pass.
+__global__ void k_mark_repair(const DevParams* __restrict__ Pp, ContactLists L,
+                              const Counters* __restrict__ cnt) {
+  if (cnt->abort) return;
+  const DevParams& P = *Pp;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= P.ncell || !L.dirty[c]) return;
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
+  int xi, xf, yi, yf, zi, zf;
+  axis_range(cx, nx, P.pbc[0], xi, xf);
+  axis_range(cy, ny, P.pbc[1], yi, yf);
+  axis_range(cz, nz, P.pbc[2], zi, zf);
+  for (int kz = zi; kz <= zf; kz++)
+    for (int ky = yi; ky <= yf; ky++)
+      for (int kx = xi; kx <= xf; kx++) {
+        const int jx = axis_wrap(cx + kx, nx, P.pbc[0]);
+        const int jy = axis_wrap(cy + ky, ny, P.pbc[1]);
+        const int jz = axis_wrap(cz + kz, nz, P.pbc[2]);
+        L.repair[jx + nx * (jy + ny * jz)] = 1;
+      }
 }
 
 // AB predictor (src/MDEM.f90:297-331) as a streaming pass over particles in

@@ -232,6 +232,12 @@ void free_state(dem_ctx* c) {
   cudaFree(c->t_key);
   cudaFree(c->CL.slot);
   cudaFree(c->CL.meta);
+  cudaFree(c->CL.slot_of_orig);
+  cudaFree(c->CL.ref_pos);
+  cudaFree(c->CL.dirty);
+  cudaFree(c->CL.repair);
+  cudaFree(c->CL.xslot);
+  cudaFree(c->CL.xmeta);
   c->CL = ContactLists{};
   for (int b = 0; b < 2; b++) {
     cudaFree(c->H[b].cnt);
@@ -321,10 +327,18 @@ int rebuild_cells(dem_ctx* c, const StateArrays& src, bool initial) {
   const int ncell = c->hp.ncell;
   if (n == 0) return DEM_OK;
   CK(cudaMemsetAsync(c->cell_cnt, 0, sizeof(int) * (size_t)ncell, c->stream));
-  launch(c, "cell_assign", k_assign, blocks_for(n, 256), 256, (const DevParams*)c->dp, n,
-         initial ? 1 : 0, (const double*)src.px, (const double*)src.py, (const double*)src.pz,
-         (const int*)c->S.orig, (const int*)c->S.cell, c->cell_cnt, c->a_cell, c->a_loc, c->a_key,
-         c->a_orig, c->cnt);
+  if (initial) {
+    launch(c, "cell_assign", k_assign, blocks_for(n, 256), 256, (const DevParams*)c->dp, n, 1,
+           (const double*)src.px, (const double*)src.py, (const double*)src.pz,
+           (const int*)c->S.orig, (const int*)c->S.cell, c->cell_cnt, c->a_cell, c->a_loc,
+           c->a_key, c->a_orig, c->cnt);
+  } else {
+    CK(cudaMemsetAsync(c->CL.dirty, 0, (size_t)ncell, c->stream));
+    launch(c, "cell_assign", k_assign_track, blocks_for(n, 256), 256, (const DevParams*)c->dp, n,
+           (const double*)src.px, (const double*)src.py, (const double*)src.pz,
+           (const int*)c->S.orig, (const int*)c->S.cell, c->cell_cnt, c->a_cell, c->a_loc,
+           c->a_key, c->a_orig, c->CL, c->cnt);
+  }
   launch(c, "scan_tiles", k_scan_tiles, (unsigned)c->n_tiles, SCAN_THREADS,
          (const int*)c->cell_cnt, ncell, c->cell_start, c->scan_bsum, (const Counters*)c->cnt);
   launch(c, "scan_bsums", k_scan_bsums, 1u, SCAN_THREADS, c->scan_bsum, c->n_tiles, c->cell_start,
@@ -361,8 +375,9 @@ int launch_force(dem_ctx* c, const StateArrays& tgt, bool update, double dt, int
   A.S = c->S;
   A.cell_start = c->cell_start;
   A.cell_of_orig = c->cell_of_orig;
-  A.cl_slot = c->CL.slot;
-  A.cl_meta = c->CL.meta;
+  A.cl_slot = c->CL.xslot;
+  A.cl_meta = c->CL.xmeta;
+  A.slot_of_orig = c->CL.slot_of_orig;
   A.Hr = c->H[c->hcur];
   A.Hw = c->H[c->hcur ^ 1];
   A.update = update ? 1 : 0;
@@ -386,13 +401,9 @@ int launch_force(dem_ctx* c, const StateArrays& tgt, bool update, double dt, int
     launch(c, "force_fp64_sweep", k_force_fp64<PPV, E, true>, g, 128, A);   \
   }
   if (c->pp) {
-    if (epi == EPI_STORE) FORCE_CASE(true, EPI_STORE)
-    else if (epi == EPI_PREDICT) FORCE_CASE(true, EPI_PREDICT)
-    else FORCE_CASE(true, EPI_CORRECT)
+    FORCE_CASE(true, EPI_STORE)
   } else {
-    if (epi == EPI_STORE) FORCE_CASE(false, EPI_STORE)
-    else if (epi == EPI_PREDICT) FORCE_CASE(false, EPI_PREDICT)
-    else FORCE_CASE(false, EPI_CORRECT)
+    FORCE_CASE(false, EPI_STORE)
   }
 #undef FORCE_CASE
   return DEM_OK;
@@ -435,6 +446,13 @@ int read_counters(dem_ctx* c) {
   return DEM_OK;
 }
 
+// every candidate row is rebuilt in the next pass (new state or cells)
+int invalidate_candidates(dem_ctx* c) {
+  if (c->n > 0) CK(cudaMemsetAsync(c->CL.meta, 0xFF, sizeof(int4) * (size_t)c->n, c->stream));
+  CK(cudaMemsetAsync(&c->cnt->force_rebuild, 0xFF, sizeof(int), c->stream));
+  return DEM_OK;
+}
+
 // forget a failed (overflowed) history-updating pass: flags and its Ncol
 int clear_abort(dem_ctx* c) {
   CK(cudaMemsetAsync(&c->cnt->ncol_pending, 0, sizeof(unsigned long long), c->stream));
@@ -452,16 +470,26 @@ int force_pass(dem_ctx* c, const StateArrays& src, const StateArrays& tgt, bool 
   st = rebuild_cells(c, src, false);
   if (st) return st;
   if (c->n > 0) {
+    // rows of particles near a cell that gained/lost a particle are rebuilt
+    CK(cudaMemsetAsync(c->CL.repair, 0, (size_t)c->hp.ncell, c->stream));
+    launch(c, "mark_repair", k_mark_repair, blocks_for(c->hp.ncell, 256), 256,
+           (const DevParams*)c->dp, c->CL, (const Counters*)c->cnt);
     if (c->pp)
-      launch_sm(c, "screen", k_screen<true>, blocks_for(c->n, SCR_THREADS), SCR_THREADS,
-                screen_smem_bytes<true>(), (const DevParams*)c->dp, c->n,
-                (const double4*)c->S.pos, (const int*)c->S.comp, (const int*)c->S.cell,
-                (const int*)c->cell_start, c->CL, c->cnt);
+      launch(c, "screen", k_screen<true>, blocks_for(c->n, 256), 256, (const DevParams*)c->dp,
+             c->n, (const double4*)c->S.pos, (const int*)c->S.comp, (const int*)c->S.cell,
+             (const int*)c->S.orig, (const int*)c->cell_start, c->CL, c->cnt);
     else
-      launch_sm(c, "screen", k_screen<false>, blocks_for(c->n, SCR_THREADS), SCR_THREADS,
-                screen_smem_bytes<false>(), (const DevParams*)c->dp, c->n,
-                (const double4*)c->S.pos, (const int*)c->S.comp, (const int*)c->S.cell,
-                (const int*)c->cell_start, c->CL, c->cnt);
+      launch(c, "screen", k_screen<false>, blocks_for(c->n, 256), 256, (const DevParams*)c->dp,
+             c->n, (const double4*)c->S.pos, (const int*)c->S.comp, (const int*)c->S.cell,
+             (const int*)c->S.orig, (const int*)c->cell_start, c->CL, c->cnt);
+    if (c->pp)
+      launch(c, "filter", k_filter<true>, blocks_for(c->n, 256), 256, (const DevParams*)c->dp,
+             c->n, (const double4*)c->S.pos, (const int*)c->S.comp, (const int*)c->S.orig, c->CL,
+             (const Counters*)c->cnt);
+    else
+      launch(c, "filter", k_filter<false>, blocks_for(c->n, 256), 256, (const DevParams*)c->dp,
+             c->n, (const double4*)c->S.pos, (const int*)c->S.comp, (const int*)c->S.orig, c->CL,
+             (const Counters*)c->cnt);
   }
   for (int attempt = 0;; attempt++) {
     st = launch_force(c, tgt, update, dt, epi, rm, tag);
@@ -725,6 +753,13 @@ int dem_create(const dem_params* p, dem_ctx** out) {
     double d = p->pp_rmax + p->pp_rmax;  // Ri + Rj <= rmax + rmax after rounding
     h.max_min_dij_sq = d * d;
   }
+  {
+    // candidate lists keep particles within MinDij + skin; a particle moving
+    // skin/4 since the last full rebuild triggers the next one
+    h.vl_skin = 0.05 * CutOff;
+    const double q = 0.25 * h.vl_skin;
+    h.vl_thr2 = q * q;
+  }
   h.pp_mass_coef = p->pp_mass_coef;
   h.pp_density = p->pp_density;
   h.pp_fluid_density = p->pp_fluid_density;
@@ -837,6 +872,12 @@ int dem_set_state(dem_ctx* c, int32_t n, const int32_t* comp, const double* radi
   CK(cudaMalloc(&c->t_key, sizeof(unsigned) * N));
   CK(cudaMalloc(&c->CL.slot, sizeof(int) * N * KC));
   CK(cudaMalloc(&c->CL.meta, sizeof(int4) * N));
+  CK(cudaMalloc(&c->CL.slot_of_orig, sizeof(int) * N));
+  CK(cudaMalloc(&c->CL.ref_pos, sizeof(double4) * N));
+  CK(cudaMalloc(&c->CL.dirty, (size_t)c->hp.ncell));
+  CK(cudaMalloc(&c->CL.repair, (size_t)c->hp.ncell));
+  CK(cudaMalloc(&c->CL.xslot, sizeof(int) * N * KC));
+  CK(cudaMalloc(&c->CL.xmeta, sizeof(int4) * N));
   for (int b = 0; b < 2; b++) {
     int st = alloc_history(c, c->H[b], c->hcap);
     if (st) return st;
@@ -1137,6 +1178,8 @@ int dem_initialize_cell_distribution(dem_ctx* c) {
   if (!c) return DEM_ERR_INVALID;
   if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
   int st = rebuild_cells(c, c->P, true);
+  if (st) return st;
+  st = invalidate_candidates(c);
   if (st) return st;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));

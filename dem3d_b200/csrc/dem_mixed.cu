@@ -178,9 +178,12 @@ __device__ __forceinline__ void common_mixed(F3 Rij, F3 N, F3 DispN, F3 Vij, F3 
     float PartialDt;
     float VijSq = dot(Vij, Vij);
     if (VijSq > 0.0f) {
+      // (R.V + sqrt((R.V)^2 + |V|^2 dD2)) / |V|^2; for approaching particles
+      // (R.V < 0) the sum cancels, so use the equal form dD2 / (sqrt(..) - R.V)
       float RijVij = dot(Rij, Vij);
       float a = 2.0f * half_dt;
-      float b = (RijVij + sqrtf(RijVij * RijVij + VijSq * DeltaDijSq)) / VijSq;
+      float root = sqrtf(RijVij * RijVij + VijSq * DeltaDijSq);
+      float b = RijVij >= 0.0f ? (RijVij + root) / VijSq : DeltaDijSq / (root - RijVij);
       PartialDt = b < a ? b : a;
     } else {
       PartialDt = 0.0f;
@@ -238,13 +241,14 @@ __device__ __forceinline__ unsigned long long wsum(unsigned long long v) {
 }
 
 template <bool PP, int EPI, bool SWEEP>
-__global__ void __launch_bounds__(128, 4) k_force_mixed(ForceArgs A, MixedView V) {
+__global__ void __launch_bounds__(128, SWEEP ? 1 : 4) k_force_mixed(ForceArgs A, MixedView V) {
   if (A.cnt->abort) return;
   if (SWEEP && A.cnt->list_overflow == 0) return;
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long n_col = 0, n_pc = 0, n_wc = 0;
   int need = 0;
   const int4 meta = s < A.n ? A.cl_meta[s] : make_int4(0, 0, 0, 0);
+  if (!SWEEP && s == 0) clear_rebuild_trigger(A);
   if (s < A.n && (meta.x < 0) == SWEEP) {
     const DevParams& P = *A.P;
     const SortedArrays& S = A.S;
@@ -325,7 +329,7 @@ __global__ void __launch_bounds__(128, 4) k_force_mixed(ForceArgs A, MixedView V
         if (update && orig < qo) record(qo, o.FT, o.FTlo, o.VT);
       }
     };
-    walk_as_i<SWEEP>(A, meta, s, c, cx, cy, cz, visit_i);
+    walk_as_i<SWEEP>(A, meta, s, orig, c, cx, cy, cz, visit_i);
 
     for (int w = 0; w < P.nw; w++) {
       const dem_wall& W = P.walls[w];
@@ -393,7 +397,7 @@ __global__ void __launch_bounds__(128, 4) k_force_mixed(ForceArgs A, MixedView V
         if (update && orig < qo) record(qo, o.FT, o.FTlo, o.VT);
       }
     };
-    walk_as_j<SWEEP>(A, meta, s, c, cx, cy, cz, visit_j, [&]() {
+    walk_as_j<SWEEP>(A, meta, s, orig, c, cx, cy, cz, visit_j, [&]() {
       F = F + iF;
       T = T + iT;
     });
@@ -702,13 +706,9 @@ void mixed_force(MixedBuffers& M, bool pp, int epi, const ForceArgs& A, int cur,
     k_force_mixed<PPV, E, true><<<g, 128, 0, st>>>(A, V);    \
   } while (0)
   if (pp) {
-    if (epi == EPI_STORE) MCASE(true, EPI_STORE);
-    else if (epi == EPI_PREDICT) MCASE(true, EPI_PREDICT);
-    else MCASE(true, EPI_CORRECT);
+    MCASE(true, EPI_STORE);
   } else {
-    if (epi == EPI_STORE) MCASE(false, EPI_STORE);
-    else if (epi == EPI_PREDICT) MCASE(false, EPI_PREDICT);
-    else MCASE(false, EPI_CORRECT);
+    MCASE(false, EPI_STORE);
   }
 #undef MCASE
 }
