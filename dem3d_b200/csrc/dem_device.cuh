@@ -27,8 +27,8 @@ struct DevParams {
   double nxbylx, nybyly, nzbylz, nxby2, nyby2, nzby2;
   double ab0, am0, ab[3], am[3];
   double max_min_dij_sq;  // largest MinDijSq of any pair (screening early-out)
-  double vl_skin;         // candidate-list skin (added to MinDij)
-  double vl_thr2;         // (skin/4)^2: displacement that forces a full rebuild
+  double vl_skin;         // candidate-row skin (added to MinDij)
+  double vl_thr;          // accumulated displacement bound that forces a full rebuild
   double comp_radius[NCM], comp_inv_mass[NCM], comp_inv_inertia[NCM], comp_eff_mass[NCM];
   double min_dij[NCM * NCM], min_dij_sq[NCM * NCM];
   double kn[NCM * NCM], yn[NCM * NCM], kt[NCM * NCM], yt[NCM * NCM], mu_sq[NCM * NCM];
@@ -44,22 +44,28 @@ struct StateArrays {
   double *px, *py, *pz, *vx, *vy, *vz, *wx, *wy, *wz, *ax, *ay, *az, *lx, *ly, *lz;
 };
 
-// Device counters (one cache line each is not needed: low traffic).
+// Device counters and status words of a context.
 struct Counters {
   unsigned long long ncol;
   unsigned long long ncol_pending;  // Ncol of the last history-updating pass
   unsigned long long pair_contacts;
   unsigned long long wall_contacts;
-  unsigned long long movers;
+  unsigned long long movers;          // particles that changed cell in the last relink
   unsigned long long escaped;
+  unsigned long long movers_pending;  // particles pushed as arrivals for the next relink
   int overflow;      // a particle needed more pair records than the capacity
   int need_capacity; // largest record count requested
   int abort;         // nonzero: later kernels of a captured sequence do nothing
-  int abort_tag;     // 1 + index (within a captured chunk) of the failing step
-  int list_overflow; // particles of this pass whose contact-list row overflowed
-  int force_rebuild; // rebuild every candidate list in the next pass
-  unsigned long long max_disp2;  // bits of the largest squared displacement since
-                                 // the last full candidate-list rebuild
+  int abort_tag;     // 1 + 2*(step within a captured chunk) + pass of the failing pass
+  int n_dirty[2];    // cells in dirty list b (transition to cell assignment b)
+  int n_repair;      // cells whose particles' candidate rows are rebuilt this pass
+  int full_due;      // this pass rebuilds every candidate row
+  int force_full;    // the next pass must rebuild every row (new state, grown rows)
+  int row_overflow;  // a candidate row needed more than kc entries
+  int need_kc;       // longest candidate row requested
+  int list_error;    // a cell-list walk exceeded its bound (corrupt lists)
+  unsigned long long disp_max;  // bits of the largest displacement bound of one pass
+  double disp_acc;   // sum of disp_max since the last full rebuild
   double wall_fn[NWM];
 };
 
@@ -73,12 +79,9 @@ struct History {
   int cap;
 };
 
-// Sorted (cell/traversal order) copies used by the force kernel.
+// Traversal-order arrays of the counting sort that builds the initial cell
+// lists (DistributeParticles3D) and serves the allocation-free entry point.
 struct SortedArrays {
-  double4* pos;  // x, y, z, radius
-  double4* v4;   // vx, vy, vz, wx
-  double2* w2;   // wy, wz
-  int* comp;     // component (table mode)
   int* orig;     // slot -> original index (also "order")
   int* cell;     // slot -> cell
 };
@@ -91,48 +94,69 @@ struct RingMap {
   int phys[5];  // phys[k] = physical slot of logical ipc(k+1); phys[nprev] = spare
 };
 
-// Candidate lists, one row of KC entries per particle (indexed by original
-// index): the particles within MinDij + skin, as original indices, first the
-// "p is i" partners in the order of p's neighbour list, then the "p is j"
-// partners in sweep order.  meta = (n1, n2 before p's own block, n2 after
-// it, 0); n1 = -1 when the row overflowed or was never built (the force
-// kernel then sweeps the cells itself for that particle).  A row stays valid
-// while no cell of its 27-cell neighbourhood gains or loses a particle (the
-// relative order of the others in the cell lists is unchanged) and no
-// particle has moved skin/4 since the last full rebuild.
-constexpr int KC = 32;
-struct ContactLists {
-  int* slot;          // [n*KC] candidate original indices
-  int4* meta;         // [n]
-  int* slot_of_orig;  // [n] traversal slot of every particle (this pass)
-  double4* ref_pos;   // [n] positions at the last full rebuild
-  unsigned char* dirty;   // [ncell] a particle entered/left the cell this pass
-  unsigned char* repair;  // [ncell] rows of this cell's particles are rebuilt
-  // this pass's exact contacts, filtered from the candidates: rows indexed by
-  // traversal slot holding traversal slots, same order and meta layout
-  int* xslot;   // [n*KC]
-  int4* xmeta;  // [n]
+// The reference's linked cell lists (FirstParticle/NextParticle of MCells),
+// kept in its order: a cell's list holds the particles that entered it in
+// the last redistribution in decreasing index, then the others in their
+// previous order.  Between passes only the cells that gained or lost a
+// particle are relinked.
+struct CellLists {
+  int* head;      // [ncell] first particle of the cell's list, -1 = empty
+  int* next;      // [n] next particle of the same list, -1 = end
+  int* cell[2];   // [n] cell of every particle under assignment b
+  int* arr_head;  // [ncell] particles entering the cell at the next relink, -1 = none
+  int* arr_next;  // [n]
+  int* mflag;     // [n] particle already pushed as an arrival
+  int* dflag;     // [ncell] cell already in a dirty list
+  int* rflag;     // [ncell] cell already in the repair list
+  int* dlist[2];  // [ncell] cells that gain or lose a particle on the way to assignment b
+  int* rlist;     // [ncell] cells whose particles' candidate rows are rebuilt
 };
 
-struct ForceArgs {
+// Candidate rows, column-major (cand[k*n + p]): the particles within
+// MinDij + skin of particle p, as original indices, in the order p meets
+// them in ComputeAccelerations' sweep -- first the "p is i" partners of
+// loop 1 (src/MForces.f90:199-272), then the "p is j" partners in sweep
+// order, split where p's own block ends.  meta = n1 | n2b << 10 | n2a << 20.
+// A row stays valid while no cell of its 27-cell neighbourhood gains or
+// loses a particle and no particle has moved skin/2 since the last full
+// rebuild.
+struct Rows {
+  int* cand;
+  int* meta;
+  int kc;
+};
+constexpr int META_BITS = 10;
+constexpr int META_MASK = (1 << META_BITS) - 1;
+constexpr int KC_MAX = META_MASK;
+
+// Arguments of one pass kernel.  V4/W2 are the velocity copies the pass
+// reads for partners (double in FP64 mode, float in mixed mode).
+template <class V4, class W2>
+struct PassArgs {
   const DevParams* P;
   int n;
-  SortedArrays S;
-  const int* cell_start;
-  const int* cell_of_orig;
-  const int* cl_slot;
-  const int4* cl_meta;
-  const int* slot_of_orig;
+  const double4* X;   // this pass's positions (x, y, z, R) by original index
+  const V4* v4;       // vx, vy, vz, wx
+  const W2* w2;       // wy, wz
+  const int* comp;
+  const int* cand;
+  const int* meta;
+  const int* cell_cur;  // cell of every particle in this pass
+  CellLists L;          // next assignment: L.cell[par_nxt]
+  int par_nxt;
   History Hr, Hw;
   int update;
   double half_dt;
   StateArrays tgt;   // where a/alpha go (EPI_STORE)
   StateArrays part;  // Particle
   StateArrays pred;  // Predicted
+  double4* Xn;       // positions of the next pass (written by the epilogue)
+  V4* v4n;
+  W2* w2n;
   double* ring;      // [(slot*9 + comp)*n + orig]
   RingMap rm;
   Counters* cnt;
-  int tag;  // index of this step within a captured chunk
+  int tag;  // 2*(step within a captured chunk) + pass
 };
 
 // ------------------------------------------------------------------------
@@ -368,289 +392,4 @@ __device__ __forceinline__ int axis_wrap(int j, int N, int pbc) {
   }
   return j;
 }
-// offsets of one axis in ascending order of the wrapped cell coordinate
-__device__ __forceinline__ int axis_sorted(int i, int N, int pbc, int off[3]) {
-  int lo, hi;
-  axis_range(i, N, pbc, lo, hi);
-  int m = 0;
-  if (pbc && i == 0) {  // -1 wraps to N-1 (largest)
-    off[m++] = 0;
-    off[m++] = 1;
-    off[m++] = -1;
-  } else if (pbc && i == N - 1) {  // +1 wraps to 0 (smallest)
-    off[m++] = 1;
-    off[m++] = -1;
-    off[m++] = 0;
-  } else {
-    for (int k = lo; k <= hi; k++) off[m++] = k;
-  }
-  return m;
-}
-
-
-// ------------------------------------------------------------------------
-// the reference's cell sweep (ComputeAccelerations, src/MForces.f90:173-324)
-// seen from one particle p at traversal slot s of cell c = (cx, cy, cz)
-
-// Loop 1 ("p is i"): the neighbour list of p's block is the rest of its own
-// cell, then the half-shell cells in the order of the FirstNeighbour list,
-// which AddAllNeighbours3D (src/MCells.f90:424-476) builds by prepending in
-// kz, ky, kx loop order with kx + Nx*(ky + Ny*kz) > 0 (so: reverse order).
-template <class Visit>
-__device__ __forceinline__ void sweep_as_i(const DevParams& P, const int* __restrict__ cs, int s,
-                                           int c, int cx, int cy, int cz, Visit&& visit) {
-  const int nx = P.nx, ny = P.ny, nz = P.nz;
-  const int e = cs[c + 1];
-  for (int t = s + 1; t < e; t++) visit(t);
-  int xi, xf, yi, yf, zi, zf;
-  axis_range(cx, nx, P.pbc[0], xi, xf);
-  axis_range(cy, ny, P.pbc[1], yi, yf);
-  axis_range(cz, nz, P.pbc[2], zi, zf);
-  for (int kz = zf; kz >= zi; kz--) {
-    const int jz = axis_wrap(cz + kz, nz, P.pbc[2]);
-    for (int ky = yf; ky >= yi; ky--) {
-      const int jy = axis_wrap(cy + ky, ny, P.pbc[1]);
-      for (int kx = xf; kx >= xi; kx--) {
-        if (kx + nx * (ky + ny * kz) <= 0) continue;
-        const int jx = axis_wrap(cx + kx, nx, P.pbc[0]);
-        const int jc = jx + nx * (jy + ny * jz);
-        const int b = cs[jc], e2 = cs[jc + 1];
-        for (int t = b; t < e2; t++) visit(t);
-      }
-    }
-  }
-}
-
-// Loop 2 ("p is j"): every particle q whose block lists p -- the earlier
-// members of p's cell and the members of the cells whose half shell holds
-// p's cell -- in the order the sweep reaches q (ascending cell index, then
-// list order); own() is called where p's own block ends (Force(i) =
-// Force(i) + iForce, src/MForces.f90:319-320).
-template <class Visit, class Own>
-__device__ __forceinline__ void sweep_as_j(const DevParams& P, const int* __restrict__ cs, int s,
-                                           int c, int cx, int cy, int cz, Visit&& visit,
-                                           Own&& own) {
-  const int nx = P.nx, ny = P.ny, nz = P.nz;
-  int ox[3], oy[3], oz[3];
-  const int mx = axis_sorted(cx, nx, P.pbc[0], ox);
-  const int my = axis_sorted(cy, ny, P.pbc[1], oy);
-  const int mz = axis_sorted(cz, nz, P.pbc[2], oz);
-  for (int a = 0; a < mz; a++) {
-    const int dz = oz[a];
-    const int jz = axis_wrap(cz + dz, nz, P.pbc[2]);
-    for (int b = 0; b < my; b++) {
-      const int dy = oy[b];
-      const int jy = axis_wrap(cy + dy, ny, P.pbc[1]);
-      for (int d = 0; d < mx; d++) {
-        const int dx = ox[d];
-        if (dx == 0 && dy == 0 && dz == 0) {
-          for (int t = cs[c]; t < s; t++) visit(t);
-          own();
-          continue;
-        }
-        // p's cell is in the half shell of the cell at offset (dx,dy,dz)
-        if (-dx + nx * (-dy + ny * -dz) <= 0) continue;
-        const int jx = axis_wrap(cx + dx, nx, P.pbc[0]);
-        const int jc = jx + nx * (jy + ny * jz);
-        const int b0 = cs[jc], e2 = cs[jc + 1];
-        for (int t = b0; t < e2; t++) visit(t);
-      }
-    }
-  }
-}
-
-// The same two sweeps, also telling the visitor how the neighbour cell was
-// reached: w = (+1 | -1 | 0) per axis when the cell index wrapped past the
-// upper | lower edge of a periodic axis.
-__device__ __forceinline__ int axis_wrap_w(int j, int N, int pbc, int& w) {
-  w = 0;
-  if (pbc) {
-    if (j == N) { j = 0; w = 1; }
-    if (j == -1) { j = N - 1; w = -1; }
-  }
-  return j;
-}
-
-template <class Visit>
-__device__ __forceinline__ void sweep_as_i_w(const DevParams& P, const int* __restrict__ cs,
-                                             int s, int c, int cx, int cy, int cz,
-                                             Visit&& visit) {
-  const int nx = P.nx, ny = P.ny, nz = P.nz;
-  const int e = cs[c + 1];
-  for (int t = s + 1; t < e; t++) visit(t, 0, 0, 0);
-  int xi, xf, yi, yf, zi, zf;
-  axis_range(cx, nx, P.pbc[0], xi, xf);
-  axis_range(cy, ny, P.pbc[1], yi, yf);
-  axis_range(cz, nz, P.pbc[2], zi, zf);
-  for (int kz = zf; kz >= zi; kz--) {
-    int wz;
-    const int jz = axis_wrap_w(cz + kz, nz, P.pbc[2], wz);
-    for (int ky = yf; ky >= yi; ky--) {
-      int wy;
-      const int jy = axis_wrap_w(cy + ky, ny, P.pbc[1], wy);
-      for (int kx = xf; kx >= xi; kx--) {
-        if (kx + nx * (ky + ny * kz) <= 0) continue;
-        int wx;
-        const int jx = axis_wrap_w(cx + kx, nx, P.pbc[0], wx);
-        const int jc = jx + nx * (jy + ny * jz);
-        const int b = cs[jc], e2 = cs[jc + 1];
-        for (int t = b; t < e2; t++) visit(t, wx, wy, wz);
-      }
-    }
-  }
-}
-
-template <class Visit, class Own>
-__device__ __forceinline__ void sweep_as_j_w(const DevParams& P, const int* __restrict__ cs,
-                                             int s, int c, int cx, int cy, int cz, Visit&& visit,
-                                             Own&& own) {
-  const int nx = P.nx, ny = P.ny, nz = P.nz;
-  int ox[3], oy[3], oz[3];
-  const int mx = axis_sorted(cx, nx, P.pbc[0], ox);
-  const int my = axis_sorted(cy, ny, P.pbc[1], oy);
-  const int mz = axis_sorted(cz, nz, P.pbc[2], oz);
-  for (int a = 0; a < mz; a++) {
-    const int dz = oz[a];
-    int wz;
-    const int jz = axis_wrap_w(cz + dz, nz, P.pbc[2], wz);
-    for (int b = 0; b < my; b++) {
-      const int dy = oy[b];
-      int wy;
-      const int jy = axis_wrap_w(cy + dy, ny, P.pbc[1], wy);
-      for (int d = 0; d < mx; d++) {
-        const int dx = ox[d];
-        if (dx == 0 && dy == 0 && dz == 0) {
-          for (int t = cs[c]; t < s; t++) visit(t, 0, 0, 0);
-          own();
-          continue;
-        }
-        if (-dx + nx * (-dy + ny * -dz) <= 0) continue;
-        int wx;
-        const int jx = axis_wrap_w(cx + dx, nx, P.pbc[0], wx);
-        const int jc = jx + nx * (jy + ny * jz);
-        const int b0 = cs[jc], e2 = cs[jc + 1];
-        for (int t = b0; t < e2; t++) visit(t, wx, wy, wz);
-      }
-    }
-  }
-}
-
-// The two sweeps as slot ranges: emit(b, e, wx, wy, wz) per visited cell
-// (own cell: the part after / before p), own() right after p's own range in
-// loop 2.
-template <class Emit>
-__device__ __forceinline__ void sweep_cells_as_i(const DevParams& P, const int* __restrict__ cs,
-                                                 int s, int c, int cx, int cy, int cz,
-                                                 Emit&& emit) {
-  const int nx = P.nx, ny = P.ny, nz = P.nz;
-  emit(s + 1, cs[c + 1], 0, 0, 0);
-  int xi, xf, yi, yf, zi, zf;
-  axis_range(cx, nx, P.pbc[0], xi, xf);
-  axis_range(cy, ny, P.pbc[1], yi, yf);
-  axis_range(cz, nz, P.pbc[2], zi, zf);
-  for (int kz = zf; kz >= zi; kz--) {
-    int wz;
-    const int jz = axis_wrap_w(cz + kz, nz, P.pbc[2], wz);
-    for (int ky = yf; ky >= yi; ky--) {
-      int wy;
-      const int jy = axis_wrap_w(cy + ky, ny, P.pbc[1], wy);
-      for (int kx = xf; kx >= xi; kx--) {
-        if (kx + nx * (ky + ny * kz) <= 0) continue;
-        int wx;
-        const int jx = axis_wrap_w(cx + kx, nx, P.pbc[0], wx);
-        const int jc = jx + nx * (jy + ny * jz);
-        emit(cs[jc], cs[jc + 1], wx, wy, wz);
-      }
-    }
-  }
-}
-
-template <class Emit, class Own>
-__device__ __forceinline__ void sweep_cells_as_j(const DevParams& P, const int* __restrict__ cs,
-                                                 int s, int c, int cx, int cy, int cz, Emit&& emit,
-                                                 Own&& own) {
-  const int nx = P.nx, ny = P.ny, nz = P.nz;
-  int ox[3], oy[3], oz[3];
-  const int mx = axis_sorted(cx, nx, P.pbc[0], ox);
-  const int my = axis_sorted(cy, ny, P.pbc[1], oy);
-  const int mz = axis_sorted(cz, nz, P.pbc[2], oz);
-  for (int a = 0; a < mz; a++) {
-    const int dz = oz[a];
-    int wz;
-    const int jz = axis_wrap_w(cz + dz, nz, P.pbc[2], wz);
-    for (int b = 0; b < my; b++) {
-      const int dy = oy[b];
-      int wy;
-      const int jy = axis_wrap_w(cy + dy, ny, P.pbc[1], wy);
-      for (int d = 0; d < mx; d++) {
-        const int dx = ox[d];
-        if (dx == 0 && dy == 0 && dz == 0) {
-          emit(cs[c], s, 0, 0, 0);
-          own();
-          continue;
-        }
-        if (-dx + nx * (-dy + ny * -dz) <= 0) continue;
-        int wx;
-        const int jx = axis_wrap_w(cx + dx, nx, P.pbc[0], wx);
-        const int jc = jx + nx * (jy + ny * jz);
-        emit(cs[jc], cs[jc + 1], wx, wy, wz);
-      }
-    }
-  }
-}
-
-// Minimum image of one component exactly as Rij(k) - Lbox(k)*nint(Rij(k)*
-// InvLbox(k)) (src/MForces.f90:212-214), given the image n the cell sweep
-// implies: if |Rij - n*L| < 0.49*L then nint(Rij/L) == n (the margin covers
-// the rounding of Rij*InvLbox), so Rij - L*n is the reference's value bit for
-// bit; otherwise the formula itself is evaluated.
-__device__ __forceinline__ double min_image(double r, int pbc, double L, double iL, int n) {
-  if (!pbc) return r;
-  const double d = r - L * (double)n;
-  if (fabs(d) < 0.49 * L) return d;
-  return r - L * fnint(r * iL);
-}
-
-// Loop 1 / loop 2 driven by the screening kernel's contact list when the
-// particle's row did not overflow, else by the full sweep (same order).
-// Full candidate-list rebuild due in this pass: requested by the host (new
-// state or cells) or some particle moved more than skin/4 since the last one.
-__device__ __forceinline__ bool rebuild_due(const DevParams& P, const Counters* cnt) {
-  return cnt->force_rebuild != 0 ||
-         __longlong_as_double((long long)cnt->max_disp2) > P.vl_thr2;
-}
-
-// Called by one thread of the force kernel (after the screening kernel has
-// read the trigger): the rebuild of this pass is done.
-__device__ __forceinline__ void clear_rebuild_trigger(const ForceArgs& A) {
-  if (rebuild_due(*A.P, A.cnt)) {
-    A.cnt->force_rebuild = 0;
-    A.cnt->max_disp2 = 0ull;
-  }
-}
-
-template <bool SWEEP, class Visit>
-__device__ __forceinline__ void walk_as_i(const ForceArgs& A, int4 meta, int s, int orig, int c,
-                                          int cx, int cy, int cz, Visit&& visit) {
-  if (!SWEEP) {
-    const int* l = A.cl_slot + (size_t)s * KC;
-    for (int k = 0; k < meta.x; k++) visit(l[k]);
-  } else {
-    sweep_as_i(*A.P, A.cell_start, s, c, cx, cy, cz, visit);
-  }
-}
-
-template <bool SWEEP, class Visit, class Own>
-__device__ __forceinline__ void walk_as_j(const ForceArgs& A, int4 meta, int s, int orig, int c,
-                                          int cx, int cy, int cz, Visit&& visit, Own&& own) {
-  if (!SWEEP) {
-    const int* l = A.cl_slot + (size_t)s * KC + meta.x;
-    for (int k = 0; k < meta.y; k++) visit(l[k]);
-    own();
-    for (int k = meta.y; k < meta.y + meta.z; k++) visit(l[k]);
-  } else {
-    sweep_as_j(*A.P, A.cell_start, s, c, cx, cy, cz, visit, own);
-  }
-}
-
 }  // namespace dem

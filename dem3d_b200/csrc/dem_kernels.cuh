@@ -1,25 +1,30 @@
-// dem_kernels.cuh -- sm_100a kernels of the FP64 DEM step.
+// dem_kernels.cuh -- sm_100a kernels of the DEM step (FP64 pass kernel and
+// the precision-independent cell-list, candidate-row and integrator kernels).
 //
-// K1  cell rebuild = counting sort of particles by cell hash into traversal
-//     order (k_assign -> scan -> k_scatter -> k_cellsort -> k_gather).
-//     Within a cell the order is exactly the reference's linked-list order:
-//     RedistributeParticles3D (src/MCells.f90:607-643) walks particles in
-//     index order and prepends every particle that changed cell
-//     (TransferParticle, :747-774), so a cell lists first the particles that
-//     entered it during this pass (highest index first) and then the ones that
-//     stayed, in their previous order.  The sort key encodes exactly that.
-// K2+K4 force kernel: one thread per particle in traversal order gathers its
-//     contacts (no atomics), evaluates every pair in the reference's
-//     orientation ("i" = the particle visited first) and adds the
-//     contributions in the order of the reference's cell sweep, so that the
-//     forces are bit-identical to ComputeAccelerations (src/MForces.f90:
-//     145-335).  The AB predictor / AM corrector (src/MDEM.f90:296-365) run in
-//     the same kernel's epilogue.
+// K1  cell lists: the reference's linked lists (src/MCells.f90), kept in its
+//     order.  The initial distribution (DistributeParticles3D) is a counting
+//     sort by cell with every cell in decreasing index, then linked.  Each
+//     later pass relinks only the cells that gained or lost a particle
+//     (RedistributeParticles3D, src/MCells.f90:607-643: the movers are
+//     prepended in increasing index order, so a cell lists the particles that
+//     entered it in this pass, highest index first, then the ones that
+//     stayed, in their previous order).
+// K2  candidate rows: for every particle, the partners within MinDij + skin
+//     in the order the reference's sweep meets them (src/MForces.f90:173-272),
+//     rebuilt by one warp per particle around relinked cells, and for every
+//     particle when the accumulated displacement bound reaches 0.4 skin.
+// K2+K4 pass kernel: one thread per particle (original index order) applies
+//     the reference's overlap test to its candidates, evaluates every contact
+//     in the reference's orientation ("i" = the particle visited first) and
+//     adds the contributions in the order of the sweep, so that the forces
+//     are bit-identical to ComputeAccelerations (src/MForces.f90:145-335).
+//     The AB predictor / AM corrector (src/MDEM.f90:296-365) run in its
+//     epilogue, which also hashes the next position into its cell.
 // K3  history: records owned by imin are double-buffered; a pass that updates
 //     them writes a fresh table (new/updated contacts + records of pairs that
 //     the sweep did not visit, as the reference keeps those untouched).
 #pragma once
-#include "dem_device.cuh"
+#include "dem_pass.cuh"
 
 namespace dem {
 
@@ -66,57 +71,6 @@ __global__ void k_assign(const DevParams* __restrict__ Pp, int n, int initial,
   }
   mv = warp_sum_u64(mv);
   if ((threadIdx.x & 31) == 0 && mv) atomicAdd(&cnt->movers, mv);
-}
-
-// k_assign for the context path: also marks the old and new cell of every
-// particle that changed cell (their neighbourhoods' candidate rows are
-// rebuilt) and tracks the largest squared displacement since the last full
-// candidate-list rebuild.
-__global__ void k_assign_track(const DevParams* __restrict__ Pp, int n,
-                               const double* __restrict__ px, const double* __restrict__ py,
-                               const double* __restrict__ pz, const int* __restrict__ order,
-                               const int* __restrict__ old_cell, int* __restrict__ cell_cnt,
-                               int* __restrict__ a_cell, int* __restrict__ a_loc,
-                               unsigned* __restrict__ a_key, int* __restrict__ a_orig,
-                               ContactLists L, Counters* __restrict__ cnt) {
-  if (cnt->abort) return;
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s == 0 && cnt->ncol_pending) {
-    cnt->ncol += cnt->ncol_pending;
-    cnt->ncol_pending = 0;
-  }
-  unsigned long long mv = 0;
-  double d2 = 0.0;
-  if (s < n) {
-    const DevParams& P = *Pp;
-    const int orig = order[s];
-    const double x = px[orig], y = py[orig], z = pz[orig];
-    const int c = current_cell(P, x, y, z);
-    const int old = old_cell[s];
-    const bool mover = c != old;
-    const unsigned key = mover ? (unsigned)(n - 1 - orig) : (unsigned)(n + s);
-    const int loc = atomicAdd(&cell_cnt[c], 1);
-    a_cell[s] = c;
-    a_loc[s] = loc;
-    a_key[s] = key;
-    a_orig[s] = orig;
-    if (mover) {
-      L.dirty[c] = 1;
-      L.dirty[old] = 1;
-      mv = 1ull;
-    }
-    const double4 r = L.ref_pos[orig];
-    const double dx = x - r.x, dy = y - r.y, dz = z - r.z;
-    d2 = dx * dx + dy * dy + dz * dz;
-    if (!(d2 <= 1e300)) d2 = 1e300;  // NaN-safe: any invalid state forces a rebuild
-  }
-  mv = warp_sum_u64(mv);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) d2 = fmax(d2, __shfl_down_sync(0xffffffffu, d2, o));
-  if ((threadIdx.x & 31) == 0) {
-    if (mv) atomicAdd(&cnt->movers, mv);
-    if (d2 > 0.0) atomicMax(&cnt->max_disp2, (unsigned long long)__double_as_longlong(d2));
-  }
 }
 
 // exclusive scan, phase 1: tiles of 4*blockDim elements
@@ -243,28 +197,6 @@ __global__ void k_cellsort(int ncell, const int* __restrict__ cell_start,
   }
 }
 
-// Copy the source state into traversal order (the "SoA reorder").
-template <bool PP>
-__global__ void k_gather(const DevParams* __restrict__ Pp, int n, StateArrays src,
-                         const double* __restrict__ radius, const int* __restrict__ comp,
-                         SortedArrays S, const Counters* __restrict__ cnt) {
-  if (cnt->abort) return;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  int o = S.orig[t];
-  double R;
-  if (PP) {
-    R = radius[o];
-  } else {
-    int k = comp[o];
-    S.comp[t] = k;
-    R = Pp->comp_radius[k];
-  }
-  S.pos[t] = make_double4(src.px[o], src.py[o], src.pz[o], R);
-  S.v4[t] = make_double4(src.vx[o], src.vy[o], src.vz[o], src.wx[o]);
-  S.w2[t] = make_double2(src.wy[o], src.wz[o]);
-}
-
 // ---------------------------------------------------------------------------
 // material helpers
 
@@ -371,598 +303,6 @@ __device__ __forceinline__ void hist_write(const History& H, int owner, int r, i
   v[0] = make_double2(ft[0], ft[1]);
   v[1] = make_double2(ft[2], vt[0]);
   v[2] = make_double2(vt[1], vt[2]);
-}
-
-// ---------------------------------------------------------------------------
-// K2+K4: force kernel (FP64, exact order)
-
-
-// SWEEP = false: particles whose contact-list row is valid; SWEEP = true:
-// the (rare) particles whose row overflowed, which sweep the cells here.
-template <bool PP, int EPI, bool SWEEP>
-__global__ void __launch_bounds__(128, SWEEP ? 1 : 4) k_force_fp64(ForceArgs A) {
-  if (A.cnt->abort) return;
-  if (SWEEP && A.cnt->list_overflow == 0) return;
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned long long n_col = 0, n_pc = 0, n_wc = 0;
-  int need = 0;
-  const int4 meta = s < A.n ? A.cl_meta[s] : make_int4(0, 0, 0, 0);
-  if (!SWEEP && s == 0) clear_rebuild_trigger(A);
-  if (s < A.n && (meta.x < 0) == SWEEP) {
-    const DevParams& P = *A.P;
-    const SortedArrays& S = A.S;
-    const int nx = P.nx, ny = P.ny, nz = P.nz;
-    const int c = S.cell[s];
-    const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
-    const double4 p4 = S.pos[s];
-    const double xp[3] = {p4.x, p4.y, p4.z};
-    const double Rp = p4.w;
-    const double4 pv4 = S.v4[s];
-    const double2 pw2 = S.w2[s];
-    const double vp[3] = {pv4.x, pv4.y, pv4.z};
-    const double wp[3] = {pv4.w, pw2.x, pw2.y};
-    const int orig = S.orig[s];
-    const int cp = PP ? 0 : S.comp[s];
-    double inv_m, inv_i, eff_m;
-    Material<PP>::self(P, cp, Rp, inv_m, inv_i, eff_m);
-    const double half_dt = A.half_dt;
-    const bool update = A.update != 0;
-    int hw_n = 0;
-    bool overflow = false;
-
-    double iF[3], iT[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-    for (int k = 0; k < 3; k++) iF[k] = eff_m * P.gravity[k];
-
-    auto record = [&](int partner, const double ft[3], const double vt[3]) {
-      if (hw_n < A.Hw.cap)
-        hist_write(A.Hw, orig, hw_n, partner, ft, vt);
-      else
-        overflow = true;
-      hw_n++;
-    };
-
-    // p is "i", slot t is "j" (src/MForces.f90:199-272)
-    auto visit_i = [&](int t) {
-      const double4 q4 = S.pos[t];
-      double Rij[3] = {q4.x - xp[0], q4.y - xp[1], q4.z - xp[2]};
-#pragma unroll
-      for (int k = 0; k < 3; k++)
-        if (P.pbc[k]) Rij[k] = Rij[k] - P.lbox[k] * fnint(Rij[k] * P.inv_lbox[k]);
-      const double DijSq = sumsq3(Rij);
-      const int cq = PP ? 0 : S.comp[t];
-      const double Delta = Material<PP>::min_dij_sq(P, cp, Rp, cq, q4.w) - DijSq;
-      if (Delta > 0.0) {
-        PairPar pp;
-        Material<PP>::pair(P, cp, Rp, cq, q4.w, pp);
-        const int qo = S.orig[t];
-        const double4 qv4 = S.v4[t];
-        const double2 qw2 = S.w2[t];
-        const double vq[3] = {qv4.x, qv4.y, qv4.z};
-        const double wq[3] = {qv4.w, qw2.x, qw2.y};
-        const int lo = orig < qo ? orig : qo, hi = orig < qo ? qo : orig;
-        double FT0[3] = {0.0, 0.0, 0.0}, VT0[3] = {0.0, 0.0, 0.0};
-        int r = hist_find(A.Hr, lo, hi);
-        bool contacting = r >= 0;
-        if (contacting) hist_read(A.Hr, lo, r, FT0, VT0);
-        if (!contacting) n_col++;
-        n_pc++;
-        ContactOut o;
-        pair_contact(Rij, DijSq, Delta, pp, Rp, vp, wp, q4.w, vq, wq, half_dt, contacting, FT0,
-                     VT0, o);
-#pragma unroll
-        for (int k = 0; k < 3; k++) iF[k] = iF[k] + o.FN[k] + o.FT[k];
-        double RN[3], tq[3];
-#pragma unroll
-        for (int k = 0; k < 3; k++) RN[k] = Rp * o.N[k];
-        cross3(RN, o.FT, tq);
-#pragma unroll
-        for (int k = 0; k < 3; k++) iT[k] = iT[k] + tq[k];
-        if (update && orig < qo) record(qo, o.FT, o.VT);
-      }
-    };
-
-    // ---- loop 1: own cell after p, then the half-shell cells in the order
-    // of the FirstNeighbour list (reverse of AddAllNeighbours3D insertion)
-    walk_as_i<SWEEP>(A, meta, s, orig, c, cx, cy, cz, visit_i);
-
-    // ---- walls (src/MForces.f90:274-314)
-    for (int w = 0; w < P.nw; w++) {
-      const dem_wall& W = P.walls[w];
-      const int wi = orig * P.nw + w;
-      bool contacting = A.Hr.wflag[wi] != 0;
-      double FT0[3] = {0.0, 0.0, 0.0}, VT0[3] = {0.0, 0.0, 0.0};
-      if (contacting) {
-        const double2* v = A.Hr.wval + (size_t)wi * 3;
-        double2 a = v[0], b = v[1], d = v[2];
-        FT0[0] = a.x; FT0[1] = a.y; FT0[2] = b.x;
-        VT0[0] = b.y; VT0[1] = d.x; VT0[2] = d.y;
-      }
-      double Dij, Nij[3], Qji[3];
-      bool ov = false;
-      if (W.shape == DEM_WALL_RECTANGLE) ov = overlap_rect(P, W, xp, Rp, Dij, Nij, Qji);
-      if (ov) {
-        n_wc++;
-        const double Delta = Rp * Rp - Dij * Dij;
-        const double dn = Dij - Rp;
-        double DispN[3], wqv[3], Vij[3], ro[3], cr[3], VijC[3], Rw[3];
-#pragma unroll
-        for (int k = 0; k < 3; k++) DispN[k] = dn * Nij[k];
-        cross3(W.omega, Qji, wqv);
-#pragma unroll
-        for (int k = 0; k < 3; k++) Vij[k] = W.velocity[k] + wqv[k] - vp[k];
-#pragma unroll
-        for (int k = 0; k < 3; k++) ro[k] = Rp * wp[k];
-        cross3(ro, Nij, cr);
-#pragma unroll
-        for (int k = 0; k < 3; k++) VijC[k] = Vij[k] - cr[k];
-#pragma unroll
-        for (int k = 0; k < 3; k++) Rw[k] = W.position[k] + Qji[k] - xp[k];
-        PairPar pp;
-        Material<PP>::wall(P, cp, Rp, w, pp);
-        ContactOut o;
-        common_calc(Rw, Nij, DispN, Vij, VijC, Delta, half_dt, contacting, FT0, VT0, pp.kn, pp.yn,
-                    pp.kt, pp.yt, pp.mu_sq, o);
-#pragma unroll
-        for (int k = 0; k < 3; k++) iF[k] = iF[k] + o.FN[k] + o.FT[k];
-        double RN[3], tq[3];
-#pragma unroll
-        for (int k = 0; k < 3; k++) RN[k] = Rp * o.N[k];
-        cross3(RN, o.FT, tq);
-#pragma unroll
-        for (int k = 0; k < 3; k++) iT[k] = iT[k] + tq[k];
-        atomicAdd(&A.cnt->wall_fn[w], sqrt(sumsq3(o.FN)));
-        if (update) {
-          A.Hw.wflag[wi] = 1;
-          double2* v = A.Hw.wval + (size_t)wi * 3;
-          v[0] = make_double2(o.FT[0], o.FT[1]);
-          v[1] = make_double2(o.FT[2], o.VT[0]);
-          v[2] = make_double2(o.VT[1], o.VT[2]);
-        }
-      } else if (update) {
-        A.Hw.wflag[wi] = 0;
-      }
-    }
-
-    // ---- loop 2: p as "j"; contributions in traversal order of the "i"
-    // particle, own block (Force(i) = Force(i) + iForce) at p's position.
-    double F[3] = {0.0, 0.0, 0.0}, T[3] = {0.0, 0.0, 0.0};
-    auto visit_j = [&](int t) {
-      const double4 q4 = S.pos[t];
-      double Rij[3] = {xp[0] - q4.x, xp[1] - q4.y, xp[2] - q4.z};
-#pragma unroll
-      for (int k = 0; k < 3; k++)
-        if (P.pbc[k]) Rij[k] = Rij[k] - P.lbox[k] * fnint(Rij[k] * P.inv_lbox[k]);
-      const double DijSq = sumsq3(Rij);
-      const int cq = PP ? 0 : S.comp[t];
-      const double Delta = Material<PP>::min_dij_sq(P, cq, q4.w, cp, Rp) - DijSq;
-      if (Delta > 0.0) {
-        PairPar pp;
-        Material<PP>::pair(P, cq, q4.w, cp, Rp, pp);
-        const int qo = S.orig[t];
-        const double4 qv4 = S.v4[t];
-        const double2 qw2 = S.w2[t];
-        const double vq[3] = {qv4.x, qv4.y, qv4.z};
-        const double wq[3] = {qv4.w, qw2.x, qw2.y};
-        const int lo = orig < qo ? orig : qo, hi = orig < qo ? qo : orig;
-        double FT0[3] = {0.0, 0.0, 0.0}, VT0[3] = {0.0, 0.0, 0.0};
-        int r = hist_find(A.Hr, lo, hi);
-        bool contacting = r >= 0;
-        if (contacting) hist_read(A.Hr, lo, r, FT0, VT0);
-        ContactOut o;
-        pair_contact(Rij, DijSq, Delta, pp, q4.w, vq, wq, Rp, vp, wp, half_dt, contacting, FT0,
-                     VT0, o);
-#pragma unroll
-        for (int k = 0; k < 3; k++) F[k] = F[k] - o.FN[k] - o.FT[k];
-#pragma unroll
-        for (int k = 0; k < 3; k++) T[k] = T[k] + Rp * o.NxFT[k];
-        if (update && orig < qo) record(qo, o.FT, o.VT);
-      }
-    };
-    walk_as_j<SWEEP>(A, meta, s, orig, c, cx, cy, cz, visit_j, [&]() {
-#pragma unroll
-      for (int k = 0; k < 3; k++) F[k] = F[k] + iF[k];
-#pragma unroll
-      for (int k = 0; k < 3; k++) T[k] = T[k] + iT[k];
-    });
-
-    // ---- records of pairs the sweep did not visit are kept as they were
-    if (update) {
-      const int nold = A.Hr.cnt[orig];
-      for (int r = 0; r < nold; r++) {
-        const int q2 = A.Hr.key[(size_t)orig * A.Hr.cap + r];
-        if (!cells_adjacent(P, c, A.cell_of_orig[q2])) {
-          double ft[3], vt[3];
-          hist_read(A.Hr, orig, r, ft, vt);
-          record(q2, ft, vt);
-        }
-      }
-      A.Hw.cnt[orig] = hw_n < A.Hw.cap ? hw_n : A.Hw.cap;
-      if (overflow) {
-        // the pass is re-run with larger tables; stop everything after it
-        atomicExch(&A.cnt->overflow, 1);
-        atomicCAS(&A.cnt->abort_tag, 0, A.tag + 1);
-        atomicExch(&A.cnt->abort, 1);
-      }
-      need = hw_n;
-    }
-
-    // ---- a = F/m, alpha = T/I (src/MForces.f90:330-333) + epilogue
-    double acc[3], alp[3];
-#pragma unroll
-    for (int k = 0; k < 3; k++) acc[k] = F[k] * inv_m;
-#pragma unroll
-    for (int k = 0; k < 3; k++) alp[k] = T[k] * inv_i;
-
-    if (EPI == EPI_STORE) {
-      A.tgt.ax[orig] = acc[0]; A.tgt.ay[orig] = acc[1]; A.tgt.az[orig] = acc[2];
-      A.tgt.lx[orig] = alp[0]; A.tgt.ly[orig] = alp[1]; A.tgt.lz[orig] = alp[2];
-    } else if (EPI == EPI_PREDICT) {
-      // src/MDEM.f90:296-331: AB predictor from x(t), v(t), w(t) (the values
-      // this pass gathered) and the ring, then store (v,a,alpha)(t).
-      const StateArrays& Q = A.part;
-      const StateArrays& R = A.pred;
-      Q.ax[orig] = acc[0]; Q.ay[orig] = acc[1]; Q.az[orig] = acc[2];
-      Q.lx[orig] = alp[0]; Q.ly[orig] = alp[1]; Q.lz[orig] = alp[2];
-      double sv[3] = {0.0, 0.0, 0.0}, sa[3] = {0.0, 0.0, 0.0}, sl[3] = {0.0, 0.0, 0.0};
-      const size_t n = (size_t)A.n;
-      for (int k = 0; k < P.nprev; k++) {
-        const double ABk = P.ab[k];
-        const double* rg = A.ring + (size_t)A.rm.phys[k] * 9 * n + orig;
-#pragma unroll
-        for (int d = 0; d < 3; d++) sv[d] = sv[d] + ABk * rg[d * n];
-#pragma unroll
-        for (int d = 0; d < 3; d++) sa[d] = sa[d] + ABk * rg[(3 + d) * n];
-#pragma unroll
-        for (int d = 0; d < 3; d++) sl[d] = sl[d] + ABk * rg[(6 + d) * n];
-      }
-      double xr[3], vr[3], wr[3];
-#pragma unroll
-      for (int d = 0; d < 3; d++) xr[d] = xp[d] + P.ab0 * vp[d] + sv[d];
-#pragma unroll
-      for (int d = 0; d < 3; d++) vr[d] = vp[d] + P.ab0 * acc[d] + sa[d];
-#pragma unroll
-      for (int d = 0; d < 3; d++) wr[d] = wp[d] + P.ab0 * alp[d] + sl[d];
-#pragma unroll
-      for (int d = 0; d < 3; d++)
-        if (P.pbc[d]) xr[d] = xr[d] - P.lbox[d] * fnint(xr[d] * P.inv_lbox[d]);
-      R.px[orig] = xr[0]; R.py[orig] = xr[1]; R.pz[orig] = xr[2];
-      R.vx[orig] = vr[0]; R.vy[orig] = vr[1]; R.vz[orig] = vr[2];
-      R.wx[orig] = wr[0]; R.wy[orig] = wr[1]; R.wz[orig] = wr[2];
-      if (P.nprev > 0) {
-        double* rg = A.ring + (size_t)A.rm.phys[P.nprev] * 9 * n + orig;
-#pragma unroll
-        for (int d = 0; d < 3; d++) rg[d * n] = vp[d];
-#pragma unroll
-        for (int d = 0; d < 3; d++) rg[(3 + d) * n] = acc[d];
-#pragma unroll
-        for (int d = 0; d < 3; d++) rg[(6 + d) * n] = alp[d];
-      }
-    } else {  // EPI_CORRECT, src/MDEM.f90:340-367
-      const StateArrays& Q = A.part;
-      const StateArrays& R = A.pred;
-      R.ax[orig] = acc[0]; R.ay[orig] = acc[1]; R.az[orig] = acc[2];
-      R.lx[orig] = alp[0]; R.ly[orig] = alp[1]; R.lz[orig] = alp[2];
-      double sv[3] = {0.0, 0.0, 0.0}, sa[3] = {0.0, 0.0, 0.0}, sl[3] = {0.0, 0.0, 0.0};
-      const size_t n = (size_t)A.n;
-      for (int k = 0; k < P.nprev; k++) {
-        const double AMk = P.am[k];
-        const double* rg = A.ring + (size_t)A.rm.phys[k] * 9 * n + orig;
-#pragma unroll
-        for (int d = 0; d < 3; d++) sv[d] = sv[d] + AMk * rg[d * n];
-#pragma unroll
-        for (int d = 0; d < 3; d++) sa[d] = sa[d] + AMk * rg[(3 + d) * n];
-#pragma unroll
-        for (int d = 0; d < 3; d++) sl[d] = sl[d] + AMk * rg[(6 + d) * n];
-      }
-      double x[3] = {Q.px[orig], Q.py[orig], Q.pz[orig]};
-      double v[3] = {Q.vx[orig], Q.vy[orig], Q.vz[orig]};
-      double w[3] = {Q.wx[orig], Q.wy[orig], Q.wz[orig]};
-#pragma unroll
-      for (int d = 0; d < 3; d++) x[d] = x[d] + P.am0 * vp[d] + sv[d];
-#pragma unroll
-      for (int d = 0; d < 3; d++) v[d] = v[d] + P.am0 * acc[d] + sa[d];
-#pragma unroll
-      for (int d = 0; d < 3; d++) w[d] = w[d] + P.am0 * alp[d] + sl[d];
-#pragma unroll
-      for (int d = 0; d < 3; d++)
-        if (P.pbc[d]) x[d] = x[d] - P.lbox[d] * fnint(x[d] * P.inv_lbox[d]);
-      Q.px[orig] = x[0]; Q.py[orig] = x[1]; Q.pz[orig] = x[2];
-      Q.vx[orig] = v[0]; Q.vy[orig] = v[1]; Q.vz[orig] = v[2];
-      Q.wx[orig] = w[0]; Q.wy[orig] = w[1]; Q.wz[orig] = w[2];
-      bool out = false;
-#pragma unroll
-      for (int d = 0; d < 3; d++) {
-        const double h = 0.5 * P.lbox[d];
-        out = out || (x[d] > h) || (x[d] < -h);
-      }
-      if (out) atomicAdd(&A.cnt->escaped, 1ull);
-    }
-  }
-  n_col = warp_sum_u64(n_col);
-  n_pc = warp_sum_u64(n_pc);
-  n_wc = warp_sum_u64(n_wc);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) need = max(need, __shfl_down_sync(0xffffffffu, need, o));
-  if ((threadIdx.x & 31) == 0) {
-    if (need) atomicMax(&A.cnt->need_capacity, need);
-    if (n_col) atomicAdd(A.update ? &A.cnt->ncol_pending : &A.cnt->ncol, n_col);
-    if (n_pc) atomicAdd(&A.cnt->pair_contacts, n_pc);
-    if (n_wc) atomicAdd(&A.cnt->wall_contacts, n_wc);
-  }
-}
-
-// ---------------------------------------------------------------------------
-// small per-particle kernels (original index order)
-
-// K2 screening: candidate lists.  For every particle whose row must be
-// (re)built -- all particles on a full rebuild, else those whose 27-cell
-// neighbourhood gained or lost a particle in this pass, and rows that
-// overflowed -- sweep the cells exactly as ComputeAccelerations does
-// (src/MForces.f90:173-272) and keep, in sweep order, the particles within
-// MinDij + skin.  The force kernels apply the exact FP64 overlap test to these
-// candidates, so contact sets, orientation and order stay the reference's.
-// Every thread also publishes its particle's slot for the orig -> slot map.
-struct ScreenRange {
-  int b, e, code;  // code: bit 0..5 image (2 bits per axis, biased by 1), bit 6: p is "j"
-};
-
-__device__ __forceinline__ int range_code(int wx, int wy, int wz, bool p_is_j) {
-  return (wx + 1) | ((wy + 1) << 2) | ((wz + 1) << 4) | (p_is_j ? 64 : 0);
-}
-
-template <bool PP>
-__global__ void __launch_bounds__(256, 4) k_screen(const DevParams* __restrict__ Pp, int n,
-                                                   const double4* __restrict__ pos,
-                                                   const int* __restrict__ comp,
-                                                   const int* __restrict__ slot_cell,
-                                                   const int* __restrict__ order,
-                                                   const int* __restrict__ cs, ContactLists L,
-                                                   Counters* __restrict__ cnt) {
-  if (cnt->abort) return;
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  const DevParams& P = *Pp;
-  const int orig = order[s];
-  L.slot_of_orig[orig] = s;
-  const int c = slot_cell[s];
-  const bool full = rebuild_due(P, cnt);
-  if (!full && !L.repair[c] && L.meta[orig].x >= 0) return;
-
-  const int nx = P.nx, ny = P.ny;
-  const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
-  // ---- the ranges, in sweep order: loop 1, then loop 2
-  ScreenRange R[29];
-  int nr = 0, own_j = -1;
-  sweep_cells_as_i(P, cs, s, c, cx, cy, cz, [&](int b, int e, int wx, int wy, int wz) {
-    R[nr++] = ScreenRange{b, e, range_code(wx, wy, wz, false)};
-  });
-  const int nr1 = nr;
-  sweep_cells_as_j(
-      P, cs, s, c, cx, cy, cz,
-      [&](int b, int e, int wx, int wy, int wz) {
-        R[nr++] = ScreenRange{b, e, range_code(wx, wy, wz, true)};
-      },
-      [&]() { own_j = nr - 1; });
-
-  // ---- one loop over all candidates
-  const double4 p4 = pos[s];
-  if (full) L.ref_pos[orig] = p4;
-  const int cp = PP ? 0 : comp[s];
-  const double skin = P.vl_skin;
-  const double maxd = sqrt(P.max_min_dij_sq) + skin;
-  const double maxsq = maxd * maxd;
-  int* out = L.slot + (size_t)orig * KC;
-  int m = 0, n1 = 0, n2b = 0;
-  for (int r = 0; r < nr; r++) {
-    const ScreenRange rr = R[r];
-    const bool pj = rr.code & 64;
-    const int sg = pj ? -1 : 1;
-    const int nxi = sg * -(((rr.code) & 3) - 1);
-    const int nyi = sg * -(((rr.code >> 2) & 3) - 1);
-    const int nzi = sg * -(((rr.code >> 4) & 3) - 1);
-    for (int t = rr.b; t < rr.e; t++) {
-      const double4 q4 = pos[t];
-      double Rij[3];
-      Rij[0] = pj ? p4.x - q4.x : q4.x - p4.x;
-      Rij[0] = min_image(Rij[0], P.pbc[0], P.lbox[0], P.inv_lbox[0], nxi);
-      if (Rij[0] * Rij[0] >= maxsq) continue;
-      Rij[1] = pj ? p4.y - q4.y : q4.y - p4.y;
-      Rij[1] = min_image(Rij[1], P.pbc[1], P.lbox[1], P.inv_lbox[1], nyi);
-      Rij[2] = pj ? p4.z - q4.z : q4.z - p4.z;
-      Rij[2] = min_image(Rij[2], P.pbc[2], P.lbox[2], P.inv_lbox[2], nzi);
-      const double DijSq = sumsq3(Rij);
-      const int cq = PP ? 0 : comp[t];
-      // candidates: within MinDij + skin (a superset of the exact overlaps)
-      double md = PP ? p4.w + q4.w : sqrt(Material<PP>::min_dij_sq(P, cp, p4.w, cq, q4.w));
-      md = md + skin;
-      if (md * md - DijSq > 0.0) {
-        if (m < KC) out[m] = order[t];
-        m++;
-      }
-    }
-    if (r == nr1 - 1) n1 = m;
-    if (r == own_j) n2b = m - n1;
-  }
-  L.meta[orig] = m <= KC ? make_int4(n1, n2b, m - n1 - n2b, 0) : make_int4(-1, 0, 0, 0);
-  if (m > KC) atomicAdd(&cnt->list_overflow, 1);
-}
-
-// This pass's exact contact rows: the candidates of every particle that
-// pass the overlap test DeltaDijSq > 0 of the force kernels (same operations,
-// src/MForces.f90:209-224), in candidate order, as traversal slots.  A light
-// kernel, so that the heavy contact arithmetic only meets real contacts.
-template <bool PP>
-__global__ void __launch_bounds__(256) k_filter(const DevParams* __restrict__ Pp, int n,
-                                                const double4* __restrict__ pos,
-                                                const int* __restrict__ comp,
-                                                const int* __restrict__ order, ContactLists L,
-                                                const Counters* __restrict__ cnt) {
-  if (cnt->abort) return;
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  const DevParams& P = *Pp;
-  const int orig = order[s];
-  const int4 meta = L.meta[orig];
-  if (meta.x < 0) {
-    L.xmeta[s] = meta;  // overflowed row: the force kernel sweeps the cells
-    return;
-  }
-  const double4 p4 = pos[s];
-  const int cp = PP ? 0 : comp[s];
-  const int* in = L.slot + (size_t)orig * KC;
-  int* out = L.xslot + (size_t)s * KC;
-  const int total = meta.x + meta.y + meta.z;
-  int m = 0, n1 = 0, n2b = 0;
-  for (int k = 0; k < total; k++) {
-    const int t = L.slot_of_orig[in[k]];
-    const double4 q4 = pos[t];
-    const bool pj = k >= meta.x;  // loop 2: p is "j", Rij = xp - xq
-    double Rij[3] = {pj ? p4.x - q4.x : q4.x - p4.x, pj ? p4.y - q4.y : q4.y - p4.y,
-                     pj ? p4.z - q4.z : q4.z - p4.z};
-#pragma unroll
-    for (int d = 0; d < 3; d++)
-      if (P.pbc[d]) Rij[d] = Rij[d] - P.lbox[d] * fnint(Rij[d] * P.inv_lbox[d]);
-    const double DijSq = sumsq3(Rij);
-    const int cq = PP ? 0 : comp[t];
-    const double Delta = pj ? Material<PP>::min_dij_sq(P, cq, q4.w, cp, p4.w) - DijSq
-                            : Material<PP>::min_dij_sq(P, cp, p4.w, cq, q4.w) - DijSq;
-    if (Delta > 0.0) out[m++] = t;
-    if (k == meta.x - 1) n1 = m;
-    if (k == meta.x + meta.y - 1) n2b = m - n1;
-  }
-  if (meta.x == 0) n1 = 0;
-  if (meta.y == 0) n2b = 0;
-  L.xmeta[s] = make_int4(n1, n2b, m - n1 - n2b, 0);
-}
-
-// A particle entered or left each dirty cell: the rows of every particle in
-// its 27-cell neighbourhood are rebuilt in this pass.
-__global__ void k_mark_repair(const DevParams* __restrict__ Pp, ContactLists L,
-                              const Counters* __restrict__ cnt) {
-  if (cnt->abort) return;
-  const DevParams& P = *Pp;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= P.ncell || !L.dirty[c]) return;
-  const int nx = P.nx, ny = P.ny, nz = P.nz;
-  const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
-  int xi, xf, yi, yf, zi, zf;
-  axis_range(cx, nx, P.pbc[0], xi, xf);
-  axis_range(cy, ny, P.pbc[1], yi, yf);
-  axis_range(cz, nz, P.pbc[2], zi, zf);
-  for (int kz = zi; kz <= zf; kz++)
-    for (int ky = yi; ky <= yf; ky++)
-      for (int kx = xi; kx <= xf; kx++) {
-        const int jx = axis_wrap(cx + kx, nx, P.pbc[0]);
-        const int jy = axis_wrap(cy + ky, ny, P.pbc[1]);
-        const int jz = axis_wrap(cz + kz, nz, P.pbc[2]);
-        L.repair[jx + nx * (jy + ny * jz)] = 1;
-      }
-}
-
-// AB predictor (src/MDEM.f90:297-331) as a streaming pass over particles in
-// index order: Predicted = x(t) + AB0*v + sum_k AB(k)*Previous(ipc(k)), PBC
-// wrap, then (v, a, alpha)(t) into the spare ring slot (the slot the
-// reference's cshift makes ipc(1)).
-__global__ void __launch_bounds__(256) k_predict(const DevParams* __restrict__ Pp, int n,
-                                                 StateArrays Q, StateArrays R,
-                                                 double* __restrict__ ring, RingMap rm,
-                                                 const Counters* __restrict__ cnt) {
-  if (cnt->abort) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const DevParams& P = *Pp;
-  const size_t N = (size_t)n;
-  const double x[3] = {Q.px[i], Q.py[i], Q.pz[i]};
-  const double v[3] = {Q.vx[i], Q.vy[i], Q.vz[i]};
-  const double w[3] = {Q.wx[i], Q.wy[i], Q.wz[i]};
-  const double a[3] = {Q.ax[i], Q.ay[i], Q.az[i]};
-  const double l[3] = {Q.lx[i], Q.ly[i], Q.lz[i]};
-  double sv[3] = {0.0, 0.0, 0.0}, sa[3] = {0.0, 0.0, 0.0}, sl[3] = {0.0, 0.0, 0.0};
-  for (int k = 0; k < P.nprev; k++) {
-    const double ABk = P.ab[k];
-    const double* rg = ring + (size_t)rm.phys[k] * 9 * N + i;
-#pragma unroll
-    for (int d = 0; d < 3; d++) sv[d] = sv[d] + ABk * rg[d * N];
-#pragma unroll
-    for (int d = 0; d < 3; d++) sa[d] = sa[d] + ABk * rg[(3 + d) * N];
-#pragma unroll
-    for (int d = 0; d < 3; d++) sl[d] = sl[d] + ABk * rg[(6 + d) * N];
-  }
-  double xr[3], vr[3], wr[3];
-#pragma unroll
-  for (int d = 0; d < 3; d++) xr[d] = x[d] + P.ab0 * v[d] + sv[d];
-#pragma unroll
-  for (int d = 0; d < 3; d++) vr[d] = v[d] + P.ab0 * a[d] + sa[d];
-#pragma unroll
-  for (int d = 0; d < 3; d++) wr[d] = w[d] + P.ab0 * l[d] + sl[d];
-#pragma unroll
-  for (int d = 0; d < 3; d++)
-    if (P.pbc[d]) xr[d] = xr[d] - P.lbox[d] * fnint(xr[d] * P.inv_lbox[d]);
-  R.px[i] = xr[0]; R.py[i] = xr[1]; R.pz[i] = xr[2];
-  R.vx[i] = vr[0]; R.vy[i] = vr[1]; R.vz[i] = vr[2];
-  R.wx[i] = wr[0]; R.wy[i] = wr[1]; R.wz[i] = wr[2];
-  if (P.nprev > 0) {
-    double* rg = ring + (size_t)rm.phys[P.nprev] * 9 * N + i;
-#pragma unroll
-    for (int d = 0; d < 3; d++) rg[d * N] = v[d];
-#pragma unroll
-    for (int d = 0; d < 3; d++) rg[(3 + d) * N] = a[d];
-#pragma unroll
-    for (int d = 0; d < 3; d++) rg[(6 + d) * N] = l[d];
-  }
-}
-
-// AM corrector (src/MDEM.f90:340-367) as a streaming pass: x = x + AM0*v~ +
-// sum_k AM(k)*Previous(ipc(k)) (ipc after the shift), likewise v and omega,
-// PBC wrap; counts the particles that left the box (src/MDEM.f90:624-625).
-__global__ void __launch_bounds__(256) k_correct(const DevParams* __restrict__ Pp, int n,
-                                                 StateArrays Q, StateArrays R,
-                                                 const double* __restrict__ ring, RingMap rm,
-                                                 Counters* __restrict__ cnt) {
-  if (cnt->abort) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  bool out = false;
-  if (i < n) {
-    const DevParams& P = *Pp;
-    const size_t N = (size_t)n;
-    double sv[3] = {0.0, 0.0, 0.0}, sa[3] = {0.0, 0.0, 0.0}, sl[3] = {0.0, 0.0, 0.0};
-    for (int k = 0; k < P.nprev; k++) {
-      const double AMk = P.am[k];
-      const double* rg = ring + (size_t)rm.phys[k] * 9 * N + i;
-#pragma unroll
-      for (int d = 0; d < 3; d++) sv[d] = sv[d] + AMk * rg[d * N];
-#pragma unroll
-      for (int d = 0; d < 3; d++) sa[d] = sa[d] + AMk * rg[(3 + d) * N];
-#pragma unroll
-      for (int d = 0; d < 3; d++) sl[d] = sl[d] + AMk * rg[(6 + d) * N];
-    }
-    const double vp[3] = {R.vx[i], R.vy[i], R.vz[i]};
-    const double ap[3] = {R.ax[i], R.ay[i], R.az[i]};
-    const double lp[3] = {R.lx[i], R.ly[i], R.lz[i]};
-    double x[3] = {Q.px[i], Q.py[i], Q.pz[i]};
-    double v[3] = {Q.vx[i], Q.vy[i], Q.vz[i]};
-    double w[3] = {Q.wx[i], Q.wy[i], Q.wz[i]};
-#pragma unroll
-    for (int d = 0; d < 3; d++) x[d] = x[d] + P.am0 * vp[d] + sv[d];
-#pragma unroll
-    for (int d = 0; d < 3; d++) v[d] = v[d] + P.am0 * ap[d] + sa[d];
-#pragma unroll
-    for (int d = 0; d < 3; d++) w[d] = w[d] + P.am0 * lp[d] + sl[d];
-#pragma unroll
-    for (int d = 0; d < 3; d++)
-      if (P.pbc[d]) x[d] = x[d] - P.lbox[d] * fnint(x[d] * P.inv_lbox[d]);
-    Q.px[i] = x[0]; Q.py[i] = x[1]; Q.pz[i] = x[2];
-    Q.vx[i] = v[0]; Q.vy[i] = v[1]; Q.vz[i] = v[2];
-    Q.wx[i] = w[0]; Q.wy[i] = w[1]; Q.wz[i] = w[2];
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      const double h = 0.5 * P.lbox[d];
-      out = out || (x[d] > h) || (x[d] < -h);
-    }
-  }
-  const unsigned long long e = warp_sum_u64(out ? 1ull : 0ull);
-  if ((threadIdx.x & 31) == 0 && e) atomicAdd(&cnt->escaped, e);
 }
 
 // ring store of MoveParticlesEuler (src/MDEM.f90:266-271): (v,a,alpha) -> slot
@@ -1080,6 +420,611 @@ __global__ void k_observables(const DevParams* __restrict__ Pp, int n, StateArra
   }
   if (threadIdx.x == 0)
     for (int k = 0; k < 8; k++) partial[blockIdx.x * 8 + k] = sh[k][0];
+}
+
+
+// ---------------------------------------------------------------------------
+// K1: linked cell lists
+
+// DistributeParticles3D (src/MCells.f90:542-564): every particle is prepended
+// to its cell in index order; the counting sort gives each cell in
+// decreasing index, which is linked here.  head[] starts at -1.
+__global__ void k_link_init(int n, const int* __restrict__ order,
+                            const int* __restrict__ slot_cell, const int* __restrict__ cell_start,
+                            int* __restrict__ head, int* __restrict__ next,
+                            int* __restrict__ cell_of) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const int p = order[s], c = slot_cell[s];
+  next[p] = s + 1 < cell_start[c + 1] ? order[s + 1] : -1;
+  if (s == cell_start[c]) head[c] = p;
+  cell_of[p] = c;
+}
+
+// Forget a prepared cell transition (arrival lists and dirty flags of
+// dirty list `par`); the count itself is reset by the host afterwards.
+__global__ void k_discard(CellLists L, int par, const Counters* __restrict__ cnt) {
+  const int m = cnt->n_dirty[par];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    const int c = L.dlist[par][i];
+    L.arr_head[c] = -1;
+    L.dflag[c] = 0;
+  }
+}
+
+// Copies of a state for the pass kernel (positions + radius, velocities) by
+// original index, the cell of every particle under the next assignment and
+// the displacement from the last pass's positions `Xlast` (NULL: none).
+template <class V4, class W2>
+__global__ void __launch_bounds__(256) k_prepare(const DevParams* __restrict__ Pp, int n,
+                                                 StateArrays src, const double* __restrict__ radius,
+                                                 double4* X, V4* __restrict__ v4,
+                                                 W2* __restrict__ w2, const double4* Xlast,
+                                                 const int* __restrict__ cell_cur, CellLists L,
+                                                 int par, Counters* cnt) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  double d2 = 0.0;
+  if (p < n) {
+    const DevParams& P = *Pp;
+    const double x[3] = {src.px[p], src.py[p], src.pz[p]};
+    if (Xlast) {
+      const double4 o = Xlast[p];
+      const double y[3] = {o.x, o.y, o.z};
+      d2 = disp2(P, x, y);
+      if (!(d2 <= 1e300)) d2 = 1e300;  // a non-finite state forces a full rebuild
+    }
+    X[p] = make_double4(x[0], x[1], x[2], radius[p]);
+    v4[p] = mk_v4<V4>(src.vx[p], src.vy[p], src.vz[p], src.wx[p]);
+    w2[p] = mk_w2<W2>(src.wy[p], src.wz[p]);
+    L.mflag[p] = 0;
+    note_cell(L, cnt, par, p, cell_cur[p], current_cell(P, x[0], x[1], x[2]));
+  }
+  publish_disp(cnt, d2);
+}
+
+// Relink, phase 1: every dirty cell of list `par` drops the particles that
+// left it (TransferParticle's unlink, src/MCells.f90:747-774).  Thread 0
+// also closes the previous pass's bookkeeping and decides whether this pass
+// rebuilds every candidate row.
+__global__ void k_relink1(const DevParams* __restrict__ Pp, CellLists L, int par, int n,
+                          int update, Counters* cnt) {
+  if (cnt->abort) return;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid == 0) {
+    const DevParams& P = *Pp;
+    cnt->n_repair = 0;
+    cnt->n_dirty[par ^ 1] = 0;
+    cnt->movers = cnt->movers_pending;
+    cnt->movers_pending = 0ull;
+    if (cnt->ncol_pending) {  // the previous history-updating pass completed
+      cnt->ncol += cnt->ncol_pending;
+      cnt->ncol_pending = 0ull;
+    }
+    cnt->pair_contacts = 0ull;
+    cnt->wall_contacts = 0ull;
+    for (int w = 0; w < NWM; w++) cnt->wall_fn[w] = 0.0;
+    if (update) cnt->need_capacity = 0;
+    else cnt->escaped = 0ull;  // escapes are counted by the current step's corrector
+    const double d = __longlong_as_double((long long)cnt->disp_max);
+    cnt->disp_max = 0ull;
+    const double acc = cnt->disp_acc + d;
+    const int full = cnt->force_full != 0 || !(acc <= P.vl_thr);
+    cnt->full_due = full;
+    cnt->disp_acc = full ? 0.0 : acc;
+    if (full) cnt->force_full = 0;
+  }
+  const int m = cnt->n_dirty[par];
+  const int* __restrict__ cell_new = L.cell[par];
+  for (int i = tid; i < m; i += gridDim.x * blockDim.x) {
+    const int c = L.dlist[par][i];
+    int prev = -1, first = -1, q = L.head[c];
+    int guard = 0;
+    while (q != -1) {
+      if (++guard > n) {
+        atomicExch(&cnt->list_error, 1);
+        atomicExch(&cnt->abort, 1);
+        return;
+      }
+      const int nq = L.next[q];
+      if (cell_new[q] == c) {
+        if (prev == -1) first = q;
+        else L.next[prev] = q;
+        prev = q;
+      }
+      q = nq;
+    }
+    if (prev != -1) L.next[prev] = -1;
+    L.head[c] = first;
+  }
+}
+
+// Relink, phase 2: every dirty cell prepends its arrivals in decreasing index
+// (AddParticle, src/MCells.f90:684-698, applied in increasing index order)
+// and marks its 27-cell neighbourhood for candidate-row repair.
+__global__ void k_relink2(const DevParams* __restrict__ Pp, CellLists L, int par, int n,
+                          Counters* cnt) {
+  if (cnt->abort) return;
+  const DevParams& P = *Pp;
+  const int m = cnt->n_dirty[par];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    const int c = L.dlist[par][i];
+    int sh = -1, tail = -1, a = L.arr_head[c];
+    int guard = 0;
+    while (a != -1) {
+      if (++guard > n) {
+        atomicExch(&cnt->list_error, 1);
+        atomicExch(&cnt->abort, 1);
+        return;
+      }
+      const int an = L.arr_next[a];
+      L.mflag[a] = 0;
+      if (sh == -1) {
+        sh = tail = a;
+        L.next[a] = -1;
+      } else if (a > sh) {
+        L.next[a] = sh;
+        sh = a;
+      } else {
+        int q = sh;
+        for (int g2 = 0; L.next[q] != -1 && L.next[q] > a && g2 < guard; g2++) q = L.next[q];
+        L.next[a] = L.next[q];
+        L.next[q] = a;
+        if (L.next[a] == -1) tail = a;
+      }
+      a = an;
+    }
+    L.arr_head[c] = -1;
+    if (sh != -1) {
+      L.next[tail] = L.head[c];
+      L.head[c] = sh;
+    }
+    L.dflag[c] = 0;
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
+    int xi, xf, yi, yf, zi, zf;
+    axis_range(cx, nx, P.pbc[0], xi, xf);
+    axis_range(cy, ny, P.pbc[1], yi, yf);
+    axis_range(cz, nz, P.pbc[2], zi, zf);
+    for (int kz = zi; kz <= zf; kz++)
+      for (int ky = yi; ky <= yf; ky++)
+        for (int kx = xi; kx <= xf; kx++) {
+          const int jc = axis_wrap(cx + kx, nx, P.pbc[0]) +
+                         nx * (axis_wrap(cy + ky, ny, P.pbc[1]) +
+                               ny * axis_wrap(cz + kz, nz, P.pbc[2]));
+          if (atomicExch(&L.rflag[jc], 1) == 0) L.rlist[atomicAdd(&cnt->n_repair, 1)] = jc;
+        }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K2: candidate rows
+
+// The row of particle p (cell c), built by one warp.  Lane L < 27 owns the
+// neighbour cell at offset (L%3-1, L/3%3-1, L/9-1); lane 13 (own cell) walks
+// the part of the list after p (loop 1), lane 27 the part before p (loop 2).
+// Segments are ordered as the sweep meets them: loop 1 = own cell after p,
+// then the half-shell cells (offset index kx + Nx*(ky + Ny*kz) > 0,
+// AddAllNeighbours3D src/MCells.f90:456) in FirstNeighbour order, i.e.
+// descending (kz, ky, kx); loop 2 = the cells whose half shell holds c, and
+// p's own cell, in ascending cell index (the order of the sweep's outer
+// loop), own cell before p's own block.
+template <bool PP>
+__device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int c,
+                                          const double4* __restrict__ X,
+                                          const int* __restrict__ comp,
+                                          const int* __restrict__ head,
+                                          const int* __restrict__ next, const Rows& R,
+                                          Counters* cnt, int tag) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
+  const double4 p4 = X[p];
+  const int cp = PP ? 0 : comp[p];
+  int start = -1, stop = -1, order = 1 << 20, jc = 0x7fffffff;
+  int loop = 0;
+  if (lane < 27) {
+    const int d[3] = {lane % 3 - 1, (lane / 3) % 3 - 1, lane / 9 - 1};
+    const int cc[3] = {cx, cy, cz};
+    const int N[3] = {nx, ny, nz};
+    bool ok = true;
+    int w[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      int j = cc[k] + d[k];
+      if (P.pbc[k]) {
+        if (j == N[k]) j = 0;
+        if (j == -1) j = N[k] - 1;
+      } else if (j < 0 || j >= N[k]) {
+        ok = false;
+      }
+      w[k] = j;
+    }
+    const int lex = d[0] + 3 * d[1] + 9 * d[2];
+    if (lane == 13) {
+      start = next[p];
+      loop = 1;
+      order = 0;
+    } else if (ok) {
+      jc = w[0] + nx * (w[1] + ny * w[2]);
+      start = head[jc];
+      if (lex > 0) {
+        loop = 1;
+        order = 1 + (13 - lex);
+      } else {
+        loop = 2;
+      }
+    }
+  } else if (lane == 27) {
+    start = head[c];
+    stop = p;
+    loop = 2;
+    jc = c;
+  }
+  // loop-2 segments in ascending cell index
+  {
+    int rank = 0;
+    for (int l = 0; l < 28; l++) {
+      const int ol = __shfl_sync(FULL, loop, l);
+      const int jl = __shfl_sync(FULL, jc, l);
+      if (ol == 2 && jl < jc) rank++;
+    }
+    if (loop == 2) order = 14 + rank;
+  }
+  const double skin = P.vl_skin;
+  auto is_cand = [&](int q) -> bool {
+    const double4 q4 = X[q];
+    double Rij[3] = {q4.x - p4.x, q4.y - p4.y, q4.z - p4.z};
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+      if (P.pbc[k]) Rij[k] = Rij[k] - P.lbox[k] * fnint(Rij[k] * P.inv_lbox[k]);
+    const double DijSq = sumsq3(Rij);
+    double md;
+    if (PP) md = p4.w + q4.w;
+    else md = sqrt(Material<PP>::min_dij_sq(P, cp, p4.w, comp[q], q4.w));
+    md = md + skin;
+    return md * md - DijSq > 0.0;
+  };
+  // pass 1: count
+  int count = 0;
+  bool bad = false;
+  {
+    int q = start, guard = 0;
+    while (q != -1 && q != stop) {
+      if (++guard > n) {
+        bad = true;
+        break;
+      }
+      if (is_cand(q)) count++;
+      q = next[q];
+    }
+  }
+  if (__any_sync(FULL, bad)) {
+    if (lane == 0) {
+      atomicExch(&cnt->list_error, 1);
+      set_abort(cnt, tag);
+    }
+    return;
+  }
+  int off = 0, n1 = 0, n2b = 0, n2a = 0;
+  const int own_order = __shfl_sync(FULL, order, 27);
+  for (int l = 0; l < 32; l++) {
+    const int ol = __shfl_sync(FULL, order, l);
+    const int cl = __shfl_sync(FULL, count, l);
+    const int pl = __shfl_sync(FULL, loop, l);
+    if (ol < order) off += cl;
+    if (pl == 1) n1 += cl;
+    else if (pl == 2 && ol <= own_order) n2b += cl;
+    else if (pl == 2) n2a += cl;
+  }
+  const int m = n1 + n2b + n2a;
+  if (m > R.kc) {
+    if (lane == 0) {
+      atomicMax(&cnt->need_kc, m);
+      atomicExch(&cnt->row_overflow, 1);
+      set_abort(cnt, tag);
+      R.meta[p] = 0;
+    }
+    return;
+  }
+  // pass 2: write
+  {
+    int q = start, k = off;
+    while (q != -1 && q != stop) {
+      if (is_cand(q)) R.cand[(size_t)(k++) * n + p] = q;
+      q = next[q];
+    }
+  }
+  if (lane == 0) R.meta[p] = n1 | (n2b << META_BITS) | (n2a << (2 * META_BITS));
+}
+
+// Rows of the particles of every repair cell (one warp per cell).
+template <bool PP>
+__global__ void __launch_bounds__(256) k_screen_repair(const DevParams* __restrict__ Pp, int n,
+                                                       const double4* __restrict__ X,
+                                                       const int* __restrict__ comp,
+                                                       CellLists L, Rows R, Counters* cnt,
+                                                       int tag) {
+  // the flags of the listed cells are cleared even when nothing is built
+  // (a stopped sequence, or a full rebuild that rebuilds every row anyway)
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int m = cnt->n_repair;
+  const bool skip = cnt->abort != 0 || cnt->full_due != 0;
+  for (int r = warp; r < m; r += nwarps) {
+    const int c = L.rlist[r];
+    if (!skip) {
+      int p = L.head[c], guard = 0;
+      while (p != -1) {
+        if (++guard > n) {
+          if (lane == 0) {
+            atomicExch(&cnt->list_error, 1);
+            set_abort(cnt, tag);
+          }
+          break;
+        }
+        build_row<PP>(*Pp, n, p, c, X, comp, L.head, L.next, R, cnt, tag);
+        p = L.next[p];
+      }
+    }
+    if (lane == 0) L.rflag[c] = 0;
+  }
+}
+
+// Every row, when the pass is due for a full rebuild (one warp per particle).
+template <bool PP>
+__global__ void __launch_bounds__(256) k_screen_full(const DevParams* __restrict__ Pp, int n,
+                                                     const double4* __restrict__ X,
+                                                     const int* __restrict__ comp,
+                                                     const int* __restrict__ cell_cur,
+                                                     CellLists L, Rows R, Counters* cnt, int tag) {
+  if (cnt->abort || !cnt->full_due) return;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int p = warp; p < n; p += nwarps)
+    build_row<PP>(*Pp, n, p, cell_cur[p], X, comp, L.head, L.next, R, cnt, tag);
+}
+
+// ---------------------------------------------------------------------------
+// K2+K4: the FP64 pass kernel (exact order)
+
+template <bool PP, int EPI>
+__global__ void __launch_bounds__(128, 4) k_pass_fp64(PassArgs<double4, double2> A) {
+  if (A.cnt->abort) return;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long n_col = 0, n_pc = 0, n_wc = 0;
+  int need = 0;
+  double d2 = 0.0;
+  if (p < A.n) {
+    const DevParams& P = *A.P;
+    const int n = A.n;
+    const int c = A.cell_cur[p];
+    const double4 p4 = A.X[p];
+    const double xp[3] = {p4.x, p4.y, p4.z};
+    const double Rp = p4.w;
+    const double4 pv4 = A.v4[p];
+    const double2 pw2 = A.w2[p];
+    const double vp[3] = {pv4.x, pv4.y, pv4.z};
+    const double wp[3] = {pv4.w, pw2.x, pw2.y};
+    const int cp = PP ? 0 : A.comp[p];
+    double inv_m, inv_i, eff_m;
+    Material<PP>::self(P, cp, Rp, inv_m, inv_i, eff_m);
+    int n1, n2b, n2a;
+    unpack_meta(A.meta[p], n1, n2b, n2a);
+    const double half_dt = A.half_dt;
+    const bool update = A.update != 0;
+    int hw_n = 0;
+    bool overflow = false;
+
+    double iF[3], iT[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < 3; k++) iF[k] = eff_m * P.gravity[k];
+
+    auto record = [&](int partner, const double ft[3], const double vt[3]) {
+      if (hw_n < A.Hw.cap)
+        hist_write(A.Hw, p, hw_n, partner, ft, vt);
+      else
+        overflow = true;
+      hw_n++;
+    };
+    // Rij = xb - xa (minimum image, src/MForces.f90:209-217) and the overlap
+    // test DeltaDijSq = MinDijSq - DijSq > 0 of the pair (a = "i", b = "j")
+    auto geometry = [&](const double xa[3], const double4 xb, double Rij[3]) -> double {
+      Rij[0] = xb.x - xa[0];
+      Rij[1] = xb.y - xa[1];
+      Rij[2] = xb.z - xa[2];
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+        if (P.pbc[k]) Rij[k] = Rij[k] - P.lbox[k] * fnint(Rij[k] * P.inv_lbox[k]);
+      return sumsq3(Rij);
+    };
+    auto contact_i = [&](int q, double4 q4) -> bool {
+      double Rij[3];
+      const double DijSq = geometry(xp, q4, Rij);
+      const int cq = PP ? 0 : A.comp[q];
+      return Material<PP>::min_dij_sq(P, cp, Rp, cq, q4.w) - DijSq > 0.0;
+    };
+    auto contact_j = [&](int q, double4 q4) -> bool {
+      double Rij[3];
+      const double qx[3] = {q4.x, q4.y, q4.z};
+      const double DijSq = geometry(qx, make_double4(xp[0], xp[1], xp[2], Rp), Rij);
+      const int cq = PP ? 0 : A.comp[q];
+      return Material<PP>::min_dij_sq(P, cq, q4.w, cp, Rp) - DijSq > 0.0;
+    };
+
+    // p is "i", q is "j" (src/MForces.f90:199-272)
+    auto visit_i = [&](int q) {
+      const double4 q4 = A.X[q];
+      double Rij[3];
+      const double DijSq = geometry(xp, q4, Rij);
+      const int cq = PP ? 0 : A.comp[q];
+      const double Delta = Material<PP>::min_dij_sq(P, cp, Rp, cq, q4.w) - DijSq;
+      PairPar pp;
+      Material<PP>::pair(P, cp, Rp, cq, q4.w, pp);
+      const double4 qv4 = A.v4[q];
+      const double2 qw2 = A.w2[q];
+      const double vq[3] = {qv4.x, qv4.y, qv4.z};
+      const double wq[3] = {qv4.w, qw2.x, qw2.y};
+      const int lo = p < q ? p : q, hi = p < q ? q : p;
+      double FT0[3] = {0.0, 0.0, 0.0}, VT0[3] = {0.0, 0.0, 0.0};
+      const int r = hist_find(A.Hr, lo, hi);
+      const bool contacting = r >= 0;
+      if (contacting) hist_read(A.Hr, lo, r, FT0, VT0);
+      if (!contacting) n_col++;
+      n_pc++;
+      ContactOut o;
+      pair_contact(Rij, DijSq, Delta, pp, Rp, vp, wp, q4.w, vq, wq, half_dt, contacting, FT0, VT0,
+                   o);
+#pragma unroll
+      for (int k = 0; k < 3; k++) iF[k] = iF[k] + o.FN[k] + o.FT[k];
+      double RN[3], tq[3];
+#pragma unroll
+      for (int k = 0; k < 3; k++) RN[k] = Rp * o.N[k];
+      cross3(RN, o.FT, tq);
+#pragma unroll
+      for (int k = 0; k < 3; k++) iT[k] = iT[k] + tq[k];
+      if (update && p < q) record(q, o.FT, o.VT);
+    };
+
+    // ---- loop 1: own cell after p, then the half-shell cells
+    walk_segment(A.cand, A.X, n, p, 0, n1, contact_i, visit_i);
+
+    // ---- walls (src/MForces.f90:274-314)
+    for (int w = 0; w < P.nw; w++) {
+      const dem_wall& W = P.walls[w];
+      const int wi = p * P.nw + w;
+      bool contacting = A.Hr.wflag[wi] != 0;
+      double FT0[3] = {0.0, 0.0, 0.0}, VT0[3] = {0.0, 0.0, 0.0};
+      if (contacting) {
+        const double2* v = A.Hr.wval + (size_t)wi * 3;
+        double2 a = v[0], b = v[1], d = v[2];
+        FT0[0] = a.x; FT0[1] = a.y; FT0[2] = b.x;
+        VT0[0] = b.y; VT0[1] = d.x; VT0[2] = d.y;
+      }
+      double Dij, Nij[3], Qji[3];
+      bool ov = false;
+      if (W.shape == DEM_WALL_RECTANGLE) ov = overlap_rect(P, W, xp, Rp, Dij, Nij, Qji);
+      if (ov) {
+        n_wc++;
+        const double Delta = Rp * Rp - Dij * Dij;
+        const double dn = Dij - Rp;
+        double DispN[3], wqv[3], Vij[3], ro[3], cr[3], VijC[3], Rw[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) DispN[k] = dn * Nij[k];
+        cross3(W.omega, Qji, wqv);
+#pragma unroll
+        for (int k = 0; k < 3; k++) Vij[k] = W.velocity[k] + wqv[k] - vp[k];
+#pragma unroll
+        for (int k = 0; k < 3; k++) ro[k] = Rp * wp[k];
+        cross3(ro, Nij, cr);
+#pragma unroll
+        for (int k = 0; k < 3; k++) VijC[k] = Vij[k] - cr[k];
+#pragma unroll
+        for (int k = 0; k < 3; k++) Rw[k] = W.position[k] + Qji[k] - xp[k];
+        PairPar pp;
+        Material<PP>::wall(P, cp, Rp, w, pp);
+        ContactOut o;
+        common_calc(Rw, Nij, DispN, Vij, VijC, Delta, half_dt, contacting, FT0, VT0, pp.kn, pp.yn,
+                    pp.kt, pp.yt, pp.mu_sq, o);
+#pragma unroll
+        for (int k = 0; k < 3; k++) iF[k] = iF[k] + o.FN[k] + o.FT[k];
+        double RN[3], tq[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) RN[k] = Rp * o.N[k];
+        cross3(RN, o.FT, tq);
+#pragma unroll
+        for (int k = 0; k < 3; k++) iT[k] = iT[k] + tq[k];
+        atomicAdd(&A.cnt->wall_fn[w], sqrt(sumsq3(o.FN)));
+        if (update) {
+          A.Hw.wflag[wi] = 1;
+          double2* v = A.Hw.wval + (size_t)wi * 3;
+          v[0] = make_double2(o.FT[0], o.FT[1]);
+          v[1] = make_double2(o.FT[2], o.VT[0]);
+          v[2] = make_double2(o.VT[1], o.VT[2]);
+        }
+      } else if (update) {
+        A.Hw.wflag[wi] = 0;
+      }
+    }
+
+    // ---- loop 2: p as "j"; contributions in the order the sweep reaches
+    // the "i" particle, own block (Force(i) = Force(i) + iForce) at p's turn.
+    double F[3] = {0.0, 0.0, 0.0}, T[3] = {0.0, 0.0, 0.0};
+    auto visit_j = [&](int q) {
+      const double4 q4 = A.X[q];
+      double Rij[3];
+      const double qx[3] = {q4.x, q4.y, q4.z};
+      const double DijSq = geometry(qx, make_double4(xp[0], xp[1], xp[2], Rp), Rij);
+      const int cq = PP ? 0 : A.comp[q];
+      const double Delta = Material<PP>::min_dij_sq(P, cq, q4.w, cp, Rp) - DijSq;
+      PairPar pp;
+      Material<PP>::pair(P, cq, q4.w, cp, Rp, pp);
+      const double4 qv4 = A.v4[q];
+      const double2 qw2 = A.w2[q];
+      const double vq[3] = {qv4.x, qv4.y, qv4.z};
+      const double wq[3] = {qv4.w, qw2.x, qw2.y};
+      const int lo = p < q ? p : q, hi = p < q ? q : p;
+      double FT0[3] = {0.0, 0.0, 0.0}, VT0[3] = {0.0, 0.0, 0.0};
+      const int r = hist_find(A.Hr, lo, hi);
+      const bool contacting = r >= 0;
+      if (contacting) hist_read(A.Hr, lo, r, FT0, VT0);
+      ContactOut o;
+      pair_contact(Rij, DijSq, Delta, pp, q4.w, vq, wq, Rp, vp, wp, half_dt, contacting, FT0,
+                   VT0, o);
+#pragma unroll
+      for (int k = 0; k < 3; k++) F[k] = F[k] - o.FN[k] - o.FT[k];
+#pragma unroll
+      for (int k = 0; k < 3; k++) T[k] = T[k] + Rp * o.NxFT[k];
+      if (update && p < q) record(q, o.FT, o.VT);
+    };
+    walk_segment(A.cand, A.X, n, p, n1, n1 + n2b, contact_j, visit_j);
+#pragma unroll
+    for (int k = 0; k < 3; k++) F[k] = F[k] + iF[k];
+#pragma unroll
+    for (int k = 0; k < 3; k++) T[k] = T[k] + iT[k];
+    walk_segment(A.cand, A.X, n, p, n1 + n2b, n1 + n2b + n2a, contact_j, visit_j);
+
+    // ---- records of pairs the sweep did not visit are kept as they were
+    if (update) {
+      const int nold = A.Hr.cnt[p];
+      for (int r = 0; r < nold; r++) {
+        const int q2 = A.Hr.key[(size_t)p * A.Hr.cap + r];
+        if (!cells_adjacent(P, c, A.cell_cur[q2])) {
+          double ft[3], vt[3];
+          hist_read(A.Hr, p, r, ft, vt);
+          record(q2, ft, vt);
+        }
+      }
+      A.Hw.cnt[p] = hw_n < A.Hw.cap ? hw_n : A.Hw.cap;
+      if (overflow) {
+        // the pass is launched again with larger tables; stop what follows
+        atomicExch(&A.cnt->overflow, 1);
+        set_abort(A.cnt, A.tag);
+      }
+      need = hw_n;
+    }
+
+    // ---- a = F/m, alpha = T/I (src/MForces.f90:330-333) + epilogue
+    double acc[3], alp[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) acc[k] = F[k] * inv_m;
+#pragma unroll
+    for (int k = 0; k < 3; k++) alp[k] = T[k] * inv_i;
+    epilogue<EPI>(A, p, xp, Rp, vp, wp, acc, alp, c, d2);
+  }
+  n_col = warp_sum_u64(n_col);
+  n_pc = warp_sum_u64(n_pc);
+  n_wc = warp_sum_u64(n_wc);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) need = max(need, __shfl_down_sync(0xffffffffu, need, o));
+  if ((threadIdx.x & 31) == 0) {
+    if (need) atomicMax(&A.cnt->need_capacity, need);
+    if (n_col) atomicAdd(A.update ? &A.cnt->ncol_pending : &A.cnt->ncol, n_col);
+    if (n_pc) atomicAdd(&A.cnt->pair_contacts, n_pc);
+    if (n_wc) atomicAdd(&A.cnt->wall_contacts, n_wc);
+  }
+  if (EPI != EPI_STORE) publish_disp(A.cnt, d2);
 }
 
 }  // namespace dem

@@ -52,15 +52,27 @@ struct dem_ctx {
   double* radius = nullptr;
   int* comp = nullptr;
 
+  // initial distribution (counting sort) buffers
   SortedArrays S{};
   int* cell_start = nullptr;
   int* cell_cnt = nullptr;
-  int* cell_of_orig = nullptr;
   int *a_cell = nullptr, *a_loc = nullptr, *a_orig = nullptr, *t_orig = nullptr;
   unsigned *a_key = nullptr, *t_key = nullptr;
   int* scan_bsum = nullptr;
   int n_tiles = 0;
-  ContactLists CL{};
+
+  // linked cell lists, candidate rows and the per-pass copies of the two
+  // sides (0 = Particle, 1 = Predicted): positions + radius, velocities
+  // (double4/double2 in FP64 mode, float4/float2 in mixed mode)
+  CellLists L{};
+  Rows rows{};
+  int kc = 32;
+  double4* X[2] = {nullptr, nullptr};
+  void* v4[2] = {nullptr, nullptr};
+  void* w2[2] = {nullptr, nullptr};
+  int par = 0;         // L.cell[par] is the assignment the lists hold
+  int prepared = -1;   // side whose copies + next assignment are ready (-1: none)
+  int last_side = -1;  // side of the last pass (its copies are intact)
 
   History H[2]{};
   int hcur = 0;  // H[hcur] holds the current records
@@ -79,7 +91,7 @@ struct dem_ctx {
   double time = 0.0;
 
   // graphs: one per (phase of the ring/history rotation)
-  cudaGraphExec_t graph[8] = {};
+  cudaGraphExec_t graph[20] = {};
   int graph_steps = 0;
   long long graph_kernels = 0;  // kernels in one captured chunk
   bool graph_valid = false;
@@ -210,6 +222,26 @@ void resolve_events(dem_ctx* c) {
 
 unsigned blocks_for(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 
+void free_lists(dem_ctx* c) {
+  CellLists& L = c->L;
+  int** f[] = {&L.head, &L.next, &L.cell[0], &L.cell[1], &L.arr_head, &L.arr_next, &L.mflag,
+               &L.dflag, &L.rflag, &L.dlist[0], &L.dlist[1], &L.rlist};
+  for (int** q : f) {
+    cudaFree(*q);
+    *q = nullptr;
+  }
+  cudaFree(c->rows.cand);
+  cudaFree(c->rows.meta);
+  c->rows = Rows{};
+  for (int b = 0; b < 2; b++) {
+    cudaFree(c->X[b]);
+    cudaFree(c->v4[b]);
+    cudaFree(c->w2[b]);
+    c->X[b] = nullptr;
+    c->v4[b] = c->w2[b] = nullptr;
+  }
+}
+
 void free_state(dem_ctx* c) {
   cudaFree(c->staging);
   c->staging = nullptr;
@@ -217,28 +249,15 @@ void free_state(dem_ctx* c) {
   cudaFree(c->ring);
   cudaFree(c->radius);
   cudaFree(c->comp);
-  cudaFree(c->S.pos);
-  cudaFree(c->S.v4);
-  cudaFree(c->S.w2);
-  cudaFree(c->S.comp);
   cudaFree(c->S.orig);
   cudaFree(c->S.cell);
-  cudaFree(c->cell_of_orig);
   cudaFree(c->a_cell);
   cudaFree(c->a_loc);
   cudaFree(c->a_orig);
   cudaFree(c->t_orig);
   cudaFree(c->a_key);
   cudaFree(c->t_key);
-  cudaFree(c->CL.slot);
-  cudaFree(c->CL.meta);
-  cudaFree(c->CL.slot_of_orig);
-  cudaFree(c->CL.ref_pos);
-  cudaFree(c->CL.dirty);
-  cudaFree(c->CL.repair);
-  cudaFree(c->CL.xslot);
-  cudaFree(c->CL.xmeta);
-  c->CL = ContactLists{};
+  free_lists(c);
   for (int b = 0; b < 2; b++) {
     cudaFree(c->H[b].cnt);
     cudaFree(c->H[b].key);
@@ -251,7 +270,7 @@ void free_state(dem_ctx* c) {
   c->state_block = c->ring = c->radius = nullptr;
   c->comp = nullptr;
   c->S = SortedArrays{};
-  c->cell_of_orig = c->a_cell = c->a_loc = c->a_orig = c->t_orig = nullptr;
+  c->a_cell = c->a_loc = c->a_orig = c->t_orig = nullptr;
   c->a_key = c->t_key = nullptr;
 }
 
@@ -320,64 +339,72 @@ StateArrays make_state(double* base, size_t n) {
 }
 
 // ---------------------------------------------------------------------------
-// K1: rebuild the cell order from the positions in `src`
+// K1: initial distribution (DistributeParticles3D) of the Particle positions
 
-int rebuild_cells(dem_ctx* c, const StateArrays& src, bool initial) {
+constexpr int LIST_BLOCKS = 148;      // relink / repair kernels (grid-stride)
+constexpr int FULL_BLOCKS = 148 * 8;  // full candidate-row rebuild (grid-stride)
+
+int init_cells(dem_ctx* c) {
   const int n = c->n;
   const int ncell = c->hp.ncell;
-  if (n == 0) return DEM_OK;
+  CellLists& L = c->L;
+  CK(cudaMemsetAsync(L.head, 0xFF, sizeof(int) * (size_t)ncell, c->stream));
+  CK(cudaMemsetAsync(L.arr_head, 0xFF, sizeof(int) * (size_t)ncell, c->stream));
+  CK(cudaMemsetAsync(L.dflag, 0, sizeof(int) * (size_t)ncell, c->stream));
+  CK(cudaMemsetAsync(L.rflag, 0, sizeof(int) * (size_t)ncell, c->stream));
+  if (n > 0) CK(cudaMemsetAsync(L.mflag, 0, sizeof(int) * (size_t)n, c->stream));
   CK(cudaMemsetAsync(c->cell_cnt, 0, sizeof(int) * (size_t)ncell, c->stream));
-  if (initial) {
+  if (n > 0) {
     launch(c, "cell_assign", k_assign, blocks_for(n, 256), 256, (const DevParams*)c->dp, n, 1,
-           (const double*)src.px, (const double*)src.py, (const double*)src.pz,
+           (const double*)c->P.px, (const double*)c->P.py, (const double*)c->P.pz,
            (const int*)c->S.orig, (const int*)c->S.cell, c->cell_cnt, c->a_cell, c->a_loc,
            c->a_key, c->a_orig, c->cnt);
-  } else {
-    CK(cudaMemsetAsync(c->CL.dirty, 0, (size_t)ncell, c->stream));
-    launch(c, "cell_assign", k_assign_track, blocks_for(n, 256), 256, (const DevParams*)c->dp, n,
-           (const double*)src.px, (const double*)src.py, (const double*)src.pz,
-           (const int*)c->S.orig, (const int*)c->S.cell, c->cell_cnt, c->a_cell, c->a_loc,
-           c->a_key, c->a_orig, c->CL, c->cnt);
+    launch(c, "scan_tiles", k_scan_tiles, (unsigned)c->n_tiles, SCAN_THREADS,
+           (const int*)c->cell_cnt, ncell, c->cell_start, c->scan_bsum, (const Counters*)c->cnt);
+    launch(c, "scan_bsums", k_scan_bsums, 1u, SCAN_THREADS, c->scan_bsum, c->n_tiles,
+           c->cell_start, ncell, (const Counters*)c->cnt);
+    launch(c, "scan_add", k_scan_add, blocks_for(ncell, 256), 256, c->cell_start, ncell,
+           (const int*)c->scan_bsum, (const Counters*)c->cnt);
+    launch(c, "cell_scatter", k_scatter, blocks_for(n, 256), 256, n, (const int*)c->a_cell,
+           (const int*)c->a_loc, (const unsigned*)c->a_key, (const int*)c->a_orig,
+           (const int*)c->cell_start, c->t_key, c->t_orig, (const Counters*)c->cnt);
+    launch(c, "cell_sort", k_cellsort, blocks_for(ncell, 128), 128, ncell,
+           (const int*)c->cell_start, c->t_key, c->t_orig, c->S.orig, c->S.cell, L.cell[c->par],
+           (const Counters*)c->cnt);
+    launch(c, "link_init", k_link_init, blocks_for(n, 256), 256, n, (const int*)c->S.orig,
+           (const int*)c->S.cell, (const int*)c->cell_start, L.head, L.next, L.cell[c->par]);
   }
-  launch(c, "scan_tiles", k_scan_tiles, (unsigned)c->n_tiles, SCAN_THREADS,
-         (const int*)c->cell_cnt, ncell, c->cell_start, c->scan_bsum, (const Counters*)c->cnt);
-  launch(c, "scan_bsums", k_scan_bsums, 1u, SCAN_THREADS, c->scan_bsum, c->n_tiles, c->cell_start,
-         ncell, (const Counters*)c->cnt);
-  launch(c, "scan_add", k_scan_add, blocks_for(ncell, 256), 256, c->cell_start, ncell,
-         (const int*)c->scan_bsum, (const Counters*)c->cnt);
-  launch(c, "cell_scatter", k_scatter, blocks_for(n, 256), 256, n, (const int*)c->a_cell,
-         (const int*)c->a_loc, (const unsigned*)c->a_key, (const int*)c->a_orig,
-         (const int*)c->cell_start, c->t_key, c->t_orig, (const Counters*)c->cnt);
-  launch(c, "cell_sort", k_cellsort, blocks_for(ncell, 128), 128, ncell, (const int*)c->cell_start,
-         c->t_key, c->t_orig, c->S.orig, c->S.cell, c->cell_of_orig, (const Counters*)c->cnt);
-  if (c->precision == DEM_PREC_MIXED) {
-    timed(c, "gather_mixed", [&]() {
-      mixed_gather(c->M, c->pp, c->dp, n, src, c->radius, c->comp, c->S, c->cnt, c->stream);
-    });
-  } else if (c->pp) {
-    launch(c, "gather", k_gather<true>, blocks_for(n, 256), 256, (const DevParams*)c->dp, n, src,
-           (const double*)c->radius, (const int*)c->comp, c->S, (const Counters*)c->cnt);
-  } else {
-    launch(c, "gather", k_gather<false>, blocks_for(n, 256), 256, (const DevParams*)c->dp, n, src,
-           (const double*)c->radius, (const int*)c->comp, c->S, (const Counters*)c->cnt);
-  }
+  // no transition pending; the first pass builds every candidate row
+  CK(cudaMemsetAsync(&c->cnt->n_dirty[0], 0, 3 * sizeof(int), c->stream));
+  CK(cudaMemsetAsync(&c->cnt->movers_pending, 0, sizeof(unsigned long long), c->stream));
+  CK(cudaMemsetAsync(&c->cnt->disp_max, 0, sizeof(unsigned long long) + sizeof(double),
+                     c->stream));
+  const int one = 1;
+  CK(cudaMemcpyAsync(&c->cnt->force_full, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  c->prepared = -1;
+  c->last_side = -1;
   return DEM_OK;
 }
 
 // ---------------------------------------------------------------------------
-// K2+K4: one force pass
+// one pass: copies of the side (if not prepared), relink, candidate rows,
+// pass kernel
 
-int launch_force(dem_ctx* c, const StateArrays& tgt, bool update, double dt, int epi,
-                 const RingMap& rm, int tag) {
-  ForceArgs A;
+template <class V4, class W2>
+PassArgs<V4, W2> pass_args(dem_ctx* c, int side, bool update, double dt, const RingMap& rm,
+                           int tag, const StateArrays& tgt) {
+  PassArgs<V4, W2> A;
   A.P = c->dp;
   A.n = c->n;
-  A.S = c->S;
-  A.cell_start = c->cell_start;
-  A.cell_of_orig = c->cell_of_orig;
-  A.cl_slot = c->CL.xslot;
-  A.cl_meta = c->CL.xmeta;
-  A.slot_of_orig = c->CL.slot_of_orig;
+  A.X = c->X[side];
+  A.v4 = (const V4*)c->v4[side];
+  A.w2 = (const W2*)c->w2[side];
+  A.comp = c->comp;
+  A.cand = c->rows.cand;
+  A.meta = c->rows.meta;
+  A.cell_cur = c->L.cell[c->par];
+  A.L = c->L;
+  A.par_nxt = c->par ^ 1;
   A.Hr = c->H[c->hcur];
   A.Hw = c->H[c->hcur ^ 1];
   A.update = update ? 1 : 0;
@@ -385,28 +412,96 @@ int launch_force(dem_ctx* c, const StateArrays& tgt, bool update, double dt, int
   A.tgt = tgt;
   A.part = c->P;
   A.pred = c->Pr;
+  A.Xn = c->X[side ^ 1];
+  A.v4n = (V4*)c->v4[side ^ 1];
+  A.w2n = (W2*)c->w2[side ^ 1];
   A.ring = c->ring;
   A.rm = rm;
   A.cnt = c->cnt;
   A.tag = tag;
-  unsigned g = blocks_for(c->n, 128);
+  return A;
+}
+
+void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, const RingMap& rm,
+                        int tag) {
+  if (c->n == 0) return;
+  const StateArrays& tgt = side ? c->Pr : c->P;
   if (c->precision == DEM_PREC_MIXED) {
-    timed(c, "force_mixed", [&]() { mixed_force(c->M, c->pp, epi, A, c->hcur, c->stream); });
-    c->launches++;  // list-driven + overflow launches
-    return DEM_OK;
+    auto A = pass_args<float4, float2>(c, side, update, dt, rm, tag, tgt);
+    timed(c, "pass_mixed", [&]() { mixed_pass(c->M, c->pp, epi, A, c->hcur, c->stream); });
+    c->launches++;
+    return;
   }
-#define FORCE_CASE(PPV, E)                                                  \
-  {                                                                         \
-    launch(c, "force_fp64", k_force_fp64<PPV, E, false>, g, 128, A);        \
-    launch(c, "force_fp64_sweep", k_force_fp64<PPV, E, true>, g, 128, A);   \
+  auto A = pass_args<double4, double2>(c, side, update, dt, rm, tag, tgt);
+  const unsigned g = blocks_for(c->n, 128);
+#define PASS_CASE(PPV)                                                                  \
+  do {                                                                                  \
+    if (epi == EPI_PREDICT)                                                             \
+      launch(c, "pass_fp64", k_pass_fp64<PPV, EPI_PREDICT>, g, 128, A);                 \
+    else if (epi == EPI_CORRECT)                                                        \
+      launch(c, "pass_fp64", k_pass_fp64<PPV, EPI_CORRECT>, g, 128, A);                 \
+    else                                                                                \
+      launch(c, "pass_fp64", k_pass_fp64<PPV, EPI_STORE>, g, 128, A);                   \
+  } while (0)
+  if (c->pp) PASS_CASE(true);
+  else PASS_CASE(false);
+#undef PASS_CASE
+}
+
+// Copies of `side` for the pass kernel and the cell transition towards its
+// positions (after forgetting a transition prepared for the other side).
+int prepare_side(dem_ctx* c, int side) {
+  const int nxt = c->par ^ 1;
+  launch(c, "discard", k_discard, (unsigned)LIST_BLOCKS, 256, c->L, nxt, (const Counters*)c->cnt);
+  CK(cudaMemsetAsync(&c->cnt->n_dirty[nxt], 0, sizeof(int), c->stream));
+  if (c->n > 0) {
+    const StateArrays& src = side ? c->Pr : c->P;
+    const double4* Xlast = c->last_side >= 0 ? c->X[c->last_side] : nullptr;
+    if (c->precision == DEM_PREC_MIXED)
+      launch(c, "prepare", k_prepare<float4, float2>, blocks_for(c->n, 256), 256,
+             (const DevParams*)c->dp, c->n, src, (const double*)c->radius, c->X[side],
+             (float4*)c->v4[side], (float2*)c->w2[side], Xlast, (const int*)c->L.cell[c->par],
+             c->L, nxt, c->cnt);
+    else
+      launch(c, "prepare", k_prepare<double4, double2>, blocks_for(c->n, 256), 256,
+             (const DevParams*)c->dp, c->n, src, (const double*)c->radius, c->X[side],
+             (double4*)c->v4[side], (double2*)c->w2[side], Xlast, (const int*)c->L.cell[c->par],
+             c->L, nxt, c->cnt);
   }
-  if (c->pp) {
-    FORCE_CASE(true, EPI_STORE)
-  } else {
-    FORCE_CASE(false, EPI_STORE)
-  }
-#undef FORCE_CASE
+  c->prepared = side;
   return DEM_OK;
+}
+
+void launch_screen_full(dem_ctx* c, int side, int tag) {
+  if (c->n == 0) return;
+  const unsigned g = std::min(blocks_for((long long)c->n * 32, 256), (unsigned)FULL_BLOCKS);
+  if (c->pp)
+    launch(c, "screen_full", k_screen_full<true>, g, 256, (const DevParams*)c->dp, c->n,
+           (const double4*)c->X[side], (const int*)c->comp, (const int*)c->L.cell[c->par], c->L,
+           c->rows, c->cnt, tag);
+  else
+    launch(c, "screen_full", k_screen_full<false>, g, 256, (const DevParams*)c->dp, c->n,
+           (const double4*)c->X[side], (const int*)c->comp, (const int*)c->L.cell[c->par], c->L,
+           c->rows, c->cnt, tag);
+}
+
+// relink towards the prepared assignment, then the candidate rows
+void pass_lists(dem_ctx* c, int side, bool update, int tag) {
+  const int b = c->par ^ 1;
+  launch(c, "relink1", k_relink1, (unsigned)LIST_BLOCKS, 256, (const DevParams*)c->dp, c->L, b,
+         c->n, update ? 1 : 0, c->cnt);
+  launch(c, "relink2", k_relink2, (unsigned)LIST_BLOCKS, 256, (const DevParams*)c->dp, c->L, b,
+         c->n, c->cnt);
+  c->par = b;
+  if (c->pp)
+    launch(c, "screen_repair", k_screen_repair<true>, (unsigned)LIST_BLOCKS, 256,
+           (const DevParams*)c->dp, c->n, (const double4*)c->X[side], (const int*)c->comp, c->L,
+           c->rows, c->cnt, tag);
+  else
+    launch(c, "screen_repair", k_screen_repair<false>, (unsigned)LIST_BLOCKS, 256,
+           (const DevParams*)c->dp, c->n, (const double4*)c->X[side], (const int*)c->comp, c->L,
+           c->rows, c->cnt, tag);
+  launch_screen_full(c, side, tag);
 }
 
 RingMap current_map(dem_ctx* c) {
@@ -426,17 +521,6 @@ void rotate_ring(dem_ctx* c) {
   c->ringmap[np] = oldest;
 }
 
-int reset_pass_counters(dem_ctx* c, bool update) {
-  // per-pass statistics; Ncol and the escape count accumulate
-  CK(cudaMemsetAsync(&c->cnt->pair_contacts, 0, 3 * sizeof(unsigned long long), c->stream));
-  CK(cudaMemsetAsync(&c->cnt->wall_fn[0], 0, sizeof(double) * NWM, c->stream));
-  CK(cudaMemsetAsync(&c->cnt->list_overflow, 0, sizeof(int), c->stream));
-  if (update) CK(cudaMemsetAsync(&c->cnt->need_capacity, 0, sizeof(int), c->stream));
-  // escapes are counted by the corrector of the current step only
-  if (!update) CK(cudaMemsetAsync(&c->cnt->escaped, 0, sizeof(unsigned long long), c->stream));
-  return DEM_OK;
-}
-
 int read_counters(dem_ctx* c) {
   CK(cudaMemcpyAsync(c->hcnt, c->cnt, sizeof(Counters), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -446,69 +530,83 @@ int read_counters(dem_ctx* c) {
   return DEM_OK;
 }
 
-// every candidate row is rebuilt in the next pass (new state or cells)
-int invalidate_candidates(dem_ctx* c) {
-  if (c->n > 0) CK(cudaMemsetAsync(c->CL.meta, 0xFF, sizeof(int4) * (size_t)c->n, c->stream));
-  CK(cudaMemsetAsync(&c->cnt->force_rebuild, 0xFF, sizeof(int), c->stream));
-  return DEM_OK;
-}
-
-// forget a failed (overflowed) history-updating pass: flags and its Ncol
+// forget a stopped pass: status words, its partial counts and its Ncol
 int clear_abort(dem_ctx* c) {
-  CK(cudaMemsetAsync(&c->cnt->ncol_pending, 0, sizeof(unsigned long long), c->stream));
-  CK(cudaMemsetAsync(&c->cnt->overflow, 0, 4 * sizeof(int), c->stream));
+  Counters* d = c->cnt;
+  CK(cudaMemsetAsync(&d->ncol_pending, 0, sizeof(unsigned long long), c->stream));
+  CK(cudaMemsetAsync(&d->pair_contacts, 0, 2 * sizeof(unsigned long long), c->stream));
+  CK(cudaMemsetAsync(&d->overflow, 0, 4 * sizeof(int), c->stream));
+  CK(cudaMemsetAsync(&d->row_overflow, 0, 2 * sizeof(int), c->stream));
+  CK(cudaMemsetAsync(&d->wall_fn[0], 0, sizeof(double) * NWM, c->stream));
   return DEM_OK;
 }
 
-// A force pass that may update the history: on capacity overflow the tables
-// grow and the force kernel is re-run (the pass only writes fresh outputs,
-// so re-running it from the unchanged inputs gives the same result).
-int force_pass(dem_ctx* c, const StateArrays& src, const StateArrays& tgt, bool update, double dt,
-               int epi, const RingMap& rm, bool check, int tag) {
-  int st = reset_pass_counters(c, update);
-  if (st) return st;
-  st = rebuild_cells(c, src, false);
-  if (st) return st;
-  if (c->n > 0) {
-    // rows of particles near a cell that gained/lost a particle are rebuilt
-    CK(cudaMemsetAsync(c->CL.repair, 0, (size_t)c->hp.ncell, c->stream));
-    launch(c, "mark_repair", k_mark_repair, blocks_for(c->hp.ncell, 256), 256,
-           (const DevParams*)c->dp, c->CL, (const Counters*)c->cnt);
-    if (c->pp)
-      launch(c, "screen", k_screen<true>, blocks_for(c->n, 256), 256, (const DevParams*)c->dp,
-             c->n, (const double4*)c->S.pos, (const int*)c->S.comp, (const int*)c->S.cell,
-             (const int*)c->S.orig, (const int*)c->cell_start, c->CL, c->cnt);
-    else
-      launch(c, "screen", k_screen<false>, blocks_for(c->n, 256), 256, (const DevParams*)c->dp,
-             c->n, (const double4*)c->S.pos, (const int*)c->S.comp, (const int*)c->S.cell,
-             (const int*)c->S.orig, (const int*)c->cell_start, c->CL, c->cnt);
-    if (c->pp)
-      launch(c, "filter", k_filter<true>, blocks_for(c->n, 256), 256, (const DevParams*)c->dp,
-             c->n, (const double4*)c->S.pos, (const int*)c->S.comp, (const int*)c->S.orig, c->CL,
-             (const Counters*)c->cnt);
-    else
-      launch(c, "filter", k_filter<false>, blocks_for(c->n, 256), 256, (const DevParams*)c->dp,
-             c->n, (const double4*)c->S.pos, (const int*)c->S.comp, (const int*)c->S.orig, c->CL,
-             (const Counters*)c->cnt);
-  }
+// longer candidate rows: the rows are rebuilt by the next full rebuild
+int grow_rows(dem_ctx* c, int need) {
+  if (need > KC_MAX) return fail(c, DEM_ERR_CAPACITY, "candidate rows longer than 1023");
+  int kc = std::max(need, c->kc + c->kc / 2);
+  kc = std::min((kc + 7) / 8 * 8, KC_MAX);
+  CK(cudaStreamSynchronize(c->stream));
+  cudaFree(c->rows.cand);
+  c->rows.cand = nullptr;
+  CK(cudaMalloc(&c->rows.cand, sizeof(int) * (size_t)std::max(c->n, 1) * kc));
+  c->kc = kc;
+  c->rows.kc = kc;
+  drop_graphs(c);
+  return DEM_OK;
+}
+
+// A pass whose relink ran and whose rows or pass kernel stopped (capacity):
+// grow what overflowed and launch the rest of the pass again.  The pass
+// kernel only writes fresh outputs and idempotent transition records, so a
+// launch that stopped half way can be repeated.
+int finish_pass(dem_ctx* c, int side, bool update, double dt, int epi, const RingMap& rm,
+                int tag) {
   for (int attempt = 0;; attempt++) {
-    st = launch_force(c, tgt, update, dt, epi, rm, tag);
+    int st = read_counters(c);
     if (st) return st;
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail(c, e, "force kernel launch");
-    if (!update || !check) break;
-    st = read_counters(c);
-    if (st) return st;
-    if (!c->hcnt->overflow) break;
-    if (attempt >= 8) return fail(c, DEM_ERR_CAPACITY, "history capacity cannot be grown");
-    int need = c->hcnt->need_capacity;
+    const Counters h = *c->hcnt;
+    if (!h.abort) return DEM_OK;
+    if (h.list_error) return fail(c, DEM_ERR_STATE, "cell lists inconsistent (walk bound hit)");
+    if (attempt >= 8) return fail(c, DEM_ERR_CAPACITY, "capacity cannot be grown");
     st = clear_abort(c);
     if (st) return st;
-    st = grow_history(c, need);
-    if (st) return st;
-    st = reset_pass_counters(c, update);
+    if (h.overflow) {
+      st = grow_history(c, std::max(h.need_capacity, c->hcap + 1));
+      if (st) return st;
+    }
+    if (h.row_overflow) {
+      st = grow_rows(c, h.need_kc);
+      if (st) return st;
+      const int one = 1;
+      CK(cudaMemcpyAsync(&c->cnt->full_due, &one, sizeof(int), cudaMemcpyHostToDevice,
+                         c->stream));
+      CK(cudaMemsetAsync(&c->cnt->disp_acc, 0, sizeof(double), c->stream));
+      launch_screen_full(c, side, tag);
+    }
+    launch_pass_kernel(c, side, update, dt, epi, rm, tag);
+  }
+}
+
+// One force pass (ComputeAccelerations) on `side` (0 = Particle, 1 =
+// Predicted) with the integrator epilogue `epi`.  check: recover from a
+// capacity overflow here (not possible inside a captured graph).
+int force_pass(dem_ctx* c, int side, bool update, double dt, int epi, const RingMap& rm,
+               bool check, int tag) {
+  if (c->prepared != side) {
+    int st = prepare_side(c, side);
     if (st) return st;
   }
+  pass_lists(c, side, update, tag);
+  launch_pass_kernel(c, side, update, dt, epi, rm, tag);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(c, e, "pass kernel launch");
+  if (check) {
+    int st = finish_pass(c, side, update, dt, epi, rm, tag);
+    if (st) return st;
+  }
+  c->last_side = side;
+  c->prepared = epi == EPI_PREDICT ? 1 : epi == EPI_CORRECT ? 0 : -1;
   if (update) c->hcur ^= 1;
   return DEM_OK;
 }
@@ -521,24 +619,17 @@ int validate_ready(dem_ctx* c) {
   return DEM_OK;
 }
 
-// MoveParticles(step) (src/MDEM.f90:285-369)
-int move_particles_impl(dem_ctx* c, int step, bool check, int tag) {
-  const int n = c->n;
+// MoveParticles(step) (src/MDEM.f90:285-369); tags 2k (pass 1), 2k+1 (pass 2)
+int move_particles_impl(dem_ctx* c, int step, bool check, int k) {
   RingMap rm = current_map(c);
-  // force pass @ x(t) with history update; a(t), alpha(t) -> Particle
-  int st = force_pass(c, c->P, c->P, true, c->params.time_step, EPI_STORE, rm, check, tag);
+  // force pass @ x(t) with history update, a(t) -> Particle, AB predictor
+  int st = force_pass(c, 0, true, c->params.time_step, EPI_PREDICT, rm, check, 2 * k);
   if (st) return st;
-  launch(c, "predict", k_predict, blocks_for(n, 256), 256, (const DevParams*)c->dp, n, c->P,
-         c->Pr, c->ring, rm, (const Counters*)c->cnt);
   rotate_ring(c);
   c->time = (double)step * c->params.time_step;
   rm = current_map(c);
-  // force pass @ prediction, history read only; a~, alpha~ -> Predicted
-  st = force_pass(c, c->Pr, c->Pr, false, c->params.time_step, EPI_STORE, rm, false, tag);
-  if (st) return st;
-  launch(c, "correct", k_correct, blocks_for(n, 256), 256, (const DevParams*)c->dp, n, c->P,
-         c->Pr, (const double*)c->ring, rm, c->cnt);
-  return DEM_OK;
+  // force pass @ prediction, history read only, AM corrector
+  return force_pass(c, 1, false, c->params.time_step, EPI_CORRECT, rm, check, 2 * k + 1);
 }
 
 // MoveParticlesEuler (src/MDEM.f90:258-281)
@@ -553,25 +644,32 @@ int move_particles_euler_impl(dem_ctx* c) {
   }
   RingMap rm = current_map(c);
   for (int s = 0; s < c->params.euler_intervals; s++) {
-    int st = force_pass(c, c->P, c->P, true, dt, EPI_STORE, rm, true, 0);
+    int st = force_pass(c, 0, true, dt, EPI_STORE, rm, true, 0);
     if (st) return st;
     launch(c, "euler_update", k_euler_update, blocks_for(n, 256), 256, n, c->P, dt,
            (const Counters*)c->cnt);
+    c->prepared = -1;
     c->time = c->time + dt;
   }
   launch(c, "apply_pbc", k_apply_pbc, blocks_for(n, 256), 256, (const DevParams*)c->dp, n, c->P,
          (const Counters*)c->cnt);
+  c->prepared = -1;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(c, e, "euler");
   return DEM_OK;
 }
 
-// Capture `steps` MoveParticles steps (no host checks) into one graph.
+// Capture `steps` MoveParticles steps (no host checks) into one graph; the
+// host bookkeeping is left as it was.
 int capture_steps(dem_ctx* c, int steps, cudaGraphExec_t* out) {
   cudaGraph_t g;
   bool prof = c->prof;
   c->prof = false;
   long long l0 = c->launches;
+  int rm[5];
+  std::memcpy(rm, c->ringmap, sizeof(rm));
+  const int hc = c->hcur, par = c->par, prep = c->prepared, last = c->last_side;
+  const double t = c->time;
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
   int st = DEM_OK;
   for (int k = 0; k < steps && !st; k++) st = move_particles_impl(c, 0, false, k);
@@ -579,6 +677,12 @@ int capture_steps(dem_ctx* c, int steps, cudaGraphExec_t* out) {
   c->prof = prof;
   c->graph_kernels = c->launches - l0;
   c->launches = l0;
+  std::memcpy(c->ringmap, rm, sizeof(rm));
+  c->hcur = hc;
+  c->par = par;
+  c->prepared = prep;
+  c->last_side = last;
+  c->time = t;
   if (st) return st;
   if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
   e = cudaGraphInstantiate(out, g, 0);
@@ -754,11 +858,12 @@ int dem_create(const dem_params* p, dem_ctx** out) {
     h.max_min_dij_sq = d * d;
   }
   {
-    // candidate lists keep particles within MinDij + skin; a particle moving
-    // skin/4 since the last full rebuild triggers the next one
+    // candidate rows keep the partners within MinDij + skin; a pair absent
+    // from them moved closer by at most twice the largest displacement since
+    // the rows were built, so the rows are complete while the accumulated
+    // displacement bound stays below skin/2 (0.4 skin keeps a margin)
     h.vl_skin = 0.05 * CutOff;
-    const double q = 0.25 * h.vl_skin;
-    h.vl_thr2 = q * q;
+    h.vl_thr = 0.4 * h.vl_skin;
   }
   h.pp_mass_coef = p->pp_mass_coef;
   h.pp_density = p->pp_density;
@@ -857,27 +962,41 @@ int dem_set_state(dem_ctx* c, int32_t n, const int32_t* comp, const double* radi
   CK(cudaMemsetAsync(c->ring, 0, sizeof(double) * 9 * N * slots, c->stream));
   CK(cudaMalloc(&c->radius, sizeof(double) * N));
   CK(cudaMalloc(&c->comp, sizeof(int) * N));
-  CK(cudaMalloc(&c->S.pos, sizeof(double4) * N));
-  CK(cudaMalloc(&c->S.v4, sizeof(double4) * N));
-  CK(cudaMalloc(&c->S.w2, sizeof(double2) * N));
-  CK(cudaMalloc(&c->S.comp, sizeof(int) * N));
   CK(cudaMalloc(&c->S.orig, sizeof(int) * N));
   CK(cudaMalloc(&c->S.cell, sizeof(int) * N));
-  CK(cudaMalloc(&c->cell_of_orig, sizeof(int) * N));
   CK(cudaMalloc(&c->a_cell, sizeof(int) * N));
   CK(cudaMalloc(&c->a_loc, sizeof(int) * N));
   CK(cudaMalloc(&c->a_orig, sizeof(int) * N));
   CK(cudaMalloc(&c->t_orig, sizeof(int) * N));
   CK(cudaMalloc(&c->a_key, sizeof(unsigned) * N));
   CK(cudaMalloc(&c->t_key, sizeof(unsigned) * N));
-  CK(cudaMalloc(&c->CL.slot, sizeof(int) * N * KC));
-  CK(cudaMalloc(&c->CL.meta, sizeof(int4) * N));
-  CK(cudaMalloc(&c->CL.slot_of_orig, sizeof(int) * N));
-  CK(cudaMalloc(&c->CL.ref_pos, sizeof(double4) * N));
-  CK(cudaMalloc(&c->CL.dirty, (size_t)c->hp.ncell));
-  CK(cudaMalloc(&c->CL.repair, (size_t)c->hp.ncell));
-  CK(cudaMalloc(&c->CL.xslot, sizeof(int) * N * KC));
-  CK(cudaMalloc(&c->CL.xmeta, sizeof(int4) * N));
+  {
+    const size_t NC = (size_t)c->hp.ncell;
+    CellLists& L = c->L;
+    CK(cudaMalloc(&L.head, sizeof(int) * NC));
+    CK(cudaMalloc(&L.next, sizeof(int) * N));
+    CK(cudaMalloc(&L.cell[0], sizeof(int) * N));
+    CK(cudaMalloc(&L.cell[1], sizeof(int) * N));
+    CK(cudaMalloc(&L.arr_head, sizeof(int) * NC));
+    CK(cudaMalloc(&L.arr_next, sizeof(int) * N));
+    CK(cudaMalloc(&L.mflag, sizeof(int) * N));
+    CK(cudaMalloc(&L.dflag, sizeof(int) * NC));
+    CK(cudaMalloc(&L.rflag, sizeof(int) * NC));
+    CK(cudaMalloc(&L.dlist[0], sizeof(int) * NC));
+    CK(cudaMalloc(&L.dlist[1], sizeof(int) * NC));
+    CK(cudaMalloc(&L.rlist, sizeof(int) * NC));
+    CK(cudaMalloc(&c->rows.cand, sizeof(int) * N * (size_t)c->kc));
+    CK(cudaMalloc(&c->rows.meta, sizeof(int) * N));
+    CK(cudaMemsetAsync(c->rows.meta, 0, sizeof(int) * N, c->stream));
+    c->rows.kc = c->kc;
+    const bool mixed = c->precision == DEM_PREC_MIXED;
+    for (int b = 0; b < 2; b++) {
+      CK(cudaMalloc(&c->X[b], sizeof(double4) * N));
+      CK(cudaMalloc(&c->v4[b], (mixed ? sizeof(float4) : sizeof(double4)) * N));
+      CK(cudaMalloc(&c->w2[b], (mixed ? sizeof(float2) : sizeof(double2)) * N));
+    }
+    c->par = 0;
+  }
   for (int b = 0; b < 2; b++) {
     int st = alloc_history(c, c->H[b], c->hcap);
     if (st) return st;
@@ -949,6 +1068,8 @@ int dem_update_state(dem_ctx* c, const double* pos, const double* vel, const dou
                      const double* acc, const double* alpha) {
   if (!c) return DEM_ERR_INVALID;
   if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
+  // the Particle copies of the pass kernel are stale from here on
+  if (c->prepared == 0) c->prepared = -1;
   return put_state_arrays(c, c->P, pos, vel, omega, acc, alpha);
 }
 
@@ -1177,9 +1298,7 @@ int dem_get_contacts(dem_ctx* c, int64_t cap, int32_t* imin, int32_t* imax, doub
 int dem_initialize_cell_distribution(dem_ctx* c) {
   if (!c) return DEM_ERR_INVALID;
   if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
-  int st = rebuild_cells(c, c->P, true);
-  if (st) return st;
-  st = invalidate_candidates(c);
+  int st = init_cells(c);
   if (st) return st;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
@@ -1200,11 +1319,27 @@ int dem_get_cells(dem_ctx* c, int32_t* cell_index, int32_t* traversal, int32_t* 
   int st = validate_ready(c);
   if (st) return st;
   CK(cudaStreamSynchronize(c->stream));
-  if (cell_index) CK(cudaMemcpy(cell_index, c->cell_of_orig, sizeof(int) * c->n, cudaMemcpyDeviceToHost));
-  if (traversal) CK(cudaMemcpy(traversal, c->S.orig, sizeof(int) * c->n, cudaMemcpyDeviceToHost));
-  if (cell_start)
-    CK(cudaMemcpy(cell_start, c->cell_start, sizeof(int) * ((size_t)c->hp.ncell + 1),
-                  cudaMemcpyDeviceToHost));
+  const int n = c->n, ncell = c->hp.ncell;
+  std::vector<int> cell((size_t)std::max(n, 1)), next((size_t)std::max(n, 1)), head((size_t)ncell);
+  if (n > 0) {
+    CK(cudaMemcpy(cell.data(), c->L.cell[c->par], sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(next.data(), c->L.next, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  }
+  CK(cudaMemcpy(head.data(), c->L.head, sizeof(int) * ncell, cudaMemcpyDeviceToHost));
+  if (cell_index && n > 0) std::memcpy(cell_index, cell.data(), sizeof(int) * n);
+  // the lists in cell order = the traversal order of ComputeAccelerations
+  int k = 0;
+  for (int cc = 0; cc < ncell; cc++) {
+    if (cell_start) cell_start[cc] = k;
+    for (int q = head[cc], guard = 0; q != -1; q = next[q]) {
+      if (++guard > n || q < 0 || q >= n || k >= n)
+        return fail(c, DEM_ERR_STATE, "cell lists inconsistent");
+      if (traversal) traversal[k] = q;
+      k++;
+    }
+  }
+  if (cell_start) cell_start[ncell] = k;
+  if (k != n) return fail(c, DEM_ERR_STATE, "cell lists do not hold every particle");
   return DEM_OK;
 }
 
@@ -1213,8 +1348,8 @@ int dem_compute_accelerations(dem_ctx* c, int32_t use_predicted, double time_ste
   if (!c) return DEM_ERR_INVALID;
   int st = validate_ready(c);
   if (st) return st;
-  const StateArrays& s = use_predicted ? c->Pr : c->P;
-  st = force_pass(c, s, s, update != 0, time_step, EPI_STORE, current_map(c), true, 0);
+  st = force_pass(c, use_predicted ? 1 : 0, update != 0, time_step, EPI_STORE, current_map(c),
+                  true, 0);
   if (st) return st;
   CK(cudaGetLastError());
   st = read_counters(c);
@@ -1264,6 +1399,7 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
   int step = s0;
   const int G = 4;
   const int HEADROOM = 2;
+  const double dt = c->params.time_step;
   while (step <= last_step) {
     int remaining = last_step - step + 1;
     if (remaining < G || c->prof) {
@@ -1278,44 +1414,72 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
       st = grow_history(c, c->hcnt->need_capacity + HEADROOM);
       if (st) return st;
     }
-    // one graph per rotation phase (ring spare slot, history parity)
-    int phase = (c->nprev > 0 ? c->ringmap[c->nprev] : 0) * 2 + c->hcur;
+    // a graph starts from prepared Particle copies
+    if (c->prepared != 0) {
+      st = prepare_side(c, 0);
+      if (st) return st;
+    }
+    // one graph per rotation phase (ring spare slot, history parity, list parity)
+    int phase = (c->nprev > 0 ? c->ringmap[c->nprev] : 0) * 4 + c->hcur * 2 + c->par;
     if (!c->graph_valid) {
       for (auto& g : c->graph) g = nullptr;
       c->graph_valid = true;
     }
     if (!c->graph[phase]) {
-      int rm[5];
-      std::memcpy(rm, c->ringmap, sizeof(rm));
-      int hc = c->hcur;
       st = capture_steps(c, G, &c->graph[phase]);
-      std::memcpy(c->ringmap, rm, sizeof(rm));
-      c->hcur = hc;
       if (st) return st;
     }
     CK(cudaGraphLaunch(c->graph[phase], c->stream));
     c->launches += c->graph_kernels;
     st = read_counters(c);
     if (st) return st;
-    int done = G;
+    int done = G, failed_pass = -1;
     if (c->hcnt->abort) {
-      done = c->hcnt->abort_tag - 1;  // steps that completed
-      if (done < 0 || done >= G) return fail(c, DEM_ERR_STATE, "bad abort tag");
+      const int tag = c->hcnt->abort_tag - 1;  // 2*(step in chunk) + pass
+      if (c->hcnt->list_error) return fail(c, DEM_ERR_STATE, "cell lists inconsistent");
+      if (tag < 0 || tag >= 2 * G) return fail(c, DEM_ERR_STATE, "bad abort tag");
+      done = tag / 2;
+      failed_pass = tag % 2;
     }
     for (int k = 0; k < done; k++) {
       rotate_ring(c);
       c->hcur ^= 1;
     }
+    if (done > 0) {
+      c->prepared = 0;
+      c->last_side = 1;
+    }
     step += done;
-    c->time = (double)(step - 1) * c->params.time_step;
-    if (done < G) {
-      int need = c->hcnt->need_capacity;
-      st = clear_abort(c);
-      if (st) return st;
-      st = grow_history(c, std::max(need, c->hcap + 1));
-      if (st) return st;
-      st = move_particles_impl(c, step, true, 0);
-      if (st) return st;
+    c->time = (double)(step - 1) * dt;
+    if (failed_pass >= 0) {
+      // the failed step: its first pass ran up to the failure (relink done),
+      // or its first pass completed and its second one failed
+      c->par ^= 1;
+      if (failed_pass == 0) {
+        RingMap rm = current_map(c);
+        st = finish_pass(c, 0, true, dt, EPI_PREDICT, rm, 0);
+        if (st) return st;
+        c->last_side = 0;
+        c->prepared = 1;
+        c->hcur ^= 1;
+        rotate_ring(c);
+        c->time = (double)step * dt;
+        rm = current_map(c);
+        st = force_pass(c, 1, false, dt, EPI_CORRECT, rm, true, 1);
+        if (st) return st;
+      } else {
+        c->last_side = 0;
+        c->prepared = 1;
+        c->hcur ^= 1;
+        rotate_ring(c);
+        c->time = (double)step * dt;
+        c->par ^= 1;
+        RingMap rm = current_map(c);
+        st = finish_pass(c, 1, false, dt, EPI_CORRECT, rm, 1);
+        if (st) return st;
+        c->last_side = 1;
+        c->prepared = 0;
+      }
       step++;
     }
   }

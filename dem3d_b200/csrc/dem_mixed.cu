@@ -14,14 +14,13 @@
 //    the predictor/corrector stay FP64.
 // This translation unit may fuse multiply-adds.
 #include "dem_mixed.cuh"
+#include "dem_pass.cuh"
 
 namespace dem {
 
 namespace {
 
 struct MixedView {
-  const float4* v4;  // traversal-order vx, vy, vz, wx
-  const float2* w2;  // wy, wz
   // history values [n*cap]: a = (ft.xyz, vt.x) b = (vt.yz, lo.xy) c = lo.z
   const float4* ra;
   const float4* rb;
@@ -240,33 +239,33 @@ __device__ __forceinline__ unsigned long long wsum(unsigned long long v) {
   return v;
 }
 
-template <bool PP, int EPI, bool SWEEP>
-__global__ void __launch_bounds__(128, SWEEP ? 1 : 4) k_force_mixed(ForceArgs A, MixedView V) {
+// The mixed-precision pass kernel: the FP64 kernel's structure (candidate
+// rows, exact FP64 overlap test, orientation, history semantics, summation
+// order), FP32 contact arithmetic, FP64 integrator epilogue.
+template <bool PP, int EPI>
+__global__ void __launch_bounds__(128, 4) k_pass_mixed(PassArgs<float4, float2> A, MixedView V) {
   if (A.cnt->abort) return;
-  if (SWEEP && A.cnt->list_overflow == 0) return;
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long n_col = 0, n_pc = 0, n_wc = 0;
   int need = 0;
-  const int4 meta = s < A.n ? A.cl_meta[s] : make_int4(0, 0, 0, 0);
-  if (!SWEEP && s == 0) clear_rebuild_trigger(A);
-  if (s < A.n && (meta.x < 0) == SWEEP) {
+  double d2 = 0.0;
+  if (p < A.n) {
     const DevParams& P = *A.P;
-    const SortedArrays& S = A.S;
-    const int nx = P.nx, ny = P.ny;
-    const int c = S.cell[s];
-    const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
-    const double4 p4 = S.pos[s];
+    const int n = A.n;
+    const int c = A.cell_cur[p];
+    const double4 p4 = A.X[p];
     const double xp[3] = {p4.x, p4.y, p4.z};
     const double Rpd = p4.w;
     const float Rp = (float)Rpd;
-    const float4 pv4 = V.v4[s];
-    const float2 pw2 = V.w2[s];
+    const float4 pv4 = A.v4[p];
+    const float2 pw2 = A.w2[p];
     const F3 vp = mk(pv4.x, pv4.y, pv4.z);
     const F3 wp = mk(pv4.w, pw2.x, pw2.y);
-    const int orig = S.orig[s];
-    const int cp = PP ? 0 : S.comp[s];
+    const int cp = PP ? 0 : A.comp[p];
     float inv_m, inv_i, eff_m;
     MMat<PP>::self(P, cp, Rp, inv_m, inv_i, eff_m);
+    int n1, n2b, n2a;
+    unpack_meta(A.meta[p], n1, n2b, n2a);
     const float half_dt = (float)A.half_dt;
     const bool update = A.update != 0;
     int hw_n = 0;
@@ -280,7 +279,7 @@ __global__ void __launch_bounds__(128, SWEEP ? 1 : 4) k_force_mixed(ForceArgs A,
 
     auto record = [&](int partner, F3 ft, F3 lo, F3 vt) {
       if (hw_n < Hw.cap) {
-        size_t i = (size_t)orig * Hw.cap + hw_n;
+        size_t i = (size_t)p * Hw.cap + hw_n;
         Hw.key[i] = partner;
         rec_write(V.wa, V.wb, V.wc, i, ft, lo, vt);
       } else {
@@ -299,41 +298,58 @@ __global__ void __launch_bounds__(128, SWEEP ? 1 : 4) k_force_mixed(ForceArgs A,
       ft = lo = vt = mk(0.f, 0.f, 0.f);
       return false;
     };
-
-    auto visit_i = [&](int t) {
-      const double4 q4 = S.pos[t];
-      double Rij[3] = {q4.x - xp[0], q4.y - xp[1], q4.z - xp[2]};
+    // Rij = xb - xa (minimum image, FP64) and DijSq
+    auto geometry = [&](double ax, double ay, double az, double bx, double by, double bz,
+                        double Rij[3]) -> double {
+      Rij[0] = bx - ax;
+      Rij[1] = by - ay;
+      Rij[2] = bz - az;
 #pragma unroll
       for (int k = 0; k < 3; k++)
         if (P.pbc[k]) Rij[k] = Rij[k] - P.lbox[k] * fnint(Rij[k] * P.inv_lbox[k]);
-      const double DijSq = sumsq3(Rij);
-      const int cq = PP ? 0 : S.comp[t];
-      const double Delta = MMat<PP>::min_dij_sq(P, cp, Rpd, cq, q4.w) - DijSq;
-      if (Delta > 0.0) {
-        const float Rq = (float)q4.w;
-        MPair m;
-        MMat<PP>::pair(P, cp, Rp, cq, Rq, m);
-        const int qo = S.orig[t];
-        const float4 qv4 = V.v4[t];
-        const float2 qw2 = V.w2[t];
-        const int lo_i = orig < qo ? orig : qo, hi_i = orig < qo ? qo : orig;
-        F3 ft0, ft0lo, vt0;
-        const bool contacting = lookup(lo_i, hi_i, ft0, ft0lo, vt0);
-        if (!contacting) n_col++;
-        n_pc++;
-        MOut o;
-        mixed_pair(Rij, DijSq, Delta, m, Rp, vp, wp, Rq, mk(qv4.x, qv4.y, qv4.z),
-                   mk(qv4.w, qw2.x, qw2.y), half_dt, contacting, ft0, ft0lo, vt0, o);
-        iF = iF + o.FN + (o.FT + o.FTlo);
-        iT = iT + cross(Rp * o.N, o.FT);
-        if (update && orig < qo) record(qo, o.FT, o.FTlo, o.VT);
-      }
+      return sumsq3(Rij);
     };
-    walk_as_i<SWEEP>(A, meta, s, orig, c, cx, cy, cz, visit_i);
+    auto contact_i = [&](int q, double4 q4) -> bool {
+      double Rij[3];
+      const double DijSq = geometry(xp[0], xp[1], xp[2], q4.x, q4.y, q4.z, Rij);
+      const int cq = PP ? 0 : A.comp[q];
+      return MMat<PP>::min_dij_sq(P, cp, Rpd, cq, q4.w) - DijSq > 0.0;
+    };
+    auto contact_j = [&](int q, double4 q4) -> bool {
+      double Rij[3];
+      const double DijSq = geometry(q4.x, q4.y, q4.z, xp[0], xp[1], xp[2], Rij);
+      const int cq = PP ? 0 : A.comp[q];
+      return MMat<PP>::min_dij_sq(P, cq, q4.w, cp, Rpd) - DijSq > 0.0;
+    };
+
+    auto visit_i = [&](int q) {
+      const double4 q4 = A.X[q];
+      double Rij[3];
+      const double DijSq = geometry(xp[0], xp[1], xp[2], q4.x, q4.y, q4.z, Rij);
+      const int cq = PP ? 0 : A.comp[q];
+      const double Delta = MMat<PP>::min_dij_sq(P, cp, Rpd, cq, q4.w) - DijSq;
+      const float Rq = (float)q4.w;
+      MPair m;
+      MMat<PP>::pair(P, cp, Rp, cq, Rq, m);
+      const float4 qv4 = A.v4[q];
+      const float2 qw2 = A.w2[q];
+      const int lo_i = p < q ? p : q, hi_i = p < q ? q : p;
+      F3 ft0, ft0lo, vt0;
+      const bool contacting = lookup(lo_i, hi_i, ft0, ft0lo, vt0);
+      if (!contacting) n_col++;
+      n_pc++;
+      MOut o;
+      mixed_pair(Rij, DijSq, Delta, m, Rp, vp, wp, Rq, mk(qv4.x, qv4.y, qv4.z),
+                 mk(qv4.w, qw2.x, qw2.y), half_dt, contacting, ft0, ft0lo, vt0, o);
+      iF = iF + o.FN + (o.FT + o.FTlo);
+      iT = iT + cross(Rp * o.N, o.FT);
+      if (update && p < q) record(q, o.FT, o.FTlo, o.VT);
+    };
+    walk_segment(A.cand, A.X, n, p, 0, n1, contact_i, visit_i);
 
     for (int w = 0; w < P.nw; w++) {
       const dem_wall& W = P.walls[w];
-      const size_t wi = (size_t)orig * P.nw + w;
+      const size_t wi = (size_t)p * P.nw + w;
       const bool contacting = Hr.wflag[wi] != 0;
       F3 ft0 = mk(0.f, 0.f, 0.f), ft0lo = ft0, vt0 = ft0;
       if (contacting) rec_read(V.rwa, V.rwb, V.rwc, wi, ft0, ft0lo, vt0);
@@ -370,145 +386,63 @@ __global__ void __launch_bounds__(128, SWEEP ? 1 : 4) k_force_mixed(ForceArgs A,
     }
 
     F3 F = mk(0.f, 0.f, 0.f), T = mk(0.f, 0.f, 0.f);
-    auto visit_j = [&](int t) {
-      const double4 q4 = S.pos[t];
-      double Rij[3] = {xp[0] - q4.x, xp[1] - q4.y, xp[2] - q4.z};
-#pragma unroll
-      for (int k = 0; k < 3; k++)
-        if (P.pbc[k]) Rij[k] = Rij[k] - P.lbox[k] * fnint(Rij[k] * P.inv_lbox[k]);
-      const double DijSq = sumsq3(Rij);
-      const int cq = PP ? 0 : S.comp[t];
+    auto visit_j = [&](int q) {
+      const double4 q4 = A.X[q];
+      double Rij[3];
+      const double DijSq = geometry(q4.x, q4.y, q4.z, xp[0], xp[1], xp[2], Rij);
+      const int cq = PP ? 0 : A.comp[q];
       const double Delta = MMat<PP>::min_dij_sq(P, cq, q4.w, cp, Rpd) - DijSq;
-      if (Delta > 0.0) {
-        const float Rq = (float)q4.w;
-        MPair m;
-        MMat<PP>::pair(P, cq, Rq, cp, Rp, m);
-        const int qo = S.orig[t];
-        const float4 qv4 = V.v4[t];
-        const float2 qw2 = V.w2[t];
-        const int lo_i = orig < qo ? orig : qo, hi_i = orig < qo ? qo : orig;
-        F3 ft0, ft0lo, vt0;
-        const bool contacting = lookup(lo_i, hi_i, ft0, ft0lo, vt0);
-        MOut o;
-        mixed_pair(Rij, DijSq, Delta, m, Rq, mk(qv4.x, qv4.y, qv4.z), mk(qv4.w, qw2.x, qw2.y), Rp,
-                   vp, wp, half_dt, contacting, ft0, ft0lo, vt0, o);
-        F = F - o.FN - (o.FT + o.FTlo);
-        T = T + Rp * o.NxFT;
-        if (update && orig < qo) record(qo, o.FT, o.FTlo, o.VT);
-      }
+      const float Rq = (float)q4.w;
+      MPair m;
+      MMat<PP>::pair(P, cq, Rq, cp, Rp, m);
+      const float4 qv4 = A.v4[q];
+      const float2 qw2 = A.w2[q];
+      const int lo_i = p < q ? p : q, hi_i = p < q ? q : p;
+      F3 ft0, ft0lo, vt0;
+      const bool contacting = lookup(lo_i, hi_i, ft0, ft0lo, vt0);
+      MOut o;
+      mixed_pair(Rij, DijSq, Delta, m, Rq, mk(qv4.x, qv4.y, qv4.z), mk(qv4.w, qw2.x, qw2.y), Rp,
+                 vp, wp, half_dt, contacting, ft0, ft0lo, vt0, o);
+      F = F - o.FN - (o.FT + o.FTlo);
+      T = T + Rp * o.NxFT;
+      if (update && p < q) record(q, o.FT, o.FTlo, o.VT);
     };
-    walk_as_j<SWEEP>(A, meta, s, orig, c, cx, cy, cz, visit_j, [&]() {
-      F = F + iF;
-      T = T + iT;
-    });
+    walk_segment(A.cand, A.X, n, p, n1, n1 + n2b, contact_j, visit_j);
+    F = F + iF;
+    T = T + iT;
+    walk_segment(A.cand, A.X, n, p, n1 + n2b, n1 + n2b + n2a, contact_j, visit_j);
 
     if (update) {
-      const int nold = Hr.cnt[orig];
+      const int nold = Hr.cnt[p];
       for (int r = 0; r < nold; r++) {
-        const size_t i = (size_t)orig * Hr.cap + r;
+        const size_t i = (size_t)p * Hr.cap + r;
         const int q2 = Hr.key[i];
-        if (!cells_adjacent(P, c, A.cell_of_orig[q2])) {
+        if (!cells_adjacent(P, c, A.cell_cur[q2])) {
           F3 ft, lo, vt;
           rec_read(V.ra, V.rb, V.rc, i, ft, lo, vt);
           record(q2, ft, lo, vt);
         }
       }
-      Hw.cnt[orig] = hw_n < Hw.cap ? hw_n : Hw.cap;
+      Hw.cnt[p] = hw_n < Hw.cap ? hw_n : Hw.cap;
       if (overflow) {
         atomicExch(&A.cnt->overflow, 1);
-        atomicCAS(&A.cnt->abort_tag, 0, A.tag + 1);
-        atomicExch(&A.cnt->abort, 1);
+        set_abort(A.cnt, A.tag);
       }
       need = hw_n;
     }
 
     const double acc[3] = {(double)(F.x * inv_m), (double)(F.y * inv_m), (double)(F.z * inv_m)};
     const double alp[3] = {(double)(T.x * inv_i), (double)(T.y * inv_i), (double)(T.z * inv_i)};
-    const size_t n = (size_t)A.n;
-    if (EPI == EPI_STORE) {
-      A.tgt.ax[orig] = acc[0]; A.tgt.ay[orig] = acc[1]; A.tgt.az[orig] = acc[2];
-      A.tgt.lx[orig] = alp[0]; A.tgt.ly[orig] = alp[1]; A.tgt.lz[orig] = alp[2];
-    } else if (EPI == EPI_PREDICT) {
-      const StateArrays& Q = A.part;
-      const StateArrays& R = A.pred;
-      Q.ax[orig] = acc[0]; Q.ay[orig] = acc[1]; Q.az[orig] = acc[2];
-      Q.lx[orig] = alp[0]; Q.ly[orig] = alp[1]; Q.lz[orig] = alp[2];
-      // FP64 velocities of Particle (the traversal copies are FP32)
-      const double vd[3] = {Q.vx[orig], Q.vy[orig], Q.vz[orig]};
-      const double wd[3] = {Q.wx[orig], Q.wy[orig], Q.wz[orig]};
-      double sv[3] = {0.0, 0.0, 0.0}, sa[3] = {0.0, 0.0, 0.0}, sl[3] = {0.0, 0.0, 0.0};
-      for (int k = 0; k < P.nprev; k++) {
-        const double ABk = P.ab[k];
-        const double* rg = A.ring + (size_t)A.rm.phys[k] * 9 * n + orig;
-#pragma unroll
-        for (int d = 0; d < 3; d++) sv[d] = sv[d] + ABk * rg[d * n];
-#pragma unroll
-        for (int d = 0; d < 3; d++) sa[d] = sa[d] + ABk * rg[(3 + d) * n];
-#pragma unroll
-        for (int d = 0; d < 3; d++) sl[d] = sl[d] + ABk * rg[(6 + d) * n];
-      }
-      double xr[3], vr[3], wr[3];
-#pragma unroll
-      for (int d = 0; d < 3; d++) xr[d] = xp[d] + P.ab0 * vd[d] + sv[d];
-#pragma unroll
-      for (int d = 0; d < 3; d++) vr[d] = vd[d] + P.ab0 * acc[d] + sa[d];
-#pragma unroll
-      for (int d = 0; d < 3; d++) wr[d] = wd[d] + P.ab0 * alp[d] + sl[d];
-#pragma unroll
-      for (int d = 0; d < 3; d++)
-        if (P.pbc[d]) xr[d] = xr[d] - P.lbox[d] * fnint(xr[d] * P.inv_lbox[d]);
-      R.px[orig] = xr[0]; R.py[orig] = xr[1]; R.pz[orig] = xr[2];
-      R.vx[orig] = vr[0]; R.vy[orig] = vr[1]; R.vz[orig] = vr[2];
-      R.wx[orig] = wr[0]; R.wy[orig] = wr[1]; R.wz[orig] = wr[2];
-      if (P.nprev > 0) {
-        double* rg = A.ring + (size_t)A.rm.phys[P.nprev] * 9 * n + orig;
-#pragma unroll
-        for (int d = 0; d < 3; d++) rg[d * n] = vd[d];
-#pragma unroll
-        for (int d = 0; d < 3; d++) rg[(3 + d) * n] = acc[d];
-#pragma unroll
-        for (int d = 0; d < 3; d++) rg[(6 + d) * n] = alp[d];
-      }
-    } else {
-      const StateArrays& Q = A.part;
-      const StateArrays& R = A.pred;
-      R.ax[orig] = acc[0]; R.ay[orig] = acc[1]; R.az[orig] = acc[2];
-      R.lx[orig] = alp[0]; R.ly[orig] = alp[1]; R.lz[orig] = alp[2];
-      const double vpd[3] = {R.vx[orig], R.vy[orig], R.vz[orig]};
-      double sv[3] = {0.0, 0.0, 0.0}, sa[3] = {0.0, 0.0, 0.0}, sl[3] = {0.0, 0.0, 0.0};
-      for (int k = 0; k < P.nprev; k++) {
-        const double AMk = P.am[k];
-        const double* rg = A.ring + (size_t)A.rm.phys[k] * 9 * n + orig;
-#pragma unroll
-        for (int d = 0; d < 3; d++) sv[d] = sv[d] + AMk * rg[d * n];
-#pragma unroll
-        for (int d = 0; d < 3; d++) sa[d] = sa[d] + AMk * rg[(3 + d) * n];
-#pragma unroll
-        for (int d = 0; d < 3; d++) sl[d] = sl[d] + AMk * rg[(6 + d) * n];
-      }
-      double x[3] = {Q.px[orig], Q.py[orig], Q.pz[orig]};
-      double v[3] = {Q.vx[orig], Q.vy[orig], Q.vz[orig]};
-      double w[3] = {Q.wx[orig], Q.wy[orig], Q.wz[orig]};
-#pragma unroll
-      for (int d = 0; d < 3; d++) x[d] = x[d] + P.am0 * vpd[d] + sv[d];
-#pragma unroll
-      for (int d = 0; d < 3; d++) v[d] = v[d] + P.am0 * acc[d] + sa[d];
-#pragma unroll
-      for (int d = 0; d < 3; d++) w[d] = w[d] + P.am0 * alp[d] + sl[d];
-#pragma unroll
-      for (int d = 0; d < 3; d++)
-        if (P.pbc[d]) x[d] = x[d] - P.lbox[d] * fnint(x[d] * P.inv_lbox[d]);
-      Q.px[orig] = x[0]; Q.py[orig] = x[1]; Q.pz[orig] = x[2];
-      Q.vx[orig] = v[0]; Q.vy[orig] = v[1]; Q.vz[orig] = v[2];
-      Q.wx[orig] = w[0]; Q.wy[orig] = w[1]; Q.wz[orig] = w[2];
-      bool out = false;
-#pragma unroll
-      for (int d = 0; d < 3; d++) {
-        const double h = 0.5 * P.lbox[d];
-        out = out || (x[d] > h) || (x[d] < -h);
-      }
-      if (out) atomicAdd(&A.cnt->escaped, 1ull);
+    // the integrator runs on FP64 velocities: Particle's for the predictor,
+    // Predicted's for the corrector (the pass copies are FP32)
+    double vd[3] = {0.0, 0.0, 0.0}, wd[3] = {0.0, 0.0, 0.0};
+    if (EPI == EPI_PREDICT) {
+      vd[0] = A.part.vx[p]; vd[1] = A.part.vy[p]; vd[2] = A.part.vz[p];
+      wd[0] = A.part.wx[p]; wd[1] = A.part.wy[p]; wd[2] = A.part.wz[p];
+    } else if (EPI == EPI_CORRECT) {
+      vd[0] = A.pred.vx[p]; vd[1] = A.pred.vy[p]; vd[2] = A.pred.vz[p];
     }
+    epilogue<EPI>(A, p, xp, Rpd, vd, wd, acc, alp, c, d2);
   }
   n_col = wsum(n_col);
   n_pc = wsum(n_pc);
@@ -521,28 +455,7 @@ __global__ void __launch_bounds__(128, SWEEP ? 1 : 4) k_force_mixed(ForceArgs A,
     if (n_pc) atomicAdd(&A.cnt->pair_contacts, n_pc);
     if (n_wc) atomicAdd(&A.cnt->wall_contacts, n_wc);
   }
-}
-
-template <bool PP>
-__global__ void k_gather_mixed(const DevParams* __restrict__ Pp, int n, StateArrays src,
-                               const double* __restrict__ radius, const int* __restrict__ comp,
-                               SortedArrays S, float4* __restrict__ v4, float2* __restrict__ w2,
-                               const Counters* __restrict__ cnt) {
-  if (cnt->abort) return;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  int o = S.orig[t];
-  double R;
-  if (PP) {
-    R = radius[o];
-  } else {
-    int k = comp[o];
-    S.comp[t] = k;
-    R = Pp->comp_radius[k];
-  }
-  S.pos[t] = make_double4(src.px[o], src.py[o], src.pz[o], R);
-  v4[t] = make_float4((float)src.vx[o], (float)src.vy[o], (float)src.vz[o], (float)src.wx[o]);
-  w2[t] = make_float2((float)src.wy[o], (float)src.wz[o]);
+  if (EPI != EPI_STORE) publish_disp(A.cnt, d2);
 }
 
 // FP64 records <-> FP32 records
@@ -613,8 +526,7 @@ bool mixed_alloc(MixedBuffers& M, int n, int nw, int cap) {
   M.n = n;
   M.nw = nw;
   M.cap = cap;
-  bool ok = cudaMalloc(&M.v4, N * sizeof(float4)) == cudaSuccess &&
-            cudaMalloc(&M.w2, N * sizeof(float2)) == cudaSuccess;
+  bool ok = true;
   for (int b = 0; b < 2 && ok; b++) {
     ok = cudaMalloc(&M.ha[b], N * cap * sizeof(float4)) == cudaSuccess &&
          cudaMalloc(&M.hb[b], N * cap * sizeof(float4)) == cudaSuccess &&
@@ -628,8 +540,6 @@ bool mixed_alloc(MixedBuffers& M, int n, int nw, int cap) {
 }
 
 void mixed_free(MixedBuffers& M) {
-  cudaFree(M.v4);
-  cudaFree(M.w2);
   for (int b = 0; b < 2; b++) {
     cudaFree(M.ha[b]);
     cudaFree(M.hb[b]);
@@ -669,24 +579,10 @@ bool mixed_regrow(MixedBuffers& M, int n, int newcap, int cur, const History& ol
   return true;
 }
 
-void mixed_gather(MixedBuffers& M, bool pp, const DevParams* dp, int n, const StateArrays& src,
-                  const double* radius, const int* comp, const SortedArrays& S, Counters* cnt,
-                  cudaStream_t st) {
-  if (n == 0) return;
-  if (pp)
-    k_gather_mixed<true><<<blocks(n, 256), 256, 0, st>>>(dp, n, src, radius, comp, S, M.v4, M.w2,
-                                                         cnt);
-  else
-    k_gather_mixed<false><<<blocks(n, 256), 256, 0, st>>>(dp, n, src, radius, comp, S, M.v4, M.w2,
-                                                          cnt);
-}
-
-void mixed_force(MixedBuffers& M, bool pp, int epi, const ForceArgs& A, int cur,
-                 cudaStream_t st) {
+void mixed_pass(MixedBuffers& M, bool pp, int epi, const PassArgs<float4, float2>& A, int cur,
+                cudaStream_t st) {
   if (A.n == 0) return;
   MixedView V;
-  V.v4 = M.v4;
-  V.w2 = M.w2;
   V.ra = M.ha[cur];
   V.rb = M.hb[cur];
   V.rc = M.hc[cur];
@@ -699,17 +595,15 @@ void mixed_force(MixedBuffers& M, bool pp, int epi, const ForceArgs& A, int cur,
   V.wwa = M.wa[cur ^ 1];
   V.wwb = M.wb[cur ^ 1];
   V.wwc = M.wc[cur ^ 1];
-  unsigned g = blocks(A.n, 128);
-#define MCASE(PPV, E)                                        \
-  do {                                                       \
-    k_force_mixed<PPV, E, false><<<g, 128, 0, st>>>(A, V);   \
-    k_force_mixed<PPV, E, true><<<g, 128, 0, st>>>(A, V);    \
+  const unsigned g = blocks(A.n, 128);
+#define MCASE(PPV)                                                                       \
+  do {                                                                                   \
+    if (epi == EPI_PREDICT) k_pass_mixed<PPV, EPI_PREDICT><<<g, 128, 0, st>>>(A, V);     \
+    else if (epi == EPI_CORRECT) k_pass_mixed<PPV, EPI_CORRECT><<<g, 128, 0, st>>>(A, V); \
+    else k_pass_mixed<PPV, EPI_STORE><<<g, 128, 0, st>>>(A, V);                          \
   } while (0)
-  if (pp) {
-    MCASE(true, EPI_STORE);
-  } else {
-    MCASE(false, EPI_STORE);
-  }
+  if (pp) MCASE(true);
+  else MCASE(false);
 #undef MCASE
 }
 

@@ -8,9 +8,6 @@ namespace dem {
 struct MixedBuffers {
   bool ready = false;
   int n = 0, nw = 0, cap = 0;
-  // traversal-order FP32 velocities / angular velocities
-  float4* v4 = nullptr;  // vx, vy, vz, wx
-  float2* w2 = nullptr;  // wy, wz
   // FP32 pair records (ft, vt, Kahan remainder of ft), double-buffered like
   // the key/count tables of History: a = (ft.xyz, vt.x), b = (vt.yz, lo.xy),
   // c = lo.z
@@ -28,11 +25,9 @@ bool mixed_alloc(MixedBuffers& M, int n, int nw, int cap);
 void mixed_free(MixedBuffers& M);
 bool mixed_regrow(MixedBuffers& M, int n, int newcap, int cur, const History& old,
                   cudaStream_t st);
-void mixed_gather(MixedBuffers& M, bool pp, const DevParams* dp, int n, const StateArrays& src,
-                  const double* radius, const int* comp, const SortedArrays& S, Counters* cnt,
-                  cudaStream_t st);
-void mixed_force(MixedBuffers& M, bool pp, int epi, const ForceArgs& A, int cur,
-                 cudaStream_t st);
+// One pass kernel launch (FP32 contact arithmetic) on the context's stream.
+void mixed_pass(MixedBuffers& M, bool pp, int epi, const PassArgs<float4, float2>& A, int cur,
+                cudaStream_t st);
 void mixed_import_history(MixedBuffers& M, const History& H, int n, int nw, int cur,
                           cudaStream_t st);
 void mixed_export_history(MixedBuffers& M, const History& H, int n, int nw, int cur,

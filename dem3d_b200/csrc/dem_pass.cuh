@@ -1,0 +1,222 @@
+// dem_pass.cuh -- device helpers shared by the FP64 and the mixed pass
+// kernels: candidate segments, the AB/AM epilogues and the cell transition
+// (RedistributeParticles3D's bookkeeping) for the next pass.
+//
+// A pass kernel runs one thread per particle in original index order.  It
+// reads its candidate row, applies the reference's overlap test to every
+// candidate, computes the contacts in the reference's order, and finishes
+// with the integrator step of the pass (AB predictor or AM corrector).  The
+// epilogue also hashes the particle's next position into its cell and, when
+// the cell changes, records the move for the next relink: the arrival list
+// of the new cell and the dirty list of both cells.  Every such side effect
+// is idempotent, so a pass kernel that was stopped by a history overflow can
+// be launched again after the tables grow.
+#pragma once
+#include "dem_device.cuh"
+
+namespace dem {
+
+__device__ __forceinline__ void mark_dirty(const CellLists& L, Counters* cnt, int par, int c) {
+  if (atomicExch(&L.dflag[c], 1) == 0) {
+    const int k = atomicAdd(&cnt->n_dirty[par], 1);
+    L.dlist[par][k] = c;
+  }
+}
+
+// Cell of particle p under the next assignment; a particle that changes cell
+// is pushed once onto its new cell's arrival list.
+__device__ __forceinline__ void note_cell(const CellLists& L, Counters* cnt, int par, int p,
+                                          int c_old, int c_new) {
+  L.cell[par][p] = c_new;
+  if (c_new != c_old) {
+    if (atomicExch(&L.mflag[p], 1) == 0) {
+      L.arr_next[p] = atomicExch(&L.arr_head[c_new], p);
+      atomicAdd(&cnt->movers_pending, 1ull);
+    }
+    mark_dirty(L, cnt, par, c_old);
+    mark_dirty(L, cnt, par, c_new);
+  }
+}
+
+// squared minimum-image displacement between two positions of a particle
+__device__ __forceinline__ double disp2(const DevParams& P, const double a[3], const double b[3]) {
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    double d = a[k] - b[k];
+    if (P.pbc[k]) d = d - P.lbox[k] * rint(d * P.inv_lbox[k]);
+    s = s + d * d;
+  }
+  return s;
+}
+
+// Largest displacement of the warp into the pass maximum (non-negative
+// doubles order like their bit patterns).
+__device__ __forceinline__ void publish_disp(Counters* cnt, double d2) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) d2 = fmax(d2, __shfl_down_sync(0xffffffffu, d2, o));
+  if ((threadIdx.x & 31) == 0 && d2 > 0.0) {
+    double d = sqrt(d2);
+    atomicMax(&cnt->disp_max, (unsigned long long)__double_as_longlong(d));
+  }
+}
+
+// Walk candidates k0..k1-1 of particle p: prefetch four at a time (index,
+// then position), keep those for which contact(q, xq) holds, and hand them
+// to visit(q) in row order.
+template <class Contact, class Visit>
+__device__ __forceinline__ void walk_segment(const int* __restrict__ cand,
+                                             const double4* __restrict__ X, int n, int p, int k0,
+                                             int k1, Contact&& contact, Visit&& visit) {
+#pragma unroll 1
+  for (int b = k0; b < k1; b += 4) {
+    int q[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) q[u] = b + u < k1 ? __ldg(cand + (size_t)(b + u) * n + p) : -1;
+    double4 xq[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+      xq[u] = q[u] >= 0 ? X[q[u]] : make_double4(0.0, 0.0, 0.0, 0.0);
+    unsigned msk = 0u;
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+      if (q[u] >= 0 && contact(q[u], xq[u])) msk |= 1u << u;
+#pragma unroll 1
+    for (int u = 0; u < 4; u++) {
+      if (!((msk >> u) & 1u)) continue;
+      const int qq = u == 0 ? q[0] : u == 1 ? q[1] : u == 2 ? q[2] : q[3];
+      visit(qq);
+    }
+  }
+}
+
+template <class T>
+__device__ __forceinline__ T mk_v4(double a, double b, double c, double d);
+template <>
+__device__ __forceinline__ double4 mk_v4<double4>(double a, double b, double c, double d) {
+  return make_double4(a, b, c, d);
+}
+template <>
+__device__ __forceinline__ float4 mk_v4<float4>(double a, double b, double c, double d) {
+  return make_float4((float)a, (float)b, (float)c, (float)d);
+}
+template <class T>
+__device__ __forceinline__ T mk_w2(double a, double b);
+template <>
+__device__ __forceinline__ double2 mk_w2<double2>(double a, double b) {
+  return make_double2(a, b);
+}
+template <>
+__device__ __forceinline__ float2 mk_w2<float2>(double a, double b) {
+  return make_float2((float)a, (float)b);
+}
+
+// The integrator part of a pass, after a = F/m and alpha = T/I
+// (src/MForces.f90:330-333):
+//  EPI_STORE   a, alpha -> tgt;
+//  EPI_PREDICT the AB predictor of MoveParticles (src/MDEM.f90:296-331) from
+//              x(t) = xp, v(t) = vp, w(t) = wp and the ring, (v,a,alpha)(t)
+//              into the spare ring slot; the prediction is the next pass's
+//              position;
+//  EPI_CORRECT the AM corrector (src/MDEM.f90:340-367) with v~ = vp; the new
+//              x(t+dt) is the next pass's position.
+// d2 receives the squared displacement from this pass's position to the next.
+template <int EPI, class V4, class W2>
+__device__ __forceinline__ void epilogue(const PassArgs<V4, W2>& A, int p, const double xp[3],
+                                         double Rp, const double vp[3], const double wp[3],
+                                         const double acc[3], const double alp[3], int c_cur,
+                                         double& d2) {
+  const DevParams& P = *A.P;
+  const size_t n = (size_t)A.n;
+  if (EPI == EPI_STORE) {
+    A.tgt.ax[p] = acc[0]; A.tgt.ay[p] = acc[1]; A.tgt.az[p] = acc[2];
+    A.tgt.lx[p] = alp[0]; A.tgt.ly[p] = alp[1]; A.tgt.lz[p] = alp[2];
+    return;
+  }
+  double sv[3] = {0.0, 0.0, 0.0}, sa[3] = {0.0, 0.0, 0.0}, sl[3] = {0.0, 0.0, 0.0};
+  for (int k = 0; k < P.nprev; k++) {
+    const double C = EPI == EPI_PREDICT ? P.ab[k] : P.am[k];
+    const double* rg = A.ring + (size_t)A.rm.phys[k] * 9 * n + p;
+#pragma unroll
+    for (int d = 0; d < 3; d++) sv[d] = sv[d] + C * rg[d * n];
+#pragma unroll
+    for (int d = 0; d < 3; d++) sa[d] = sa[d] + C * rg[(3 + d) * n];
+#pragma unroll
+    for (int d = 0; d < 3; d++) sl[d] = sl[d] + C * rg[(6 + d) * n];
+  }
+  double x[3], v[3], w[3];
+  if (EPI == EPI_PREDICT) {
+    const StateArrays& Q = A.part;
+    const StateArrays& R = A.pred;
+    Q.ax[p] = acc[0]; Q.ay[p] = acc[1]; Q.az[p] = acc[2];
+    Q.lx[p] = alp[0]; Q.ly[p] = alp[1]; Q.lz[p] = alp[2];
+#pragma unroll
+    for (int d = 0; d < 3; d++) x[d] = xp[d] + P.ab0 * vp[d] + sv[d];
+#pragma unroll
+    for (int d = 0; d < 3; d++) v[d] = vp[d] + P.ab0 * acc[d] + sa[d];
+#pragma unroll
+    for (int d = 0; d < 3; d++) w[d] = wp[d] + P.ab0 * alp[d] + sl[d];
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+      if (P.pbc[d]) x[d] = x[d] - P.lbox[d] * fnint(x[d] * P.inv_lbox[d]);
+    R.px[p] = x[0]; R.py[p] = x[1]; R.pz[p] = x[2];
+    R.vx[p] = v[0]; R.vy[p] = v[1]; R.vz[p] = v[2];
+    R.wx[p] = w[0]; R.wy[p] = w[1]; R.wz[p] = w[2];
+    if (P.nprev > 0) {
+      double* rg = A.ring + (size_t)A.rm.phys[P.nprev] * 9 * n + p;
+#pragma unroll
+      for (int d = 0; d < 3; d++) rg[d * n] = vp[d];
+#pragma unroll
+      for (int d = 0; d < 3; d++) rg[(3 + d) * n] = acc[d];
+#pragma unroll
+      for (int d = 0; d < 3; d++) rg[(6 + d) * n] = alp[d];
+    }
+  } else {
+    const StateArrays& Q = A.part;
+    const StateArrays& R = A.pred;
+    R.ax[p] = acc[0]; R.ay[p] = acc[1]; R.az[p] = acc[2];
+    R.lx[p] = alp[0]; R.ly[p] = alp[1]; R.lz[p] = alp[2];
+    x[0] = Q.px[p]; x[1] = Q.py[p]; x[2] = Q.pz[p];
+    v[0] = Q.vx[p]; v[1] = Q.vy[p]; v[2] = Q.vz[p];
+    w[0] = Q.wx[p]; w[1] = Q.wy[p]; w[2] = Q.wz[p];
+#pragma unroll
+    for (int d = 0; d < 3; d++) x[d] = x[d] + P.am0 * vp[d] + sv[d];
+#pragma unroll
+    for (int d = 0; d < 3; d++) v[d] = v[d] + P.am0 * acc[d] + sa[d];
+#pragma unroll
+    for (int d = 0; d < 3; d++) w[d] = w[d] + P.am0 * alp[d] + sl[d];
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+      if (P.pbc[d]) x[d] = x[d] - P.lbox[d] * fnint(x[d] * P.inv_lbox[d]);
+    Q.px[p] = x[0]; Q.py[p] = x[1]; Q.pz[p] = x[2];
+    Q.vx[p] = v[0]; Q.vy[p] = v[1]; Q.vz[p] = v[2];
+    Q.wx[p] = w[0]; Q.wy[p] = w[1]; Q.wz[p] = w[2];
+    bool out = false;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const double h = 0.5 * P.lbox[d];
+      out = out || (x[d] > h) || (x[d] < -h);
+    }
+    if (out) atomicAdd(&A.cnt->escaped, 1ull);
+  }
+  // the next pass's copies, cell and displacement
+  A.Xn[p] = make_double4(x[0], x[1], x[2], Rp);
+  A.v4n[p] = mk_v4<V4>(v[0], v[1], v[2], w[0]);
+  A.w2n[p] = mk_w2<W2>(w[1], w[2]);
+  note_cell(A.L, A.cnt, A.par_nxt, p, c_cur, current_cell(P, x[0], x[1], x[2]));
+  d2 = disp2(P, x, xp);
+}
+
+// Meta word of a candidate row.
+__device__ __forceinline__ void unpack_meta(int m, int& n1, int& n2b, int& n2a) {
+  n1 = m & META_MASK;
+  n2b = (m >> META_BITS) & META_MASK;
+  n2a = (m >> (2 * META_BITS)) & META_MASK;
+}
+
+__device__ __forceinline__ void set_abort(Counters* cnt, int tag) {
+  atomicCAS(&cnt->abort_tag, 0, tag + 1);
+  atomicExch(&cnt->abort, 1);
+}
+
+}  // namespace dem
