@@ -792,105 +792,122 @@ __global__ void __launch_bounds__(256) k_screen_full(const DevParams* __restrict
 template <bool PP, int EPI>
 __global__ void __launch_bounds__(128, 4) k_pass_fp64(PassArgs<double4, double2> A) {
   if (A.cnt->abort) return;
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = p0 < A.n;
+  const int p = valid ? p0 : 0;
+  const DevParams& P = *A.P;
+  const int n = A.n;
   unsigned long long n_col = 0, n_pc = 0, n_wc = 0;
   int need = 0;
   double d2 = 0.0;
-  if (p < A.n) {
-    const DevParams& P = *A.P;
-    const int n = A.n;
-    const int c = A.cell_cur[p];
-    const double4 p4 = A.X[p];
-    const double xp[3] = {p4.x, p4.y, p4.z};
-    const double Rp = p4.w;
-    const double4 pv4 = A.v4[p];
-    const double2 pw2 = A.w2[p];
-    const double vp[3] = {pv4.x, pv4.y, pv4.z};
-    const double wp[3] = {pv4.w, pw2.x, pw2.y};
-    const int cp = PP ? 0 : A.comp[p];
-    double inv_m, inv_i, eff_m;
-    Material<PP>::self(P, cp, Rp, inv_m, inv_i, eff_m);
-    int n1, n2b, n2a;
-    unpack_meta(A.meta[p], n1, n2b, n2a);
-    const double half_dt = A.half_dt;
-    const bool update = A.update != 0;
-    int hw_n = 0;
-    bool overflow = false;
 
-    double iF[3], iT[3] = {0.0, 0.0, 0.0};
+  const int c = A.cell_cur[p];
+  const double4 p4 = A.X[p];
+  const double xp[3] = {p4.x, p4.y, p4.z};
+  const double Rp = p4.w;
+  const double4 pv4 = A.v4[p];
+  const double2 pw2 = A.w2[p];
+  const double vp[3] = {pv4.x, pv4.y, pv4.z};
+  const double wp[3] = {pv4.w, pw2.x, pw2.y};
+  const int cp = PP ? 0 : A.comp[p];
+  double inv_m, inv_i, eff_m;
+  Material<PP>::self(P, cp, Rp, inv_m, inv_i, eff_m);
+  int n1, n2b, n2a;
+  unpack_meta(A.meta[p], n1, n2b, n2a);
+  const double half_dt = A.half_dt;
+  const bool update = A.update != 0;
+  int hw_n = 0;
+  bool overflow = false;
+
+  double iF[3], iT[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-    for (int k = 0; k < 3; k++) iF[k] = eff_m * P.gravity[k];
+  for (int k = 0; k < 3; k++) iF[k] = eff_m * P.gravity[k];
+  double F[3] = {0.0, 0.0, 0.0}, T[3] = {0.0, 0.0, 0.0};
 
-    auto record = [&](int partner, const double ft[3], const double vt[3]) {
-      if (hw_n < A.Hw.cap)
-        hist_write(A.Hw, p, hw_n, partner, ft, vt);
-      else
-        overflow = true;
-      hw_n++;
-    };
-    // Rij = xb - xa (minimum image, src/MForces.f90:209-217) and the overlap
-    // test DeltaDijSq = MinDijSq - DijSq > 0 of the pair (a = "i", b = "j")
-    auto geometry = [&](const double xa[3], const double4 xb, double Rij[3]) -> double {
-      Rij[0] = xb.x - xa[0];
-      Rij[1] = xb.y - xa[1];
-      Rij[2] = xb.z - xa[2];
+  auto record = [&](int partner, const double ft[3], const double vt[3]) {
+    if (hw_n < A.Hw.cap)
+      hist_write(A.Hw, p, hw_n, partner, ft, vt);
+    else
+      overflow = true;
+    hw_n++;
+  };
+  // Rij = x_j - x_i (minimum image, src/MForces.f90:209-217); candidate k
+  // of the row is "j" (p is "i") for k < n1, else "i"
+  auto geometry = [&](bool pi, const double4& q4, double Rij[3]) -> double {
+    Rij[0] = pi ? q4.x - xp[0] : xp[0] - q4.x;
+    Rij[1] = pi ? q4.y - xp[1] : xp[1] - q4.y;
+    Rij[2] = pi ? q4.z - xp[2] : xp[2] - q4.z;
 #pragma unroll
-      for (int k = 0; k < 3; k++)
-        if (P.pbc[k]) Rij[k] = Rij[k] - P.lbox[k] * fnint(Rij[k] * P.inv_lbox[k]);
-      return sumsq3(Rij);
-    };
-    auto contact_i = [&](int q, double4 q4) -> bool {
-      double Rij[3];
-      const double DijSq = geometry(xp, q4, Rij);
-      const int cq = PP ? 0 : A.comp[q];
-      return Material<PP>::min_dij_sq(P, cp, Rp, cq, q4.w) - DijSq > 0.0;
-    };
-    auto contact_j = [&](int q, double4 q4) -> bool {
-      double Rij[3];
-      const double qx[3] = {q4.x, q4.y, q4.z};
-      const double DijSq = geometry(qx, make_double4(xp[0], xp[1], xp[2], Rp), Rij);
-      const int cq = PP ? 0 : A.comp[q];
-      return Material<PP>::min_dij_sq(P, cq, q4.w, cp, Rp) - DijSq > 0.0;
-    };
-
-    // p is "i", q is "j" (src/MForces.f90:199-272)
-    auto visit_i = [&](int q) {
-      const double4 q4 = A.X[q];
-      double Rij[3];
-      const double DijSq = geometry(xp, q4, Rij);
-      const int cq = PP ? 0 : A.comp[q];
-      const double Delta = Material<PP>::min_dij_sq(P, cp, Rp, cq, q4.w) - DijSq;
-      PairPar pp;
-      Material<PP>::pair(P, cp, Rp, cq, q4.w, pp);
-      const double4 qv4 = A.v4[q];
-      const double2 qw2 = A.w2[q];
-      const double vq[3] = {qv4.x, qv4.y, qv4.z};
-      const double wq[3] = {qv4.w, qw2.x, qw2.y};
-      const int lo = p < q ? p : q, hi = p < q ? q : p;
-      double FT0[3] = {0.0, 0.0, 0.0}, VT0[3] = {0.0, 0.0, 0.0};
-      const int r = hist_find(A.Hr, lo, hi);
-      const bool contacting = r >= 0;
-      if (contacting) hist_read(A.Hr, lo, r, FT0, VT0);
+    for (int k = 0; k < 3; k++)
+      if (P.pbc[k]) Rij[k] = Rij[k] - P.lbox[k] * fnint(Rij[k] * P.inv_lbox[k]);
+    return sumsq3(Rij);
+  };
+  // the overlap test DeltaDijSq = MinDijSq - DijSq > 0 (src/MForces.f90:218-224)
+  auto test = [&](int k, int q, const double4& q4) -> bool {
+    const bool pi = k < n1;
+    double Rij[3];
+    const double DijSq = geometry(pi, q4, Rij);
+    const int cq = PP ? 0 : A.comp[q];
+    const double mds = pi ? Material<PP>::min_dij_sq(P, cp, Rp, cq, q4.w)
+                          : Material<PP>::min_dij_sq(P, cq, q4.w, cp, Rp);
+    return mds - DijSq > 0.0;
+  };
+  // one contact in the reference's orientation (src/MForces.f90:199-272)
+  auto visit = [&](int k) {
+    const int q = __ldg(A.cand + (size_t)k * n + p);
+    const bool pi = k < n1;
+    const double4 q4 = A.X[q];
+    double Rij[3];
+    const double DijSq = geometry(pi, q4, Rij);
+    const int cq = PP ? 0 : A.comp[q];
+    const int ca = pi ? cp : cq, cb = pi ? cq : cp;
+    const double Ra = pi ? Rp : q4.w, Rb = pi ? q4.w : Rp;
+    const double Delta = Material<PP>::min_dij_sq(P, ca, Ra, cb, Rb) - DijSq;
+    PairPar pp;
+    Material<PP>::pair(P, ca, Ra, cb, Rb, pp);
+    const double4 qv4 = A.v4[q];
+    const double2 qw2 = A.w2[q];
+    const double vq[3] = {qv4.x, qv4.y, qv4.z};
+    const double wq[3] = {qv4.w, qw2.x, qw2.y};
+    double va[3], wa[3], vb[3], wb[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      va[d] = pi ? vp[d] : vq[d];
+      wa[d] = pi ? wp[d] : wq[d];
+      vb[d] = pi ? vq[d] : vp[d];
+      wb[d] = pi ? wq[d] : wp[d];
+    }
+    const int lo = p < q ? p : q, hi = p < q ? q : p;
+    double FT0[3] = {0.0, 0.0, 0.0}, VT0[3] = {0.0, 0.0, 0.0};
+    const int r = hist_find(A.Hr, lo, hi);
+    const bool contacting = r >= 0;
+    if (contacting) hist_read(A.Hr, lo, r, FT0, VT0);
+    if (pi) {
       if (!contacting) n_col++;
       n_pc++;
-      ContactOut o;
-      pair_contact(Rij, DijSq, Delta, pp, Rp, vp, wp, q4.w, vq, wq, half_dt, contacting, FT0, VT0,
-                   o);
+    }
+    ContactOut o;
+    pair_contact(Rij, DijSq, Delta, pp, Ra, va, wa, Rb, vb, wb, half_dt, contacting, FT0, VT0,
+                 o);
+    if (pi) {
 #pragma unroll
-      for (int k = 0; k < 3; k++) iF[k] = iF[k] + o.FN[k] + o.FT[k];
+      for (int d = 0; d < 3; d++) iF[d] = iF[d] + o.FN[d] + o.FT[d];
       double RN[3], tq[3];
 #pragma unroll
-      for (int k = 0; k < 3; k++) RN[k] = Rp * o.N[k];
+      for (int d = 0; d < 3; d++) RN[d] = Rp * o.N[d];
       cross3(RN, o.FT, tq);
 #pragma unroll
-      for (int k = 0; k < 3; k++) iT[k] = iT[k] + tq[k];
-      if (update && p < q) record(q, o.FT, o.VT);
-    };
-
-    // ---- loop 1: own cell after p, then the half-shell cells
-    walk_segment(A.cand, A.X, n, p, 0, n1, contact_i, visit_i);
-
-    // ---- walls (src/MForces.f90:274-314)
+      for (int d = 0; d < 3; d++) iT[d] = iT[d] + tq[d];
+    } else {
+#pragma unroll
+      for (int d = 0; d < 3; d++) F[d] = F[d] - o.FN[d] - o.FT[d];
+#pragma unroll
+      for (int d = 0; d < 3; d++) T[d] = T[d] + Rp * o.NxFT[d];
+    }
+    if (update && p < q) record(q, o.FT, o.VT);
+  };
+  // walls (src/MForces.f90:274-314)
+  auto walls = [&]() {
     for (int w = 0; w < P.nw; w++) {
       const dem_wall& W = P.walls[w];
       const int wi = p * P.nw + w;
@@ -947,44 +964,18 @@ __global__ void __launch_bounds__(128, 4) k_pass_fp64(PassArgs<double4, double2>
         A.Hw.wflag[wi] = 0;
       }
     }
-
-    // ---- loop 2: p as "j"; contributions in the order the sweep reaches
-    // the "i" particle, own block (Force(i) = Force(i) + iForce) at p's turn.
-    double F[3] = {0.0, 0.0, 0.0}, T[3] = {0.0, 0.0, 0.0};
-    auto visit_j = [&](int q) {
-      const double4 q4 = A.X[q];
-      double Rij[3];
-      const double qx[3] = {q4.x, q4.y, q4.z};
-      const double DijSq = geometry(qx, make_double4(xp[0], xp[1], xp[2], Rp), Rij);
-      const int cq = PP ? 0 : A.comp[q];
-      const double Delta = Material<PP>::min_dij_sq(P, cq, q4.w, cp, Rp) - DijSq;
-      PairPar pp;
-      Material<PP>::pair(P, cq, q4.w, cp, Rp, pp);
-      const double4 qv4 = A.v4[q];
-      const double2 qw2 = A.w2[q];
-      const double vq[3] = {qv4.x, qv4.y, qv4.z};
-      const double wq[3] = {qv4.w, qw2.x, qw2.y};
-      const int lo = p < q ? p : q, hi = p < q ? q : p;
-      double FT0[3] = {0.0, 0.0, 0.0}, VT0[3] = {0.0, 0.0, 0.0};
-      const int r = hist_find(A.Hr, lo, hi);
-      const bool contacting = r >= 0;
-      if (contacting) hist_read(A.Hr, lo, r, FT0, VT0);
-      ContactOut o;
-      pair_contact(Rij, DijSq, Delta, pp, q4.w, vq, wq, Rp, vp, wp, half_dt, contacting, FT0,
-                   VT0, o);
-#pragma unroll
-      for (int k = 0; k < 3; k++) F[k] = F[k] - o.FN[k] - o.FT[k];
-#pragma unroll
-      for (int k = 0; k < 3; k++) T[k] = T[k] + Rp * o.NxFT[k];
-      if (update && p < q) record(q, o.FT, o.VT);
-    };
-    walk_segment(A.cand, A.X, n, p, n1, n1 + n2b, contact_j, visit_j);
+  };
+  // Force(i) = Force(i) + iForce where p's own block ends (src/MForces.f90:319-320)
+  auto own = [&]() {
 #pragma unroll
     for (int k = 0; k < 3; k++) F[k] = F[k] + iF[k];
 #pragma unroll
     for (int k = 0; k < 3; k++) T[k] = T[k] + iT[k];
-    walk_segment(A.cand, A.X, n, p, n1 + n2b, n1 + n2b + n2a, contact_j, visit_j);
+  };
+  contact_loop(A.cand, A.X, n, p, valid, n1, n2b, n1 + n2b + n2a, P.nw > 0, test, visit, walls,
+               own);
 
+  if (valid) {
     // ---- records of pairs the sweep did not visit are kept as they were
     if (update) {
       const int nold = A.Hr.cnt[p];
@@ -1004,7 +995,6 @@ __global__ void __launch_bounds__(128, 4) k_pass_fp64(PassArgs<double4, double2>
       }
       need = hw_n;
     }
-
     // ---- a = F/m, alpha = T/I (src/MForces.f90:330-333) + epilogue
     double acc[3], alp[3];
 #pragma unroll

@@ -245,108 +245,117 @@ __device__ __forceinline__ unsigned long long wsum(unsigned long long v) {
 template <bool PP, int EPI>
 __global__ void __launch_bounds__(128, 4) k_pass_mixed(PassArgs<float4, float2> A, MixedView V) {
   if (A.cnt->abort) return;
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = p0 < A.n;
+  const int p = valid ? p0 : 0;
+  const DevParams& P = *A.P;
+  const int n = A.n;
   unsigned long long n_col = 0, n_pc = 0, n_wc = 0;
   int need = 0;
   double d2 = 0.0;
-  if (p < A.n) {
-    const DevParams& P = *A.P;
-    const int n = A.n;
-    const int c = A.cell_cur[p];
-    const double4 p4 = A.X[p];
-    const double xp[3] = {p4.x, p4.y, p4.z};
-    const double Rpd = p4.w;
-    const float Rp = (float)Rpd;
-    const float4 pv4 = A.v4[p];
-    const float2 pw2 = A.w2[p];
-    const F3 vp = mk(pv4.x, pv4.y, pv4.z);
-    const F3 wp = mk(pv4.w, pw2.x, pw2.y);
-    const int cp = PP ? 0 : A.comp[p];
-    float inv_m, inv_i, eff_m;
-    MMat<PP>::self(P, cp, Rp, inv_m, inv_i, eff_m);
-    int n1, n2b, n2a;
-    unpack_meta(A.meta[p], n1, n2b, n2a);
-    const float half_dt = (float)A.half_dt;
-    const bool update = A.update != 0;
-    int hw_n = 0;
-    bool overflow = false;
-    const History& Hr = A.Hr;
-    const History& Hw = A.Hw;
 
-    F3 iF = mk(eff_m * (float)P.gravity[0], eff_m * (float)P.gravity[1],
-               eff_m * (float)P.gravity[2]);
-    F3 iT = mk(0.f, 0.f, 0.f);
+  const int c = A.cell_cur[p];
+  const double4 p4 = A.X[p];
+  const double xp[3] = {p4.x, p4.y, p4.z};
+  const double Rpd = p4.w;
+  const float Rp = (float)Rpd;
+  const float4 pv4 = A.v4[p];
+  const float2 pw2 = A.w2[p];
+  const F3 vp = mk(pv4.x, pv4.y, pv4.z);
+  const F3 wp = mk(pv4.w, pw2.x, pw2.y);
+  const int cp = PP ? 0 : A.comp[p];
+  float inv_m, inv_i, eff_m;
+  MMat<PP>::self(P, cp, Rp, inv_m, inv_i, eff_m);
+  int n1, n2b, n2a;
+  unpack_meta(A.meta[p], n1, n2b, n2a);
+  const float half_dt = (float)A.half_dt;
+  const bool update = A.update != 0;
+  int hw_n = 0;
+  bool overflow = false;
+  const History& Hr = A.Hr;
+  const History& Hw = A.Hw;
 
-    auto record = [&](int partner, F3 ft, F3 lo, F3 vt) {
-      if (hw_n < Hw.cap) {
-        size_t i = (size_t)p * Hw.cap + hw_n;
-        Hw.key[i] = partner;
-        rec_write(V.wa, V.wb, V.wc, i, ft, lo, vt);
-      } else {
-        overflow = true;
+  F3 iF = mk(eff_m * (float)P.gravity[0], eff_m * (float)P.gravity[1],
+             eff_m * (float)P.gravity[2]);
+  F3 iT = mk(0.f, 0.f, 0.f);
+  F3 F = mk(0.f, 0.f, 0.f), T = mk(0.f, 0.f, 0.f);
+
+  auto record = [&](int partner, F3 ft, F3 lo, F3 vt) {
+    if (hw_n < Hw.cap) {
+      size_t i = (size_t)p * Hw.cap + hw_n;
+      Hw.key[i] = partner;
+      rec_write(V.wa, V.wb, V.wc, i, ft, lo, vt);
+    } else {
+      overflow = true;
+    }
+    hw_n++;
+  };
+  auto lookup = [&](int lo_i, int hi_i, F3& ft, F3& lo, F3& vt) -> bool {
+    const int cnt = Hr.cnt[lo_i];
+    const int* k = Hr.key + (size_t)lo_i * Hr.cap;
+    for (int r = 0; r < cnt; r++)
+      if (k[r] == hi_i) {
+        rec_read(V.ra, V.rb, V.rc, (size_t)lo_i * Hr.cap + r, ft, lo, vt);
+        return true;
       }
-      hw_n++;
-    };
-    auto lookup = [&](int lo_i, int hi_i, F3& ft, F3& lo, F3& vt) -> bool {
-      const int cnt = Hr.cnt[lo_i];
-      const int* k = Hr.key + (size_t)lo_i * Hr.cap;
-      for (int r = 0; r < cnt; r++)
-        if (k[r] == hi_i) {
-          rec_read(V.ra, V.rb, V.rc, (size_t)lo_i * Hr.cap + r, ft, lo, vt);
-          return true;
-        }
-      ft = lo = vt = mk(0.f, 0.f, 0.f);
-      return false;
-    };
-    // Rij = xb - xa (minimum image, FP64) and DijSq
-    auto geometry = [&](double ax, double ay, double az, double bx, double by, double bz,
-                        double Rij[3]) -> double {
-      Rij[0] = bx - ax;
-      Rij[1] = by - ay;
-      Rij[2] = bz - az;
+    ft = lo = vt = mk(0.f, 0.f, 0.f);
+    return false;
+  };
+  // Rij = x_j - x_i (minimum image, FP64); candidate k is "j" for k < n1
+  auto geometry = [&](bool pi, const double4& q4, double Rij[3]) -> double {
+    Rij[0] = pi ? q4.x - xp[0] : xp[0] - q4.x;
+    Rij[1] = pi ? q4.y - xp[1] : xp[1] - q4.y;
+    Rij[2] = pi ? q4.z - xp[2] : xp[2] - q4.z;
 #pragma unroll
-      for (int k = 0; k < 3; k++)
-        if (P.pbc[k]) Rij[k] = Rij[k] - P.lbox[k] * fnint(Rij[k] * P.inv_lbox[k]);
-      return sumsq3(Rij);
-    };
-    auto contact_i = [&](int q, double4 q4) -> bool {
-      double Rij[3];
-      const double DijSq = geometry(xp[0], xp[1], xp[2], q4.x, q4.y, q4.z, Rij);
-      const int cq = PP ? 0 : A.comp[q];
-      return MMat<PP>::min_dij_sq(P, cp, Rpd, cq, q4.w) - DijSq > 0.0;
-    };
-    auto contact_j = [&](int q, double4 q4) -> bool {
-      double Rij[3];
-      const double DijSq = geometry(q4.x, q4.y, q4.z, xp[0], xp[1], xp[2], Rij);
-      const int cq = PP ? 0 : A.comp[q];
-      return MMat<PP>::min_dij_sq(P, cq, q4.w, cp, Rpd) - DijSq > 0.0;
-    };
-
-    auto visit_i = [&](int q) {
-      const double4 q4 = A.X[q];
-      double Rij[3];
-      const double DijSq = geometry(xp[0], xp[1], xp[2], q4.x, q4.y, q4.z, Rij);
-      const int cq = PP ? 0 : A.comp[q];
-      const double Delta = MMat<PP>::min_dij_sq(P, cp, Rpd, cq, q4.w) - DijSq;
-      const float Rq = (float)q4.w;
-      MPair m;
-      MMat<PP>::pair(P, cp, Rp, cq, Rq, m);
-      const float4 qv4 = A.v4[q];
-      const float2 qw2 = A.w2[q];
-      const int lo_i = p < q ? p : q, hi_i = p < q ? q : p;
-      F3 ft0, ft0lo, vt0;
-      const bool contacting = lookup(lo_i, hi_i, ft0, ft0lo, vt0);
+    for (int k = 0; k < 3; k++)
+      if (P.pbc[k]) Rij[k] = Rij[k] - P.lbox[k] * fnint(Rij[k] * P.inv_lbox[k]);
+    return sumsq3(Rij);
+  };
+  auto test = [&](int k, int q, const double4& q4) -> bool {
+    const bool pi = k < n1;
+    double Rij[3];
+    const double DijSq = geometry(pi, q4, Rij);
+    const int cq = PP ? 0 : A.comp[q];
+    const double mds = pi ? MMat<PP>::min_dij_sq(P, cp, Rpd, cq, q4.w)
+                          : MMat<PP>::min_dij_sq(P, cq, q4.w, cp, Rpd);
+    return mds - DijSq > 0.0;
+  };
+  auto visit = [&](int k) {
+    const int q = __ldg(A.cand + (size_t)k * n + p);
+    const bool pi = k < n1;
+    const double4 q4 = A.X[q];
+    double Rij[3];
+    const double DijSq = geometry(pi, q4, Rij);
+    const int cq = PP ? 0 : A.comp[q];
+    const int ca = pi ? cp : cq, cb = pi ? cq : cp;
+    const double Rad = pi ? Rpd : q4.w, Rbd = pi ? q4.w : Rpd;
+    const double Delta = MMat<PP>::min_dij_sq(P, ca, Rad, cb, Rbd) - DijSq;
+    const float Ra = (float)Rad, Rb = (float)Rbd;
+    MPair m;
+    MMat<PP>::pair(P, ca, Ra, cb, Rb, m);
+    const float4 qv4 = A.v4[q];
+    const float2 qw2 = A.w2[q];
+    const F3 vq = mk(qv4.x, qv4.y, qv4.z), wq = mk(qv4.w, qw2.x, qw2.y);
+    const int lo_i = p < q ? p : q, hi_i = p < q ? q : p;
+    F3 ft0, ft0lo, vt0;
+    const bool contacting = lookup(lo_i, hi_i, ft0, ft0lo, vt0);
+    if (pi) {
       if (!contacting) n_col++;
       n_pc++;
-      MOut o;
-      mixed_pair(Rij, DijSq, Delta, m, Rp, vp, wp, Rq, mk(qv4.x, qv4.y, qv4.z),
-                 mk(qv4.w, qw2.x, qw2.y), half_dt, contacting, ft0, ft0lo, vt0, o);
+    }
+    MOut o;
+    mixed_pair(Rij, DijSq, Delta, m, Ra, pi ? vp : vq, pi ? wp : wq, Rb, pi ? vq : vp,
+               pi ? wq : wp, half_dt, contacting, ft0, ft0lo, vt0, o);
+    if (pi) {
       iF = iF + o.FN + (o.FT + o.FTlo);
       iT = iT + cross(Rp * o.N, o.FT);
-      if (update && p < q) record(q, o.FT, o.FTlo, o.VT);
-    };
-    walk_segment(A.cand, A.X, n, p, 0, n1, contact_i, visit_i);
-
+    } else {
+      F = F - o.FN - (o.FT + o.FTlo);
+      T = T + Rp * o.NxFT;
+    }
+    if (update && p < q) record(q, o.FT, o.FTlo, o.VT);
+  };
+  auto walls = [&]() {
     for (int w = 0; w < P.nw; w++) {
       const dem_wall& W = P.walls[w];
       const size_t wi = (size_t)p * P.nw + w;
@@ -384,34 +393,15 @@ __global__ void __launch_bounds__(128, 4) k_pass_mixed(PassArgs<float4, float2> 
         Hw.wflag[wi] = 0;
       }
     }
-
-    F3 F = mk(0.f, 0.f, 0.f), T = mk(0.f, 0.f, 0.f);
-    auto visit_j = [&](int q) {
-      const double4 q4 = A.X[q];
-      double Rij[3];
-      const double DijSq = geometry(q4.x, q4.y, q4.z, xp[0], xp[1], xp[2], Rij);
-      const int cq = PP ? 0 : A.comp[q];
-      const double Delta = MMat<PP>::min_dij_sq(P, cq, q4.w, cp, Rpd) - DijSq;
-      const float Rq = (float)q4.w;
-      MPair m;
-      MMat<PP>::pair(P, cq, Rq, cp, Rp, m);
-      const float4 qv4 = A.v4[q];
-      const float2 qw2 = A.w2[q];
-      const int lo_i = p < q ? p : q, hi_i = p < q ? q : p;
-      F3 ft0, ft0lo, vt0;
-      const bool contacting = lookup(lo_i, hi_i, ft0, ft0lo, vt0);
-      MOut o;
-      mixed_pair(Rij, DijSq, Delta, m, Rq, mk(qv4.x, qv4.y, qv4.z), mk(qv4.w, qw2.x, qw2.y), Rp,
-                 vp, wp, half_dt, contacting, ft0, ft0lo, vt0, o);
-      F = F - o.FN - (o.FT + o.FTlo);
-      T = T + Rp * o.NxFT;
-      if (update && p < q) record(q, o.FT, o.FTlo, o.VT);
-    };
-    walk_segment(A.cand, A.X, n, p, n1, n1 + n2b, contact_j, visit_j);
+  };
+  auto own = [&]() {
     F = F + iF;
     T = T + iT;
-    walk_segment(A.cand, A.X, n, p, n1 + n2b, n1 + n2b + n2a, contact_j, visit_j);
+  };
+  contact_loop(A.cand, A.X, n, p, valid, n1, n2b, n1 + n2b + n2a, P.nw > 0, test, visit, walls,
+               own);
 
+  if (valid) {
     if (update) {
       const int nold = Hr.cnt[p];
       for (int r = 0; r < nold; r++) {
@@ -430,7 +420,6 @@ __global__ void __launch_bounds__(128, 4) k_pass_mixed(PassArgs<float4, float2> 
       }
       need = hw_n;
     }
-
     const double acc[3] = {(double)(F.x * inv_m), (double)(F.y * inv_m), (double)(F.z * inv_m)};
     const double alp[3] = {(double)(T.x * inv_i), (double)(T.y * inv_i), (double)(T.z * inv_i)};
     // the integrator runs on FP64 velocities: Particle's for the predictor,

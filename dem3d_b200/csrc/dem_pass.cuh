@@ -61,33 +61,62 @@ __device__ __forceinline__ void publish_disp(Counters* cnt, double d2) {
   }
 }
 
-// Walk candidates k0..k1-1 of particle p: prefetch four at a time (index,
-// then position), keep those for which contact(q, xq) holds, and hand them
-// to visit(q) in row order.
-template <class Contact, class Visit>
-__device__ __forceinline__ void walk_segment(const int* __restrict__ cand,
-                                             const double4* __restrict__ X, int n, int p, int k0,
-                                             int k1, Contact&& contact, Visit&& visit) {
+// The contacts of particle p in row order, processed in lockstep across the
+// warp.  The row's candidates are tested first (test(k, q, xq), four
+// prefetched at a time) into a bit mask per chunk of 64 candidates; then
+// every lane takes its next contact in the same iteration, so the heavy
+// contact arithmetic runs max-over-lanes times per warp instead of once per
+// contact of every lane.  Row order fixes the reference's summation order:
+// loop-1 contacts (k < n1), then walls(), then the loop-2 contacts before
+// p's own block (k < n1 + n2b), own(), then the rest.  All 32 lanes must
+// call this; `valid` is false for lanes without a particle.
+template <class Test, class Visit, class Walls, class Own>
+__device__ __forceinline__ void contact_loop(const int* __restrict__ cand,
+                                             const double4* __restrict__ X, int n, int p,
+                                             bool valid, int n1, int n2b, int m, bool has_walls,
+                                             Test&& test, Visit&& visit, Walls&& walls,
+                                             Own&& own) {
+  const unsigned FULL = 0xffffffffu;
+  bool walls_pending = valid && has_walls;
+  bool own_pending = valid;
+  if (!valid) m = 0;
+  const int mmax = (int)__reduce_max_sync(FULL, (unsigned)m);
+  for (int base = 0; base < mmax; base += 64) {
+    unsigned long long mask = 0ull;
+    const int end = m < base + 64 ? m : base + 64;
 #pragma unroll 1
-  for (int b = k0; b < k1; b += 4) {
-    int q[4];
+    for (int b = base; b < end; b += 4) {
+      int q[4];
 #pragma unroll
-    for (int u = 0; u < 4; u++) q[u] = b + u < k1 ? __ldg(cand + (size_t)(b + u) * n + p) : -1;
-    double4 xq[4];
+      for (int u = 0; u < 4; u++) q[u] = b + u < end ? __ldg(cand + (size_t)(b + u) * n + p) : -1;
+      double4 xq[4];
 #pragma unroll
-    for (int u = 0; u < 4; u++)
-      xq[u] = q[u] >= 0 ? X[q[u]] : make_double4(0.0, 0.0, 0.0, 0.0);
-    unsigned msk = 0u;
+      for (int u = 0; u < 4; u++)
+        xq[u] = q[u] >= 0 ? X[q[u]] : make_double4(0.0, 0.0, 0.0, 0.0);
 #pragma unroll
-    for (int u = 0; u < 4; u++)
-      if (q[u] >= 0 && contact(q[u], xq[u])) msk |= 1u << u;
+      for (int u = 0; u < 4; u++)
+        if (q[u] >= 0 && test(b + u, q[u], xq[u])) mask |= 1ull << (b + u - base);
+    }
 #pragma unroll 1
-    for (int u = 0; u < 4; u++) {
-      if (!((msk >> u) & 1u)) continue;
-      const int qq = u == 0 ? q[0] : u == 1 ? q[1] : u == 2 ? q[2] : q[3];
-      visit(qq);
+    while (true) {
+      const int k = mask ? base + __ffsll((long long)mask) - 1 : -1;
+      if (walls_pending && k >= n1) {
+        walls();
+        walls_pending = false;
+      }
+      if (own_pending && !walls_pending && k >= n1 + n2b) {
+        own();
+        own_pending = false;
+      }
+      if (!__any_sync(FULL, k >= 0)) break;
+      if (k >= 0) {
+        visit(k);
+        mask &= mask - 1ull;
+      }
     }
   }
+  if (walls_pending) walls();
+  if (own_pending) own();
 }
 
 template <class T>
