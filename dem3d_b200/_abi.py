@@ -134,7 +134,9 @@ NOALLOC_MAX_PARTICLES = 262144
 NOALLOC_MAX_CELLS = 262144
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libdem3d_b200.so")
+# DEM3D_B200_LIB selects another build of the same library (e.g. one compiled
+# with different launch bounds); the default is the in-tree build.
+LIB_PATH = os.environ.get("DEM3D_B200_LIB") or os.path.join(HERE, "libdem3d_b200.so")
 
 
 def bind(lib: C.CDLL, prefix: str, table: dict) -> None:

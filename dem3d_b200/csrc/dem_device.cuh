@@ -29,6 +29,7 @@ struct DevParams {
   double max_min_dij_sq;  // largest MinDijSq of any pair (screening early-out)
   double vl_skin;         // candidate-row skin (added to MinDij)
   double vl_thr;          // accumulated displacement bound that forces a full rebuild
+  double inv_nx, inv_ny;  // 1/Nx, 1/Ny (cell coordinates without integer division)
   double comp_radius[NCM], comp_inv_mass[NCM], comp_inv_inertia[NCM], comp_eff_mass[NCM];
   double min_dij[NCM * NCM], min_dij_sq[NCM * NCM];
   double kn[NCM * NCM], yn[NCM * NCM], kt[NCM * NCM], yt[NCM * NCM], mu_sq[NCM * NCM];
@@ -64,20 +65,26 @@ struct Counters {
   int row_overflow;  // a candidate row needed more than kc entries
   int need_kc;       // longest candidate row requested
   int list_error;    // a cell-list walk exceeded its bound (corrupt lists)
-  unsigned long long disp_max;  // bits of the largest displacement bound of one pass
+  unsigned int disp_max;  // FP32 bits (rounded up) of the largest displacement of one pass
   double disp_acc;   // sum of disp_max since the last full rebuild
   double wall_fn[NWM];
 };
 
-// Contact history, one table per buffer: records owned by imin.
+// Contact history, one table per buffer: records owned by imin, stored slot
+// major (record r of particle i at r*n + i), so that the first records of
+// neighbouring particles share cache lines.
 struct History {
   int* cnt;       // [n] records owned by particle
-  int* key;       // [n*cap] partner (imax)
-  double2* val;   // [n*cap*3] (ft.x,ft.y) (ft.z,vt.x) (vt.y,vt.z)
+  int* key;       // [cap*n] partner (imax)
+  double2* val;   // [cap*n*3] (ft.x,ft.y) (ft.z,vt.x) (vt.y,vt.z)
   int* wflag;     // [n*nw] wall record present
   double2* wval;  // [n*nw*3]
   int cap;
+  int n;          // particles (rows of every slot)
 };
+__device__ __host__ __forceinline__ size_t hslot(const History& H, int i, int r) {
+  return (size_t)r * (size_t)H.n + (size_t)i;
+}
 
 // Traversal-order arrays of the counting sort that builds the initial cell
 // lists (DistributeParticles3D) and serves the allocation-free entry point.
@@ -131,9 +138,28 @@ constexpr int KC_MAX = META_MASK;
 
 // Arguments of one pass kernel.  V4/W2 are the velocity copies the pass
 // reads for partners (double in FP64 mode, float in mixed mode).
+// Periodic box of a pass, passed by value (kernel parameter space) so the
+// per-candidate minimum image reads no memory.
+struct Box {
+  double lbox[3], inv_lbox[3];
+  double half_lim[3];  // 0.49 lbox: |r| below it has nint(r/L) = 0 exactly
+  int pbc[3];
+};
+
+// Minimum image of one component, Rij(k) - Lbox(k)*nint(Rij(k)*InvLbox(k))
+// (src/MForces.f90:212-214), bit for bit: when |r| < 0.49 L the nint is 0
+// and the expression is r itself, so the formula is only evaluated for
+// pairs that straddle the periodic boundary.
+__device__ __forceinline__ double min_image_exact(double r, const Box& B, int k) {
+  if (B.pbc[k] && !(fabs(r) < B.half_lim[k]))
+    r = r - B.lbox[k] * (double)(int)round(r * B.inv_lbox[k]);
+  return r;
+}
+
 template <class V4, class W2>
 struct PassArgs {
   const DevParams* P;
+  Box box;
   int n;
   const double4* X;   // this pass's positions (x, y, z, R) by original index
   const V4* v4;       // vx, vy, vz, wx
@@ -363,9 +389,34 @@ __device__ __forceinline__ int current_cell(const DevParams& P, double x, double
 // other's half-shell list)?  With >= 3 cells along every periodic axis this
 // is plain adjacency with wrap-around (VerifyPBC/ApplyPBC, src/MCells.f90:
 // 1030-1052).
+// q = c / d and c - q*d for 0 <= c < 2^31, d >= 1, from a reciprocal (one
+// correction step makes it exact)
+__device__ __forceinline__ int div_fast(int c, int d, double inv_d, int& rem) {
+  int q = (int)((double)c * inv_d);
+  int r = c - q * d;
+  if (r >= d) {
+    q++;
+    r -= d;
+  } else if (r < 0) {
+    q--;
+    r += d;
+  }
+  rem = r;
+  return q;
+}
+__device__ __forceinline__ void cell_coords(const DevParams& P, int c, int& x, int& y, int& z) {
+  const int t = div_fast(c, P.nx, P.inv_nx, x);
+  z = div_fast(t, P.ny, P.inv_ny, y);
+}
+
+// Are two cells neighbours in the sweep sense (same cell, or one in the
+// other's half-shell list)?  With >= 3 cells along every periodic axis this
+// is plain adjacency with wrap-around (VerifyPBC/ApplyPBC, src/MCells.f90:
+// 1030-1052).
 __device__ __forceinline__ bool cells_adjacent(const DevParams& P, int a, int b) {
-  int ax = a % P.nx, ay = (a / P.nx) % P.ny, az = a / (P.nx * P.ny);
-  int bx = b % P.nx, by = (b / P.nx) % P.ny, bz = b / (P.nx * P.ny);
+  int ax, ay, az, bx, by, bz;
+  cell_coords(P, a, ax, ay, az);
+  cell_coords(P, b, bx, by, bz);
   int d[3] = {bx - ax, by - ay, bz - az};
   int N[3] = {P.nx, P.ny, P.nz};
 #pragma unroll

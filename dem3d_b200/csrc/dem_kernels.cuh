@@ -280,17 +280,9 @@ struct Material<true> {
 // ---------------------------------------------------------------------------
 // history access
 
-__device__ __forceinline__ int hist_find(const History& H, int owner, int partner) {
-  int c = H.cnt[owner];
-  const int* k = H.key + (size_t)owner * H.cap;
-  for (int r = 0; r < c; r++)
-    if (k[r] == partner) return r;
-  return -1;
-}
-
 __device__ __forceinline__ void hist_read(const History& H, int owner, int r, double ft[3],
                                           double vt[3]) {
-  const double2* v = H.val + ((size_t)owner * H.cap + r) * 3;
+  const double2* v = H.val + hslot(H, owner, r) * 3;
   double2 a = v[0], b = v[1], c = v[2];
   ft[0] = a.x; ft[1] = a.y; ft[2] = b.x;
   vt[0] = b.y; vt[1] = c.x; vt[2] = c.y;
@@ -298,8 +290,8 @@ __device__ __forceinline__ void hist_read(const History& H, int owner, int r, do
 
 __device__ __forceinline__ void hist_write(const History& H, int owner, int r, int partner,
                                            const double ft[3], const double vt[3]) {
-  H.key[(size_t)owner * H.cap + r] = partner;
-  double2* v = H.val + ((size_t)owner * H.cap + r) * 3;
+  H.key[hslot(H, owner, r)] = partner;
+  double2* v = H.val + hslot(H, owner, r) * 3;
   v[0] = make_double2(ft[0], ft[1]);
   v[1] = make_double2(ft[2], vt[0]);
   v[2] = make_double2(vt[1], vt[2]);
@@ -375,9 +367,8 @@ __global__ void k_hist_regrow(int n, History src, History dst) {
   int c = src.cnt[i];
   dst.cnt[i] = c;
   for (int r = 0; r < c; r++) {
-    dst.key[(size_t)i * dst.cap + r] = src.key[(size_t)i * src.cap + r];
-    for (int k = 0; k < 3; k++)
-      dst.val[((size_t)i * dst.cap + r) * 3 + k] = src.val[((size_t)i * src.cap + r) * 3 + k];
+    dst.key[hslot(dst, i, r)] = src.key[hslot(src, i, r)];
+    for (int k = 0; k < 3; k++) dst.val[hslot(dst, i, r) * 3 + k] = src.val[hslot(src, i, r) * 3 + k];
   }
 }
 
@@ -505,8 +496,8 @@ __global__ void k_relink1(const DevParams* __restrict__ Pp, CellLists L, int par
     for (int w = 0; w < NWM; w++) cnt->wall_fn[w] = 0.0;
     if (update) cnt->need_capacity = 0;
     else cnt->escaped = 0ull;  // escapes are counted by the current step's corrector
-    const double d = __longlong_as_double((long long)cnt->disp_max);
-    cnt->disp_max = 0ull;
+    const double d = (double)__uint_as_float(cnt->disp_max);
+    cnt->disp_max = 0u;
     const double acc = cnt->disp_acc + d;
     const int full = cnt->force_full != 0 || !(acc <= P.vl_thr);
     cnt->full_due = full;
@@ -789,15 +780,34 @@ __global__ void __launch_bounds__(256) k_screen_full(const DevParams* __restrict
 // ---------------------------------------------------------------------------
 // K2+K4: the FP64 pass kernel (exact order)
 
+// resident blocks of 128 threads per SM the pass kernels are compiled for
+// (registers per thread = 65536 / (128 * blocks))
+#ifndef DEM_PASS_BLOCKS_FP64
+#define DEM_PASS_BLOCKS_FP64 4
+#endif
+
+// Owner data handed to the lane that computes one of its contacts.
+struct OwnerF64 {
+  double x, y, z, R, vx, vy, vz, wx, wy, wz;
+  int p, cp, n1, pad;
+};
+
 template <bool PP, int EPI>
-__global__ void __launch_bounds__(128, 4) k_pass_fp64(PassArgs<double4, double2> A) {
+__global__ void __launch_bounds__(128, DEM_PASS_BLOCKS_FP64) k_pass_fp64(
+    PassArgs<double4, double2> A) {
+  // per warp: the current 32 contacts (candidate index, owner lane, partner)
+  // and their results FN, FT, VT, torque term (12 doubles, lane-contiguous)
+  __shared__ int s_k[4][32], s_o[4][32], s_q[4][32];
+  __shared__ double s_r[12][4][32];
   if (A.cnt->abort) return;
+  const int wid = threadIdx.x >> 5;
   const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = p0 < A.n;
   const int p = valid ? p0 : 0;
   const DevParams& P = *A.P;
+  const Box& B = A.box;
   const int n = A.n;
-  unsigned long long n_col = 0, n_pc = 0, n_wc = 0;
+  unsigned n_col = 0, n_pc = 0, n_wc = 0;
   int need = 0;
   double d2 = 0.0;
 
@@ -832,79 +842,106 @@ __global__ void __launch_bounds__(128, 4) k_pass_fp64(PassArgs<double4, double2>
     hw_n++;
   };
   // Rij = x_j - x_i (minimum image, src/MForces.f90:209-217); candidate k
-  // of the row is "j" (p is "i") for k < n1, else "i"
-  auto geometry = [&](bool pi, const double4& q4, double Rij[3]) -> double {
-    Rij[0] = pi ? q4.x - xp[0] : xp[0] - q4.x;
-    Rij[1] = pi ? q4.y - xp[1] : xp[1] - q4.y;
-    Rij[2] = pi ? q4.z - xp[2] : xp[2] - q4.z;
+  // of a row is "j" (its owner is "i") for k < n1, else "i"
+  auto geometry = [&](bool oi, const double xo[3], const double4& q4, double Rij[3]) -> double {
+    Rij[0] = oi ? q4.x - xo[0] : xo[0] - q4.x;
+    Rij[1] = oi ? q4.y - xo[1] : xo[1] - q4.y;
+    Rij[2] = oi ? q4.z - xo[2] : xo[2] - q4.z;
 #pragma unroll
-    for (int k = 0; k < 3; k++)
-      if (P.pbc[k]) Rij[k] = Rij[k] - P.lbox[k] * fnint(Rij[k] * P.inv_lbox[k]);
+    for (int k = 0; k < 3; k++) Rij[k] = min_image_exact(Rij[k], B, k);
     return sumsq3(Rij);
   };
   // the overlap test DeltaDijSq = MinDijSq - DijSq > 0 (src/MForces.f90:218-224)
   auto test = [&](int k, int q, const double4& q4) -> bool {
     const bool pi = k < n1;
     double Rij[3];
-    const double DijSq = geometry(pi, q4, Rij);
+    const double DijSq = geometry(pi, xp, q4, Rij);
     const int cq = PP ? 0 : A.comp[q];
     const double mds = pi ? Material<PP>::min_dij_sq(P, cp, Rp, cq, q4.w)
                           : Material<PP>::min_dij_sq(P, cq, q4.w, cp, Rp);
     return mds - DijSq > 0.0;
   };
-  // one contact in the reference's orientation (src/MForces.f90:199-272)
-  auto visit = [&](int k) {
-    const int q = __ldg(A.cand + (size_t)k * n + p);
-    const bool pi = k < n1;
+  // one contact of owner `o` in the reference's orientation
+  // (src/MForces.f90:199-272), computed by this lane
+  auto compute = [&](const OwnerF64& o, int k, int slot) {
+    const int q = __ldg(A.cand + (size_t)k * n + o.p);
+    const bool oi = k < o.n1;
     const double4 q4 = A.X[q];
+    const double xo[3] = {o.x, o.y, o.z};
     double Rij[3];
-    const double DijSq = geometry(pi, q4, Rij);
+    const double DijSq = geometry(oi, xo, q4, Rij);
     const int cq = PP ? 0 : A.comp[q];
-    const int ca = pi ? cp : cq, cb = pi ? cq : cp;
-    const double Ra = pi ? Rp : q4.w, Rb = pi ? q4.w : Rp;
+    const int ca = oi ? o.cp : cq, cb = oi ? cq : o.cp;
+    const double Ra = oi ? o.R : q4.w, Rb = oi ? q4.w : o.R;
     const double Delta = Material<PP>::min_dij_sq(P, ca, Ra, cb, Rb) - DijSq;
     PairPar pp;
     Material<PP>::pair(P, ca, Ra, cb, Rb, pp);
     const double4 qv4 = A.v4[q];
     const double2 qw2 = A.w2[q];
-    const double vq[3] = {qv4.x, qv4.y, qv4.z};
-    const double wq[3] = {qv4.w, qw2.x, qw2.y};
+    const double vo[3] = {o.vx, o.vy, o.vz}, wo[3] = {o.wx, o.wy, o.wz};
+    const double vq[3] = {qv4.x, qv4.y, qv4.z}, wq[3] = {qv4.w, qw2.x, qw2.y};
     double va[3], wa[3], vb[3], wb[3];
 #pragma unroll
     for (int d = 0; d < 3; d++) {
-      va[d] = pi ? vp[d] : vq[d];
-      wa[d] = pi ? wp[d] : wq[d];
-      vb[d] = pi ? vq[d] : vp[d];
-      wb[d] = pi ? wq[d] : wp[d];
+      va[d] = oi ? vo[d] : vq[d];
+      wa[d] = oi ? wo[d] : wq[d];
+      vb[d] = oi ? vq[d] : vo[d];
+      wb[d] = oi ? wq[d] : wo[d];
     }
-    const int lo = p < q ? p : q, hi = p < q ? q : p;
+    const int lo = o.p < q ? o.p : q, hi = o.p < q ? q : o.p;
     double FT0[3] = {0.0, 0.0, 0.0}, VT0[3] = {0.0, 0.0, 0.0};
-    const int r = hist_find(A.Hr, lo, hi);
+    const int r = find_record(A.Hr, lo, hi);
     const bool contacting = r >= 0;
     if (contacting) hist_read(A.Hr, lo, r, FT0, VT0);
-    if (pi) {
+    if (oi) {
       if (!contacting) n_col++;
       n_pc++;
     }
-    ContactOut o;
+    ContactOut out;
     pair_contact(Rij, DijSq, Delta, pp, Ra, va, wa, Rb, vb, wb, half_dt, contacting, FT0, VT0,
-                 o);
-    if (pi) {
+                 out);
+    double tq[3];
+    if (oi) {
+      double RN[3];
 #pragma unroll
-      for (int d = 0; d < 3; d++) iF[d] = iF[d] + o.FN[d] + o.FT[d];
-      double RN[3], tq[3];
+      for (int d = 0; d < 3; d++) RN[d] = o.R * out.N[d];
+      cross3(RN, out.FT, tq);
+    } else {
 #pragma unroll
-      for (int d = 0; d < 3; d++) RN[d] = Rp * o.N[d];
-      cross3(RN, o.FT, tq);
+      for (int d = 0; d < 3; d++) tq[d] = o.R * out.NxFT[d];
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      s_r[d][wid][slot] = out.FN[d];
+      s_r[3 + d][wid][slot] = out.FT[d];
+      s_r[6 + d][wid][slot] = out.VT[d];
+      s_r[9 + d][wid][slot] = tq[d];
+    }
+    s_q[wid][slot] = q;
+  };
+  // the owner adds one contact (iForce/iTorque as "i", Force/Torque as "j")
+  auto accum = [&](int slot, int k) {
+    double FN[3], FT[3], VT[3], tq[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      FN[d] = s_r[d][wid][slot];
+      FT[d] = s_r[3 + d][wid][slot];
+      VT[d] = s_r[6 + d][wid][slot];
+      tq[d] = s_r[9 + d][wid][slot];
+    }
+    if (k < n1) {
+#pragma unroll
+      for (int d = 0; d < 3; d++) iF[d] = iF[d] + FN[d] + FT[d];
 #pragma unroll
       for (int d = 0; d < 3; d++) iT[d] = iT[d] + tq[d];
     } else {
 #pragma unroll
-      for (int d = 0; d < 3; d++) F[d] = F[d] - o.FN[d] - o.FT[d];
+      for (int d = 0; d < 3; d++) F[d] = F[d] - FN[d] - FT[d];
 #pragma unroll
-      for (int d = 0; d < 3; d++) T[d] = T[d] + Rp * o.NxFT[d];
+      for (int d = 0; d < 3; d++) T[d] = T[d] + tq[d];
     }
-    if (update && p < q) record(q, o.FT, o.VT);
+    const int q = s_q[wid][slot];
+    if (update && p < q) record(q, FT, VT);
   };
   // walls (src/MForces.f90:274-314)
   auto walls = [&]() {
@@ -972,15 +1009,17 @@ __global__ void __launch_bounds__(128, 4) k_pass_fp64(PassArgs<double4, double2>
 #pragma unroll
     for (int k = 0; k < 3; k++) T[k] = T[k] + iT[k];
   };
-  contact_loop(A.cand, A.X, n, p, valid, n1, n2b, n1 + n2b + n2a, P.nw > 0, test, visit, walls,
-               own);
+  const OwnerF64 me{xp[0], xp[1], xp[2], Rp, vp[0], vp[1], vp[2], wp[0], wp[1], wp[2],
+                    p, cp, n1, 0};
+  contact_loop(A.cand, A.X, n, p, valid, n1, n2b, n1 + n2b + n2a, P.nw > 0, me, s_k[wid],
+               s_o[wid], test, compute, accum, walls, own);
 
   if (valid) {
     // ---- records of pairs the sweep did not visit are kept as they were
     if (update) {
       const int nold = A.Hr.cnt[p];
       for (int r = 0; r < nold; r++) {
-        const int q2 = A.Hr.key[(size_t)p * A.Hr.cap + r];
+        const int q2 = A.Hr.key[hslot(A.Hr, p, r)];
         if (!cells_adjacent(P, c, A.cell_cur[q2])) {
           double ft[3], vt[3];
           hist_read(A.Hr, p, r, ft, vt);
@@ -1003,17 +1042,7 @@ __global__ void __launch_bounds__(128, 4) k_pass_fp64(PassArgs<double4, double2>
     for (int k = 0; k < 3; k++) alp[k] = T[k] * inv_i;
     epilogue<EPI>(A, p, xp, Rp, vp, wp, acc, alp, c, d2);
   }
-  n_col = warp_sum_u64(n_col);
-  n_pc = warp_sum_u64(n_pc);
-  n_wc = warp_sum_u64(n_wc);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) need = max(need, __shfl_down_sync(0xffffffffu, need, o));
-  if ((threadIdx.x & 31) == 0) {
-    if (need) atomicMax(&A.cnt->need_capacity, need);
-    if (n_col) atomicAdd(A.update ? &A.cnt->ncol_pending : &A.cnt->ncol, n_col);
-    if (n_pc) atomicAdd(&A.cnt->pair_contacts, n_pc);
-    if (n_wc) atomicAdd(&A.cnt->wall_contacts, n_wc);
-  }
+  publish_counts(A.cnt, A.update != 0, n_col, n_pc, n_wc, (unsigned)need);
   if (EPI != EPI_STORE) publish_disp(A.cnt, d2);
 }
 

@@ -287,12 +287,14 @@ int alloc_history(dem_ctx* c, History& H, int cap) {
   size_t n = (size_t)std::max(c->n, 1);
   int nw = std::max(c->params.n_walls, 1);
   H.cap = cap;
+  H.n = (int)n;
   CK(cudaMalloc(&H.cnt, n * sizeof(int)));
   CK(cudaMalloc(&H.key, n * cap * sizeof(int)));
   CK(cudaMalloc(&H.val, n * cap * 3 * sizeof(double2)));
   CK(cudaMalloc(&H.wflag, n * nw * sizeof(int)));
   CK(cudaMalloc(&H.wval, n * nw * 3 * sizeof(double2)));
   CK(cudaMemsetAsync(H.cnt, 0, n * sizeof(int), c->stream));
+  CK(cudaMemsetAsync(H.key, 0xFF, n * cap * sizeof(int), c->stream));
   CK(cudaMemsetAsync(H.wflag, 0, n * nw * sizeof(int), c->stream));
   return DEM_OK;
 }
@@ -377,8 +379,8 @@ int init_cells(dem_ctx* c) {
   // no transition pending; the first pass builds every candidate row
   CK(cudaMemsetAsync(&c->cnt->n_dirty[0], 0, 3 * sizeof(int), c->stream));
   CK(cudaMemsetAsync(&c->cnt->movers_pending, 0, sizeof(unsigned long long), c->stream));
-  CK(cudaMemsetAsync(&c->cnt->disp_max, 0, sizeof(unsigned long long) + sizeof(double),
-                     c->stream));
+  CK(cudaMemsetAsync(&c->cnt->disp_max, 0, sizeof(unsigned), c->stream));
+  CK(cudaMemsetAsync(&c->cnt->disp_acc, 0, sizeof(double), c->stream));
   const int one = 1;
   CK(cudaMemcpyAsync(&c->cnt->force_full, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
   c->prepared = -1;
@@ -395,6 +397,12 @@ PassArgs<V4, W2> pass_args(dem_ctx* c, int side, bool update, double dt, const R
                            int tag, const StateArrays& tgt) {
   PassArgs<V4, W2> A;
   A.P = c->dp;
+  for (int k = 0; k < 3; k++) {
+    A.box.lbox[k] = c->hp.lbox[k];
+    A.box.inv_lbox[k] = c->hp.inv_lbox[k];
+    A.box.pbc[k] = c->hp.pbc[k];
+    A.box.half_lim[k] = 0.49 * c->hp.lbox[k];
+  }
   A.n = c->n;
   A.X = c->X[side];
   A.v4 = (const V4*)c->v4[side];
@@ -828,6 +836,8 @@ int dem_create(const dem_params* p, dem_ctx** out) {
   h.nxby2 = (double)Nx * 0.5;
   h.nyby2 = (double)Ny * 0.5;
   h.nzby2 = (double)Nz * 0.5;
+  h.inv_nx = 1.0 / (double)Nx;
+  h.inv_ny = 1.0 / (double)Ny;
   // material tables
   for (int i = 0; i < NCM; i++) {
     h.comp_radius[i] = p->comp_radius[i];
@@ -1171,7 +1181,7 @@ int dem_set_contacts(dem_ctx* c, int64_t m, const int32_t* imin, const int32_t* 
     if (st) return st;
   }
   const int cap = c->hcap;
-  std::vector<int> key(N * cap, 0);
+  std::vector<int> key(N * cap, -1);
   std::vector<double2> val(N * cap * 3);
   std::fill(cnt.begin(), cnt.end(), 0);
   // records kept sorted by partner as the reference lists are
@@ -1183,8 +1193,8 @@ int dem_set_contacts(dem_ctx* c, int64_t m, const int32_t* imin, const int32_t* 
   for (int64_t q = 0; q < m; q++) {
     int64_t r = idx[q];
     int o = imin[r], k = cnt[o]++;
-    key[(size_t)o * cap + k] = imax[r];
-    double2* v = &val[((size_t)o * cap + k) * 3];
+    key[(size_t)k * N + o] = imax[r];  // slot major
+    double2* v = &val[((size_t)k * N + o) * 3];
     v[0] = make_double2(ft[3 * r], ft[3 * r + 1]);
     v[1] = make_double2(ft[3 * r + 2], vt[3 * r]);
     v[2] = make_double2(vt[3 * r + 1], vt[3 * r + 2]);
@@ -1262,7 +1272,7 @@ int dem_get_contacts(dem_ctx* c, int64_t cap, int32_t* imin, int32_t* imax, doub
   HostHist h;
   int st = download_history(c, h);
   if (st) return st;
-  const int hc = c->hcap;
+  const size_t N = (size_t)std::max(c->n, 1);
   int64_t a = 0, b = 0;
   std::vector<int> ord;
   for (int i = 0; i < c->n; i++) {
@@ -1270,12 +1280,12 @@ int dem_get_contacts(dem_ctx* c, int64_t cap, int32_t* imin, int32_t* imax, doub
     ord.resize(k);
     for (int r = 0; r < k; r++) ord[r] = r;
     std::sort(ord.begin(), ord.end(),
-              [&](int x, int y) { return h.key[(size_t)i * hc + x] < h.key[(size_t)i * hc + y]; });
+              [&](int x, int y) { return h.key[(size_t)x * N + i] < h.key[(size_t)y * N + i]; });
     for (int r : ord) {
       if (a >= cap) return fail(c, DEM_ERR_INVALID, "pair record buffer too small");
       imin[a] = i;
-      imax[a] = h.key[(size_t)i * hc + r];
-      const double2* v = &h.val[((size_t)i * hc + r) * 3];
+      imax[a] = h.key[(size_t)r * N + i];
+      const double2* v = &h.val[((size_t)r * N + i) * 3];
       ft[3 * a] = v[0].x; ft[3 * a + 1] = v[0].y; ft[3 * a + 2] = v[1].x;
       vt[3 * a] = v[1].y; vt[3 * a + 1] = v[2].x; vt[3 * a + 2] = v[2].y;
       a++;

@@ -242,15 +242,33 @@ __device__ __forceinline__ unsigned long long wsum(unsigned long long v) {
 // The mixed-precision pass kernel: the FP64 kernel's structure (candidate
 // rows, exact FP64 overlap test, orientation, history semantics, summation
 // order), FP32 contact arithmetic, FP64 integrator epilogue.
+#ifndef DEM_PASS_BLOCKS_MIXED
+#define DEM_PASS_BLOCKS_MIXED 4
+#endif
+
+// Owner data handed to the lane that computes one of its contacts.
+struct OwnerMixed {
+  double x, y, z, R;
+  float vx, vy, vz, wx, wy, wz;
+  int p, cp, n1, pad;
+};
+
 template <bool PP, int EPI>
-__global__ void __launch_bounds__(128, 4) k_pass_mixed(PassArgs<float4, float2> A, MixedView V) {
+__global__ void __launch_bounds__(128, DEM_PASS_BLOCKS_MIXED) k_pass_mixed(
+    PassArgs<float4, float2> A, MixedView V) {
+  // per warp: the current 32 contacts (candidate index, owner lane, partner)
+  // and their results FN, FT, FT remainder, VT, torque term (15 floats)
+  __shared__ int s_k[4][32], s_o[4][32], s_q[4][32];
+  __shared__ float s_r[15][4][32];
   if (A.cnt->abort) return;
+  const int wid = threadIdx.x >> 5;
   const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = p0 < A.n;
   const int p = valid ? p0 : 0;
   const DevParams& P = *A.P;
+  const Box& B = A.box;
   const int n = A.n;
-  unsigned long long n_col = 0, n_pc = 0, n_wc = 0;
+  unsigned n_col = 0, n_pc = 0, n_wc = 0;
   int need = 0;
   double d2 = 0.0;
 
@@ -282,7 +300,7 @@ __global__ void __launch_bounds__(128, 4) k_pass_mixed(PassArgs<float4, float2> 
 
   auto record = [&](int partner, F3 ft, F3 lo, F3 vt) {
     if (hw_n < Hw.cap) {
-      size_t i = (size_t)p * Hw.cap + hw_n;
+      const size_t i = hslot(Hw, p, hw_n);
       Hw.key[i] = partner;
       rec_write(V.wa, V.wb, V.wc, i, ft, lo, vt);
     } else {
@@ -290,45 +308,35 @@ __global__ void __launch_bounds__(128, 4) k_pass_mixed(PassArgs<float4, float2> 
     }
     hw_n++;
   };
-  auto lookup = [&](int lo_i, int hi_i, F3& ft, F3& lo, F3& vt) -> bool {
-    const int cnt = Hr.cnt[lo_i];
-    const int* k = Hr.key + (size_t)lo_i * Hr.cap;
-    for (int r = 0; r < cnt; r++)
-      if (k[r] == hi_i) {
-        rec_read(V.ra, V.rb, V.rc, (size_t)lo_i * Hr.cap + r, ft, lo, vt);
-        return true;
-      }
-    ft = lo = vt = mk(0.f, 0.f, 0.f);
-    return false;
-  };
-  // Rij = x_j - x_i (minimum image, FP64); candidate k is "j" for k < n1
-  auto geometry = [&](bool pi, const double4& q4, double Rij[3]) -> double {
-    Rij[0] = pi ? q4.x - xp[0] : xp[0] - q4.x;
-    Rij[1] = pi ? q4.y - xp[1] : xp[1] - q4.y;
-    Rij[2] = pi ? q4.z - xp[2] : xp[2] - q4.z;
+  // Rij = x_j - x_i (minimum image, FP64); candidate k of a row is "j" (its
+  // owner is "i") for k < n1
+  auto geometry = [&](bool oi, const double xo[3], const double4& q4, double Rij[3]) -> double {
+    Rij[0] = oi ? q4.x - xo[0] : xo[0] - q4.x;
+    Rij[1] = oi ? q4.y - xo[1] : xo[1] - q4.y;
+    Rij[2] = oi ? q4.z - xo[2] : xo[2] - q4.z;
 #pragma unroll
-    for (int k = 0; k < 3; k++)
-      if (P.pbc[k]) Rij[k] = Rij[k] - P.lbox[k] * fnint(Rij[k] * P.inv_lbox[k]);
+    for (int k = 0; k < 3; k++) Rij[k] = min_image_exact(Rij[k], B, k);
     return sumsq3(Rij);
   };
   auto test = [&](int k, int q, const double4& q4) -> bool {
     const bool pi = k < n1;
     double Rij[3];
-    const double DijSq = geometry(pi, q4, Rij);
+    const double DijSq = geometry(pi, xp, q4, Rij);
     const int cq = PP ? 0 : A.comp[q];
     const double mds = pi ? MMat<PP>::min_dij_sq(P, cp, Rpd, cq, q4.w)
                           : MMat<PP>::min_dij_sq(P, cq, q4.w, cp, Rpd);
     return mds - DijSq > 0.0;
   };
-  auto visit = [&](int k) {
-    const int q = __ldg(A.cand + (size_t)k * n + p);
-    const bool pi = k < n1;
+  auto compute = [&](const OwnerMixed& o, int k, int slot) {
+    const int q = __ldg(A.cand + (size_t)k * n + o.p);
+    const bool oi = k < o.n1;
     const double4 q4 = A.X[q];
+    const double xo[3] = {o.x, o.y, o.z};
     double Rij[3];
-    const double DijSq = geometry(pi, q4, Rij);
+    const double DijSq = geometry(oi, xo, q4, Rij);
     const int cq = PP ? 0 : A.comp[q];
-    const int ca = pi ? cp : cq, cb = pi ? cq : cp;
-    const double Rad = pi ? Rpd : q4.w, Rbd = pi ? q4.w : Rpd;
+    const int ca = oi ? o.cp : cq, cb = oi ? cq : o.cp;
+    const double Rad = oi ? o.R : q4.w, Rbd = oi ? q4.w : o.R;
     const double Delta = MMat<PP>::min_dij_sq(P, ca, Rad, cb, Rbd) - DijSq;
     const float Ra = (float)Rad, Rb = (float)Rbd;
     MPair m;
@@ -336,24 +344,43 @@ __global__ void __launch_bounds__(128, 4) k_pass_mixed(PassArgs<float4, float2> 
     const float4 qv4 = A.v4[q];
     const float2 qw2 = A.w2[q];
     const F3 vq = mk(qv4.x, qv4.y, qv4.z), wq = mk(qv4.w, qw2.x, qw2.y);
-    const int lo_i = p < q ? p : q, hi_i = p < q ? q : p;
-    F3 ft0, ft0lo, vt0;
-    const bool contacting = lookup(lo_i, hi_i, ft0, ft0lo, vt0);
-    if (pi) {
+    const F3 vo = mk(o.vx, o.vy, o.vz), wo = mk(o.wx, o.wy, o.wz);
+    const int lo_i = o.p < q ? o.p : q, hi_i = o.p < q ? q : o.p;
+    F3 ft0 = mk(0.f, 0.f, 0.f), ft0lo = ft0, vt0 = ft0;
+    const int r = find_record(Hr, lo_i, hi_i);
+    const bool contacting = r >= 0;
+    if (contacting) rec_read(V.ra, V.rb, V.rc, hslot(Hr, lo_i, r), ft0, ft0lo, vt0);
+    if (oi) {
       if (!contacting) n_col++;
       n_pc++;
     }
-    MOut o;
-    mixed_pair(Rij, DijSq, Delta, m, Ra, pi ? vp : vq, pi ? wp : wq, Rb, pi ? vq : vp,
-               pi ? wq : wp, half_dt, contacting, ft0, ft0lo, vt0, o);
-    if (pi) {
-      iF = iF + o.FN + (o.FT + o.FTlo);
-      iT = iT + cross(Rp * o.N, o.FT);
+    MOut out;
+    mixed_pair(Rij, DijSq, Delta, m, Ra, oi ? vo : vq, oi ? wo : wq, Rb, oi ? vq : vo,
+               oi ? wq : wo, half_dt, contacting, ft0, ft0lo, vt0, out);
+    const float Ro = (float)o.R;
+    const F3 tq = oi ? cross(Ro * out.N, out.FT) : Ro * out.NxFT;
+    const float vals[15] = {out.FN.x, out.FN.y, out.FN.z, out.FT.x, out.FT.y, out.FT.z,
+                            out.FTlo.x, out.FTlo.y, out.FTlo.z, out.VT.x, out.VT.y, out.VT.z,
+                            tq.x, tq.y, tq.z};
+#pragma unroll
+    for (int i = 0; i < 15; i++) s_r[i][wid][slot] = vals[i];
+    s_q[wid][slot] = q;
+  };
+  auto accum = [&](int slot, int k) {
+    float v[15];
+#pragma unroll
+    for (int i = 0; i < 15; i++) v[i] = s_r[i][wid][slot];
+    const F3 FN = mk(v[0], v[1], v[2]), FT = mk(v[3], v[4], v[5]), FTlo = mk(v[6], v[7], v[8]);
+    const F3 VT = mk(v[9], v[10], v[11]), tq = mk(v[12], v[13], v[14]);
+    if (k < n1) {
+      iF = iF + FN + (FT + FTlo);
+      iT = iT + tq;
     } else {
-      F = F - o.FN - (o.FT + o.FTlo);
-      T = T + Rp * o.NxFT;
+      F = F - FN - (FT + FTlo);
+      T = T + tq;
     }
-    if (update && p < q) record(q, o.FT, o.FTlo, o.VT);
+    const int q = s_q[wid][slot];
+    if (update && p < q) record(q, FT, FTlo, VT);
   };
   auto walls = [&]() {
     for (int w = 0; w < P.nw; w++) {
@@ -398,14 +425,15 @@ __global__ void __launch_bounds__(128, 4) k_pass_mixed(PassArgs<float4, float2> 
     F = F + iF;
     T = T + iT;
   };
-  contact_loop(A.cand, A.X, n, p, valid, n1, n2b, n1 + n2b + n2a, P.nw > 0, test, visit, walls,
-               own);
+  const OwnerMixed me{xp[0], xp[1], xp[2], Rpd, vp.x, vp.y, vp.z, wp.x, wp.y, wp.z, p, cp, n1, 0};
+  contact_loop(A.cand, A.X, n, p, valid, n1, n2b, n1 + n2b + n2a, P.nw > 0, me, s_k[wid],
+               s_o[wid], test, compute, accum, walls, own);
 
   if (valid) {
     if (update) {
       const int nold = Hr.cnt[p];
       for (int r = 0; r < nold; r++) {
-        const size_t i = (size_t)p * Hr.cap + r;
+        const size_t i = hslot(Hr, p, r);
         const int q2 = Hr.key[i];
         if (!cells_adjacent(P, c, A.cell_cur[q2])) {
           F3 ft, lo, vt;
@@ -433,17 +461,7 @@ __global__ void __launch_bounds__(128, 4) k_pass_mixed(PassArgs<float4, float2> 
     }
     epilogue<EPI>(A, p, xp, Rpd, vd, wd, acc, alp, c, d2);
   }
-  n_col = wsum(n_col);
-  n_pc = wsum(n_pc);
-  n_wc = wsum(n_wc);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) need = max(need, __shfl_down_sync(0xffffffffu, need, o));
-  if ((threadIdx.x & 31) == 0) {
-    if (need) atomicMax(&A.cnt->need_capacity, need);
-    if (n_col) atomicAdd(A.update ? &A.cnt->ncol_pending : &A.cnt->ncol, n_col);
-    if (n_pc) atomicAdd(&A.cnt->pair_contacts, n_pc);
-    if (n_wc) atomicAdd(&A.cnt->wall_contacts, n_wc);
-  }
+  publish_counts(A.cnt, A.update != 0, n_col, n_pc, n_wc, (unsigned)need);
   if (EPI != EPI_STORE) publish_disp(A.cnt, d2);
 }
 
@@ -453,7 +471,7 @@ __global__ void k_hist_to_mixed(int n, History H, float4* a, float4* b, float* c
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   for (int r = 0; r < H.cnt[i]; r++) {
-    size_t k = (size_t)i * H.cap + r;
+    const size_t k = hslot(H, i, r);
     double2 x = H.val[3 * k], y = H.val[3 * k + 1], z = H.val[3 * k + 2];
     a[k] = make_float4((float)x.x, (float)x.y, (float)y.x, (float)y.y);
     b[k] = make_float4((float)z.x, (float)z.y, 0.f, 0.f);
@@ -474,7 +492,7 @@ __global__ void k_hist_from_mixed(int n, History H, const float4* a, const float
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   for (int r = 0; r < H.cnt[i]; r++) {
-    size_t k = (size_t)i * H.cap + r;
+    const size_t k = hslot(H, i, r);
     float4 x = a[k], y = b[k];
     H.val[3 * k] = make_double2((double)x.x + y.z, (double)x.y + y.w);
     H.val[3 * k + 1] = make_double2((double)x.z + c[k], (double)x.w);
@@ -495,7 +513,7 @@ __global__ void k_mixed_regrow(int n, const int* cnt, int oldcap, int newcap, co
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   for (int r = 0; r < cnt[i]; r++) {
-    size_t s = (size_t)i * oldcap + r, d = (size_t)i * newcap + r;
+    const size_t s = (size_t)r * n + i, d = s;  // slot-major: same index in both
     na[d] = a[s];
     nb[d] = b[s];
     nc[d] = c[s];

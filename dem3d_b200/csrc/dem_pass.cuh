@@ -12,6 +12,8 @@
 // is idempotent, so a pass kernel that was stopped by a history overflow can
 // be launched again after the tables grow.
 #pragma once
+#include <cstring>
+
 #include "dem_device.cuh"
 
 namespace dem {
@@ -39,7 +41,8 @@ __device__ __forceinline__ void note_cell(const CellLists& L, Counters* cnt, int
 }
 
 // squared minimum-image displacement between two positions of a particle
-__device__ __forceinline__ double disp2(const DevParams& P, const double a[3], const double b[3]) {
+template <class BoxT>
+__device__ __forceinline__ double disp2(const BoxT& P, const double a[3], const double b[3]) {
   double s = 0.0;
 #pragma unroll
   for (int k = 0; k < 3; k++) {
@@ -50,33 +53,75 @@ __device__ __forceinline__ double disp2(const DevParams& P, const double a[3], c
   return s;
 }
 
-// Largest displacement of the warp into the pass maximum (non-negative
-// doubles order like their bit patterns).
+// Largest displacement of the warp into the pass maximum (FP32 rounded up;
+// non-negative floats order like their bit patterns).
 __device__ __forceinline__ void publish_disp(Counters* cnt, double d2) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) d2 = fmax(d2, __shfl_down_sync(0xffffffffu, d2, o));
-  if ((threadIdx.x & 31) == 0 && d2 > 0.0) {
-    double d = sqrt(d2);
-    atomicMax(&cnt->disp_max, (unsigned long long)__double_as_longlong(d));
+  const unsigned bits = __float_as_uint(__double2float_ru(sqrt(d2)));
+  const unsigned m = __reduce_max_sync(0xffffffffu, bits);
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(&cnt->disp_max, m);
+}
+
+// Per-warp pass statistics: one atomic per counter per warp.
+__device__ __forceinline__ void publish_counts(Counters* cnt, bool update, unsigned n_col,
+                                               unsigned n_pc, unsigned n_wc, unsigned need) {
+  const unsigned FULL = 0xffffffffu;
+  n_col = __reduce_add_sync(FULL, n_col);
+  n_pc = __reduce_add_sync(FULL, n_pc);
+  n_wc = __reduce_add_sync(FULL, n_wc);
+  need = __reduce_max_sync(FULL, need);
+  if ((threadIdx.x & 31) == 0) {
+    if (need) atomicMax(&cnt->need_capacity, (int)need);
+    if (n_col) atomicAdd(update ? &cnt->ncol_pending : &cnt->ncol, (unsigned long long)n_col);
+    if (n_pc) atomicAdd(&cnt->pair_contacts, (unsigned long long)n_pc);
+    if (n_wc) atomicAdd(&cnt->wall_contacts, (unsigned long long)n_wc);
   }
 }
 
-// The contacts of particle p in row order, processed in lockstep across the
-// warp.  The row's candidates are tested first (test(k, q, xq), four
-// prefetched at a time) into a bit mask per chunk of 64 candidates; then
-// every lane takes its next contact in the same iteration, so the heavy
-// contact arithmetic runs max-over-lanes times per warp instead of once per
-// contact of every lane.  Row order fixes the reference's summation order:
-// loop-1 contacts (k < n1), then walls(), then the loop-2 contacts before
-// p's own block (k < n1 + n2b), own(), then the rest.  All 32 lanes must
-// call this; `valid` is false for lanes without a particle.
-template <class Test, class Visit, class Walls, class Own>
+// Slot of partner `hi` among the records of `lo`; -1: no record.
+__device__ __forceinline__ int find_record(const History& H, int lo, int hi) {
+  const int c = H.cnt[lo];
+  for (int r = 0; r < c; r++)
+    if (H.key[hslot(H, lo, r)] == hi) return r;
+  return -1;
+}
+
+// Broadcast a small trivially copyable object from lane `src`.
+template <class T>
+__device__ __forceinline__ T shfl_obj(const T& v, int src) {
+  static_assert(sizeof(T) % 4 == 0, "shuffle in 4-byte words");
+  constexpr int W = (int)(sizeof(T) / 4);
+  unsigned w[W];
+  memcpy(w, &v, sizeof(T));
+#pragma unroll
+  for (int i = 0; i < W; i++) w[i] = __shfl_sync(0xffffffffu, w[i], src);
+  T r;
+  memcpy(&r, w, sizeof(T));
+  return r;
+}
+
+// The contacts of the warp's particles, in three steps per window of 64
+// candidates:
+//  1. every lane tests its own candidates (test(k, q, xq), four prefetched at
+//     a time) into a bit mask;
+//  2. the warp's contacts are laid out owner by owner in row order (prefix
+//     sum) and computed 32 at a time, one per lane: compute(owner, k, slot)
+//     gets the owning particle's data by shuffle and leaves its results in
+//     shared-memory slot `slot`;
+//  3. every owner folds its own results in row order: accum(slot, k) for the
+//     loop-1 contacts (k < n1), then walls(), then the loop-2 contacts before
+//     its own block (k < n1 + n2b), own(), then the rest -- the reference's
+//     summation order.
+// s_k / s_o: 32 ints of shared memory per warp.  All 32 lanes must call
+// this; `valid` is false for lanes without a particle.
+template <class Owner, class Test, class Compute, class Accum, class Walls, class Own>
 __device__ __forceinline__ void contact_loop(const int* __restrict__ cand,
                                              const double4* __restrict__ X, int n, int p,
                                              bool valid, int n1, int n2b, int m, bool has_walls,
-                                             Test&& test, Visit&& visit, Walls&& walls,
+                                             const Owner& me, int* s_k, int* s_o, Test&& test,
+                                             Compute&& compute, Accum&& accum, Walls&& walls,
                                              Own&& own) {
   const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
   bool walls_pending = valid && has_walls;
   bool own_pending = valid;
   if (!valid) m = 0;
@@ -97,22 +142,46 @@ __device__ __forceinline__ void contact_loop(const int* __restrict__ cand,
       for (int u = 0; u < 4; u++)
         if (q[u] >= 0 && test(b + u, q[u], xq[u])) mask |= 1ull << (b + u - base);
     }
-#pragma unroll 1
-    while (true) {
-      const int k = mask ? base + __ffsll((long long)mask) - 1 : -1;
-      if (walls_pending && k >= n1) {
-        walls();
-        walls_pending = false;
+    const int cnt = __popcll(mask);
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int start = incl - cnt;
+    const int total = __shfl_sync(FULL, incl, 31);
+    unsigned long long rem = mask;
+    int e_pub = start;
+    for (int t0 = 0; t0 < total; t0 += 32) {
+      while (rem && e_pub < t0 + 32) {
+        s_k[e_pub - t0] = base + __ffsll((long long)rem) - 1;
+        s_o[e_pub - t0] = lane;
+        rem &= rem - 1ull;
+        e_pub++;
       }
-      if (own_pending && !walls_pending && k >= n1 + n2b) {
-        own();
-        own_pending = false;
+      __syncwarp();
+      const bool has = t0 + lane < total;
+      const int kk = has ? s_k[lane] : 0;
+      const int oo = has ? s_o[lane] : lane;
+      const Owner ow = shfl_obj(me, oo);
+      if (has) compute(ow, kk, lane);
+      __syncwarp();
+      const int e0 = start > t0 ? start : t0;
+      const int e1 = start + cnt < t0 + 32 ? start + cnt : t0 + 32;
+      for (int e = e0; e < e1; e++) {
+        const int k = s_k[e - t0];
+        if (walls_pending && k >= n1) {
+          walls();
+          walls_pending = false;
+        }
+        if (own_pending && !walls_pending && k >= n1 + n2b) {
+          own();
+          own_pending = false;
+        }
+        accum(e - t0, k);
       }
-      if (!__any_sync(FULL, k >= 0)) break;
-      if (k >= 0) {
-        visit(k);
-        mask &= mask - 1ull;
-      }
+      __syncwarp();
     }
   }
   if (walls_pending) walls();
@@ -156,6 +225,7 @@ __device__ __forceinline__ void epilogue(const PassArgs<V4, W2>& A, int p, const
                                          const double acc[3], const double alp[3], int c_cur,
                                          double& d2) {
   const DevParams& P = *A.P;
+  const Box& B = A.box;
   const size_t n = (size_t)A.n;
   if (EPI == EPI_STORE) {
     A.tgt.ax[p] = acc[0]; A.tgt.ay[p] = acc[1]; A.tgt.az[p] = acc[2];
@@ -187,7 +257,7 @@ __device__ __forceinline__ void epilogue(const PassArgs<V4, W2>& A, int p, const
     for (int d = 0; d < 3; d++) w[d] = wp[d] + P.ab0 * alp[d] + sl[d];
 #pragma unroll
     for (int d = 0; d < 3; d++)
-      if (P.pbc[d]) x[d] = x[d] - P.lbox[d] * fnint(x[d] * P.inv_lbox[d]);
+      if (B.pbc[d]) x[d] = x[d] - B.lbox[d] * fnint(x[d] * B.inv_lbox[d]);
     R.px[p] = x[0]; R.py[p] = x[1]; R.pz[p] = x[2];
     R.vx[p] = v[0]; R.vy[p] = v[1]; R.vz[p] = v[2];
     R.wx[p] = w[0]; R.wy[p] = w[1]; R.wz[p] = w[2];
@@ -216,14 +286,14 @@ __device__ __forceinline__ void epilogue(const PassArgs<V4, W2>& A, int p, const
     for (int d = 0; d < 3; d++) w[d] = w[d] + P.am0 * alp[d] + sl[d];
 #pragma unroll
     for (int d = 0; d < 3; d++)
-      if (P.pbc[d]) x[d] = x[d] - P.lbox[d] * fnint(x[d] * P.inv_lbox[d]);
+      if (B.pbc[d]) x[d] = x[d] - B.lbox[d] * fnint(x[d] * B.inv_lbox[d]);
     Q.px[p] = x[0]; Q.py[p] = x[1]; Q.pz[p] = x[2];
     Q.vx[p] = v[0]; Q.vy[p] = v[1]; Q.vz[p] = v[2];
     Q.wx[p] = w[0]; Q.wy[p] = w[1]; Q.wz[p] = w[2];
     bool out = false;
 #pragma unroll
     for (int d = 0; d < 3; d++) {
-      const double h = 0.5 * P.lbox[d];
+      const double h = 0.5 * B.lbox[d];
       out = out || (x[d] > h) || (x[d] < -h);
     }
     if (out) atomicAdd(&A.cnt->escaped, 1ull);
@@ -233,7 +303,7 @@ __device__ __forceinline__ void epilogue(const PassArgs<V4, W2>& A, int p, const
   A.v4n[p] = mk_v4<V4>(v[0], v[1], v[2], w[0]);
   A.w2n[p] = mk_w2<W2>(w[1], w[2]);
   note_cell(A.L, A.cnt, A.par_nxt, p, c_cur, current_cell(P, x[0], x[1], x[2]));
-  d2 = disp2(P, x, xp);
+  d2 = disp2(B, x, xp);
 }
 
 // Meta word of a candidate row.
