@@ -106,22 +106,41 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def force_bytes_per_particle(z_pp, z_pw, nw, update):
-    """Algorithmic (compulsory) DRAM bytes of one force-kernel launch per
-    particle (FP64 layout): own traversal copies (pos+R, v+wx, wy+wz, orig,
-    cell) and contact-list meta, the history records (each pair record read
-    once: Z/2 per particle) and, in the updating pass, the records written,
-    then a and alpha stored.  Neighbour data is counted once (it is re-read
-    from L1/L2).  z_pp: pair contacts per particle, z_pw: wall contacts."""
-    own = 32 + 32 + 16 + 4 + 4 + 16 + 4 * z_pp
-    rec = 4 + 48
-    hist = 4 + 0.5 * z_pp * rec + nw * 4 + z_pw * 48
-    return own + hist * (2 if update else 1) + 48
+def pass_bytes_per_particle(mixed, epi, z_pp, m_cand, z_pw=0.0, nw=0, nprev=3):
+    """Algorithmic DRAM bytes of one pass-kernel launch per particle: every
+    input and output of the pass read or written once.  Partner data is other
+    particles' own data (re-read from L1/L2), so it adds nothing.
+      own copies: position+R 32, velocities 24 (FP32) / 48 (FP64), row meta 4,
+        cell 4, history count 4; candidate row 4*m_cand;
+      history: each pair record once (key 4 + 36 B FP32 / 48 B FP64) per
+        pair, read, and written again by the updating pass (+ count 4);
+        wall records 4 + record per wall;
+      epi "predict" (pass 1, src/MDEM.f90:296-331): ring nprev*72 read,
+        Particle v,w 48 read (mixed: FP64 copies), a,alpha 48 + Predicted
+        x,v,w 72 + ring slot 72 + next-pass copies (32 + velocities) + cell 4
+        written;
+      epi "correct" (pass 2, :340-367): ring read, Predicted v 24 (mixed),
+        Particle x,v,w 72 read and written, Predicted a,alpha 48 + next-pass
+        copies + cell 4 written."""
+    vel = 24 if mixed else 48
+    rec = 4 + (36 if mixed else 48)
+    own = 32 + vel + 4 + 4 + 4 + 4 * m_cand
+    hist = 0.5 * z_pp * rec + nw * 4 + z_pw * (rec - 4)
+    ring = nprev * 72
+    if epi == "predict":
+        hist += 4 + 0.5 * z_pp * rec + nw * 4 + z_pw * (rec - 4)  # updated tables
+        epil = ring + (48 if mixed else 0) + 48 + 72 + (72 if nprev else 0) + 32 + vel + 4
+    else:
+        epil = ring + (24 if mixed else 0) + 72 + 72 + 48 + 32 + vel + 4
+    return own + hist + epil
 
 
-def rebuild_bytes_per_particle():
-    """k_assign 48 + k_scatter 28 + k_cellsort 20 + k_gather 164."""
-    return 48 + 28 + 20 + 164
+def step_bytes_per_particle(mixed, z_pp, m_cand, z_pw=0.0, nw=0, nprev=3):
+    """Compulsory bytes of one particle-update (MoveParticles: two passes);
+    the relink and candidate-row kernels touch only the few particles near
+    cells that changed and are not counted."""
+    return (pass_bytes_per_particle(mixed, "predict", z_pp, m_cand, z_pw, nw, nprev) +
+            pass_bytes_per_particle(mixed, "correct", z_pp, m_cand, z_pw, nw, nprev))
 
 
 def reduce_max(x, world, device="cuda"):
@@ -294,9 +313,9 @@ def run_reference(args):
 # GPU arm
 
 def traffic_per_particle():
-    """DRAM bytes per particle of the force kernel from a committed ncu
-    capture summary (profiles/force_traffic.json), if present."""
-    p = os.path.join(ROOT, "profiles", "force_traffic.json")
+    """DRAM bytes per particle of the pass kernels from a committed ncu
+    capture summary (profiles/pass_traffic.json), if present."""
+    p = os.path.join(ROOT, "profiles", "pass_traffic.json")
     if os.path.exists(p):
         try:
             return json.load(open(p))
@@ -305,42 +324,11 @@ def traffic_per_particle():
     return None
 
 
-def screen_bytes_per_particle(z_pp):
-    """k_screen: own position + cell, the staged neighbourhood (each position
-    read once from DRAM), the contact-list row and its meta."""
-    return 32 + 4 + 16 + 4 * z_pp
-
-
-def integrator_bytes_per_particle(kind, nprev=3):
-    """k_predict: x,v,w,a,alpha + ring read, Predicted + ring store written;
-    k_correct: x,v,w + v~,a~,alpha~ + ring read, x,v,w written."""
-    if kind == "predict":
-        return 120 + nprev * 72 + 72 + 72
-    return 72 + 72 + nprev * 72 + 72
-
-
-def step_bytes_per_particle(z_pp, nw=0, nprev=3):
-    """Compulsory bytes of one particle-update (two passes + AB + AM)."""
-    return (2 * rebuild_bytes_per_particle() + 2 * screen_bytes_per_particle(z_pp)
-            + force_bytes_per_particle(z_pp, 0.0, nw, True)
-            + force_bytes_per_particle(z_pp, 0.0, nw, False)
-            + integrator_bytes_per_particle("predict", nprev)
-            + integrator_bytes_per_particle("correct", nprev))
-
-
-def kernel_bytes(name, n, z_pp, nw):
-    """Bytes of one launch (the force kernels: mean of the two passes)."""
-    if name.startswith("force"):
-        return n * 0.5 * (force_bytes_per_particle(z_pp, 0.0, nw, True) +
-                          force_bytes_per_particle(z_pp, 0.0, nw, False))
-    if name == "screen":
-        return n * screen_bytes_per_particle(z_pp)
-    if name == "predict":
-        return n * integrator_bytes_per_particle("predict")
-    if name == "correct":
-        return n * integrator_bytes_per_particle("correct")
-    if name.startswith("gather"):
-        return n * 164
+def kernel_bytes(name, n, mixed, z_pp, m_cand, z_pw, nw):
+    """Algorithmic bytes of one pass-kernel launch (mean of the two passes)."""
+    if name.startswith("pass"):
+        return n * 0.5 * (pass_bytes_per_particle(mixed, "predict", z_pp, m_cand, z_pw, nw) +
+                          pass_bytes_per_particle(mixed, "correct", z_pp, m_cand, z_pw, nw))
     return None
 
 
@@ -454,11 +442,15 @@ def run_ours(args):
         if prec != headline:
             sy.close()
 
-    # contacts per particle for the byte model
+    # contacts and candidates per particle for the byte model
     ps = s.pass_stats()
     obs = s.observables()
     z_pp = 2.0 * obs["n_pair_contacts"] / n
+    z_pw = obs["n_wall_contacts"] / n
     nw = int(w.params.n_walls)
+    rs = s.row_stats()
+    m_cand = rs["candidates"] / n
+    mixed = headline == "mixed"
     # per-kernel timing (instrumented steps, not graph-replayed)
     s.reset_kernel_stats()
     s.set_profiling(True)
@@ -470,7 +462,7 @@ def run_ours(args):
     last += nprof
     total_prof = sum(v[1] for v in stats.values())
     dom = max(stats, key=lambda k: stats[k][1])
-    b_launch = kernel_bytes(dom, n, z_pp, nw)
+    b_launch = kernel_bytes(dom, n, mixed, z_pp, m_cand, z_pw, nw)
     avg_ms = stats[dom][1] / stats[dom][0]
     achieved = b_launch / (avg_ms / 1000.0) / 1e9 if b_launch else None
     peaks = {}
@@ -482,7 +474,7 @@ def run_ours(args):
     traffic = None
     if tr and dom in tr.get("bytes_per_particle", {}):
         traffic = tr["bytes_per_particle"][dom] * n
-    step_b = step_bytes_per_particle(z_pp, nw)
+    step_b = step_bytes_per_particle(mixed, z_pp, m_cand, z_pw, nw)
     step_gbs = step_b * n / (ms / args.steps / 1000.0) / 1e9
 
     # e2e: each step uploads Particle(1:n) from pinned host memory, advances
@@ -540,7 +532,8 @@ def run_ours(args):
                          "kernel_share": {k: round(v[1] / total_prof, 4)
                                           for k, v in sorted(stats.items(),
                                                              key=lambda kv: -kv[1][1])}},
-            "contacts_per_particle": z_pp, "movers_last_pass": ps["movers"],
+            "contacts_per_particle": z_pp, "candidates_per_particle": m_cand,
+            "movers_last_pass": ps["movers"],
             "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
             "gen_s": round(t_gen, 2),
         }

@@ -113,6 +113,7 @@ struct CellLists {
   int* arr_head;  // [ncell] particles entering the cell at the next relink, -1 = none
   int* arr_next;  // [n]
   int* mflag;     // [n] particle already pushed as an arrival
+  int* mnext;     // [n] a mover's successor in the list it leaves
   int* dflag;     // [ncell] cell already in a dirty list
   int* rflag;     // [ncell] cell already in the repair list
   int* dlist[2];  // [ncell] cells that gain or lose a particle on the way to assignment b

@@ -473,16 +473,21 @@ __global__ void __launch_bounds__(256) k_prepare(const DevParams* __restrict__ P
   publish_disp(cnt, d2);
 }
 
-// Relink, phase 1: every dirty cell of list `par` drops the particles that
-// left it (TransferParticle's unlink, src/MCells.f90:747-774).  Thread 0
-// also closes the previous pass's bookkeeping and decides whether this pass
-// rebuilds every candidate row.
-__global__ void k_relink1(const DevParams* __restrict__ Pp, CellLists L, int par, int n,
-                          int update, Counters* cnt) {
+// Relink (RedistributeParticles3D's list updates, src/MCells.f90:607-643):
+// one thread per dirty cell of list `par` drops the particles that left it
+// (TransferParticle's unlink, :747-774) and prepends its arrivals in
+// decreasing index (AddParticle, :684-698, applied in increasing index
+// order), then marks its 27-cell neighbourhood for candidate-row repair.
+// The walk over the old list follows a leaver's successor saved when it
+// moved (mnext), so no thread reads a link that another thread rewrites.
+// Thread 0 also closes the previous pass's bookkeeping and decides whether
+// this pass rebuilds every candidate row.
+__global__ void k_relink(const DevParams* __restrict__ Pp, CellLists L, int par, int n,
+                         int update, Counters* cnt) {
   if (cnt->abort) return;
+  const DevParams& P = *Pp;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   if (tid == 0) {
-    const DevParams& P = *Pp;
     cnt->n_repair = 0;
     cnt->n_dirty[par ^ 1] = 0;
     cnt->movers = cnt->movers_pending;
@@ -508,6 +513,7 @@ __global__ void k_relink1(const DevParams* __restrict__ Pp, CellLists L, int par
   const int* __restrict__ cell_new = L.cell[par];
   for (int i = tid; i < m; i += gridDim.x * blockDim.x) {
     const int c = L.dlist[par][i];
+    // 1. unlink the leavers
     int prev = -1, first = -1, q = L.head[c];
     int guard = 0;
     while (q != -1) {
@@ -516,8 +522,9 @@ __global__ void k_relink1(const DevParams* __restrict__ Pp, CellLists L, int par
         atomicExch(&cnt->abort, 1);
         return;
       }
-      const int nq = L.next[q];
-      if (cell_new[q] == c) {
+      const bool stays = cell_new[q] == c;
+      const int nq = stays ? L.next[q] : L.mnext[q];
+      if (stays) {
         if (prev == -1) first = q;
         else L.next[prev] = q;
         prev = q;
@@ -525,22 +532,9 @@ __global__ void k_relink1(const DevParams* __restrict__ Pp, CellLists L, int par
       q = nq;
     }
     if (prev != -1) L.next[prev] = -1;
-    L.head[c] = first;
-  }
-}
-
-// Relink, phase 2: every dirty cell prepends its arrivals in decreasing index
-// (AddParticle, src/MCells.f90:684-698, applied in increasing index order)
-// and marks its 27-cell neighbourhood for candidate-row repair.
-__global__ void k_relink2(const DevParams* __restrict__ Pp, CellLists L, int par, int n,
-                          Counters* cnt) {
-  if (cnt->abort) return;
-  const DevParams& P = *Pp;
-  const int m = cnt->n_dirty[par];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-    const int c = L.dlist[par][i];
+    // 2. prepend the arrivals, highest index first
     int sh = -1, tail = -1, a = L.arr_head[c];
-    int guard = 0;
+    guard = 0;
     while (a != -1) {
       if (++guard > n) {
         atomicExch(&cnt->list_error, 1);
@@ -556,34 +550,45 @@ __global__ void k_relink2(const DevParams* __restrict__ Pp, CellLists L, int par
         L.next[a] = sh;
         sh = a;
       } else {
-        int q = sh;
-        for (int g2 = 0; L.next[q] != -1 && L.next[q] > a && g2 < guard; g2++) q = L.next[q];
-        L.next[a] = L.next[q];
-        L.next[q] = a;
+        int q2 = sh;
+        for (int g2 = 0; L.next[q2] != -1 && L.next[q2] > a && g2 < guard; g2++) q2 = L.next[q2];
+        L.next[a] = L.next[q2];
+        L.next[q2] = a;
         if (L.next[a] == -1) tail = a;
       }
       a = an;
     }
     L.arr_head[c] = -1;
     if (sh != -1) {
-      L.next[tail] = L.head[c];
-      L.head[c] = sh;
+      L.next[tail] = first;
+      first = sh;
     }
+    L.head[c] = first;
     L.dflag[c] = 0;
+    // 3. the rows of every particle around c are rebuilt in this pass: the
+    // 27 flag exchanges are issued together, then one append per cell
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
-    int xi, xf, yi, yf, zi, zf;
-    axis_range(cx, nx, P.pbc[0], xi, xf);
-    axis_range(cy, ny, P.pbc[1], yi, yf);
-    axis_range(cz, nz, P.pbc[2], zi, zf);
-    for (int kz = zi; kz <= zf; kz++)
-      for (int ky = yi; ky <= yf; ky++)
-        for (int kx = xi; kx <= xf; kx++) {
-          const int jc = axis_wrap(cx + kx, nx, P.pbc[0]) +
-                         nx * (axis_wrap(cy + ky, ny, P.pbc[1]) +
-                               ny * axis_wrap(cz + kz, nz, P.pbc[2]));
-          if (atomicExch(&L.rflag[jc], 1) == 0) L.rlist[atomicAdd(&cnt->n_repair, 1)] = jc;
-        }
+    int jcs[27];
+    unsigned fresh = 0u;
+#pragma unroll
+    for (int o = 0; o < 27; o++) {
+      const int jx = cx + o % 3 - 1, jy = cy + (o / 3) % 3 - 1, jz = cz + o / 9 - 1;
+      const bool ok = (P.pbc[0] || (jx >= 0 && jx < nx)) && (P.pbc[1] || (jy >= 0 && jy < ny)) &&
+                      (P.pbc[2] || (jz >= 0 && jz < nz));
+      jcs[o] = ok ? axis_wrap(jx, nx, P.pbc[0]) +
+                        nx * (axis_wrap(jy, ny, P.pbc[1]) + ny * axis_wrap(jz, nz, P.pbc[2]))
+                  : -1;
+    }
+#pragma unroll
+    for (int o = 0; o < 27; o++)
+      if (jcs[o] >= 0 && atomicExch(&L.rflag[jcs[o]], 1) == 0) fresh |= 1u << o;
+    if (fresh) {
+      int k = atomicAdd(&cnt->n_repair, __popc(fresh));
+#pragma unroll
+      for (int o = 0; o < 27; o++)
+        if ((fresh >> o) & 1u) L.rlist[k++] = jcs[o];
+    }
   }
 }
 
@@ -676,11 +681,29 @@ __device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int 
     md = md + skin;
     return md * md - DijSq > 0.0;
   };
-  // pass 1: count
-  int count = 0;
+  // pass 1: walk and count; the first 8 list elements and their test
+  // results stay in registers for pass 2
+  int count = 0, walked = 0;
+  unsigned hits = 0u;
+  int cache[8];
   bool bad = false;
+  int q = start;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    cache[i] = -1;
+    if (q != -1 && q != stop) {
+      cache[i] = q;
+      walked = i + 1;
+      if (is_cand(q)) {
+        hits |= 1u << i;
+        count++;
+      }
+      q = next[q];
+    }
+  }
+  const int resume = q;  // first element not cached (-1 or stop: none)
   {
-    int q = start, guard = 0;
+    int guard = 0;
     while (q != -1 && q != stop) {
       if (++guard > n) {
         bad = true;
@@ -718,34 +741,40 @@ __device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int 
     }
     return;
   }
-  // pass 2: write
+  // pass 2: write (the cached part, then the rest of the list)
   {
-    int q = start, k = off;
-    while (q != -1 && q != stop) {
-      if (is_cand(q)) R.cand[(size_t)(k++) * n + p] = q;
-      q = next[q];
+    int k = off;
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+      if (i < walked && ((hits >> i) & 1u)) R.cand[(size_t)(k++) * n + p] = cache[i];
+    int q2 = resume;
+    while (q2 != -1 && q2 != stop) {
+      if (is_cand(q2)) R.cand[(size_t)(k++) * n + p] = q2;
+      q2 = next[q2];
     }
   }
   if (lane == 0) R.meta[p] = n1 | (n2b << META_BITS) | (n2a << (2 * META_BITS));
 }
 
-// Rows of the particles of every repair cell (one warp per cell).
+// Candidate rows of the pass: every row when the pass is due for a full
+// rebuild (one warp per particle), else the rows of the particles of every
+// repair cell (one warp per cell).  The repair flags of the listed cells are
+// cleared in every case (also when a stopped sequence skips the work).
 template <bool PP>
-__global__ void __launch_bounds__(256) k_screen_repair(const DevParams* __restrict__ Pp, int n,
-                                                       const double4* __restrict__ X,
-                                                       const int* __restrict__ comp,
-                                                       CellLists L, Rows R, Counters* cnt,
-                                                       int tag) {
-  // the flags of the listed cells are cleared even when nothing is built
-  // (a stopped sequence, or a full rebuild that rebuilds every row anyway)
+__global__ void __launch_bounds__(256) k_screen(const DevParams* __restrict__ Pp, int n,
+                                                const double4* __restrict__ X,
+                                                const int* __restrict__ comp,
+                                                const int* __restrict__ cell_cur, CellLists L,
+                                                Rows R, Counters* cnt, int tag) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const bool skip = cnt->abort != 0;
+  const bool full = cnt->full_due != 0;
   const int m = cnt->n_repair;
-  const bool skip = cnt->abort != 0 || cnt->full_due != 0;
   for (int r = warp; r < m; r += nwarps) {
     const int c = L.rlist[r];
-    if (!skip) {
+    if (!skip && !full) {
       int p = L.head[c], guard = 0;
       while (p != -1) {
         if (++guard > n) {
@@ -761,20 +790,9 @@ __global__ void __launch_bounds__(256) k_screen_repair(const DevParams* __restri
     }
     if (lane == 0) L.rflag[c] = 0;
   }
-}
-
-// Every row, when the pass is due for a full rebuild (one warp per particle).
-template <bool PP>
-__global__ void __launch_bounds__(256) k_screen_full(const DevParams* __restrict__ Pp, int n,
-                                                     const double4* __restrict__ X,
-                                                     const int* __restrict__ comp,
-                                                     const int* __restrict__ cell_cur,
-                                                     CellLists L, Rows R, Counters* cnt, int tag) {
-  if (cnt->abort || !cnt->full_due) return;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (int p = warp; p < n; p += nwarps)
-    build_row<PP>(*Pp, n, p, cell_cur[p], X, comp, L.head, L.next, R, cnt, tag);
+  if (!skip && full)
+    for (int p = warp; p < n; p += nwarps)
+      build_row<PP>(*Pp, n, p, cell_cur[p], X, comp, L.head, L.next, R, cnt, tag);
 }
 
 // ---------------------------------------------------------------------------

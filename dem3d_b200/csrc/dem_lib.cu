@@ -224,8 +224,8 @@ unsigned blocks_for(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 
 void free_lists(dem_ctx* c) {
   CellLists& L = c->L;
-  int** f[] = {&L.head, &L.next, &L.cell[0], &L.cell[1], &L.arr_head, &L.arr_next, &L.mflag,
-               &L.dflag, &L.rflag, &L.dlist[0], &L.dlist[1], &L.rlist};
+  int** f[] = {&L.head,  &L.next,  &L.cell[0], &L.cell[1], &L.arr_head, &L.arr_next, &L.mflag,
+               &L.mnext, &L.dflag, &L.rflag,   &L.dlist[0], &L.dlist[1],  &L.rlist};
   for (int** q : f) {
     cudaFree(*q);
     *q = nullptr;
@@ -480,15 +480,16 @@ int prepare_side(dem_ctx* c, int side) {
   return DEM_OK;
 }
 
-void launch_screen_full(dem_ctx* c, int side, int tag) {
+// candidate rows of the pass (repair or full rebuild, decided on the device)
+void launch_screen(dem_ctx* c, int side, int tag) {
   if (c->n == 0) return;
   const unsigned g = std::min(blocks_for((long long)c->n * 32, 256), (unsigned)FULL_BLOCKS);
   if (c->pp)
-    launch(c, "screen_full", k_screen_full<true>, g, 256, (const DevParams*)c->dp, c->n,
+    launch(c, "screen", k_screen<true>, g, 256, (const DevParams*)c->dp, c->n,
            (const double4*)c->X[side], (const int*)c->comp, (const int*)c->L.cell[c->par], c->L,
            c->rows, c->cnt, tag);
   else
-    launch(c, "screen_full", k_screen_full<false>, g, 256, (const DevParams*)c->dp, c->n,
+    launch(c, "screen", k_screen<false>, g, 256, (const DevParams*)c->dp, c->n,
            (const double4*)c->X[side], (const int*)c->comp, (const int*)c->L.cell[c->par], c->L,
            c->rows, c->cnt, tag);
 }
@@ -496,20 +497,10 @@ void launch_screen_full(dem_ctx* c, int side, int tag) {
 // relink towards the prepared assignment, then the candidate rows
 void pass_lists(dem_ctx* c, int side, bool update, int tag) {
   const int b = c->par ^ 1;
-  launch(c, "relink1", k_relink1, (unsigned)LIST_BLOCKS, 256, (const DevParams*)c->dp, c->L, b,
+  launch(c, "relink", k_relink, (unsigned)LIST_BLOCKS, 256, (const DevParams*)c->dp, c->L, b,
          c->n, update ? 1 : 0, c->cnt);
-  launch(c, "relink2", k_relink2, (unsigned)LIST_BLOCKS, 256, (const DevParams*)c->dp, c->L, b,
-         c->n, c->cnt);
   c->par = b;
-  if (c->pp)
-    launch(c, "screen_repair", k_screen_repair<true>, (unsigned)LIST_BLOCKS, 256,
-           (const DevParams*)c->dp, c->n, (const double4*)c->X[side], (const int*)c->comp, c->L,
-           c->rows, c->cnt, tag);
-  else
-    launch(c, "screen_repair", k_screen_repair<false>, (unsigned)LIST_BLOCKS, 256,
-           (const DevParams*)c->dp, c->n, (const double4*)c->X[side], (const int*)c->comp, c->L,
-           c->rows, c->cnt, tag);
-  launch_screen_full(c, side, tag);
+  launch_screen(c, side, tag);
 }
 
 RingMap current_map(dem_ctx* c) {
@@ -590,7 +581,8 @@ int finish_pass(dem_ctx* c, int side, bool update, double dt, int epi, const Rin
       CK(cudaMemcpyAsync(&c->cnt->full_due, &one, sizeof(int), cudaMemcpyHostToDevice,
                          c->stream));
       CK(cudaMemsetAsync(&c->cnt->disp_acc, 0, sizeof(double), c->stream));
-      launch_screen_full(c, side, tag);
+      CK(cudaMemsetAsync(&c->cnt->n_repair, 0, sizeof(int), c->stream));
+      launch_screen(c, side, tag);
     }
     launch_pass_kernel(c, side, update, dt, epi, rm, tag);
   }
@@ -990,6 +982,7 @@ int dem_set_state(dem_ctx* c, int32_t n, const int32_t* comp, const double* radi
     CK(cudaMalloc(&L.arr_head, sizeof(int) * NC));
     CK(cudaMalloc(&L.arr_next, sizeof(int) * N));
     CK(cudaMalloc(&L.mflag, sizeof(int) * N));
+    CK(cudaMalloc(&L.mnext, sizeof(int) * N));
     CK(cudaMalloc(&L.dflag, sizeof(int) * NC));
     CK(cudaMalloc(&L.rflag, sizeof(int) * NC));
     CK(cudaMalloc(&L.dlist[0], sizeof(int) * NC));
@@ -1620,6 +1613,24 @@ int dem_get_pass_stats(dem_ctx* c, int64_t* pair_contacts, int64_t* wall_contact
   if (wall_contacts) *wall_contacts = c->last_walls;
   if (movers) *movers = c->last_movers;
   if (hist_capacity) *hist_capacity = c->hcap;
+  return DEM_OK;
+}
+
+int dem_get_row_stats(dem_ctx* c, int64_t* candidates, int32_t* row_capacity) {
+  if (!c) return DEM_ERR_INVALID;
+  if (row_capacity) *row_capacity = c->kc;
+  if (candidates) {
+    *candidates = 0;
+    if (c->state_set && c->n > 0) {
+      std::vector<int> meta((size_t)c->n);
+      CK(cudaStreamSynchronize(c->stream));
+      CK(cudaMemcpy(meta.data(), c->rows.meta, sizeof(int) * c->n, cudaMemcpyDeviceToHost));
+      int64_t t = 0;
+      for (int m : meta)
+        t += (m & META_MASK) + ((m >> META_BITS) & META_MASK) + ((m >> (2 * META_BITS)) & META_MASK);
+      *candidates = t;
+    }
+  }
   return DEM_OK;
 }
 

@@ -32,6 +32,7 @@ __device__ __forceinline__ void note_cell(const CellLists& L, Counters* cnt, int
   L.cell[par][p] = c_new;
   if (c_new != c_old) {
     if (atomicExch(&L.mflag[p], 1) == 0) {
+      L.mnext[p] = L.next[p];  // the relink walks the old list past p with it
       L.arr_next[p] = atomicExch(&L.arr_head[c_new], p);
       atomicAdd(&cnt->movers_pending, 1ull);
     }

@@ -285,3 +285,9 @@ class DEMSystem:
         self._call("get_pass_stats", C.byref(a), C.byref(b), C.byref(m), C.byref(cap))
         return {"pair_contacts": a.value, "wall_contacts": b.value, "movers": m.value,
                 "hist_capacity": cap.value}
+
+    def row_stats(self):
+        """Candidate-row entries of the last pass and the row capacity."""
+        t, kc = C.c_int64(), C.c_int32()
+        self._call("get_row_stats", C.byref(t), C.byref(kc))
+        return {"candidates": t.value, "row_capacity": kc.value}

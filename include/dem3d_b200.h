@@ -233,6 +233,9 @@ int dem_get_stream(dem_ctx* ctx, void** stream);
  * bytes the last pass touched by design (for roofline accounting). */
 int dem_get_pass_stats(dem_ctx* ctx, int64_t* pair_contacts, int64_t* wall_contacts,
                        int64_t* movers, int32_t* hist_capacity);
+/* Candidate rows of the last pass: total entries over all particles and the
+ * row capacity (for byte accounting). */
+int dem_get_row_stats(dem_ctx* ctx, int64_t* candidates, int32_t* row_capacity);
 
 /* Allocation-free cell distribution.  No counterpart in the reference: it
  * serves callers that may not allocate device memory while they run, such
