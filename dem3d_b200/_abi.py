@@ -126,6 +126,8 @@ GPU_ONLY = {
     "get_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "get_pass_stats": (C.c_int, [_P, _I64P, _I64P, _I64P, _I32P]),
     "get_row_stats": (C.c_int, [_P, _I64P, _I32P]),
+    "create_ensemble": (C.c_int, [C.POINTER(DemParams), C.c_int32, C.POINTER(_P)]),
+    "set_system_counts": (C.c_int, [_P, _I32P]),
     # device pointers for positions and outputs; see the header
     "distribute_particles_noalloc": (C.c_int, [C.POINTER(DemParams), C.c_int32, _P, _P, _P, _P,
                                                _I32P, _P, C.c_char_p, C.c_int32]),

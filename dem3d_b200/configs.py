@@ -3,6 +3,10 @@
 ``settling``     -- gravity settling of monodisperse spheres on a jittered
                     lattice in a box periodic in x/y with a frictional floor
                     (the 2,000-sphere CPU-runnable case; any N).
+``settling_ensemble`` -- many independent gravity-settling systems of uneven
+                    size (log-uniform particle counts), radii uniform in
+                    [0.45, 0.55], per-system friction and restitution, each
+                    in its own 10 x 10 x-y periodic box with a floor.
 ``dense_packing``-- polydisperse spheres, radii uniform in [0.4, 0.6], fully
                     periodic cube at a given volume fraction (the 1M / 16M
                     cases).  Positions: a jittered cubic lattice filled in a
@@ -163,6 +167,83 @@ def bidisperse_settling(n=4_000_000, seed=1004, width=200.0, ratio=3.0, number_r
         max_ncell=max_ncell, precision=precision)
     return Workload("bidisperse_settling", prm, pos, vel, np.zeros((nn, 3)), comp=comp,
                     info={"lbox": (width, width, lz), "seed": seed, "n_large": n_large})
+
+
+@dataclass
+class Ensemble:
+    """Independent systems for DEMSystem.ensemble: per-system parameters and
+    sizes, particle arrays concatenated by system."""
+    params: list
+    counts: np.ndarray
+    pos: np.ndarray
+    vel: np.ndarray
+    omega: np.ndarray
+    radius: np.ndarray
+    info: dict
+
+    @property
+    def n(self):
+        return self.pos.shape[0]
+
+    def system(self, s):
+        """(params, pos, vel, omega, radius) of system s alone."""
+        o = int(self.counts[:s].sum())
+        k = int(self.counts[s])
+        return (self.params[s], self.pos[o:o + k], self.vel[o:o + k], self.omega[o:o + k],
+                self.radius[o:o + k])
+
+
+def settling_ensemble(n_systems=4096, seed=1003, nmin=200, nmax=20000, width=10.0,
+                      rmin=0.45, rmax=0.55, mu_range=(0.2, 0.8), e_range=(0.5, 0.95),
+                      dt=1e-4, gravity=1.0, headroom=45.0, method_order=4, euler_intervals=100,
+                      max_ncell=30000, precision=P.PREC_FP64, sigma_v=0.1, counts=None):
+    """An ensemble of gravity-settling systems (the batched workload).
+
+    Per system s: N_s = round(exp(U[ln nmin, ln nmax])) spheres (or
+    ``counts``), radii U[rmin, rmax], mu_s ~ U(mu_range), restitution
+    e_s ~ U(e_range) (normal = tangential, particle-particle and
+    particle-floor).  Box ``width`` x ``width`` periodic in x/y, floor at the
+    bottom; spheres on a lattice of floor(width / 2 rmax) sites per row and
+    layers 2 rmax * 1.8 apart, jittered by U(+-0.02) in z and a rigid
+    U(+-0.02) xy shift per layer, numbered layer by layer; velocities
+    N(0, sigma_v^2)."""
+    rng = np.random.default_rng(seed)
+    if counts is None:
+        counts = np.rint(np.exp(rng.uniform(math.log(nmin), math.log(nmax), n_systems)))
+    counts = np.asarray(counts, dtype=np.int64)
+    side = int(width / (2.0 * rmax))
+    a = width / side
+    dz = 1.8 * (2.0 * rmax)
+    params, P_, V_, R_ = [], [], [], []
+    for s, n in enumerate(counts):
+        n = int(n)
+        mu = float(rng.uniform(*mu_range))
+        e = float(rng.uniform(*e_range))
+        per = side * side
+        layers = (n + per - 1) // per
+        lz = layers * dz + headroom
+        k = np.arange(n)
+        iz, r = np.divmod(k, per)
+        iy, ix = np.divmod(r, side)
+        shift = rng.uniform(-0.02, 0.02, size=(layers, 2))
+        pos = np.empty((n, 3))
+        pos[:, 0] = -0.5 * width + (ix + 0.5) * a + shift[iz, 0]
+        pos[:, 1] = -0.5 * width + (iy + 0.5) * a + shift[iz, 1]
+        pos[:, 2] = -0.5 * lz + rmax + iz * dz + rng.uniform(-0.02, 0.02, size=n)
+        P_.append(pos)
+        V_.append(rng.normal(0.0, sigma_v, size=(n, 3)))
+        R_.append(rng.uniform(rmin, rmax, size=n))
+        floor = P.rectangle((0.0, 0.0, -0.5 * lz), width, width)
+        params.append(P.per_particle_params(
+            density=DENSITY, kn=KN, kt=KT, en=e, et=e, mu=mu, rmax=rmax,
+            lbox=(width, width, lz), pbc=(True, True, False), gravity=(0.0, 0.0, -gravity),
+            time_step=dt, walls=[floor], knw=[KN], ktw=[KT], enw=[e], etw=[e], muw=[mu],
+            method_order=method_order, euler_intervals=euler_intervals, max_ncell=max_ncell,
+            precision=precision))
+    pos = np.concatenate(P_)
+    return Ensemble(params, counts, pos, np.concatenate(V_), np.zeros_like(pos),
+                    np.concatenate(R_), {"seed": seed, "n_systems": len(counts),
+                                         "width": width})
 
 
 def cell_major_order_box(pos, lbox, cutoff):

@@ -16,7 +16,27 @@ namespace dem {
 constexpr int NCM = DEM_MAX_COMPONENTS;
 constexpr int NWM = DEM_MAX_WALLS;
 
-// Parameters resident in device memory (one copy per context).
+// Periodic box of a system.
+struct Box {
+  double lbox[3], inv_lbox[3];
+  double half_lim[3];  // 0.49 lbox: |r| below it has nint(r/L) = 0 exactly
+  int pbc[3];
+};
+
+// Minimum image of one component, Rij(k) - Lbox(k)*nint(Rij(k)*InvLbox(k))
+// (src/MForces.f90:212-214), bit for bit: when |r| < 0.49 L the nint is 0
+// and the expression is r itself, so the formula is only evaluated for
+// pairs that straddle the periodic boundary.
+__device__ __forceinline__ double min_image_exact(double r, const Box& B, int k) {
+  if (B.pbc[k] && !(fabs(r) < B.half_lim[k]))
+    r = r - B.lbox[k] * (double)(int)round(r * B.inv_lbox[k]);
+  return r;
+}
+
+// Parameters of one system, resident in device memory (a context holds a
+// table of them: one per independent system of an ensemble, all sharing the
+// integrator settings).  Cells and particles of system s are numbered
+// globally from coff / poff.
 struct DevParams {
   int nc, nw;
   int pbc[3];
@@ -30,6 +50,9 @@ struct DevParams {
   double vl_skin;         // candidate-row skin (added to MinDij)
   double vl_thr;          // accumulated displacement bound that forces a full rebuild
   double inv_nx, inv_ny;  // 1/Nx, 1/Ny (cell coordinates without integer division)
+  Box box;                // lbox, inv_lbox, pbc again, with the minimum-image shortcut bound
+  int coff, poff, np;     // first cell, first particle, particles of this system
+  int sys;                // index of this system
   double comp_radius[NCM], comp_inv_mass[NCM], comp_inv_inertia[NCM], comp_eff_mass[NCM];
   double min_dij[NCM * NCM], min_dij_sq[NCM * NCM];
   double kn[NCM * NCM], yn[NCM * NCM], kt[NCM * NCM], yt[NCM * NCM], mu_sq[NCM * NCM];
@@ -139,28 +162,10 @@ constexpr int KC_MAX = META_MASK;
 
 // Arguments of one pass kernel.  V4/W2 are the velocity copies the pass
 // reads for partners (double in FP64 mode, float in mixed mode).
-// Periodic box of a pass, passed by value (kernel parameter space) so the
-// per-candidate minimum image reads no memory.
-struct Box {
-  double lbox[3], inv_lbox[3];
-  double half_lim[3];  // 0.49 lbox: |r| below it has nint(r/L) = 0 exactly
-  int pbc[3];
-};
-
-// Minimum image of one component, Rij(k) - Lbox(k)*nint(Rij(k)*InvLbox(k))
-// (src/MForces.f90:212-214), bit for bit: when |r| < 0.49 L the nint is 0
-// and the expression is r itself, so the formula is only evaluated for
-// pairs that straddle the periodic boundary.
-__device__ __forceinline__ double min_image_exact(double r, const Box& B, int k) {
-  if (B.pbc[k] && !(fabs(r) < B.half_lim[k]))
-    r = r - B.lbox[k] * (double)(int)round(r * B.inv_lbox[k]);
-  return r;
-}
-
 template <class V4, class W2>
 struct PassArgs {
-  const DevParams* P;
-  Box box;
+  const DevParams* P;   // system table
+  const int* sysid;     // system of every particle (NULL: one system)
   int n;
   const double4* X;   // this pass's positions (x, y, z, R) by original index
   const V4* v4;       // vx, vy, vz, wx
@@ -372,7 +377,12 @@ __device__ __forceinline__ bool overlap_rect(const DevParams& P, const dem_wall&
   return ov;
 }
 
-// CurrentCell3D (src/MCells.f90:498-513), 0-based.
+// System parameters of particle p (or of cell c with a cell->system map).
+__device__ __forceinline__ const DevParams& sys_params(const DevParams* T, const int* sid, int i) {
+  return T[sid ? sid[i] : 0];
+}
+
+// CurrentCell3D (src/MCells.f90:498-513), 0-based, as a global cell index.
 __device__ __forceinline__ int current_cell(const DevParams& P, double x, double y, double z) {
   int ix = (int)(P.nxbylx * x + P.nxby2);
   int iy = (int)(P.nybyly * y + P.nyby2);
@@ -383,7 +393,7 @@ __device__ __forceinline__ int current_cell(const DevParams& P, double x, double
   ix = ix > 0 ? ix : 0;
   iy = iy > 0 ? iy : 0;
   iz = iz > 0 ? iz : 0;
-  return ix + (iy + iz * P.ny) * P.nx;
+  return P.coff + ix + (iy + iz * P.ny) * P.nx;
 }
 
 // Are two cells neighbours in the sweep sense (same cell, or one in the
@@ -405,8 +415,9 @@ __device__ __forceinline__ int div_fast(int c, int d, double inv_d, int& rem) {
   rem = r;
   return q;
 }
+// coordinates of global cell c of system P
 __device__ __forceinline__ void cell_coords(const DevParams& P, int c, int& x, int& y, int& z) {
-  const int t = div_fast(c, P.nx, P.inv_nx, x);
+  const int t = div_fast(c - P.coff, P.nx, P.inv_nx, x);
   z = div_fast(t, P.ny, P.inv_ny, y);
 }
 

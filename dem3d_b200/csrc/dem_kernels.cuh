@@ -40,9 +40,10 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
 // K1: cell rebuild
 
 // One thread per current slot: new cell, mover flag, sort key, slot in cell.
-__global__ void k_assign(const DevParams* __restrict__ Pp, int n, int initial,
-                         const double* __restrict__ px, const double* __restrict__ py,
-                         const double* __restrict__ pz, const int* __restrict__ order,
+__global__ void k_assign(const DevParams* __restrict__ PT, const int* __restrict__ sysid, int n,
+                         int initial, const double* __restrict__ px,
+                         const double* __restrict__ py, const double* __restrict__ pz,
+                         const int* __restrict__ order,
                          const int* __restrict__ old_cell, int* __restrict__ cell_cnt,
                          int* __restrict__ a_cell, int* __restrict__ a_loc,
                          unsigned* __restrict__ a_key, int* __restrict__ a_orig,
@@ -56,8 +57,8 @@ __global__ void k_assign(const DevParams* __restrict__ Pp, int n, int initial,
   }
   unsigned long long mv = 0;
   if (s < n) {
-    const DevParams& P = *Pp;
     int orig = initial ? s : order[s];
+    const DevParams& P = sys_params(PT, sysid, orig);
     int c = current_cell(P, px[orig], py[orig], pz[orig]);
     int old = initial ? -1 : old_cell[s];
     bool mover = c != old;
@@ -327,12 +328,12 @@ __global__ void k_euler_update(int n, StateArrays Q, double dt, const Counters* 
 }
 
 // ApplyPeriodicBoundaryConditions (src/MDEM.f90:373-388)
-__global__ void k_apply_pbc(const DevParams* __restrict__ Pp, int n, StateArrays Q,
-                            const Counters* __restrict__ cnt) {
+__global__ void k_apply_pbc(const DevParams* __restrict__ PT, const int* __restrict__ sysid,
+                            int n, StateArrays Q, const Counters* __restrict__ cnt) {
   if (cnt->abort) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const DevParams& P = *Pp;
+  const DevParams& P = sys_params(PT, sysid, i);
   double* p[3] = {Q.px, Q.py, Q.pz};
 #pragma unroll
   for (int d = 0; d < 3; d++)
@@ -374,12 +375,13 @@ __global__ void k_hist_regrow(int n, History src, History dst) {
 
 // observables: per-block partial sums (fixed order), reduced on the host
 template <bool PP>
-__global__ void k_observables(const DevParams* __restrict__ Pp, int n, StateArrays Q,
-                              const double* __restrict__ radius, const int* __restrict__ comp,
+__global__ void k_observables(const DevParams* __restrict__ PT, const int* __restrict__ sysid,
+                              int n, StateArrays Q, const double* __restrict__ radius,
+                              const int* __restrict__ comp,
                               double* __restrict__ partial /* [grid][8] */) {
-  const DevParams& P = *Pp;
   double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const DevParams& P = sys_params(PT, sysid, i);
     double R, m, I;
     if (PP) {
       R = radius[i];
@@ -447,7 +449,8 @@ __global__ void k_discard(CellLists L, int par, const Counters* __restrict__ cnt
 // original index, the cell of every particle under the next assignment and
 // the displacement from the last pass's positions `Xlast` (NULL: none).
 template <class V4, class W2>
-__global__ void __launch_bounds__(256) k_prepare(const DevParams* __restrict__ Pp, int n,
+__global__ void __launch_bounds__(256) k_prepare(const DevParams* __restrict__ PT,
+                                                 const int* __restrict__ sysid, int n,
                                                  StateArrays src, const double* __restrict__ radius,
                                                  double4* X, V4* __restrict__ v4,
                                                  W2* __restrict__ w2, const double4* Xlast,
@@ -456,7 +459,7 @@ __global__ void __launch_bounds__(256) k_prepare(const DevParams* __restrict__ P
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   double d2 = 0.0;
   if (p < n) {
-    const DevParams& P = *Pp;
+    const DevParams& P = sys_params(PT, sysid, p);
     const double x[3] = {src.px[p], src.py[p], src.pz[p]};
     if (Xlast) {
       const double4 o = Xlast[p];
@@ -482,12 +485,12 @@ __global__ void __launch_bounds__(256) k_prepare(const DevParams* __restrict__ P
 // moved (mnext), so no thread reads a link that another thread rewrites.
 // Thread 0 also closes the previous pass's bookkeeping and decides whether
 // this pass rebuilds every candidate row.
-__global__ void k_relink(const DevParams* __restrict__ Pp, CellLists L, int par, int n,
-                         int update, Counters* cnt) {
+__global__ void k_relink(const DevParams* __restrict__ PT, const int* __restrict__ cellsys,
+                         CellLists L, int par, int n, int update, Counters* cnt) {
   if (cnt->abort) return;
-  const DevParams& P = *Pp;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   if (tid == 0) {
+    const DevParams& P = PT[0];  // the integrator settings are shared
     cnt->n_repair = 0;
     cnt->n_dirty[par ^ 1] = 0;
     cnt->movers = cnt->movers_pending;
@@ -567,8 +570,10 @@ __global__ void k_relink(const DevParams* __restrict__ Pp, CellLists L, int par,
     L.dflag[c] = 0;
     // 3. the rows of every particle around c are rebuilt in this pass: the
     // 27 flag exchanges are issued together, then one append per cell
+    const DevParams& P = sys_params(PT, cellsys, c);
     const int nx = P.nx, ny = P.ny, nz = P.nz;
-    const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
+    const int cl = c - P.coff;
+    const int cx = cl % nx, cy = (cl / nx) % ny, cz = cl / (nx * ny);
     int jcs[27];
     unsigned fresh = 0u;
 #pragma unroll
@@ -576,7 +581,7 @@ __global__ void k_relink(const DevParams* __restrict__ Pp, CellLists L, int par,
       const int jx = cx + o % 3 - 1, jy = cy + (o / 3) % 3 - 1, jz = cz + o / 9 - 1;
       const bool ok = (P.pbc[0] || (jx >= 0 && jx < nx)) && (P.pbc[1] || (jy >= 0 && jy < ny)) &&
                       (P.pbc[2] || (jz >= 0 && jz < nz));
-      jcs[o] = ok ? axis_wrap(jx, nx, P.pbc[0]) +
+      jcs[o] = ok ? P.coff + axis_wrap(jx, nx, P.pbc[0]) +
                         nx * (axis_wrap(jy, ny, P.pbc[1]) + ny * axis_wrap(jz, nz, P.pbc[2]))
                   : -1;
     }
@@ -614,7 +619,8 @@ __device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int 
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int nx = P.nx, ny = P.ny, nz = P.nz;
-  const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
+  const int cl = c - P.coff;
+  const int cx = cl % nx, cy = (cl / nx) % ny, cz = cl / (nx * ny);
   const double4 p4 = X[p];
   const int cp = PP ? 0 : comp[p];
   int start = -1, stop = -1, order = 1 << 20, jc = 0x7fffffff;
@@ -642,7 +648,7 @@ __device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int 
       loop = 1;
       order = 0;
     } else if (ok) {
-      jc = w[0] + nx * (w[1] + ny * w[2]);
+      jc = P.coff + w[0] + nx * (w[1] + ny * w[2]);
       start = head[jc];
       if (lex > 0) {
         loop = 1;
@@ -672,8 +678,7 @@ __device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int 
     const double4 q4 = X[q];
     double Rij[3] = {q4.x - p4.x, q4.y - p4.y, q4.z - p4.z};
 #pragma unroll
-    for (int k = 0; k < 3; k++)
-      if (P.pbc[k]) Rij[k] = Rij[k] - P.lbox[k] * fnint(Rij[k] * P.inv_lbox[k]);
+    for (int k = 0; k < 3; k++) Rij[k] = min_image_exact(Rij[k], P.box, k);
     const double DijSq = sumsq3(Rij);
     double md;
     if (PP) md = p4.w + q4.w;
@@ -761,7 +766,9 @@ __device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int 
 // repair cell (one warp per cell).  The repair flags of the listed cells are
 // cleared in every case (also when a stopped sequence skips the work).
 template <bool PP>
-__global__ void __launch_bounds__(256) k_screen(const DevParams* __restrict__ Pp, int n,
+__global__ void __launch_bounds__(256) k_screen(const DevParams* __restrict__ PT,
+                                                const int* __restrict__ sysid,
+                                                const int* __restrict__ cellsys, int n,
                                                 const double4* __restrict__ X,
                                                 const int* __restrict__ comp,
                                                 const int* __restrict__ cell_cur, CellLists L,
@@ -784,7 +791,8 @@ __global__ void __launch_bounds__(256) k_screen(const DevParams* __restrict__ Pp
           }
           break;
         }
-        build_row<PP>(*Pp, n, p, c, X, comp, L.head, L.next, R, cnt, tag);
+        build_row<PP>(sys_params(PT, cellsys, c), n, p, c, X, comp, L.head, L.next, R, cnt,
+                      tag);
         p = L.next[p];
       }
     }
@@ -792,7 +800,8 @@ __global__ void __launch_bounds__(256) k_screen(const DevParams* __restrict__ Pp
   }
   if (!skip && full)
     for (int p = warp; p < n; p += nwarps)
-      build_row<PP>(*Pp, n, p, cell_cur[p], X, comp, L.head, L.next, R, cnt, tag);
+      build_row<PP>(sys_params(PT, sysid, p), n, p, cell_cur[p], X, comp, L.head, L.next, R, cnt,
+                    tag);
 }
 
 // ---------------------------------------------------------------------------
@@ -807,7 +816,7 @@ __global__ void __launch_bounds__(256) k_screen(const DevParams* __restrict__ Pp
 // Owner data handed to the lane that computes one of its contacts.
 struct OwnerF64 {
   double x, y, z, R, vx, vy, vz, wx, wy, wz;
-  int p, cp, n1, pad;
+  int p, cp, n1, sys;
 };
 
 template <bool PP, int EPI>
@@ -822,8 +831,8 @@ __global__ void __launch_bounds__(128, DEM_PASS_BLOCKS_FP64) k_pass_fp64(
   const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = p0 < A.n;
   const int p = valid ? p0 : 0;
-  const DevParams& P = *A.P;
-  const Box& B = A.box;
+  const DevParams& P = sys_params(A.P, A.sysid, p);  // this particle's system
+  const Box& B = P.box;
   const int n = A.n;
   unsigned n_col = 0, n_pc = 0, n_wc = 0;
   int need = 0;
@@ -861,19 +870,20 @@ __global__ void __launch_bounds__(128, DEM_PASS_BLOCKS_FP64) k_pass_fp64(
   };
   // Rij = x_j - x_i (minimum image, src/MForces.f90:209-217); candidate k
   // of a row is "j" (its owner is "i") for k < n1, else "i"
-  auto geometry = [&](bool oi, const double xo[3], const double4& q4, double Rij[3]) -> double {
+  auto geometry = [&](const Box& Bx, bool oi, const double xo[3], const double4& q4,
+                      double Rij[3]) -> double {
     Rij[0] = oi ? q4.x - xo[0] : xo[0] - q4.x;
     Rij[1] = oi ? q4.y - xo[1] : xo[1] - q4.y;
     Rij[2] = oi ? q4.z - xo[2] : xo[2] - q4.z;
 #pragma unroll
-    for (int k = 0; k < 3; k++) Rij[k] = min_image_exact(Rij[k], B, k);
+    for (int k = 0; k < 3; k++) Rij[k] = min_image_exact(Rij[k], Bx, k);
     return sumsq3(Rij);
   };
   // the overlap test DeltaDijSq = MinDijSq - DijSq > 0 (src/MForces.f90:218-224)
   auto test = [&](int k, int q, const double4& q4) -> bool {
     const bool pi = k < n1;
     double Rij[3];
-    const double DijSq = geometry(pi, xp, q4, Rij);
+    const double DijSq = geometry(B, pi, xp, q4, Rij);
     const int cq = PP ? 0 : A.comp[q];
     const double mds = pi ? Material<PP>::min_dij_sq(P, cp, Rp, cq, q4.w)
                           : Material<PP>::min_dij_sq(P, cq, q4.w, cp, Rp);
@@ -887,13 +897,14 @@ __global__ void __launch_bounds__(128, DEM_PASS_BLOCKS_FP64) k_pass_fp64(
     const double4 q4 = A.X[q];
     const double xo[3] = {o.x, o.y, o.z};
     double Rij[3];
-    const double DijSq = geometry(oi, xo, q4, Rij);
+    const DevParams& PO = A.P[o.sys];  // the owner's system (a warp may span two)
+    const double DijSq = geometry(PO.box, oi, xo, q4, Rij);
     const int cq = PP ? 0 : A.comp[q];
     const int ca = oi ? o.cp : cq, cb = oi ? cq : o.cp;
     const double Ra = oi ? o.R : q4.w, Rb = oi ? q4.w : o.R;
-    const double Delta = Material<PP>::min_dij_sq(P, ca, Ra, cb, Rb) - DijSq;
+    const double Delta = Material<PP>::min_dij_sq(PO, ca, Ra, cb, Rb) - DijSq;
     PairPar pp;
-    Material<PP>::pair(P, ca, Ra, cb, Rb, pp);
+    Material<PP>::pair(PO, ca, Ra, cb, Rb, pp);
     const double4 qv4 = A.v4[q];
     const double2 qw2 = A.w2[q];
     const double vo[3] = {o.vx, o.vy, o.vz}, wo[3] = {o.wx, o.wy, o.wz};
@@ -1028,7 +1039,7 @@ __global__ void __launch_bounds__(128, DEM_PASS_BLOCKS_FP64) k_pass_fp64(
     for (int k = 0; k < 3; k++) T[k] = T[k] + iT[k];
   };
   const OwnerF64 me{xp[0], xp[1], xp[2], Rp, vp[0], vp[1], vp[2], wp[0], wp[1], wp[2],
-                    p, cp, n1, 0};
+                    p, cp, n1, A.sysid ? A.sysid[p] : 0};
   contact_loop(A.cand, A.X, n, p, valid, n1, n2b, n1 + n2b + n2a, P.nw > 0, me, s_k[wid],
                s_o[wid], test, compute, accum, walls, own);
 
@@ -1058,7 +1069,7 @@ __global__ void __launch_bounds__(128, DEM_PASS_BLOCKS_FP64) k_pass_fp64(
     for (int k = 0; k < 3; k++) acc[k] = F[k] * inv_m;
 #pragma unroll
     for (int k = 0; k < 3; k++) alp[k] = T[k] * inv_i;
-    epilogue<EPI>(A, p, xp, Rp, vp, wp, acc, alp, c, d2);
+    epilogue<EPI>(A, P, p, xp, Rp, vp, wp, acc, alp, c, d2);
   }
   publish_counts(A.cnt, A.update != 0, n_col, n_pc, n_wc, (unsigned)need);
   if (EPI != EPI_STORE) publish_disp(A.cnt, d2);

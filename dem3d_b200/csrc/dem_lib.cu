@@ -34,9 +34,16 @@ struct PendingEvent {
 }  // namespace
 
 struct dem_ctx {
-  dem_params params{};
-  DevParams hp{};
-  DevParams* dp = nullptr;
+  dem_params params{};  // of system 0 (shared integrator settings)
+  DevParams hp{};       // system 0
+  DevParams* dp = nullptr;  // device table, one entry per system
+  int nsys = 1;
+  std::vector<DevParams> hsys;        // host copies of the table
+  std::vector<dem_params> sys_params; // the parameters each system was created with
+  std::vector<int> counts;            // particles per system (ensembles)
+  int ncell_total = 0;
+  int* cellsys = nullptr;  // [ncell_total] system of every cell (ensembles only)
+  int* sysid = nullptr;    // [n] system of every particle (ensembles only)
   int n = 0;
   int nprev = 0;
   bool state_set = false;
@@ -243,6 +250,8 @@ void free_lists(dem_ctx* c) {
 }
 
 void free_state(dem_ctx* c) {
+  cudaFree(c->sysid);
+  c->sysid = nullptr;
   cudaFree(c->staging);
   c->staging = nullptr;
   cudaFree(c->state_block);
@@ -348,7 +357,7 @@ constexpr int FULL_BLOCKS = 148 * 8;  // full candidate-row rebuild (grid-stride
 
 int init_cells(dem_ctx* c) {
   const int n = c->n;
-  const int ncell = c->hp.ncell;
+  const int ncell = c->ncell_total;
   CellLists& L = c->L;
   CK(cudaMemsetAsync(L.head, 0xFF, sizeof(int) * (size_t)ncell, c->stream));
   CK(cudaMemsetAsync(L.arr_head, 0xFF, sizeof(int) * (size_t)ncell, c->stream));
@@ -357,8 +366,8 @@ int init_cells(dem_ctx* c) {
   if (n > 0) CK(cudaMemsetAsync(L.mflag, 0, sizeof(int) * (size_t)n, c->stream));
   CK(cudaMemsetAsync(c->cell_cnt, 0, sizeof(int) * (size_t)ncell, c->stream));
   if (n > 0) {
-    launch(c, "cell_assign", k_assign, blocks_for(n, 256), 256, (const DevParams*)c->dp, n, 1,
-           (const double*)c->P.px, (const double*)c->P.py, (const double*)c->P.pz,
+    launch(c, "cell_assign", k_assign, blocks_for(n, 256), 256, (const DevParams*)c->dp,
+           (const int*)c->sysid, n, 1, (const double*)c->P.px, (const double*)c->P.py, (const double*)c->P.pz,
            (const int*)c->S.orig, (const int*)c->S.cell, c->cell_cnt, c->a_cell, c->a_loc,
            c->a_key, c->a_orig, c->cnt);
     launch(c, "scan_tiles", k_scan_tiles, (unsigned)c->n_tiles, SCAN_THREADS,
@@ -397,12 +406,7 @@ PassArgs<V4, W2> pass_args(dem_ctx* c, int side, bool update, double dt, const R
                            int tag, const StateArrays& tgt) {
   PassArgs<V4, W2> A;
   A.P = c->dp;
-  for (int k = 0; k < 3; k++) {
-    A.box.lbox[k] = c->hp.lbox[k];
-    A.box.inv_lbox[k] = c->hp.inv_lbox[k];
-    A.box.pbc[k] = c->hp.pbc[k];
-    A.box.half_lim[k] = 0.49 * c->hp.lbox[k];
-  }
+  A.sysid = c->sysid;
   A.n = c->n;
   A.X = c->X[side];
   A.v4 = (const V4*)c->v4[side];
@@ -467,12 +471,12 @@ int prepare_side(dem_ctx* c, int side) {
     const double4* Xlast = c->last_side >= 0 ? c->X[c->last_side] : nullptr;
     if (c->precision == DEM_PREC_MIXED)
       launch(c, "prepare", k_prepare<float4, float2>, blocks_for(c->n, 256), 256,
-             (const DevParams*)c->dp, c->n, src, (const double*)c->radius, c->X[side],
+             (const DevParams*)c->dp, (const int*)c->sysid, c->n, src, (const double*)c->radius, c->X[side],
              (float4*)c->v4[side], (float2*)c->w2[side], Xlast, (const int*)c->L.cell[c->par],
              c->L, nxt, c->cnt);
     else
       launch(c, "prepare", k_prepare<double4, double2>, blocks_for(c->n, 256), 256,
-             (const DevParams*)c->dp, c->n, src, (const double*)c->radius, c->X[side],
+             (const DevParams*)c->dp, (const int*)c->sysid, c->n, src, (const double*)c->radius, c->X[side],
              (double4*)c->v4[side], (double2*)c->w2[side], Xlast, (const int*)c->L.cell[c->par],
              c->L, nxt, c->cnt);
   }
@@ -485,11 +489,13 @@ void launch_screen(dem_ctx* c, int side, int tag) {
   if (c->n == 0) return;
   const unsigned g = std::min(blocks_for((long long)c->n * 32, 256), (unsigned)FULL_BLOCKS);
   if (c->pp)
-    launch(c, "screen", k_screen<true>, g, 256, (const DevParams*)c->dp, c->n,
+    launch(c, "screen", k_screen<true>, g, 256, (const DevParams*)c->dp, (const int*)c->sysid,
+           (const int*)c->cellsys, c->n,
            (const double4*)c->X[side], (const int*)c->comp, (const int*)c->L.cell[c->par], c->L,
            c->rows, c->cnt, tag);
   else
-    launch(c, "screen", k_screen<false>, g, 256, (const DevParams*)c->dp, c->n,
+    launch(c, "screen", k_screen<false>, g, 256, (const DevParams*)c->dp, (const int*)c->sysid,
+           (const int*)c->cellsys, c->n,
            (const double4*)c->X[side], (const int*)c->comp, (const int*)c->L.cell[c->par], c->L,
            c->rows, c->cnt, tag);
 }
@@ -497,8 +503,8 @@ void launch_screen(dem_ctx* c, int side, int tag) {
 // relink towards the prepared assignment, then the candidate rows
 void pass_lists(dem_ctx* c, int side, bool update, int tag) {
   const int b = c->par ^ 1;
-  launch(c, "relink", k_relink, (unsigned)LIST_BLOCKS, 256, (const DevParams*)c->dp, c->L, b,
-         c->n, update ? 1 : 0, c->cnt);
+  launch(c, "relink", k_relink, (unsigned)LIST_BLOCKS, 256, (const DevParams*)c->dp,
+         (const int*)c->cellsys, c->L, b, c->n, update ? 1 : 0, c->cnt);
   c->par = b;
   launch_screen(c, side, tag);
 }
@@ -651,7 +657,8 @@ int move_particles_euler_impl(dem_ctx* c) {
     c->prepared = -1;
     c->time = c->time + dt;
   }
-  launch(c, "apply_pbc", k_apply_pbc, blocks_for(n, 256), 256, (const DevParams*)c->dp, n, c->P,
+  launch(c, "apply_pbc", k_apply_pbc, blocks_for(n, 256), 256, (const DevParams*)c->dp,
+         (const int*)c->sysid, n, c->P,
          (const Counters*)c->cnt);
   c->prepared = -1;
   cudaError_t e = cudaGetLastError();
@@ -712,14 +719,15 @@ int dem_select_device(int32_t device) {
 
 const char* dem_last_error(const dem_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
-int dem_create(const dem_params* p, dem_ctx** out) {
-  if (!p || !out) return DEM_ERR_INVALID;
-  *out = nullptr;
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-    cudaGetLastError();
-    return DEM_ERR_NO_DEVICE;
-  }
+}  // extern "C"
+
+namespace {
+
+// DevParams of one system: scaled parameters, ABM coefficients
+// (InitializeAuxiliaries, src/MDEM.f90:110-162), the cell grid
+// (InitCellStructure3D, src/MCells.f90:155-227) and the force tables
+// (InitializeForce, src/MForces.f90:54-87).
+int build_system(const dem_params* p, DevParams& h) {
   if (p->method_order < 1 || p->method_order > 4) return DEM_ERR_INVALID;
   if (p->n_walls < 0 || p->n_walls > NWM) return DEM_ERR_INVALID;
   if (p->n_components < 0 || p->n_components > NCM) return DEM_ERR_INVALID;
@@ -728,20 +736,7 @@ int dem_create(const dem_params* p, dem_ctx** out) {
   if (p->precision == DEM_PREC_MIXED && !mixed_available()) return DEM_ERR_UNSUPPORTED;
   for (int w = 0; w < p->n_walls; w++)
     if (p->walls[w].shape != DEM_WALL_RECTANGLE) return DEM_ERR_UNSUPPORTED;
-
-  dem_ctx* c = new dem_ctx();
-  c->params = *p;
-  c->pp = p->n_components == 0;
-  c->precision = p->precision;
-  c->nprev = p->method_order - 1;
-  c->hcap = p->hist_capacity > 0 ? p->hist_capacity : 16;
-  cudaGetDevice(&c->device);
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
-    delete c;
-    return DEM_ERR_CUDA;
-  }
-
-  DevParams& h = c->hp;
+  h = DevParams{};
   h.nc = p->n_components;
   h.nw = p->n_walls;
   for (int k = 0; k < 3; k++) {
@@ -750,7 +745,7 @@ int dem_create(const dem_params* p, dem_ctx** out) {
     h.inv_lbox[k] = 1.0 / p->lbox[k];  // ScaleVariables, src/DEM.f90:825
     h.gravity[k] = p->gravity[k];
   }
-  h.nprev = c->nprev;
+  h.nprev = p->method_order - 1;
   // ABM coefficients, src/MDEM.f90:127-154
   double dt = p->time_step;
   switch (p->method_order) {
@@ -784,8 +779,6 @@ int dem_create(const dem_params* p, dem_ctx** out) {
   }
   double CutOff = 2.0 * rmax;
   if (!(CutOff > 0.0)) {
-    cudaStreamDestroy(c->stream);
-    delete c;
     return DEM_ERR_INVALID;
   }
   int MaxNCell = p->max_ncell > 0 ? p->max_ncell : 30000;
@@ -806,15 +799,11 @@ int dem_create(const dem_params* p, dem_ctx** out) {
   int N[3] = {Nx, Ny, Nz};
   for (int k = 0; k < 3; k++) {
     if (N[k] < 1) {
-      cudaStreamDestroy(c->stream);
-      delete c;
       return DEM_ERR_INVALID;
     }
     // with 1 or 2 cells along a periodic axis the reference lists a cell
     // twice in a half shell (duplicate pair visits); not reproduced here
     if (p->pbc[k] && N[k] < 3) {
-      cudaStreamDestroy(c->stream);
-      delete c;
       return DEM_ERR_UNSUPPORTED;
     }
   }
@@ -884,15 +873,79 @@ int dem_create(const dem_params* p, dem_ctx** out) {
     h.walls[w] = p->walls[w];
   }
 
-  cudaError_t e = cudaMalloc(&c->dp, sizeof(DevParams));
+  for (int k = 0; k < 3; k++) {
+    h.box.lbox[k] = h.lbox[k];
+    h.box.inv_lbox[k] = h.inv_lbox[k];
+    h.box.half_lim[k] = 0.49 * h.lbox[k];
+    h.box.pbc[k] = h.pbc[k];
+  }
+  return DEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dem_create(const dem_params* p, dem_ctx** out) { return dem_create_ensemble(p, 1, out); }
+
+int dem_create_ensemble(const dem_params* ps, int32_t nsys, dem_ctx** out) {
+  if (!ps || !out || nsys < 1) return DEM_ERR_INVALID;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return DEM_ERR_NO_DEVICE;
+  }
+  std::vector<DevParams> hs((size_t)nsys);
+  long long ncell = 0;
+  for (int s = 0; s < nsys; s++) {
+    const dem_params* p = ps + s;
+    // the systems share the integrator and the precision
+    if (p->method_order != ps->method_order || p->euler_intervals != ps->euler_intervals ||
+        p->time_step != ps->time_step || p->precision != ps->precision ||
+        (p->n_components == 0) != (ps->n_components == 0))
+      return DEM_ERR_INVALID;
+    int st = build_system(p, hs[(size_t)s]);
+    if (st) return st;
+    hs[(size_t)s].coff = (int)ncell;
+    hs[(size_t)s].sys = s;
+    ncell += hs[(size_t)s].ncell;
+    if (ncell >= (1LL << 30)) return DEM_ERR_INVALID;
+  }
+  const dem_params* p = ps;
+  dem_ctx* c = new dem_ctx();
+  c->params = *p;
+  c->pp = p->n_components == 0;
+  c->precision = p->precision;
+  c->nprev = p->method_order - 1;
+  c->hcap = p->hist_capacity > 0 ? p->hist_capacity : 16;
+  c->nsys = nsys;
+  c->hsys = hs;
+  c->hp = hs[0];
+  c->ncell_total = (int)ncell;
+  c->sys_params.assign(ps, ps + nsys);
+  cudaGetDevice(&c->device);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return DEM_ERR_CUDA;
+  }
+  const size_t NC = (size_t)c->ncell_total;
+  cudaError_t e = cudaMalloc(&c->dp, sizeof(DevParams) * (size_t)nsys);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(c->dp, &h, sizeof(DevParams), cudaMemcpyHostToDevice, c->stream);
+    e = cudaMemcpy(c->dp, hs.data(), sizeof(DevParams) * (size_t)nsys, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && nsys > 1) {
+    std::vector<int> cs(NC);
+    for (int s = 0; s < nsys; s++)
+      for (int k = 0; k < hs[(size_t)s].ncell; k++) cs[(size_t)hs[(size_t)s].coff + k] = s;
+    e = cudaMalloc(&c->cellsys, sizeof(int) * NC);
+    if (e == cudaSuccess) e = cudaMemcpy(c->cellsys, cs.data(), sizeof(int) * NC, cudaMemcpyHostToDevice);
+  }
   if (e == cudaSuccess) e = cudaMalloc(&c->cnt, sizeof(Counters));
   if (e == cudaSuccess) e = cudaMemsetAsync(c->cnt, 0, sizeof(Counters), c->stream);
   if (e == cudaSuccess) e = cudaMallocHost(&c->hcnt, sizeof(Counters));
-  if (e == cudaSuccess) e = cudaMalloc(&c->cell_start, sizeof(int) * ((size_t)h.ncell + 1));
-  if (e == cudaSuccess) e = cudaMalloc(&c->cell_cnt, sizeof(int) * (size_t)h.ncell);
-  c->n_tiles = (h.ncell + SCAN_TILE - 1) / SCAN_TILE;
+  if (e == cudaSuccess) e = cudaMalloc(&c->cell_start, sizeof(int) * (NC + 1));
+  if (e == cudaSuccess) e = cudaMalloc(&c->cell_cnt, sizeof(int) * NC);
+  c->n_tiles = (int)((NC + SCAN_TILE - 1) / SCAN_TILE);
   if (e == cudaSuccess) e = cudaMalloc(&c->scan_bsum, sizeof(int) * (size_t)c->n_tiles);
   if (e == cudaSuccess) e = cudaMalloc(&c->obs_partial, sizeof(double) * 8 * 1184);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
@@ -906,12 +959,31 @@ int dem_create(const dem_params* p, dem_ctx** out) {
   return DEM_OK;
 }
 
+int dem_set_system_counts(dem_ctx* c, const int32_t* counts) {
+  if (!c || !counts) return DEM_ERR_INVALID;
+  long long off = 0;
+  for (int s = 0; s < c->nsys; s++) {
+    if (counts[s] < 0) return fail(c, DEM_ERR_INVALID, "negative system size");
+    c->hsys[(size_t)s].poff = (int)off;
+    c->hsys[(size_t)s].np = counts[s];
+    off += counts[s];
+    if (off >= (1LL << 30)) return fail(c, DEM_ERR_INVALID, "too many particles");
+  }
+  c->counts.assign(counts, counts + c->nsys);
+  c->hp = c->hsys[0];
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpy(c->dp, c->hsys.data(), sizeof(DevParams) * (size_t)c->nsys,
+                cudaMemcpyHostToDevice));
+  return DEM_OK;
+}
+
 void dem_destroy(dem_ctx* c) {
   if (!c) return;
   if (c->stream) cudaStreamSynchronize(c->stream);
   drop_graphs(c);
   free_state(c);
   cudaFree(c->dp);
+  cudaFree(c->cellsys);
   cudaFree(c->cnt);
   if (c->hcnt) cudaFreeHost(c->hcnt);
   cudaFree(c->cell_start);
@@ -941,13 +1013,28 @@ int dem_set_state(dem_ctx* c, int32_t n, const int32_t* comp, const double* radi
   if (!c->pp && !comp) return fail(c, DEM_ERR_INVALID, "component indices required");
   if (c->pp && !radius) return fail(c, DEM_ERR_INVALID, "per-particle radii required");
   if (n >= (1 << 30)) return fail(c, DEM_ERR_INVALID, "too many particles");
+  // system of every particle (an ensemble's particles are concatenated by system)
+  std::vector<int> sid;
+  if (c->nsys > 1) {
+    if ((int)c->counts.size() != c->nsys)
+      return fail(c, DEM_ERR_STATE, "ensemble: call dem_set_system_counts first");
+    long long tot = 0;
+    for (int k : c->counts) tot += k;
+    if (tot != n) return fail(c, DEM_ERR_INVALID, "n differs from the sum of the system sizes");
+    sid.resize((size_t)n);
+    for (int s = 0, i = 0; s < c->nsys; s++)
+      for (int k = 0; k < c->counts[(size_t)s]; k++) sid[(size_t)i++] = s;
+  }
+  auto sys_of = [&](int i) -> const dem_params& {
+    return c->sys_params[sid.empty() ? 0 : (size_t)sid[(size_t)i]];
+  };
   if (!c->pp)
     for (int i = 0; i < n; i++)
-      if (comp[i] < 0 || comp[i] >= c->params.n_components)
+      if (comp[i] < 0 || comp[i] >= sys_of(i).n_components)
         return fail(c, DEM_ERR_INVALID, "component index out of range");
   if (c->pp)
     for (int i = 0; i < n; i++)
-      if (!(radius[i] > 0.0) || radius[i] > c->params.pp_rmax)
+      if (!(radius[i] > 0.0) || radius[i] > sys_of(i).pp_rmax)
         return fail(c, DEM_ERR_INVALID, "radius must lie in (0, pp_rmax]");
   CK(cudaStreamSynchronize(c->stream));
   drop_graphs(c);
@@ -973,7 +1060,7 @@ int dem_set_state(dem_ctx* c, int32_t n, const int32_t* comp, const double* radi
   CK(cudaMalloc(&c->a_key, sizeof(unsigned) * N));
   CK(cudaMalloc(&c->t_key, sizeof(unsigned) * N));
   {
-    const size_t NC = (size_t)c->hp.ncell;
+    const size_t NC = (size_t)c->ncell_total;
     CellLists& L = c->L;
     CK(cudaMalloc(&L.head, sizeof(int) * NC));
     CK(cudaMalloc(&L.next, sizeof(int) * N));
@@ -1017,7 +1104,11 @@ int dem_set_state(dem_ctx* c, int32_t n, const int32_t* comp, const double* radi
   std::vector<double> rr(N, 0.0);
   for (int i = 0; i < n; i++) {
     ci[i] = comp ? comp[i] : 0;
-    rr[i] = radius ? radius[i] : c->params.comp_radius[ci[i]];
+    rr[i] = radius ? radius[i] : sys_of(i).comp_radius[ci[i]];
+  }
+  if (!sid.empty()) {
+    CK(cudaMalloc(&c->sysid, sizeof(int) * N));
+    CK(cudaMemcpy(c->sysid, sid.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice));
   }
   CK(cudaMemcpy(c->comp, ci.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->radius, rr.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
@@ -1322,7 +1413,7 @@ int dem_get_cells(dem_ctx* c, int32_t* cell_index, int32_t* traversal, int32_t* 
   int st = validate_ready(c);
   if (st) return st;
   CK(cudaStreamSynchronize(c->stream));
-  const int n = c->n, ncell = c->hp.ncell;
+  const int n = c->n, ncell = c->ncell_total;
   std::vector<int> cell((size_t)std::max(n, 1)), next((size_t)std::max(n, 1)), head((size_t)ncell);
   if (n > 0) {
     CK(cudaMemcpy(cell.data(), c->L.cell[c->par], sizeof(int) * n, cudaMemcpyDeviceToHost));
@@ -1533,10 +1624,12 @@ int dem_get_observables(dem_ctx* c, dem_observables* o) {
   const int grid = 148 * 4;
   if (c->n > 0) {
     if (c->pp)
-      launch(c, "observables", k_observables<true>, grid, 256, (const DevParams*)c->dp, c->n, c->P,
+      launch(c, "observables", k_observables<true>, grid, 256, (const DevParams*)c->dp,
+             (const int*)c->sysid, c->n, c->P,
              (const double*)c->radius, (const int*)c->comp, c->obs_partial);
     else
-      launch(c, "observables", k_observables<false>, grid, 256, (const DevParams*)c->dp, c->n,
+      launch(c, "observables", k_observables<false>, grid, 256, (const DevParams*)c->dp,
+             (const int*)c->sysid, c->n,
              c->P, (const double*)c->radius, (const int*)c->comp, c->obs_partial);
   }
   std::vector<double> part((size_t)grid * 8, 0.0);
@@ -1548,7 +1641,9 @@ int dem_get_observables(dem_ctx* c, dem_observables* o) {
     for (int k = 0; k < 8; k++) acc[k] += part[(size_t)b * 8 + k];
   o->kinetic_energy = 0.5 * acc[0];
   o->potential_energy = acc[1];
-  o->packing_fraction = acc[2] / (c->params.lbox[0] * c->params.lbox[1] * c->params.lbox[2]);
+  double vol = 0.0;  // ensembles: all boxes together
+  for (const dem_params& q : c->sys_params) vol += q.lbox[0] * q.lbox[1] * q.lbox[2];
+  o->packing_fraction = acc[2] / vol;
   o->momentum[0] = acc[3];
   o->momentum[1] = acc[4];
   o->momentum[2] = acc[5];
@@ -1780,7 +1875,7 @@ extern "C" int dem_distribute_particles_noalloc(const dem_params* p, int32_t n,
   if (n > 0) {
     k_rows_to_soa<<<blocks_for(n, 256), 256, 0, st>>>(n, d_pos, S->px, S->py, S->pz);
     // DistributeParticles3D: every particle enters its cell in index order
-    k_assign<<<blocks_for(n, 256), 256, 0, st>>>(dp, n, 1, S->px, S->py, S->pz, d_traversal,
+    k_assign<<<blocks_for(n, 256), 256, 0, st>>>(dp, nullptr, n, 1, S->px, S->py, S->pz, d_traversal,
                                                    S->slot_cell, S->cell_cnt, S->a_cell, S->a_loc,
                                                    S->a_key, S->a_orig, cnt);
   }

@@ -250,7 +250,7 @@ __device__ __forceinline__ unsigned long long wsum(unsigned long long v) {
 struct OwnerMixed {
   double x, y, z, R;
   float vx, vy, vz, wx, wy, wz;
-  int p, cp, n1, pad;
+  int p, cp, n1, sys;
 };
 
 template <bool PP, int EPI>
@@ -265,8 +265,8 @@ __global__ void __launch_bounds__(128, DEM_PASS_BLOCKS_MIXED) k_pass_mixed(
   const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = p0 < A.n;
   const int p = valid ? p0 : 0;
-  const DevParams& P = *A.P;
-  const Box& B = A.box;
+  const DevParams& P = sys_params(A.P, A.sysid, p);  // this particle's system
+  const Box& B = P.box;
   const int n = A.n;
   unsigned n_col = 0, n_pc = 0, n_wc = 0;
   int need = 0;
@@ -310,18 +310,19 @@ __global__ void __launch_bounds__(128, DEM_PASS_BLOCKS_MIXED) k_pass_mixed(
   };
   // Rij = x_j - x_i (minimum image, FP64); candidate k of a row is "j" (its
   // owner is "i") for k < n1
-  auto geometry = [&](bool oi, const double xo[3], const double4& q4, double Rij[3]) -> double {
+  auto geometry = [&](const Box& Bx, bool oi, const double xo[3], const double4& q4,
+                      double Rij[3]) -> double {
     Rij[0] = oi ? q4.x - xo[0] : xo[0] - q4.x;
     Rij[1] = oi ? q4.y - xo[1] : xo[1] - q4.y;
     Rij[2] = oi ? q4.z - xo[2] : xo[2] - q4.z;
 #pragma unroll
-    for (int k = 0; k < 3; k++) Rij[k] = min_image_exact(Rij[k], B, k);
+    for (int k = 0; k < 3; k++) Rij[k] = min_image_exact(Rij[k], Bx, k);
     return sumsq3(Rij);
   };
   auto test = [&](int k, int q, const double4& q4) -> bool {
     const bool pi = k < n1;
     double Rij[3];
-    const double DijSq = geometry(pi, xp, q4, Rij);
+    const double DijSq = geometry(B, pi, xp, q4, Rij);
     const int cq = PP ? 0 : A.comp[q];
     const double mds = pi ? MMat<PP>::min_dij_sq(P, cp, Rpd, cq, q4.w)
                           : MMat<PP>::min_dij_sq(P, cq, q4.w, cp, Rpd);
@@ -333,14 +334,15 @@ __global__ void __launch_bounds__(128, DEM_PASS_BLOCKS_MIXED) k_pass_mixed(
     const double4 q4 = A.X[q];
     const double xo[3] = {o.x, o.y, o.z};
     double Rij[3];
-    const double DijSq = geometry(oi, xo, q4, Rij);
+    const DevParams& PO = A.P[o.sys];  // the owner's system (a warp may span two)
+    const double DijSq = geometry(PO.box, oi, xo, q4, Rij);
     const int cq = PP ? 0 : A.comp[q];
     const int ca = oi ? o.cp : cq, cb = oi ? cq : o.cp;
     const double Rad = oi ? o.R : q4.w, Rbd = oi ? q4.w : o.R;
-    const double Delta = MMat<PP>::min_dij_sq(P, ca, Rad, cb, Rbd) - DijSq;
+    const double Delta = MMat<PP>::min_dij_sq(PO, ca, Rad, cb, Rbd) - DijSq;
     const float Ra = (float)Rad, Rb = (float)Rbd;
     MPair m;
-    MMat<PP>::pair(P, ca, Ra, cb, Rb, m);
+    MMat<PP>::pair(PO, ca, Ra, cb, Rb, m);
     const float4 qv4 = A.v4[q];
     const float2 qw2 = A.w2[q];
     const F3 vq = mk(qv4.x, qv4.y, qv4.z), wq = mk(qv4.w, qw2.x, qw2.y);
@@ -425,7 +427,8 @@ __global__ void __launch_bounds__(128, DEM_PASS_BLOCKS_MIXED) k_pass_mixed(
     F = F + iF;
     T = T + iT;
   };
-  const OwnerMixed me{xp[0], xp[1], xp[2], Rpd, vp.x, vp.y, vp.z, wp.x, wp.y, wp.z, p, cp, n1, 0};
+  const OwnerMixed me{xp[0], xp[1], xp[2], Rpd, vp.x, vp.y, vp.z, wp.x, wp.y, wp.z, p, cp, n1,
+                      A.sysid ? A.sysid[p] : 0};
   contact_loop(A.cand, A.X, n, p, valid, n1, n2b, n1 + n2b + n2a, P.nw > 0, me, s_k[wid],
                s_o[wid], test, compute, accum, walls, own);
 
@@ -459,7 +462,7 @@ __global__ void __launch_bounds__(128, DEM_PASS_BLOCKS_MIXED) k_pass_mixed(
     } else if (EPI == EPI_CORRECT) {
       vd[0] = A.pred.vx[p]; vd[1] = A.pred.vy[p]; vd[2] = A.pred.vz[p];
     }
-    epilogue<EPI>(A, p, xp, Rpd, vd, wd, acc, alp, c, d2);
+    epilogue<EPI>(A, P, p, xp, Rpd, vd, wd, acc, alp, c, d2);
   }
   publish_counts(A.cnt, A.update != 0, n_col, n_pc, n_wc, (unsigned)need);
   if (EPI != EPI_STORE) publish_disp(A.cnt, d2);

@@ -221,12 +221,11 @@ __device__ __forceinline__ float2 mk_w2<float2>(double a, double b) {
 //              x(t+dt) is the next pass's position.
 // d2 receives the squared displacement from this pass's position to the next.
 template <int EPI, class V4, class W2>
-__device__ __forceinline__ void epilogue(const PassArgs<V4, W2>& A, int p, const double xp[3],
-                                         double Rp, const double vp[3], const double wp[3],
-                                         const double acc[3], const double alp[3], int c_cur,
-                                         double& d2) {
-  const DevParams& P = *A.P;
-  const Box& B = A.box;
+__device__ __forceinline__ void epilogue(const PassArgs<V4, W2>& A, const DevParams& P, int p,
+                                         const double xp[3], double Rp, const double vp[3],
+                                         const double wp[3], const double acc[3],
+                                         const double alp[3], int c_cur, double& d2) {
+  const Box& B = P.box;
   const size_t n = (size_t)A.n;
   if (EPI == EPI_STORE) {
     A.tgt.ax[p] = acc[0]; A.tgt.ay[p] = acc[1]; A.tgt.az[p] = acc[2];

@@ -70,6 +70,26 @@ class DEMSystem:
             raise DEMError(st, "create failed" + (": no CUDA device" if st == -7 else ""))
         self.n = 0
 
+    @classmethod
+    def ensemble(cls, params_list, counts, lib=None):
+        """Independent systems in one context (dem_create_ensemble): every
+        stage of a step is one launch over all systems.  ``counts`` are the
+        particles per system; particle arrays are concatenated by system."""
+        self = cls.__new__(cls)
+        self.lib = lib if lib is not None else _abi.load_library()
+        self.prefix = "dem_"
+        self.params = params_list[0]
+        self.nprev = int(self.params.method_order) - 1
+        self._ctx = C.c_void_p()
+        arr = (DemParams * len(params_list))(*params_list)
+        st = self.lib.dem_create_ensemble(arr, len(params_list), C.byref(self._ctx))
+        if st != 0:
+            raise DEMError(st, "create_ensemble failed")
+        self.n = 0
+        cnt = np.ascontiguousarray(counts, dtype=np.int32)
+        self._call("set_system_counts", _iptr(cnt))
+        return self
+
     # -- plumbing ---------------------------------------------------------
     def _fn(self, name):
         return getattr(self.lib, self.prefix + name)

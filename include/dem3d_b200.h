@@ -134,6 +134,17 @@ int dem_select_device(int32_t device);
  * (src/MDEM.f90:110-162: ABM coefficients, InitializeCellList
  * src/MForces.f90:91-106, InitializeForce :54-87). */
 int dem_create(const dem_params* params, dem_ctx** out);
+/* An ensemble of n_systems independent systems in one context (no
+ * counterpart in the reference, which runs one system per process): every
+ * system has its own box, walls, cell grid and material parameters; the
+ * integrator (method_order, euler_intervals, time_step) and the precision are
+ * shared.  Every stage of a step runs as one launch over all systems.
+ * Particles are concatenated by system (sizes from dem_set_system_counts,
+ * called before dem_set_state); particle and cell numbers are global, so a
+ * system's particle i is global index offset_s + i.  dem_get_grid returns
+ * system 0's grid; contacts, Ncol and observables cover all systems. */
+int dem_create_ensemble(const dem_params* params, int32_t n_systems, dem_ctx** out);
+int dem_set_system_counts(dem_ctx* ctx, const int32_t* counts);
 /* FinalizeDEM, src/MDEM.f90:166-179. */
 void dem_destroy(dem_ctx* ctx);
 const char* dem_last_error(const dem_ctx* ctx);
