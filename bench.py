@@ -342,9 +342,14 @@ def kernel_bytes(name, n, mixed, z_pp, m_cand, z_pw, nw):
 
 
 def measure(s, w, args, world, local, torch, dist):
-    """Warm-up, then the timed region (graph replay of K steps)."""
+    """Warm-up (and the autotuner's trials, on the live run), then the timed
+    region (graph replay of K steps)."""
     s.run(1, 3 + args.warmup)
     first = 4 + args.warmup
+    tuning = None
+    if not args.no_autotune:
+        tuning = s.autotune(first, 40)
+        first = tuning["last_step"] + 1
     last = first + args.steps - 1
     if world > 1:
         dist.barrier()
@@ -357,7 +362,7 @@ def measure(s, w, args, world, local, torch, dist):
     launches = s.launch_count() - l0
     ms = reduce_max(ms, world)
     return {"ms": ms, "launches": launches, "last": last, "clocks": clk.summary(),
-            "value": aggregate_rate(w.n, world, args.steps, ms)}
+            "value": aggregate_rate(w.n, world, args.steps, ms), "tuning": tuning}
 
 
 def force_error(w_fp64, w_mixed, src):
@@ -526,7 +531,8 @@ def run_ours(args):
             "dtype": "f64" if headline == "fp64" else "f32+f64", "data": "synthetic",
             "config": config_block(args.workload, w, world, headline),
             "gpu_launches": int(launches),
-            "precisions": {p: {"value": r["value"], "ms_per_step": r["ms"] / args.steps}
+            "precisions": {p: {"value": r["value"], "ms_per_step": r["ms"] / args.steps,
+                               "tuning": r["tuning"]}
                            for p, r in res.items()},
             "mixed_over_fp64": (res["mixed"]["value"] / res["fp64"]["value"]
                                 if "mixed" in res and "fp64" in res else None),
@@ -647,6 +653,7 @@ def run_ensemble(args):
                        "particles_per_gpu": n, "precision": prec,
                        "l2": "inputs larger than L2", "parallelism": f"{world} ensembles"},
             "gpu_launches": int(res["launches"]),
+            "tuning": res["tuning"],
             "sequential_fp64_systems": seq,
             "ensemble_over_sequential_fp64": value / seq["value"] if seq else None,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
@@ -676,6 +683,8 @@ def main():
     ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="skip the autotuner's trials (default settings)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -128,6 +128,9 @@ GPU_ONLY = {
     "get_row_stats": (C.c_int, [_P, _I64P, _I32P]),
     "create_ensemble": (C.c_int, [C.POINTER(DemParams), C.c_int32, C.POINTER(_P)]),
     "set_system_counts": (C.c_int, [_P, _I32P]),
+    "set_tuning": (C.c_int, [_P, C.c_double, C.c_int32]),
+    "get_tuning": (C.c_int, [_P, _DP, _I32P]),
+    "autotune": (C.c_int, [_P, C.c_int32, C.c_int32, _I32P, _DP]),
     # device pointers for positions and outputs; see the header
     "distribute_particles_noalloc": (C.c_int, [C.POINTER(DemParams), C.c_int32, _P, _P, _P, _P,
                                                _I32P, _P, C.c_char_p, C.c_int32]),

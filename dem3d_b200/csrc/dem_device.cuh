@@ -47,6 +47,7 @@ struct DevParams {
   double nxbylx, nybyly, nzbylz, nxby2, nyby2, nzby2;
   double ab0, am0, ab[3], am[3];
   double max_min_dij_sq;  // largest MinDijSq of any pair (screening early-out)
+  double cutoff;          // CutOff = 2 * largest radius (cell size floor)
   double vl_skin;         // candidate-row skin (added to MinDij)
   double vl_thr;          // accumulated displacement bound that forces a full rebuild
   double inv_nx, inv_ny;  // 1/Nx, 1/Ny (cell coordinates without integer division)
@@ -88,6 +89,7 @@ struct Counters {
   int row_overflow;  // a candidate row needed more than kc entries
   int need_kc;       // longest candidate row requested
   int list_error;    // a cell-list walk exceeded its bound (corrupt lists)
+  int nonfinite;     // a particle position became NaN or infinite
   unsigned int disp_max;  // FP32 bits (rounded up) of the largest displacement of one pass
   double disp_acc;   // sum of disp_max since the last full rebuild
   double wall_fn[NWM];

@@ -467,6 +467,10 @@ __global__ void __launch_bounds__(256) k_prepare(const DevParams* __restrict__ P
       d2 = disp2(P, x, y);
       if (!(d2 <= 1e300)) d2 = 1e300;  // a non-finite state forces a full rebuild
     }
+    if (!isfinite(x[0] + x[1] + x[2])) {
+      atomicExch(&cnt->nonfinite, 1);
+      atomicExch(&cnt->abort, 1);
+    }
     X[p] = make_double4(x[0], x[1], x[2], radius[p]);
     v4[p] = mk_v4<V4>(src.vx[p], src.vy[p], src.vz[p], src.wx[p]);
     w2[p] = mk_w2<W2>(src.wy[p], src.wz[p]);
@@ -807,20 +811,16 @@ __global__ void __launch_bounds__(256) k_screen(const DevParams* __restrict__ PT
 // ---------------------------------------------------------------------------
 // K2+K4: the FP64 pass kernel (exact order)
 
-// resident blocks of 128 threads per SM the pass kernels are compiled for
-// (registers per thread = 65536 / (128 * blocks))
-#ifndef DEM_PASS_BLOCKS_FP64
-#define DEM_PASS_BLOCKS_FP64 4
-#endif
-
 // Owner data handed to the lane that computes one of its contacts.
 struct OwnerF64 {
   double x, y, z, R, vx, vy, vz, wx, wy, wz;
   int p, cp, n1, sys;
 };
 
-template <bool PP, int EPI>
-__global__ void __launch_bounds__(128, DEM_PASS_BLOCKS_FP64) k_pass_fp64(
+// MINB: resident blocks of 128 threads per SM the kernel is compiled for
+// (registers per thread <= 65536 / (128 * MINB)); the autotuner picks one.
+template <bool PP, int EPI, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_pass_fp64(
     PassArgs<double4, double2> A) {
   // per warp: the current 32 contacts (candidate index, owner lane, partner)
   // and their results FN, FT, VT, torque term (12 doubles, lane-contiguous)

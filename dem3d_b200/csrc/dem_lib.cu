@@ -77,6 +77,8 @@ struct dem_ctx {
   double4* X[2] = {nullptr, nullptr};
   void* v4[2] = {nullptr, nullptr};
   void* w2[2] = {nullptr, nullptr};
+  int pass_variant = 0;  // pass kernel compiled for 4 (0) or 3 (1) blocks per SM
+  double skin_factor = 0.05;  // candidate-row skin / CutOff
   int par = 0;         // L.cell[par] is the assignment the lists hold
   int prepared = -1;   // side whose copies + next assignment are ready (-1: none)
   int last_side = -1;  // side of the last pass (its copies are intact)
@@ -440,23 +442,29 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
   const StateArrays& tgt = side ? c->Pr : c->P;
   if (c->precision == DEM_PREC_MIXED) {
     auto A = pass_args<float4, float2>(c, side, update, dt, rm, tag, tgt);
-    timed(c, "pass_mixed", [&]() { mixed_pass(c->M, c->pp, epi, A, c->hcur, c->stream); });
+    timed(c, "pass_mixed",
+          [&]() { mixed_pass(c->M, c->pp, epi, c->pass_variant, A, c->hcur, c->stream); });
     c->launches++;
     return;
   }
   auto A = pass_args<double4, double2>(c, side, update, dt, rm, tag, tgt);
   const unsigned g = blocks_for(c->n, 128);
-#define PASS_CASE(PPV)                                                                  \
+#define PASS_CASE(PPV, MB)                                                              \
   do {                                                                                  \
     if (epi == EPI_PREDICT)                                                             \
-      launch(c, "pass_fp64", k_pass_fp64<PPV, EPI_PREDICT>, g, 128, A);                 \
+      launch(c, "pass_fp64", k_pass_fp64<PPV, EPI_PREDICT, MB>, g, 128, A);             \
     else if (epi == EPI_CORRECT)                                                        \
-      launch(c, "pass_fp64", k_pass_fp64<PPV, EPI_CORRECT>, g, 128, A);                 \
+      launch(c, "pass_fp64", k_pass_fp64<PPV, EPI_CORRECT, MB>, g, 128, A);             \
     else                                                                                \
-      launch(c, "pass_fp64", k_pass_fp64<PPV, EPI_STORE>, g, 128, A);                   \
+      launch(c, "pass_fp64", k_pass_fp64<PPV, EPI_STORE, MB>, g, 128, A);               \
   } while (0)
-  if (c->pp) PASS_CASE(true);
-  else PASS_CASE(false);
+  if (c->pass_variant == 1) {
+    if (c->pp) PASS_CASE(true, 3);
+    else PASS_CASE(false, 3);
+  } else {
+    if (c->pp) PASS_CASE(true, 4);
+    else PASS_CASE(false, 4);
+  }
 #undef PASS_CASE
 }
 
@@ -572,6 +580,7 @@ int finish_pass(dem_ctx* c, int side, bool update, double dt, int epi, const Rin
     if (st) return st;
     const Counters h = *c->hcnt;
     if (!h.abort) return DEM_OK;
+    if (h.nonfinite) return fail(c, DEM_ERR_STATE, "a particle position is not finite");
     if (h.list_error) return fail(c, DEM_ERR_STATE, "cell lists inconsistent (walk bound hit)");
     if (attempt >= 8) return fail(c, DEM_ERR_CAPACITY, "capacity cannot be grown");
     st = clear_abort(c);
@@ -853,6 +862,7 @@ int build_system(const dem_params* p, DevParams& h) {
     // from them moved closer by at most twice the largest displacement since
     // the rows were built, so the rows are complete while the accumulated
     // displacement bound stays below skin/2 (0.4 skin keeps a margin)
+    h.cutoff = CutOff;
     h.vl_skin = 0.05 * CutOff;
     h.vl_thr = 0.4 * h.vl_skin;
   }
@@ -1530,6 +1540,7 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
     int done = G, failed_pass = -1;
     if (c->hcnt->abort) {
       const int tag = c->hcnt->abort_tag - 1;  // 2*(step in chunk) + pass
+      if (c->hcnt->nonfinite) return fail(c, DEM_ERR_STATE, "a particle position is not finite");
       if (c->hcnt->list_error) return fail(c, DEM_ERR_STATE, "cell lists inconsistent");
       if (tag < 0 || tag >= 2 * G) return fail(c, DEM_ERR_STATE, "bad abort tag");
       done = tag / 2;
@@ -1708,6 +1719,72 @@ int dem_get_pass_stats(dem_ctx* c, int64_t* pair_contacts, int64_t* wall_contact
   if (wall_contacts) *wall_contacts = c->last_walls;
   if (movers) *movers = c->last_movers;
   if (hist_capacity) *hist_capacity = c->hcap;
+  return DEM_OK;
+}
+
+int dem_set_tuning(dem_ctx* c, double skin_factor, int32_t pass_variant) {
+  if (!c) return DEM_ERR_INVALID;
+  if (!(skin_factor > 0.0 && skin_factor <= 0.5) || pass_variant < 0 || pass_variant > 1)
+    return fail(c, DEM_ERR_INVALID, "skin factor must lie in (0, 0.5], variant in {0, 1}");
+  CK(cudaStreamSynchronize(c->stream));
+  if (skin_factor != c->skin_factor) {
+    for (DevParams& h : c->hsys) {
+      h.vl_skin = skin_factor * h.cutoff;
+      h.vl_thr = 0.4 * h.vl_skin;
+    }
+    c->hp = c->hsys[0];
+    CK(cudaMemcpy(c->dp, c->hsys.data(), sizeof(DevParams) * (size_t)c->nsys,
+                  cudaMemcpyHostToDevice));
+    // rows built with the old skin are rebuilt by the next pass
+    const int one = 1;
+    CK(cudaMemcpy(&c->cnt->force_full, &one, sizeof(int), cudaMemcpyHostToDevice));
+    c->skin_factor = skin_factor;
+  }
+  if (pass_variant != c->pass_variant) {
+    c->pass_variant = pass_variant;
+    drop_graphs(c);
+  }
+  return DEM_OK;
+}
+
+int dem_get_tuning(dem_ctx* c, double* skin_factor, int32_t* pass_variant) {
+  if (!c) return DEM_ERR_INVALID;
+  if (skin_factor) *skin_factor = c->skin_factor;
+  if (pass_variant) *pass_variant = c->pass_variant;
+  return DEM_OK;
+}
+
+int dem_autotune(dem_ctx* c, int32_t first_step, int32_t steps_per_trial, int32_t* last_step,
+                 double* trial_ms) {
+  if (!c || steps_per_trial < 4) return DEM_ERR_INVALID;
+  int st = validate_ready(c);
+  if (st) return st;
+  const double skins[3] = {0.025, 0.05, 0.1};
+  const int trials = 6;
+  const int timed_steps = (steps_per_trial + 3) / 4 * 4;  // whole graph chunks
+  int step = first_step;
+  double best_ms = 1e300;
+  int best = 0;
+  for (int t = 0; t < trials; t++) {
+    st = dem_set_tuning(c, skins[t / 2], t % 2);
+    if (st) return st;
+    // one untimed chunk takes the graph capture and the forced full rebuild
+    st = dem_run(c, step, step + 3);
+    if (st) return st;
+    step += 4;
+    double ms = 0.0;
+    st = dem_run_timed(c, step, step + timed_steps - 1, &ms);
+    if (st) return st;
+    step += timed_steps;
+    if (trial_ms) trial_ms[t] = ms;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = t;
+    }
+  }
+  st = dem_set_tuning(c, skins[best / 2], best % 2);
+  if (st) return st;
+  if (last_step) *last_step = step - 1;
   return DEM_OK;
 }
 

@@ -242,9 +242,6 @@ __device__ __forceinline__ unsigned long long wsum(unsigned long long v) {
 // The mixed-precision pass kernel: the FP64 kernel's structure (candidate
 // rows, exact FP64 overlap test, orientation, history semantics, summation
 // order), FP32 contact arithmetic, FP64 integrator epilogue.
-#ifndef DEM_PASS_BLOCKS_MIXED
-#define DEM_PASS_BLOCKS_MIXED 4
-#endif
 
 // Owner data handed to the lane that computes one of its contacts.
 struct OwnerMixed {
@@ -253,8 +250,10 @@ struct OwnerMixed {
   int p, cp, n1, sys;
 };
 
-template <bool PP, int EPI>
-__global__ void __launch_bounds__(128, DEM_PASS_BLOCKS_MIXED) k_pass_mixed(
+// MINB: resident blocks of 128 threads per SM the kernel is compiled for
+// (registers per thread <= 65536 / (128 * MINB)); the autotuner picks one.
+template <bool PP, int EPI, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_pass_mixed(
     PassArgs<float4, float2> A, MixedView V) {
   // per warp: the current 32 contacts (candidate index, owner lane, partner)
   // and their results FN, FT, FT remainder, VT, torque term (15 floats)
@@ -589,8 +588,8 @@ bool mixed_regrow(MixedBuffers& M, int n, int newcap, int cur, const History& ol
   return true;
 }
 
-void mixed_pass(MixedBuffers& M, bool pp, int epi, const PassArgs<float4, float2>& A, int cur,
-                cudaStream_t st) {
+void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant,
+                const PassArgs<float4, float2>& A, int cur, cudaStream_t st) {
   if (A.n == 0) return;
   MixedView V;
   V.ra = M.ha[cur];
@@ -606,14 +605,19 @@ void mixed_pass(MixedBuffers& M, bool pp, int epi, const PassArgs<float4, float2
   V.wwb = M.wb[cur ^ 1];
   V.wwc = M.wc[cur ^ 1];
   const unsigned g = blocks(A.n, 128);
-#define MCASE(PPV)                                                                       \
-  do {                                                                                   \
-    if (epi == EPI_PREDICT) k_pass_mixed<PPV, EPI_PREDICT><<<g, 128, 0, st>>>(A, V);     \
-    else if (epi == EPI_CORRECT) k_pass_mixed<PPV, EPI_CORRECT><<<g, 128, 0, st>>>(A, V); \
-    else k_pass_mixed<PPV, EPI_STORE><<<g, 128, 0, st>>>(A, V);                          \
+#define MCASE(PPV, MB)                                                                      \
+  do {                                                                                      \
+    if (epi == EPI_PREDICT) k_pass_mixed<PPV, EPI_PREDICT, MB><<<g, 128, 0, st>>>(A, V);     \
+    else if (epi == EPI_CORRECT) k_pass_mixed<PPV, EPI_CORRECT, MB><<<g, 128, 0, st>>>(A, V); \
+    else k_pass_mixed<PPV, EPI_STORE, MB><<<g, 128, 0, st>>>(A, V);                          \
   } while (0)
-  if (pp) MCASE(true);
-  else MCASE(false);
+  if (variant == 1) {
+    if (pp) MCASE(true, 3);
+    else MCASE(false, 3);
+  } else {
+    if (pp) MCASE(true, 4);
+    else MCASE(false, 4);
+  }
 #undef MCASE
 }
 

@@ -26,8 +26,9 @@ void mixed_free(MixedBuffers& M);
 bool mixed_regrow(MixedBuffers& M, int n, int newcap, int cur, const History& old,
                   cudaStream_t st);
 // One pass kernel launch (FP32 contact arithmetic) on the context's stream.
-void mixed_pass(MixedBuffers& M, bool pp, int epi, const PassArgs<float4, float2>& A, int cur,
-                cudaStream_t st);
+// variant: 0 = compiled for 4 resident blocks per SM, 1 = for 3
+void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant,
+                const PassArgs<float4, float2>& A, int cur, cudaStream_t st);
 void mixed_import_history(MixedBuffers& M, const History& H, int n, int nw, int cur,
                           cudaStream_t st);
 void mixed_export_history(MixedBuffers& M, const History& H, int n, int nw, int cur,

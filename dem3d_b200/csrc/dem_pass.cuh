@@ -304,6 +304,11 @@ __device__ __forceinline__ void epilogue(const PassArgs<V4, W2>& A, const DevPar
   A.w2n[p] = mk_w2<W2>(w[1], w[2]);
   note_cell(A.L, A.cnt, A.par_nxt, p, c_cur, current_cell(P, x[0], x[1], x[2]));
   d2 = disp2(B, x, xp);
+  if (!isfinite(x[0] + x[1] + x[2])) {
+    // a diverged state would put every particle into one cell; stop here
+    atomicExch(&A.cnt->nonfinite, 1);
+    set_abort(A.cnt, A.tag);
+  }
 }
 
 // Meta word of a candidate row.

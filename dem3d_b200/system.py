@@ -306,6 +306,23 @@ class DEMSystem:
         return {"pair_contacts": a.value, "wall_contacts": b.value, "movers": m.value,
                 "hist_capacity": cap.value}
 
+    def set_tuning(self, skin_factor: float, pass_variant: int) -> None:
+        self._call("set_tuning", C.c_double(skin_factor), C.c_int32(pass_variant))
+
+    def tuning(self):
+        f, v = C.c_double(), C.c_int32()
+        self._call("get_tuning", C.byref(f), C.byref(v))
+        return {"skin_factor": f.value, "pass_variant": v.value}
+
+    def autotune(self, first_step: int, steps_per_trial: int = 20):
+        """Runs six timed trials on the live system (dem_autotune); returns
+        the last step advanced, the chosen setting and the trial times."""
+        last = C.c_int32()
+        ms = (C.c_double * 6)()
+        self._call("autotune", C.c_int32(first_step), C.c_int32(steps_per_trial),
+                   C.byref(last), ms)
+        return {"last_step": last.value, **self.tuning(), "trial_ms": list(ms)}
+
     def row_stats(self):
         """Candidate-row entries of the last pass and the row capacity."""
         t, kc = C.c_int64(), C.c_int32()
