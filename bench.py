@@ -47,6 +47,7 @@ WORKLOADS = {
     "dense16m": dict(n=16_000_000, phi=0.60, seed=1002, tile=16000),
     "dense64k": dict(n=64_000, phi=0.55, seed=1001, tile=8000),
     "ensemble4096": dict(kind="ensemble", n_systems=4096, seed=1003),
+    "bidisperse4m": dict(kind="bidisperse", n=4_000_000, seed=1004),
     "ensemble64": dict(kind="ensemble", n_systems=64, seed=1003),
 }
 
@@ -180,12 +181,22 @@ def make_workload(name, precision, rank, factory=None):
     from dem3d_b200 import params as P
     spec = WORKLOADS[name]
     prec = P.PREC_MIXED if precision == "mixed" else P.PREC_FP64
+    if spec.get("kind") == "bidisperse":
+        return configs.bidisperse_settling(n=spec["n"], seed=rank_seed(spec["seed"], rank),
+                                           precision=prec)
     return configs.dense_packing(n=spec["n"], phi=spec["phi"], seed=rank_seed(spec["seed"], rank),
                                  tile=spec["tile"], precision=prec, system_factory=factory)
 
 
 def config_block(name, w, world, precision):
     spec = WORKLOADS[name]
+    if spec.get("kind") == "bidisperse":
+        return {
+            "workload": (f"{w.n:,} bidisperse spheres (d 1 and 3, {w.info['n_large']:,} large), "
+                         "settling under gravity in a 200x200 box with floor and four side walls, "
+                         "mu=0.5, e=0.7, dt=5e-5, ABM4"),
+            "particles_per_gpu": w.n, "global_particles": w.n * world, "precision": precision,
+            "l2": "inputs larger than L2", "parallelism": f"{world} independent systems"}
     return {
         "workload": (f"{spec['n']:,} polydisperse spheres R~U[0.4,0.6], periodic cube "
                      f"phi={spec['phi']}, kn=1e5, e=0.8, mu=0.5, dt=1e-4, ABM4"),
@@ -450,8 +461,19 @@ def run_ours(args):
     clocks = res[headline]["clocks"]
 
     ferr = None
+    obs_cmp = None
     if "fp64" in systems and "mixed" in systems:
         ferr = force_error(works["fp64"], works["mixed"], systems["fp64"])
+        # both runs advanced the same steps from the same state: ensemble
+        # observables of the mixed run against the FP64 run
+        ob = {p: systems[p].observables() for p in ("fp64", "mixed")}
+        keys = ("kinetic_energy", "mean_coordination", "packing_fraction")
+        pick = {p: {k: ob[p][k] for k in keys} for p in ob}
+        for p in ob:
+            pick[p]["floor_force"] = ob[p]["wall_normal_force"][0]
+        rel = {k: (abs(pick["mixed"][k] - pick["fp64"][k]) / abs(pick["fp64"][k])
+                   if pick["fp64"][k] else None) for k in pick["fp64"]}
+        obs_cmp = {"after_step": res["fp64"]["last"], **pick, "rel_diff": rel}
     for prec, sy in systems.items():
         if prec != headline:
             sy.close()
@@ -537,6 +559,7 @@ def run_ours(args):
             "mixed_over_fp64": (res["mixed"]["value"] / res["fp64"]["value"]
                                 if "mixed" in res and "fp64" in res else None),
             "force_err_vs_fp64": ferr,
+            "observables_mixed_vs_fp64": obs_cmp,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                          "traffic": traffic, "algorithmic_bytes_per_launch": b_launch,
