@@ -95,6 +95,48 @@ def settling(n=2000, seed=1000, layer_side=10, dt=1e-4, e=0.8, mu=0.5, gravity=1
                     info={"lbox": (L, L, lz), "seed": seed})
 
 
+def hopper(n=600, seed=1005, e=0.7, mu=0.5, dt=1e-4, gravity=1.0, length=10.0, d_out=3.0,
+           d_in=14.0, method_order=4, euler_intervals=20, precision=P.PREC_FP64,
+           sigma_v=1.0, v_radial=3.0, max_ncell=30000):
+    """Monodisperse spheres (d = 1) thrown against a conic hopper: a Cone wall
+    (axis z, ``length`` long, opening diameters ``d_out`` at the bottom and
+    ``d_in`` at the top) above a floor, in a closed (non-periodic) box.  The
+    spheres start on a lattice inside the upper part of the cone, moving
+    outwards at ``v_radial`` plus N(0, sigma_v^2) noise."""
+    rng = np.random.default_rng(seed)
+    L = d_in + 4.0
+    lz = 3.0 * length
+    side = int((0.5 * d_in - 1.0) * 2.0 / 1.1)
+    pts = []
+    z = 0.5 * length - 1.0
+    while len(pts) < n:
+        for iy in range(side):
+            for ix in range(side):
+                x = (ix - 0.5 * (side - 1)) * 1.1
+                y = (iy - 0.5 * (side - 1)) * 1.1
+                # inside the cone's cross-section at height z, with a margin
+                r_z = 0.5 * d_out + (z + 0.5 * length) / length * 0.5 * (d_in - d_out)
+                if math.hypot(x, y) < r_z - 0.55 and len(pts) < n:
+                    pts.append((x, y, z))
+        z += 1.1
+    pos = np.asarray(pts) + rng.uniform(-0.03, 0.03, size=(n, 3))
+    vel = rng.normal(0.0, sigma_v, size=(n, 3))
+    rr = np.hypot(pos[:, 0], pos[:, 1])
+    vel[:, 0] += v_radial * pos[:, 0] / np.maximum(rr, 1e-9)
+    vel[:, 1] += v_radial * pos[:, 1] / np.maximum(rr, 1e-9)
+    cone = P.cone((0.0, 0.0, 0.0), length, d_out, d_in, stiffness=2.0 * KN,
+                  shear_stiffness=2.0 * KT)
+    floor = P.rectangle((0.0, 0.0, -0.5 * lz + 1.0), 0.5 * L, 0.5 * L, stiffness=2.0 * KN,
+                        shear_stiffness=2.0 * KT)
+    prm, _ = P.component_params(
+        [P.Component(n, 1.0, DENSITY, 2.0 * KN, 2.0 * KT)], [cone, floor], [[e]], [[e]], [[mu]],
+        [[e, e]], [[e, e]], [[mu, mu]], lbox=(L, L, lz), pbc=(False, False, False),
+        gravity=(0.0, 0.0, -gravity), time_step=dt, method_order=method_order,
+        euler_intervals=euler_intervals, max_ncell=max_ncell, precision=precision)
+    return Workload("hopper", prm, pos, vel, np.zeros((n, 3)), comp=np.zeros(n, dtype=np.int32),
+                    info={"lbox": (L, L, lz), "seed": seed})
+
+
 def bidisperse_settling(n=4_000_000, seed=1004, width=200.0, ratio=3.0, number_ratio=20,
                         e=0.7, mu=0.5, dt=5e-5, gravity=1.0, headroom=20.0, method_order=4,
                         euler_intervals=100, max_ncell=1 << 30, precision=P.PREC_FP64,

@@ -379,6 +379,101 @@ __device__ __forceinline__ bool overlap_rect(const DevParams& P, const dem_wall&
   return ov;
 }
 
+// Wij of Overlap (src/MConfig.f90:797-819): the unit radial direction of the
+// particle from the cone axis.  For a particle exactly on the axis (AlphaW =
+// 0) the reference draws a random unit vector; here the coordinate axis
+// least aligned with U, made orthogonal to U, is taken instead (the oracle
+// does the same).
+__device__ __forceinline__ void cone_radial(const double RijW[3], double AlphaW, const double U[3],
+                                            double W[3]) {
+  if (AlphaW == 0.0) {
+    int k0 = 0;
+    for (int k = 1; k < 3; k++)
+      if (fabs(U[k]) < fabs(U[k0])) k0 = k;
+    double e[3] = {0.0, 0.0, 0.0};
+    e[k0] = 1.0;
+    const double WdotU = dot3(e, U);
+#pragma unroll
+    for (int k = 0; k < 3; k++) W[k] = e[k] - WdotU * U[k];
+    const double nn = sqrt(sumsq3(W));
+#pragma unroll
+    for (int k = 0; k < 3; k++) W[k] = W[k] / nn;
+  } else {
+#pragma unroll
+    for (int k = 0; k < 3; k++) W[k] = RijW[k] / AlphaW;
+  }
+}
+
+// Overlap (src/MConfig.f90:692-822): Rectangle and Cone (conic frustum with
+// half length L1 along U, radii L2 and L3 at its two ends; the auxiliary
+// quantities of ConfigureWalls, src/MConfig.f90:661-684, for radius Ri).
+__device__ __forceinline__ bool overlap_wall(const DevParams& P, const dem_wall& w,
+                                             const double x[3], double Ri, double& Dij,
+                                             double Nij[3], double Qji[3]) {
+  if (w.shape == DEM_WALL_RECTANGLE) return overlap_rect(P, w, x, Ri, Dij, Nij, Qji);
+  if (w.shape != DEM_WALL_CONE) return false;
+  double Rij[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    Rij[k] = w.position[k] - x[k];
+    if (P.pbc[k]) Rij[k] = Rij[k] - P.lbox[k] * fnint(Rij[k] * P.inv_lbox[k]);
+  }
+  const double L_2 = w.l1, L = 2.0 * L_2, Ra = w.l2, Rp = w.l3;
+  const double Aux = sqrt(L * L + (Rp - Ra) * (Rp - Ra));
+  const double Rap = Aux, SinTheta = L / Aux, CosTheta = (Rp - Ra) / Aux;
+  const double MaxAlphaU = L_2 + Ri;
+  double mn = (Ra < Rp ? Ra : Rp) - Ri;
+  mn = 0.0 > mn ? 0.0 : mn;
+  const double MinAlphaWSq = mn * mn;
+  const double mx = (Ra > Rp ? Ra : Rp) + Ri;
+  const double MaxAlphaWSq = mx * mx;
+  const double AlphaU = dot3(Rij, w.u);
+  bool ov = fabs(AlphaU) < MaxAlphaU;
+  if (!ov) return false;
+  double RijW[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) RijW[k] = Rij[k] - AlphaU * w.u[k];
+  const double AlphaWSq = sumsq3(RijW);
+  ov = (AlphaWSq >= MinAlphaWSq) && (AlphaWSq < MaxAlphaWSq);
+  if (!ov) return false;
+  const double AlphaW = sqrt(AlphaWSq);
+  const double Lby2_AlphaU = w.l1 - AlphaU;
+  const double Ra_AlphaW = w.l2 - AlphaW;
+  double Lambda = Lby2_AlphaU * SinTheta - Ra_AlphaW * CosTheta;
+  double W[3];
+  cone_radial(RijW, AlphaW, w.u, W);
+  if (Lambda >= 0.0 && Lambda <= Rap) {
+    const double SignedDij = -(Lby2_AlphaU * CosTheta + Ra_AlphaW * SinTheta);
+    Dij = fabs(SignedDij);
+    ov = Dij < Ri;
+    if (ov) {
+#pragma unroll
+      for (int k = 0; k < 3; k++) Nij[k] = SinTheta * W[k] + CosTheta * w.u[k];
+#pragma unroll
+      for (int k = 0; k < 3; k++) Qji[k] = SignedDij * Nij[k] - Rij[k];
+#pragma unroll
+      for (int k = 0; k < 3; k++) Nij[k] = (Qji[k] + Rij[k]) / Dij;
+    }
+  } else {
+    const double t = Lambda < Rap ? Lambda : Rap;
+    Lambda = 0.0 > t ? 0.0 : t;
+    const double a = SinTheta * Lambda - Lby2_AlphaU;
+    const double b = CosTheta * Lambda + Ra_AlphaW;
+#pragma unroll
+    for (int k = 0; k < 3; k++) Nij[k] = a * w.u[k] - b * W[k];
+    const double DijSq = sumsq3(Nij);
+    ov = DijSq < Ri * Ri;
+    if (ov) {
+      Dij = sqrt(DijSq);
+#pragma unroll
+      for (int k = 0; k < 3; k++) Qji[k] = Nij[k] - Rij[k];
+#pragma unroll
+      for (int k = 0; k < 3; k++) Nij[k] = Nij[k] / Dij;
+    }
+  }
+  return ov;
+}
+
 // System parameters of particle p (or of cell c with a cell->system map).
 __device__ __forceinline__ const DevParams& sys_params(const DevParams* T, const int* sid, int i) {
   return T[sid ? sid[i] : 0];

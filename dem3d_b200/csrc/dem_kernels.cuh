@@ -987,7 +987,7 @@ __global__ void __launch_bounds__(128, MINB) k_pass_fp64(
       }
       double Dij, Nij[3], Qji[3];
       bool ov = false;
-      if (W.shape == DEM_WALL_RECTANGLE) ov = overlap_rect(P, W, xp, Rp, Dij, Nij, Qji);
+      ov = overlap_wall(P, W, xp, Rp, Dij, Nij, Qji);
       if (ov) {
         n_wc++;
         const double Delta = Rp * Rp - Dij * Dij;

@@ -744,7 +744,8 @@ int build_system(const dem_params* p, DevParams& h) {
   if (p->precision != DEM_PREC_FP64 && p->precision != DEM_PREC_MIXED) return DEM_ERR_INVALID;
   if (p->precision == DEM_PREC_MIXED && !mixed_available()) return DEM_ERR_UNSUPPORTED;
   for (int w = 0; w < p->n_walls; w++)
-    if (p->walls[w].shape != DEM_WALL_RECTANGLE) return DEM_ERR_UNSUPPORTED;
+    if (p->walls[w].shape != DEM_WALL_RECTANGLE && p->walls[w].shape != DEM_WALL_CONE)
+      return DEM_ERR_UNSUPPORTED;
   h = DevParams{};
   h.nc = p->n_components;
   h.nw = p->n_walls;

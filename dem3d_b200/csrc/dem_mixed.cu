@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(128, MINB) k_pass_mixed(
       if (contacting) rec_read(V.rwa, V.rwb, V.rwc, wi, ft0, ft0lo, vt0);
       double Dij, Nij[3], Qji[3];
       bool ov = false;
-      if (W.shape == DEM_WALL_RECTANGLE) ov = overlap_rect(P, W, xp, Rpd, Dij, Nij, Qji);
+      ov = overlap_wall(P, W, xp, Rpd, Dij, Nij, Qji);
       if (ov) {
         n_wc++;
         const double Delta = Rpd * Rpd - Dij * Dij;

@@ -28,7 +28,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from ._abi import (MAX_COMPONENTS, MAX_WALLS, PREC_FP64, PREC_MIXED,  # noqa: F401
-                   WALL_RECTANGLE, DemParams, DemWall)
+                   WALL_CONE, WALL_RECTANGLE, DemParams, DemWall)
 
 PI = 3.141592653589793238  # the reference's literal (src/DEM.f90:249)
 
@@ -93,6 +93,16 @@ def rectangle(center, half_u: float, half_w: float, u=(1.0, 0.0, 0.0), w=(0.0, 1
               stiffness: float = 1.0, shear_stiffness: float = 1.0) -> Wall:
     """A flat rectangular wall centred at ``center`` spanning +-half_u, +-half_w."""
     return Wall(WALL_RECTANGLE, 2.0 * half_u, 2.0 * half_w, 0.0, stiffness, shear_stiffness,
+                tuple(center), tuple(u), tuple(w))
+
+
+def cone(center, length: float, diameter_a: float, diameter_p: float, u=(0.0, 0.0, 1.0),
+         w=(1.0, 0.0, 0.0), stiffness: float = 1.0, shear_stiffness: float = 1.0) -> Wall:
+    """A conic frustum wall (Overlap's Cone branch, src/MConfig.f90:751-793):
+    axis ``u`` through ``center``, ``length`` along it, end diameters
+    ``diameter_a`` (at the -u end) and ``diameter_p`` (at the +u end), as an
+    input file gives them (halved on conversion)."""
+    return Wall(WALL_CONE, length, diameter_a, diameter_p, stiffness, shear_stiffness,
                 tuple(center), tuple(u), tuple(w))
 
 

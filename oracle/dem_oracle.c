@@ -614,7 +614,27 @@ static void common_calculations(orc_ctx* c, const double* Rij, double Kn, double
   for (int k = 0; k < 3; k++) c->iTorque[k] = c->iTorque[k] + tq[k];
 }
 
-/* Overlap, Rectangle branch, src/MConfig.f90:692-749 */
+/* Wij of Overlap (src/MConfig.f90:797-819); on the axis (AlphaW = 0) the
+ * reference draws a random unit vector: here the coordinate axis least
+ * aligned with U, made orthogonal to U (the library does the same). */
+static void cone_radial(const double RijW[3], double AlphaW, const double U[3], double W[3]) {
+  if (AlphaW == 0.0) {
+    int k0 = 0;
+    for (int k = 1; k < 3; k++)
+      if (fabs(U[k]) < fabs(U[k0])) k0 = k;
+    double e[3] = {0.0, 0.0, 0.0};
+    e[k0] = 1.0;
+    double WdotU = dot3(e, U);
+    for (int k = 0; k < 3; k++) W[k] = e[k] - WdotU * U[k];
+    double nn = sqrt(sumsq3(W));
+    for (int k = 0; k < 3; k++) W[k] = W[k] / nn;
+  } else {
+    for (int k = 0; k < 3; k++) W[k] = RijW[k] / AlphaW;
+  }
+}
+
+/* Overlap, src/MConfig.f90:692-822: Rectangle (:717-749) and Cone (:751-793,
+ * with the auxiliary quantities of ConfigureWalls, :661-684, for radius Ri) */
 static int overlap_wall(const orc_ctx* c, const OParticle* ip, const dem_wall* w,
                         double Ri, double* Dij, double* Nij, double* Qji) {
   double Rij[3];
@@ -651,6 +671,55 @@ static int overlap_wall(const orc_ctx* c, const OParticle* ip, const dem_wall* w
           ov = DijSq < Ri * Ri;
           if (ov) {
             *Dij = sqrt(DijSq);
+            for (int k = 0; k < 3; k++) Nij[k] = Nij[k] / *Dij;
+          }
+        }
+      }
+    }
+  } else if (w->shape == DEM_WALL_CONE) {
+    double L_2 = w->l1, L = 2.0 * L_2, Ra = w->l2, Rp = w->l3;
+    double Aux = sqrt(L * L + (Rp - Ra) * (Rp - Ra));
+    double Rap = Aux, SinTheta = L / Aux, CosTheta = (Rp - Ra) / Aux;
+    double MaxAlphaU = L_2 + Ri;
+    double mn = (Ra < Rp ? Ra : Rp) - Ri;
+    mn = 0.0 > mn ? 0.0 : mn;
+    double MinAlphaWSq = mn * mn;
+    double mx = (Ra > Rp ? Ra : Rp) + Ri;
+    double MaxAlphaWSq = mx * mx;
+    double AlphaU = dot3(Rij, w->u);
+    ov = fabs(AlphaU) < MaxAlphaU;
+    if (ov) {
+      double RijW[3];
+      for (int k = 0; k < 3; k++) RijW[k] = Rij[k] - AlphaU * w->u[k];
+      double AlphaWSq = sumsq3(RijW);
+      ov = (AlphaWSq >= MinAlphaWSq) && (AlphaWSq < MaxAlphaWSq);
+      if (ov) {
+        double AlphaW = sqrt(AlphaWSq);
+        double Lby2_AlphaU = w->l1 - AlphaU;
+        double Ra_AlphaW = w->l2 - AlphaW;
+        double Lambda = Lby2_AlphaU * SinTheta - Ra_AlphaW * CosTheta;
+        double W[3];
+        cone_radial(RijW, AlphaW, w->u, W);
+        if (Lambda >= 0.0 && Lambda <= Rap) {
+          double SignedDij = -(Lby2_AlphaU * CosTheta + Ra_AlphaW * SinTheta);
+          *Dij = fabs(SignedDij);
+          ov = *Dij < Ri;
+          if (ov) {
+            for (int k = 0; k < 3; k++) Nij[k] = SinTheta * W[k] + CosTheta * w->u[k];
+            for (int k = 0; k < 3; k++) Qji[k] = SignedDij * Nij[k] - Rij[k];
+            for (int k = 0; k < 3; k++) Nij[k] = (Qji[k] + Rij[k]) / *Dij;
+          }
+        } else {
+          double t = Lambda < Rap ? Lambda : Rap;
+          Lambda = 0.0 > t ? 0.0 : t;
+          double a = SinTheta * Lambda - Lby2_AlphaU;
+          double b = CosTheta * Lambda + Ra_AlphaW;
+          for (int k = 0; k < 3; k++) Nij[k] = a * w->u[k] - b * W[k];
+          double DijSq = sumsq3(Nij);
+          ov = DijSq < Ri * Ri;
+          if (ov) {
+            *Dij = sqrt(DijSq);
+            for (int k = 0; k < 3; k++) Qji[k] = Nij[k] - Rij[k];
             for (int k = 0; k < 3; k++) Nij[k] = Nij[k] / *Dij;
           }
         }
@@ -884,7 +953,8 @@ int orc_create(const dem_params* p, orc_ctx** out) {
   if (p->n_components < 0 || p->n_components > NCM) return DEM_ERR_INVALID;
   if (p->euler_intervals < 1) return DEM_ERR_INVALID;
   for (int w = 0; w < p->n_walls; w++)
-    if (p->walls[w].shape != DEM_WALL_RECTANGLE) return DEM_ERR_UNSUPPORTED;
+    if (p->walls[w].shape != DEM_WALL_RECTANGLE && p->walls[w].shape != DEM_WALL_CONE)
+      return DEM_ERR_UNSUPPORTED;
   orc_ctx* c = (orc_ctx*)calloc(1, sizeof(orc_ctx));
   c->p = *p;
   for (int k = 0; k < 3; k++) c->inv_lbox[k] = 1.0 / p->lbox[k];

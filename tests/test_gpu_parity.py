@@ -215,3 +215,17 @@ def test_bidisperse_walls_bit_exact():
     assert_same_contacts(g, o, "bidisperse")
     assert_same_cells(g, o, "bidisperse")
     assert g.ncol() == o.ncol()
+
+
+def test_cone_hopper_bit_exact():
+    """Spheres falling into a conic hopper (Cone wall + floor): wall contacts
+    through Overlap's Cone branch (src/MConfig.f90:751-793)."""
+    w = configs.hopper(n=600, seed=1005)
+    g, o = make_pair(w)
+    for s in (g, o):
+        s.run(1, 800)
+    assert_same_state(g, o, "hopper")
+    assert_same_contacts(g, o, "hopper")
+    assert g.ncol() == o.ncol()
+    cw = g.get_contacts()
+    assert np.count_nonzero(cw["iw"] == 0) > 0  # the cone is touched

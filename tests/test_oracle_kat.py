@@ -160,3 +160,40 @@ def test_rectangle_wall_geometry(where, expect_overlap):
         assert np.allclose(a / prm.comp_inv_mass[0], f, rtol=1e-12, atol=1e-9)
     else:
         assert np.all(a == 0.0)
+
+
+@pytest.mark.parametrize("s_ax, r, expect_overlap", [
+    (0.0, 3.2, True),     # inside, against the slanted face
+    (-5.2, 2.1, True),    # beyond the narrow end, against its rim
+    (5.3, 5.2, True),     # beyond the wide end, against its rim
+    (0.0, 1.0, False),    # near the axis
+    (6.0, 1.0, False),    # past the end, far from the rim
+])
+def test_cone_wall_geometry(s_ax, r, expect_overlap):
+    """Overlap's Cone branch (src/MConfig.f90:751-793): a resting sphere feels
+    the elastic force kn*(R - d) along the line from the closest point of the
+    frustum's generatrix segment (axial -5 -> radius 2, +5 -> radius 5)."""
+    cone = P.cone((0.0, 0.0, 0.0), 10.0, 4.0, 10.0, stiffness=2 * KN, shear_stiffness=2 * KT)
+    prm, _ = P.component_params([P.Component(1, 1.0, DENSITY, 2 * KN, 2 * KT)], [cone], [[0.8]],
+                                [[0.8]], [[0.5]], [[0.8]], [[0.8]], [[0.5]],
+                                lbox=(30.0, 30.0, 30.0), pbc=(False, False, False),
+                                gravity=(0, 0, 0), time_step=1e-4)
+    s = oracle_system(prm)
+    where = np.array([r, 0.0, s_ax])  # axis z, radial direction x
+    s.set_state(where[None, :], np.zeros((1, 3)), np.zeros((1, 3)), comp=np.zeros(1, np.int32))
+    s.initialize_cell_distribution()
+    s.compute_accelerations(update=True)
+    a = s.get_state()["acc"][0]
+    A, B, Pt = np.array([-5.0, 2.0]), np.array([5.0, 5.0]), np.array([s_ax, r])
+    t = np.clip(np.dot(Pt - A, B - A) / np.dot(B - A, B - A), 0.0, 1.0)
+    C = A + t * (B - A)
+    q = np.array([C[1], 0.0, C[0]])
+    d = where - q
+    dist = np.linalg.norm(d)
+    if expect_overlap:
+        assert dist < 0.5
+        f = prm.knw[0] * (0.5 - dist) * d / dist
+        assert np.allclose(a / prm.comp_inv_mass[0], f, rtol=1e-12, atol=1e-9)
+    else:
+        assert dist > 0.5
+        assert np.all(a == 0.0)
