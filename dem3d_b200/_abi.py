@@ -69,6 +69,15 @@ class DemParams(C.Structure):
     ]
 
 
+class DemWallMotion(C.Structure):
+    """TWallMovement (src/MDEM.f90:39-45): harmonic motion of one wall."""
+
+    _fields_ = [
+        ("constant_factor", _d3), ("amplitude", _d3), ("velocity_amplitude", _d3),
+        ("two_pi_frequency", _d3), ("phase_angle", _d3),
+    ]
+
+
 class DemObservables(C.Structure):
     _fields_ = [
         ("kinetic_energy", C.c_double), ("potential_energy", C.c_double),
@@ -110,6 +119,8 @@ SIGNATURES = {
     "get_ncol": (C.c_int, [_P, _I64P]),
     "get_escaped": (C.c_int, [_P, _I64P]),
     "get_observables": (C.c_int, [_P, C.POINTER(DemObservables)]),
+    "set_wall_motion": (C.c_int, [_P, C.POINTER(DemWallMotion)]),
+    "get_walls": (C.c_int, [_P, C.POINTER(DemWall)]),
 }
 
 # entry points only the CUDA library has

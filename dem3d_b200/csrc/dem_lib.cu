@@ -6,6 +6,7 @@
 // instrumentation used by the benchmark.
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -77,6 +78,13 @@ struct dem_ctx {
   double4* X[2] = {nullptr, nullptr};
   void* v4[2] = {nullptr, nullptr};
   void* w2[2] = {nullptr, nullptr};
+  // moving walls (WallsInMovement): MoveWalls is evaluated on the host; in a
+  // captured chunk the walls of step k come from pinned slot k, which the
+  // host fills before every replay
+  std::vector<dem_wall_motion> wm;
+  dem_wall* wall_slots = nullptr;  // pinned, [5][NWM]: 4 chunk slots + staging
+  bool capturing = false;
+  bool walls_moved = false;  // MoveWalls has run at least once (at `time`)
   int pass_variant = 0;  // pass kernel compiled for 4 (0) or 3 (1) blocks per SM
   double skin_factor = 0.05;  // candidate-row skin / CutOff
   int par = 0;         // L.cell[par] is the assignment the lists hold
@@ -626,6 +634,60 @@ int force_pass(dem_ctx* c, int side, bool update, double dt, int epi, const Ring
   return DEM_OK;
 }
 
+// MoveWalls (src/MDEM.f90:392-408) at Time, into walls[0:NW) of system 0.
+void move_walls_host(const dem_ctx* c, double Time, dem_wall* walls) {
+  const double Pi = 3.1415926535897932384626433832795;  // src/MUtil.f90
+  const double TwoPi = 2.0 * Pi;
+  for (size_t j = 0; j < c->wm.size(); j++) {
+    const dem_wall_motion& m = c->wm[j];
+    for (int k = 0; k < 3; k++) {
+      double Phase = m.two_pi_frequency[k] * Time + m.phase_angle[k];
+      Phase = Phase - TwoPi * (double)(int)(Phase / TwoPi);
+      walls[j].position[k] = m.constant_factor[k] + m.amplitude[k] * cos(Phase);
+      walls[j].velocity[k] = m.velocity_amplitude[k] * sin(Phase);
+    }
+  }
+}
+
+// if (WallsInMovement) call MoveWalls(Time): the walls at c->time into the
+// device table (from slot k of the chunk while a chunk is being captured).
+int apply_walls(dem_ctx* c, int k) {
+  if (c->wm.empty()) return DEM_OK;
+  const size_t nb = sizeof(dem_wall) * c->wm.size();
+  dem_wall* dst = reinterpret_cast<dem_wall*>(reinterpret_cast<char*>(c->dp) +
+                                              offsetof(DevParams, walls));  // system 0
+  c->walls_moved = true;
+  if (c->capturing) {
+    CK(cudaMemcpyAsync(dst, c->wall_slots + (size_t)k * NWM, nb, cudaMemcpyHostToDevice,
+                       c->stream));
+    return DEM_OK;
+  }
+  dem_wall* w = c->wall_slots + (size_t)4 * NWM;  // staging, not a chunk slot
+  CK(cudaStreamSynchronize(c->stream));  // the previous upload has been read
+  for (size_t j = 0; j < c->wm.size(); j++) w[j] = c->hsys[0].walls[j];
+  move_walls_host(c, c->time, w);
+  CK(cudaMemcpyAsync(dst, w, nb, cudaMemcpyHostToDevice, c->stream));
+  return DEM_OK;
+}
+
+// the host copy of system 0's walls follows the device one (before any
+// upload of the parameter table, and for dem_get_walls)
+void sync_host_walls(dem_ctx* c) {
+  if (c->wm.empty() || !c->walls_moved) return;
+  move_walls_host(c, c->time, c->hsys[0].walls);
+  c->hp = c->hsys[0];
+}
+
+// the walls of the G steps of the chunk that starts at `step` into the slots
+void fill_wall_slots(dem_ctx* c, int step, int G) {
+  if (c->wm.empty()) return;
+  for (int k = 0; k < G; k++) {
+    dem_wall* w = c->wall_slots + (size_t)k * NWM;
+    for (size_t j = 0; j < c->wm.size(); j++) w[j] = c->hsys[0].walls[j];
+    move_walls_host(c, (double)(step + k) * c->params.time_step, w);
+  }
+}
+
 int validate_ready(dem_ctx* c) {
   if (!c->state_set) return fail(c, DEM_ERR_STATE, "no particle state set");
   if (!c->cells_ready)
@@ -642,6 +704,8 @@ int move_particles_impl(dem_ctx* c, int step, bool check, int k) {
   if (st) return st;
   rotate_ring(c);
   c->time = (double)step * c->params.time_step;
+  st = apply_walls(c, k);
+  if (st) return st;
   rm = current_map(c);
   // force pass @ prediction, history read only, AM corrector
   return force_pass(c, 1, false, c->params.time_step, EPI_CORRECT, rm, check, 2 * k + 1);
@@ -665,6 +729,8 @@ int move_particles_euler_impl(dem_ctx* c) {
            (const Counters*)c->cnt);
     c->prepared = -1;
     c->time = c->time + dt;
+    st = apply_walls(c, 0);
+    if (st) return st;
   }
   launch(c, "apply_pbc", k_apply_pbc, blocks_for(n, 256), 256, (const DevParams*)c->dp,
          (const int*)c->sysid, n, c->P,
@@ -688,7 +754,9 @@ int capture_steps(dem_ctx* c, int steps, cudaGraphExec_t* out) {
   const double t = c->time;
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
   int st = DEM_OK;
+  c->capturing = true;
   for (int k = 0; k < steps && !st; k++) st = move_particles_impl(c, 0, false, k);
+  c->capturing = false;
   cudaError_t e = cudaStreamEndCapture(c->stream, &g);
   c->prof = prof;
   c->graph_kernels = c->launches - l0;
@@ -981,6 +1049,7 @@ int dem_set_system_counts(dem_ctx* c, const int32_t* counts) {
     if (off >= (1LL << 30)) return fail(c, DEM_ERR_INVALID, "too many particles");
   }
   c->counts.assign(counts, counts + c->nsys);
+  sync_host_walls(c);
   c->hp = c->hsys[0];
   CK(cudaStreamSynchronize(c->stream));
   CK(cudaMemcpy(c->dp, c->hsys.data(), sizeof(DevParams) * (size_t)c->nsys,
@@ -994,6 +1063,7 @@ void dem_destroy(dem_ctx* c) {
   drop_graphs(c);
   free_state(c);
   cudaFree(c->dp);
+  if (c->wall_slots) cudaFreeHost(c->wall_slots);
   cudaFree(c->cellsys);
   cudaFree(c->cnt);
   if (c->hcnt) cudaFreeHost(c->hcnt);
@@ -1128,6 +1198,8 @@ int dem_set_state(dem_ctx* c, int32_t n, const int32_t* comp, const double* radi
   CK(cudaStreamSynchronize(c->stream));
   c->state_set = true;
   c->cells_ready = false;
+  sync_host_walls(c);  // walls keep their place; their motion restarts at Time = 0
+  c->walls_moved = false;
   c->time = 0.0;
   return DEM_OK;
 }
@@ -1534,6 +1606,7 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
       st = capture_steps(c, G, &c->graph[phase]);
       if (st) return st;
     }
+    fill_wall_slots(c, step, G);  // the previous replay has completed
     CK(cudaGraphLaunch(c->graph[phase], c->stream));
     c->launches += c->graph_kernels;
     st = read_counters(c);
@@ -1558,6 +1631,9 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
     step += done;
     c->time = (double)(step - 1) * dt;
     if (failed_pass >= 0) {
+      // the replay's later wall uploads ran: back to the walls of step-1
+      st = apply_walls(c, 0);
+      if (st) return st;
       // the failed step: its first pass ran up to the failure (relink done),
       // or its first pass completed and its second one failed
       c->par ^= 1;
@@ -1570,6 +1646,8 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
         c->hcur ^= 1;
         rotate_ring(c);
         c->time = (double)step * dt;
+        st = apply_walls(c, 0);
+        if (st) return st;
         rm = current_map(c);
         st = force_pass(c, 1, false, dt, EPI_CORRECT, rm, true, 1);
         if (st) return st;
@@ -1579,6 +1657,8 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
         c->hcur ^= 1;
         rotate_ring(c);
         c->time = (double)step * dt;
+        st = apply_walls(c, 0);
+        if (st) return st;
         c->par ^= 1;
         RingMap rm = current_map(c);
         st = finish_pass(c, 1, false, dt, EPI_CORRECT, rm, 1);
@@ -1618,6 +1698,37 @@ int dem_get_ncol(dem_ctx* c, int64_t* ncol) {
   // the last history-updating pass completed (no abort is pending after an
   // API call returns), so its count is part of Ncol
   *ncol = (int64_t)(c->hcnt->ncol + c->hcnt->ncol_pending);
+  return DEM_OK;
+}
+
+int dem_set_wall_motion(dem_ctx* c, const dem_wall_motion* motion) {
+  if (!c) return DEM_ERR_INVALID;
+  if (c->nsys > 1) return fail(c, DEM_ERR_UNSUPPORTED, "moving walls need a single-system context");
+  drop_graphs(c);
+  sync_host_walls(c);  // walls stay where the last motion left them
+  c->walls_moved = false;
+  if (!motion) {
+    c->wm.clear();
+    return DEM_OK;
+  }
+  const int nw = c->params.n_walls;
+  for (int j = 0; j < nw; j++)
+    for (int k = 0; k < 3; k++) {
+      const dem_wall_motion& m = motion[j];
+      if (!std::isfinite(m.constant_factor[k]) || !std::isfinite(m.amplitude[k]) ||
+          !std::isfinite(m.velocity_amplitude[k]) || !std::isfinite(m.two_pi_frequency[k]) ||
+          !std::isfinite(m.phase_angle[k]) || m.two_pi_frequency[k] < 0.0)
+        return fail(c, DEM_ERR_INVALID, "wall motion must be finite with frequency >= 0");
+    }
+  if (!c->wall_slots) CK(cudaMallocHost(&c->wall_slots, sizeof(dem_wall) * NWM * 5));
+  c->wm.assign(motion, motion + nw);
+  return DEM_OK;
+}
+
+int dem_get_walls(dem_ctx* c, dem_wall* walls) {
+  if (!c || !walls) return DEM_ERR_INVALID;
+  sync_host_walls(c);
+  for (int j = 0; j < c->params.n_walls; j++) walls[j] = c->hsys[0].walls[j];
   return DEM_OK;
 }
 
@@ -1729,6 +1840,7 @@ int dem_set_tuning(dem_ctx* c, double skin_factor, int32_t pass_variant) {
     return fail(c, DEM_ERR_INVALID, "skin factor must lie in (0, 0.5], variant in {0, 1}");
   CK(cudaStreamSynchronize(c->stream));
   if (skin_factor != c->skin_factor) {
+    sync_host_walls(c);
     for (DevParams& h : c->hsys) {
       h.vl_skin = skin_factor * h.cutoff;
       h.vl_thr = 0.4 * h.vl_skin;

@@ -106,6 +106,30 @@ def cone(center, length: float, diameter_a: float, diameter_p: float, u=(0.0, 0.
                 tuple(center), tuple(u), tuple(w))
 
 
+def wall_motion(position, amplitude, frequency, phase, scales: "Scales | None" = None) -> dict:
+    """WM(j) of a wall at ``position`` that oscillates with ``amplitude``,
+    ``frequency`` (>= 0) and phase fraction ``phase`` per axis, derived as the
+    input reader does (src/DEM.f90:719-733) and, with ``scales``, scaled like
+    ScaleVariables (src/DEM.f90:841-847).  The record for
+    :meth:`DEMSystem.set_wall_motion`."""
+    two_pi = 2.0 * PI
+    tpf = [two_pi * float(f) for f in frequency]
+    if any(f < 0.0 for f in frequency):
+        raise ValueError("wall frequencies cannot be negative")
+    ph = [two_pi * float(x) for x in phase]
+    amp = [float(a) for a in amplitude]
+    m = {"two_pi_frequency": tpf, "phase_angle": ph, "amplitude": amp,
+         "velocity_amplitude": [-f * a for f, a in zip(tpf, amp)],
+         "constant_factor": [float(x) - a * math.cos(q) for x, a, q in zip(position, amp, ph)]}
+    if scales is not None:
+        L, T = scales.length, scales.time
+        m["constant_factor"] = [x / L for x in m["constant_factor"]]
+        m["amplitude"] = [x / L for x in m["amplitude"]]
+        m["velocity_amplitude"] = [x * T / L for x in m["velocity_amplitude"]]
+        m["two_pi_frequency"] = [x * T for x in m["two_pi_frequency"]]
+    return m
+
+
 @dataclass
 class Component:
     number: int

@@ -15,6 +15,9 @@ DEMSystem method                   reference routine
 ``move_particles``                  MoveParticles (src/MDEM.f90:285)
 ``move_particles_euler``            MoveParticlesEuler (src/MDEM.f90:258)
 ``run``                             main loop, src/DEM.f90:85-99
+``set_wall_motion``                 WallsInMovement + WM(:) (MoveWalls,
+                                    src/MDEM.f90:392, is called by the steps)
+``walls``                           Wall(1:NW)%Position, %Velocity
 ``kinetic_energy`` etc.             KineticEnergy/PotentialEnergy
                                     (src/MDEM.f90:183-213)
 =================================  ==========================================
@@ -28,7 +31,7 @@ import ctypes as C
 import numpy as np
 
 from . import _abi
-from ._abi import DemObservables, DemParams
+from ._abi import MAX_WALLS, DemObservables, DemParams, DemWall, DemWallMotion
 
 
 class DEMError(RuntimeError):
@@ -245,6 +248,27 @@ class DEMSystem:
         v = C.c_int64()
         self._call("get_escaped", C.byref(v))
         return v.value
+
+    # -- moving walls -----------------------------------------------------
+    def set_wall_motion(self, motions):
+        """WallsInMovement with WM(1:NW) = ``motions`` (dicts with the fields
+        of :class:`DemWallMotion`), or ``None`` to stop the walls."""
+        if motions is None:
+            self._call("set_wall_motion", None)
+            return
+        arr = (DemWallMotion * max(len(motions), 1))()
+        for j, m in enumerate(motions):
+            for key, val in m.items():
+                getattr(arr[j], key)[:] = [float(x) for x in val]
+        self._call("set_wall_motion", arr)
+
+    def walls(self):
+        """Position and velocity of every wall, as the last step left them."""
+        out = (DemWall * MAX_WALLS)()
+        self._call("get_walls", out)
+        nw = self.params.n_walls
+        return {"position": np.array([list(out[j].position) for j in range(nw)]),
+                "velocity": np.array([list(out[j].velocity) for j in range(nw)])}
 
     def observables(self):
         o = DemObservables()

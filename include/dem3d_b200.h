@@ -122,6 +122,18 @@ typedef struct dem_observables {
   int64_t n_wall_contacts;
 } dem_observables;
 
+/* TWallMovement (src/MDEM.f90:39-45) of one wall, in reduced units (as
+ * after ScaleVariables, src/DEM.f90:841-847): position = constant_factor +
+ * amplitude*cos(phase), velocity = velocity_amplitude*sin(phase), phase =
+ * two_pi_frequency*Time + phase_angle (per component). */
+typedef struct dem_wall_motion {
+  double constant_factor[3];
+  double amplitude[3];
+  double velocity_amplitude[3];
+  double two_pi_frequency[3];
+  double phase_angle[3];
+} dem_wall_motion;
+
 typedef struct dem_ctx dem_ctx;
 
 /* Library build/version string (also proves the .so loads). */
@@ -220,6 +232,15 @@ int dem_run(dem_ctx* ctx, int32_t first_step, int32_t last_step);
 /* dem_run bracketed by CUDA events on the context's stream; device_ms is the
  * elapsed device time (host synchronisation gaps between replays included). */
 int dem_run_timed(dem_ctx* ctx, int32_t first_step, int32_t last_step, double* device_ms);
+
+/* WallsInMovement = YES with WM(1:NW) (src/DEM.f90:714-733): after every
+ * Euler sub-step and after every predictor the library evaluates MoveWalls
+ * (src/MDEM.f90:392-408) on the host (so positions match a CPU build bit for
+ * bit) and moves every wall.  motion: NW records, or NULL to stop moving
+ * them.  Contexts with one system only. */
+int dem_set_wall_motion(dem_ctx* ctx, const dem_wall_motion* motion);
+/* Wall(1:NW) as the last pass saw them (system 0). */
+int dem_get_walls(dem_ctx* ctx, dem_wall* walls);
 
 /* Ncol (src/MForces.f90:47,227). */
 int dem_get_ncol(dem_ctx* ctx, int64_t* ncol);

@@ -112,6 +112,8 @@ typedef struct orc_ctx {
   int Contacting;
   int64_t ncol;
   double wall_fn[NWM];
+  int moving;               /* WallsInMovement */
+  dem_wall_motion wm[NWM];  /* WM(j) */
   char err[256];
 } orc_ctx;
 
@@ -869,6 +871,21 @@ static int euler(orc_ctx* c, double TimeStep) {
   return DEM_OK;
 }
 
+/* MoveWalls, src/MDEM.f90:392-408 (Pi as in src/MUtil.f90) */
+static void move_walls(orc_ctx* c, double Time) {
+  const double Pi = 3.1415926535897932384626433832795;
+  const double TwoPi = 2.0 * Pi;
+  for (int32_t j = 0; j < c->p.n_walls; j++) {
+    const dem_wall_motion* m = &c->wm[j];
+    for (int k = 0; k < 3; k++) {
+      double Phase = m->two_pi_frequency[k] * Time + m->phase_angle[k];
+      Phase = Phase - TwoPi * (double)(int)(Phase / TwoPi);
+      c->p.walls[j].position[k] = m->constant_factor[k] + m->amplitude[k] * cos(Phase);
+      c->p.walls[j].velocity[k] = m->velocity_amplitude[k] * sin(Phase);
+    }
+  }
+}
+
 /* MoveParticlesEuler, src/MDEM.f90:258-281 */
 static int move_particles_euler(orc_ctx* c) {
   double NewTimeStep = c->p.time_step / (double)c->p.euler_intervals;
@@ -885,6 +902,7 @@ static int move_particles_euler(orc_ctx* c) {
     int st = euler(c, NewTimeStep);
     if (st) return st;
     c->time = c->time + NewTimeStep;
+    if (c->moving) move_walls(c, c->time);
   }
   apply_pbc_particles(c, c->part);
   return DEM_OK;
@@ -920,6 +938,7 @@ static int move_particles(orc_ctx* c, int32_t step) {
     }
   }
   c->time = (double)step * c->p.time_step;
+  if (c->moving) move_walls(c, c->time);
   st = compute_accelerations(c, c->pred, c->p.time_step, 0);
   if (st) return st;
   for (int32_t i = 0; i < c->n; i++) {
@@ -1110,6 +1129,20 @@ int orc_get_predicted(orc_ctx* c, double* pos, double* vel, double* omega, doubl
 }
 
 int orc_get_n(orc_ctx* c, int32_t* n) { *n = c->n; return DEM_OK; }
+
+int orc_set_wall_motion(orc_ctx* c, const dem_wall_motion* m) {
+  if (!c) return DEM_ERR_INVALID;
+  if (!m) { c->moving = 0; return DEM_OK; }
+  for (int32_t j = 0; j < c->p.n_walls; j++) c->wm[j] = m[j];
+  c->moving = 1;
+  return DEM_OK;
+}
+
+int orc_get_walls(orc_ctx* c, dem_wall* walls) {
+  if (!c || !walls) return DEM_ERR_INVALID;
+  for (int32_t j = 0; j < c->p.n_walls; j++) walls[j] = c->p.walls[j];
+  return DEM_OK;
+}
 
 int orc_set_integration(orc_ctx* c, const double* previous, const int32_t* ipc) {
   for (int k = 0; k < c->nprev; k++) {

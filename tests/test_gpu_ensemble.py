@@ -75,3 +75,11 @@ def test_ensemble_rejects_mismatched_integrators():
     e.params[1].time_step = e.params[0].time_step * 2
     with pytest.raises(Exception):
         DEMSystem.ensemble(e.params, e.counts)
+
+
+def test_ensemble_rejects_moving_walls():
+    e = small_ensemble(P.PREC_FP64)
+    s = DEMSystem.ensemble(e.params, e.counts)
+    with pytest.raises(Exception):
+        s.set_wall_motion([P.wall_motion((0, 0, 0), (0, 0, 0.1), (0, 0, 1.0), (0, 0, 0))])
+    s.close()

@@ -229,3 +229,68 @@ def test_cone_hopper_bit_exact():
     assert g.ncol() == o.ncol()
     cw = g.get_contacts()
     assert np.count_nonzero(cw["iw"] == 0) > 0  # the cone is touched
+
+
+def _vibration(w):
+    # the cone shakes sideways and vertically, the floor vertically; over 800
+    # steps of 1e-4 the phases pass 2*pi (the phase reduction of MoveWalls)
+    cone, floor = w.params.walls[0], w.params.walls[1]
+    return [configs.P.wall_motion(list(cone.position), (0.01, 0.0, 0.03), (5.0, 0.0, 25.0),
+                                  (0.25, 0.0, 0.6)),
+            configs.P.wall_motion(list(floor.position), (0.0, 0.0, 0.02), (0.0, 0.0, 20.0),
+                                  (0.0, 0.0, 0.1))]
+
+
+def assert_same_walls(g, o, what=""):
+    a, b = g.walls(), o.walls()
+    for k in a:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=f"{what} walls.{k}")
+
+
+def test_vibrating_hopper_bit_exact():
+    """WallsInMovement: MoveWalls after every Euler sub-step and before every
+    corrector; graph replays read each step's walls from pinned slots."""
+    w = configs.hopper(n=600, seed=1005)
+    g, o = make_pair(w)
+    for s in (g, o):
+        s.set_wall_motion(_vibration(w))
+        s.run(1, 800)
+    assert_same_state(g, o, "vibrating hopper")
+    assert_same_contacts(g, o, "vibrating hopper")
+    assert_same_walls(g, o, "vibrating hopper")
+    assert g.ncol() == o.ncol()
+    cw = g.get_contacts()
+    assert np.count_nonzero(cw["iw"] == 0) > 0
+    # the motion really moved the walls
+    assert g.walls()["position"][1][2] != w.params.walls[1].position[2]
+
+
+def test_moving_walls_with_table_growth_and_stepwise():
+    """Aborted replays (history tables growing from one record) restore the
+    walls of the failed step; stepwise calls give the same trajectory."""
+    w = configs.hopper(n=400, seed=1008, euler_intervals=10)
+    w.params.hist_capacity = 1
+    g, o = make_pair(w)
+    g2 = DEMSystem(w.params)
+    g2.set_state(w.pos, w.vel, w.omega, comp=w.comp, radius=w.radius)
+    g2.initialize_cell_distribution()
+    for s in (g, o, g2):
+        s.set_wall_motion(_vibration(w))
+    g.run(1, 403)
+    o.run(1, 403)
+    g2.run(1, 4)
+    for step in range(5, 404):
+        g2.move_particles(step)
+    assert g.pass_stats()["hist_capacity"] > 1
+    assert_same_state(g, o, "grown, moving")
+    assert_same_contacts(g, o, "grown, moving")
+    assert_same_walls(g, o, "grown, moving")
+    assert_same_state(g2, o, "stepwise, moving")
+    assert_same_walls(g2, o, "stepwise, moving")
+    assert g.ncol() == o.ncol() == g2.ncol()
+    # stopping: the walls stay where the last step left them
+    for s in (g, o):
+        s.set_wall_motion(None)
+        s.run(404, 420)
+    assert_same_state(g, o, "stopped")
+    assert_same_walls(g, o, "stopped")
