@@ -112,11 +112,13 @@ SIGNATURES = {
     "initialize_cell_distribution": (C.c_int, [_P]),
     "get_grid": (C.c_int, [_P, _I32P]),
     "get_cells": (C.c_int, [_P, _I32P, _I32P, _I32P]),
+    "set_cells": (C.c_int, [_P, _I32P, _I32P]),
     "compute_accelerations": (C.c_int, [_P, C.c_int32, C.c_double, C.c_int32]),
     "move_particles": (C.c_int, [_P, C.c_int32]),
     "move_particles_euler": (C.c_int, [_P]),
     "run": (C.c_int, [_P, C.c_int32, C.c_int32]),
     "get_ncol": (C.c_int, [_P, _I64P]),
+    "set_ncol": (C.c_int, [_P, C.c_int64]),
     "get_escaped": (C.c_int, [_P, _I64P]),
     "get_observables": (C.c_int, [_P, C.POINTER(DemObservables)]),
     "set_wall_motion": (C.c_int, [_P, C.POINTER(DemWallMotion)]),

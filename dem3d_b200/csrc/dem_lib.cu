@@ -1520,6 +1520,60 @@ int dem_get_cells(dem_ctx* c, int32_t* cell_index, int32_t* traversal, int32_t* 
   return DEM_OK;
 }
 
+// ReadCellDistribution (src/MForces.f90:121-131): CellIndex from the
+// positions, then the lists as stored (ReadCellStructure, src/MCells.f90:
+// 988-1026), so that a resumed run walks the cells in the order the saved run
+// would have.  The lists must hold every particle once, in its own cell.
+int dem_set_cells(dem_ctx* c, const int32_t* traversal, const int32_t* cell_start) {
+  if (!c || !traversal || !cell_start) return DEM_ERR_INVALID;
+  if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
+  const int n = c->n, ncell = c->ncell_total;
+  if (cell_start[0] != 0 || cell_start[ncell] != n)
+    return fail(c, DEM_ERR_INVALID, "cell_start must run from 0 to n");
+  drop_graphs(c);
+  c->cells_ready = false;
+  int st = init_cells(c);  // CellIndex, flags and counters as a fresh distribution
+  if (st) return st;
+  std::vector<int> cell((size_t)std::max(n, 1));
+  if (n > 0)
+    CK(cudaMemcpyAsync(cell.data(), c->L.cell[c->par], sizeof(int) * n, cudaMemcpyDeviceToHost,
+                       c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  std::vector<int> head((size_t)ncell, -1), next((size_t)std::max(n, 1), -1);
+  std::vector<char> seen((size_t)std::max(n, 1), 0);
+  for (int cc = 0; cc < ncell; cc++) {
+    const int a = cell_start[cc], b = cell_start[cc + 1];
+    if (b < a) return fail(c, DEM_ERR_INVALID, "cell_start decreases");
+    for (int k = a; k < b; k++) {
+      const int q = traversal[k];
+      if (q < 0 || q >= n || seen[(size_t)q] || cell[(size_t)q] != cc)
+        return fail(c, DEM_ERR_INVALID, "cell lists must hold every particle once, in its cell");
+      seen[(size_t)q] = 1;
+      next[(size_t)q] = k + 1 < b ? traversal[k + 1] : -1;
+    }
+    if (b > a) head[(size_t)cc] = traversal[a];
+  }
+  CK(cudaMemcpyAsync(c->L.head, head.data(), sizeof(int) * (size_t)ncell, cudaMemcpyHostToDevice,
+                     c->stream));
+  if (n > 0)
+    CK(cudaMemcpyAsync(c->L.next, next.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice,
+                       c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->cells_ready = true;
+  return DEM_OK;
+}
+
+// Ncol as read from a state file (ReadState, src/DEM.f90:1109)
+int dem_set_ncol(dem_ctx* c, int64_t ncol) {
+  if (!c || ncol < 0) return DEM_ERR_INVALID;
+  CK(cudaStreamSynchronize(c->stream));
+  const unsigned long long v[2] = {(unsigned long long)ncol, 0ull};  // ncol, ncol_pending
+  CK(cudaMemcpy(&c->cnt->ncol, v, sizeof(v), cudaMemcpyHostToDevice));
+  c->hcnt->ncol = v[0];
+  c->hcnt->ncol_pending = 0;
+  return DEM_OK;
+}
+
 int dem_compute_accelerations(dem_ctx* c, int32_t use_predicted, double time_step,
                               int32_t update) {
   if (!c) return DEM_ERR_INVALID;

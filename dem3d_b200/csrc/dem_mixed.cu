@@ -233,12 +233,6 @@ __device__ __forceinline__ void rec_write(float4* a, float4* b, float* c, size_t
   c[i] = lo.z;
 }
 
-__device__ __forceinline__ unsigned long long wsum(unsigned long long v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  return v;
-}
-
 // The mixed-precision pass kernel: the FP64 kernel's structure (candidate
 // rows, exact FP64 overlap test, orientation, history semantics, summation
 // order), FP32 contact arithmetic, FP64 integrator epilogue.

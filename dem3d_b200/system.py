@@ -134,6 +134,8 @@ class DEMSystem:
         self._call("set_state", n, _iptr(c), _dptr(r), _dptr(p), _dptr(v), _dptr(w), _dptr(a),
                    _dptr(al))
         self.n = n
+        # Particle%Index - 1, kept for state files (it does not change in a run)
+        self.comp = np.zeros(n, np.int32) if c is None else c.copy()
         self._keep = None
 
     def update_state(self, pos=None, vel=None, omega=None, acc=None, alpha=None):
@@ -218,6 +220,12 @@ class DEMSystem:
         self._call("get_cells", _iptr(ci), _iptr(tr), _iptr(cs))
         return ci, tr, cs
 
+    def set_cells(self, traversal, cell_start):
+        """ReadCellDistribution: the cell lists as saved (list order per cell)."""
+        tr = np.ascontiguousarray(traversal, dtype=np.int32)
+        cs = np.ascontiguousarray(cell_start, dtype=np.int32)
+        self._call("set_cells", _iptr(tr), _iptr(cs))
+
     # -- dynamics ---------------------------------------------------------
     def compute_accelerations(self, use_predicted=False, time_step=None, update=True):
         ts = float(self.params.time_step if time_step is None else time_step)
@@ -243,6 +251,9 @@ class DEMSystem:
         v = C.c_int64()
         self._call("get_ncol", C.byref(v))
         return v.value
+
+    def set_ncol(self, ncol: int) -> None:
+        self._call("set_ncol", int(ncol))
 
     def escaped(self):
         v = C.c_int64()

@@ -214,6 +214,12 @@ int dem_get_grid(dem_ctx* ctx, int32_t* nxyz);
  * cell_start[ncell+1]. */
 int dem_get_cells(dem_ctx* ctx, int32_t* cell_index, int32_t* traversal,
                   int32_t* cell_start);
+/* ReadCellDistribution (src/MForces.f90:121-131, ReadCellStructure
+ * src/MCells.f90:988-1026): CellIndex from the positions and the cell lists
+ * as saved (the layout dem_get_cells returns), instead of a fresh
+ * distribution.  Every particle must appear once, in the cell its position
+ * hashes to (DEM_ERR_INVALID otherwise). */
+int dem_set_cells(dem_ctx* ctx, const int32_t* traversal, const int32_t* cell_start);
 
 /* ComputeAccelerations(Particle or Predicted, NP, TimeStep, Update)
  * (src/MForces.f90:145-335), including RedistributeParticles3D. */
@@ -244,6 +250,8 @@ int dem_get_walls(dem_ctx* ctx, dem_wall* walls);
 
 /* Ncol (src/MForces.f90:47,227). */
 int dem_get_ncol(dem_ctx* ctx, int64_t* ncol);
+/* Ncol read back from a state file (ReadState, src/DEM.f90:1109). */
+int dem_set_ncol(dem_ctx* ctx, int64_t ncol);
 /* Particles that left the box (UpdateParticleList test src/MDEM.f90:624-625)
  * after the last corrector; removal itself is not done by this library. */
 int dem_get_escaped(dem_ctx* ctx, int64_t* count);

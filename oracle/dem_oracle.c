@@ -1252,6 +1252,40 @@ int orc_get_cells(orc_ctx* c, int32_t* cell_index, int32_t* traversal, int32_t* 
   return DEM_OK;
 }
 
+/* ReadCellDistribution (src/MForces.f90:121-131): CellIndex from the
+ * positions, then the lists as stored (ReadCellStructure, src/MCells.f90:
+ * 988-1026).  The lists must hold every particle once, in its own cell. */
+int orc_set_cells(orc_ctx* c, const int32_t* traversal, const int32_t* cell_start) {
+  if (!c || !traversal || !cell_start) return DEM_ERR_INVALID;
+  if (cell_start[0] != 0 || cell_start[c->Nt] != c->n) return DEM_ERR_INVALID;
+  for (int32_t i = 0; i < c->n; i++)
+    c->cell_index[i] = current_cell(c, c->part[i].pos[0], c->part[i].pos[1], c->part[i].pos[2]);
+  char* seen = (char*)calloc((size_t)(c->n > 0 ? c->n : 1), 1);
+  int bad = 0;
+  for (int32_t cc = 0; cc < c->Nt && !bad; cc++) {
+    if (cell_start[cc + 1] < cell_start[cc]) { bad = 1; break; }
+    for (int32_t k = cell_start[cc]; k < cell_start[cc + 1]; k++) {
+      int32_t q = traversal[k];
+      if (q < 0 || q >= c->n || seen[q] || c->cell_index[q] != cc) { bad = 1; break; }
+      seen[q] = 1;
+    }
+  }
+  free(seen);
+  if (bad) return DEM_ERR_INVALID;
+  clear_cell_particles(c);
+  for (int32_t cc = 0; cc < c->Nt; cc++)
+    for (int32_t k = cell_start[cc + 1] - 1; k >= cell_start[cc]; k--)
+      add_particle(c, traversal[k], cc);  /* prepending in reverse keeps the order */
+  c->cells_ready = 1;
+  return DEM_OK;
+}
+
+int orc_set_ncol(orc_ctx* c, int64_t ncol) {
+  if (!c || ncol < 0) return DEM_ERR_INVALID;
+  c->ncol = ncol;
+  return DEM_OK;
+}
+
 int orc_compute_accelerations(orc_ctx* c, int32_t use_predicted, double time_step,
                               int32_t update) {
   if (!c->cells_ready) return DEM_ERR_STATE;
