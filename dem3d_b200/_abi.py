@@ -119,6 +119,10 @@ SIGNATURES = {
     "run": (C.c_int, [_P, C.c_int32, C.c_int32]),
     "get_ncol": (C.c_int, [_P, _I64P]),
     "set_ncol": (C.c_int, [_P, C.c_int64]),
+    "update_particle_list": (C.c_int, [_P, _I64P]),
+    "set_particle_removal": (C.c_int, [_P, C.c_int32]),
+    "get_components": (C.c_int, [_P, _I32P]),
+    "get_removal_stats": (C.c_int, [_P, _I64P]),
     "get_escaped": (C.c_int, [_P, _I64P]),
     "get_observables": (C.c_int, [_P, C.POINTER(DemObservables)]),
     "set_wall_motion": (C.c_int, [_P, C.POINTER(DemWallMotion)]),

@@ -95,6 +95,92 @@ def settling(n=2000, seed=1000, layer_side=10, dt=1e-4, e=0.8, mu=0.5, gravity=1
                     info={"lbox": (L, L, lz), "seed": seed})
 
 
+def draining_column(n=600, seed=1013, layer_side=8, dt=5e-4, e=0.7, mu=0.5, gravity=10.0,
+                    v_down=10.0, sigma_v=0.5, headroom=2.0, method_order=4, euler_intervals=10,
+                    max_ncell=30000, precision=P.PREC_FP64):
+    """A column of spheres (d = 1) falling out of the bottom of a box with no
+    floor: ``layer_side`` x ``layer_side`` per layer at spacing 1, periodic in
+    x/y, layers touching (z jitter U(+-0.01)), moving down at ``v_down``.
+    Particles leave through z = -lz/2 layer after layer, in contact with the
+    layer above, which exercises UpdateParticleList.  Indices grow from the
+    top layer to the bottom one and are shuffled within each layer, so the
+    last particle often sits next to the one that leaves."""
+    rng = np.random.default_rng(seed)
+    per_layer = layer_side * layer_side
+    n_layers = (n + per_layer - 1) // per_layer
+    lz = float(n_layers) + headroom
+    L = float(layer_side)
+    pos = np.empty((n, 3))
+    k = 0
+    for layer in range(n_layers):  # top layer first
+        sx, sy = rng.uniform(-0.05, 0.05, size=2)
+        z0 = 0.5 * lz - 0.5 - 1.0 * layer - 0.5 * headroom
+        order = rng.permutation(per_layer)
+        for site in order:
+            if k >= n:
+                break
+            ix, iy = site % layer_side, site // layer_side
+            pos[k] = (-0.5 * L + 0.5 + ix + sx, -0.5 * L + 0.5 + iy + sy,
+                      z0 + rng.uniform(-0.01, 0.01))
+            k += 1
+    vel = rng.normal(0.0, sigma_v, size=(n, 3))
+    vel[:, 2] -= v_down
+    comp = np.zeros(n, dtype=np.int32)
+    prm, _ = P.component_params(
+        [P.Component(n, 1.0, DENSITY, 2.0 * KN, 2.0 * KT)], [], [[e]], [[e]], [[mu]],
+        [], [], [], lbox=(L, L, lz), pbc=(True, True, False), gravity=(0.0, 0.0, -gravity),
+        time_step=dt, method_order=method_order, euler_intervals=euler_intervals,
+        max_ncell=max_ncell, precision=precision)
+    return Workload("draining_column", prm, pos, vel, np.zeros((n, 3)), comp=comp,
+                    info={"lbox": (L, L, lz), "seed": seed})
+
+
+def discharge(n=360, seed=1014, e=0.7, mu=0.5, dt=4e-4, gravity=20.0, v_down=6.0,
+              sigma_v=0.3, length=10.0, d_out=3.0, d_in=14.0, method_order=4,
+              euler_intervals=10, max_ncell=30000, precision=P.PREC_FP64):
+    """A conic hopper (Cone wall, axis z, opening ``d_out`` at the bottom)
+    emptying out of a box with no floor: the box ends 0.6 below the outlet,
+    so the spheres (d = 1) that pass the outlet leave the box while still
+    touching the ones above.  The spheres fill the cone from the outlet up on
+    a lattice of spacing 1.02, moving down at ``v_down``; indices grow from
+    the top layer down and are shuffled within each layer, so the last
+    particle usually sits near the outlet too."""
+    rng = np.random.default_rng(seed)
+    L = d_in + 4.0
+    lz = 2.0 * (0.5 * length + 0.6)
+    a = 1.02
+    layers = []
+    z = -0.5 * length + 0.6
+    total = 0
+    while total < n:
+        if z > 0.5 * length - 0.5:
+            raise ValueError("the cone holds fewer spheres")
+        r_z = 0.5 * d_out + (z + 0.5 * length) / length * 0.5 * (d_in - d_out)
+        m = int(r_z / a) + 1
+        pts = [(ix * a, iy * a, z) for iy in range(-m, m + 1) for ix in range(-m, m + 1)
+               if math.hypot(ix * a, iy * a) < r_z - 0.6]
+        layers.append(pts)
+        total += len(pts)
+        z += a
+    pos = []
+    for pts in reversed(layers):  # top layer first
+        for k in rng.permutation(len(pts)):
+            if len(pos) < n:
+                pos.append(pts[k])
+    pos = np.asarray(pos) + rng.uniform(-0.005, 0.005, size=(n, 3))
+    vel = rng.normal(0.0, sigma_v, size=(n, 3))
+    vel[:, 2] -= v_down
+    cone = P.cone((0.0, 0.0, 0.0), length, d_out, d_in, stiffness=2.0 * KN,
+                  shear_stiffness=2.0 * KT)
+    prm, _ = P.component_params(
+        [P.Component(n, 1.0, DENSITY, 2.0 * KN, 2.0 * KT)], [cone], [[e]], [[e]], [[mu]],
+        [[e]], [[e]], [[mu]], lbox=(L, L, lz), pbc=(False, False, False),
+        gravity=(0.0, 0.0, -gravity), time_step=dt, method_order=method_order,
+        euler_intervals=euler_intervals, max_ncell=max_ncell, precision=precision)
+    return Workload("discharge", prm, pos, vel, np.zeros((n, 3)), comp=np.zeros(n, dtype=np.int32),
+                    info={"lbox": (L, L, lz), "seed": seed})
+
+
 def hopper(n=600, seed=1005, e=0.7, mu=0.5, dt=1e-4, gravity=1.0, length=10.0, d_out=3.0,
            d_in=14.0, method_order=4, euler_intervals=20, precision=P.PREC_FP64,
            sigma_v=1.0, v_radial=3.0, max_ncell=30000):

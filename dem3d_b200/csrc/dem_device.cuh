@@ -93,6 +93,7 @@ struct Counters {
   unsigned int disp_max;  // FP32 bits (rounded up) of the largest displacement of one pass
   double disp_acc;   // sum of disp_max since the last full rebuild
   double wall_fn[NWM];
+  int escape_stop;   // a captured chunk stopped before a step: particles had left the box
 };
 
 // Contact history, one table per buffer: records owned by imin, stored slot

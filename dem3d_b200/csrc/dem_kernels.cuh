@@ -490,8 +490,19 @@ __global__ void __launch_bounds__(256) k_prepare(const DevParams* __restrict__ P
 // Thread 0 also closes the previous pass's bookkeeping and decides whether
 // this pass rebuilds every candidate row.
 __global__ void k_relink(const DevParams* __restrict__ PT, const int* __restrict__ cellsys,
-                         CellLists L, int par, int n, int update, Counters* cnt) {
+                         CellLists L, int par, int n, int update, int stop_tag, Counters* cnt) {
   if (cnt->abort) return;
+  // inside a captured chunk, particles that left the box in the last step
+  // stop the chunk before this step (the host runs UpdateParticleList); the
+  // count is final here (written by the previous kernel), so every block
+  // takes the same branch
+  if (stop_tag >= 0 && cnt->escaped != 0ull) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      cnt->escape_stop = 1;
+      set_abort(cnt, stop_tag);
+    }
+    return;
+  }
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   if (tid == 0) {
     const DevParams& P = PT[0];  // the integrator settings are shared
@@ -1045,11 +1056,13 @@ __global__ void __launch_bounds__(128, MINB) k_pass_fp64(
 
   if (valid) {
     // ---- records of pairs the sweep did not visit are kept as they were
+    // (a partner index past the last particle is a record that particle
+    // removal left behind: never visited)
     if (update) {
       const int nold = A.Hr.cnt[p];
       for (int r = 0; r < nold; r++) {
         const int q2 = A.Hr.key[hslot(A.Hr, p, r)];
-        if (!cells_adjacent(P, c, A.cell_cur[q2])) {
+        if (q2 >= A.n || !cells_adjacent(P, c, A.cell_cur[q2])) {
           double ft[3], vt[3];
           hist_read(A.Hr, p, r, ft, vt);
           record(q2, ft, vt);

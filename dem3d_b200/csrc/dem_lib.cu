@@ -14,6 +14,7 @@
 
 #include "dem_kernels.cuh"
 #include "dem_mixed.cuh"
+#include "dem_remove.cuh"
 
 using namespace dem;
 
@@ -85,6 +86,13 @@ struct dem_ctx {
   dem_wall* wall_slots = nullptr;  // pinned, [5][NWM]: 4 chunk slots + staging
   bool capturing = false;
   bool walls_moved = false;  // MoveWalls has run at least once (at `time`)
+  // UpdateParticleList after every step of dem_run (single-system contexts);
+  // captured chunks then stop before a step that follows escapes
+  bool removal = true;
+  bool stop_on_escape = false;
+  int* rm_buf = nullptr;  // escaped list + status words of the removal kernel
+  int rm_cap = 0;
+  long long rm_stats[3] = {0, 0, 0};  // removals, swaps, records renamed or moved
   int pass_variant = 0;  // pass kernel compiled for 4 (0) or 3 (1) blocks per SM
   double skin_factor = 0.05;  // candidate-row skin / CutOff
   int par = 0;         // L.cell[par] is the assignment the lists hold
@@ -519,8 +527,9 @@ void launch_screen(dem_ctx* c, int side, int tag) {
 // relink towards the prepared assignment, then the candidate rows
 void pass_lists(dem_ctx* c, int side, bool update, int tag) {
   const int b = c->par ^ 1;
+  const int stop_tag = c->capturing && c->stop_on_escape && update ? tag : -1;
   launch(c, "relink", k_relink, (unsigned)LIST_BLOCKS, 256, (const DevParams*)c->dp,
-         (const int*)c->cellsys, c->L, b, c->n, update ? 1 : 0, c->cnt);
+         (const int*)c->cellsys, c->L, b, c->n, update ? 1 : 0, stop_tag, c->cnt);
   c->par = b;
   launch_screen(c, side, tag);
 }
@@ -632,6 +641,106 @@ int force_pass(dem_ctx* c, int side, bool update, double dt, int epi, const Ring
   c->prepared = epi == EPI_PREDICT ? 1 : epi == EPI_CORRECT ? 0 : -1;
   if (update) c->hcur ^= 1;
   return DEM_OK;
+}
+
+// UpdateParticleList (src/MDEM.f90:612-671): the escaped particles are
+// listed by one grid-wide kernel, then removed by k_remove (one block, in
+// decreasing index).  A removal that would overflow the history tables asks
+// for capacity before it changes anything; the tables grow and the kernel
+// carries on.  Afterwards the ring and the tables are laid out for the new
+// particle count, and the next pass rebuilds every candidate row.
+int update_particle_list_impl(dem_ctx* c, int64_t* removed) {
+  if (removed) *removed = 0;
+  if (c->nsys > 1) return fail(c, DEM_ERR_UNSUPPORTED, "particle removal needs one system");
+  const int n0 = c->n;
+  if (n0 == 0) return DEM_OK;
+  CK(cudaStreamSynchronize(c->stream));
+  if (c->rm_cap < n0) {
+    cudaFree(c->rm_buf);
+    c->rm_buf = nullptr;
+    CK(cudaMalloc(&c->rm_buf, sizeof(int) * ((size_t)n0 + 16)));
+    c->rm_cap = n0;
+  }
+  int* state = c->rm_buf;      // 8 status words, then the list
+  int* list = c->rm_buf + 16;
+  int hs[8] = {n0, 0, 0, 0, 0, 0, 0, 0};  // [7]: escaped count
+  CK(cudaMemcpyAsync(state, hs, sizeof(hs), cudaMemcpyHostToDevice, c->stream));
+  launch(c, "escape_list", k_escape_list, blocks_for(n0, 256), 256, (const DevParams*)c->dp, n0,
+         c->P, list, state + 7);
+  CK(cudaMemcpyAsync(hs, state, sizeof(hs), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const int n_list = hs[7];
+  if (n_list > 0) {
+    for (int attempt = 0;; attempt++) {
+      RemovalArgs A;
+      A.PT = c->dp;
+      A.P = c->P;
+      A.radius = c->radius;
+      A.comp = c->comp;
+      A.ring = c->ring;
+      A.ring_slots = c->nprev + 1;
+      A.ring_stride = n0;
+      A.L = c->L;
+      A.par = c->par;
+      A.H = c->H[c->hcur];
+      const bool mixed = c->precision == DEM_PREC_MIXED;
+      A.ha = mixed ? c->M.ha[c->hcur] : nullptr;
+      A.hb = mixed ? c->M.hb[c->hcur] : nullptr;
+      A.hc = mixed ? c->M.hc[c->hcur] : nullptr;
+      A.wa = mixed ? c->M.wa[c->hcur] : nullptr;
+      A.wb = mixed ? c->M.wb[c->hcur] : nullptr;
+      A.wc = mixed ? c->M.wc[c->hcur] : nullptr;
+      A.nw = c->params.n_walls;
+      A.list = list;
+      A.n_list = n_list;
+      A.state = state;
+      launch(c, "remove", k_remove, 1u, (unsigned)RM_THREADS, A);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(hs, state, sizeof(hs), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      if (hs[1] == RM_OK) break;
+      if (hs[1] == RM_NEED_CAPACITY && attempt < 8) {
+        int st = grow_history(c, hs[2] + 2);  // same particle count: same layout
+        if (st) return st;
+        const int zero = 0;
+        CK(cudaMemcpyAsync(state + 1, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        continue;
+      }
+      if (hs[1] == RM_NB_OVERFLOW)
+        return fail(c, DEM_ERR_CAPACITY, "a removed particle's neighbourhood is too crowded");
+      return fail(c, DEM_ERR_STATE, "cell lists inconsistent during particle removal");
+    }
+  }
+  const int n1 = hs[0];
+  c->rm_stats[0] += hs[3];
+  c->rm_stats[1] += hs[4];
+  c->rm_stats[2] += hs[5];
+  if (n1 != n0) {
+    // the ring and the history tables laid out for n1 particles
+    const int slots9 = 9 * (c->nprev + 1);
+    double* nr = nullptr;
+    CK(cudaMalloc(&nr, sizeof(double) * (size_t)slots9 * (size_t)std::max(n1, 1)));
+    if (n1 > 0)
+      launch(c, "ring_restride", k_ring_restride, 592u, 256u, (const double*)c->ring, nr, slots9,
+             n0, n1);
+    CK(cudaStreamSynchronize(c->stream));
+    cudaFree(c->ring);
+    c->ring = nr;
+    c->n = n1;
+    int st = grow_history(c, c->hcap);
+    if (st) return st;
+  }
+  CK(cudaMemsetAsync(&c->cnt->escaped, 0, sizeof(unsigned long long), c->stream));
+  const int one = 1;
+  CK(cudaMemcpyAsync(&c->cnt->force_full, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  // the cell transition towards the current positions, for the new numbering
+  c->last_side = -1;
+  int st = prepare_side(c, 0);
+  if (st) return st;
+  drop_graphs(c);
+  if (removed) *removed = n0 - n1;
+  CK(cudaGetLastError());
+  return read_counters(c);
 }
 
 // MoveWalls (src/MDEM.f90:392-408) at Time, into walls[0:NW) of system 0.
@@ -999,6 +1108,7 @@ int dem_create_ensemble(const dem_params* ps, int32_t nsys, dem_ctx** out) {
   c->nprev = p->method_order - 1;
   c->hcap = p->hist_capacity > 0 ? p->hist_capacity : 16;
   c->nsys = nsys;
+  c->removal = nsys == 1;
   c->hsys = hs;
   c->hp = hs[0];
   c->ncell_total = (int)ncell;
@@ -1063,6 +1173,7 @@ void dem_destroy(dem_ctx* c) {
   drop_graphs(c);
   free_state(c);
   cudaFree(c->dp);
+  cudaFree(c->rm_buf);
   if (c->wall_slots) cudaFreeHost(c->wall_slots);
   cudaFree(c->cellsys);
   cudaFree(c->cnt);
@@ -1336,8 +1447,10 @@ int dem_set_contacts(dem_ctx* c, int64_t m, const int32_t* imin, const int32_t* 
   int nw = std::max(c->params.n_walls, 1);
   std::vector<int> cnt(N, 0);
   for (int64_t r = 0; r < m; r++) {
-    if (imin[r] < 0 || imin[r] >= imax[r] || imax[r] >= n)
-      return fail(c, DEM_ERR_INVALID, "bad pair record (need 0 <= imin < imax < n)");
+    // a partner past the last particle is a record that particle removal
+    // left behind (never looked up again); the owner must exist
+    if (imin[r] < 0 || imin[r] >= n || imin[r] >= imax[r])
+      return fail(c, DEM_ERR_INVALID, "bad pair record (need 0 <= imin < n, imin < imax)");
     cnt[imin[r]]++;
   }
   int need = 0;
@@ -1620,12 +1733,25 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
   int st = validate_ready(c);
   if (st) return st;
   int s0 = first_step;
+  // the main loop calls UpdateParticleList after every step (src/DEM.f90:96),
+  // the Euler start-up does not
+  const bool removal = c->removal && c->nsys == 1;
+  c->stop_on_escape = removal;
+  auto remove_escaped = [&]() -> int {
+    if (!removal) return DEM_OK;
+    int s = read_counters(c);
+    if (s) return s;
+    return c->hcnt->escaped ? update_particle_list_impl(c, nullptr) : DEM_OK;
+  };
   if (first_step == 1) {
     for (int s = 1; s <= c->params.method_order - 1; s++) {
       st = move_particles_euler_impl(c);
       if (st) return st;
     }
     s0 = c->params.method_order;
+  } else {
+    st = remove_escaped();  // escapes left by a step run through another call
+    if (st) return st;
   }
   int step = s0;
   const int G = 4;
@@ -1635,6 +1761,8 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
     int remaining = last_step - step + 1;
     if (remaining < G || c->prof) {
       st = move_particles_impl(c, step, true, 0);
+      if (st) return st;
+      st = remove_escaped();
       if (st) return st;
       step++;
       continue;
@@ -1666,13 +1794,16 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
     st = read_counters(c);
     if (st) return st;
     int done = G, failed_pass = -1;
+    bool escape_stop = false;
     if (c->hcnt->abort) {
       const int tag = c->hcnt->abort_tag - 1;  // 2*(step in chunk) + pass
       if (c->hcnt->nonfinite) return fail(c, DEM_ERR_STATE, "a particle position is not finite");
       if (c->hcnt->list_error) return fail(c, DEM_ERR_STATE, "cell lists inconsistent");
       if (tag < 0 || tag >= 2 * G) return fail(c, DEM_ERR_STATE, "bad abort tag");
       done = tag / 2;
-      failed_pass = tag % 2;
+      escape_stop = c->hcnt->escape_stop != 0;
+      // an escape stop happens before the step starts: nothing to finish
+      failed_pass = escape_stop ? -1 : tag % 2;
     }
     for (int k = 0; k < done; k++) {
       rotate_ring(c);
@@ -1684,6 +1815,16 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
     }
     step += done;
     c->time = (double)(step - 1) * dt;
+    if (escape_stop) {
+      // the replay's later wall copies ran: back to the walls of step-1
+      st = apply_walls(c, 0);
+      if (st) return st;
+      CK(cudaMemsetAsync(&c->cnt->abort, 0, 2 * sizeof(int), c->stream));  // abort, abort_tag
+      CK(cudaMemsetAsync(&c->cnt->escape_stop, 0, sizeof(int), c->stream));
+      st = update_particle_list_impl(c, nullptr);
+      if (st) return st;
+      continue;
+    }
     if (failed_pass >= 0) {
       // the replay's later wall uploads ran: back to the walls of step-1
       st = apply_walls(c, 0);
@@ -1722,6 +1863,8 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
       }
       step++;
     }
+    st = remove_escaped();  // escapes of the chunk's last step
+    if (st) return st;
   }
   CK(cudaGetLastError());
   return DEM_OK;
@@ -1752,6 +1895,36 @@ int dem_get_ncol(dem_ctx* c, int64_t* ncol) {
   // the last history-updating pass completed (no abort is pending after an
   // API call returns), so its count is part of Ncol
   *ncol = (int64_t)(c->hcnt->ncol + c->hcnt->ncol_pending);
+  return DEM_OK;
+}
+
+int dem_update_particle_list(dem_ctx* c, int64_t* removed) {
+  if (!c) return DEM_ERR_INVALID;
+  int st = validate_ready(c);
+  if (st) return st;
+  return update_particle_list_impl(c, removed);
+}
+
+int dem_set_particle_removal(dem_ctx* c, int32_t enable) {
+  if (!c) return DEM_ERR_INVALID;
+  if (enable && c->nsys > 1)
+    return fail(c, DEM_ERR_UNSUPPORTED, "particle removal needs a single-system context");
+  c->removal = enable != 0;
+  drop_graphs(c);
+  return DEM_OK;
+}
+
+int dem_get_components(dem_ctx* c, int32_t* comp) {
+  if (!c || !comp) return DEM_ERR_INVALID;
+  if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
+  CK(cudaStreamSynchronize(c->stream));
+  if (c->n > 0) CK(cudaMemcpy(comp, c->comp, sizeof(int) * (size_t)c->n, cudaMemcpyDeviceToHost));
+  return DEM_OK;
+}
+
+int dem_get_removal_stats(dem_ctx* c, int64_t* stats) {
+  if (!c || !stats) return DEM_ERR_INVALID;
+  for (int k = 0; k < 3; k++) stats[k] = c->rm_stats[k];
   return DEM_OK;
 }
 

@@ -431,7 +431,7 @@ __global__ void __launch_bounds__(128, MINB) k_pass_mixed(
       for (int r = 0; r < nold; r++) {
         const size_t i = hslot(Hr, p, r);
         const int q2 = Hr.key[i];
-        if (!cells_adjacent(P, c, A.cell_cur[q2])) {
+        if (q2 >= A.n || !cells_adjacent(P, c, A.cell_cur[q2])) {
           F3 ft, lo, vt;
           rec_read(V.ra, V.rb, V.rc, i, ft, lo, vt);
           record(q2, ft, lo, vt);
@@ -503,13 +503,14 @@ __global__ void k_hist_from_mixed(int n, History H, const float4* a, const float
   }
 }
 
-__global__ void k_mixed_regrow(int n, const int* cnt, int oldcap, int newcap, const float4* a,
-                               const float4* b, const float* c, float4* na, float4* nb,
-                               float* nc) {
+__global__ void k_mixed_regrow(int n, int ns, const int* cnt, const float4* a, const float4* b,
+                               const float* c, float4* na, float4* nb, float* nc) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   for (int r = 0; r < cnt[i]; r++) {
-    const size_t s = (size_t)r * n + i, d = s;  // slot-major: same index in both
+    // slot-major: record r of particle i at r*stride + i, the old tables laid
+    // out for ns particles, the new ones for n
+    const size_t s = (size_t)r * ns + i, d = (size_t)r * n + i;
     na[d] = a[s];
     nb[d] = b[s];
     nc[d] = c[s];
@@ -566,9 +567,8 @@ bool mixed_regrow(MixedBuffers& M, int n, int newcap, int cur, const History& ol
       return false;
   }
   if (n > 0)
-    k_mixed_regrow<<<blocks(n, 256), 256, 0, st>>>(n, old.cnt, old.cap, newcap, M.ha[cur],
-                                                    M.hb[cur], M.hc[cur], na[cur], nb[cur],
-                                                    nc[cur]);
+    k_mixed_regrow<<<blocks(n, 256), 256, 0, st>>>(n, old.n, old.cnt, M.ha[cur], M.hb[cur],
+                                                    M.hc[cur], na[cur], nb[cur], nc[cur]);
   cudaStreamSynchronize(st);
   for (int b = 0; b < 2; b++) {
     cudaFree(M.ha[b]);

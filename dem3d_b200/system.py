@@ -239,11 +239,13 @@ class DEMSystem:
 
     def run(self, first_step, last_step):
         self._call("run", int(first_step), int(last_step))
+        self._refresh_n()  # UpdateParticleList may have removed particles
 
     def run_timed(self, first_step, last_step):
         """dem_run with device-side CUDA-event timing; returns milliseconds."""
         ms = C.c_double()
         self._call("run_timed", int(first_step), int(last_step), C.byref(ms))
+        self._refresh_n()
         return ms.value
 
     # -- diagnostics ------------------------------------------------------
@@ -251,6 +253,33 @@ class DEMSystem:
         v = C.c_int64()
         self._call("get_ncol", C.byref(v))
         return v.value
+
+    # -- particle removal ---------------------------------------------------
+    def _refresh_n(self):
+        v = C.c_int32()
+        self._call("get_n", C.byref(v))
+        if v.value != self.n:
+            self.n = v.value
+            comp = np.zeros(self.n, np.int32)
+            if self.n:
+                self._call("get_components", _iptr(comp))
+            self.comp = comp
+
+    def update_particle_list(self) -> int:
+        """UpdateParticleList: remove the particles outside the box."""
+        v = C.c_int64()
+        self._call("update_particle_list", C.byref(v))
+        self._refresh_n()
+        return v.value
+
+    def set_particle_removal(self, on: bool) -> None:
+        """Whether ``run`` removes escaped particles after every step."""
+        self._call("set_particle_removal", 1 if on else 0)
+
+    def removal_stats(self):
+        s = (C.c_int64 * 3)()
+        self._call("get_removal_stats", s)
+        return {"removed": s[0], "swaps": s[1], "records_moved": s[2]}
 
     def set_ncol(self, ncol: int) -> None:
         self._call("set_ncol", int(ncol))

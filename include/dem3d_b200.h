@@ -194,7 +194,8 @@ int dem_get_integration(dem_ctx* ctx, double* previous, int32_t* ipc);
  * records (imin < imax) and wall records (particle, wall), Vector1 = ft
  * (previous tangential force), Vector2 = vt (previous tangential contact
  * velocity).  get_* returns them sorted by key like the reference's lists
- * (SaveContactList, src/MContacts.f90:75-117). */
+ * (SaveContactList, src/MContacts.f90:75-117).  imax may exceed n - 1: a
+ * record that particle removal left behind, as in the reference. */
 int dem_set_contacts(dem_ctx* ctx, int64_t m, const int32_t* imin,
                      const int32_t* imax, const double* ft, const double* vt,
                      int64_t mw, const int32_t* ip, const int32_t* iw,
@@ -247,6 +248,24 @@ int dem_run_timed(dem_ctx* ctx, int32_t first_step, int32_t last_step, double* d
 int dem_set_wall_motion(dem_ctx* ctx, const dem_wall_motion* motion);
 /* Wall(1:NW) as the last pass saw them (system 0). */
 int dem_get_walls(dem_ctx* ctx, dem_wall* walls);
+
+/* UpdateParticleList (src/MDEM.f90:612-671): every particle outside
+ * [-L/2, L/2] is removed, highest index first; the last particle takes its
+ * place (Particle, Previous, cell lists, contact records renamed as
+ * RemoveParticleFromContactList/ChangeIndexInContactList do,
+ * src/MContacts.f90:173-252, 579-633).  removed: how many left.  The
+ * particle count shrinks (dem_get_n); dem_get_components gives the new
+ * Particle%Index order.  Contexts with one system only. */
+int dem_update_particle_list(dem_ctx* ctx, int64_t* removed);
+/* Whether dem_run calls UpdateParticleList after every step, as the
+ * reference's main loop does (src/DEM.f90:94-98).  On by default for
+ * single-system contexts; off means escapes are only counted. */
+int dem_set_particle_removal(dem_ctx* ctx, int32_t enable);
+/* Particle%Index - 1 of every particle (changes when particles are removed). */
+int dem_get_components(dem_ctx* ctx, int32_t* comp);
+/* Removals so far: {particles removed, swaps with the last particle,
+ * contact records renamed or handed over}. */
+int dem_get_removal_stats(dem_ctx* ctx, int64_t* stats);
 
 /* Ncol (src/MForces.f90:47,227). */
 int dem_get_ncol(dem_ctx* ctx, int64_t* ncol);

@@ -79,6 +79,7 @@ typedef struct {
 typedef struct orc_ctx {
   dem_params p;
   int32_t n;
+  int32_t nalloc;  /* rows of the arrays (n shrinks when particles leave) */
   OParticle* part;
   OParticle* pred;
   OPrev* prev; /* [nprev][n] */
@@ -113,6 +114,8 @@ typedef struct orc_ctx {
   int64_t ncol;
   double wall_fn[NWM];
   int moving;               /* WallsInMovement */
+  int removal;              /* run() calls UpdateParticleList after each step */
+  int64_t removal_count, removal_swaps, removal_moved;  /* test diagnostics */
   dem_wall_motion wm[NWM];  /* WM(j) */
   char err[256];
 } orc_ctx;
@@ -845,7 +848,7 @@ static void apply_pbc_particles(orc_ctx* c, OParticle* P) {
 }
 
 static inline OPrev* prev_at(orc_ctx* c, int32_t slot1 /* 1-based */, int32_t i) {
-  return &c->prev[(size_t)(slot1 - 1) * (size_t)c->n + (size_t)i];
+  return &c->prev[(size_t)(slot1 - 1) * (size_t)c->nalloc + (size_t)i];
 }
 
 /* ipc = cshift(ipc, shift=-1) */
@@ -961,6 +964,202 @@ static int move_particles(orc_ctx* c, int32_t step) {
 }
 
 /* ------------------------------------------------------------------ */
+/* UpdateParticleList (src/MDEM.f90:612-671): particles that left the   */
+/* box are removed; the last particle takes the place of each one.      */
+
+/* AllNeighbourParticles (src/MCells.f90:833-860) over the MonteCarlo list
+ * of iCell (NeighbourCells3D with MonteCarlo, :353-375, AddAllNeighbours3D
+ * :424-476): the particles of iCell, then of each neighbour cell. */
+static int32_t all_neighbour_particles(orc_ctx* c, int32_t iCell, int32_t** out) {
+  int32_t iz = iCell / (c->Nx * c->Ny);
+  int32_t iy = iCell / c->Nx - iz * c->Ny;
+  int32_t ix = iCell - (iy + iz * c->Ny) * c->Nx;
+  const int pbc[3] = {c->p.pbc[0], c->p.pbc[1], c->p.pbc[2]};
+  const int32_t N[3] = {c->Nx, c->Ny, c->Nz};
+  const int32_t I[3] = {ix, iy, iz};
+  int32_t lo[3], hi[3];
+  for (int d = 0; d < 3; d++) { /* VerifyPBC, :1030-1040 */
+    lo[d] = -1;
+    hi[d] = 1;
+    if (!pbc[d]) {
+      if (I[d] == 0) lo[d] = 0;
+      if (I[d] == N[d] - 1) hi[d] = 0;
+    }
+  }
+  int32_t cells[27], m = 0;
+  cells[m++] = iCell;
+  for (int32_t kz = lo[2]; kz <= hi[2]; kz++)
+    for (int32_t ky = lo[1]; ky <= hi[1]; ky++)
+      for (int32_t kx = lo[0]; kx <= hi[0]; kx++) {
+        if (kx == 0 && ky == 0 && kz == 0) continue;
+        int32_t j[3] = {ix + kx, iy + ky, iz + kz};
+        for (int d = 0; d < 3; d++) /* ApplyPBC, :1044-1052 */
+          if (pbc[d]) {
+            if (j[d] == N[d]) j[d] = 0;
+            if (j[d] == -1) j[d] = N[d] - 1;
+          }
+        cells[m++] = j[0] + c->Nx * (j[1] + c->Ny * j[2]);
+      }
+  int32_t cnt = 0;
+  for (int k = 0; k < m; k++)
+    for (CNode* q = c->cell[cells[k]].first_particle; q; q = q->next) cnt++;
+  int32_t* nb = (int32_t*)malloc(sizeof(int32_t) * (size_t)(cnt > 0 ? cnt : 1));
+  cnt = 0;
+  for (int k = 0; k < m; k++)
+    for (CNode* q = c->cell[cells[k]].first_particle; q; q = q->next) nb[cnt++] = q->index;
+  *out = nb;
+  return cnt;
+}
+
+/* RemoveParticleFromCell (src/MCells.f90:702-724) */
+static void remove_particle_from_cell(orc_ctx* c, int32_t i, int32_t iCell) {
+  CNode* cur = c->cell[iCell].first_particle;
+  if (cur->index == i) {
+    c->cell[iCell].first_particle = cur->next;
+    free(cur);
+  } else {
+    while (cur->next->index != i) cur = cur->next;
+    CNode* aux = cur->next;
+    cur->next = aux->next;
+    free(aux);
+  }
+}
+
+/* ReplaceParticleIndexInCell (src/MCells.f90:728-743) */
+static void replace_particle_index_in_cell(orc_ctx* c, int32_t i, int32_t iCell, int32_t j) {
+  CNode* cur = c->cell[iCell].first_particle;
+  while (cur->index != i) cur = cur->next;
+  cur->index = j;
+}
+
+static void free_partners(Partner* p) {
+  while (p) { Partner* a = p; p = p->next; free(a); }
+}
+
+/* RemoveParticleFromContactList (src/MContacts.f90:579-633) */
+static void remove_particle_from_contact_list(orc_ctx* c, int32_t i, int32_t npsc,
+                                              const int32_t* nb) {
+  for (int32_t jj = 0; jj < npsc; jj++) {
+    int32_t j = nb[jj];
+    Partner* cur = c->mainp[j].first_partner;
+    if (!cur) continue;
+    Partner* prev = cur;
+    while (cur->index < i && cur->next) {
+      prev = cur;
+      cur = cur->next;
+    }
+    if (cur->index == i) {
+      if (prev->index == i) c->mainp[j].first_partner = cur->next;
+      else prev->next = cur->next;
+      free(cur);
+    }
+  }
+  free_partners(c->mainp[i].first_partner);
+  free_partners(c->mainp[i].first_wall);
+  c->mainp[i].first_partner = NULL;
+  c->mainp[i].first_wall = NULL;
+}
+
+/* ChangeIndexInContactList (src/MContacts.f90:173-252), NP -> i.  One
+ * deliberate deviation: the records that particle i inherits as main
+ * particle (partners j > i of NP) are inserted in index order, where the
+ * reference appends them in neighbour order (:225-241).  An appended list can
+ * be out of order, and the reference's ordered search (VerifyPairContact,
+ * src/MContacts.f90:329-372) then misses some of its records; keeping the
+ * list ordered keeps every record reachable. */
+static void change_index_in_contact_list(orc_ctx* c, int32_t NP, int32_t i, int32_t npsc,
+                                         const int32_t* nb, int64_t* moved) {
+  Partner* first = NULL;
+  for (int32_t jj = 0; jj < npsc; jj++) {
+    int32_t j = nb[jj];
+    Partner* cur = c->mainp[j].first_partner;
+    if (!cur) continue;
+    if (j < i) {
+      Partner *prev = NULL, *point = NULL;
+      while (cur->next) {
+        prev = cur;
+        if (cur->index < i) point = cur;
+        cur = cur->next;
+      }
+      if (cur->index == NP) {
+        (*moved)++;
+        if (prev) {
+          prev->next = cur->next;
+          cur->index = i;
+          if (point) {
+            cur->next = point->next;
+            point->next = cur;
+          } else {
+            cur->next = c->mainp[j].first_partner;
+            c->mainp[j].first_partner = cur;
+          }
+        } else {
+          cur->index = i;
+        }
+      }
+    } else {
+      Partner* prev = NULL;
+      while (cur->next) {
+        prev = cur;
+        cur = cur->next;
+      }
+      if (cur->index == NP) {
+        (*moved)++;
+        cur->index = j;
+        if (prev) prev->next = NULL;
+        else c->mainp[j].first_partner = NULL;
+        /* ordered insert into i's new list (see above) */
+        Partner** at = &first;
+        while (*at && (*at)->index < j) at = &(*at)->next;
+        cur->next = *at;
+        *at = cur;
+      }
+    }
+  }
+  c->mainp[i].first_partner = first;
+  c->mainp[i].first_wall = c->mainp[NP].first_wall;
+  c->mainp[NP].first_wall = NULL;
+  /* NP's own partner list is not carried over; it lies beyond the new NP */
+  free_partners(c->mainp[NP].first_partner);
+  c->mainp[NP].first_partner = NULL;
+}
+
+static int update_particle_list(orc_ctx* c, int64_t* removed) {
+  int64_t nrem = 0;
+  for (int32_t i = c->n - 1; i >= 0; i--) {
+    const OParticle* q = &c->part[i];
+    int out = 0;
+    for (int k = 0; k < 3; k++) {
+      const double h = 0.5 * c->p.lbox[k];
+      if (q->pos[k] > h || q->pos[k] < -h) out = 1;
+    }
+    if (!out) continue;
+    int32_t iCell = c->cell_index[i];
+    int32_t* nb = NULL;
+    int32_t npsc = all_neighbour_particles(c, iCell, &nb);
+    remove_particle_from_cell(c, i, iCell);
+    remove_particle_from_contact_list(c, i, npsc, nb);
+    int32_t NP = c->n - 1;
+    if (i != NP) {
+      c->part[i] = c->part[NP];
+      c->pred[i].index = c->part[NP].index;
+      c->pred[i].radius = c->part[NP].radius;
+      for (int32_t k = 1; k <= c->nprev; k++) *prev_at(c, k, i) = *prev_at(c, k, NP);
+      replace_particle_index_in_cell(c, NP, c->cell_index[NP], i);
+      c->cell_index[i] = c->cell_index[NP];
+      change_index_in_contact_list(c, NP, i, npsc, nb, &c->removal_moved);
+      c->removal_swaps++;
+    }
+    free(nb);
+    c->n = NP;
+    nrem++;
+  }
+  c->removal_count += nrem;
+  if (removed) *removed = nrem;
+  return DEM_OK;
+}
+
+/* ------------------------------------------------------------------ */
 /* public API (mirrors include/dem3d_b200.h with an orc_ prefix)        */
 
 const char* orc_last_error(const orc_ctx* c) { return c ? c->err : "null context"; }
@@ -975,6 +1174,7 @@ int orc_create(const dem_params* p, orc_ctx** out) {
     if (p->walls[w].shape != DEM_WALL_RECTANGLE && p->walls[w].shape != DEM_WALL_CONE)
       return DEM_ERR_UNSUPPORTED;
   orc_ctx* c = (orc_ctx*)calloc(1, sizeof(orc_ctx));
+  c->removal = 1; /* the main loop always calls UpdateParticleList (src/DEM.f90:96) */
   c->p = *p;
   for (int k = 0; k < 3; k++) c->inv_lbox[k] = 1.0 / p->lbox[k];
   /* InitializeAuxiliaries, src/MDEM.f90:110-162 */
@@ -1060,6 +1260,7 @@ int orc_set_state(orc_ctx* c, int32_t n, const int32_t* comp, const double* radi
   free(c->force);
   free(c->torque);
   c->n = n;
+  c->nalloc = n;
   size_t N = (size_t)(n > 0 ? n : 1);
   c->part = (OParticle*)calloc(N, sizeof(OParticle));
   c->pred = (OParticle*)calloc(N, sizeof(OParticle));
@@ -1148,7 +1349,7 @@ int orc_set_integration(orc_ctx* c, const double* previous, const int32_t* ipc) 
   for (int k = 0; k < c->nprev; k++) {
     c->ipc[k] = ipc[k];
     for (int32_t i = 0; i < c->n; i++) {
-      OPrev* pv = &c->prev[(size_t)k * c->n + i];
+      OPrev* pv = &c->prev[(size_t)k * c->nalloc + i];
       const double* s = previous + ((size_t)k * c->n + i) * 9;
       memcpy(pv->v, s, 24);
       memcpy(pv->a, s + 3, 24);
@@ -1163,7 +1364,7 @@ int orc_get_integration(orc_ctx* c, double* previous, int32_t* ipc) {
     if (ipc) ipc[k] = c->ipc[k];
     if (previous)
       for (int32_t i = 0; i < c->n; i++) {
-        const OPrev* pv = &c->prev[(size_t)k * c->n + i];
+        const OPrev* pv = &c->prev[(size_t)k * c->nalloc + i];
         double* d = previous + ((size_t)k * c->n + i) * 9;
         memcpy(d, pv->v, 24);
         memcpy(d + 3, pv->a, 24);
@@ -1178,7 +1379,8 @@ int orc_set_contacts(orc_ctx* c, int64_t m, const int32_t* imin, const int32_t* 
                      const int32_t* iw, const double* ftw, const double* vtw) {
   destroy_contacts(c);
   for (int64_t r = 0; r < m; r++) {
-    if (imin[r] < 0 || imin[r] >= imax[r] || imax[r] >= c->n) return DEM_ERR_INVALID;
+    /* a partner past the last particle is a record left by particle removal */
+    if (imin[r] < 0 || imin[r] >= c->n || imin[r] >= imax[r]) return DEM_ERR_INVALID;
     insert_sorted(&c->mainp[imin[r]].first_partner, imax[r], ft + 3 * r, vt + 3 * r);
   }
   for (int64_t r = 0; r < mw; r++) {
@@ -1280,6 +1482,31 @@ int orc_set_cells(orc_ctx* c, const int32_t* traversal, const int32_t* cell_star
   return DEM_OK;
 }
 
+int orc_update_particle_list(orc_ctx* c, int64_t* removed) {
+  if (!c || !c->cells_ready) return DEM_ERR_STATE;
+  return update_particle_list(c, removed);
+}
+
+int orc_set_particle_removal(orc_ctx* c, int32_t enable) {
+  if (!c) return DEM_ERR_INVALID;
+  c->removal = enable != 0;
+  return DEM_OK;
+}
+
+int orc_get_components(orc_ctx* c, int32_t* comp) {
+  if (!c || !comp) return DEM_ERR_INVALID;
+  for (int32_t i = 0; i < c->n; i++) comp[i] = c->part[i].index;
+  return DEM_OK;
+}
+
+/* test diagnostics: removals, swaps with the last particle, records renamed */
+int orc_get_removal_stats(orc_ctx* c, int64_t* stats) {
+  stats[0] = c->removal_count;
+  stats[1] = c->removal_swaps;
+  stats[2] = c->removal_moved;
+  return DEM_OK;
+}
+
 int orc_set_ncol(orc_ctx* c, int64_t ncol) {
   if (!c || ncol < 0) return DEM_ERR_INVALID;
   c->ncol = ncol;
@@ -1316,6 +1543,7 @@ int orc_run(orc_ctx* c, int32_t first_step, int32_t last_step) {
   for (int32_t s = s0; s <= last_step; s++) {
     int st = move_particles(c, s);
     if (st) return st;
+    if (c->removal) update_particle_list(c, NULL);
   }
   return DEM_OK;
 }

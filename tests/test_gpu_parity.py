@@ -169,10 +169,11 @@ def test_contacts_roundtrip_and_import():
 
 def test_escape_detection():
     """Particles outside +-L/2 after the corrector (UpdateParticleList's test,
-    src/MDEM.f90:624-625) are counted, not removed."""
+    src/MDEM.f90:624-625) are counted, not removed, when removal is off."""
     w = configs.settling(n=100, seed=9, headroom=2.0, sigma_v=30.0)
     g, o = make_pair(w)
     for s in (g, o):
+        s.set_particle_removal(False)
         s.run(1, 50)
     assert_same_state(g, o, "escape")
     st = o.get_state()
