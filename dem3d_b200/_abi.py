@@ -78,6 +78,27 @@ class DemWallMotion(C.Structure):
     ]
 
 
+POUR_RECTANGLE = 1
+POUR_CIRCLE = 2
+
+
+class DemPouring(C.Structure):
+    """Pouring settings (src/DEM.f90:745-800, src/MDEM.f90:412-532)."""
+
+    _fields_ = [
+        ("interval", C.c_int32), ("shape", C.c_int32), ("max_attempts", C.c_int32),
+        ("target_number", C.c_int32 * MAX_COMPONENTS), ("size", C.c_double * 2),
+        ("velocity_z", C.c_double),
+    ]
+
+
+class DemRng(C.Structure):
+    """ranf's state (src/MUtil.f90:10-11)."""
+
+    _fields_ = [("aam", C.c_double), ("dummy", C.c_int32), ("iix", C.c_int32),
+                ("iiy", C.c_int32), ("iik", C.c_int32)]
+
+
 class DemObservables(C.Structure):
     _fields_ = [
         ("kinetic_energy", C.c_double), ("potential_energy", C.c_double),
@@ -123,6 +144,10 @@ SIGNATURES = {
     "set_particle_removal": (C.c_int, [_P, C.c_int32]),
     "get_components": (C.c_int, [_P, _I32P]),
     "get_removal_stats": (C.c_int, [_P, _I64P]),
+    "set_pouring": (C.c_int, [_P, C.POINTER(DemPouring)]),
+    "pour_particle": (C.c_int, [_P, _I32P]),
+    "set_rng": (C.c_int, [_P, C.POINTER(DemRng)]),
+    "get_rng": (C.c_int, [_P, C.POINTER(DemRng)]),
     "get_escaped": (C.c_int, [_P, _I64P]),
     "get_observables": (C.c_int, [_P, C.POINTER(DemObservables)]),
     "set_wall_motion": (C.c_int, [_P, C.POINTER(DemWallMotion)]),

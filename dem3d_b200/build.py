@@ -23,7 +23,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relax
           "-Xptxas", "-warn-spills"]
 # dem_mixed.cu: FP32 contact arithmetic within a stated 1e-5 tolerance, so
 # division and square root may use the hardware approximations (~1 ulp)
-SOURCES = [("dem_lib.cu", ["-fmad=false"]),
+SOURCES = [("dem_lib.cu", ["-fmad=false", "-Xcompiler", "-ffp-contract=off"]),
            ("dem_mixed.cu", ["--prec-div=false", "--prec-sqrt=false"])]
 
 

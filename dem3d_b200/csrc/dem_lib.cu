@@ -5,6 +5,7 @@
 // CUDA-graph replay of whole steps, contact-history import/export and the
 // instrumentation used by the benchmark.
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstddef>
 #include <cstdio>
@@ -47,6 +48,8 @@ struct dem_ctx {
   int* cellsys = nullptr;  // [ncell_total] system of every cell (ensembles only)
   int* sysid = nullptr;    // [n] system of every particle (ensembles only)
   int n = 0;
+  int ncap = 0;       // rows allocated for every per-particle array (>= n)
+  int ncap_hint = 0;  // capacity the next dem_set_state allocates at least
   int nprev = 0;
   bool state_set = false;
   bool cells_ready = false;
@@ -90,6 +93,14 @@ struct dem_ctx {
   // captured chunks then stop before a step that follows escapes
   bool removal = true;
   bool stop_on_escape = false;
+  // pouring (PouringAttempt before every step of dem_run) and ranf's state
+  bool pouring = false;
+  dem_pouring pour{};
+  dem_rng rng{0.0, 0, -1, -1, 0};
+  std::vector<int> comp_count;  // Component(:)%Number
+  double2* pour_cand = nullptr;  // candidate points of one PourParticle call
+  int* pour_fits = nullptr;
+  int pour_cap = 0;
   int* rm_buf = nullptr;  // escaped list + status words of the removal kernel
   int rm_cap = 0;
   long long rm_stats[3] = {0, 0, 0};  // removals, swaps, records renamed or moved
@@ -310,8 +321,10 @@ void drop_graphs(dem_ctx* c) {
   c->graph_valid = false;
 }
 
+// tables laid out for the allocated capacity (record r of particle i at
+// r*ncap + i), so the particle count can change without moving records
 int alloc_history(dem_ctx* c, History& H, int cap) {
-  size_t n = (size_t)std::max(c->n, 1);
+  size_t n = (size_t)std::max(c->ncap, 1);
   int nw = std::max(c->params.n_walls, 1);
   H.cap = cap;
   H.n = (int)n;
@@ -337,13 +350,15 @@ int grow_history(dem_ctx* c, int need) {
   }
   History& cur = c->H[c->hcur];
   launch(c, "hist_regrow", k_hist_regrow, blocks_for(c->n, 256), 256, c->n, cur, nh[c->hcur]);
-  size_t n = (size_t)std::max(c->n, 1);
+  // wall records are particle major (i*nw + w): the first n rows move as they are
+  size_t n = (size_t)std::max(std::min(c->n, cur.n), 1);
   int nw = std::max(c->params.n_walls, 1);
   CK(cudaMemcpyAsync(nh[c->hcur].wflag, cur.wflag, n * nw * sizeof(int), cudaMemcpyDeviceToDevice,
                      c->stream));
   CK(cudaMemcpyAsync(nh[c->hcur].wval, cur.wval, n * nw * 3 * sizeof(double2),
                      cudaMemcpyDeviceToDevice, c->stream));
-  if (c->precision == DEM_PREC_MIXED && !mixed_regrow(c->M, c->n, cap, c->hcur, cur, c->stream))
+  if (c->precision == DEM_PREC_MIXED &&
+      !mixed_regrow(c->M, c->n, c->ncap, cap, c->hcur, cur, c->stream))
     return fail(c, DEM_ERR_CAPACITY, "mixed history regrow failed");
   CK(cudaStreamSynchronize(c->stream));
   for (int b = 0; b < 2; b++) {
@@ -356,6 +371,99 @@ int grow_history(dem_ctx* c, int need) {
   }
   c->hcap = cap;
   drop_graphs(c);
+  return DEM_OK;
+}
+
+StateArrays make_state(double* base, size_t n);
+
+// Room for `newcap` particles in every per-particle array (the values of the
+// current n particles are kept; the per-pass copies, the candidate rows and
+// the prepared cell transition are rebuilt by the next pass).
+int grow_capacity(dem_ctx* c, int newcap) {
+  if (newcap <= c->ncap) return DEM_OK;
+  CK(cudaStreamSynchronize(c->stream));
+  drop_graphs(c);
+  const size_t n = (size_t)c->n, N = (size_t)newcap;
+  auto fresh = [&](auto*& p, size_t elems, size_t keep) -> cudaError_t {
+    using T = std::remove_reference_t<decltype(*p)>;
+    T* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, sizeof(T) * std::max<size_t>(elems, 1));
+    if (e != cudaSuccess) return e;
+    if (keep) e = cudaMemcpyAsync(q, p, sizeof(T) * keep, cudaMemcpyDeviceToDevice, c->stream);
+    cudaStreamSynchronize(c->stream);
+    cudaFree(p);
+    p = q;
+    return e;
+  };
+  // Particle keeps its values; Predicted is rebuilt by every step
+  double* sb = nullptr;
+  CK(cudaMalloc(&sb, sizeof(double) * 30 * N));
+  CK(cudaMemsetAsync(sb, 0, sizeof(double) * 30 * N, c->stream));
+  StateArrays nP = make_state(sb, N);
+  double* const from[15] = {c->P.px, c->P.py, c->P.pz, c->P.vx, c->P.vy, c->P.vz, c->P.wx, c->P.wy,
+                            c->P.wz, c->P.ax, c->P.ay, c->P.az, c->P.lx, c->P.ly, c->P.lz};
+  double* const to[15] = {nP.px, nP.py, nP.pz, nP.vx, nP.vy, nP.vz, nP.wx, nP.wy,
+                          nP.wz, nP.ax, nP.ay, nP.az, nP.lx, nP.ly, nP.lz};
+  for (int k = 0; k < 15 && n; k++)
+    CK(cudaMemcpyAsync(to[k], from[k], sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  cudaFree(c->state_block);
+  c->state_block = sb;
+  c->P = nP;
+  c->Pr = make_state(sb + 15 * N, N);
+  const size_t slots9 = 9 * (size_t)(c->nprev + 1);
+  CK(fresh(c->staging, 15 * N, 0));
+  CK(fresh(c->ring, slots9 * N, slots9 * n));  // laid out for n: the first slots9*n
+  CK(fresh(c->radius, N, n));
+  CK(fresh(c->comp, N, n));
+  CK(fresh(c->S.orig, N, 0));
+  CK(fresh(c->S.cell, N, 0));
+  CK(fresh(c->a_cell, N, 0));
+  CK(fresh(c->a_loc, N, 0));
+  CK(fresh(c->a_orig, N, 0));
+  CK(fresh(c->t_orig, N, 0));
+  CK(fresh(c->a_key, N, 0));
+  CK(fresh(c->t_key, N, 0));
+  CellLists& L = c->L;
+  CK(fresh(L.next, N, n));
+  CK(fresh(L.cell[0], N, n));
+  CK(fresh(L.cell[1], N, n));
+  CK(fresh(L.arr_next, N, n));
+  CK(fresh(L.mflag, N, n));
+  CK(fresh(L.mnext, N, n));
+  CK(fresh(c->rows.cand, N * (size_t)c->rows.kc, 0));
+  CK(fresh(c->rows.meta, N, 0));
+  CK(cudaMemsetAsync(c->rows.meta, 0, sizeof(int) * N, c->stream));
+  if (N > n) CK(cudaMemsetAsync(L.mflag + n, 0, sizeof(int) * (N - n), c->stream));
+  for (int b = 0; b < 2; b++) {
+    CK(fresh(c->X[b], N, 0));
+    if (c->precision == DEM_PREC_MIXED) {
+      float4* v = (float4*)c->v4[b];
+      float2* w = (float2*)c->w2[b];
+      CK(fresh(v, N, 0));
+      CK(fresh(w, N, 0));
+      c->v4[b] = v;
+      c->w2[b] = w;
+    } else {
+      double4* v = (double4*)c->v4[b];
+      double2* w = (double2*)c->w2[b];
+      CK(fresh(v, N, 0));
+      CK(fresh(w, N, 0));
+      c->v4[b] = v;
+      c->w2[b] = w;
+    }
+  }
+  // history tables laid out for the new capacity
+  c->ncap = (int)N;
+  int st = grow_history(c, c->hcap);
+  if (st) return st;
+  if (c->precision == DEM_PREC_MIXED && !mixed_grow_walls(c->M, c->n, c->ncap, c->hcur, c->stream))
+    return fail(c, DEM_ERR_CUDA, "mixed wall records");
+  const int one = 1;
+  CK(cudaMemcpyAsync(&c->cnt->force_full, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  c->prepared = -1;
+  c->last_side = -1;
+  CK(cudaStreamSynchronize(c->stream));
   return DEM_OK;
 }
 
@@ -647,8 +755,9 @@ int force_pass(dem_ctx* c, int side, bool update, double dt, int epi, const Ring
 // listed by one grid-wide kernel, then removed by k_remove (one block, in
 // decreasing index).  A removal that would overflow the history tables asks
 // for capacity before it changes anything; the tables grow and the kernel
-// carries on.  Afterwards the ring and the tables are laid out for the new
-// particle count, and the next pass rebuilds every candidate row.
+// carries on.  Afterwards the ring is laid out for the new particle count
+// (the history tables are laid out for the capacity and stay), and the next
+// pass rebuilds every candidate row.
 int update_particle_list_impl(dem_ctx* c, int64_t* removed) {
   if (removed) *removed = 0;
   if (c->nsys > 1) return fail(c, DEM_ERR_UNSUPPORTED, "particle removal needs one system");
@@ -658,12 +767,12 @@ int update_particle_list_impl(dem_ctx* c, int64_t* removed) {
   if (c->rm_cap < n0) {
     cudaFree(c->rm_buf);
     c->rm_buf = nullptr;
-    CK(cudaMalloc(&c->rm_buf, sizeof(int) * ((size_t)n0 + 16)));
+    CK(cudaMalloc(&c->rm_buf, sizeof(int) * ((size_t)n0 + RM_STATE_WORDS)));
     c->rm_cap = n0;
   }
-  int* state = c->rm_buf;      // 8 status words, then the list
-  int* list = c->rm_buf + 16;
-  int hs[8] = {n0, 0, 0, 0, 0, 0, 0, 0};  // [7]: escaped count
+  int* state = c->rm_buf;  // status words, then the list
+  int* list = c->rm_buf + RM_STATE_WORDS;
+  int hs[RM_STATE_WORDS] = {n0};  // [7]: escaped count
   CK(cudaMemcpyAsync(state, hs, sizeof(hs), cudaMemcpyHostToDevice, c->stream));
   launch(c, "escape_list", k_escape_list, blocks_for(n0, 256), 256, (const DevParams*)c->dp, n0,
          c->P, list, state + 7);
@@ -712,6 +821,8 @@ int update_particle_list_impl(dem_ctx* c, int64_t* removed) {
     }
   }
   const int n1 = hs[0];
+  if (!c->pp)
+    for (size_t k = 0; k < c->comp_count.size(); k++) c->comp_count[k] -= hs[8 + k];
   c->rm_stats[0] += hs[3];
   c->rm_stats[1] += hs[4];
   c->rm_stats[2] += hs[5];
@@ -726,9 +837,7 @@ int update_particle_list_impl(dem_ctx* c, int64_t* removed) {
     CK(cudaStreamSynchronize(c->stream));
     cudaFree(c->ring);
     c->ring = nr;
-    c->n = n1;
-    int st = grow_history(c, c->hcap);
-    if (st) return st;
+    c->n = n1;  // the history tables keep their layout (stride = capacity)
   }
   CK(cudaMemsetAsync(&c->cnt->escaped, 0, sizeof(unsigned long long), c->stream));
   const int one = 1;
@@ -741,6 +850,172 @@ int update_particle_list_impl(dem_ctx* c, int64_t* removed) {
   if (removed) *removed = n0 - n1;
   CK(cudaGetLastError());
   return read_counters(c);
+}
+
+// ranf (src/MUtil.f90:17-48): Marsaglia shift register combined with the
+// Park-Miller generator (Schrage's method); aam in single precision, as
+// nearest(1.0,-1.0)/IM is computed, then widened.
+double ranf_host(dem_rng& r) {
+  const int32_t IA = 16807, IM = 2147483647, IQ = 127773, IR = 2836;
+  if (r.dummy <= 0 || r.iiy < 0) {
+    volatile float one_minus = std::nextafter(1.0f, -1.0f);
+    volatile float a = one_minus / (float)IM;
+    const int32_t ad = r.dummy < 0 ? -r.dummy : r.dummy;
+    r.aam = (double)a;
+    r.iiy = (888889999 ^ ad) | 1;
+    r.iix = 777755555 ^ ad;
+    r.dummy = ad + 1;
+  }
+  uint32_t x = (uint32_t)r.iix;
+  x ^= x << 13;
+  x ^= x >> 17;  // ishft(iix,-17) is a logical shift
+  x ^= x << 5;
+  r.iix = (int32_t)x;
+  r.iik = r.iiy / IQ;
+  r.iiy = IA * (r.iiy - r.iik * IQ) - IR * r.iik;
+  if (r.iiy < 0) r.iiy += IM;
+  return r.aam * (double)((IM & (r.iix ^ r.iiy)) | 1);
+}
+
+// the point of one pouring attempt (src/MDEM.f90:455-472)
+void pour_point(const dem_pouring& P, double Di, dem_rng& r, double& x, double& y) {
+  if (P.shape == DEM_POUR_RECTANGLE) {
+    x = (P.size[0] - Di) * (ranf_host(r) - 0.5);
+    y = (P.size[1] - Di) * (ranf_host(r) - 0.5);
+  } else {
+    const double TwoPi = 2.0 * 3.1415926535897932384626433832795;
+    const double Rad = 0.5 * ranf_host(r) * (P.size[0] - Di);
+    const double Angle = TwoPi * ranf_host(r);
+    x = Rad * sin(Angle);
+    y = Rad * cos(Angle);
+  }
+}
+
+// rows the per-particle arrays need while pouring: every component up to its
+// target (removals only lower the counts)
+int pour_capacity(const dem_ctx* c, const std::vector<int>& counts, int n) {
+  if (!c->pouring) return n;
+  long long tot = 0;
+  for (int k = 0; k < c->params.n_components; k++)
+    tot += std::max(counts[(size_t)k], c->pour.target_number[k]);
+  return (int)std::min<long long>(std::max<long long>(tot, n), (1 << 30) - 1);
+}
+
+bool pour_active(const dem_ctx* c) {
+  if (!c->pouring) return false;
+  for (int k = 0; k < c->params.n_components; k++)
+    if (c->comp_count[(size_t)k] < c->pour.target_number[k]) return true;
+  return false;
+}
+
+// PourParticle (src/MDEM.f90:412-532) with InsertParticle (:536-561).  The
+// points of all MaxAttempts attempts are drawn on the host from a copy of the
+// generator and tested at once on the device (k_pour_test); the generator
+// then advances over the attempts the reference makes (up to the first point
+// that fits), and the sphere goes in at index n.
+int pour_particle_impl(dem_ctx* c, int32_t* inserted) {
+  if (inserted) *inserted = 0;
+  if (!pour_active(c)) return DEM_OK;
+  const dem_pouring& Pp = c->pour;
+  const int NC = c->params.n_components;
+  int not_reached[NCM], nnr = 0;
+  for (int k = 0; k < NC; k++)
+    if (c->comp_count[(size_t)k] < Pp.target_number[k]) not_reached[nnr++] = k;
+  const int j = (int)((double)nnr * ranf_host(c->rng));
+  const int comp = not_reached[j];
+  int ibig = 0;  // maxloc(Component%Radius)
+  for (int k = 1; k < NC; k++)
+    if (c->params.comp_radius[k] > c->params.comp_radius[ibig]) ibig = k;
+  const double Ri = c->params.comp_radius[ibig], Di = 2.0 * Ri;
+  const double z = 0.5 * c->params.lbox[2] - Ri;
+  const int na = Pp.max_attempts;
+  if (na <= 0) return DEM_OK;
+  std::vector<double2> cand((size_t)na);
+  dem_rng r = c->rng;
+  for (int a = 0; a < na; a++) pour_point(Pp, Di, r, cand[(size_t)a].x, cand[(size_t)a].y);
+  if (c->pour_cap < na) {
+    cudaFree(c->pour_cand);
+    cudaFree(c->pour_fits);
+    c->pour_cand = nullptr;
+    c->pour_fits = nullptr;
+    CK(cudaMalloc(&c->pour_cand, sizeof(double2) * (size_t)na));
+    CK(cudaMalloc(&c->pour_fits, sizeof(int) * (size_t)na));
+    c->pour_cap = na;
+  }
+  CK(cudaMemcpyAsync(c->pour_cand, cand.data(), sizeof(double2) * (size_t)na,
+                     cudaMemcpyHostToDevice, c->stream));
+  PourTest T;
+  T.PT = c->dp;
+  T.px = c->P.px;
+  T.py = c->P.py;
+  T.pz = c->P.pz;
+  T.comp = c->comp;
+  T.L = c->L;
+  T.cand = c->pour_cand;
+  T.z = z;
+  T.Ri = Ri;
+  T.ibig = ibig;
+  T.n_att = na;
+  T.n = c->n;
+  T.fits = c->pour_fits;
+  launch(c, "pour_test", k_pour_test, (unsigned)((na + 3) / 4), 128u, T);
+  std::vector<int> fits((size_t)na);
+  CK(cudaMemcpyAsync(fits.data(), c->pour_fits, sizeof(int) * (size_t)na, cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  int first = -1;
+  for (int a = 0; a < na && first < 0; a++)
+    if (fits[(size_t)a]) first = a;
+  const int used = first >= 0 ? first + 1 : na;
+  for (int a = 0; a < used; a++) {
+    double x, y;
+    pour_point(Pp, Di, c->rng, x, y);
+  }
+  if (first < 0) return DEM_OK;
+  // InsertParticle at index n
+  const int n0 = c->n;
+  if (n0 + 1 > c->ncap) {
+    int st = grow_capacity(c, std::max(c->ncap + 1, (int)(1.05 * (double)c->ncap)));
+    if (st) return st;
+  }
+  const int slots9 = 9 * (c->nprev + 1);
+  double* nr = nullptr;
+  CK(cudaMalloc(&nr, sizeof(double) * (size_t)slots9 * (size_t)c->ncap));
+  launch(c, "ring_widen", k_ring_widen, 592u, 256u, (const double*)c->ring, nr, slots9, n0,
+         n0 + 1);
+  CK(cudaStreamSynchronize(c->stream));
+  cudaFree(c->ring);
+  c->ring = nr;
+  InsertArgs A;
+  A.PT = c->dp;
+  A.P = c->P;
+  A.radius = c->radius;
+  A.comp = c->comp;
+  A.L = c->L;
+  A.par = c->par;
+  A.H0 = c->H[0];
+  A.H1 = c->H[1];
+  A.nw = c->params.n_walls;
+  A.n = n0;
+  A.comp_new = comp;
+  A.pos[0] = cand[(size_t)first].x;
+  A.pos[1] = cand[(size_t)first].y;
+  A.pos[2] = z;
+  A.vel_z = Pp.velocity_z;
+  A.radius_new = c->params.comp_radius[comp];
+  launch(c, "insert", k_insert, 1u, 32u, A);  // (in mixed mode too: the wall flags and
+                                              // record counts live in the key tables)
+  c->n = n0 + 1;
+  c->comp_count[(size_t)comp]++;
+  const int one = 1;
+  CK(cudaMemcpyAsync(&c->cnt->force_full, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  c->prepared = -1;
+  c->last_side = -1;
+  drop_graphs(c);
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaGetLastError());
+  if (inserted) *inserted = 1;
+  return DEM_OK;
 }
 
 // MoveWalls (src/MDEM.f90:392-408) at Time, into walls[0:NW) of system 0.
@@ -1174,6 +1449,8 @@ void dem_destroy(dem_ctx* c) {
   free_state(c);
   cudaFree(c->dp);
   cudaFree(c->rm_buf);
+  cudaFree(c->pour_cand);
+  cudaFree(c->pour_fits);
   if (c->wall_slots) cudaFreeHost(c->wall_slots);
   cudaFree(c->cellsys);
   cudaFree(c->cnt);
@@ -1232,7 +1509,12 @@ int dem_set_state(dem_ctx* c, int32_t n, const int32_t* comp, const double* radi
   drop_graphs(c);
   free_state(c);
   c->n = n;
-  size_t N = (size_t)std::max(n, 1);
+  // Component(:)%Number, and room for pouring up to the targets
+  c->comp_count.assign((size_t)std::max(c->params.n_components, 0), 0);
+  if (!c->pp && c->nsys == 1)
+    for (int i = 0; i < n; i++) c->comp_count[(size_t)comp[i]]++;
+  size_t N = (size_t)std::max(std::max(std::max(n, c->ncap_hint), pour_capacity(c, c->comp_count, n)), 1);
+  c->ncap = (int)N;
   CK(cudaMalloc(&c->state_block, sizeof(double) * 30 * N));
   CK(cudaMalloc(&c->staging, sizeof(double) * 15 * N));
   CK(cudaMemsetAsync(c->state_block, 0, sizeof(double) * 30 * N, c->stream));
@@ -1285,7 +1567,8 @@ int dem_set_state(dem_ctx* c, int32_t n, const int32_t* comp, const double* radi
   }
   c->hcur = 0;
   if (c->precision == DEM_PREC_MIXED) {
-    if (!mixed_alloc(c->M, n, c->params.n_walls, c->hcap)) return fail(c, DEM_ERR_CUDA, "mixed alloc");
+    if (!mixed_alloc(c->M, c->ncap, c->params.n_walls, c->hcap))
+      return fail(c, DEM_ERR_CUDA, "mixed alloc");
   }
   // host -> device (positions etc. are n x 3 rows)
   {
@@ -1461,9 +1744,10 @@ int dem_set_contacts(dem_ctx* c, int64_t m, const int32_t* imin, const int32_t* 
     if (st) return st;
   }
   const int cap = c->hcap;
-  std::vector<int> key(N * cap, -1);
-  std::vector<double2> val(N * cap * 3);
-  std::fill(cnt.begin(), cnt.end(), 0);
+  const size_t S = (size_t)c->H[c->hcur].n;  // slot stride of the tables
+  cnt.assign(S, 0);
+  std::vector<int> key(S * cap, -1);
+  std::vector<double2> val(S * cap * 3);
   // records kept sorted by partner as the reference lists are
   std::vector<int64_t> idx(m);
   for (int64_t r = 0; r < m; r++) idx[r] = r;
@@ -1473,8 +1757,8 @@ int dem_set_contacts(dem_ctx* c, int64_t m, const int32_t* imin, const int32_t* 
   for (int64_t q = 0; q < m; q++) {
     int64_t r = idx[q];
     int o = imin[r], k = cnt[o]++;
-    key[(size_t)k * N + o] = imax[r];  // slot major
-    double2* v = &val[((size_t)k * N + o) * 3];
+    key[(size_t)k * S + o] = imax[r];  // slot major
+    double2* v = &val[((size_t)k * S + o) * 3];
     v[0] = make_double2(ft[3 * r], ft[3 * r + 1]);
     v[1] = make_double2(ft[3 * r + 2], vt[3 * r]);
     v[2] = make_double2(vt[3 * r + 1], vt[3 * r + 2]);
@@ -1491,7 +1775,7 @@ int dem_set_contacts(dem_ctx* c, int64_t m, const int32_t* imin, const int32_t* 
     wv[wi * 3 + 2] = make_double2(vtw[3 * r + 1], vtw[3 * r + 2]);
   }
   History& H = c->H[c->hcur];
-  CK(cudaMemcpy(H.cnt, cnt.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(H.cnt, cnt.data(), sizeof(int) * S, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(H.key, key.data(), sizeof(int) * key.size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(H.val, val.data(), sizeof(double2) * val.size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(H.wflag, wf.data(), sizeof(int) * wf.size(), cudaMemcpyHostToDevice));
@@ -1507,9 +1791,9 @@ struct HostHist {
   std::vector<double2> val, wv;
 };
 int download_history(dem_ctx* c, HostHist& h) {
-  size_t N = (size_t)std::max(c->n, 1);
   int nw = std::max(c->params.n_walls, 1);
   History H = c->H[c->hcur];
+  size_t N = (size_t)H.n;  // slot stride (the allocated capacity)
   if (c->precision == DEM_PREC_MIXED) {
     // the mixed path keeps FP32 records; export them widened
     H = c->H[c->hcur];
@@ -1552,7 +1836,7 @@ int dem_get_contacts(dem_ctx* c, int64_t cap, int32_t* imin, int32_t* imax, doub
   HostHist h;
   int st = download_history(c, h);
   if (st) return st;
-  const size_t N = (size_t)std::max(c->n, 1);
+  const size_t N = (size_t)c->H[c->hcur].n;  // slot stride
   int64_t a = 0, b = 0;
   std::vector<int> ord;
   for (int i = 0; i < c->n; i++) {
@@ -1757,9 +2041,22 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
   const int G = 4;
   const int HEADROOM = 2;
   const double dt = c->params.time_step;
+  int poured_step = s0 - 1;
   while (step <= last_step) {
     int remaining = last_step - step + 1;
-    if (remaining < G || c->prof) {
+    // PouringAttempt(Step) (src/DEM.f90:95, 115-123); a chunk holds no other
+    // pouring step, so those steps run one at a time
+    bool pour_inside = false;
+    if (pour_active(c)) {
+      if (step % c->pour.interval == 0 && poured_step != step) {
+        st = pour_particle_impl(c, nullptr);
+        if (st) return st;
+      }
+      for (int k = 1; k < G; k++)
+        if ((step + k) % c->pour.interval == 0) pour_inside = true;
+    }
+    poured_step = step;
+    if (remaining < G || c->prof || pour_inside) {
       st = move_particles_impl(c, step, true, 0);
       if (st) return st;
       st = remove_escaped();
@@ -1895,6 +2192,49 @@ int dem_get_ncol(dem_ctx* c, int64_t* ncol) {
   // the last history-updating pass completed (no abort is pending after an
   // API call returns), so its count is part of Ncol
   *ncol = (int64_t)(c->hcnt->ncol + c->hcnt->ncol_pending);
+  return DEM_OK;
+}
+
+int dem_set_pouring(dem_ctx* c, const dem_pouring* p) {
+  if (!c) return DEM_ERR_INVALID;
+  if (!p) {
+    c->pouring = false;
+    drop_graphs(c);
+    return DEM_OK;
+  }
+  if (c->nsys > 1 || c->pp)
+    return fail(c, DEM_ERR_UNSUPPORTED, "pouring needs one system with a component table");
+  if (p->interval < 1 || p->max_attempts < 0 ||
+      (p->shape != DEM_POUR_RECTANGLE && p->shape != DEM_POUR_CIRCLE))
+    return fail(c, DEM_ERR_INVALID, "pouring: interval >= 1, attempts >= 0, known shape");
+  for (int k = 0; k < c->params.n_components; k++)
+    if (p->target_number[k] < 0) return fail(c, DEM_ERR_INVALID, "negative target number");
+  c->pour = *p;
+  c->pouring = true;
+  drop_graphs(c);
+  if (c->state_set) {
+    const int need = pour_capacity(c, c->comp_count, c->n);
+    if (need > c->ncap) return grow_capacity(c, need);
+  }
+  return DEM_OK;
+}
+
+int dem_pour_particle(dem_ctx* c, int32_t* inserted) {
+  if (!c) return DEM_ERR_INVALID;
+  int st = validate_ready(c);
+  if (st) return st;
+  return pour_particle_impl(c, inserted);
+}
+
+int dem_set_rng(dem_ctx* c, const dem_rng* r) {
+  if (!c || !r) return DEM_ERR_INVALID;
+  c->rng = *r;
+  return DEM_OK;
+}
+
+int dem_get_rng(dem_ctx* c, dem_rng* r) {
+  if (!c || !r) return DEM_ERR_INVALID;
+  *r = c->rng;
   return DEM_OK;
 }
 

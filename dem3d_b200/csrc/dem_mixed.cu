@@ -503,14 +503,15 @@ __global__ void k_hist_from_mixed(int n, History H, const float4* a, const float
   }
 }
 
-__global__ void k_mixed_regrow(int n, int ns, const int* cnt, const float4* a, const float4* b,
-                               const float* c, float4* na, float4* nb, float* nc) {
+__global__ void k_mixed_regrow(int n, int ns, int nd, const int* cnt, const float4* a,
+                               const float4* b, const float* c, float4* na, float4* nb,
+                               float* nc) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   for (int r = 0; r < cnt[i]; r++) {
     // slot-major: record r of particle i at r*stride + i, the old tables laid
-    // out for ns particles, the new ones for n
-    const size_t s = (size_t)r * ns + i, d = (size_t)r * n + i;
+    // out for ns rows, the new ones for nd
+    const size_t s = (size_t)r * ns + i, d = (size_t)r * nd + i;
     na[d] = a[s];
     nb[d] = b[s];
     nc[d] = c[s];
@@ -555,9 +556,9 @@ void mixed_free(MixedBuffers& M) {
   M = MixedBuffers{};
 }
 
-bool mixed_regrow(MixedBuffers& M, int n, int newcap, int cur, const History& old,
+bool mixed_regrow(MixedBuffers& M, int n, int stride, int newcap, int cur, const History& old,
                   cudaStream_t st) {
-  size_t N = (size_t)(n > 0 ? n : 1);
+  size_t N = (size_t)(stride > 0 ? stride : 1);
   float4 *na[2], *nb[2];
   float* nc[2];
   for (int b = 0; b < 2; b++) {
@@ -567,8 +568,9 @@ bool mixed_regrow(MixedBuffers& M, int n, int newcap, int cur, const History& ol
       return false;
   }
   if (n > 0)
-    k_mixed_regrow<<<blocks(n, 256), 256, 0, st>>>(n, old.n, old.cnt, M.ha[cur], M.hb[cur],
-                                                    M.hc[cur], na[cur], nb[cur], nc[cur]);
+    k_mixed_regrow<<<blocks(n, 256), 256, 0, st>>>(n, old.n, (int)N, old.cnt, M.ha[cur],
+                                                    M.hb[cur], M.hc[cur], na[cur], nb[cur],
+                                                    nc[cur]);
   cudaStreamSynchronize(st);
   for (int b = 0; b < 2; b++) {
     cudaFree(M.ha[b]);
@@ -579,6 +581,34 @@ bool mixed_regrow(MixedBuffers& M, int n, int newcap, int cur, const History& ol
     M.hc[b] = nc[b];
   }
   M.cap = newcap;
+  return true;
+}
+
+bool mixed_grow_walls(MixedBuffers& M, int n, int stride, int cur, cudaStream_t st) {
+  const size_t W = (size_t)(stride > 0 ? stride : 1) * (size_t)(M.nw > 0 ? M.nw : 1);
+  const size_t keep = (size_t)n * (size_t)(M.nw > 0 ? M.nw : 1);
+  float4 *na[2], *nb[2];
+  float* nc[2];
+  for (int b = 0; b < 2; b++)
+    if (cudaMalloc(&na[b], W * sizeof(float4)) != cudaSuccess ||
+        cudaMalloc(&nb[b], W * sizeof(float4)) != cudaSuccess ||
+        cudaMalloc(&nc[b], W * sizeof(float)) != cudaSuccess)
+      return false;
+  if (keep) {
+    cudaMemcpyAsync(na[cur], M.wa[cur], keep * sizeof(float4), cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(nb[cur], M.wb[cur], keep * sizeof(float4), cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(nc[cur], M.wc[cur], keep * sizeof(float), cudaMemcpyDeviceToDevice, st);
+  }
+  cudaStreamSynchronize(st);
+  for (int b = 0; b < 2; b++) {
+    cudaFree(M.wa[b]);
+    cudaFree(M.wb[b]);
+    cudaFree(M.wc[b]);
+    M.wa[b] = na[b];
+    M.wb[b] = nb[b];
+    M.wc[b] = nc[b];
+  }
+  M.n = stride;
   return true;
 }
 

@@ -23,8 +23,12 @@ struct MixedBuffers {
 bool mixed_available();
 bool mixed_alloc(MixedBuffers& M, int n, int nw, int cap);
 void mixed_free(MixedBuffers& M);
-bool mixed_regrow(MixedBuffers& M, int n, int newcap, int cur, const History& old,
+// the current records of `n` particles into tables of capacity newcap laid
+// out for `stride` rows (old: the tables they come from, with their stride)
+bool mixed_regrow(MixedBuffers& M, int n, int stride, int newcap, int cur, const History& old,
                   cudaStream_t st);
+// the wall records of the first n particles into arrays for `stride` rows
+bool mixed_grow_walls(MixedBuffers& M, int n, int stride, int cur, cudaStream_t st);
 // One pass kernel launch (FP32 contact arithmetic) on the context's stream.
 // variant: 0 = compiled for 4 resident blocks per SM, 1 = for 3
 void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant,

@@ -49,8 +49,10 @@ struct RemovalArgs {
   int* list;    // escaped particles, -1 once removed
   int n_list;
   int* state;   // [0] particle count, [1] status, [2] capacity asked for,
-                // [3] removals, [4] swaps, [5] records renamed or moved
+                // [3] removals, [4] swaps, [5] records renamed or moved,
+                // [8 + k] particles of component k removed
 };
+constexpr int RM_STATE_WORDS = 32;
 
 // escaped particles: any coordinate outside [-L/2, L/2] (src/MDEM.f90:624-625)
 __global__ void k_escape_list(const DevParams* __restrict__ PT, int n, StateArrays Q,
@@ -229,6 +231,7 @@ __global__ void __launch_bounds__(RM_THREADS, 1) k_remove(RemovalArgs A) {
     // ---- RemoveParticleFromCell (src/MCells.f90:702-724)
     if (t == 0) {
       A.list[s_slot] = -1;
+      A.state[8 + A.comp[i]] += 1;  // Component(Index)%Number - 1
       int q = A.L.head[iCell];
       if (q == i) {
         A.L.head[iCell] = A.L.next[i];
@@ -349,6 +352,118 @@ __global__ void k_ring_restride(const double* __restrict__ src, double* __restri
        k += (size_t)gridDim.x * blockDim.x) {
     const size_t b = k / nd, i = k - b * nd;
     dst[k] = src[b * ns + i];
+  }
+}
+
+}  // namespace dem
+
+namespace dem {
+
+// ---------------------------------------------------------------------------
+// Pouring (PourParticle, src/MDEM.f90:412-532): the candidate points of all
+// attempts (drawn on the host from the reference's generator) are tested at
+// once, one warp per attempt; the host takes the first that fits.
+
+struct PourTest {
+  const DevParams* PT;
+  const double* px;
+  const double* py;
+  const double* pz;
+  const int* comp;
+  CellLists L;
+  const double2* cand;  // (x, y) of every attempt
+  double z;             // pHalfLbox(3) - Ri
+  double Ri;            // the largest component radius
+  int ibig;             // its component (maxloc)
+  int n_att;
+  int n;                // particles (bound of every list walk)
+  int* fits;            // [n_att] 1: no particle or wall overlaps the sphere
+};
+
+__global__ void __launch_bounds__(128) k_pour_test(PourTest T) {
+  __shared__ int s_cells[4][27];
+  __shared__ int s_nc[4];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int a = blockIdx.x * 4 + wid;
+  if (a >= T.n_att) return;
+  const DevParams& P = T.PT[0];
+  const double2 c2 = T.cand[a];
+  const double x[3] = {c2.x, c2.y, T.z};
+  if (lane == 0) s_nc[wid] = rm_neighbour_cells(P, current_cell(P, x[0], x[1], x[2]), s_cells[wid]);
+  __syncwarp();
+  bool clash = false;
+  if (lane < s_nc[wid]) {
+    int guard = 0;
+    for (int q = T.L.head[s_cells[wid][lane]]; q != -1 && !clash && ++guard <= T.n;
+         q = T.L.next[q]) {
+      // Rij is integer(ib) in PourParticle: each component is truncated
+      const int r0 = (int)(T.px[q] - x[0]), r1 = (int)(T.py[q] - x[1]),
+                r2 = (int)(T.pz[q] - x[2]);
+      const int s = r0 * r0 + r1 * r1 + r2 * r2;
+      clash = !((double)s > P.min_dij_sq[T.ibig * NCM + T.comp[q]]);
+    }
+  }
+  if (lane < P.nw) {
+    double Dij, Nij[3], Qji[3];
+    clash = clash || overlap_wall(P, P.walls[lane], x, T.Ri, Dij, Nij, Qji);
+  }
+  clash = __any_sync(0xffffffffu, clash);
+  if (lane == 0) T.fits[a] = clash ? 0 : 1;
+}
+
+// InsertParticle (src/MDEM.f90:536-561) at index n (the ring already laid
+// out for n + 1 particles, its new entries zero)
+struct InsertArgs {
+  const DevParams* PT;
+  StateArrays P;
+  double* radius;
+  int* comp;
+  CellLists L;
+  int par;
+  History H0, H1;
+  int nw;
+  int n;
+  int comp_new;
+  double pos[3], vel_z, radius_new;
+};
+
+__global__ void k_insert(InsertArgs A) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const DevParams& P = A.PT[0];
+  const int i = A.n;
+  double* const f[15] = {A.P.px, A.P.py, A.P.pz, A.P.vx, A.P.vy, A.P.vz, A.P.wx, A.P.wy,
+                         A.P.wz, A.P.ax, A.P.ay, A.P.az, A.P.lx, A.P.ly, A.P.lz};
+  for (int k = 0; k < 15; k++) f[k][i] = 0.0;
+  A.P.px[i] = A.pos[0];
+  A.P.py[i] = A.pos[1];
+  A.P.pz[i] = A.pos[2];
+  A.P.vz[i] = A.vel_z;
+  A.radius[i] = A.radius_new;
+  A.comp[i] = A.comp_new;
+  // CellIndex(NP) and AddParticle (prepend, src/MCells.f90:684-698); the
+  // prepared transition sees the new particle staying in its cell
+  const int c = current_cell(P, A.pos[0], A.pos[1], A.pos[2]);
+  A.L.next[i] = A.L.head[c];
+  A.L.head[c] = i;
+  A.L.cell[A.par][i] = c;
+  A.L.cell[A.par ^ 1][i] = c;
+  A.L.mflag[i] = 0;
+  A.H0.cnt[i] = 0;
+  A.H1.cnt[i] = 0;
+  for (int w = 0; w < A.nw; w++) {
+    A.H0.wflag[(size_t)i * A.nw + w] = 0;
+    A.H1.wflag[(size_t)i * A.nw + w] = 0;
+  }
+}
+
+// the ring laid out for nd > ns particles (entries of the new particles zero)
+__global__ void k_ring_widen(const double* __restrict__ src, double* __restrict__ dst, int slots9,
+                             int ns, int nd) {
+  const size_t total = (size_t)slots9 * nd;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total;
+       k += (size_t)gridDim.x * blockDim.x) {
+    const size_t b = k / nd, i = k - b * nd;
+    dst[k] = i < (size_t)ns ? src[b * ns + i] : 0.0;
   }
 }
 

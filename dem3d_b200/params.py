@@ -130,6 +130,30 @@ def wall_motion(position, amplitude, frequency, phase, scales: "Scales | None" =
     return m
 
 
+def pouring(target_number, shape: int, size, max_attempts: int, interval: float,
+            time_step: float, scales: "Scales | None" = None):
+    """Pouring settings as ReadPouringFile and CalculateProperties derive them
+    (src/DEM.f90:745-800, 346, 861): ``interval`` is PouringInterval (time),
+    IPouring = max(1, nint(interval/time_step)); ``size`` the rectangle sides
+    or the circle diameter; with ``scales`` the size is scaled like
+    ScaleVariables, and the new spheres get the reference's initial velocity
+    -1e-4*LengthScale/TimeScale (src/MDEM.f90:522)."""
+    from ._abi import DemPouring
+    p = DemPouring()
+    p.interval = max(1, int(math.floor(interval / time_step + 0.5)))  # nint, positive
+    p.shape = int(shape)
+    p.max_attempts = int(max_attempts)
+    for k, t in enumerate(target_number):
+        if t < 0:
+            raise ValueError("target numbers cannot be negative")
+        p.target_number[k] = int(t)
+    L = scales.length if scales is not None else 1.0
+    for k, s in enumerate(size):
+        p.size[k] = float(s) / L
+    p.velocity_z = -1e-4 * (scales.length / scales.time if scales is not None else 1.0)
+    return p
+
+
 @dataclass
 class Component:
     number: int

@@ -520,6 +520,9 @@ def capture(system, *, components, wall_stiffness, step: int, scales=(1.0, 1.0, 
                         walls, comp, st["pos"], st["vel"], st["omega"])
     _, trav, cs = system.get_cells()
     prev, ipc = system.get_integration()
+    if "rng" not in header:  # the pouring generator (aam, Dummy, iix, iiy, iik)
+        r = system.rng()
+        header["rng"] = (r["aam"], r["dummy"], r["iix"], r["iiy"], r["iik"])
     return StateFile(cfg, trav, cs, ipc, prev, system.get_contacts(), step + 1, system.ncol(),
                      **header)
 
@@ -556,4 +559,6 @@ def restore(system, state: StateFile) -> int:
     system.set_contacts(ct["imin"], ct["imax"], ct["ft"], ct["vt"], ct["ip"], ct["iw"],
                         ct["ftw"], ct["vtw"])
     system.set_ncol(state.ncol)
+    aam, dummy, iix, iiy, iik = state.rng
+    system.set_rng(aam, dummy, iix, iiy, iik)
     return int(state.initial_step)

@@ -31,7 +31,8 @@ import ctypes as C
 import numpy as np
 
 from . import _abi
-from ._abi import MAX_WALLS, DemObservables, DemParams, DemWall, DemWallMotion
+from ._abi import (MAX_WALLS, DemObservables, DemParams, DemPouring, DemRng, DemWall,
+                   DemWallMotion)
 
 
 class DEMError(RuntimeError):
@@ -280,6 +281,27 @@ class DEMSystem:
         s = (C.c_int64 * 3)()
         self._call("get_removal_stats", s)
         return {"removed": s[0], "swaps": s[1], "records_moved": s[2]}
+
+    # -- pouring -------------------------------------------------------------
+    def set_pouring(self, pouring: DemPouring | None) -> None:
+        """Pouring for ``run`` (PouringAttempt before every step), or None."""
+        self._call("set_pouring", None if pouring is None else C.byref(pouring))
+
+    def pour_particle(self) -> bool:
+        """PourParticle once; True if a sphere went in."""
+        v = C.c_int32()
+        self._call("pour_particle", C.byref(v))
+        self._refresh_n()
+        return bool(v.value)
+
+    def rng(self) -> dict:
+        r = DemRng()
+        self._call("get_rng", C.byref(r))
+        return {"aam": r.aam, "dummy": r.dummy, "iix": r.iix, "iiy": r.iiy, "iik": r.iik}
+
+    def set_rng(self, aam=0.0, dummy=0, iix=-1, iiy=-1, iik=0) -> None:
+        r = DemRng(aam, dummy, iix, iiy, iik)
+        self._call("set_rng", C.byref(r))
 
     def set_ncol(self, ncol: int) -> None:
         self._call("set_ncol", int(ncol))

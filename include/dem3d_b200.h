@@ -134,6 +134,28 @@ typedef struct dem_wall_motion {
   double phase_angle[3];
 } dem_wall_motion;
 
+/* Pouring (PouringAttempt/PourParticle, src/DEM.f90:115-123,
+ * src/MDEM.f90:412-532): every `interval` steps one sphere of a component
+ * still below its target count is dropped at a random point of the pouring
+ * surface just under the top of the box, if it overlaps nothing there. */
+#define DEM_POUR_RECTANGLE 1 /* Rect (src/MDEM.f90:34) */
+#define DEM_POUR_CIRCLE 2    /* Circle */
+typedef struct dem_pouring {
+  int32_t interval;     /* IPouring = max(1, nint(PouringInterval/TimeStep)) */
+  int32_t shape;        /* PouringShape */
+  int32_t max_attempts; /* MaxAttempts */
+  int32_t target_number[DEM_MAX_COMPONENTS]; /* TargetNumber(1:NC) */
+  double size[2];       /* PouringSize (simulation units): sides, or diameter */
+  double velocity_z;    /* velocity of a new sphere: -1e-4*LengthScale/TimeScale */
+} dem_pouring;
+
+/* State of ranf (src/MUtil.f90:10-11): Dummy (the seed, negative to start),
+ * the Marsaglia and Park-Miller words iix, iiy, iik and the scale aam. */
+typedef struct dem_rng {
+  double aam;
+  int32_t dummy, iix, iiy, iik;
+} dem_rng;
+
 typedef struct dem_ctx dem_ctx;
 
 /* Library build/version string (also proves the .so loads). */
@@ -266,6 +288,15 @@ int dem_get_components(dem_ctx* ctx, int32_t* comp);
 /* Removals so far: {particles removed, swaps with the last particle,
  * contact records renamed or handed over}. */
 int dem_get_removal_stats(dem_ctx* ctx, int64_t* stats);
+
+/* Pouring for dem_run (NULL: off).  Single-system contexts with a component
+ * table.  The per-particle arrays grow to hold every component's target. */
+int dem_set_pouring(dem_ctx* ctx, const dem_pouring* pouring);
+/* PourParticle once (inserted: 1 if a sphere went in, else 0). */
+int dem_pour_particle(dem_ctx* ctx, int32_t* inserted);
+/* The generator state, as SaveState/ReadState keep it (src/DEM.f90:995-999). */
+int dem_set_rng(dem_ctx* ctx, const dem_rng* rng);
+int dem_get_rng(dem_ctx* ctx, dem_rng* rng);
 
 /* Ncol (src/MForces.f90:47,227). */
 int dem_get_ncol(dem_ctx* ctx, int64_t* ncol);

@@ -115,6 +115,10 @@ typedef struct orc_ctx {
   double wall_fn[NWM];
   int moving;               /* WallsInMovement */
   int removal;              /* run() calls UpdateParticleList after each step */
+  int pouring;              /* run() calls PouringAttempt before each step */
+  dem_pouring pour;
+  dem_rng rng;              /* ranf's state (src/MUtil.f90:10-11) */
+  int32_t comp_count[NCM];  /* Component(:)%Number */
   int64_t removal_count, removal_swaps, removal_moved;  /* test diagnostics */
   dem_wall_motion wm[NWM];  /* WM(j) */
   char err[256];
@@ -1134,6 +1138,7 @@ static int update_particle_list(orc_ctx* c, int64_t* removed) {
       if (q->pos[k] > h || q->pos[k] < -h) out = 1;
     }
     if (!out) continue;
+    if (c->p.n_components > 0) c->comp_count[q->index]--;
     int32_t iCell = c->cell_index[i];
     int32_t* nb = NULL;
     int32_t npsc = all_neighbour_particles(c, iCell, &nb);
@@ -1160,6 +1165,133 @@ static int update_particle_list(orc_ctx* c, int64_t* removed) {
 }
 
 /* ------------------------------------------------------------------ */
+/* Pouring (PourParticle / InsertParticle, src/MDEM.f90:412-561)         */
+
+/* ranf (src/MUtil.f90:17-48): Marsaglia shift register combined with the
+ * Park-Miller generator (Schrage's method).  aam is computed in default
+ * (single) precision, as nearest(1.0,-1.0)/IM is, then widened. */
+static double ranf(dem_rng* r) {
+  const int32_t IA = 16807, IM = 2147483647, IQ = 127773, IR = 2836;
+  if (r->dummy <= 0 || r->iiy < 0) {
+    volatile float one_minus = nextafterf(1.0f, -1.0f);
+    volatile float a = one_minus / (float)IM;
+    int32_t ad = r->dummy < 0 ? -r->dummy : r->dummy;
+    r->aam = (double)a;
+    r->iiy = (888889999 ^ ad) | 1;
+    r->iix = 777755555 ^ ad;
+    r->dummy = ad + 1;
+  }
+  uint32_t x = (uint32_t)r->iix;
+  x ^= x << 13; /* ishft(iix,13) */
+  x ^= x >> 17; /* ishft(iix,-17): logical shift */
+  x ^= x << 5;
+  r->iix = (int32_t)x;
+  r->iik = r->iiy / IQ;
+  r->iiy = IA * (r->iiy - r->iik * IQ) - IR * r->iik;
+  if (r->iiy < 0) r->iiy += IM;
+  return r->aam * (double)((IM & (r->iix ^ r->iiy)) | 1);
+}
+
+/* room for `cap` particles (ResizeVariables grows MaxNP, src/MDEM.f90:565-608) */
+static void reserve_particles(orc_ctx* c, int32_t cap) {
+  if (cap <= c->nalloc) return;
+  size_t N = (size_t)cap, n = (size_t)c->n;
+  c->part = (OParticle*)realloc(c->part, N * sizeof(OParticle));
+  c->pred = (OParticle*)realloc(c->pred, N * sizeof(OParticle));
+  c->cell_index = (int32_t*)realloc(c->cell_index, N * sizeof(int32_t));
+  c->mainp = (OMain*)realloc(c->mainp, N * sizeof(OMain));
+  memset(c->mainp + n, 0, (N - n) * sizeof(OMain));
+  c->force = (double*)realloc(c->force, 3 * N * sizeof(double));
+  c->torque = (double*)realloc(c->torque, 3 * N * sizeof(double));
+  int32_t slots = c->nprev > 0 ? c->nprev : 1;
+  OPrev* pv = (OPrev*)calloc(N * (size_t)slots, sizeof(OPrev));
+  for (int32_t k = 0; k < c->nprev; k++)
+    memcpy(pv + (size_t)k * N, c->prev + (size_t)k * c->nalloc, n * sizeof(OPrev));
+  free(c->prev);
+  c->prev = pv;
+  c->nalloc = cap;
+}
+
+/* InsertParticle (src/MDEM.f90:536-561) */
+static void insert_particle(orc_ctx* c, const OParticle* part) {
+  if (c->n == c->nalloc) {
+    int32_t grown = (int32_t)(1.05 * (double)c->nalloc);
+    reserve_particles(c, grown > c->nalloc + 1 ? grown : c->nalloc + 1);
+  }
+  int32_t NP = c->n;
+  c->n = NP + 1;
+  c->comp_count[part->index]++;
+  c->part[NP] = *part;
+  c->pred[NP].index = part->index;
+  c->pred[NP].radius = part->radius;
+  for (int32_t k = 1; k <= c->nprev; k++) memset(prev_at(c, k, NP), 0, sizeof(OPrev));
+  c->cell_index[NP] = current_cell(c, part->pos[0], part->pos[1], part->pos[2]);
+  add_particle(c, NP, c->cell_index[NP]);
+  c->mainp[NP].first_partner = NULL;
+  c->mainp[NP].first_wall = NULL;
+}
+
+/* PourParticle (src/MDEM.f90:412-532).  As in the reference, every attempt
+ * tests the largest component's radius (the "<test>" lines), and the
+ * particle-particle test squares the separation converted to integer(ib):
+ * Rij is declared integer there, so each component is truncated. */
+static int pour_particle(orc_ctx* c, int32_t* inserted) {
+  *inserted = 0;
+  const dem_pouring* P = &c->pour;
+  const int32_t NC = c->p.n_components;
+  int32_t not_reached[NCM], nnr = 0;
+  for (int32_t k = 0; k < NC; k++)
+    if (c->comp_count[k] < P->target_number[k]) not_reached[nnr++] = k;
+  if (nnr == 0) return DEM_OK;
+  int32_t j = (int32_t)((double)nnr * ranf(&c->rng));
+  OParticle iPart;
+  memset(&iPart, 0, sizeof(iPart));
+  iPart.index = not_reached[j];
+  int32_t iBig = 0;
+  for (int32_t k = 1; k < NC; k++)
+    if (c->p.comp_radius[k] > c->p.comp_radius[iBig]) iBig = k;
+  const double Ri = c->p.comp_radius[iBig];
+  const double Di = 2.0 * Ri;
+  iPart.pos[2] = 0.5 * c->p.lbox[2] - Ri;
+  const double TwoPi = 2.0 * 3.1415926535897932384626433832795;
+  int possible = 0;
+  int32_t attempt = 0;
+  while (!possible && attempt < P->max_attempts) {
+    possible = 1;
+    attempt++;
+    if (P->shape == DEM_POUR_RECTANGLE) {
+      for (int k = 0; k < 2; k++) iPart.pos[k] = (P->size[k] - Di) * (ranf(&c->rng) - 0.5);
+    } else {
+      double Rad = 0.5 * ranf(&c->rng) * (P->size[0] - Di);
+      double Angle = TwoPi * ranf(&c->rng);
+      iPart.pos[0] = Rad * sin(Angle);
+      iPart.pos[1] = Rad * cos(Angle);
+    }
+    int32_t iCell = current_cell(c, iPart.pos[0], iPart.pos[1], iPart.pos[2]);
+    int32_t* nb = NULL;
+    int32_t npsc = all_neighbour_particles(c, iCell, &nb);
+    for (int32_t jj = 0; possible && jj < npsc; jj++) {
+      const OParticle* jPart = &c->part[nb[jj]];
+      int32_t R[3];
+      for (int k = 0; k < 3; k++) R[k] = (int32_t)(jPart->pos[k] - iPart.pos[k]);
+      int32_t s = R[0] * R[0] + R[1] * R[1] + R[2] * R[2];
+      possible = (double)s > c->p.min_dij_sq[iBig * NCM + jPart->index];
+    }
+    free(nb);
+    for (int32_t w = 0; possible && w < c->p.n_walls; w++) {
+      double Dij, Nij[3], Qji[3];
+      possible = !overlap_wall(c, &iPart, &c->p.walls[w], Ri, &Dij, Nij, Qji);
+    }
+  }
+  if (possible) {
+    iPart.vel[2] = P->velocity_z;
+    insert_particle(c, &iPart);
+    *inserted = 1;
+  }
+  return DEM_OK;
+}
+
+/* ------------------------------------------------------------------ */
 /* public API (mirrors include/dem3d_b200.h with an orc_ prefix)        */
 
 const char* orc_last_error(const orc_ctx* c) { return c ? c->err : "null context"; }
@@ -1175,6 +1307,8 @@ int orc_create(const dem_params* p, orc_ctx** out) {
       return DEM_ERR_UNSUPPORTED;
   orc_ctx* c = (orc_ctx*)calloc(1, sizeof(orc_ctx));
   c->removal = 1; /* the main loop always calls UpdateParticleList (src/DEM.f90:96) */
+  c->rng.iix = -1;  /* src/MUtil.f90:11 */
+  c->rng.iiy = -1;
   c->p = *p;
   for (int k = 0; k < 3; k++) c->inv_lbox[k] = 1.0 / p->lbox[k];
   /* InitializeAuxiliaries, src/MDEM.f90:110-162 */
@@ -1285,6 +1419,9 @@ int orc_set_state(orc_ctx* c, int32_t n, const int32_t* comp, const double* radi
     c->pred[i].index = q->index;
     c->pred[i].radius = q->radius;
   }
+  memset(c->comp_count, 0, sizeof(c->comp_count));
+  if (c->p.n_components > 0)
+    for (int32_t i = 0; i < n; i++) c->comp_count[c->part[i].index]++;
   for (int k = 0; k < c->nprev; k++) c->ipc[k] = k + 1;
   c->ncol = 0;
   c->cells_ready = 0;
@@ -1482,6 +1619,44 @@ int orc_set_cells(orc_ctx* c, const int32_t* traversal, const int32_t* cell_star
   return DEM_OK;
 }
 
+int orc_set_pouring(orc_ctx* c, const dem_pouring* p) {
+  if (!c) return DEM_ERR_INVALID;
+  if (!p) { c->pouring = 0; return DEM_OK; }
+  if (c->p.n_components <= 0) return DEM_ERR_UNSUPPORTED;
+  if (p->interval < 1 || p->max_attempts < 0 ||
+      (p->shape != DEM_POUR_RECTANGLE && p->shape != DEM_POUR_CIRCLE))
+    return DEM_ERR_INVALID;
+  c->pour = *p;
+  c->pouring = 1;
+  return DEM_OK;
+}
+
+int orc_pour_particle(orc_ctx* c, int32_t* inserted) {
+  if (!c || !c->cells_ready) return DEM_ERR_STATE;
+  int32_t ins = 0;
+  int st = pour_particle(c, &ins);
+  if (inserted) *inserted = ins;
+  return st;
+}
+
+int orc_set_rng(orc_ctx* c, const dem_rng* r) {
+  if (!c || !r) return DEM_ERR_INVALID;
+  c->rng = *r;
+  return DEM_OK;
+}
+
+/* test hook: `count` successive ranf values from state r (r advances) */
+int orc_ranf(dem_rng* r, int32_t count, double* out) {
+  for (int32_t k = 0; k < count; k++) out[k] = ranf(r);
+  return DEM_OK;
+}
+
+int orc_get_rng(orc_ctx* c, dem_rng* r) {
+  if (!c || !r) return DEM_ERR_INVALID;
+  *r = c->rng;
+  return DEM_OK;
+}
+
 int orc_update_particle_list(orc_ctx* c, int64_t* removed) {
   if (!c || !c->cells_ready) return DEM_ERR_STATE;
   return update_particle_list(c, removed);
@@ -1541,6 +1716,10 @@ int orc_run(orc_ctx* c, int32_t first_step, int32_t last_step) {
     s0 = c->p.method_order;
   }
   for (int32_t s = s0; s <= last_step; s++) {
+    if (c->pouring && s % c->pour.interval == 0) { /* PouringAttempt (src/DEM.f90:115-123) */
+      int32_t ins;
+      pour_particle(c, &ins);
+    }
     int st = move_particles(c, s);
     if (st) return st;
     if (c->removal) update_particle_list(c, NULL);
