@@ -127,21 +127,23 @@ def pass_bytes_per_particle(mixed, epi, z_pp, m_cand, z_pw=0.0, nw=0, nprev=3):
         wall records 4 + record per wall;
       epi "predict" (pass 1, src/MDEM.f90:296-331): ring nprev*72 read,
         Particle v,w 48 read (mixed: FP64 copies), a,alpha 48 + Predicted
-        x,v,w 72 + ring slot 72 + next-pass copies (32 + velocities) + cell 4
-        written;
-      epi "correct" (pass 2, :340-367): ring read, Predicted v 24 (mixed),
-        Particle x,v,w 72 read and written, Predicted a,alpha 48 + next-pass
-        copies + cell 4 written."""
+        x,v,w 72 + ring slot 72 + the corrector's ring sums 72 + next-pass
+        copies (32 + velocities) + cell 4 written;
+      epi "correct" (pass 2, :340-367): the ring sums 72, Predicted v 24
+        (mixed) read, Particle x,v,w 72 read and written, Predicted a,alpha
+        48 + next-pass copies + cell 4 written."""
     vel = 24 if mixed else 48
     rec = 4 + (36 if mixed else 48)
     own = 32 + vel + 4 + 4 + 4 + 4 * m_cand
     hist = 0.5 * z_pp * rec + nw * 4 + z_pw * (rec - 4)
     ring = nprev * 72
+    sums = 72 if nprev else 0  # sum_k AM(k)*Previous(ipc(k)), predictor -> corrector
     if epi == "predict":
         hist += 4 + 0.5 * z_pp * rec + nw * 4 + z_pw * (rec - 4)  # updated tables
-        epil = ring + (48 if mixed else 0) + 48 + 72 + (72 if nprev else 0) + 32 + vel + 4
+        epil = (ring + (48 if mixed else 0) + 48 + 72 + (72 if nprev else 0) + sums + 32 + vel
+                + 4)
     else:
-        epil = ring + (24 if mixed else 0) + 72 + 72 + 48 + 32 + vel + 4
+        epil = sums + (24 if mixed else 0) + 72 + 72 + 48 + 32 + vel + 4
     return own + hist + epil
 
 
@@ -513,30 +515,35 @@ def run_ours(args):
     step_b = step_bytes_per_particle(mixed, z_pp, m_cand, z_pw, nw)
     step_gbs = step_b * n / (ms / args.steps / 1000.0) / 1e9
 
-    # e2e: each step uploads Particle(1:n) from pinned host memory, advances
-    # one MoveParticles through the C-ABI and downloads the state.
+    # e2e: a driver that keeps Particle(1:n) on the host: each step uploads
+    # positions, velocities and angular velocities from pinned host memory,
+    # advances one MoveParticles through the C-ABI and downloads them again
+    # (accelerations are recomputed by the step's first pass and are not an
+    # input of MoveParticles).
     e2e = None
     if not args.no_e2e:
         import ctypes as C
         ke = max(3, min(args.steps, 20))
+        fields = ("pos", "vel", "omega")
         host = {k: torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
-                for k in ("pos", "vel", "omega", "acc", "alpha")}
+                for k in fields}
         stt = s.get_state()
         for k in host:
             host[k][...] = stt[k]
+        ptr = {k: host[k].ctypes.data_as(C.POINTER(C.c_double)) for k in fields}
         if world > 1:
             dist.barrier()
         s.timer_start()
         for k in range(ke):
-            s.update_state(host["pos"], host["vel"], host["omega"], host["acc"], host["alpha"])
+            s._call("update_state", ptr["pos"], ptr["vel"], ptr["omega"], None, None)
             s.move_particles(last + 1 + k)
-            s._call("get_state", *(host[x].ctypes.data_as(C.POINTER(C.c_double))
-                                   for x in ("pos", "vel", "omega", "acc", "alpha")))
+            s._call("get_state", ptr["pos"], ptr["vel"], ptr["omega"], None, None)
         e2e_ms = barrier_max(s.timer_stop())
         last += ke
         e2e = {"value": n * world * ke / (e2e_ms / 1000.0), "unit": UNIT,
-               "h2d_bytes_per_step": 5 * 24 * n, "d2h_bytes_per_step": 5 * 24 * n,
-               "steps": ke, "path": "dem_update_state + dem_move_particles + dem_get_state"}
+               "h2d_bytes_per_step": 3 * 24 * n, "d2h_bytes_per_step": 3 * 24 * n,
+               "steps": ke, "path": "dem_update_state + dem_move_particles + dem_get_state "
+                                    "(positions, velocities, angular velocities)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

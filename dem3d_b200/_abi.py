@@ -99,6 +99,14 @@ class DemRng(C.Structure):
                 ("iiy", C.c_int32), ("iik", C.c_int32)]
 
 
+class DemFluid(C.Structure):
+    """Fluid settings (ReadFluidSpecifications, src/mFluid.f90:27-52)."""
+
+    _fields_ = [("viscosity", C.c_double), ("flow_rate", C.c_double), ("density", C.c_double),
+                ("comp_density", C.c_double * MAX_COMPONENTS), ("levels", C.c_int32),
+                ("pad_", C.c_int32)]
+
+
 class DemObservables(C.Structure):
     _fields_ = [
         ("kinetic_energy", C.c_double), ("potential_energy", C.c_double),
@@ -145,6 +153,7 @@ SIGNATURES = {
     "get_components": (C.c_int, [_P, _I32P]),
     "get_removal_stats": (C.c_int, [_P, _I64P]),
     "set_pouring": (C.c_int, [_P, C.POINTER(DemPouring)]),
+    "set_fluid": (C.c_int, [_P, C.POINTER(DemFluid)]),
     "pour_particle": (C.c_int, [_P, _I32P]),
     "set_rng": (C.c_int, [_P, C.POINTER(DemRng)]),
     "get_rng": (C.c_int, [_P, C.POINTER(DemRng)]),

@@ -53,7 +53,7 @@ class Workload:
 
 def settling(n=2000, seed=1000, layer_side=10, dt=1e-4, e=0.8, mu=0.5, gravity=1.0,
              headroom=45.0, method_order=4, euler_intervals=100, max_ncell=30000,
-             precision=P.PREC_FP64, sigma_v=0.1, first_height=1.0):
+             precision=P.PREC_FP64, sigma_v=0.1, first_height=1.0, fluid_density=0.0):
     """Monodisperse gravity settling (d = 1, m = 1).
 
     ``layer_side`` x ``layer_side`` spheres per layer at xy spacing 1.0 in a
@@ -90,7 +90,8 @@ def settling(n=2000, seed=1000, layer_side=10, dt=1e-4, e=0.8, mu=0.5, gravity=1
         [P.Component(n, 1.0, DENSITY, 2.0 * KN, 2.0 * KT)], [floor], [[e]], [[e]], [[mu]],
         [[e]], [[e]], [[mu]], lbox=(L, L, lz), pbc=(True, True, False),
         gravity=(0.0, 0.0, -gravity), time_step=dt, method_order=method_order,
-        euler_intervals=euler_intervals, max_ncell=max_ncell, precision=precision)
+        euler_intervals=euler_intervals, max_ncell=max_ncell, precision=precision,
+        fluid_density=fluid_density)
     return Workload("settling", prm, pos, vel, omega, comp=comp,
                     info={"lbox": (L, L, lz), "seed": seed})
 

@@ -192,6 +192,10 @@ struct PassArgs {
   RingMap rm;
   Counters* cnt;
   int tag;  // 2*(step within a captured chunk) + pass
+  const double* drag;  // [3n] fluid drag of every sphere (NULL: no fluid)
+  // the corrector's ring sums sum_k AM(k)*Previous(ipc(k)) (v, a, alpha:
+  // [9][n]), formed by the predictor pass, which holds every term of them
+  double* amsum;
 };
 
 // ------------------------------------------------------------------------
@@ -405,14 +409,12 @@ __device__ __forceinline__ void cone_radial(const double RijW[3], double AlphaW,
   }
 }
 
-// Overlap (src/MConfig.f90:692-822): Rectangle and Cone (conic frustum with
-// half length L1 along U, radii L2 and L3 at its two ends; the auxiliary
-// quantities of ConfigureWalls, src/MConfig.f90:661-684, for radius Ri).
-__device__ __forceinline__ bool overlap_wall(const DevParams& P, const dem_wall& w,
+// Overlap's Cone branch (src/MConfig.f90:751-793): conic frustum with half
+// length L1 along U, radii L2 and L3 at its two ends; the auxiliary
+// quantities of ConfigureWalls (src/MConfig.f90:661-684) for radius Ri.
+__device__ __forceinline__ bool overlap_cone(const DevParams& P, const dem_wall& w,
                                              const double x[3], double Ri, double& Dij,
                                              double Nij[3], double Qji[3]) {
-  if (w.shape == DEM_WALL_RECTANGLE) return overlap_rect(P, w, x, Ri, Dij, Nij, Qji);
-  if (w.shape != DEM_WALL_CONE) return false;
   double Rij[3];
 #pragma unroll
   for (int k = 0; k < 3; k++) {
@@ -473,6 +475,18 @@ __device__ __forceinline__ bool overlap_wall(const DevParams& P, const dem_wall&
     }
   }
   return ov;
+}
+
+// Overlap (src/MConfig.f90:692-822): Rectangle or Cone.  CONE = false
+// compiles the rectangle branch only, for kernels launched on systems without
+// cone walls (the cone branch costs registers wherever it is compiled in).
+template <bool CONE = true>
+__device__ __forceinline__ bool overlap_wall(const DevParams& P, const dem_wall& w,
+                                             const double x[3], double Ri, double& Dij,
+                                             double Nij[3], double Qji[3]) {
+  if (w.shape == DEM_WALL_RECTANGLE) return overlap_rect(P, w, x, Ri, Dij, Nij, Qji);
+  if (!CONE || w.shape != DEM_WALL_CONE) return false;
+  return overlap_cone(P, w, x, Ri, Dij, Nij, Qji);
 }
 
 // System parameters of particle p (or of cell c with a cell->system map).

@@ -1044,6 +1044,10 @@ __global__ void __launch_bounds__(128, MINB) k_pass_fp64(
   };
   // Force(i) = Force(i) + iForce where p's own block ends (src/MForces.f90:319-320)
   auto own = [&]() {
+    if (A.drag) {  // iForce = iForce + DragForce(iPart) (src/MForces.f90:316)
+#pragma unroll
+      for (int k = 0; k < 3; k++) iF[k] = iF[k] + A.drag[(size_t)3 * p + k];
+    }
 #pragma unroll
     for (int k = 0; k < 3; k++) F[k] = F[k] + iF[k];
 #pragma unroll

@@ -16,6 +16,7 @@
 #include "dem_kernels.cuh"
 #include "dem_mixed.cuh"
 #include "dem_remove.cuh"
+#include "dem_fluid.cuh"
 
 using namespace dem;
 
@@ -98,6 +99,14 @@ struct dem_ctx {
   dem_pouring pour{};
   dem_rng rng{0.0, 0, -1, -1, 0};
   std::vector<int> comp_count;  // Component(:)%Number
+  // fluid drag (FluidFlow): level tables Vf/Ef and the drag of every sphere
+  bool fluid = false;
+  FluidArgs fa{};
+  double* fl_vf = nullptr;  // [2*(NL+1)]: Vf then Ef
+  double* drag = nullptr;   // [3*ncap]
+  int drag_cap = 0;
+  double* amsum = nullptr;  // [9*ncap] corrector ring sums (predictor -> corrector)
+  int amsum_cap = 0;
   double2* pour_cand = nullptr;  // candidate points of one PourParticle call
   int* pour_fits = nullptr;
   int pour_cap = 0;
@@ -105,6 +114,7 @@ struct dem_ctx {
   int rm_cap = 0;
   long long rm_stats[3] = {0, 0, 0};  // removals, swaps, records renamed or moved
   int pass_variant = 0;  // pass kernel compiled for 4 (0) or 3 (1) blocks per SM
+  bool has_cone = false; // some wall of some system is a cone
   double skin_factor = 0.05;  // candidate-row skin / CutOff
   int par = 0;         // L.cell[par] is the assignment the lists hold
   int prepared = -1;   // side whose copies + next assignment are ready (-1: none)
@@ -375,6 +385,7 @@ int grow_history(dem_ctx* c, int need) {
 }
 
 StateArrays make_state(double* base, size_t n);
+int ensure_drag(dem_ctx* c);
 
 // Room for `newcap` particles in every per-particle array (the values of the
 // current n particles are kept; the per-pass copies, the candidate rows and
@@ -464,7 +475,7 @@ int grow_capacity(dem_ctx* c, int newcap) {
   c->prepared = -1;
   c->last_side = -1;
   CK(cudaStreamSynchronize(c->stream));
-  return DEM_OK;
+  return ensure_drag(c);
 }
 
 StateArrays make_state(double* base, size_t n) {
@@ -557,7 +568,41 @@ PassArgs<V4, W2> pass_args(dem_ctx* c, int side, bool update, double dt, const R
   A.rm = rm;
   A.cnt = c->cnt;
   A.tag = tag;
+  A.drag = c->fluid ? c->drag : nullptr;
+  A.amsum = c->amsum;
   return A;
+}
+
+// room for the drag of every sphere and the corrector ring sums (outside
+// graph capture)
+int ensure_drag(dem_ctx* c) {
+  if (c->nprev > 0 && c->amsum_cap < std::max(c->ncap, 1)) {
+    cudaFree(c->amsum);
+    c->amsum = nullptr;
+    c->amsum_cap = 0;
+    CK(cudaMalloc(&c->amsum, sizeof(double) * 9 * (size_t)std::max(c->ncap, 1)));
+    c->amsum_cap = std::max(c->ncap, 1);
+  }
+  if (!c->fluid || c->drag_cap >= std::max(c->ncap, 1)) return DEM_OK;
+  cudaFree(c->drag);
+  c->drag = nullptr;
+  c->drag_cap = 0;
+  CK(cudaMalloc(&c->drag, sizeof(double) * 3 * (size_t)std::max(c->ncap, 1)));
+  c->drag_cap = std::max(c->ncap, 1);
+  return DEM_OK;
+}
+
+// UpdateVelocityField + DragForce for the state the pass evaluates
+void fluid_prepare(dem_ctx* c, int side) {
+  if (!c->fluid || c->n == 0) return;
+  const StateArrays& Q = side ? c->Pr : c->P;
+  const int nl1 = c->fa.levels + 1;
+  launch(c, "fluid_levels", k_fluid_levels, (unsigned)nl1, (unsigned)FLUID_THREADS, c->fa, c->n,
+         (const double*)Q.pz, (const double*)Q.vz, (const int*)c->comp, c->fl_vf, c->fl_vf + nl1,
+         (const Counters*)c->cnt);
+  launch(c, "fluid_drag", k_fluid_drag, blocks_for(c->n, 256), 256u, c->fa, c->n, Q,
+         (const int*)c->comp, (const double*)c->fl_vf, (const double*)(c->fl_vf + nl1), c->drag,
+         (const Counters*)c->cnt);
 }
 
 void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, const RingMap& rm,
@@ -567,7 +612,9 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
   if (c->precision == DEM_PREC_MIXED) {
     auto A = pass_args<float4, float2>(c, side, update, dt, rm, tag, tgt);
     timed(c, "pass_mixed",
-          [&]() { mixed_pass(c->M, c->pp, epi, c->pass_variant, A, c->hcur, c->stream); });
+          [&]() {
+            mixed_pass(c->M, c->pp, epi, c->pass_variant, c->has_cone, A, c->hcur, c->stream);
+          });
     c->launches++;
     return;
   }
@@ -738,6 +785,7 @@ int force_pass(dem_ctx* c, int side, bool update, double dt, int epi, const Ring
     if (st) return st;
   }
   pass_lists(c, side, update, tag);
+  fluid_prepare(c, side);
   launch_pass_kernel(c, side, update, dt, epi, rm, tag);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(c, e, "pass kernel launch");
@@ -1384,6 +1432,9 @@ int dem_create_ensemble(const dem_params* ps, int32_t nsys, dem_ctx** out) {
   c->hcap = p->hist_capacity > 0 ? p->hist_capacity : 16;
   c->nsys = nsys;
   c->removal = nsys == 1;
+  for (int s = 0; s < nsys; s++)
+    for (int w = 0; w < ps[s].n_walls; w++)
+      if (ps[s].walls[w].shape == DEM_WALL_CONE) c->has_cone = true;
   c->hsys = hs;
   c->hp = hs[0];
   c->ncell_total = (int)ncell;
@@ -1451,6 +1502,9 @@ void dem_destroy(dem_ctx* c) {
   cudaFree(c->rm_buf);
   cudaFree(c->pour_cand);
   cudaFree(c->pour_fits);
+  cudaFree(c->fl_vf);
+  cudaFree(c->drag);
+  cudaFree(c->amsum);
   if (c->wall_slots) cudaFreeHost(c->wall_slots);
   cudaFree(c->cellsys);
   cudaFree(c->cnt);
@@ -1591,6 +1645,10 @@ int dem_set_state(dem_ctx* c, int32_t n, const int32_t* comp, const double* radi
   for (int k = 0; k < 5; k++) c->ringmap[k] = k;
   CK(cudaStreamSynchronize(c->stream));
   c->state_set = true;
+  {
+    int st = ensure_drag(c);
+    if (st) return st;
+  }
   c->cells_ready = false;
   sync_host_walls(c);  // walls keep their place; their motion restarts at Time = 0
   c->walls_moved = false;
@@ -2021,10 +2079,13 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
   // the Euler start-up does not
   const bool removal = c->removal && c->nsys == 1;
   c->stop_on_escape = removal;
-  auto remove_escaped = [&]() -> int {
+  // fresh: the host mirror of the counters was read after the last pass
+  auto remove_escaped = [&](bool fresh = false) -> int {
     if (!removal) return DEM_OK;
-    int s = read_counters(c);
-    if (s) return s;
+    if (!fresh) {
+      int s = read_counters(c);
+      if (s) return s;
+    }
     return c->hcnt->escaped ? update_particle_list_impl(c, nullptr) : DEM_OK;
   };
   if (first_step == 1) {
@@ -2160,7 +2221,7 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
       }
       step++;
     }
-    st = remove_escaped();  // escapes of the chunk's last step
+    st = remove_escaped(failed_pass < 0);  // escapes of the chunk's last step
     if (st) return st;
   }
   CK(cudaGetLastError());
@@ -2193,6 +2254,37 @@ int dem_get_ncol(dem_ctx* c, int64_t* ncol) {
   // API call returns), so its count is part of Ncol
   *ncol = (int64_t)(c->hcnt->ncol + c->hcnt->ncol_pending);
   return DEM_OK;
+}
+
+int dem_set_fluid(dem_ctx* c, const dem_fluid* f) {
+  if (!c) return DEM_ERR_INVALID;
+  drop_graphs(c);
+  if (!f) {
+    c->fluid = false;
+    return DEM_OK;
+  }
+  if (c->nsys > 1 || c->pp)
+    return fail(c, DEM_ERR_UNSUPPORTED, "fluid flow needs one system with a component table");
+  if (f->levels < 1 || !(f->viscosity > 0.0))
+    return fail(c, DEM_ERR_INVALID, "fluid: NL >= 1 and a positive viscosity");
+  // InitializeFluid (src/mFluid.f90:72-92)
+  FluidArgs& F = c->fa;
+  F.levels = f->levels;
+  F.area = c->params.lbox[0] * c->params.lbox[1];
+  F.dz = c->params.lbox[2] / (double)f->levels;
+  F.vf0 = f->flow_rate / F.area;
+  F.h2 = c->params.lbox[2] / 2.0;
+  F.density = f->density;
+  F.viscosity = f->viscosity;
+  for (int k = 0; k < NCM; k++) {
+    F.comp_density[k] = f->comp_density[k];
+    F.comp_radius[k] = c->params.comp_radius[k];
+  }
+  cudaFree(c->fl_vf);
+  c->fl_vf = nullptr;
+  CK(cudaMalloc(&c->fl_vf, sizeof(double) * 2 * (size_t)(f->levels + 1)));
+  c->fluid = true;
+  return ensure_drag(c);
 }
 
 int dem_set_pouring(dem_ctx* c, const dem_pouring* p) {

@@ -246,7 +246,9 @@ struct OwnerMixed {
 
 // MINB: resident blocks of 128 threads per SM the kernel is compiled for
 // (registers per thread <= 65536 / (128 * MINB)); the autotuner picks one.
-template <bool PP, int EPI, int MINB>
+// CONE: cone walls compiled in (only with MINB = 3: the branch costs
+// registers, and systems without cone walls launch CONE = false kernels).
+template <bool PP, int EPI, int MINB, bool CONE>
 __global__ void __launch_bounds__(128, MINB) k_pass_mixed(
     PassArgs<float4, float2> A, MixedView V) {
   // per warp: the current 32 contacts (candidate index, owner lane, partner)
@@ -386,7 +388,7 @@ __global__ void __launch_bounds__(128, MINB) k_pass_mixed(
       if (contacting) rec_read(V.rwa, V.rwb, V.rwc, wi, ft0, ft0lo, vt0);
       double Dij, Nij[3], Qji[3];
       bool ov = false;
-      ov = overlap_wall(P, W, xp, Rpd, Dij, Nij, Qji);
+      ov = overlap_wall<CONE>(P, W, xp, Rpd, Dij, Nij, Qji);
       if (ov) {
         n_wc++;
         const double Delta = Rpd * Rpd - Dij * Dij;
@@ -417,6 +419,9 @@ __global__ void __launch_bounds__(128, MINB) k_pass_mixed(
     }
   };
   auto own = [&]() {
+    if (A.drag)  // iForce = iForce + DragForce(iPart) (src/MForces.f90:316)
+      iF = iF + mk((float)A.drag[(size_t)3 * p], (float)A.drag[(size_t)3 * p + 1],
+                   (float)A.drag[(size_t)3 * p + 2]);
     F = F + iF;
     T = T + iT;
   };
@@ -612,7 +617,7 @@ bool mixed_grow_walls(MixedBuffers& M, int n, int stride, int cur, cudaStream_t 
   return true;
 }
 
-void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant,
+void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant, bool cone,
                 const PassArgs<float4, float2>& A, int cur, cudaStream_t st) {
   if (A.n == 0) return;
   MixedView V;
@@ -629,18 +634,22 @@ void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant,
   V.wwb = M.wb[cur ^ 1];
   V.wwc = M.wc[cur ^ 1];
   const unsigned g = blocks(A.n, 128);
-#define MCASE(PPV, MB)                                                                      \
-  do {                                                                                      \
-    if (epi == EPI_PREDICT) k_pass_mixed<PPV, EPI_PREDICT, MB><<<g, 128, 0, st>>>(A, V);     \
-    else if (epi == EPI_CORRECT) k_pass_mixed<PPV, EPI_CORRECT, MB><<<g, 128, 0, st>>>(A, V); \
-    else k_pass_mixed<PPV, EPI_STORE, MB><<<g, 128, 0, st>>>(A, V);                          \
+#define MCASE(PPV, MB, CN)                                                                   \
+  do {                                                                                       \
+    if (epi == EPI_PREDICT) k_pass_mixed<PPV, EPI_PREDICT, MB, CN><<<g, 128, 0, st>>>(A, V);  \
+    else if (epi == EPI_CORRECT)                                                             \
+      k_pass_mixed<PPV, EPI_CORRECT, MB, CN><<<g, 128, 0, st>>>(A, V);                       \
+    else k_pass_mixed<PPV, EPI_STORE, MB, CN><<<g, 128, 0, st>>>(A, V);                       \
   } while (0)
-  if (variant == 1) {
-    if (pp) MCASE(true, 3);
-    else MCASE(false, 3);
+  if (cone) {
+    if (pp) MCASE(true, 3, true);
+    else MCASE(false, 3, true);
+  } else if (variant == 1) {
+    if (pp) MCASE(true, 3, false);
+    else MCASE(false, 3, false);
   } else {
-    if (pp) MCASE(true, 4);
-    else MCASE(false, 4);
+    if (pp) MCASE(true, 4, false);
+    else MCASE(false, 4, false);
   }
 #undef MCASE
 }

@@ -233,15 +233,59 @@ __device__ __forceinline__ void epilogue(const PassArgs<V4, W2>& A, const DevPar
     return;
   }
   double sv[3] = {0.0, 0.0, 0.0}, sa[3] = {0.0, 0.0, 0.0}, sl[3] = {0.0, 0.0, 0.0};
-  for (int k = 0; k < P.nprev; k++) {
-    const double C = EPI == EPI_PREDICT ? P.ab[k] : P.am[k];
-    const double* rg = A.ring + (size_t)A.rm.phys[k] * 9 * n + p;
+  if (EPI == EPI_CORRECT && A.amsum) {
+    // sum_k AM(k)*Previous(ipc(k)) over the rotated ring, as the predictor
+    // pass formed it (same terms, same order)
 #pragma unroll
-    for (int d = 0; d < 3; d++) sv[d] = sv[d] + C * rg[d * n];
+    for (int d = 0; d < 3; d++) sv[d] = A.amsum[d * n + p];
 #pragma unroll
-    for (int d = 0; d < 3; d++) sa[d] = sa[d] + C * rg[(3 + d) * n];
+    for (int d = 0; d < 3; d++) sa[d] = A.amsum[(3 + d) * n + p];
 #pragma unroll
-    for (int d = 0; d < 3; d++) sl[d] = sl[d] + C * rg[(6 + d) * n];
+    for (int d = 0; d < 3; d++) sl[d] = A.amsum[(6 + d) * n + p];
+  } else {
+    // the predictor also forms the corrector's sums: after the ring rotation
+    // its slot k is this pass's (v, a, alpha) for k = 0, else the slot k-1
+    // read here
+    const bool am = EPI == EPI_PREDICT && A.amsum && P.nprev > 0;
+    double mv[3], ma[3], ml[3];
+    if (am) {
+#pragma unroll
+      for (int d = 0; d < 3; d++) mv[d] = 0.0 + P.am[0] * vp[d];
+#pragma unroll
+      for (int d = 0; d < 3; d++) ma[d] = 0.0 + P.am[0] * acc[d];
+#pragma unroll
+      for (int d = 0; d < 3; d++) ml[d] = 0.0 + P.am[0] * alp[d];
+    }
+    for (int k = 0; k < P.nprev; k++) {
+      const double C = EPI == EPI_PREDICT ? P.ab[k] : P.am[k];
+      const double* rg = A.ring + (size_t)A.rm.phys[k] * 9 * n + p;
+      double t[9];
+#pragma unroll
+      for (int d = 0; d < 9; d++) t[d] = rg[d * n];
+#pragma unroll
+      for (int d = 0; d < 3; d++) sv[d] = sv[d] + C * t[d];
+#pragma unroll
+      for (int d = 0; d < 3; d++) sa[d] = sa[d] + C * t[3 + d];
+#pragma unroll
+      for (int d = 0; d < 3; d++) sl[d] = sl[d] + C * t[6 + d];
+      if (am && k + 1 < P.nprev) {
+        const double M = P.am[k + 1];
+#pragma unroll
+        for (int d = 0; d < 3; d++) mv[d] = mv[d] + M * t[d];
+#pragma unroll
+        for (int d = 0; d < 3; d++) ma[d] = ma[d] + M * t[3 + d];
+#pragma unroll
+        for (int d = 0; d < 3; d++) ml[d] = ml[d] + M * t[6 + d];
+      }
+    }
+    if (am) {
+#pragma unroll
+      for (int d = 0; d < 3; d++) A.amsum[d * n + p] = mv[d];
+#pragma unroll
+      for (int d = 0; d < 3; d++) A.amsum[(3 + d) * n + p] = ma[d];
+#pragma unroll
+      for (int d = 0; d < 3; d++) A.amsum[(6 + d) * n + p] = ml[d];
+    }
   }
   double x[3], v[3], w[3];
   if (EPI == EPI_PREDICT) {

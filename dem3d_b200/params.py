@@ -130,6 +130,27 @@ def wall_motion(position, amplitude, frequency, phase, scales: "Scales | None" =
     return m
 
 
+def fluid(viscosity: float, flow_rate: float, levels: int, density: float, comp_density,
+          scales: "Scales | None" = None):
+    """FluidFlow settings (ReadFluidSpecifications, src/mFluid.f90:27-52):
+    viscosity, volumetric flow rate, NL levels, the fluid's and the
+    components' densities; with ``scales`` converted like
+    ScaleFluidProperties/ScaleVariables (src/mFluid.f90:56-68,
+    src/DEM.f90:826-858)."""
+    from ._abi import DemFluid
+    f = DemFluid()
+    L = scales.length if scales is not None else 1.0
+    M = scales.mass if scales is not None else 1.0
+    T = scales.time if scales is not None else 1.0
+    f.viscosity = viscosity * L * T / M
+    f.flow_rate = flow_rate * T / L ** 3
+    f.density = density * L ** 3 / M
+    for k, d in enumerate(comp_density):
+        f.comp_density[k] = d * L ** 3 / M
+    f.levels = int(levels)
+    return f
+
+
 def pouring(target_number, shape: int, size, max_attempts: int, interval: float,
             time_step: float, scales: "Scales | None" = None):
     """Pouring settings as ReadPouringFile and CalculateProperties derive them

@@ -31,8 +31,8 @@ import ctypes as C
 import numpy as np
 
 from . import _abi
-from ._abi import (MAX_WALLS, DemObservables, DemParams, DemPouring, DemRng, DemWall,
-                   DemWallMotion)
+from ._abi import (MAX_WALLS, DemFluid, DemObservables, DemParams, DemPouring, DemRng,
+                   DemWall, DemWallMotion)
 
 
 class DEMError(RuntimeError):
@@ -281,6 +281,11 @@ class DEMSystem:
         s = (C.c_int64 * 3)()
         self._call("get_removal_stats", s)
         return {"removed": s[0], "swaps": s[1], "records_moved": s[2]}
+
+    # -- fluid drag ----------------------------------------------------------
+    def set_fluid(self, fluid: DemFluid | None) -> None:
+        """FluidFlow with its settings (mFluid), or None for no fluid."""
+        self._call("set_fluid", None if fluid is None else C.byref(fluid))
 
     # -- pouring -------------------------------------------------------------
     def set_pouring(self, pouring: DemPouring | None) -> None:

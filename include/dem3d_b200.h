@@ -156,6 +156,19 @@ typedef struct dem_rng {
   int32_t dummy, iix, iiy, iik;
 } dem_rng;
 
+/* Fluid drag (mFluid, src/mFluid.f90): a one-dimensional upward flow through
+ * the bed, its velocity and porosity averaged over NL+1 horizontal levels
+ * (UpdateVelocityField, :96-139), drives a drag force on every sphere
+ * (DragForce, :143-197).  Simulation units (after ScaleFluidProperties). */
+typedef struct dem_fluid {
+  double viscosity;                        /* FluidViscosity */
+  double flow_rate;                        /* FluidFlowRate */
+  double density;                          /* FluidDensity */
+  double comp_density[DEM_MAX_COMPONENTS]; /* Component(:)%Density */
+  int32_t levels;                          /* NL */
+  int32_t pad_;
+} dem_fluid;
+
 typedef struct dem_ctx dem_ctx;
 
 /* Library build/version string (also proves the .so loads). */
@@ -297,6 +310,10 @@ int dem_pour_particle(dem_ctx* ctx, int32_t* inserted);
 /* The generator state, as SaveState/ReadState keep it (src/DEM.f90:995-999). */
 int dem_set_rng(dem_ctx* ctx, const dem_rng* rng);
 int dem_get_rng(dem_ctx* ctx, dem_rng* rng);
+
+/* FluidFlow with its settings (NULL: off).  Single-system contexts with a
+ * component table; InitializeFluid (src/mFluid.f90:72-92) is done here. */
+int dem_set_fluid(dem_ctx* ctx, const dem_fluid* fluid);
 
 /* Ncol (src/MForces.f90:47,227). */
 int dem_get_ncol(dem_ctx* ctx, int64_t* ncol);

@@ -116,6 +116,11 @@ typedef struct orc_ctx {
   int moving;               /* WallsInMovement */
   int removal;              /* run() calls UpdateParticleList after each step */
   int pouring;              /* run() calls PouringAttempt before each step */
+  int fluid;                /* FluidFlow */
+  dem_fluid fl;
+  double fl_area, fl_dz, fl_vf0, fl_h2, fl_mh2;  /* InitializeFluid */
+  double* vf;               /* Vf(0:NL) */
+  double* ef;               /* Ef(0:NL) */
   dem_pouring pour;
   dem_rng rng;              /* ranf's state (src/MUtil.f90:10-11) */
   int32_t comp_count[NCM];  /* Component(:)%Number */
@@ -738,6 +743,79 @@ static int overlap_wall(const orc_ctx* c, const OParticle* ip, const dem_wall* w
   return ov;
 }
 
+/* ------------------------------------------------------------------ */
+/* mFluid                                                                */
+
+static const double FL_PI = 3.1415926535897932384626433832795; /* src/MUtil.f90 */
+
+/* UpdateVelocityField (src/mFluid.f90:96-139) */
+static void update_velocity_field(orc_ctx* c, const OParticle* P) {
+  for (int32_t k = 0; k <= c->fl.levels; k++) {
+    const double Zk = c->fl_mh2 + (double)k * c->fl_dz;
+    double SumA = 0.0, SumB = 0.0, SumC = 0.0;
+    for (int32_t i = 0; i < c->n; i++) {
+      const int32_t ind = P[i].index;
+      const double d = Zk - P[i].pos[2];
+      const double Diff2 = d * d;
+      const double R = c->p.comp_radius[ind];
+      const double R2 = R * R;
+      if (Diff2 < R2) {
+        const double Ai = FL_PI * (R2 - Diff2);
+        SumA = SumA + Ai;
+        const double DensAi = Ai * c->fl.comp_density[ind];
+        SumB = SumB + DensAi * P[i].vel[2];
+        SumC = SumC + DensAi;
+      }
+    }
+    if (SumA == 0.0) {
+      c->vf[k] = c->fl_vf0;
+      c->ef[k] = 1.0;
+    } else {
+      const double Es = SumA / c->fl_area;
+      c->ef[k] = 1.0 - Es;
+      const double Vs = SumB / SumC;
+      c->vf[k] = (c->fl_vf0 - Es * Vs) / c->ef[k];
+    }
+  }
+}
+
+/* DragForce (src/mFluid.f90:143-197).  The level index is kept inside
+ * 0..NL-1 (the reference would read past Vf(NL) for a sphere above the box). */
+static void drag_force(const orc_ctx* c, const OParticle* ip, double FD[3]) {
+  const double Zi = ip->pos[2];
+  const double jr = (Zi + c->fl_h2) / c->fl_dz;
+  int32_t j = (int32_t)jr;
+  if (j < 0) j = 0;
+  if (j > c->fl.levels - 1) j = c->fl.levels - 1;
+  double Vfz = c->vf[j];
+  Vfz = Vfz + (jr - (double)j) * (c->vf[j + 1] - Vfz);
+  double Efz = c->ef[j];
+  Efz = Efz + (jr - (double)j) * (c->ef[j + 1] - Efz);
+  double Vr[3] = {-ip->vel[0], -ip->vel[1], -ip->vel[2]};
+  Vr[2] = Vfz + Vr[2];
+  const double Vra = sqrt((Vr[0] * Vr[0] + Vr[1] * Vr[1]) + Vr[2] * Vr[2]);
+  if (Vra > 0.0) {
+    const double Ri = c->p.comp_radius[ip->index];
+    const double Re = 2.0 * Efz * Ri * Vra * c->fl.density / c->fl.viscosity;
+    double n = 3.6, n0 = n + 1.0, x = 0.0;
+    for (int it = 0; fabs(n - n0) > 1.e-8 && it < 1000; it++) {
+      n0 = n;
+      x = Re / pow(Efz, n);
+      const double x75 = pow(x, 0.75);
+      n = (4.8 + 0.42 * x75) / (1.0 + 0.175 * x75);
+    }
+    double a = 0.63 + 4.8 / sqrt(x);
+    const double Cd1 = a * a;
+    a = 0.63 + 4.8 / sqrt(Re);
+    const double CD = a * a;
+    const double fi = (Cd1 / CD) * pow(Efz, 2.0 * (1.0 - n));
+    const double s = CD * (FL_PI / 2.0) * Ri * Ri * c->fl.density * Vra;
+    for (int k = 0; k < 3; k++) FD[k] = s * Vr[k] * fi;
+  } else {
+    FD[0] = FD[1] = FD[2] = 0.0;
+  }
+}
+
 /* ComputeAccelerations, src/MForces.f90:145-335 */
 static int compute_accelerations(orc_ctx* c, OParticle* P, double TimeStep, int Update) {
   const int32_t n = c->n;
@@ -746,6 +824,7 @@ static int compute_accelerations(orc_ctx* c, OParticle* P, double TimeStep, int 
   memset(c->force, 0, sizeof(double) * 3 * (size_t)n);
   memset(c->torque, 0, sizeof(double) * 3 * (size_t)n);
   for (int w = 0; w < NWM; w++) c->wall_fn[w] = 0.0;
+  if (c->fluid) update_velocity_field(c, P);
   for (int32_t iCell = 0; iCell < c->Nt; iCell++) {
     int32_t NPCC, NPSC;
     if (!neighbour_particles(c, iCell, &NPCC, &NPSC)) {
@@ -822,6 +901,11 @@ static int compute_accelerations(orc_ctx* c, OParticle* P, double TimeStep, int 
         } else {
           if (c->Contacting && Update) remove_contact(c, c->iwall, &c->mainp[c->imin].first_wall);
         }
+      }
+      if (c->fluid) { /* iForce = iForce + DragForce(iPart), src/MForces.f90:316 */
+        double FD[3];
+        drag_force(c, &iPart, FD);
+        for (int k = 0; k < 3; k++) c->iForce[k] = c->iForce[k] + FD[k];
       }
       for (int k = 0; k < 3; k++) c->force[3 * i + k] = c->force[3 * i + k] + c->iForce[k];
       for (int k = 0; k < 3; k++) c->torque[3 * i + k] = c->torque[3 * i + k] + c->iTorque[k];
@@ -1366,6 +1450,8 @@ void orc_destroy(orc_ctx* c) {
   free(c->neighbour);
   free(c->force);
   free(c->torque);
+  free(c->vf);
+  free(c->ef);
   free(c);
 }
 
@@ -1616,6 +1702,28 @@ int orc_set_cells(orc_ctx* c, const int32_t* traversal, const int32_t* cell_star
     for (int32_t k = cell_start[cc + 1] - 1; k >= cell_start[cc]; k--)
       add_particle(c, traversal[k], cc);  /* prepending in reverse keeps the order */
   c->cells_ready = 1;
+  return DEM_OK;
+}
+
+/* FluidFlow and InitializeFluid (src/mFluid.f90:72-92) */
+int orc_set_fluid(orc_ctx* c, const dem_fluid* f) {
+  if (!c) return DEM_ERR_INVALID;
+  free(c->vf);
+  free(c->ef);
+  c->vf = c->ef = NULL;
+  c->fluid = 0;
+  if (!f) return DEM_OK;
+  if (c->p.n_components <= 0) return DEM_ERR_UNSUPPORTED;
+  if (f->levels < 1 || !(f->viscosity > 0.0)) return DEM_ERR_INVALID;
+  c->fl = *f;
+  c->fl_area = c->p.lbox[0] * c->p.lbox[1];
+  c->fl_dz = c->p.lbox[2] / (double)f->levels;
+  c->fl_vf0 = f->flow_rate / c->fl_area;
+  c->fl_h2 = c->p.lbox[2] / 2.0;
+  c->fl_mh2 = -c->fl_h2;
+  c->vf = (double*)calloc((size_t)f->levels + 1, sizeof(double));
+  c->ef = (double*)calloc((size_t)f->levels + 1, sizeof(double));
+  c->fluid = 1;
   return DEM_OK;
 }
 
