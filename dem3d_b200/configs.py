@@ -182,6 +182,43 @@ def discharge(n=360, seed=1014, e=0.7, mu=0.5, dt=4e-4, gravity=20.0, v_down=6.0
                     info={"lbox": (L, L, lz), "seed": seed})
 
 
+def ball_bearings(precision=P.PREC_FP64, pouring_interval=0.5, max_ncell=30000):
+    """The reference's shipped example, examples/ball-bearings/ball-bearings.inp
+    and ball-bearings.prg, with its values in SI units and scaled as the
+    reference scales them (ScaleVariables): an empty 0.11 x 0.11 x 0.05 m box
+    with five cone walls (two of them flat discs, one a flat annulus), all
+    orbiting on 1 cm circles at 1.5 Hz (WallsInMovement), and 1 cm steel
+    spheres poured from a 2 cm circle every ``pouring_interval`` seconds
+    (0.5 s in the example) up to 39 spheres, 10 attempts each; e = 0.7,
+    mu = 0.3, gravity 9.8 m/s^2, ABM4 with 10 steps per collision and 100
+    Euler sub-steps, 30 s simulated.  Returns (Workload with no spheres,
+    wall motions, pouring settings, generator seed)."""
+    comps = [P.Component(0, 0.01, 7.8e3, 1.e5, 1.e5)]
+    # shape 2 = cone: L1 (height), L2, L3 (end diameters), stiffnesses,
+    # position, U, W -- the NW rows of the example
+    rows = [(0.015, 0.070, 0.070, -0.0165), (0.000, 0.000, 0.070, -0.0240),
+            (0.016, 0.072, 0.072, -0.0170), (0.000, 0.000, 0.072, -0.0250),
+            (0.000, 0.070, 0.072, -0.0090)]
+    walls = [P.cone((0.01, 0.0, z), l1, l2, l3, u=(0.0, 0.0, 1.0), w=(0.0, 1.0, 0.0),
+                    stiffness=1.e5, shear_stiffness=1.e5) for l1, l2, l3, z in rows]
+    nw = len(walls)
+    prm, sc = P.component_params(
+        comps, walls, [[0.7]], [[0.7]], [[0.3]], [[0.7] * nw], [[0.7] * nw], [[0.3] * nw],
+        lbox=(0.11, 0.11, 0.05), pbc=(False, False, False), gravity=(0.0, 0.0, -9.8),
+        method_order=4, euler_intervals=100, max_ncell=max_ncell, min_steps_per_collision=10.0,
+        total_time=30.0, fluid_density=0.0, scale=True, precision=precision)
+    # V = -2*Pi*A*sin(2*Pi*(f*t + phi)): A = (0.01, 0.01, 0), f = 1.5 Hz, phi = (0, -0.25, 0)
+    motion = [P.wall_motion(w.position, (0.01, 0.01, 0.0), (1.5, 1.5, 1.5), (0.0, -0.25, 0.0),
+                            scales=sc) for w in walls]
+    ts = prm.time_step * sc.time  # the time step in seconds
+    pour = P.pouring([39], P.POUR_CIRCLE, (0.02,), 10, pouring_interval, ts, scales=sc)
+    empty = np.zeros((0, 3))
+    w = Workload("ball_bearings", prm, empty, empty.copy(), empty.copy(),
+                 comp=np.zeros(0, dtype=np.int32),
+                 info={"scales": sc, "steps": int(round(30.0 / ts))})
+    return w, motion, pour, -20
+
+
 def hopper(n=600, seed=1005, e=0.7, mu=0.5, dt=1e-4, gravity=1.0, length=10.0, d_out=3.0,
            d_in=14.0, method_order=4, euler_intervals=20, precision=P.PREC_FP64,
            sigma_v=1.0, v_radial=3.0, max_ncell=30000):

@@ -27,8 +27,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from ._abi import (MAX_COMPONENTS, MAX_WALLS, PREC_FP64, PREC_MIXED,  # noqa: F401
-                   WALL_CONE, WALL_RECTANGLE, DemParams, DemWall)
+from ._abi import (MAX_COMPONENTS, MAX_WALLS, POUR_CIRCLE, POUR_RECTANGLE,  # noqa: F401
+                   PREC_FP64, PREC_MIXED, WALL_CONE, WALL_RECTANGLE, DemParams, DemWall)
 
 PI = 3.141592653589793238  # the reference's literal (src/DEM.f90:249)
 
