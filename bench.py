@@ -367,15 +367,38 @@ def measure(s, w, args, world, local, torch, dist):
     if world > 1:
         dist.barrier()
     l0 = s.launch_count()
+    steps_done = args.steps
+    retunes = []
     with ClockSampler(local) as clk:
         # NVTX range "dem_timed": lets a profiler select exactly these launches
         torch.cuda.nvtx.range_push("dem_timed")
-        ms = s.run_timed(first, last)
+        if args.retune_every > 0 and tuning is not None:
+            # long runs whose dynamics change: the autotuner's trials (real
+            # steps of the same run) again every `retune_every` steps
+            s.timer_start()
+            step, steps_done = first, 0
+            while steps_done < args.steps:
+                seg = min(args.retune_every, args.steps - steps_done)
+                s.run(step, step + seg - 1)
+                step += seg
+                steps_done += seg
+                if steps_done < args.steps:
+                    t = s.autotune(step, 40)
+                    retunes.append((step, t["skin_factor"], t["pass_variant"]))
+                    steps_done += t["last_step"] - step + 1
+                    step = t["last_step"] + 1
+            ms = s.timer_stop()
+            last = step - 1
+        else:
+            ms = s.run_timed(first, last)
         torch.cuda.nvtx.range_pop()
     launches = s.launch_count() - l0
     ms = reduce_max(ms, world)
+    if retunes:
+        tuning = dict(tuning, retunes=retunes, steps_timed=steps_done)
     return {"ms": ms, "launches": launches, "last": last, "clocks": clk.summary(),
-            "value": aggregate_rate(w.n, world, args.steps, ms), "tuning": tuning}
+            "value": aggregate_rate(w.n, world, steps_done, ms), "tuning": tuning,
+            "steps": steps_done}
 
 
 def force_error(w_fp64, w_mixed, src):
@@ -513,7 +536,7 @@ def run_ours(args):
     if tr and dom in tr.get("bytes_per_particle", {}):
         traffic = tr["bytes_per_particle"][dom] * n
     step_b = step_bytes_per_particle(mixed, z_pp, m_cand, z_pw, nw)
-    step_gbs = step_b * n / (ms / args.steps / 1000.0) / 1e9
+    step_gbs = step_b * n / (ms / res[headline]["steps"] / 1000.0) / 1e9
 
     # e2e: a driver that keeps Particle(1:n) on the host: each step uploads
     # positions, velocities and angular velocities from pinned host memory,
@@ -555,12 +578,13 @@ def run_ours(args):
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "steps": res[headline]["steps"], "warmup": args.warmup,
+            "ms_per_step": ms / res[headline]["steps"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if headline == "fp64" else "f32+f64", "data": "synthetic",
             "config": config_block(args.workload, w, world, headline),
             "gpu_launches": int(launches),
-            "precisions": {p: {"value": r["value"], "ms_per_step": r["ms"] / args.steps,
+            "precisions": {p: {"value": r["value"], "ms_per_step": r["ms"] / r["steps"],
                                "tuning": r["tuning"]}
                            for p, r in res.items()},
             "mixed_over_fp64": (res["mixed"]["value"] / res["fp64"]["value"]
@@ -672,8 +696,8 @@ def run_ensemble(args):
     if rank == 0:
         value = res["value"]
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": res["ms"] / args.steps,
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": res["steps"],
+            "warmup": args.warmup, "ms_per_step": res["ms"] / res["steps"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64" if prec == "mixed" else "f64", "data": "synthetic",
             "config": {"workload": (f"{len(e.counts)} gravity-settling systems, sizes log-uniform "
@@ -713,6 +737,8 @@ def main():
     ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--retune-every", type=int, default=0,
+                    help="run the autotuner's trials again every N timed steps (0: never)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="skip the autotuner's trials (default settings)")
     args = ap.parse_args()
