@@ -499,6 +499,17 @@ def run_ours(args):
         rel = {k: (abs(pick["mixed"][k] - pick["fp64"][k]) / abs(pick["fp64"][k])
                    if pick["fp64"][k] else None) for k in pick["fp64"]}
         obs_cmp = {"after_step": res["fp64"]["last"], **pick, "rel_diff": rel}
+    cell_occ = None
+    if WORKLOADS[args.workload].get("kind") == "bidisperse":
+        # cell-cost imbalance: cells are sized by the large spheres, so a cell
+        # of small ones holds many; spheres per occupied cell at the end
+        _, _, cs = systems[headline].get_cells()
+        cnt = np.diff(cs)
+        occ = cnt[cnt > 0]
+        cell_occ = {"cells": int(cnt.size), "occupied": int(occ.size),
+                    "mean_per_occupied_cell": float(occ.mean()) if occ.size else 0.0,
+                    "p99": float(np.percentile(occ, 99)) if occ.size else 0.0,
+                    "max": int(occ.max()) if occ.size else 0}
     for prec, sy in systems.items():
         if prec != headline:
             sy.close()
@@ -606,6 +617,8 @@ def run_ours(args):
             "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
             "gen_s": round(t_gen, 2),
         }
+        if cell_occ is not None:
+            line["cell_occupancy"] = cell_occ
         print(json.dumps(line), flush=True)
     s.close()
     if world > 1:
