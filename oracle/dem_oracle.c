@@ -103,6 +103,7 @@ typedef struct orc_ctx {
   int32_t* neighbour;
   int32_t neighbour_cap;
   int32_t literal_neighbour_cap; /* 0 = growable, else hard cap (reference: 50) */
+  int32_t literal_removal;       /* 1: renamed records appended as the reference does */
   double* force;
   double* torque;
   /* MForces module variables (src/MForces.f90:36-44) */
@@ -1057,7 +1058,9 @@ static int move_particles(orc_ctx* c, int32_t step) {
 
 /* AllNeighbourParticles (src/MCells.f90:833-860) over the MonteCarlo list
  * of iCell (NeighbourCells3D with MonteCarlo, :353-375, AddAllNeighbours3D
- * :424-476): the particles of iCell, then of each neighbour cell. */
+ * :424-476): the particles of iCell, then of each neighbour cell in list
+ * order -- AddNeighbour prepends (:666-680), so the list runs opposite to
+ * the loops that build it. */
 static int32_t all_neighbour_particles(orc_ctx* c, int32_t iCell, int32_t** out) {
   int32_t iz = iCell / (c->Nx * c->Ny);
   int32_t iy = iCell / c->Nx - iz * c->Ny;
@@ -1074,8 +1077,7 @@ static int32_t all_neighbour_particles(orc_ctx* c, int32_t iCell, int32_t** out)
       if (I[d] == N[d] - 1) hi[d] = 0;
     }
   }
-  int32_t cells[27], m = 0;
-  cells[m++] = iCell;
+  int32_t built[26], nb_cells = 0;
   for (int32_t kz = lo[2]; kz <= hi[2]; kz++)
     for (int32_t ky = lo[1]; ky <= hi[1]; ky++)
       for (int32_t kx = lo[0]; kx <= hi[0]; kx++) {
@@ -1086,8 +1088,11 @@ static int32_t all_neighbour_particles(orc_ctx* c, int32_t iCell, int32_t** out)
             if (j[d] == N[d]) j[d] = 0;
             if (j[d] == -1) j[d] = N[d] - 1;
           }
-        cells[m++] = j[0] + c->Nx * (j[1] + c->Ny * j[2]);
+        built[nb_cells++] = j[0] + c->Nx * (j[1] + c->Ny * j[2]);
       }
+  int32_t cells[27], m = 0;
+  cells[m++] = iCell;
+  for (int32_t k = nb_cells - 1; k >= 0; k--) cells[m++] = built[k];
   int32_t cnt = 0;
   for (int k = 0; k < m; k++)
     for (CNode* q = c->cell[cells[k]].first_particle; q; q = q->next) cnt++;
@@ -1196,9 +1201,14 @@ static void change_index_in_contact_list(orc_ctx* c, int32_t NP, int32_t i, int3
         cur->index = j;
         if (prev) prev->next = NULL;
         else c->mainp[j].first_partner = NULL;
-        /* ordered insert into i's new list (see above) */
         Partner** at = &first;
-        while (*at && (*at)->index < j) at = &(*at)->next;
+        if (c->literal_removal) {
+          /* the reference's append in neighbour order (src/MContacts.f90:225-241) */
+          while (*at) at = &(*at)->next;
+        } else {
+          /* ordered insert into i's new list (see above) */
+          while (*at && (*at)->index < j) at = &(*at)->next;
+        }
         cur->next = *at;
         *at = cur;
       }
@@ -1453,6 +1463,12 @@ void orc_destroy(orc_ctx* c) {
   free(c->vf);
   free(c->ef);
   free(c);
+}
+
+/* test hook: the reference's unordered append in ChangeIndexInContactList */
+int orc_set_literal_removal(orc_ctx* c, int32_t on) {
+  c->literal_removal = on != 0;
+  return DEM_OK;
 }
 
 int orc_set_literal_neighbour_cap(orc_ctx* c, int32_t cap) {

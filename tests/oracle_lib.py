@@ -24,6 +24,8 @@ def load_oracle(variant: str = "libdem_oracle.so") -> C.CDLL:
     _abi.bind(lib, "orc_", _abi.SIGNATURES)
     lib.orc_set_literal_neighbour_cap.argtypes = [C.c_void_p, C.c_int32]
     lib.orc_set_literal_neighbour_cap.restype = C.c_int
+    lib.orc_set_literal_removal.argtypes = [C.c_void_p, C.c_int32]
+    lib.orc_set_literal_removal.restype = C.c_int
     _CACHE[variant] = lib
     return lib
 

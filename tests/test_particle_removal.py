@@ -15,7 +15,9 @@ from tests.oracle_lib import oracle_system
 
 def neighbourhood(cell, grid, pbc):
     """The cell and its MonteCarlo neighbour cells (NeighbourCells3D,
-    src/MCells.f90:353-375, VerifyPBC/ApplyPBC :1030-1052)."""
+    src/MCells.f90:353-375, VerifyPBC/ApplyPBC :1030-1052) in list order:
+    AddNeighbour prepends (:666-680), so the neighbours come in the reverse
+    of the loop order."""
     nx, ny, nz = grid
     iz = cell // (nx * ny)
     iy = cell // nx - iz * ny
@@ -27,7 +29,7 @@ def neighbourhood(cell, grid, pbc):
             lo = 0 if c == 0 else -1
             hi = 0 if c == n - 1 else 1
         ranges.append((lo, hi))
-    out = [cell]
+    out = []
     for kz in range(ranges[2][0], ranges[2][1] + 1):
         for ky in range(ranges[1][0], ranges[1][1] + 1):
             for kx in range(ranges[0][0], ranges[0][1] + 1):
@@ -38,11 +40,13 @@ def neighbourhood(cell, grid, pbc):
                     if p:
                         j[d] = 0 if j[d] == n else (n - 1 if j[d] == -1 else j[d])
                 out.append(j[0] + nx * (j[1] + ny * j[2]))
-    return out
+    return [cell] + out[::-1]
 
 
-def restated_removal(state, lbox, grid, pbc):
-    """UpdateParticleList over plain Python lists (independent of the C code)."""
+def restated_removal(state, lbox, grid, pbc, literal=False):
+    """UpdateParticleList over plain Python lists (independent of the C code).
+    literal: the records particle i inherits keep the reference's append
+    order instead of being ordered by partner."""
     pos = [list(p) for p in state["pos"]]
     vel = [list(v) for v in state["vel"]]
     ring = [list(map(list, slot)) for slot in state["prev"]]
@@ -87,7 +91,7 @@ def restated_removal(state, lbox, grid, pbc):
                 else:
                     rec[0] = j
                     first.append(rec)
-            pairs[i] = sorted(first)
+            pairs[i] = first if literal else sorted(first)
             walls[i], walls[NP] = walls[NP], []
             pairs[NP] = []
         n -= 1
@@ -184,3 +188,34 @@ def test_run_removes_after_every_step_and_can_be_switched_off():
     L = np.array(list(w.params.lbox))
     pa = a.get_state()["pos"]
     assert not np.any((pa > 0.5 * L) | (pa < -0.5 * L))
+
+
+def test_literal_append_order_shows_the_deviation():
+    """The reference appends the records particle i inherits in neighbour
+    order (src/MContacts.f90:225-241); its ordered search (VerifyPairContact,
+    src/MContacts.f90:329-372) then misses the later of two out-of-order
+    records, and the next updating pass adds a second record for that pair.
+    The oracle's literal mode does exactly that; the default mode (the one
+    the GPU follows) keeps the list ordered and the history of the pair."""
+    from tests.oracle_lib import load_oracle
+    lib = load_oracle()
+    after = {}
+    for literal in (0, 1):
+        w, o = dense_case(oracle_system, seed=51)
+        lib.orc_set_literal_removal(o._ctx, literal)
+        pos = o.get_state()["pos"].copy()
+        pos[531, 0] = 0.51 * w.params.lbox[0]  # particle 531 leaves; the last one replaces it
+        o.update_state(pos=pos)
+        want = restated_removal(export(o), list(w.params.lbox), o.grid(), [1, 1, 1],
+                                literal=bool(literal))
+        assert o.update_particle_list() == 1
+        ct = o.get_contacts()
+        np.testing.assert_array_equal(ct["imin"], want["imin"])
+        np.testing.assert_array_equal(ct["imax"], want["imax"])
+        inherited = list(ct["imax"][ct["imin"] == 531])
+        assert inherited == ([592, 591] if literal else [591, 592])
+        o.compute_accelerations(update=True)
+        ct = o.get_contacts()
+        after[literal] = list(ct["imax"][ct["imin"] == 531])
+    assert after[0] == [591, 592]
+    assert sorted(after[1]) == [591, 591, 592]  # two records for one pair
