@@ -143,6 +143,7 @@ SIGNATURES = {
     "get_cells": (C.c_int, [_P, _I32P, _I32P, _I32P]),
     "set_cells": (C.c_int, [_P, _I32P, _I32P]),
     "compute_accelerations": (C.c_int, [_P, C.c_int32, C.c_double, C.c_int32]),
+    "compute_forces": (C.c_int, [_P, C.c_int32, C.c_double, C.c_int32, _DP, _DP]),
     "move_particles": (C.c_int, [_P, C.c_int32]),
     "move_particles_euler": (C.c_int, [_P]),
     "run": (C.c_int, [_P, C.c_int32, C.c_int32]),

@@ -193,8 +193,12 @@ struct PassArgs {
   Counters* cnt;
   int tag;  // 2*(step within a captured chunk) + pass
   const double* drag;  // [3n] fluid drag of every sphere (NULL: no fluid)
-  // the corrector's ring sums sum_k AM(k)*Previous(ipc(k)) (v, a, alpha:
-  // [9][n]), formed by the predictor pass, which holds every term of them
+  // EPI_PREDICT/EPI_CORRECT: the corrector's ring sums sum_k AM(k)*
+  // Previous(ipc(k)) (v, a, alpha: [9][n]), formed by the predictor pass,
+  // which holds every term of them.  EPI_STORE: ComputeAccelerations'
+  // Force(i) and Torque(i) before the division by mass and inertia
+  // (src/MForces.f90:319-333) as amsum[3p+k], then amsum[3n+3p+k]; NULL: not
+  // kept
   double* amsum;
 };
 

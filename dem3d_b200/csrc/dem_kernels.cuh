@@ -1080,6 +1080,13 @@ __global__ void __launch_bounds__(128, MINB) k_pass_fp64(
       }
       need = hw_n;
     }
+    if (EPI == EPI_STORE && A.amsum) {
+      const size_t n3 = (size_t)3 * A.n;
+#pragma unroll
+      for (int k = 0; k < 3; k++) A.amsum[(size_t)3 * p + k] = F[k];
+#pragma unroll
+      for (int k = 0; k < 3; k++) A.amsum[n3 + (size_t)3 * p + k] = T[k];
+    }
     // ---- a = F/m, alpha = T/I (src/MForces.f90:330-333) + epilogue
     double acc[3], alp[3];
 #pragma unroll

@@ -131,6 +131,7 @@ struct dem_ctx {
   double* obs_partial = nullptr;
 
   double* staging = nullptr;  // 15*n doubles, rows layout for host I/O
+  double* force_out = nullptr;  // set during dem_compute_forces: Force, Torque rows
   cudaEvent_t timer[2] = {nullptr, nullptr};
 
   int ringmap[5] = {0, 1, 2, 3, 4};
@@ -611,6 +612,7 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
   const StateArrays& tgt = side ? c->Pr : c->P;
   if (c->precision == DEM_PREC_MIXED) {
     auto A = pass_args<float4, float2>(c, side, update, dt, rm, tag, tgt);
+    if (epi == EPI_STORE) A.amsum = c->force_out;
     timed(c, "pass_mixed",
           [&]() {
             mixed_pass(c->M, c->pp, epi, c->pass_variant, c->has_cone, A, c->hcur, c->stream);
@@ -619,6 +621,7 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
     return;
   }
   auto A = pass_args<double4, double2>(c, side, update, dt, rm, tag, tgt);
+  if (epi == EPI_STORE) A.amsum = c->force_out;
   const unsigned g = blocks_for(c->n, 128);
 #define PASS_CASE(PPV, MB)                                                              \
   do {                                                                                  \
@@ -2040,6 +2043,32 @@ int dem_compute_accelerations(dem_ctx* c, int32_t use_predicted, double time_ste
   CK(cudaGetLastError());
   st = read_counters(c);
   return st;
+}
+
+// ComputeAccelerations with its Force and Torque arrays (src/MForces.f90:154,
+// summed at :319-320 and divided at :330-333) copied out as rows of three.
+// The pass kernel writes them into the host I/O staging buffer, which holds
+// 15 doubles per particle.
+int dem_compute_forces(dem_ctx* c, int32_t use_predicted, double time_step, int32_t update,
+                       double* force, double* torque) {
+  if (!c || !force || !torque) return DEM_ERR_INVALID;
+  int st = validate_ready(c);
+  if (st) return st;
+  c->force_out = c->staging;
+  st = force_pass(c, use_predicted ? 1 : 0, update != 0, time_step, EPI_STORE, current_map(c),
+                  true, 0);
+  c->force_out = nullptr;
+  if (st) return st;
+  CK(cudaGetLastError());
+  st = read_counters(c);
+  if (st) return st;
+  const size_t n3 = (size_t)3 * c->n;
+  if (n3 == 0) return DEM_OK;
+  CK(cudaMemcpyAsync(force, c->staging, sizeof(double) * n3, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(torque, c->staging + n3, sizeof(double) * n3, cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DEM_OK;
 }
 
 int dem_move_particles(dem_ctx* c, int32_t step) {

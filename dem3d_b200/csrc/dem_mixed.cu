@@ -449,6 +449,11 @@ __global__ void __launch_bounds__(128, MINB) k_pass_mixed(
       }
       need = hw_n;
     }
+    if (EPI == EPI_STORE && A.amsum) {
+      const size_t n3 = (size_t)3 * A.n, q = (size_t)3 * p;
+      A.amsum[q] = F.x; A.amsum[q + 1] = F.y; A.amsum[q + 2] = F.z;
+      A.amsum[n3 + q] = T.x; A.amsum[n3 + q + 1] = T.y; A.amsum[n3 + q + 2] = T.z;
+    }
     const double acc[3] = {(double)(F.x * inv_m), (double)(F.y * inv_m), (double)(F.z * inv_m)};
     const double alp[3] = {(double)(T.x * inv_i), (double)(T.y * inv_i), (double)(T.z * inv_i)};
     // the integrator runs on FP64 velocities: Particle's for the predictor,

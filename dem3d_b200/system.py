@@ -12,6 +12,7 @@ DEMSystem method                   reference routine
 ``initialize_cell_distribution``    InitializeCellDistribution
                                     (src/MForces.f90:110)
 ``compute_accelerations``           ComputeAccelerations (src/MForces.f90:145)
+``compute_forces``                  the same, with its Force/Torque arrays
 ``move_particles``                  MoveParticles (src/MDEM.f90:285)
 ``move_particles_euler``            MoveParticlesEuler (src/MDEM.f90:258)
 ``run``                             main loop, src/DEM.f90:85-99
@@ -231,6 +232,17 @@ class DEMSystem:
     def compute_accelerations(self, use_predicted=False, time_step=None, update=True):
         ts = float(self.params.time_step if time_step is None else time_step)
         self._call("compute_accelerations", 1 if use_predicted else 0, ts, 1 if update else 0)
+
+    def compute_forces(self, use_predicted=False, time_step=None, update=True):
+        """ComputeAccelerations, returning also its Force and Torque sums
+        (src/MForces.f90:319-320, before the division by mass and inertia)
+        as two (n, 3) arrays."""
+        ts = float(self.params.time_step if time_step is None else time_step)
+        f = np.zeros((self.n, 3))
+        t = np.zeros((self.n, 3))
+        self._call("compute_forces", 1 if use_predicted else 0, ts, 1 if update else 0,
+                   _dptr(f), _dptr(t))
+        return f, t
 
     def move_particles(self, step):
         self._call("move_particles", int(step))

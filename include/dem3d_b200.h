@@ -261,6 +261,13 @@ int dem_set_cells(dem_ctx* ctx, const int32_t* traversal, const int32_t* cell_st
  * (src/MForces.f90:145-335), including RedistributeParticles3D. */
 int dem_compute_accelerations(dem_ctx* ctx, int32_t use_predicted,
                               double time_step, int32_t update);
+/* The same pass, also returning its Force(NP,3) and Torque(NP,3) arrays
+ * (src/MForces.f90:154, summed at :319-320 before the division by mass and
+ * inertia at :330-333; gravity and fluid drag included) as rows of three:
+ * force[3*i + k], torque[3*i + k] for i < n.  Mixed precision returns its
+ * FP32 sums widened. */
+int dem_compute_forces(dem_ctx* ctx, int32_t use_predicted, double time_step,
+                       int32_t update, double* force, double* torque);
 /* MoveParticles(step) (src/MDEM.f90:285-369): force pass @x(t) with history
  * update, AB predictor, ring store, force pass @prediction, AM corrector. */
 int dem_move_particles(dem_ctx* ctx, int32_t step);

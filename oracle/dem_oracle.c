@@ -1818,6 +1818,18 @@ int orc_compute_accelerations(orc_ctx* c, int32_t use_predicted, double time_ste
   return compute_accelerations(c, use_predicted ? c->pred : c->part, time_step, update);
 }
 
+/* ComputeAccelerations' Force and Torque arrays (src/MForces.f90:154,
+ * summed at :319-320), rows of three as the pass left them */
+int orc_compute_forces(orc_ctx* c, int32_t use_predicted, double time_step, int32_t update,
+                       double* force, double* torque) {
+  if (!force || !torque) return DEM_ERR_INVALID;
+  int st = orc_compute_accelerations(c, use_predicted, time_step, update);
+  if (st) return st;
+  memcpy(force, c->force, sizeof(double) * 3 * (size_t)c->n);
+  memcpy(torque, c->torque, sizeof(double) * 3 * (size_t)c->n);
+  return DEM_OK;
+}
+
 int orc_move_particles(orc_ctx* c, int32_t step) {
   if (!c->cells_ready) return DEM_ERR_STATE;
   return move_particles(c, step);

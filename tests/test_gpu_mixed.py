@@ -59,8 +59,11 @@ def test_mixed_one_pass_error():
     o2.set_integration(prev, ipc)
     o2.set_contacts(c["imin"], c["imax"], c["ft"], c["vt"], c["ip"], c["iw"], c["ftw"], c["vtw"])
     o2.initialize_cell_distribution()
-    for s in (m, o2):
-        s.compute_accelerations(update=True)
+    (fm, tm), (fo, to) = (s.compute_forces(update=True) for s in (m, o2))
+    # the Force and Torque sums themselves (dem_compute_forces)
+    for x, y, kk in ((fm, fo, "force"), (tm, to, "torque")):
+        err = np.abs(x - y).max() / np.abs(y).max()
+        assert err <= FORCE_TOL, (kk, err)
     a, b = m.get_state(), o2.get_state()
     for k, kk in (("acc", "acceleration"), ("alpha", "angular acceleration")):
         scale = np.abs(b[k]).max()

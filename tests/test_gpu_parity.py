@@ -57,6 +57,28 @@ def test_initial_distribution_and_one_pass():
     assert g.ncol() == o.ncol()
 
 
+def test_force_arrays_bit_exact():
+    """dem_compute_forces: the Force and Torque sums of a pass, before the
+    division by mass and inertia, equal the oracle's bit for bit, on the
+    current and on the predicted positions of a settling bed (walls,
+    gravity, stored histories)."""
+    w = configs.settling(n=600, seed=21)
+    g, o = make_pair(w)
+    for s in (g, o):
+        s.run(1, 60)
+    for pred in (False, True):
+        (fg, tg), (fo, to) = (s.compute_forces(use_predicted=pred, update=False) for s in (g, o))
+        assert np.abs(fg).max() > 0 and np.abs(tg).max() > 0
+        np.testing.assert_array_equal(fg, fo, err_msg=f"force predicted={pred}")
+        np.testing.assert_array_equal(tg, to, err_msg=f"torque predicted={pred}")
+        assert_same_state(g, o, f"state after forces predicted={pred}")
+        assert_same_predicted(g, o, f"predicted after forces predicted={pred}")
+    assert_same_contacts(g, o, "after force passes")
+    for s in (g, o):
+        s.run(61, 80)
+    assert_same_state(g, o, "run after force passes")
+
+
 def test_settling_trajectory_bit_exact():
     w = configs.settling(n=400, seed=7, sigma_v=0.5)
     g, o = make_pair(w)

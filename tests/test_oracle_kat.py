@@ -94,6 +94,32 @@ def test_momentum_and_third_law():
     assert s.count_contacts()[0] > 0
 
 
+def test_force_arrays():
+    """orc_compute_forces: the pass's Force and Torque sums obey the third
+    law (no walls, no gravity) and give the stored accelerations as F/m and
+    T/I."""
+    rng = np.random.default_rng(6)
+    n = 300
+    prm = P.per_particle_params(density=DENSITY, kn=KN, kt=KT, en=0.7, et=0.7, mu=0.4,
+                                rmax=0.6, lbox=(8.0, 8.0, 8.0), pbc=(True, True, True),
+                                gravity=(0, 0, 0), time_step=1e-4)
+    radius = rng.uniform(0.4, 0.6, n)
+    from dem3d_b200.configs import lattice_positions
+    s = oracle_system(prm)
+    s.set_state(lattice_positions(n, 8.0, rng), rng.normal(0, 0.3, (n, 3)),
+                rng.normal(0, 0.3, (n, 3)), radius=radius)
+    s.initialize_cell_distribution()
+    s.run(1, 20)
+    f, t = s.compute_forces(update=False)
+    assert f.shape == t.shape == (n, 3) and np.abs(f).max() > 0
+    assert np.abs(f.sum(0)).max() < 1e-9 * np.abs(f).max()
+    m = 4.0 / 3.0 * math.pi * DENSITY * radius ** 3
+    inertia = 0.4 * m * radius ** 2
+    st = s.get_state()
+    np.testing.assert_allclose(st["acc"], f / m[:, None], rtol=1e-13, atol=0)
+    np.testing.assert_allclose(st["alpha"], t / inertia[:, None], rtol=1e-13, atol=0)
+
+
 def test_coulomb_cap_on_records():
     """Every stored tangential force obeys |FT| <= mu |FN| at storage time:
     check a sliding block of spheres on a frictional floor."""
