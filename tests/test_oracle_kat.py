@@ -120,6 +120,38 @@ def test_force_arrays():
     np.testing.assert_allclose(st["alpha"], t / inertia[:, None], rtol=1e-13, atol=0)
 
 
+@pytest.mark.parametrize("en,mu", [(1.0, 0.0), (0.7, 0.4)])
+def test_energy_between_collisions(en, mu):
+    """A periodic gas without gravity, sampled when no contact is open (no
+    elastic energy stored): with e = 1 and no friction the kinetic energy
+    (translation + rotation) is conserved to the integrator's accuracy over
+    hundreds of collisions; with e < 1 and friction it never rises and has
+    fallen by the end."""
+    rng = np.random.default_rng(11)
+    n, L = 216, 11.0
+    prm = P.per_particle_params(density=DENSITY, kn=KN, kt=KT, en=en, et=en, mu=mu, rmax=0.55,
+                                lbox=(L, L, L), pbc=(True, True, True), gravity=(0, 0, 0),
+                                time_step=1e-4)
+    from dem3d_b200.configs import lattice_positions
+    s = oracle_system(prm)
+    s.set_state(lattice_positions(n, L, rng), rng.normal(0, 1.0, (n, 3)),
+                rng.normal(0, 1.0, (n, 3)), radius=rng.uniform(0.45, 0.55, n))
+    s.initialize_cell_distribution()
+    e0 = s.observables()["kinetic_energy"]
+    free = []
+    for first in range(1, 16001, 20):
+        s.run(first, first + 19)
+        if s.count_contacts() == (0, 0):
+            free.append(s.observables()["kinetic_energy"] / e0)
+    assert s.ncol() > 300 and len(free) > 100
+    free = np.array(free)
+    if en == 1.0:
+        assert np.abs(free - 1.0).max() < 5e-5
+    else:
+        assert np.diff(free).max() <= 1e-12
+        assert free[-1] < 0.8
+
+
 def test_coulomb_cap_on_records():
     """Every stored tangential force obeys |FT| <= mu |FN| at storage time:
     check a sliding block of spheres on a frictional floor."""

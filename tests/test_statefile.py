@@ -36,6 +36,96 @@ def _random_state(rng, n=37, nc=2, nw=2, nprev=3, ncell=11):
                         (5, 6, 7, 890), (0.5, 3, 4, 5, 6), 17)
 
 
+class _Fread:
+    """MATLAB's fread(file, count, precision) on a little-endian byte string."""
+
+    def __init__(self, data):
+        self.data, self.at = data, 0
+
+    def __call__(self, count, fmt):
+        size = {"int8": 1, "int32": 4, "float64": 8}[fmt]
+        code = {"int8": "<i1", "int32": "<i4", "float64": "<f8"}[fmt]
+        out = np.frombuffer(self.data, dtype=code, count=count, offset=self.at)
+        self.at += count * size
+        return out.astype(np.float64)
+
+
+def _matlab_readfile(data):
+    """The Complete branch of the reference's MATLAB reader, matlab/readfile.m,
+    in its order of fread calls (ib = int32, rb = float64, dim = 3)."""
+    fread = _Fread(data)
+    out = {}
+    assert fread(1, "int32")[0] == 1129137476                       # :25-26
+    version = int(fread(1, "int8")[0])                               # :27
+    dim = int(fread(1, "int8")[0])
+    dav, ini = 2 * dim - 3, 7 - 2 * dim                              # :29-30
+    full = int(fread(1, "int8")[0]) == 72                            # :31-33
+    assert full and dim == 3
+    out["scales"] = [fread(1, "float64")[0] for _ in range(3)]      # :35-37
+    out["time"] = fread(1, "float64")[0]                             # :38
+    out["lbox"] = fread(dim, "float64")                              # :39
+    comps = []
+    for _ in range(int(fread(1, "int32")[0])):                       # :43-66
+        rec = [fread(1, "int32")[0], fread(1, "float64")[0], fread(1, "float64")[0],
+               fread(1, "float64")[0]]
+        rec.append(fread(1, "float64")[0] if version == 2 else 2.0 / 7.0 * rec[3])
+        rec += [fread(1, "float64")[0], fread(1, "float64")[0]]
+        comps.append(rec)
+    out["components"] = comps
+    walls = []
+    for _ in range(int(fread(1, "int32")[0])):                       # :69-112
+        wl = {"type": fread(1, "int32")[0], "l": fread(3, "float64")}
+        for k in ("u", "w", "n", "position", "velocity"):
+            wl[k] = fread(dim, "float64")
+        om = np.zeros(3)
+        om[ini - 1:] = fread(dav, "float64")
+        wl["omega"] = om
+        if version == 2:
+            wl["k"] = (fread(1, "float64")[0], fread(1, "float64")[0])
+        walls.append(wl)
+    out["walls"] = walls
+    vectors = fread(1, "int8")[0] != 0                               # :115
+    npart = int(sum(c[0] for c in comps))                            # :114
+    idx, x, v, w = [], [], [], []
+    for _ in range(npart):                                           # :131-141
+        idx.append(fread(1, "int32")[0])
+        x.append(fread(dim, "float64"))
+        v.append(fread(dim, "float64"))
+        w.append(fread(dav, "float64"))
+        if vectors:
+            fread(3 * dim, "float64")
+    out.update(index=np.array(idx), pos=np.array(x), vel=np.array(v), omega=np.array(w))
+    out["consumed"] = fread.at
+    return out
+
+
+def test_configuration_reads_with_the_matlab_reader(tmp_path):
+    """The Complete configuration written here is what the reference's own
+    MATLAB reader expects, field by field, to the last byte."""
+    rng = np.random.default_rng(8)
+    cfg = _random_state(rng, n=23, nc=3, nw=3).config
+    path = os.path.join(tmp_path, "x.cfg")
+    SF.write_configuration(path, cfg)
+    data = open(path, "rb").read()
+    m = _matlab_readfile(data)
+    assert m["consumed"] == len(data)
+    assert m["scales"] == [cfg.length_scale, cfg.time_scale, cfg.mass_scale]
+    assert m["time"] == cfg.time
+    np.testing.assert_array_equal(m["lbox"], cfg.lbox)
+    for got, k in zip(m["components"], cfg.components):
+        assert got == [k.number, k.radius, k.density, k.stiffness, k.shear_stiffness, k.mass,
+                       k.inertia]
+    for got, wl in zip(m["walls"], cfg.walls):
+        assert got["type"] == wl.shape
+        np.testing.assert_array_equal(got["l"], [wl.l1, wl.l2, wl.l3])
+        for k in ("u", "w", "n", "position", "velocity", "omega"):
+            np.testing.assert_array_equal(got[k], getattr(wl, k))
+        assert got["k"] == (wl.stiffness, wl.shear_stiffness)
+    np.testing.assert_array_equal(m["index"], cfg.index + 1)
+    for k in ("pos", "vel", "omega"):
+        np.testing.assert_array_equal(m[k], getattr(cfg, k))
+
+
 def test_state_file_round_trip_and_layout(tmp_path):
     rng = np.random.default_rng(5)
     s = _random_state(rng)
