@@ -152,6 +152,37 @@ def test_energy_between_collisions(en, mu):
         assert free[-1] < 0.8
 
 
+def test_sliding_sphere_rolls_at_five_sevenths():
+    """A sphere launched without spin along a frictional floor (linear
+    model, Coulomb sliding): while it slides, friction mu*m*g slows it at
+    mu*g and spins it up at 5*mu*g/(2R); it rolls from t* = 2*v0/(7*mu*g) on,
+    at v = 5/7 v0 with omega*R = v."""
+    mu, g, v0, R, dt = 0.5, 1.0, 1.0, 0.5, 1e-4
+    L, lz = 10.0, 4.0
+    floor = P.rectangle((0.0, 0.0, -0.5 * lz), L, L, stiffness=2.0 * KN,
+                        shear_stiffness=2.0 * KT)
+    prm, _ = P.component_params([P.Component(1, 1.0, DENSITY, 2.0 * KN, 2.0 * KT)], [floor],
+                                [[0.8]], [[0.8]], [[mu]], [[0.8]], [[0.8]], [[mu]],
+                                lbox=(L, L, lz), pbc=(True, True, False),
+                                gravity=(0.0, 0.0, -g), time_step=dt)
+    s = oracle_system(prm)
+    m = 1.0  # d = 1 at DENSITY
+    s.set_state(np.array([[0.0, 0.0, -0.5 * lz + R - m * g / KN]]), np.array([[v0, 0.0, 0.0]]),
+                np.zeros((1, 3)), comp=np.zeros(1, np.int32))
+    s.initialize_cell_distribution()
+    t_roll = 2.0 * v0 / (7.0 * mu * g)
+    half = int(round(0.5 * t_roll / dt))
+    s.run(1, half)
+    st = s.get_state()
+    assert abs(st["vel"][0, 0] - (v0 - mu * g * half * dt)) < 1e-4
+    assert abs(st["omega"][0, 1] - 2.5 * mu * g / R * half * dt) < 1e-4
+    s.run(half + 1, int(2.1 * t_roll / dt))
+    st = s.get_state()
+    assert abs(st["vel"][0, 0] - 5.0 / 7.0 * v0) < 1e-6
+    assert abs(st["omega"][0, 1] * R - st["vel"][0, 0]) < 1e-6
+    assert abs(st["vel"][0, 1]) < 1e-12 and abs(st["omega"][0, 0]) < 1e-12
+
+
 def test_coulomb_cap_on_records():
     """Every stored tangential force obeys |FT| <= mu |FN| at storage time:
     check a sliding block of spheres on a frictional floor."""
