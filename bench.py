@@ -229,8 +229,9 @@ def _oracle_variant():
         return libs["libdem_oracle_fast.so"], "-O3 -ffp-contract=off"
 
 
-def cpu_time_steps(w, max_steps=3, budget_s=25.0, lib_path=None):
-    """Time oracle MoveParticles steps on w (single thread)."""
+def cpu_time_steps(w, max_steps=3, budget_s=25.0, lib_path=None, warmup=1):
+    """Time oracle MoveParticles steps on w (single thread), after `warmup`
+    untimed steps (the first steps also allocate the contact lists)."""
     import ctypes as C
 
     from dem3d_b200 import _abi
@@ -241,10 +242,12 @@ def cpu_time_steps(w, max_steps=3, budget_s=25.0, lib_path=None):
     try:
         s.set_state(w.pos, w.vel, w.omega, comp=w.comp, radius=w.radius)
         s.initialize_cell_distribution()
+        for k in range(warmup):
+            s.move_particles(4 + k)
         steps = 0
         t0 = time.perf_counter()
         while steps < max_steps:
-            s.move_particles(4 + steps)
+            s.move_particles(4 + warmup + steps)
             steps += 1
             if time.perf_counter() - t0 > budget_s:
                 break
@@ -255,7 +258,7 @@ def cpu_time_steps(w, max_steps=3, budget_s=25.0, lib_path=None):
 
 
 def _ref_worker(args):
-    name, rank, tile_pos, tile_rad, L_t, lib_path, steps_cap, budget = args
+    name, rank, tile_pos, tile_rad, L_t, lib_path, steps_cap, warmup, budget = args
     from dem3d_b200 import configs
     spec = WORKLOADS[name]
     k = configs.tile_count(spec["n"], spec["tile"])
@@ -266,7 +269,7 @@ def _ref_worker(args):
     prm = configs.dense_packing_params(0.6, L)
     w = configs.Workload("dense_packing", prm, pos, vel, np.zeros((n, 3)), radius=radius,
                          info={"L": L, "copies": k ** 3})
-    return cpu_time_steps(w, steps_cap, budget, lib_path)
+    return cpu_time_steps(w, steps_cap, budget, lib_path, warmup)
 
 
 def run_reference(args):
@@ -301,10 +304,12 @@ def run_reference(args):
     per_proc = 1.6e9 * spec["n"] / 1e6
     procs = max(1, min(cores, int(mem * 0.6 // per_proc), 32))
     steps_cap = max(1, min(args.steps, 3))
+    warmup = max(0, min(args.warmup, 3))
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(procs) as pool:
-        res = pool.map(_ref_worker, [(args.workload, r, tp, tr, L_t, lib_path, steps_cap, 60.0)
+        res = pool.map(_ref_worker, [(args.workload, r, tp, tr, L_t, lib_path, steps_cap, warmup,
+                                      60.0)
                                      for r in range(procs)])
     wall = time.perf_counter() - t0
     value = sum(r[0] for r in res)
@@ -312,13 +317,14 @@ def run_reference(args):
                                        configs.tile_count(spec["n"], spec["tile"]),
                                        "copies": configs.tile_count(spec["n"],
                                                                     spec["tile"]) ** 3}})
-    sample = (f"{procs} processes x {res[0][1]} MoveParticles steps of an independent "
+    sample = (f"{procs} processes x {res[0][1]} MoveParticles steps (after {warmup} untimed) "
+              f"of an independent "
               f"{spec['n']:,}-sphere system each (oracle C port {flags}; reference Fortran "
               f"not buildable here: no Fortran compiler); tile relaxed by the oracle in "
               f"{t_relax:.1f}s")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-        "steps": res[0][1], "warmup": 0, "ms_per_step": 1000.0 * max(r[2] / r[1] for r in res),
+        "steps": res[0][1], "warmup": warmup, "ms_per_step": 1000.0 * max(r[2] / r[1] for r in res),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": config_block(args.workload, w_dummy, 1, "fp64"),
@@ -584,7 +590,8 @@ def run_ours(args):
         lib_path, flags = _oracle_variant()
         v, k, dt = cpu_time_steps(base, max_steps=3, budget_s=25.0, lib_path=lib_path)
         cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": f"{k} MoveParticles steps of the same {n:,}-sphere system, oracle "
+               "sample": f"{k} MoveParticles steps (after 1 untimed) of the same {n:,}-sphere "
+                         f"system, oracle "
                          f"C port ({flags}), 1 thread, {dt:.1f}s"}
     if rank == 0:
         line = {
