@@ -229,9 +229,23 @@ def _oracle_variant():
         return libs["libdem_oracle_fast.so"], "-O3 -ffp-contract=off"
 
 
-def cpu_time_steps(w, max_steps=3, budget_s=25.0, lib_path=None, warmup=1):
+def cpu_model():
+    """The host CPU's model name (first "model name" line of /proc/cpuinfo)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown CPU"
+
+
+def cpu_time_steps(w, max_steps=3, budget_s=25.0, lib_path=None, warmup=1, core=None):
     """Time oracle MoveParticles steps on w (single thread), after `warmup`
-    untimed steps (the first steps also allocate the contact lists)."""
+    untimed steps (the first steps also allocate the contact lists).  With
+    `core`, the calling thread is pinned to that core (the k-th core it may
+    run on) while it times, and its affinity is restored afterwards."""
     import ctypes as C
 
     from dem3d_b200 import _abi
@@ -239,6 +253,11 @@ def cpu_time_steps(w, max_steps=3, budget_s=25.0, lib_path=None, warmup=1):
     lib = C.CDLL(lib_path)
     _abi.bind(lib, "orc_", _abi.SIGNATURES)
     s = DEMSystem(w.params, lib=lib, prefix="orc_")
+    old = None
+    if core is not None and hasattr(os, "sched_setaffinity"):
+        old = os.sched_getaffinity(0)
+        allowed = sorted(old)
+        os.sched_setaffinity(0, {allowed[core % len(allowed)]})
     try:
         s.set_state(w.pos, w.vel, w.omega, comp=w.comp, radius=w.radius)
         s.initialize_cell_distribution()
@@ -254,6 +273,8 @@ def cpu_time_steps(w, max_steps=3, budget_s=25.0, lib_path=None, warmup=1):
         dt = time.perf_counter() - t0
     finally:
         s.close()
+        if old is not None:
+            os.sched_setaffinity(0, old)
     return w.n * steps / dt, steps, dt
 
 
@@ -269,7 +290,7 @@ def _ref_worker(args):
     prm = configs.dense_packing_params(0.6, L)
     w = configs.Workload("dense_packing", prm, pos, vel, np.zeros((n, 3)), radius=radius,
                          info={"L": L, "copies": k ** 3})
-    return cpu_time_steps(w, steps_cap, budget, lib_path, warmup)
+    return cpu_time_steps(w, steps_cap, budget, lib_path, warmup, core=rank)
 
 
 def run_reference(args):
@@ -319,7 +340,8 @@ def run_reference(args):
                                                                     spec["tile"]) ** 3}})
     sample = (f"{procs} processes x {res[0][1]} MoveParticles steps (after {warmup} untimed) "
               f"of an independent "
-              f"{spec['n']:,}-sphere system each (oracle C port {flags}; reference Fortran "
+              f"{spec['n']:,}-sphere system each, one process pinned per core of "
+              f"{cpu_model()} (oracle C port {flags}; reference Fortran "
               f"not buildable here: no Fortran compiler); tile relaxed by the oracle in "
               f"{t_relax:.1f}s")
     line = {
@@ -588,11 +610,12 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         lib_path, flags = _oracle_variant()
-        v, k, dt = cpu_time_steps(base, max_steps=3, budget_s=25.0, lib_path=lib_path)
+        v, k, dt = cpu_time_steps(base, max_steps=3, budget_s=25.0, lib_path=lib_path, core=0)
         cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
                "sample": f"{k} MoveParticles steps (after 1 untimed) of the same {n:,}-sphere "
                          f"system, oracle "
-                         f"C port ({flags}), 1 thread, {dt:.1f}s"}
+                         f"C port ({flags}), 1 thread pinned to one core of {cpu_model()}, "
+                         f"{dt:.1f}s"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
