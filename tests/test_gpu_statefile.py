@@ -127,3 +127,19 @@ def test_gpu_resume_after_removals(tmp_path):
     o = fresh(oracle_system)
     o.run(1, 700)
     _same(full, o, "gpu vs oracle")
+
+
+def test_gpu_resume_while_pouring(tmp_path):
+    """The shipped example (pouring, orbiting cone walls) saved on the GPU
+    mid-pour and resumed on the GPU: bit-identical with the uninterrupted
+    GPU run, which is bit-identical with the oracle's."""
+    from tests.test_ball_bearings import start
+    from tests.test_particle_removal import export
+    from tests.test_statefile import _resume_ball_bearings
+    full = _resume_ball_bearings(DEMSystem, tmp_path)
+    _, _, _, o = start(oracle_system)
+    o.run(1, 24000)
+    a, b = export(full, True), export(o, True)
+    for k in ("pos", "vel", "cell_index", "traversal", "cell_start", "prev"):
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    assert full.rng() == o.rng()

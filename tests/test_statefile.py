@@ -280,3 +280,40 @@ def test_oracle_resume_after_removals(tmp_path):
     for k in ca:
         np.testing.assert_array_equal(ca[k], cb[k], err_msg=k)
     assert full.ncol() == res.ncol()
+
+
+def _resume_ball_bearings(make, tmp_path, save_at=12000, end=24000):
+    """The shipped example saved mid-pour and resumed: the generator, the
+    poured spheres, the orbiting cones and the contacts come back, and the
+    resumed run continues as the uninterrupted one."""
+    from tests.test_ball_bearings import start
+    from tests.test_particle_removal import export
+    w, motion, pour, full = start(make)
+    full.run(1, end)
+    _, _, _, part = start(make)
+    part.run(1, save_at)
+    assert 0 < part.n < full.n
+    comps = SF.component_records([P.Component(part.n, 1.0, configs.DENSITY, 2.0 * configs.KN,
+                                              2.0 * configs.KT)])
+    st = SF.capture(part, components=comps, wall_stiffness=[(1.0, 1.0)] * 5, step=save_at)
+    path = os.path.join(tmp_path, "bb.stt")
+    SF.write_state(path, st)
+    back = SF.read_state(path, w.params.method_order - 1)
+    res = make(SF.params_with_walls(w.params, back))
+    res.set_wall_motion(motion)
+    res.set_pouring(pour)
+    assert SF.restore(res, back) == save_at + 1
+    assert res.rng() == part.rng()
+    res.run(save_at + 1, end)
+    a, b = export(full, True), export(res, True)
+    for k in ("pos", "vel", "cell_index", "traversal", "cell_start", "prev"):
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    for k in a["contacts"]:
+        np.testing.assert_array_equal(a["contacts"][k], b["contacts"][k], err_msg=k)
+    assert full.rng() == res.rng() and full.ncol() == res.ncol()
+    np.testing.assert_array_equal(full.walls()["position"], res.walls()["position"])
+    return full
+
+
+def test_oracle_resume_while_pouring(tmp_path):
+    _resume_ball_bearings(oracle_system, tmp_path)
