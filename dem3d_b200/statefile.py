@@ -417,6 +417,29 @@ def _get_contacts(r: _Reader):
     return ct, n_main
 
 
+def state_file_for_step(step: int, save_interval: int, state_file: str, state_file2: str,
+                        finished: bool = False):
+    """The file PerformPeriodicTasks saves after ``step`` (src/DEM.f90:164-170),
+    or None: every ``save_interval`` steps, alternately ``state_file`` and
+    ``state_file2`` (the second one on multiples of twice the interval and when
+    the run has finished), so that a crash while writing one leaves the
+    other intact."""
+    if step % save_interval != 0 and not finished:
+        return None
+    return state_file2 if (step % (2 * save_interval) == 0 or finished) else state_file
+
+
+def resume_file(state_file: str, state_file2: str):
+    """The file a resumed run reads (src/DEM.f90:73-83): ``state_file`` if it
+    exists, else ``state_file2``, else None (the run starts afresh).  As in
+    the reference, the two files' ages are not compared."""
+    import os
+    for path in (state_file, state_file2):
+        if os.path.exists(path):
+            return path
+    return None
+
+
 def read_state(path: str, nprev: int) -> StateFile:
     """ReadState (src/DEM.f90:1018-1134).  ``nprev`` = MethodOrder - 1 comes
     from the specification, as in the reference (the file does not hold it)."""

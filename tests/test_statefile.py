@@ -317,3 +317,74 @@ def _resume_ball_bearings(make, tmp_path, save_at=12000, end=24000):
 
 def test_oracle_resume_while_pouring(tmp_path):
     _resume_ball_bearings(oracle_system, tmp_path)
+
+
+def test_double_buffered_saves_and_resume_choice(tmp_path):
+    """SaveState alternates between the two state files and a resumed run
+    reads the first one that exists, whatever their ages."""
+    a, b = os.path.join(tmp_path, "r.stt"), os.path.join(tmp_path, "r.st2")
+    picks = [SF.state_file_for_step(k, 100, a, b) for k in range(50, 650, 50)]
+    assert picks == [None, a, None, b, None, a, None, b, None, a, None, b]
+    assert SF.state_file_for_step(123, 100, a, b, finished=True) == b
+    assert SF.resume_file(a, b) is None
+    open(b, "wb").close()
+    assert SF.resume_file(a, b) == b
+    open(a, "wb").close()
+    assert SF.resume_file(a, b) == a
+
+
+def test_periodic_saves_and_resume_after_a_crash(tmp_path):
+    """A run that saves every 60 steps into the two files stops at step 250
+    (as if it had crashed). The resumed run reads the first file that exists,
+    the one written at step 180 (the other one holds step 240), and reaches
+    step 400 bit-identical with the uninterrupted run."""
+    w = configs.hopper(n=300, seed=1006)
+    comps = SF.component_records([P.Component(len(w.pos), 1.0, configs.DENSITY,
+                                              2.0 * configs.KN, 2.0 * configs.KT)])
+    stiff = [(2.0 * configs.KN, 2.0 * configs.KT)] * w.params.n_walls
+    a, b = os.path.join(tmp_path, "h.stt"), os.path.join(tmp_path, "h.st2")
+
+    def fresh(params):
+        s = oracle_system(params)
+        s.set_state(w.pos, w.vel, w.omega, comp=w.comp)
+        s.initialize_cell_distribution()
+        return s
+    full = fresh(w.params)
+    full.run(1, 400)
+    crashed = fresh(w.params)
+    for first, last in ((1, 60), (61, 120), (121, 180), (181, 240), (241, 250)):
+        crashed.run(first, last)
+        path = SF.state_file_for_step(last, 60, a, b)
+        if path:
+            SF.write_state(path, SF.capture(crashed, components=comps, wall_stiffness=stiff,
+                                            step=last))
+    path = SF.resume_file(a, b)
+    assert path == a
+    back = SF.read_state(path, w.params.method_order - 1)
+    assert back.initial_step == 181
+    res = oracle_system(SF.params_with_walls(w.params, back))
+    res.run(SF.restore(res, back), 400)
+    sa, sb = full.get_state(), res.get_state()
+    for k in ("pos", "vel", "omega"):
+        np.testing.assert_array_equal(sa[k], sb[k], err_msg=k)
+    ca, cb = full.get_contacts(), res.get_contacts()
+    for k in ca:
+        np.testing.assert_array_equal(ca[k], cb[k], err_msg=k)
+    assert full.ncol() == res.ncol()
+
+
+def test_corrupt_state_files_are_errors(tmp_path):
+    """A file that is not a state file, or holds another dimension, is an
+    error, as ReadConfFromUnit's checks are (src/MConfig.f90:109-448)."""
+    rng = np.random.default_rng(9)
+    path = os.path.join(tmp_path, "c.stt")
+    SF.write_state(path, _random_state(rng))
+    data = bytearray(open(path, "rb").read())
+    at = data.index(b"DEMC")
+    for offset, value in ((0, ord("X")), (5, 2)):   # signature; int(dim,1)
+        bad = bytearray(data)
+        bad[at + offset] = value
+        with open(path, "wb") as f:
+            f.write(bad)
+        with pytest.raises(ValueError):
+            SF.read_state(path, 3)
