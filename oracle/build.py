@@ -1,6 +1,6 @@
 """Build recipe for the CPU oracle (test infrastructure only).
 
-``libdem_oracle.so``      -O2 -ffp-contract=off: the checker used by the tests.
+``libdem_oracle.so``      -O2 -ffp-contract=off: the oracle the tests compare against.
 ``libdem_oracle_fast.so`` -O3 -ffp-contract=off: the same code built with the
                           reference Makefile's optimisation level, timed as the
                           CPU baseline (portable ISA; the bench may rebuild it

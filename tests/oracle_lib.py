@@ -1,5 +1,5 @@
 """Loads the CPU oracle (oracle/dem_oracle.c) behind the same ABI as the
-CUDA library, for use as the checker in tests (never as the product)."""
+CUDA library, for the tests to compare against (never as the product)."""
 from __future__ import annotations
 
 import ctypes as C
