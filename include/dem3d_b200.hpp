@@ -61,6 +61,16 @@ class System {
     check(dem_compute_accelerations(ctx_, predicted ? 1 : 0, time_step, update ? 1 : 0),
           "ComputeAccelerations");
   }
+  // The same pass, also returning its Force and Torque arrays (rows of three,
+  // before the division by mass and inertia).
+  void ComputeForces(bool predicted, double time_step, bool update, std::vector<double>& force,
+                     std::vector<double>& torque) {
+    force.assign(3 * (size_t)NP(), 0.0);
+    torque.assign(force.size(), 0.0);
+    check(dem_compute_forces(ctx_, predicted ? 1 : 0, time_step, update ? 1 : 0, force.data(),
+                             torque.data()),
+          "ComputeForces");
+  }
   void MoveParticlesEuler() { check(dem_move_particles_euler(ctx_), "MoveParticlesEuler"); }
   void MoveParticles(int step) { check(dem_move_particles(ctx_, step), "MoveParticles"); }
   // Returns the number of particles removed.
