@@ -787,6 +787,12 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    world = env_int("WORLD_SIZE", 1)
+    if args.gpus != world:
+        # one process per GPU: N > 1 must come from a launcher (torchrun)
+        print(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}; launch --gpus N with "
+              "python -m torch.distributed.run --nproc-per-node N", file=sys.stderr)
+        return 2
     if args.impl == "reference":
         return run_reference(args)
     if WORKLOADS[args.workload].get("kind") == "ensemble":

@@ -2615,8 +2615,10 @@ int dem_get_row_stats(dem_ctx* c, int64_t* candidates, int32_t* row_capacity) {
 // For callers that may not allocate device memory: the working memory of the
 // counting sort lives in one file-scope device array of fixed size instead
 // of per-context buffers.  Host code only ever sees the array's host-side
-// stand-in symbol, which is not a device address; the device address is
-// looked up once per device with cudaGetSymbolAddress.
+// stand-in symbol, which is not a device address; every call looks the
+// device address up on the current device with cudaGetSymbolAddress (a
+// host-side query), so no address outlives a device reset or belongs to
+// another context.
 
 namespace {
 
@@ -2640,9 +2642,6 @@ struct NoAllocScratch {
   double py[NA_MAXN];
   double pz[NA_MAXN];
 };
-
-constexpr int NA_MAX_DEVICES = 64;
-void* g_na_base[NA_MAX_DEVICES] = {};
 
 }  // namespace
 
@@ -2708,21 +2707,20 @@ extern "C" int dem_distribute_particles_noalloc(const dem_params* p, int32_t n,
   if (ncell_out) *ncell_out = ncell;
 
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NA_MAX_DEVICES) {
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) {
     cudaGetLastError();
     return say(DEM_ERR_NO_DEVICE, "no usable CUDA device");
   }
-  // once per device, with that device current: the array's device address
-  if (!g_na_base[dev]) {
-    void* base = nullptr;
+  // the array's device address on the current device (the first call on a
+  // device also loads the device code there)
+  void* base = nullptr;
+  {
     cudaError_t e = cudaGetSymbolAddress(&base, g_noalloc_scratch);
     if (e != cudaSuccess || !base) {
       cudaGetLastError();
       return say(DEM_ERR_CUDA, "cudaGetSymbolAddress of the scratch array failed");
     }
-    g_na_base[dev] = base;
   }
-  unsigned char* base = (unsigned char*)g_na_base[dev];
   NoAllocScratch* S = (NoAllocScratch*)base;  // device addresses only
   DevParams* dp = &S->params;
   Counters* cnt = &S->counters;

@@ -367,10 +367,12 @@ int dem_autotune(dem_ctx* ctx, int32_t first_step, int32_t steps_per_trial,
                  int32_t* last_step, double* trial_ms);
 
 /* Allocation-free cell distribution.  No counterpart in the reference: it
- * serves callers that may not allocate device memory while they run, such
- * as code recording work into a CUDA graph, a host application whose device
- * memory is all handed out by its own pool or framework, or a service that
- * forbids allocation after start-up.  It computes what
+ * serves callers that may not allocate device memory while they run: a host
+ * application whose device memory is all handed out by its own pool or
+ * framework (a cudaMalloc behind its back breaks its budget and fragments
+ * its pool), or a service that forbids allocation after start-up (cudaMalloc
+ * and cudaFree synchronise the device and can take milliseconds).  It
+ * computes what
  * dem_initialize_cell_distribution computes (the cell of every particle and
  * the particles of every cell in list order) for one particle set, without a
  * context and without calling cudaMalloc/cudaFree or any allocating library:
@@ -384,8 +386,10 @@ int dem_autotune(dem_ctx* ctx, int32_t first_step, int32_t steps_per_trial,
  *    in err, if given); the other checks of dem_create apply;
  *  - stream: a cudaStream_t (NULL = the default stream); the call waits for
  *    its own work before returning;
- *  - the first call on a device looks up the array's device address, so on
- *    each device make that first call before any stream capture;
+ *  - every call looks up the array's device address on the current device
+ *    (cudaGetSymbolAddress, a host-side query); the first call on a device
+ *    also loads the library's device code there, so on each device make
+ *    that first call before any stream capture;
  *  - all calls share the one array: calls that overlap on the GPU (other
  *    threads, other streams) race and must be serialised by the caller. */
 #define DEM_NOALLOC_MAX_PARTICLES 262144

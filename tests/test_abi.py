@@ -65,14 +65,3 @@ def test_params_struct_layout():
     assert a == C.sizeof(_abi.DemParams)
     assert b == C.sizeof(_abi.DemWall)
     assert o == C.sizeof(_abi.DemObservables)
-
-
-def test_integration_document_matches_the_header():
-    """INTEGRATION.md lists every entry point of the header in its table, and
-    its Fortran module binds only names the header declares."""
-    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    names = set(declared_symbols())
-    listed = set(re.findall(r"`(dem_[a-z0-9_]+)", doc))
-    assert names <= listed, sorted(names - listed)
-    bound = set(re.findall(r'bind\(C,\s*name="(dem_[a-z0-9_]+)"\)', doc))
-    assert bound and bound <= names, sorted(bound - names)

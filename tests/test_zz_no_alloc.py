@@ -1,11 +1,12 @@
 """The allocation-free cell distribution against the context-based one.
 
 dem_distribute_particles_noalloc exists for callers that may not allocate
-device memory while they run (code recording a CUDA graph, applications whose
-device memory all comes from their own pool, services that forbid allocation
-after start-up).  It must give exactly what dem_initialize_cell_distribution
-gives -- the cell of every particle and every cell's particles in list order
--- on consecutive calls that reuse its one static scratch array.  The inputs
+device memory while they run (applications whose device memory all comes from
+their own pool, services that forbid allocation after start-up because
+cudaMalloc synchronises the device).  It must give exactly what
+dem_initialize_cell_distribution gives -- the cell of every particle and every
+cell's particles in list order -- on consecutive calls that reuse its one
+static scratch array.  The inputs
 and outputs here are device buffers owned by the test (torch tensors); the
 entry point itself allocates nothing.
 
