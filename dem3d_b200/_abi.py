@@ -113,6 +113,8 @@ class DemObservables(C.Structure):
         ("mean_coordination", C.c_double), ("packing_fraction", C.c_double),
         ("wall_normal_force", C.c_double * MAX_WALLS), ("momentum", _d3),
         ("n_pair_contacts", C.c_int64), ("n_wall_contacts", C.c_int64),
+        ("wall_pressure", C.c_double * MAX_WALLS), ("bed_height", C.c_double),
+        ("n_pair_records", C.c_int64),
     ]
 
 

@@ -88,20 +88,26 @@ struct Counters {
   int force_full;    // the next pass must rebuild every row (new state, grown rows)
   int row_overflow;  // a candidate row needed more than kc entries
   int need_kc;       // longest candidate row requested
+  int in_overflow;   // a particle received more "j" contact results than fit
+  int need_in;       // most "j" contact results of one particle in the last step
   int list_error;    // a cell-list walk exceeded its bound (corrupt lists)
   int nonfinite;     // a particle position became NaN or infinite
   unsigned int disp_max;  // FP32 bits (rounded up) of the largest displacement of one pass
   double disp_acc;   // sum of disp_max since the last full rebuild
-  double wall_fn[NWM];
   int escape_stop;   // a captured chunk stopped before a step: particles had left the box
 };
 
-// Contact history, one table per buffer: records owned by imin, stored slot
-// major (record r of particle i at r*n + i), so that the first records of
-// neighbouring particles share cache lines.
+// Contact history, one table per buffer, stored slot major (record r of
+// particle i at r*n + i), so that the first records of neighbouring particles
+// share cache lines.  The record of a pair (the reference's node keyed by
+// (imin, imax), src/MContacts.f90:329-437) sits in the table of one of its
+// two particles: after a history-updating pass, the one that evaluated the
+// contact as "i"; after an import or before a removal, imin.  A lookup tries
+// the evaluating particle's table, then the partner's; a pair has at most one
+// record.
 struct History {
-  int* cnt;       // [n] records owned by particle
-  int* key;       // [cap*n] partner (imax)
+  int* cnt;       // [n] records held by particle
+  int* key;       // [cap*n] partner
   double2* val;   // [cap*n*3] (ft.x,ft.y) (ft.z,vt.x) (vt.y,vt.z)
   int* wflag;     // [n*nw] wall record present
   double2* wval;  // [n*nw*3]
@@ -147,24 +153,52 @@ struct CellLists {
 };
 
 // Candidate rows, column-major (cand[k*n + p]): the particles within
-// MinDij + skin of particle p, as original indices, in the order p meets
-// them in ComputeAccelerations' sweep -- first the "p is i" partners of
-// loop 1 (src/MForces.f90:199-272), then the "p is j" partners in sweep
-// order, split where p's own block ends.  meta = n1 | n2b << 10 | n2a << 20.
-// A row stays valid while no cell of its 27-cell neighbourhood gains or
-// loses a particle and no particle has moved skin/2 since the last full
-// rebuild.
+// MinDij + skin of particle p that the sweep visits with p as "i" (loop jj
+// of src/MForces.f90:199-272: the rest of p's cell list, then the half-shell
+// cells in FirstNeighbour order), as original indices, in that order.
+// meta = the row length; rank = p's position in its cell's list, which with
+// the cell gives the place of p's block in the sweep.  A row stays valid
+// while no cell of its 27-cell neighbourhood gains or loses a particle and
+// no particle has moved skin/2 since the last full rebuild.
 struct Rows {
   int* cand;
   int* meta;
+  int* rank;
   int kc;
 };
 constexpr int META_BITS = 10;
 constexpr int META_MASK = (1 << META_BITS) - 1;
 constexpr int KC_MAX = META_MASK;
 
-// Arguments of one pass kernel.  V4/W2 are the velocity copies the pass
-// reads for partners (double in FP64 mode, float in mixed mode).
+// Place of particle i's block in ComputeAccelerations' sweep (cells in
+// increasing index, then the cell's list order): contributions to a
+// particle's Force and Torque arrive in the order of these keys.
+__device__ __forceinline__ unsigned long long sweep_key(int cell, int rank) {
+  return ((unsigned long long)(unsigned)cell << 32) | (unsigned)rank;
+}
+
+// Contact results handed from the contact kernel to the fold kernel.
+//  - "j" side: what particle j adds for one contact that particle i
+//    evaluated (Force(j) - FN - FT, Torque(j) + Rj*(Nij x FT)), with i's sweep
+//    key; record s of particle j at s*stride + j.
+//  - "i" side: the particle's own block, iForce and iTorque after its loop
+//    over partners, its walls and its drag.
+struct alignas(16) InRec64 {
+  double2 a, b, c, d, e;  // (key, FN.x) (FN.y, FN.z) (FT.x, FT.y) (FT.z, NxFT.x) (NxFT.y, NxFT.z)
+};
+struct alignas(16) InRec32 {
+  float4 a, b, c;  // (key lo, key hi, FN.x, FN.y) (FN.z, FT.xyz) (NxFT.xyz, 0)
+};
+struct alignas(16) Own64 {
+  double2 a, b, c;  // (iF.x, iF.y) (iF.z, iT.x) (iT.y, iT.z)
+};
+struct alignas(8) Own32 {
+  float2 a, b, c;   // (iF.x, iF.y) (iF.z, iT.x) (iT.y, iT.z)
+};
+
+// Arguments of the two kernels of a force pass (contact kernel, fold
+// kernel).  V4/W2 are the velocity copies the pass reads for partners
+// (double in FP64 mode, float in mixed mode).
 template <class V4, class W2>
 struct PassArgs {
   const DevParams* P;   // system table
@@ -200,7 +234,40 @@ struct PassArgs {
   // (src/MForces.f90:319-333) as amsum[3p+k], then amsum[3n+3p+k]; NULL: not
   // kept
   double* amsum;
+  // contact kernel -> fold kernel: "j" results of every particle (count,
+  // records: InRec64 / InRec32 [in_cap][in_stride]) and the "i" blocks
+  // (Own64 / Own32 [n]); the fold kernel resets the counts
+  const int* rank;
+  int* in_cnt;
+  void* in_rec;
+  int in_cap, in_stride;
+  void* own;
+  // normal force on each wall, summed per block of the contact kernel in a
+  // fixed order ([block][DEM_MAX_WALLS]); nw_max: walls of the system with
+  // the most
+  double* wall_part;
+  int nw_max;
 };
+
+// The |FN| of every wall contact of a block of 128 particles, summed in a
+// fixed order (lanes of warp 0 over the four warps, then a shuffle tree):
+// s_w[w][thread] holds each thread's value.  All threads of the block call.
+template <class T>
+__device__ __forceinline__ void wall_partials(const T (*s_w)[128], int nw_max, double* out) {
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int l = threadIdx.x;
+    for (int w = 0; w < nw_max; w++) {
+      double v = (double)s_w[w][l];
+      v = v + (double)s_w[w][l + 32];
+      v = v + (double)s_w[w][l + 64];
+      v = v + (double)s_w[w][l + 96];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, o);
+      if (l == 0) out[(size_t)blockIdx.x * NWM + w] = v;
+    }
+  }
+}
 
 // ------------------------------------------------------------------------
 // exact helpers (left-to-right sums as gfortran evaluates sum/dot_product)

@@ -373,6 +373,44 @@ __global__ void k_hist_regrow(int n, History src, History dst) {
   }
 }
 
+// Canonical tables: every pair record moved to the table of its smaller
+// index (the reference's owner, imin), as particle removal expects them
+// (src/MContacts.f90:173-252, 579-633).  dst counts start at zero; the
+// records of a table come in no particular order (lookups go by partner).
+// status[0]: a table would overflow, status[1]: largest count asked for.
+// FP32 record values of the mixed mode move with them (sa.. -> da.., or
+// null in FP64 mode).
+__global__ void k_hist_canon(int n, History src, History dst, const float4* __restrict__ sa,
+                             const float4* __restrict__ sb, const float* __restrict__ sc,
+                             float4* __restrict__ da, float4* __restrict__ db,
+                             float* __restrict__ dc, int* status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int c = src.cnt[i];
+  for (int r = 0; r < c; r++) {
+    const size_t from = hslot(src, i, r);
+    const int q = src.key[from];
+    const bool move = q >= 0 && q < i;
+    const int o = move ? q : i;
+    const int s = atomicAdd(&dst.cnt[o], 1);
+    if (s >= dst.cap) {
+      atomicExch(&status[0], 1);
+      atomicMax(&status[1], s + 1);
+      continue;
+    }
+    const size_t to = hslot(dst, o, s);
+    dst.key[to] = move ? i : q;
+    if (sa) {
+      da[to] = sa[from];
+      db[to] = sb[from];
+      dc[to] = sc[from];
+    } else {
+#pragma unroll
+      for (int k = 0; k < 3; k++) dst.val[to * 3 + k] = src.val[from * 3 + k];
+    }
+  }
+}
+
 // observables: per-block partial sums (fixed order), reduced on the host
 template <bool PP>
 __global__ void k_observables(const DevParams* __restrict__ PT, const int* __restrict__ sysid,
@@ -516,8 +554,10 @@ __global__ void k_relink(const DevParams* __restrict__ PT, const int* __restrict
     }
     cnt->pair_contacts = 0ull;
     cnt->wall_contacts = 0ull;
-    for (int w = 0; w < NWM; w++) cnt->wall_fn[w] = 0.0;
-    if (update) cnt->need_capacity = 0;
+    if (update) {
+      cnt->need_capacity = 0;
+      cnt->need_in = 0;
+    }
     else cnt->escaped = 0ull;  // escapes are counted by the current step's corrector
     const double d = (double)__uint_as_float(cnt->disp_max);
     cnt->disp_max = 0u;
@@ -617,13 +657,12 @@ __global__ void k_relink(const DevParams* __restrict__ PT, const int* __restrict
 
 // The row of particle p (cell c), built by one warp.  Lane L < 27 owns the
 // neighbour cell at offset (L%3-1, L/3%3-1, L/9-1); lane 13 (own cell) walks
-// the part of the list after p (loop 1), lane 27 the part before p (loop 2).
-// Segments are ordered as the sweep meets them: loop 1 = own cell after p,
+// the part of the list after p, lane 27 the part before p (p's rank).  The
+// row holds the partners the sweep meets with p as "i": the own cell after p,
 // then the half-shell cells (offset index kx + Nx*(ky + Ny*kz) > 0,
 // AddAllNeighbours3D src/MCells.f90:456) in FirstNeighbour order, i.e.
-// descending (kz, ky, kx); loop 2 = the cells whose half shell holds c, and
-// p's own cell, in ascending cell index (the order of the sweep's outer
-// loop), own cell before p's own block.
+// descending (kz, ky, kx) -- NeighbourParticles' list (src/MCells.f90:
+// 793-829) from p on.
 template <bool PP>
 __device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int c,
                                           const double4* __restrict__ X,
@@ -638,8 +677,8 @@ __device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int 
   const int cx = cl % nx, cy = (cl / nx) % ny, cz = cl / (nx * ny);
   const double4 p4 = X[p];
   const int cp = PP ? 0 : comp[p];
-  int start = -1, stop = -1, order = 1 << 20, jc = 0x7fffffff;
-  int loop = 0;
+  int start = -1, order = 1 << 20;
+  bool walk = false;
   if (lane < 27) {
     const int d[3] = {lane % 3 - 1, (lane / 3) % 3 - 1, lane / 9 - 1};
     const int cc[3] = {cx, cy, cz};
@@ -660,33 +699,13 @@ __device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int 
     const int lex = d[0] + 3 * d[1] + 9 * d[2];
     if (lane == 13) {
       start = next[p];
-      loop = 1;
       order = 0;
-    } else if (ok) {
-      jc = P.coff + w[0] + nx * (w[1] + ny * w[2]);
-      start = head[jc];
-      if (lex > 0) {
-        loop = 1;
-        order = 1 + (13 - lex);
-      } else {
-        loop = 2;
-      }
+      walk = true;
+    } else if (ok && lex > 0) {
+      start = head[P.coff + w[0] + nx * (w[1] + ny * w[2])];
+      order = 1 + (13 - lex);
+      walk = true;
     }
-  } else if (lane == 27) {
-    start = head[c];
-    stop = p;
-    loop = 2;
-    jc = c;
-  }
-  // loop-2 segments in ascending cell index
-  {
-    int rank = 0;
-    for (int l = 0; l < 28; l++) {
-      const int ol = __shfl_sync(FULL, loop, l);
-      const int jl = __shfl_sync(FULL, jc, l);
-      if (ol == 2 && jl < jc) rank++;
-    }
-    if (loop == 2) order = 14 + rank;
   }
   const double skin = P.vl_skin;
   auto is_cand = [&](int q) -> bool {
@@ -702,35 +721,50 @@ __device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int 
     return md * md - DijSq > 0.0;
   };
   // pass 1: walk and count; the first 8 list elements and their test
-  // results stay in registers for pass 2
+  // results stay in registers for pass 2.  Lane 27 counts the list before p.
   int count = 0, walked = 0;
   unsigned hits = 0u;
   int cache[8];
   bool bad = false;
   int q = start;
 #pragma unroll
-  for (int i = 0; i < 8; i++) {
-    cache[i] = -1;
-    if (q != -1 && q != stop) {
-      cache[i] = q;
-      walked = i + 1;
-      if (is_cand(q)) {
-        hits |= 1u << i;
-        count++;
+  for (int i = 0; i < 8; i++) cache[i] = -1;
+  if (walk) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      if (q != -1) {
+        cache[i] = q;
+        walked = i + 1;
+        if (is_cand(q)) {
+          hits |= 1u << i;
+          count++;
+        }
+        q = next[q];
       }
-      q = next[q];
     }
   }
-  const int resume = q;  // first element not cached (-1 or stop: none)
+  const int resume = q;  // first element not cached (-1: none)
   {
     int guard = 0;
-    while (q != -1 && q != stop) {
-      if (++guard > n) {
-        bad = true;
-        break;
+    if (walk) {
+      while (q != -1) {
+        if (++guard > n) {
+          bad = true;
+          break;
+        }
+        if (is_cand(q)) count++;
+        q = next[q];
       }
-      if (is_cand(q)) count++;
-      q = next[q];
+    } else if (lane == 27) {
+      q = head[c];
+      while (q != p) {
+        if (q == -1 || ++guard > n) {
+          bad = true;
+          break;
+        }
+        count++;
+        q = next[q];
+      }
     }
   }
   if (__any_sync(FULL, bad)) {
@@ -740,18 +774,14 @@ __device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int 
     }
     return;
   }
-  int off = 0, n1 = 0, n2b = 0, n2a = 0;
-  const int own_order = __shfl_sync(FULL, order, 27);
-  for (int l = 0; l < 32; l++) {
+  int off = 0, m = 0;
+  for (int l = 0; l < 27; l++) {
     const int ol = __shfl_sync(FULL, order, l);
-    const int cl = __shfl_sync(FULL, count, l);
-    const int pl = __shfl_sync(FULL, loop, l);
-    if (ol < order) off += cl;
-    if (pl == 1) n1 += cl;
-    else if (pl == 2 && ol <= own_order) n2b += cl;
-    else if (pl == 2) n2a += cl;
+    const int cl2 = __shfl_sync(FULL, walk ? count : 0, l);
+    if (ol < order) off += cl2;
+    m += cl2;
   }
-  const int m = n1 + n2b + n2a;
+  const int rank = __shfl_sync(FULL, count, 27);
   if (m > R.kc) {
     if (lane == 0) {
       atomicMax(&cnt->need_kc, m);
@@ -762,18 +792,21 @@ __device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int 
     return;
   }
   // pass 2: write (the cached part, then the rest of the list)
-  {
+  if (walk) {
     int k = off;
 #pragma unroll
     for (int i = 0; i < 8; i++)
       if (i < walked && ((hits >> i) & 1u)) R.cand[(size_t)(k++) * n + p] = cache[i];
     int q2 = resume;
-    while (q2 != -1 && q2 != stop) {
+    while (q2 != -1) {
       if (is_cand(q2)) R.cand[(size_t)(k++) * n + p] = q2;
       q2 = next[q2];
     }
   }
-  if (lane == 0) R.meta[p] = n1 | (n2b << META_BITS) | (n2a << (2 * META_BITS));
+  if (lane == 0) {
+    R.meta[p] = m;
+    R.rank[p] = rank;
+  }
 }
 
 // Candidate rows of the pass: every row when the pass is due for a full
@@ -820,25 +853,46 @@ __global__ void __launch_bounds__(256) k_screen(const DevParams* __restrict__ PT
 }
 
 // ---------------------------------------------------------------------------
-// K2+K4: the FP64 pass kernel (exact order)
+// K2+K4: the FP64 force pass (exact order), two kernels.
+//
+// k_contact_fp64: one thread per particle p, as "i" of its row: the overlap
+//   test over the row, every contact evaluated once (one lane per contact),
+//   the "i" part folded by p in row order (iForce, iTorque), then p's walls
+//   and drag -- p's whole block of the sweep.  The "j" part of each contact
+//   (FN, FT, Nij x FT) goes to the partner's incoming records with p's sweep
+//   key.  The history record of the pair is looked up in p's table, then in
+//   the partner's, and rewritten into p's new table.
+// k_fold_fp64: one thread per particle: its incoming "j" results and its own
+//   block added in sweep order (Force(j) = Force(j) - FN - FT,
+//   Torque(j) = Torque(j) + Rj*Nij_x_FT, Force(i) = Force(i) + iForce,
+//   src/MForces.f90:254-259, 319-320), a = F/m, alpha = T/I, then the
+//   integrator epilogue.
+
+// record keys of the owner kept in shared memory by the contact kernels
+constexpr int KREG = 8;
 
 // Owner data handed to the lane that computes one of its contacts.
 struct OwnerF64 {
   double x, y, z, R, vx, vy, vz, wx, wy, wz;
-  int p, cp, n1, sys;
+  int p, cp, sys, pad;
+  unsigned long long key;
 };
 
 // MINB: resident blocks of 128 threads per SM the kernel is compiled for
 // (registers per thread <= 65536 / (128 * MINB)); the autotuner picks one.
-template <bool PP, int EPI, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_pass_fp64(
-    PassArgs<double4, double2> A) {
-  // per warp: the current 32 contacts (candidate index, owner lane, partner)
-  // and their results FN, FT, VT, torque term (12 doubles, lane-contiguous)
+template <bool PP, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_contact_fp64(PassArgs<double4, double2> A) {
+  // per warp: the current 32 contacts (candidate index, owner lane), their
+  // "i" results FN, FT, VT, torque term (12 doubles), the owners' first
+  // record keys, record counts and the records their contacts matched
   __shared__ int s_k[4][32], s_o[4][32], s_q[4][32];
+  __shared__ int s_hk[4][KREG][32], s_hc[4][32];
+  __shared__ unsigned s_match[4][32];
   __shared__ double s_r[12][4][32];
+  __shared__ double s_w[NWM][128];  // |FN| of each wall contact
   if (A.cnt->abort) return;
-  const int wid = threadIdx.x >> 5;
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int w = 0; w < A.nw_max; w++) s_w[w][threadIdx.x] = 0.0;
   const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = p0 < A.n;
   const int p = valid ? p0 : 0;
@@ -846,8 +900,8 @@ __global__ void __launch_bounds__(128, MINB) k_pass_fp64(
   const Box& B = P.box;
   const int n = A.n;
   unsigned n_col = 0, n_pc = 0, n_wc = 0;
-  int need = 0;
-  double d2 = 0.0;
+  int need = 0, need_in = 0;
+  bool in_over = false;
 
   const int c = A.cell_cur[p];
   const double4 p4 = A.X[p];
@@ -860,17 +914,22 @@ __global__ void __launch_bounds__(128, MINB) k_pass_fp64(
   const int cp = PP ? 0 : A.comp[p];
   double inv_m, inv_i, eff_m;
   Material<PP>::self(P, cp, Rp, inv_m, inv_i, eff_m);
-  int n1, n2b, n2a;
-  unpack_meta(A.meta[p], n1, n2b, n2a);
+  const int n1 = A.meta[p] & META_MASK;
+  const unsigned long long key_p = sweep_key(c, A.rank[p]);
   const double half_dt = A.half_dt;
   const bool update = A.update != 0;
   int hw_n = 0;
   bool overflow = false;
+  const int hc = valid ? A.Hr.cnt[p] : 0;
+#pragma unroll
+  for (int r = 0; r < KREG; r++) s_hk[wid][r][lane] = r < hc ? A.Hr.key[hslot(A.Hr, p, r)] : -1;
+  s_hc[wid][lane] = hc;
+  s_match[wid][lane] = 0u;
+  __syncwarp();
 
   double iF[3], iT[3] = {0.0, 0.0, 0.0};
 #pragma unroll
   for (int k = 0; k < 3; k++) iF[k] = eff_m * P.gravity[k];
-  double F[3] = {0.0, 0.0, 0.0}, T[3] = {0.0, 0.0, 0.0};
 
   auto record = [&](int partner, const double ft[3], const double vt[3]) {
     if (hw_n < A.Hw.cap)
@@ -879,77 +938,81 @@ __global__ void __launch_bounds__(128, MINB) k_pass_fp64(
       overflow = true;
     hw_n++;
   };
-  // Rij = x_j - x_i (minimum image, src/MForces.f90:209-217); candidate k
-  // of a row is "j" (its owner is "i") for k < n1, else "i"
-  auto geometry = [&](const Box& Bx, bool oi, const double xo[3], const double4& q4,
+  // Rij = x_j - x_i (minimum image, src/MForces.f90:209-217)
+  auto geometry = [&](const Box& Bx, const double xo[3], const double4& q4,
                       double Rij[3]) -> double {
-    Rij[0] = oi ? q4.x - xo[0] : xo[0] - q4.x;
-    Rij[1] = oi ? q4.y - xo[1] : xo[1] - q4.y;
-    Rij[2] = oi ? q4.z - xo[2] : xo[2] - q4.z;
+    Rij[0] = q4.x - xo[0];
+    Rij[1] = q4.y - xo[1];
+    Rij[2] = q4.z - xo[2];
 #pragma unroll
     for (int k = 0; k < 3; k++) Rij[k] = min_image_exact(Rij[k], Bx, k);
     return sumsq3(Rij);
   };
   // the overlap test DeltaDijSq = MinDijSq - DijSq > 0 (src/MForces.f90:218-224)
-  auto test = [&](int k, int q, const double4& q4) -> bool {
-    const bool pi = k < n1;
+  auto test = [&](int, int q, const double4& q4) -> bool {
     double Rij[3];
-    const double DijSq = geometry(B, pi, xp, q4, Rij);
+    const double DijSq = geometry(B, xp, q4, Rij);
     const int cq = PP ? 0 : A.comp[q];
-    const double mds = pi ? Material<PP>::min_dij_sq(P, cp, Rp, cq, q4.w)
-                          : Material<PP>::min_dij_sq(P, cq, q4.w, cp, Rp);
-    return mds - DijSq > 0.0;
+    return Material<PP>::min_dij_sq(P, cp, Rp, cq, q4.w) - DijSq > 0.0;
   };
-  // one contact of owner `o` in the reference's orientation
-  // (src/MForces.f90:199-272), computed by this lane
-  auto compute = [&](const OwnerF64& o, int k, int slot) {
+  // one contact of owner `o` ("i") with candidate k ("j"), computed by this
+  // lane (src/MForces.f90:199-252)
+  auto compute = [&](const OwnerF64& o, int oo, int k, int slot) {
     const int q = __ldg(A.cand + (size_t)k * n + o.p);
-    const bool oi = k < o.n1;
+    const int s_in = atomicAdd(&A.in_cnt[q], 1);  // q's "j" record (returns early)
     const double4 q4 = A.X[q];
+    const double2 qw2 = A.w2[q];
+    const double4 qv4 = A.v4[q];
     const double xo[3] = {o.x, o.y, o.z};
     double Rij[3];
     const DevParams& PO = A.P[o.sys];  // the owner's system (a warp may span two)
-    const double DijSq = geometry(PO.box, oi, xo, q4, Rij);
+    const double DijSq = geometry(PO.box, xo, q4, Rij);
     const int cq = PP ? 0 : A.comp[q];
-    const int ca = oi ? o.cp : cq, cb = oi ? cq : o.cp;
-    const double Ra = oi ? o.R : q4.w, Rb = oi ? q4.w : o.R;
-    const double Delta = Material<PP>::min_dij_sq(PO, ca, Ra, cb, Rb) - DijSq;
+    const double Delta = Material<PP>::min_dij_sq(PO, o.cp, o.R, cq, q4.w) - DijSq;
     PairPar pp;
-    Material<PP>::pair(PO, ca, Ra, cb, Rb, pp);
-    const double4 qv4 = A.v4[q];
-    const double2 qw2 = A.w2[q];
-    const double vo[3] = {o.vx, o.vy, o.vz}, wo[3] = {o.wx, o.wy, o.wz};
-    const double vq[3] = {qv4.x, qv4.y, qv4.z}, wq[3] = {qv4.w, qw2.x, qw2.y};
-    double va[3], wa[3], vb[3], wb[3];
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      va[d] = oi ? vo[d] : vq[d];
-      wa[d] = oi ? wo[d] : wq[d];
-      vb[d] = oi ? vq[d] : vo[d];
-      wb[d] = oi ? wq[d] : wo[d];
-    }
-    const int lo = o.p < q ? o.p : q, hi = o.p < q ? q : o.p;
+    Material<PP>::pair(PO, o.cp, o.R, cq, q4.w, pp);
+    const double va[3] = {o.vx, o.vy, o.vz}, wa[3] = {o.wx, o.wy, o.wz};
+    const double vb[3] = {qv4.x, qv4.y, qv4.z}, wb[3] = {qv4.w, qw2.x, qw2.y};
+    // VerifyPairContact: the owner's records, then the partner's
     double FT0[3] = {0.0, 0.0, 0.0}, VT0[3] = {0.0, 0.0, 0.0};
-    const int r = find_record(A.Hr, lo, hi);
-    const bool contacting = r >= 0;
-    if (contacting) hist_read(A.Hr, lo, r, FT0, VT0);
-    if (oi) {
-      if (!contacting) n_col++;
-      n_pc++;
-    }
-    ContactOut out;
-    pair_contact(Rij, DijSq, Delta, pp, Ra, va, wa, Rb, vb, wb, half_dt, contacting, FT0, VT0,
-                 out);
-    double tq[3];
-    if (oi) {
-      double RN[3];
+    const int oc = s_hc[wid][oo];
+    int r = -1;
 #pragma unroll
-      for (int d = 0; d < 3; d++) RN[d] = o.R * out.N[d];
-      cross3(RN, out.FT, tq);
+    for (int rr = 0; rr < KREG; rr++)
+      if (rr < oc && s_hk[wid][rr][oo] == q) r = rr;
+    for (int rr = KREG; r < 0 && rr < oc; rr++)
+      if (A.Hr.key[hslot(A.Hr, o.p, rr)] == q) r = rr;
+    bool contacting = r >= 0;
+    if (contacting) {
+      hist_read(A.Hr, o.p, r, FT0, VT0);
+      if (r < 32) atomicOr(&s_match[wid][oo], 1u << r);
     } else {
-#pragma unroll
-      for (int d = 0; d < 3; d++) tq[d] = o.R * out.NxFT[d];
+      const int r2 = find_record(A.Hr, q, o.p);
+      contacting = r2 >= 0;
+      if (contacting) hist_read(A.Hr, q, r2, FT0, VT0);
     }
+    if (!contacting) n_col++;
+    n_pc++;
+    ContactOut out;
+    pair_contact(Rij, DijSq, Delta, pp, o.R, va, wa, q4.w, vb, wb, half_dt, contacting, FT0, VT0,
+                 out);
+    // "j" side into q's incoming records
+    if (s_in < A.in_cap) {
+      InRec64* rec = (InRec64*)A.in_rec + (size_t)s_in * A.in_stride + q;
+      rec->a = make_double2(__longlong_as_double((long long)o.key), out.FN[0]);
+      rec->b = make_double2(out.FN[1], out.FN[2]);
+      rec->c = make_double2(out.FT[0], out.FT[1]);
+      rec->d = make_double2(out.FT[2], out.NxFT[0]);
+      rec->e = make_double2(out.NxFT[1], out.NxFT[2]);
+    } else {
+      in_over = true;
+    }
+    need_in = need_in > s_in + 1 ? need_in : s_in + 1;
+    // "i" side to the owner (iTorque + (Ri*Nij) x FT)
+    double RN[3], tq[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) RN[d] = o.R * out.N[d];
+    cross3(RN, out.FT, tq);
 #pragma unroll
     for (int d = 0; d < 3; d++) {
       s_r[d][wid][slot] = out.FN[d];
@@ -959,8 +1022,8 @@ __global__ void __launch_bounds__(128, MINB) k_pass_fp64(
     }
     s_q[wid][slot] = q;
   };
-  // the owner adds one contact (iForce/iTorque as "i", Force/Torque as "j")
-  auto accum = [&](int slot, int k) {
+  // the owner adds one contact (iForce = iForce + FN + FT) and stores its record
+  auto accum = [&](int slot, int) {
     double FN[3], FT[3], VT[3], tq[3];
 #pragma unroll
     for (int d = 0; d < 3; d++) {
@@ -969,22 +1032,18 @@ __global__ void __launch_bounds__(128, MINB) k_pass_fp64(
       VT[d] = s_r[6 + d][wid][slot];
       tq[d] = s_r[9 + d][wid][slot];
     }
-    if (k < n1) {
 #pragma unroll
-      for (int d = 0; d < 3; d++) iF[d] = iF[d] + FN[d] + FT[d];
+    for (int d = 0; d < 3; d++) iF[d] = iF[d] + FN[d] + FT[d];
 #pragma unroll
-      for (int d = 0; d < 3; d++) iT[d] = iT[d] + tq[d];
-    } else {
-#pragma unroll
-      for (int d = 0; d < 3; d++) F[d] = F[d] - FN[d] - FT[d];
-#pragma unroll
-      for (int d = 0; d < 3; d++) T[d] = T[d] + tq[d];
-    }
-    const int q = s_q[wid][slot];
-    if (update && p < q) record(q, FT, VT);
+    for (int d = 0; d < 3; d++) iT[d] = iT[d] + tq[d];
+    if (update) record(s_q[wid][slot], FT, VT);
   };
-  // walls (src/MForces.f90:274-314)
-  auto walls = [&]() {
+  const OwnerF64 me{xp[0], xp[1], xp[2], Rp, vp[0], vp[1], vp[2], wp[0], wp[1], wp[2],
+                    p, cp, A.sysid ? A.sysid[p] : 0, 0, key_p};
+  contact_loop(A.cand, A.X, n, p, valid, n1, me, s_k[wid], s_o[wid], test, compute, accum);
+
+  if (valid) {
+    // ---- walls (src/MForces.f90:274-314)
     for (int w = 0; w < P.nw; w++) {
       const dem_wall& W = P.walls[w];
       const int wi = p * P.nw + w;
@@ -997,8 +1056,7 @@ __global__ void __launch_bounds__(128, MINB) k_pass_fp64(
         VT0[0] = b.y; VT0[1] = d.x; VT0[2] = d.y;
       }
       double Dij, Nij[3], Qji[3];
-      bool ov = false;
-      ov = overlap_wall(P, W, xp, Rp, Dij, Nij, Qji);
+      const bool ov = overlap_wall(P, W, xp, Rp, Dij, Nij, Qji);
       if (ov) {
         n_wc++;
         const double Delta = Rp * Rp - Dij * Dij;
@@ -1029,7 +1087,7 @@ __global__ void __launch_bounds__(128, MINB) k_pass_fp64(
         cross3(RN, o.FT, tq);
 #pragma unroll
         for (int k = 0; k < 3; k++) iT[k] = iT[k] + tq[k];
-        atomicAdd(&A.cnt->wall_fn[w], sqrt(sumsq3(o.FN)));
+        s_w[w][threadIdx.x] = sqrt(sumsq3(o.FN));
         if (update) {
           A.Hw.wflag[wi] = 1;
           double2* v = A.Hw.wval + (size_t)wi * 3;
@@ -1041,30 +1099,23 @@ __global__ void __launch_bounds__(128, MINB) k_pass_fp64(
         A.Hw.wflag[wi] = 0;
       }
     }
-  };
-  // Force(i) = Force(i) + iForce where p's own block ends (src/MForces.f90:319-320)
-  auto own = [&]() {
     if (A.drag) {  // iForce = iForce + DragForce(iPart) (src/MForces.f90:316)
 #pragma unroll
       for (int k = 0; k < 3; k++) iF[k] = iF[k] + A.drag[(size_t)3 * p + k];
     }
-#pragma unroll
-    for (int k = 0; k < 3; k++) F[k] = F[k] + iF[k];
-#pragma unroll
-    for (int k = 0; k < 3; k++) T[k] = T[k] + iT[k];
-  };
-  const OwnerF64 me{xp[0], xp[1], xp[2], Rp, vp[0], vp[1], vp[2], wp[0], wp[1], wp[2],
-                    p, cp, n1, A.sysid ? A.sysid[p] : 0};
-  contact_loop(A.cand, A.X, n, p, valid, n1, n2b, n1 + n2b + n2a, P.nw > 0, me, s_k[wid],
-               s_o[wid], test, compute, accum, walls, own);
-
-  if (valid) {
-    // ---- records of pairs the sweep did not visit are kept as they were
-    // (a partner index past the last particle is a record that particle
-    // removal left behind: never visited)
+    Own64* ow = (Own64*)A.own + p;
+    ow->a = make_double2(iF[0], iF[1]);
+    ow->b = make_double2(iF[2], iT[0]);
+    ow->c = make_double2(iT[1], iT[2]);
+    // ---- the records this particle holds and no contact of the pass
+    // matched: kept if the sweep did not visit the pair (its cells are not
+    // neighbours, or the partner index lies past the last particle, a record
+    // that particle removal left behind), else the contact ended
+    // (RemovePairContact) or the other particle evaluated it
     if (update) {
-      const int nold = A.Hr.cnt[p];
-      for (int r = 0; r < nold; r++) {
+      const unsigned matched = s_match[wid][lane];
+      for (int r = 0; r < hc; r++) {
+        if (r < 32 && ((matched >> r) & 1u)) continue;
         const int q2 = A.Hr.key[hslot(A.Hr, p, r)];
         if (q2 >= A.n || !cells_adjacent(P, c, A.cell_cur[q2])) {
           double ft[3], vt[3];
@@ -1073,13 +1124,71 @@ __global__ void __launch_bounds__(128, MINB) k_pass_fp64(
         }
       }
       A.Hw.cnt[p] = hw_n < A.Hw.cap ? hw_n : A.Hw.cap;
-      if (overflow) {
-        // the pass is launched again with larger tables; stop what follows
-        atomicExch(&A.cnt->overflow, 1);
-        set_abort(A.cnt, A.tag);
-      }
       need = hw_n;
     }
+  }
+  if (A.nw_max > 0) wall_partials(s_w, A.nw_max, A.wall_part);
+  // a table that overflowed: the pass is launched again with larger tables;
+  // stop what follows
+  if (overflow) {
+    atomicExch(&A.cnt->overflow, 1);
+    set_abort(A.cnt, A.tag);
+  }
+  if (in_over) {
+    atomicExch(&A.cnt->in_overflow, 1);
+    set_abort(A.cnt, A.tag);
+  }
+  need_in = (int)__reduce_max_sync(0xffffffffu, (unsigned)need_in);
+  if (lane == 0 && need_in) atomicMax(&A.cnt->need_in, need_in);
+  publish_counts(A.cnt, A.update != 0, n_col, n_pc, n_wc, (unsigned)need);
+}
+
+// The fold kernel: Force and Torque of every particle in sweep order, a =
+// F/m, alpha = T/I (src/MForces.f90:330-333), then the integrator epilogue.
+template <bool PP, int EPI, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_fold_fp64(PassArgs<double4, double2> A) {
+  if (A.cnt->abort) return;
+  const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = p0 < A.n;
+  const int p = valid ? p0 : 0;
+  double d2 = 0.0;
+  if (valid) {
+    const DevParams& P = sys_params(A.P, A.sysid, p);
+    const int c = A.cell_cur[p];
+    const unsigned long long key_p = sweep_key(c, A.rank[p]);
+    const int ni = A.in_cnt[p];
+    A.in_cnt[p] = 0;  // for the next pass's contact kernel
+    const double4 p4 = A.X[p];
+    const double xp[3] = {p4.x, p4.y, p4.z};
+    const double Rp = p4.w;
+    const int cp = PP ? 0 : A.comp[p];
+    double inv_m, inv_i, eff_m;
+    Material<PP>::self(P, cp, Rp, inv_m, inv_i, eff_m);
+    const Own64 ow = ((const Own64*)A.own)[p];
+    const InRec64* in = (const InRec64*)A.in_rec + p;
+    const size_t st = (size_t)A.in_stride;
+    double F[3] = {0.0, 0.0, 0.0}, T[3] = {0.0, 0.0, 0.0};
+    fold_in_order(
+        ni, key_p,
+        [&](int e) {
+          return (unsigned long long)__double_as_longlong(((const double*)(in + e * st))[0]);
+        },
+        [&]() {
+          const double iF[3] = {ow.a.x, ow.a.y, ow.b.x}, iT[3] = {ow.b.y, ow.c.x, ow.c.y};
+#pragma unroll
+          for (int k = 0; k < 3; k++) F[k] = F[k] + iF[k];
+#pragma unroll
+          for (int k = 0; k < 3; k++) T[k] = T[k] + iT[k];
+        },
+        [&](int e) {
+          const InRec64 r = in[e * st];
+          const double FN[3] = {r.a.y, r.b.x, r.b.y}, FT[3] = {r.c.x, r.c.y, r.d.x};
+          const double NxFT[3] = {r.d.y, r.e.x, r.e.y};
+#pragma unroll
+          for (int k = 0; k < 3; k++) F[k] = F[k] - FN[k] - FT[k];
+#pragma unroll
+          for (int k = 0; k < 3; k++) T[k] = T[k] + Rp * NxFT[k];
+        });
     if (EPI == EPI_STORE && A.amsum) {
       const size_t n3 = (size_t)3 * A.n;
 #pragma unroll
@@ -1087,15 +1196,17 @@ __global__ void __launch_bounds__(128, MINB) k_pass_fp64(
 #pragma unroll
       for (int k = 0; k < 3; k++) A.amsum[n3 + (size_t)3 * p + k] = T[k];
     }
-    // ---- a = F/m, alpha = T/I (src/MForces.f90:330-333) + epilogue
     double acc[3], alp[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) acc[k] = F[k] * inv_m;
 #pragma unroll
     for (int k = 0; k < 3; k++) alp[k] = T[k] * inv_i;
+    const double4 pv4 = A.v4[p];
+    const double2 pw2 = A.w2[p];
+    const double vp[3] = {pv4.x, pv4.y, pv4.z};
+    const double wp[3] = {pv4.w, pw2.x, pw2.y};
     epilogue<EPI>(A, P, p, xp, Rp, vp, wp, acc, alp, c, d2);
   }
-  publish_counts(A.cnt, A.update != 0, n_col, n_pc, n_wc, (unsigned)need);
   if (EPI != EPI_STORE) publish_disp(A.cnt, d2);
 }
 

@@ -107,6 +107,16 @@ struct dem_ctx {
   int drag_cap = 0;
   double* amsum = nullptr;  // [9*ncap] corrector ring sums (predictor -> corrector)
   int amsum_cap = 0;
+  // contact kernel -> fold kernel of a pass: "j" results per particle
+  // (count, in_cap records of InRec64/InRec32 laid out for pass_cap rows) and
+  // the "i" block of every particle (Own64/Own32)
+  int* in_cnt = nullptr;
+  void* in_rec = nullptr;
+  void* own = nullptr;
+  double* wall_part = nullptr;  // [contact-kernel blocks][NWM] wall normal forces
+  int nw_max = 0;               // walls of the system with the most
+  int in_cap = 8;
+  int pass_cap = 0;
   double2* pour_cand = nullptr;  // candidate points of one PourParticle call
   int* pour_fits = nullptr;
   int pour_cap = 0;
@@ -279,7 +289,17 @@ void free_lists(dem_ctx* c) {
   }
   cudaFree(c->rows.cand);
   cudaFree(c->rows.meta);
+  cudaFree(c->rows.rank);
   c->rows = Rows{};
+  cudaFree(c->in_cnt);
+  cudaFree(c->in_rec);
+  cudaFree(c->own);
+  cudaFree(c->wall_part);
+  c->in_cnt = nullptr;
+  c->in_rec = nullptr;
+  c->own = nullptr;
+  c->wall_part = nullptr;
+  c->pass_cap = 0;
   for (int b = 0; b < 2; b++) {
     cudaFree(c->X[b]);
     cudaFree(c->v4[b]);
@@ -446,6 +466,8 @@ int grow_capacity(dem_ctx* c, int newcap) {
   CK(fresh(c->rows.cand, N * (size_t)c->rows.kc, 0));
   CK(fresh(c->rows.meta, N, 0));
   CK(cudaMemsetAsync(c->rows.meta, 0, sizeof(int) * N, c->stream));
+  CK(fresh(c->rows.rank, N, 0));
+  CK(cudaMemsetAsync(c->rows.rank, 0, sizeof(int) * N, c->stream));
   if (N > n) CK(cudaMemsetAsync(L.mflag + n, 0, sizeof(int) * (N - n), c->stream));
   for (int b = 0; b < 2; b++) {
     CK(fresh(c->X[b], N, 0));
@@ -571,12 +593,72 @@ PassArgs<V4, W2> pass_args(dem_ctx* c, int side, bool update, double dt, const R
   A.tag = tag;
   A.drag = c->fluid ? c->drag : nullptr;
   A.amsum = c->amsum;
+  A.rank = c->rows.rank;
+  A.in_cnt = c->in_cnt;
+  A.in_rec = c->in_rec;
+  A.in_cap = c->in_cap;
+  A.in_stride = c->pass_cap;
+  A.own = c->own;
+  A.wall_part = c->wall_part;
+  A.nw_max = c->nw_max;
   return A;
+}
+
+size_t in_rec_bytes(const dem_ctx* c) {
+  return c->precision == DEM_PREC_MIXED ? sizeof(InRec32) : sizeof(InRec64);
+}
+
+// the "j" records of a pass laid out for in_cap records of pass_cap rows
+int alloc_incoming(dem_ctx* c, int cap) {
+  cudaFree(c->in_rec);
+  c->in_rec = nullptr;
+  CK(cudaMalloc(&c->in_rec, in_rec_bytes(c) * (size_t)cap * (size_t)c->pass_cap));
+  c->in_cap = cap;
+  return DEM_OK;
+}
+
+// more "j" records per particle (the records only live within a pass)
+int grow_incoming(dem_ctx* c, int need) {
+  int cap = std::max(c->in_cap, 1);
+  while (cap < need) cap *= 2;
+  if (cap == c->in_cap) return DEM_OK;
+  CK(cudaStreamSynchronize(c->stream));
+  int st = alloc_incoming(c, cap);
+  if (st) return st;
+  drop_graphs(c);
+  return DEM_OK;
+}
+
+// room for the two-kernel handover of a pass (counts start at zero)
+int ensure_pass_buffers(dem_ctx* c) {
+  const int N = std::max(c->ncap, 1);
+  if (c->pass_cap >= N) return DEM_OK;
+  CK(cudaStreamSynchronize(c->stream));
+  cudaFree(c->in_cnt);
+  cudaFree(c->own);
+  cudaFree(c->wall_part);
+  c->in_cnt = nullptr;
+  c->own = nullptr;
+  c->wall_part = nullptr;
+  c->pass_cap = N;
+  CK(cudaMalloc(&c->in_cnt, sizeof(int) * (size_t)N));
+  CK(cudaMemset(c->in_cnt, 0, sizeof(int) * (size_t)N));
+  CK(cudaMalloc(&c->own, (c->precision == DEM_PREC_MIXED ? sizeof(Own32) : sizeof(Own64)) *
+                             (size_t)N));
+  const size_t parts = (size_t)blocks_for(N, 128) * NWM;
+  CK(cudaMalloc(&c->wall_part, sizeof(double) * parts));
+  CK(cudaMemset(c->wall_part, 0, sizeof(double) * parts));
+  drop_graphs(c);
+  return alloc_incoming(c, c->in_cap);
 }
 
 // room for the drag of every sphere and the corrector ring sums (outside
 // graph capture)
 int ensure_drag(dem_ctx* c) {
+  {
+    int st = ensure_pass_buffers(c);
+    if (st) return st;
+  }
   if (c->nprev > 0 && c->amsum_cap < std::max(c->ncap, 1)) {
     cudaFree(c->amsum);
     c->amsum = nullptr;
@@ -613,33 +695,38 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
   if (c->precision == DEM_PREC_MIXED) {
     auto A = pass_args<float4, float2>(c, side, update, dt, rm, tag, tgt);
     if (epi == EPI_STORE) A.amsum = c->force_out;
-    timed(c, "pass_mixed",
-          [&]() {
-            mixed_pass(c->M, c->pp, epi, c->pass_variant, c->has_cone, A, c->hcur, c->stream);
-          });
-    c->launches++;
+    for (int part = 0; part < 2; part++) {
+      timed(c, part ? "fold_mixed" : "contact_mixed", [&]() {
+        mixed_pass(c->M, c->pp, epi, c->pass_variant, c->has_cone, A, c->hcur, c->stream, part);
+      });
+      c->launches++;
+    }
     return;
   }
   auto A = pass_args<double4, double2>(c, side, update, dt, rm, tag, tgt);
   if (epi == EPI_STORE) A.amsum = c->force_out;
   const unsigned g = blocks_for(c->n, 128);
-#define PASS_CASE(PPV, MB)                                                              \
-  do {                                                                                  \
-    if (epi == EPI_PREDICT)                                                             \
-      launch(c, "pass_fp64", k_pass_fp64<PPV, EPI_PREDICT, MB>, g, 128, A);             \
-    else if (epi == EPI_CORRECT)                                                        \
-      launch(c, "pass_fp64", k_pass_fp64<PPV, EPI_CORRECT, MB>, g, 128, A);             \
-    else                                                                                \
-      launch(c, "pass_fp64", k_pass_fp64<PPV, EPI_STORE, MB>, g, 128, A);               \
-  } while (0)
+#define CONTACT_CASE(PPV, MB) launch(c, "contact_fp64", k_contact_fp64<PPV, MB>, g, 128, A)
   if (c->pass_variant == 1) {
-    if (c->pp) PASS_CASE(true, 3);
-    else PASS_CASE(false, 3);
+    if (c->pp) CONTACT_CASE(true, 3);
+    else CONTACT_CASE(false, 3);
   } else {
-    if (c->pp) PASS_CASE(true, 4);
-    else PASS_CASE(false, 4);
+    if (c->pp) CONTACT_CASE(true, 4);
+    else CONTACT_CASE(false, 4);
   }
-#undef PASS_CASE
+#undef CONTACT_CASE
+#define FOLD_CASE(PPV)                                                            \
+  do {                                                                            \
+    if (epi == EPI_PREDICT)                                                       \
+      launch(c, "fold_fp64", k_fold_fp64<PPV, EPI_PREDICT, 4>, g, 128, A);        \
+    else if (epi == EPI_CORRECT)                                                  \
+      launch(c, "fold_fp64", k_fold_fp64<PPV, EPI_CORRECT, 4>, g, 128, A);        \
+    else                                                                          \
+      launch(c, "fold_fp64", k_fold_fp64<PPV, EPI_STORE, 4>, g, 128, A);          \
+  } while (0)
+  if (c->pp) FOLD_CASE(true);
+  else FOLD_CASE(false);
+#undef FOLD_CASE
 }
 
 // Copies of `side` for the pass kernel and the cell transition towards its
@@ -724,8 +811,10 @@ int clear_abort(dem_ctx* c) {
   CK(cudaMemsetAsync(&d->ncol_pending, 0, sizeof(unsigned long long), c->stream));
   CK(cudaMemsetAsync(&d->pair_contacts, 0, 2 * sizeof(unsigned long long), c->stream));
   CK(cudaMemsetAsync(&d->overflow, 0, 4 * sizeof(int), c->stream));
-  CK(cudaMemsetAsync(&d->row_overflow, 0, 2 * sizeof(int), c->stream));
-  CK(cudaMemsetAsync(&d->wall_fn[0], 0, sizeof(double) * NWM, c->stream));
+  CK(cudaMemsetAsync(&d->row_overflow, 0, 4 * sizeof(int), c->stream));  // .. in_overflow, need_in
+  // the stopped contact kernel may have counted "j" records
+  if (c->pass_cap > 0)
+    CK(cudaMemsetAsync(c->in_cnt, 0, sizeof(int) * (size_t)c->pass_cap, c->stream));
   return DEM_OK;
 }
 
@@ -762,6 +851,10 @@ int finish_pass(dem_ctx* c, int side, bool update, double dt, int epi, const Rin
     if (st) return st;
     if (h.overflow) {
       st = grow_history(c, std::max(h.need_capacity, c->hcap + 1));
+      if (st) return st;
+    }
+    if (h.in_overflow) {
+      st = grow_incoming(c, std::max(h.need_in, c->in_cap + 1));
       if (st) return st;
     }
     if (h.row_overflow) {
@@ -802,6 +895,53 @@ int force_pass(dem_ctx* c, int side, bool update, double dt, int epi, const Ring
   return DEM_OK;
 }
 
+// Pair records into the tables of their imin (the current records go to the
+// other buffer, which becomes current); the wall records are copied along.
+int canonical_history(dem_ctx* c) {
+  const int n = c->n;
+  if (n == 0) return DEM_OK;
+  const bool mixed = c->precision == DEM_PREC_MIXED;
+  // two status words past the removal's own (state[0..8+NCM) of k_remove)
+  static_assert(8 + NCM + 2 <= RM_STATE_WORDS, "status words");
+  int* status = c->rm_buf + RM_STATE_WORDS - 2;
+  for (int attempt = 0;; attempt++) {
+    const int cur = c->hcur, nxt = cur ^ 1;
+    History& S = c->H[cur];
+    History& D = c->H[nxt];
+    CK(cudaMemsetAsync(status, 0, 2 * sizeof(int), c->stream));
+    CK(cudaMemsetAsync(D.cnt, 0, sizeof(int) * (size_t)n, c->stream));
+    launch(c, "hist_canon", k_hist_canon, blocks_for(n, 256), 256, n, S, D,
+           (const float4*)(mixed ? c->M.ha[cur] : nullptr),
+           (const float4*)(mixed ? c->M.hb[cur] : nullptr),
+           (const float*)(mixed ? c->M.hc[cur] : nullptr), mixed ? c->M.ha[nxt] : nullptr,
+           mixed ? c->M.hb[nxt] : nullptr, mixed ? c->M.hc[nxt] : nullptr, status);
+    int hs[2] = {0, 0};
+    CK(cudaMemcpyAsync(hs, status, sizeof(hs), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (hs[0]) {
+      if (attempt >= 4) return fail(c, DEM_ERR_CAPACITY, "history tables cannot be grown");
+      int st = grow_history(c, hs[1] + 2);
+      if (st) return st;
+      continue;
+    }
+    const size_t w = (size_t)n * (size_t)std::max(c->params.n_walls, 1);
+    CK(cudaMemcpyAsync(D.wflag, S.wflag, sizeof(int) * w, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(D.wval, S.wval, sizeof(double2) * 3 * w, cudaMemcpyDeviceToDevice,
+                       c->stream));
+    if (mixed) {
+      CK(cudaMemcpyAsync(c->M.wa[nxt], c->M.wa[cur], sizeof(float4) * w,
+                         cudaMemcpyDeviceToDevice, c->stream));
+      CK(cudaMemcpyAsync(c->M.wb[nxt], c->M.wb[cur], sizeof(float4) * w,
+                         cudaMemcpyDeviceToDevice, c->stream));
+      CK(cudaMemcpyAsync(c->M.wc[nxt], c->M.wc[cur], sizeof(float) * w, cudaMemcpyDeviceToDevice,
+                         c->stream));
+    }
+    c->hcur = nxt;
+    drop_graphs(c);
+    return DEM_OK;
+  }
+}
+
 // UpdateParticleList (src/MDEM.f90:612-671): the escaped particles are
 // listed by one grid-wide kernel, then removed by k_remove (one block, in
 // decreasing index).  A removal that would overflow the history tables asks
@@ -831,6 +971,8 @@ int update_particle_list_impl(dem_ctx* c, int64_t* removed) {
   CK(cudaStreamSynchronize(c->stream));
   const int n_list = hs[7];
   if (n_list > 0) {
+    int st = canonical_history(c);
+    if (st) return st;
     for (int attempt = 0;; attempt++) {
       RemovalArgs A;
       A.PT = c->dp;
@@ -1435,9 +1577,11 @@ int dem_create_ensemble(const dem_params* ps, int32_t nsys, dem_ctx** out) {
   c->hcap = p->hist_capacity > 0 ? p->hist_capacity : 16;
   c->nsys = nsys;
   c->removal = nsys == 1;
-  for (int s = 0; s < nsys; s++)
+  for (int s = 0; s < nsys; s++) {
+    c->nw_max = std::max(c->nw_max, ps[s].n_walls);
     for (int w = 0; w < ps[s].n_walls; w++)
       if (ps[s].walls[w].shape == DEM_WALL_CONE) c->has_cone = true;
+  }
   c->hsys = hs;
   c->hp = hs[0];
   c->ncell_total = (int)ncell;
@@ -1609,6 +1753,8 @@ int dem_set_state(dem_ctx* c, int32_t n, const int32_t* comp, const double* radi
     CK(cudaMalloc(&c->rows.cand, sizeof(int) * N * (size_t)c->kc));
     CK(cudaMalloc(&c->rows.meta, sizeof(int) * N));
     CK(cudaMemsetAsync(c->rows.meta, 0, sizeof(int) * N, c->stream));
+    CK(cudaMalloc(&c->rows.rank, sizeof(int) * N));
+    CK(cudaMemsetAsync(c->rows.rank, 0, sizeof(int) * N, c->stream));
     c->rows.kc = c->kc;
     const bool mixed = c->precision == DEM_PREC_MIXED;
     for (int b = 0; b < 2; b++) {
@@ -1898,23 +2044,32 @@ int dem_get_contacts(dem_ctx* c, int64_t cap, int32_t* imin, int32_t* imax, doub
   int st = download_history(c, h);
   if (st) return st;
   const size_t N = (size_t)c->H[c->hcur].n;  // slot stride
-  int64_t a = 0, b = 0;
-  std::vector<int> ord;
-  for (int i = 0; i < c->n; i++) {
-    int k = h.cnt[i];
-    ord.resize(k);
-    for (int r = 0; r < k; r++) ord[r] = r;
-    std::sort(ord.begin(), ord.end(),
-              [&](int x, int y) { return h.key[(size_t)x * N + i] < h.key[(size_t)y * N + i]; });
-    for (int r : ord) {
-      if (a >= cap) return fail(c, DEM_ERR_INVALID, "pair record buffer too small");
-      imin[a] = i;
-      imax[a] = h.key[(size_t)r * N + i];
-      const double2* v = &h.val[((size_t)r * N + i) * 3];
-      ft[3 * a] = v[0].x; ft[3 * a + 1] = v[0].y; ft[3 * a + 2] = v[1].x;
-      vt[3 * a] = v[1].y; vt[3 * a + 1] = v[2].x; vt[3 * a + 2] = v[2].y;
-      a++;
+  // a record sits with either particle of its pair: export it as the
+  // reference's node (imin, imax), all nodes ordered by imin, then imax
+  struct Rec {
+    int lo, hi;
+    size_t slot;
+  };
+  std::vector<Rec> recs;
+  for (int i = 0; i < c->n; i++)
+    for (int r = 0; r < h.cnt[i]; r++) {
+      const size_t sl = (size_t)r * N + i;
+      const int k = h.key[sl];
+      recs.push_back(k < i ? Rec{k, i, sl} : Rec{i, k, sl});
     }
+  std::sort(recs.begin(), recs.end(),
+            [](const Rec& x, const Rec& y) { return x.lo != y.lo ? x.lo < y.lo : x.hi < y.hi; });
+  if ((int64_t)recs.size() > cap) return fail(c, DEM_ERR_INVALID, "pair record buffer too small");
+  int64_t a = 0, b = 0;
+  for (const Rec& q : recs) {
+    imin[a] = q.lo;
+    imax[a] = q.hi;
+    const double2* v = &h.val[q.slot * 3];
+    ft[3 * a] = v[0].x; ft[3 * a + 1] = v[0].y; ft[3 * a + 2] = v[1].x;
+    vt[3 * a] = v[1].y; vt[3 * a + 1] = v[2].x; vt[3 * a + 2] = v[2].y;
+    a++;
+  }
+  for (int i = 0; i < c->n; i++)
     for (int w = 0; w < c->params.n_walls; w++) {
       size_t wi = (size_t)i * c->params.n_walls + w;
       if (!h.wf[wi]) continue;
@@ -1926,7 +2081,6 @@ int dem_get_contacts(dem_ctx* c, int64_t cap, int32_t* imin, int32_t* imax, doub
       vtw[3 * b] = v[1].y; vtw[3 * b + 1] = v[2].x; vtw[3 * b + 2] = v[2].y;
       b++;
     }
-  }
   return DEM_OK;
 }
 
@@ -2158,6 +2312,10 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
     if (st) return st;
     if (c->hcnt->need_capacity + HEADROOM > c->hcap) {
       st = grow_history(c, c->hcnt->need_capacity + HEADROOM);
+      if (st) return st;
+    }
+    if (c->hcnt->need_in + HEADROOM > c->in_cap) {
+      st = grow_incoming(c, c->hcnt->need_in + HEADROOM);
       if (st) return st;
     }
     // a graph starts from prepared Particle copies
@@ -2428,6 +2586,66 @@ int dem_get_escaped(dem_ctx* c, int64_t* count) {
   return DEM_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Area of a wall that the spheres of a box can press on: a rectangle's
+// extent along each in-plane axis (the box axis it runs along) up to the box
+// length there, or a cone's lateral area.
+double wall_area(const dem_wall& W, const double* L) {
+  auto axis = [](const double* v) {
+    int k = 0;
+    for (int j = 1; j < 3; j++)
+      if (std::fabs(v[j]) > std::fabs(v[k])) k = j;
+    return k;
+  };
+  if (W.shape == DEM_WALL_RECTANGLE)
+    return std::min(2.0 * W.l1, L[axis(W.u)]) * std::min(2.0 * W.l2, L[axis(W.w)]);
+  if (W.shape == DEM_WALL_CONE) {
+    const double len = 2.0 * W.l1, dr = W.l3 - W.l2;
+    return 3.14159265358979323846 * (W.l2 + W.l3) * std::sqrt(len * len + dr * dr);
+  }
+  return 0.0;
+}
+
+// Solid volume and region volume of one system (see dem_observables): the
+// bed's lower 0.8*H for a system with gravity along -z and no periodicity
+// in z, else the whole box.  Returns whether the system has a bed (h = H).
+bool solid_fraction(const dem_params& q, const double* z, const double* R, int n,
+                    double& solid, double& region, double& h) {
+  const double pi = 3.14159265358979323846;
+  solid = 0.0;
+  h = 0.0;
+  if (!(q.gravity[2] < 0.0) || q.pbc[2] || n == 0) {
+    for (int i = 0; i < n; i++) solid += 4.0 / 3.0 * pi * R[i] * R[i] * R[i];
+    region = n ? q.lbox[0] * q.lbox[1] * q.lbox[2] : 0.0;
+    return false;
+  }
+  double base = -0.5 * q.lbox[2];
+  bool floor = false;
+  for (int w = 0; w < q.n_walls; w++) {
+    const dem_wall& W = q.walls[w];
+    if (W.shape == DEM_WALL_RECTANGLE && std::fabs(W.n[2]) > 0.99 &&
+        (!floor || W.position[2] < base)) {
+      base = W.position[2];
+      floor = true;
+    }
+  }
+  double mean = 0.0;
+  for (int i = 0; i < n; i++) mean += z[i] - base;
+  h = 2.0 * (mean / n);
+  const double top = 0.8 * h;
+  for (int i = 0; i < n; i++)
+    if (z[i] - base < top) solid += 4.0 / 3.0 * pi * R[i] * R[i] * R[i];
+  region = q.lbox[0] * q.lbox[1] * top;
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
 int dem_get_observables(dem_ctx* c, dem_observables* o) {
   if (!c || !o) return DEM_ERR_INVALID;
   if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
@@ -2452,21 +2670,59 @@ int dem_get_observables(dem_ctx* c, dem_observables* o) {
     for (int k = 0; k < 8; k++) acc[k] += part[(size_t)b * 8 + k];
   o->kinetic_energy = 0.5 * acc[0];
   o->potential_energy = acc[1];
-  double vol = 0.0;  // ensembles: all boxes together
-  for (const dem_params& q : c->sys_params) vol += q.lbox[0] * q.lbox[1] * q.lbox[2];
-  o->packing_fraction = acc[2] / vol;
   o->momentum[0] = acc[3];
   o->momentum[1] = acc[4];
   o->momentum[2] = acc[5];
+  // solid fraction (bed or whole box) and bed height, per system, in index
+  // order on the host
+  {
+    std::vector<double> z((size_t)std::max(c->n, 1)), rad((size_t)std::max(c->n, 1));
+    if (c->n > 0) {
+      CK(cudaMemcpy(z.data(), c->P.pz, sizeof(double) * c->n, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(rad.data(), c->radius, sizeof(double) * c->n, cudaMemcpyDeviceToHost));
+    }
+    double solid = 0.0, region = 0.0, hsum = 0.0;
+    int nbed = 0;
+    for (int s = 0, off = 0; s < c->nsys; s++) {
+      const int cnt = c->nsys > 1 ? c->counts[(size_t)s] : c->n;
+      const dem_params& q = c->sys_params[(size_t)s];
+      double so = 0.0, re = 0.0, h = 0.0;
+      const bool bed = solid_fraction(q, z.data() + off, rad.data() + off, cnt, so, re, h);
+      solid += so;
+      region += re;
+      if (bed) {
+        hsum += h;
+        nbed++;
+      }
+      off += cnt;
+    }
+    o->packing_fraction = region > 0.0 ? solid / region : 0.0;
+    o->bed_height = nbed ? hsum / nbed : 0.0;
+  }
   int64_t np = 0, nw = 0;
   int st = dem_count_contacts(c, &np, &nw);
   if (st) return st;
-  o->n_pair_contacts = np;
-  o->n_wall_contacts = nw;
-  o->mean_coordination = c->n ? 2.0 * (double)np / (double)c->n : 0.0;
+  o->n_pair_records = np;
   st = read_counters(c);
   if (st) return st;
-  for (int w = 0; w < NWM; w++) o->wall_normal_force[w] = c->hcnt->wall_fn[w];
+  o->n_pair_contacts = (int64_t)c->hcnt->pair_contacts;
+  o->n_wall_contacts = (int64_t)c->hcnt->wall_contacts;
+  o->mean_coordination = c->n ? 2.0 * (double)o->n_pair_contacts / (double)c->n : 0.0;
+  // wall normal forces of the last contact kernel: block sums in block order
+  if (c->n > 0 && c->nw_max > 0) {
+    const size_t nb = blocks_for(c->n, 128);
+    std::vector<double> part(nb * NWM);
+    CK(cudaMemcpy(part.data(), c->wall_part, sizeof(double) * part.size(),
+                  cudaMemcpyDeviceToHost));
+    for (size_t b = 0; b < nb; b++)
+      for (int w = 0; w < c->nw_max; w++) o->wall_normal_force[w] += part[b * NWM + w];
+  }
+  for (int w = 0; w < c->nw_max; w++) {
+    double area = 0.0;
+    for (const dem_params& q : c->sys_params)
+      if (w < q.n_walls) area += wall_area(q.walls[w], q.lbox);
+    o->wall_pressure[w] = area > 0.0 ? o->wall_normal_force[w] / area : 0.0;
+  }
   return DEM_OK;
 }
 
@@ -2599,8 +2855,7 @@ int dem_get_row_stats(dem_ctx* c, int64_t* candidates, int32_t* row_capacity) {
       CK(cudaStreamSynchronize(c->stream));
       CK(cudaMemcpy(meta.data(), c->rows.meta, sizeof(int) * c->n, cudaMemcpyDeviceToHost));
       int64_t t = 0;
-      for (int m : meta)
-        t += (m & META_MASK) + ((m >> META_BITS) & META_MASK) + ((m >> (2 * META_BITS)) & META_MASK);
+      for (int m : meta) t += m & META_MASK;
       *candidates = t;
     }
   }

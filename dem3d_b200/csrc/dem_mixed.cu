@@ -233,30 +233,39 @@ __device__ __forceinline__ void rec_write(float4* a, float4* b, float* c, size_t
   c[i] = lo.z;
 }
 
-// The mixed-precision pass kernel: the FP64 kernel's structure (candidate
-// rows, exact FP64 overlap test, orientation, history semantics, summation
-// order), FP32 contact arithmetic, FP64 integrator epilogue.
+// The mixed-precision force pass: the FP64 kernels' structure (candidate
+// rows, exact FP64 overlap test, orientation, history semantics, each contact
+// evaluated once, summation order), FP32 contact arithmetic, FP64 integrator
+// epilogue.
+
+constexpr int KREG = 8;  // record keys of the owner kept in shared memory
 
 // Owner data handed to the lane that computes one of its contacts.
 struct OwnerMixed {
   double x, y, z, R;
   float vx, vy, vz, wx, wy, wz;
-  int p, cp, n1, sys;
+  int p, cp, sys, pad;
+  unsigned long long key;
 };
 
 // MINB: resident blocks of 128 threads per SM the kernel is compiled for
 // (registers per thread <= 65536 / (128 * MINB)); the autotuner picks one.
 // CONE: cone walls compiled in (only with MINB = 3: the branch costs
 // registers, and systems without cone walls launch CONE = false kernels).
-template <bool PP, int EPI, int MINB, bool CONE>
-__global__ void __launch_bounds__(128, MINB) k_pass_mixed(
+template <bool PP, int MINB, bool CONE>
+__global__ void __launch_bounds__(128, MINB) k_contact_mixed(
     PassArgs<float4, float2> A, MixedView V) {
-  // per warp: the current 32 contacts (candidate index, owner lane, partner)
-  // and their results FN, FT, FT remainder, VT, torque term (15 floats)
+  // per warp: the current 32 contacts (candidate index, owner lane, partner),
+  // their "i" results FN, FT, FT remainder, VT, torque term (15 floats), the
+  // owners' first record keys, record counts and matched records
   __shared__ int s_k[4][32], s_o[4][32], s_q[4][32];
+  __shared__ int s_hk[4][KREG][32], s_hc[4][32];
+  __shared__ unsigned s_match[4][32];
   __shared__ float s_r[15][4][32];
+  __shared__ float s_w[NWM][128];  // |FN| of each wall contact
   if (A.cnt->abort) return;
-  const int wid = threadIdx.x >> 5;
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int w = 0; w < A.nw_max; w++) s_w[w][threadIdx.x] = 0.f;
   const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = p0 < A.n;
   const int p = valid ? p0 : 0;
@@ -264,8 +273,8 @@ __global__ void __launch_bounds__(128, MINB) k_pass_mixed(
   const Box& B = P.box;
   const int n = A.n;
   unsigned n_col = 0, n_pc = 0, n_wc = 0;
-  int need = 0;
-  double d2 = 0.0;
+  int need = 0, need_in = 0;
+  bool in_over = false;
 
   const int c = A.cell_cur[p];
   const double4 p4 = A.X[p];
@@ -279,19 +288,24 @@ __global__ void __launch_bounds__(128, MINB) k_pass_mixed(
   const int cp = PP ? 0 : A.comp[p];
   float inv_m, inv_i, eff_m;
   MMat<PP>::self(P, cp, Rp, inv_m, inv_i, eff_m);
-  int n1, n2b, n2a;
-  unpack_meta(A.meta[p], n1, n2b, n2a);
+  const int n1 = A.meta[p] & META_MASK;
+  const unsigned long long key_p = sweep_key(c, A.rank[p]);
   const float half_dt = (float)A.half_dt;
   const bool update = A.update != 0;
   int hw_n = 0;
   bool overflow = false;
   const History& Hr = A.Hr;
   const History& Hw = A.Hw;
+  const int hc = valid ? Hr.cnt[p] : 0;
+#pragma unroll
+  for (int r = 0; r < KREG; r++) s_hk[wid][r][lane] = r < hc ? Hr.key[hslot(Hr, p, r)] : -1;
+  s_hc[wid][lane] = hc;
+  s_match[wid][lane] = 0u;
+  __syncwarp();
 
   F3 iF = mk(eff_m * (float)P.gravity[0], eff_m * (float)P.gravity[1],
              eff_m * (float)P.gravity[2]);
   F3 iT = mk(0.f, 0.f, 0.f);
-  F3 F = mk(0.f, 0.f, 0.f), T = mk(0.f, 0.f, 0.f);
 
   auto record = [&](int partner, F3 ft, F3 lo, F3 vt) {
     if (hw_n < Hw.cap) {
@@ -303,59 +317,76 @@ __global__ void __launch_bounds__(128, MINB) k_pass_mixed(
     }
     hw_n++;
   };
-  // Rij = x_j - x_i (minimum image, FP64); candidate k of a row is "j" (its
-  // owner is "i") for k < n1
-  auto geometry = [&](const Box& Bx, bool oi, const double xo[3], const double4& q4,
+  // Rij = x_j - x_i (minimum image, FP64)
+  auto geometry = [&](const Box& Bx, const double xo[3], const double4& q4,
                       double Rij[3]) -> double {
-    Rij[0] = oi ? q4.x - xo[0] : xo[0] - q4.x;
-    Rij[1] = oi ? q4.y - xo[1] : xo[1] - q4.y;
-    Rij[2] = oi ? q4.z - xo[2] : xo[2] - q4.z;
+    Rij[0] = q4.x - xo[0];
+    Rij[1] = q4.y - xo[1];
+    Rij[2] = q4.z - xo[2];
 #pragma unroll
     for (int k = 0; k < 3; k++) Rij[k] = min_image_exact(Rij[k], Bx, k);
     return sumsq3(Rij);
   };
-  auto test = [&](int k, int q, const double4& q4) -> bool {
-    const bool pi = k < n1;
+  auto test = [&](int, int q, const double4& q4) -> bool {
     double Rij[3];
-    const double DijSq = geometry(B, pi, xp, q4, Rij);
+    const double DijSq = geometry(B, xp, q4, Rij);
     const int cq = PP ? 0 : A.comp[q];
-    const double mds = pi ? MMat<PP>::min_dij_sq(P, cp, Rpd, cq, q4.w)
-                          : MMat<PP>::min_dij_sq(P, cq, q4.w, cp, Rpd);
-    return mds - DijSq > 0.0;
+    return MMat<PP>::min_dij_sq(P, cp, Rpd, cq, q4.w) - DijSq > 0.0;
   };
-  auto compute = [&](const OwnerMixed& o, int k, int slot) {
+  auto compute = [&](const OwnerMixed& o, int oo, int k, int slot) {
     const int q = __ldg(A.cand + (size_t)k * n + o.p);
-    const bool oi = k < o.n1;
+    const int s_in = atomicAdd(&A.in_cnt[q], 1);  // q's "j" record (returns early)
     const double4 q4 = A.X[q];
+    const float4 qv4 = A.v4[q];
+    const float2 qw2 = A.w2[q];
     const double xo[3] = {o.x, o.y, o.z};
     double Rij[3];
     const DevParams& PO = A.P[o.sys];  // the owner's system (a warp may span two)
-    const double DijSq = geometry(PO.box, oi, xo, q4, Rij);
+    const double DijSq = geometry(PO.box, xo, q4, Rij);
     const int cq = PP ? 0 : A.comp[q];
-    const int ca = oi ? o.cp : cq, cb = oi ? cq : o.cp;
-    const double Rad = oi ? o.R : q4.w, Rbd = oi ? q4.w : o.R;
-    const double Delta = MMat<PP>::min_dij_sq(PO, ca, Rad, cb, Rbd) - DijSq;
-    const float Ra = (float)Rad, Rb = (float)Rbd;
+    const double Delta = MMat<PP>::min_dij_sq(PO, o.cp, o.R, cq, q4.w) - DijSq;
+    const float Ra = (float)o.R, Rb = (float)q4.w;
     MPair m;
-    MMat<PP>::pair(PO, ca, Ra, cb, Rb, m);
-    const float4 qv4 = A.v4[q];
-    const float2 qw2 = A.w2[q];
+    MMat<PP>::pair(PO, o.cp, Ra, cq, Rb, m);
     const F3 vq = mk(qv4.x, qv4.y, qv4.z), wq = mk(qv4.w, qw2.x, qw2.y);
     const F3 vo = mk(o.vx, o.vy, o.vz), wo = mk(o.wx, o.wy, o.wz);
-    const int lo_i = o.p < q ? o.p : q, hi_i = o.p < q ? q : o.p;
+    // the owner's records, then the partner's
     F3 ft0 = mk(0.f, 0.f, 0.f), ft0lo = ft0, vt0 = ft0;
-    const int r = find_record(Hr, lo_i, hi_i);
-    const bool contacting = r >= 0;
-    if (contacting) rec_read(V.ra, V.rb, V.rc, hslot(Hr, lo_i, r), ft0, ft0lo, vt0);
-    if (oi) {
-      if (!contacting) n_col++;
-      n_pc++;
+    const int oc = s_hc[wid][oo];
+    int r = -1;
+#pragma unroll
+    for (int rr = 0; rr < KREG; rr++)
+      if (rr < oc && s_hk[wid][rr][oo] == q) r = rr;
+    for (int rr = KREG; r < 0 && rr < oc; rr++)
+      if (Hr.key[hslot(Hr, o.p, rr)] == q) r = rr;
+    bool contacting = r >= 0;
+    if (contacting) {
+      rec_read(V.ra, V.rb, V.rc, hslot(Hr, o.p, r), ft0, ft0lo, vt0);
+      if (r < 32) atomicOr(&s_match[wid][oo], 1u << r);
+    } else {
+      const int r2 = find_record(Hr, q, o.p);
+      contacting = r2 >= 0;
+      if (contacting) rec_read(V.ra, V.rb, V.rc, hslot(Hr, q, r2), ft0, ft0lo, vt0);
     }
+    if (!contacting) n_col++;
+    n_pc++;
     MOut out;
-    mixed_pair(Rij, DijSq, Delta, m, Ra, oi ? vo : vq, oi ? wo : wq, Rb, oi ? vq : vo,
-               oi ? wq : wo, half_dt, contacting, ft0, ft0lo, vt0, out);
-    const float Ro = (float)o.R;
-    const F3 tq = oi ? cross(Ro * out.N, out.FT) : Ro * out.NxFT;
+    mixed_pair(Rij, DijSq, Delta, m, Ra, vo, wo, Rb, vq, wq, half_dt, contacting, ft0, ft0lo,
+               vt0, out);
+    // "j" side into q's incoming records
+    if (s_in < A.in_cap) {
+      const F3 FTs = out.FT + out.FTlo;
+      InRec32* rec = (InRec32*)A.in_rec + (size_t)s_in * A.in_stride + q;
+      rec->a = make_float4(__uint_as_float((unsigned)o.key),
+                           __uint_as_float((unsigned)(o.key >> 32)), out.FN.x, out.FN.y);
+      rec->b = make_float4(out.FN.z, FTs.x, FTs.y, FTs.z);
+      rec->c = make_float4(out.NxFT.x, out.NxFT.y, out.NxFT.z, 0.f);
+    } else {
+      in_over = true;
+    }
+    need_in = need_in > s_in + 1 ? need_in : s_in + 1;
+    // "i" side to the owner
+    const F3 tq = cross(Ra * out.N, out.FT);
     const float vals[15] = {out.FN.x, out.FN.y, out.FN.z, out.FT.x, out.FT.y, out.FT.z,
                             out.FTlo.x, out.FTlo.y, out.FTlo.z, out.VT.x, out.VT.y, out.VT.z,
                             tq.x, tq.y, tq.z};
@@ -363,23 +394,21 @@ __global__ void __launch_bounds__(128, MINB) k_pass_mixed(
     for (int i = 0; i < 15; i++) s_r[i][wid][slot] = vals[i];
     s_q[wid][slot] = q;
   };
-  auto accum = [&](int slot, int k) {
+  auto accum = [&](int slot, int) {
     float v[15];
 #pragma unroll
     for (int i = 0; i < 15; i++) v[i] = s_r[i][wid][slot];
     const F3 FN = mk(v[0], v[1], v[2]), FT = mk(v[3], v[4], v[5]), FTlo = mk(v[6], v[7], v[8]);
     const F3 VT = mk(v[9], v[10], v[11]), tq = mk(v[12], v[13], v[14]);
-    if (k < n1) {
-      iF = iF + FN + (FT + FTlo);
-      iT = iT + tq;
-    } else {
-      F = F - FN - (FT + FTlo);
-      T = T + tq;
-    }
-    const int q = s_q[wid][slot];
-    if (update && p < q) record(q, FT, FTlo, VT);
+    iF = iF + FN + (FT + FTlo);
+    iT = iT + tq;
+    if (update) record(s_q[wid][slot], FT, FTlo, VT);
   };
-  auto walls = [&]() {
+  const OwnerMixed me{xp[0], xp[1], xp[2], Rpd, vp.x, vp.y, vp.z, wp.x, wp.y, wp.z, p, cp,
+                      A.sysid ? A.sysid[p] : 0, 0, key_p};
+  contact_loop(A.cand, A.X, n, p, valid, n1, me, s_k[wid], s_o[wid], test, compute, accum);
+
+  if (valid) {
     for (int w = 0; w < P.nw; w++) {
       const dem_wall& W = P.walls[w];
       const size_t wi = (size_t)p * P.nw + w;
@@ -387,8 +416,7 @@ __global__ void __launch_bounds__(128, MINB) k_pass_mixed(
       F3 ft0 = mk(0.f, 0.f, 0.f), ft0lo = ft0, vt0 = ft0;
       if (contacting) rec_read(V.rwa, V.rwb, V.rwc, wi, ft0, ft0lo, vt0);
       double Dij, Nij[3], Qji[3];
-      bool ov = false;
-      ov = overlap_wall<CONE>(P, W, xp, Rpd, Dij, Nij, Qji);
+      const bool ov = overlap_wall<CONE>(P, W, xp, Rpd, Dij, Nij, Qji);
       if (ov) {
         n_wc++;
         const double Delta = Rpd * Rpd - Dij * Dij;
@@ -408,7 +436,7 @@ __global__ void __launch_bounds__(128, MINB) k_pass_mixed(
                      ft0lo, vt0, m, o);
         iF = iF + o.FN + (o.FT + o.FTlo);
         iT = iT + cross(Rp * o.N, o.FT);
-        atomicAdd(&A.cnt->wall_fn[w], (double)sqrtf(dot(o.FN, o.FN)));
+        s_w[w][threadIdx.x] = sqrtf(dot(o.FN, o.FN));
         if (update) {
           Hw.wflag[wi] = 1;
           rec_write(V.wwa, V.wwb, V.wwc, wi, o.FT, o.FTlo, o.VT);
@@ -417,23 +445,17 @@ __global__ void __launch_bounds__(128, MINB) k_pass_mixed(
         Hw.wflag[wi] = 0;
       }
     }
-  };
-  auto own = [&]() {
     if (A.drag)  // iForce = iForce + DragForce(iPart) (src/MForces.f90:316)
       iF = iF + mk((float)A.drag[(size_t)3 * p], (float)A.drag[(size_t)3 * p + 1],
                    (float)A.drag[(size_t)3 * p + 2]);
-    F = F + iF;
-    T = T + iT;
-  };
-  const OwnerMixed me{xp[0], xp[1], xp[2], Rpd, vp.x, vp.y, vp.z, wp.x, wp.y, wp.z, p, cp, n1,
-                      A.sysid ? A.sysid[p] : 0};
-  contact_loop(A.cand, A.X, n, p, valid, n1, n2b, n1 + n2b + n2a, P.nw > 0, me, s_k[wid],
-               s_o[wid], test, compute, accum, walls, own);
-
-  if (valid) {
+    Own32* ow = (Own32*)A.own + p;
+    ow->a = make_float2(iF.x, iF.y);
+    ow->b = make_float2(iF.z, iT.x);
+    ow->c = make_float2(iT.y, iT.z);
     if (update) {
-      const int nold = Hr.cnt[p];
-      for (int r = 0; r < nold; r++) {
+      const unsigned matched = s_match[wid][lane];
+      for (int r = 0; r < hc; r++) {
+        if (r < 32 && ((matched >> r) & 1u)) continue;
         const size_t i = hslot(Hr, p, r);
         const int q2 = Hr.key[i];
         if (q2 >= A.n || !cells_adjacent(P, c, A.cell_cur[q2])) {
@@ -443,12 +465,67 @@ __global__ void __launch_bounds__(128, MINB) k_pass_mixed(
         }
       }
       Hw.cnt[p] = hw_n < Hw.cap ? hw_n : Hw.cap;
-      if (overflow) {
-        atomicExch(&A.cnt->overflow, 1);
-        set_abort(A.cnt, A.tag);
-      }
       need = hw_n;
     }
+  }
+  if (A.nw_max > 0) wall_partials(s_w, A.nw_max, A.wall_part);
+  if (overflow) {
+    atomicExch(&A.cnt->overflow, 1);
+    set_abort(A.cnt, A.tag);
+  }
+  if (in_over) {
+    atomicExch(&A.cnt->in_overflow, 1);
+    set_abort(A.cnt, A.tag);
+  }
+  need_in = (int)__reduce_max_sync(0xffffffffu, (unsigned)need_in);
+  if (lane == 0 && need_in) atomicMax(&A.cnt->need_in, need_in);
+  publish_counts(A.cnt, A.update != 0, n_col, n_pc, n_wc, (unsigned)need);
+}
+
+// The fold kernel: Force and Torque in sweep order (FP32), a = F/m,
+// alpha = T/I, then the FP64 integrator epilogue.
+template <bool PP, int EPI>
+__global__ void __launch_bounds__(128, 4) k_fold_mixed(PassArgs<float4, float2> A) {
+  if (A.cnt->abort) return;
+  const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = p0 < A.n;
+  const int p = valid ? p0 : 0;
+  double d2 = 0.0;
+  if (valid) {
+    const DevParams& P = sys_params(A.P, A.sysid, p);
+    const int c = A.cell_cur[p];
+    const unsigned long long key_p = sweep_key(c, A.rank[p]);
+    const int ni = A.in_cnt[p];
+    A.in_cnt[p] = 0;  // for the next pass's contact kernel
+    const double4 p4 = A.X[p];
+    const double xp[3] = {p4.x, p4.y, p4.z};
+    const double Rpd = p4.w;
+    const float Rp = (float)Rpd;
+    const int cp = PP ? 0 : A.comp[p];
+    float inv_m, inv_i, eff_m;
+    MMat<PP>::self(P, cp, Rp, inv_m, inv_i, eff_m);
+    const Own32 ow = ((const Own32*)A.own)[p];
+    const InRec32* in = (const InRec32*)A.in_rec + p;
+    const size_t st = (size_t)A.in_stride;
+    F3 F = mk(0.f, 0.f, 0.f), T = mk(0.f, 0.f, 0.f);
+    fold_in_order(
+        ni, key_p,
+        [&](int e) {
+          const float2 k = *(const float2*)(in + e * st);
+          return (unsigned long long)__float_as_uint(k.x) |
+                 ((unsigned long long)__float_as_uint(k.y) << 32);
+        },
+        [&]() {
+          F = F + mk(ow.a.x, ow.a.y, ow.b.x);
+          T = T + mk(ow.b.y, ow.c.x, ow.c.y);
+        },
+        [&](int e) {
+          const InRec32 r = in[e * st];
+          const F3 FN = mk(r.a.z, r.a.w, r.b.x), FTs = mk(r.b.y, r.b.z, r.b.w);
+          const F3 NxFT = mk(r.c.x, r.c.y, r.c.z);
+          F = F - FN - FTs;
+          T = T + Rp * NxFT;
+        });
     if (EPI == EPI_STORE && A.amsum) {
       const size_t n3 = (size_t)3 * A.n, q = (size_t)3 * p;
       A.amsum[q] = F.x; A.amsum[q + 1] = F.y; A.amsum[q + 2] = F.z;
@@ -467,7 +544,6 @@ __global__ void __launch_bounds__(128, MINB) k_pass_mixed(
     }
     epilogue<EPI>(A, P, p, xp, Rpd, vd, wd, acc, alp, c, d2);
   }
-  publish_counts(A.cnt, A.update != 0, n_col, n_pc, n_wc, (unsigned)need);
   if (EPI != EPI_STORE) publish_disp(A.cnt, d2);
 }
 
@@ -623,7 +699,7 @@ bool mixed_grow_walls(MixedBuffers& M, int n, int stride, int cur, cudaStream_t 
 }
 
 void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant, bool cone,
-                const PassArgs<float4, float2>& A, int cur, cudaStream_t st) {
+                const PassArgs<float4, float2>& A, int cur, cudaStream_t st, int part) {
   if (A.n == 0) return;
   MixedView V;
   V.ra = M.ha[cur];
@@ -639,24 +715,30 @@ void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant, bool cone,
   V.wwb = M.wb[cur ^ 1];
   V.wwc = M.wc[cur ^ 1];
   const unsigned g = blocks(A.n, 128);
-#define MCASE(PPV, MB, CN)                                                                   \
-  do {                                                                                       \
-    if (epi == EPI_PREDICT) k_pass_mixed<PPV, EPI_PREDICT, MB, CN><<<g, 128, 0, st>>>(A, V);  \
-    else if (epi == EPI_CORRECT)                                                             \
-      k_pass_mixed<PPV, EPI_CORRECT, MB, CN><<<g, 128, 0, st>>>(A, V);                       \
-    else k_pass_mixed<PPV, EPI_STORE, MB, CN><<<g, 128, 0, st>>>(A, V);                       \
-  } while (0)
-  if (cone) {
-    if (pp) MCASE(true, 3, true);
-    else MCASE(false, 3, true);
-  } else if (variant == 1) {
-    if (pp) MCASE(true, 3, false);
-    else MCASE(false, 3, false);
-  } else {
-    if (pp) MCASE(true, 4, false);
-    else MCASE(false, 4, false);
-  }
+  if (part == 0) {
+#define MCASE(PPV, MB, CN) k_contact_mixed<PPV, MB, CN><<<g, 128, 0, st>>>(A, V)
+    if (cone) {
+      if (pp) MCASE(true, 3, true);
+      else MCASE(false, 3, true);
+    } else if (variant == 1) {
+      if (pp) MCASE(true, 3, false);
+      else MCASE(false, 3, false);
+    } else {
+      if (pp) MCASE(true, 4, false);
+      else MCASE(false, 4, false);
+    }
 #undef MCASE
+    return;
+  }
+#define FCASE(PPV)                                                                      \
+  do {                                                                                  \
+    if (epi == EPI_PREDICT) k_fold_mixed<PPV, EPI_PREDICT><<<g, 128, 0, st>>>(A);      \
+    else if (epi == EPI_CORRECT) k_fold_mixed<PPV, EPI_CORRECT><<<g, 128, 0, st>>>(A); \
+    else k_fold_mixed<PPV, EPI_STORE><<<g, 128, 0, st>>>(A);                            \
+  } while (0)
+  if (pp) FCASE(true);
+  else FCASE(false);
+#undef FCASE
 }
 
 void mixed_import_history(MixedBuffers& M, const History& H, int n, int nw, int cur,

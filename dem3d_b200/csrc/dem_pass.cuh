@@ -1,16 +1,18 @@
-// dem_pass.cuh -- device helpers shared by the FP64 and the mixed pass
-// kernels: candidate segments, the AB/AM epilogues and the cell transition
-// (RedistributeParticles3D's bookkeeping) for the next pass.
+// dem_pass.cuh -- device helpers shared by the FP64 and the mixed force
+// passes: the contact loop, the ordered fold, the AB/AM epilogues and the
+// cell transition (RedistributeParticles3D's bookkeeping) for the next pass.
 //
-// A pass kernel runs one thread per particle in original index order.  It
-// reads its candidate row, applies the reference's overlap test to every
-// candidate, computes the contacts in the reference's order, and finishes
-// with the integrator step of the pass (AB predictor or AM corrector).  The
-// epilogue also hashes the particle's next position into its cell and, when
-// the cell changes, records the move for the next relink: the arrival list
-// of the new cell and the dirty list of both cells.  Every such side effect
-// is idempotent, so a pass kernel that was stopped by a history overflow can
-// be launched again after the tables grow.
+// A force pass is two kernels, each one thread per particle in original
+// index order.  The contact kernel reads the particle's candidate row (the
+// partners it meets as "i"), applies the reference's overlap test, evaluates
+// every contact once and hands the "j" half of each contact to the partner.
+// The fold kernel adds the particle's received halves and its own block in
+// the sweep's order and finishes with the integrator step of the pass (AB
+// predictor or AM corrector).  Its epilogue also hashes the particle's next
+// position into its cell and, when the cell changes, records the move for
+// the next relink: the arrival list of the new cell and the dirty list of
+// both cells.  Every such side effect is idempotent, so a pass that was
+// stopped by a table overflow can be launched again after the tables grow.
 #pragma once
 #include <cstring>
 
@@ -100,31 +102,26 @@ __device__ __forceinline__ T shfl_obj(const T& v, int src) {
   return r;
 }
 
-// The contacts of the warp's particles, in three steps per window of 64
-// candidates:
+// The contacts of the warp's particles, each particle as "i" of its row, in
+// three steps per window of 64 candidates:
 //  1. every lane tests its own candidates (test(k, q, xq), four prefetched at
 //     a time) into a bit mask;
 //  2. the warp's contacts are laid out owner by owner in row order (prefix
-//     sum) and computed 32 at a time, one per lane: compute(owner, k, slot)
-//     gets the owning particle's data by shuffle and leaves its results in
-//     shared-memory slot `slot`;
-//  3. every owner folds its own results in row order: accum(slot, k) for the
-//     loop-1 contacts (k < n1), then walls(), then the loop-2 contacts before
-//     its own block (k < n1 + n2b), own(), then the rest -- the reference's
-//     summation order.
+//     sum) and computed 32 at a time, one per lane: compute(owner, lane of the
+//     owner, k, slot) gets the owning particle's data by shuffle and leaves
+//     the owner's results in shared-memory slot `slot`;
+//  3. every owner folds its own results in row order, accum(slot, k): the
+//     order of the reference's loop over jj (src/MForces.f90:199-272).
 // s_k / s_o: 32 ints of shared memory per warp.  All 32 lanes must call
 // this; `valid` is false for lanes without a particle.
-template <class Owner, class Test, class Compute, class Accum, class Walls, class Own>
+template <class Owner, class Test, class Compute, class Accum>
 __device__ __forceinline__ void contact_loop(const int* __restrict__ cand,
                                              const double4* __restrict__ X, int n, int p,
-                                             bool valid, int n1, int n2b, int m, bool has_walls,
-                                             const Owner& me, int* s_k, int* s_o, Test&& test,
-                                             Compute&& compute, Accum&& accum, Walls&& walls,
-                                             Own&& own) {
+                                             bool valid, int m, const Owner& me, int* s_k,
+                                             int* s_o, Test&& test, Compute&& compute,
+                                             Accum&& accum) {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
-  bool walls_pending = valid && has_walls;
-  bool own_pending = valid;
   if (!valid) m = 0;
   const int mmax = (int)__reduce_max_sync(FULL, (unsigned)m);
   for (int base = 0; base < mmax; base += 64) {
@@ -166,27 +163,54 @@ __device__ __forceinline__ void contact_loop(const int* __restrict__ cand,
       const int kk = has ? s_k[lane] : 0;
       const int oo = has ? s_o[lane] : lane;
       const Owner ow = shfl_obj(me, oo);
-      if (has) compute(ow, kk, lane);
+      if (has) compute(ow, oo, kk, lane);
       __syncwarp();
       const int e0 = start > t0 ? start : t0;
       const int e1 = start + cnt < t0 + 32 ? start + cnt : t0 + 32;
-      for (int e = e0; e < e1; e++) {
-        const int k = s_k[e - t0];
-        if (walls_pending && k >= n1) {
-          walls();
-          walls_pending = false;
-        }
-        if (own_pending && !walls_pending && k >= n1 + n2b) {
-          own();
-          own_pending = false;
-        }
-        accum(e - t0, k);
-      }
+      for (int e = e0; e < e1; e++) accum(e - t0, s_k[e - t0]);
       __syncwarp();
     }
   }
-  if (walls_pending) walls();
-  if (own_pending) own();
+}
+
+// The "j" results a particle received in this pass, in the order of the
+// givers' blocks in the sweep (their keys), with the particle's own block
+// (key_p) at its place: the order in which ComputeAccelerations adds them to
+// Force(p) and Torque(p) (src/MForces.f90:254-259, 319-320).  key_of(e)
+// returns the key of record e; own() and add(e) fold.  The keys of the first
+// 8 records are kept in registers; records past those are rare.
+template <class KeyOf, class Own, class Add>
+__device__ __forceinline__ void fold_in_order(int ni, unsigned long long key_p, KeyOf&& key_of,
+                                              Own&& own, Add&& add) {
+  unsigned long long kr[8];
+#pragma unroll
+  for (int e = 0; e < 8; e++) kr[e] = e < ni ? key_of(e) : ~0ull;
+  bool own_done = false;
+  unsigned long long lo = 0ull;  // every key >= lo is still to be folded
+  for (int t = 0; t < ni; t++) {
+    int best = -1;
+    unsigned long long km = ~0ull;
+#pragma unroll
+    for (int e = 0; e < 8; e++)
+      if (e < ni && kr[e] >= lo && kr[e] < km) {
+        km = kr[e];
+        best = e;
+      }
+    for (int e = 8; e < ni; e++) {
+      const unsigned long long k = key_of(e);
+      if (k >= lo && k < km) {
+        km = k;
+        best = e;
+      }
+    }
+    if (!own_done && key_p < km) {
+      own();
+      own_done = true;
+    }
+    add(best);
+    lo = km + 1ull;
+  }
+  if (!own_done) own();
 }
 
 template <class T>
@@ -353,13 +377,6 @@ __device__ __forceinline__ void epilogue(const PassArgs<V4, W2>& A, const DevPar
     atomicExch(&A.cnt->nonfinite, 1);
     set_abort(A.cnt, A.tag);
   }
-}
-
-// Meta word of a candidate row.
-__device__ __forceinline__ void unpack_meta(int m, int& n1, int& n2b, int& n2a) {
-  n1 = m & META_MASK;
-  n2b = (m >> META_BITS) & META_MASK;
-  n2a = (m >> (2 * META_BITS)) & META_MASK;
 }
 
 __device__ __forceinline__ void set_abort(Counters* cnt, int tag) {

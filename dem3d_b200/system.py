@@ -361,6 +361,9 @@ class DEMSystem:
             "momentum": list(o.momentum),
             "n_pair_contacts": o.n_pair_contacts,
             "n_wall_contacts": o.n_wall_contacts,
+            "wall_pressure": list(o.wall_pressure),
+            "bed_height": o.bed_height,
+            "n_pair_records": o.n_pair_records,
         }
 
     # -- GPU-only instrumentation -------------------------------------------

@@ -110,16 +110,31 @@ typedef struct dem_params {
   dem_wall walls[DEM_MAX_WALLS];
 } dem_params;
 
-/* Observables (K5).  kinetic/potential: src/MDEM.f90:183-213. */
+/* Observables (K5).  kinetic/potential: src/MDEM.f90:183-213; the others
+ * have no counterpart in the reference and are defined here.  Ensembles: sums
+ * over all systems, fractions as ratios of sums. */
 typedef struct dem_observables {
   double kinetic_energy;
   double potential_energy;
-  double mean_coordination;   /* 2*(pair contacts)/N, from the history records */
-  double packing_fraction;    /* sum of particle volumes / box volume */
-  double wall_normal_force[DEM_MAX_WALLS]; /* sum of normal force on each wall */
+  double mean_coordination;   /* 2*(pair contacts of the last force pass)/N */
+  /* Solid fraction.  A system with gravity along -z and no periodicity in z
+   * holds a bed: its base is the lowest rectangle wall facing z (else the
+   * box bottom), its filled height H is twice the mean height of the sphere
+   * centres above the base, and the fraction is the volume of the spheres
+   * whose centres lie in the lower 0.8*H, over Lx*Ly*0.8*H.  Otherwise: the
+   * volume of all spheres over the box volume. */
+  double packing_fraction;
+  double wall_normal_force[DEM_MAX_WALLS]; /* sum of |FN| on each wall, last force pass */
   double momentum[3];
-  int64_t n_pair_contacts;
-  int64_t n_wall_contacts;
+  int64_t n_pair_contacts;    /* overlapping pairs in the last force pass */
+  int64_t n_wall_contacts;    /* overlapping sphere-wall pairs in the last force pass */
+  /* wall_normal_force over the wall's area: a rectangle's extent along each
+   * of its in-plane axes up to the box length along that axis, a cone's
+   * lateral area */
+  double wall_pressure[DEM_MAX_WALLS];
+  double bed_height;          /* H above (mean over the systems with a bed; 0: none) */
+  int64_t n_pair_records;     /* pair history records held (the contacts of the
+                                 last updating pass and the records it kept) */
 } dem_observables;
 
 /* TWallMovement (src/MDEM.f90:39-45) of one wall, in reduced units (as

@@ -114,6 +114,7 @@ typedef struct orc_ctx {
   int Contacting;
   int64_t ncol;
   double wall_fn[NWM];
+  int64_t last_pairs, last_walls;  /* overlapping pairs of the last force pass */
   int moving;               /* WallsInMovement */
   int removal;              /* run() calls UpdateParticleList after each step */
   int pouring;              /* run() calls PouringAttempt before each step */
@@ -825,6 +826,8 @@ static int compute_accelerations(orc_ctx* c, OParticle* P, double TimeStep, int 
   memset(c->force, 0, sizeof(double) * 3 * (size_t)n);
   memset(c->torque, 0, sizeof(double) * 3 * (size_t)n);
   for (int w = 0; w < NWM; w++) c->wall_fn[w] = 0.0;
+  c->last_pairs = 0;
+  c->last_walls = 0;
   if (c->fluid) update_velocity_field(c, P);
   for (int32_t iCell = 0; iCell < c->Nt; iCell++) {
     int32_t NPCC, NPSC;
@@ -855,6 +858,7 @@ static int compute_accelerations(orc_ctx* c, OParticle* P, double TimeStep, int 
         c->DeltaDijSq = pp.min_dij_sq - c->DijSq;
         if (c->DeltaDijSq > 0.0) {
           if (!c->Contacting) c->ncol = c->ncol + 1;
+          c->last_pairs++;
           c->Dij = sqrt(c->DijSq);
           for (int k = 0; k < 3; k++) c->Nij[k] = c->Rij[k] / c->Dij;
           double dn = c->Dij - pp.min_dij;
@@ -881,6 +885,7 @@ static int compute_accelerations(orc_ctx* c, OParticle* P, double TimeStep, int 
         verify_wall_contact(c, i, w, &c->Contacting, c->ijForceT0, c->VijT0);
         if (overlap_wall(c, &iPart, jWall, c->Ri, &c->Dij, c->Nij, c->Qji)) {
           c->DeltaDijSq = c->Ri * c->Ri - c->Dij * c->Dij;
+          c->last_walls++;
           double dn = c->Dij - c->Ri;
           for (int k = 0; k < 3; k++) c->ijDispN[k] = dn * c->Nij[k];
           double wq[3];
@@ -1880,10 +1885,36 @@ int orc_get_escaped(orc_ctx* c, int64_t* count) {
   return DEM_OK;
 }
 
-/* KineticEnergy / PotentialEnergy (src/MDEM.f90:183-213) + extras */
+/* Area of a wall that the spheres can press on: a rectangle's extent along
+ * each in-plane axis (the box axis it runs along) up to the box length there,
+ * or a cone's lateral area. */
+static double o_wall_area(const dem_wall* W, const double* L) {
+  if (W->shape == DEM_WALL_RECTANGLE) {
+    int ku = 0, kw = 0;
+    for (int j = 1; j < 3; j++) {
+      if (fabs(W->u[j]) > fabs(W->u[ku])) ku = j;
+      if (fabs(W->w[j]) > fabs(W->w[kw])) kw = j;
+    }
+    double a = 2.0 * W->l1 < L[ku] ? 2.0 * W->l1 : L[ku];
+    double b = 2.0 * W->l2 < L[kw] ? 2.0 * W->l2 : L[kw];
+    return a * b;
+  }
+  if (W->shape == DEM_WALL_CONE) {
+    double len = 2.0 * W->l1, dr = W->l3 - W->l2;
+    return 3.14159265358979323846 * (W->l2 + W->l3) * sqrt(len * len + dr * dr);
+  }
+  return 0.0;
+}
+
+/* KineticEnergy / PotentialEnergy (src/MDEM.f90:183-213) + extras: solid
+ * fraction (of the bed's lower 0.8*H, H = twice the mean centre height above
+ * the lowest rectangle wall facing z, for a system with gravity along -z and
+ * no periodicity in z; else of the box), contacts of the last force pass,
+ * wall forces and pressures */
 int orc_get_observables(orc_ctx* c, dem_observables* o) {
   memset(o, 0, sizeof(*o));
-  double Ek = 0.0, Ep = 0.0, vol = 0.0;
+  const double pi = 3.14159265358979323846;
+  double Ek = 0.0, Ep = 0.0;
   for (int32_t i = 0; i < c->n; i++) {
     const OParticle* q = &c->part[i];
     double m = 1.0 / o_inv_mass(c, q);
@@ -1895,18 +1926,51 @@ int orc_get_observables(orc_ctx* c, dem_observables* o) {
     }
     Ek = Ek + m * sumsq3(q->vel) + I * sumsq3(q->omega);
     Ep = Ep - m * dot3(q->pos, c->p.gravity);
-    double R = o_radius(c, q);
-    vol += 4.0 / 3.0 * 3.14159265358979323846 * R * R * R;
     for (int d = 0; d < 3; d++) o->momentum[d] += m * q->vel[d];
   }
   o->kinetic_energy = 0.5 * Ek;
   o->potential_energy = Ep;
-  o->packing_fraction = vol / (c->p.lbox[0] * c->p.lbox[1] * c->p.lbox[2]);
+  double solid = 0.0, region = 0.0;
+  if (!(c->p.gravity[2] < 0.0) || c->p.pbc[2] || c->n == 0) {
+    for (int32_t i = 0; i < c->n; i++) {
+      double R = o_radius(c, &c->part[i]);
+      solid += 4.0 / 3.0 * pi * R * R * R;
+    }
+    region = c->n ? c->p.lbox[0] * c->p.lbox[1] * c->p.lbox[2] : 0.0;
+  } else {
+    double base = -0.5 * c->p.lbox[2];
+    int floor = 0;
+    for (int w = 0; w < c->p.n_walls; w++) {
+      const dem_wall* W = &c->p.walls[w];
+      if (W->shape == DEM_WALL_RECTANGLE && fabs(W->n[2]) > 0.99 &&
+          (!floor || W->position[2] < base)) {
+        base = W->position[2];
+        floor = 1;
+      }
+    }
+    double mean = 0.0;
+    for (int32_t i = 0; i < c->n; i++) mean += c->part[i].pos[2] - base;
+    double h = 2.0 * (mean / c->n);
+    double top = 0.8 * h;
+    for (int32_t i = 0; i < c->n; i++)
+      if (c->part[i].pos[2] - base < top) {
+        double R = o_radius(c, &c->part[i]);
+        solid += 4.0 / 3.0 * pi * R * R * R;
+      }
+    region = c->p.lbox[0] * c->p.lbox[1] * top;
+    o->bed_height = h;
+  }
+  o->packing_fraction = region > 0.0 ? solid / region : 0.0;
   int64_t np, nw;
   orc_count_contacts(c, &np, &nw);
-  o->n_pair_contacts = np;
-  o->n_wall_contacts = nw;
-  o->mean_coordination = c->n ? 2.0 * (double)np / (double)c->n : 0.0;
+  o->n_pair_records = np;
+  o->n_pair_contacts = c->last_pairs;
+  o->n_wall_contacts = c->last_walls;
+  o->mean_coordination = c->n ? 2.0 * (double)c->last_pairs / (double)c->n : 0.0;
   for (int w = 0; w < NWM; w++) o->wall_normal_force[w] = c->wall_fn[w];
+  for (int w = 0; w < c->p.n_walls; w++) {
+    double a = o_wall_area(&c->p.walls[w], c->p.lbox);
+    o->wall_pressure[w] = a > 0.0 ? o->wall_normal_force[w] / a : 0.0;
+  }
   return DEM_OK;
 }

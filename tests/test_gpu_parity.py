@@ -205,14 +205,22 @@ def test_escape_detection():
 
 
 def test_observables_match_oracle():
-    w = configs.settling(n=500, seed=12)
+    """Energies, bed packing fraction and height, contacts of the last pass,
+    wall forces and pressures: the first layer starts on the floor."""
+    w = configs.settling(n=500, seed=12, sigma_v=0.01, first_height=0.47)
     g, o = make_pair(w)
     for s in (g, o):
         s.run(1, 30)
     a, b = g.observables(), o.observables()
-    for k in ("kinetic_energy", "potential_energy", "packing_fraction", "mean_coordination"):
+    for k in ("kinetic_energy", "potential_energy", "packing_fraction", "mean_coordination",
+              "bed_height"):
         assert abs(a[k] - b[k]) <= 1e-12 * max(1.0, abs(b[k])), k
-    assert a["n_pair_contacts"] == b["n_pair_contacts"]
+    for k in ("wall_normal_force", "wall_pressure"):
+        assert b[k][0] > 0.0, k  # the bed rests on the floor
+        np.testing.assert_allclose(a[k], b[k], rtol=1e-12, atol=0.0, err_msg=k)
+    for k in ("n_pair_contacts", "n_wall_contacts", "n_pair_records"):
+        assert a[k] == b[k], k
+    assert 0.3 < b["packing_fraction"] < 0.75
 
 
 @pytest.mark.slow
