@@ -46,9 +46,13 @@ WORKLOADS = {
     "dense1m": dict(n=1_000_000, phi=0.55, seed=1001, tile=8000),
     "dense16m": dict(n=16_000_000, phi=0.60, seed=1002, tile=16000),
     "dense64k": dict(n=64_000, phi=0.55, seed=1001, tile=8000),
-    "ensemble4096": dict(kind="ensemble", n_systems=4096, seed=1003),
+    "ensemble4096": dict(kind="ensemble", n_systems=4096, seed=1003, skip=3000),
     "bidisperse4m": dict(kind="bidisperse", n=4_000_000, seed=1004),
     "ensemble64": dict(kind="ensemble", n_systems=64, seed=1003),
+    # above jamming (about six contacts per sphere): the contact-dense case
+    "jammed1m": dict(n=1_000_000, phi=0.66, seed=1012, tile=8000, relax=4000),
+    "jammed16m": dict(n=16_000_000, phi=0.66, seed=1012, tile=16000, relax=4000),
+    "jammed216k": dict(n=216_000, phi=0.66, seed=1012, tile=8000, relax=4000),
 }
 
 
@@ -116,43 +120,71 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def pass_bytes_per_particle(mixed, epi, z_pp, m_cand, z_pw=0.0, nw=0, nprev=3):
-    """Algorithmic DRAM bytes of one pass-kernel launch per particle: every
-    input and output of the pass read or written once.  Partner data is other
-    particles' own data (re-read from L1/L2), so it adds nothing.
-      own copies: position+R 32, velocities 24 (FP32) / 48 (FP64), row meta 4,
-        cell 4, history count 4; candidate row 4*m_cand;
-      history: each pair record once (key 4 + 36 B FP32 / 48 B FP64) per
-        pair, read, and written again by the updating pass (+ count 4);
-        wall records 4 + record per wall;
+def contact_bytes_per_particle(mixed, update, z_pp, m_cand, z_pw=0.0, nw=0):
+    """Algorithmic DRAM bytes of one contact-kernel launch per particle (the
+    particle as "i" of its row): every input and output once; partner data
+    is other particles' own data (re-read from L1/L2) and adds nothing.
+      reads: position+R 32, velocities 24 (FP32) / 48 (FP64), row length 4,
+        rank 4, cell 4, record count 4, candidate row 4*m_cand (the row holds
+        the "i" partners only), the pair records (key 4 + 36 B FP32 / 48 B
+        FP64) once per pair (0.5*z_pp per particle), wall flags and records;
+      writes: the "i" block 24 (FP32) / 48 (FP64), one "j" record per pair
+        (48 B FP32 / 80 B FP64) and its count 4, and in the history-updating
+        pass the new tables (count 4, records, wall records)."""
+    vel = 24 if mixed else 48
+    rec = 4 + (36 if mixed else 48)
+    jrec = (48 if mixed else 80) + 4
+    own = 32 + vel + 4 + 4 + 4 + 4 + 4 * m_cand
+    hist = 0.5 * z_pp * rec + nw * 4 + z_pw * (rec - 4)
+    out = (24 if mixed else 48) + 0.5 * z_pp * jrec
+    if update:
+        hist += 4 + 0.5 * z_pp * rec + nw * 4 + z_pw * (rec - 4)
+    return own + hist + out
+
+
+def fold_bytes_per_particle(mixed, epi, z_pp, nprev=3):
+    """Algorithmic DRAM bytes of one fold-kernel launch per particle:
+      reads: cell 4, rank 4, "j" count 4 (reset: written 4), the "i" block
+        24 / 48, the "j" records (0.5*z_pp per particle, 48 / 80 B), position
+        + R 32 (and the FP64 velocity copies 48 in FP64 mode);
       epi "predict" (pass 1, src/MDEM.f90:296-331): ring nprev*72 read,
-        Particle v,w 48 read (mixed: FP64 copies), a,alpha 48 + Predicted
-        x,v,w 72 + ring slot 72 + the corrector's ring sums 72 + next-pass
-        copies (32 + velocities) + cell 4 written;
+        Particle v,w 48 read (mixed), a,alpha 48 + Predicted x,v,w 72 + ring
+        slot 72 + the corrector's ring sums 72 + next-pass copies (32 +
+        velocities) + cell 4 written;
       epi "correct" (pass 2, :340-367): the ring sums 72, Predicted v 24
         (mixed) read, Particle x,v,w 72 read and written, Predicted a,alpha
         48 + next-pass copies + cell 4 written."""
     vel = 24 if mixed else 48
-    rec = 4 + (36 if mixed else 48)
-    own = 32 + vel + 4 + 4 + 4 + 4 * m_cand
-    hist = 0.5 * z_pp * rec + nw * 4 + z_pw * (rec - 4)
-    ring = nprev * 72
-    sums = 72 if nprev else 0  # sum_k AM(k)*Previous(ipc(k)), predictor -> corrector
+    base = 4 + 4 + 8 + (24 if mixed else 48) + 0.5 * z_pp * (48 if mixed else 80) + 32 + (
+        0 if mixed else 48)
+    sums = 72 if nprev else 0
     if epi == "predict":
-        hist += 4 + 0.5 * z_pp * rec + nw * 4 + z_pw * (rec - 4)  # updated tables
-        epil = (ring + (48 if mixed else 0) + 48 + 72 + (72 if nprev else 0) + sums + 32 + vel
-                + 4)
+        epil = (nprev * 72 + (48 if mixed else 0) + 48 + 72 + (72 if nprev else 0) + sums + 32
+                + vel + 4)
     else:
         epil = sums + (24 if mixed else 0) + 72 + 72 + 48 + 32 + vel + 4
-    return own + hist + epil
+    return base + epil
 
 
 def step_bytes_per_particle(mixed, z_pp, m_cand, z_pw=0.0, nw=0, nprev=3):
-    """Compulsory bytes of one particle-update (MoveParticles: two passes);
-    the relink and candidate-row kernels touch only the few particles near
-    cells that changed and are not counted."""
-    return (pass_bytes_per_particle(mixed, "predict", z_pp, m_cand, z_pw, nw, nprev) +
-            pass_bytes_per_particle(mixed, "correct", z_pp, m_cand, z_pw, nw, nprev))
+    """Bytes of one particle-update (MoveParticles: two passes of a contact
+    and a fold kernel) under the kernels' own model; the relink and
+    candidate-row kernels touch only the few particles near cells that
+    changed and are not counted."""
+    return (contact_bytes_per_particle(mixed, True, z_pp, m_cand, z_pw, nw) +
+            contact_bytes_per_particle(mixed, False, z_pp, m_cand, z_pw, nw) +
+            fold_bytes_per_particle(mixed, "predict", z_pp, nprev) +
+            fold_bytes_per_particle(mixed, "correct", z_pp, nprev))
+
+
+def survey_bytes_per_particle(mixed, z_pp, z_pw=0.0):
+    """Compulsory bytes of one particle-update of a fused gather design
+    (the hot-path scope table's model): FP64 656 + 84*Z_pp + 168*Z_pw,
+    mixed 608 + 48*Z_pp + 96*Z_pw, with Z_pp the pair contacts and Z_pw the
+    wall contacts per particle."""
+    if mixed:
+        return 608.0 + 48.0 * z_pp + 96.0 * z_pw
+    return 656.0 + 84.0 * z_pp + 168.0 * z_pw
 
 
 def reduce_max(x, world, device="cuda"):
@@ -187,7 +219,8 @@ def make_workload(name, precision, rank, factory=None):
         return configs.bidisperse_settling(n=spec["n"], seed=rank_seed(spec["seed"], rank),
                                            precision=prec)
     return configs.dense_packing(n=spec["n"], phi=spec["phi"], seed=rank_seed(spec["seed"], rank),
-                                 tile=spec["tile"], precision=prec, system_factory=factory)
+                                 tile=spec["tile"], precision=prec, system_factory=factory,
+                                 relax_steps=spec.get("relax", 2000))
 
 
 def config_block(name, w, world, precision):
@@ -204,7 +237,8 @@ def config_block(name, w, world, precision):
                      f"phi={spec['phi']}, kn=1e5, e=0.8, mu=0.5, dt=1e-4, ABM4"),
         "particles_per_gpu": spec["n"], "global_particles": spec["n"] * world,
         "box": round(w.info["L"], 4), "precision": precision,
-        "input": f"relaxed {spec['tile']}-sphere tile x {w.info['copies']} copies, seeded",
+        "input": (f"{spec['tile']}-sphere tile relaxed {spec.get('relax', 2000)} steps "
+                  f"(e=0.1, no friction) x {w.info['copies']} copies, seeded"),
         "l2": "inputs larger than L2 (state + history >> 126 MB)",
         "parallelism": f"{world} independent systems (ensemble, seed+rank)",
     }
@@ -318,6 +352,7 @@ def run_reference(args):
         return DEMSystem(p, lib=lib, prefix="orc_")
     t0 = time.perf_counter()
     tp, tr, L_t = configs.relaxed_tile(spec["tile"], spec["phi"], spec["seed"],
+                                       relax_steps=spec.get("relax", 2000),
                                        system_factory=factory)
     t_relax = time.perf_counter() - t0
     cores = os.cpu_count() or 1
@@ -375,18 +410,22 @@ def traffic_per_particle():
 
 
 def kernel_bytes(name, n, mixed, z_pp, m_cand, z_pw, nw):
-    """Algorithmic bytes of one pass-kernel launch (mean of the two passes)."""
-    if name.startswith("pass"):
-        return n * 0.5 * (pass_bytes_per_particle(mixed, "predict", z_pp, m_cand, z_pw, nw) +
-                          pass_bytes_per_particle(mixed, "correct", z_pp, m_cand, z_pw, nw))
+    """Algorithmic bytes of one launch of a force-pass kernel (mean of the
+    two passes of a step)."""
+    if name.startswith("contact"):
+        return n * 0.5 * (contact_bytes_per_particle(mixed, True, z_pp, m_cand, z_pw, nw) +
+                          contact_bytes_per_particle(mixed, False, z_pp, m_cand, z_pw, nw))
+    if name.startswith("fold"):
+        return n * 0.5 * (fold_bytes_per_particle(mixed, "predict", z_pp) +
+                          fold_bytes_per_particle(mixed, "correct", z_pp))
     return None
 
 
-def measure(s, w, args, world, local, torch, dist):
+def measure(s, w, args, world, local, torch, dist, first_step=1):
     """Warm-up (and the autotuner's trials, on the live run), then the timed
     region (graph replay of K steps)."""
-    s.run(1, 3 + args.warmup)
-    first = 4 + args.warmup
+    s.run(first_step, first_step + 2 + args.warmup)
+    first = first_step + 3 + args.warmup
     tuning = None
     if not args.no_autotune:
         tuning = s.autotune(first, 40)
@@ -520,10 +559,11 @@ def run_ours(args):
         # both runs advanced the same steps from the same state: ensemble
         # observables of the mixed run against the FP64 run
         ob = {p: systems[p].observables() for p in ("fp64", "mixed")}
-        keys = ("kinetic_energy", "mean_coordination", "packing_fraction")
+        keys = ("kinetic_energy", "mean_coordination", "packing_fraction", "bed_height")
         pick = {p: {k: ob[p][k] for k in keys} for p in ob}
         for p in ob:
             pick[p]["floor_force"] = ob[p]["wall_normal_force"][0]
+            pick[p]["floor_pressure"] = ob[p]["wall_pressure"][0]
         rel = {k: (abs(pick["mixed"][k] - pick["fp64"][k]) / abs(pick["fp64"][k])
                    if pick["fp64"][k] else None) for k in pick["fp64"]}
         obs_cmp = {"after_step": res["fp64"]["last"], **pick, "rel_diff": rel}
@@ -571,11 +611,22 @@ def run_ours(args):
         peaks = json.load(open(pk))
     peak = peaks.get("hbm_gbs", 6650.0)
     tr = traffic_per_particle()
-    traffic = None
+    traffic, traffic_src = None, None
     if tr and dom in tr.get("bytes_per_particle", {}):
+        # ncu DRAM bytes per particle of one launch, captured on a smaller
+        # case of the same workload, scaled to this launch by the particles
         traffic = tr["bytes_per_particle"][dom] * n
+        traffic_src = tr.get("state", "profiles/pass_traffic.json")
     step_b = step_bytes_per_particle(mixed, z_pp, m_cand, z_pw, nw)
-    step_gbs = step_b * n / (ms / res[headline]["steps"] / 1000.0) / 1e9
+    step_ms = ms / res[headline]["steps"]
+    step_gbs = step_b * n / (step_ms / 1000.0) / 1e9
+    # the hot-path table's compulsory bytes per particle-update over the
+    # whole step (every kernel of it) and over the force-pass kernels alone
+    surv_b = survey_bytes_per_particle(mixed, z_pp, z_pw)
+    pass_ms = sum(v[1] for k, v in stats.items()
+                  if k.startswith(("contact", "fold"))) / nprof
+    surv_step = surv_b * n / (step_ms / 1000.0) / 1e9
+    surv_pass = surv_b * n / (pass_ms / 1000.0) / 1e9 if pass_ms > 0 else None
 
     # e2e: a driver that keeps Particle(1:n) on the host: each step uploads
     # positions, velocities and angular velocities from pinned host memory,
@@ -612,7 +663,8 @@ def run_ours(args):
         lib_path, flags = _oracle_variant()
         v, k, dt = cpu_time_steps(base, max_steps=3, budget_s=25.0, lib_path=lib_path, core=0)
         cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": f"{k} MoveParticles steps (after 1 untimed) of the same {n:,}-sphere "
+               "sample": f"{k} MoveParticles steps (after 1 untimed; the GPU arm times "
+                         f"{res[headline]['steps']}) of the same {n:,}-sphere "
                          f"system, oracle "
                          f"C port ({flags}), 1 thread pinned to one core of {cpu_model()}, "
                          f"{dt:.1f}s"}
@@ -637,8 +689,12 @@ def run_ours(args):
                          "traffic": traffic, "algorithmic_bytes_per_launch": b_launch,
                          "avg_launch_ms": avg_ms, "peak_source": "MEASURED_PEAKS.json hbm_gbs"
                          if "hbm_gbs" in peaks else "fallback 6650 GB/s",
+                         "traffic_source": traffic_src,
                          "step_bytes_per_particle_update": step_b,
                          "step_achieved_gbs": step_gbs, "step_frac": step_gbs / peak,
+                         "survey_bytes_per_particle_update": surv_b,
+                         "frac_survey": surv_step / peak,
+                         "frac_survey_force_passes": surv_pass / peak if surv_pass else None,
                          "kernel_share": {k: round(v[1] / total_prof, 4)
                                           for k, v in sorted(stats.items(),
                                                              key=lambda kv: -kv[1][1])}},
@@ -683,18 +739,36 @@ def run_ensemble(args):
     spec = WORKLOADS[args.workload]
     prec = "fp64" if args.precision == "fp64" else "mixed"
     t0 = time.perf_counter()
-    e = configs.settling_ensemble(n_systems=spec["n_systems"], seed=rank_seed(spec["seed"], rank),
-                                  precision=P.PREC_MIXED if prec == "mixed" else P.PREC_FP64)
+    # one ensemble for the whole job; rank r advances every world-th system
+    # (no exchange between ranks: the systems are independent)
+    e_all = configs.settling_ensemble(n_systems=spec["n_systems"], seed=spec["seed"],
+                                      precision=P.PREC_MIXED if prec == "mixed" else P.PREC_FP64)
+    e = e_all.shard(rank, world)
     t_gen = time.perf_counter() - t0
     n = e.n
     s = DEMSystem.ensemble(e.params, e.counts)
     s.set_state(e.pos, e.vel, e.omega, radius=e.radius)
     s.initialize_cell_distribution()
+    skip = args.skip_steps if args.skip_steps >= 0 else spec.get("skip", 0)
+    if skip > 0:
+        # the beds start to form: untimed steps before the warm-up
+        s.run(1, skip)
     w = type("W", (), {"n": n})
-    res = measure(s, w, args, world, local, torch, dist)
+    res = measure(s, w, args, world, local, torch, dist, first_step=skip + 1)
+    # whole-job rate: every particle of the ensemble over the slowest rank's time
+    res["value"] = e_all.n * res["steps"] / (res["ms"] / 1000.0)
     obs = s.observables()
     z_pp = 2.0 * obs["n_pair_contacts"] / n
     z_pw = obs["n_wall_contacts"] / n
+    # job-wide observables: sums over the ranks' systems
+    tot = np.array([obs["kinetic_energy"], obs["n_pair_contacts"], obs["n_wall_contacts"], n],
+                   dtype=np.float64)
+    if world > 1:
+        t = torch.tensor(tot, device="cuda")
+        dist.all_reduce(t)
+        tot = t.cpu().numpy()
+    job_obs = {"kinetic_energy": float(tot[0]), "pair_contacts": int(tot[1]),
+               "wall_contacts": int(tot[2]), "particles": int(tot[3])}
     m_cand = s.row_stats()["candidates"] / n
     # per-kernel timing of a few instrumented steps
     s.reset_kernel_stats()
@@ -741,14 +815,18 @@ def run_ensemble(args):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": res["steps"],
             "warmup": args.warmup, "ms_per_step": res["ms"] / res["steps"],
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "f32+f64" if prec == "mixed" else "f64", "data": "synthetic",
             "config": {"workload": (f"{len(e.counts)} gravity-settling systems, sizes log-uniform "
                                     f"in [200, 20000] ({n:,} spheres), R~U[0.45,0.55], per-system "
                                     "mu~U[0.2,0.8], e~U[0.5,0.95], 10x10 x-y periodic box with "
                                     "floor, dt=1e-4, ABM4, one context"),
-                       "particles_per_gpu": n, "precision": prec,
-                       "l2": "inputs larger than L2", "parallelism": f"{world} ensembles"},
+                       "particles_per_gpu": n, "global_particles": e_all.n,
+                       "precision": prec, "timed_from_step": res["last"] - res["steps"] + 1,
+                       "l2": "inputs larger than L2",
+                       "parallelism": f"systems sharded over {world} ranks (every "
+                                      f"{world}-th system per rank), no exchange"},
+            "job_observables": job_obs,
             "gpu_launches": int(res["launches"]),
             "tuning": res["tuning"],
             "sequential_fp64_systems": seq,
@@ -784,6 +862,9 @@ def main():
                     help="run the autotuner's trials again every N timed steps (0: never)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="skip the autotuner's trials (default settings)")
+    ap.add_argument("--skip-steps", type=int, default=-1,
+                    help="untimed steps before the warm-up (ensembles: the beds start to "
+                         "form; default: the workload's own)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

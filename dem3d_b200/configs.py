@@ -358,6 +358,18 @@ class Ensemble:
         return (self.params[s], self.pos[o:o + k], self.vel[o:o + k], self.omega[o:o + k],
                 self.radius[o:o + k])
 
+    def shard(self, rank, world):
+        """The systems rank `rank` of `world` advances: every world-th system
+        from `rank` on (sizes are drawn at random, so interleaving balances
+        the particle counts), as an Ensemble of its own."""
+        idx = list(range(rank, len(self.counts), world))
+        off = np.concatenate([[0], np.cumsum(self.counts)])
+        sel = np.concatenate([np.arange(off[k], off[k + 1]) for k in idx]) if idx else \
+            np.zeros(0, dtype=np.int64)
+        return Ensemble([self.params[k] for k in idx], np.asarray(self.counts)[idx],
+                        self.pos[sel], self.vel[sel], self.omega[sel], self.radius[sel],
+                        dict(self.info, shard=(rank, world), systems=idx))
+
 
 def settling_ensemble(n_systems=4096, seed=1003, nmin=200, nmax=20000, width=10.0,
                       rmin=0.45, rmax=0.55, mu_range=(0.2, 0.8), e_range=(0.5, 0.95),
@@ -530,6 +542,29 @@ def dense_packing(n=1_000_000, phi=0.55, seed=1001, rmin=0.4, rmax=0.6, relax_st
             "copies": k ** 3}
     prm = dense_packing_params(rmax, L, precision=precision, max_ncell=max_ncell)
     return Workload("dense_packing", prm, pos, vel, omega, radius=radius, info=info)
+
+
+# Volume fraction of the jammed workload.  Radii U[0.4, 0.6] jam near
+# 0.64-0.65 without friction; a frictionless relaxation at a volume fraction
+# below that ends with almost no contacts (0.55 gives about 0.3 contacts per
+# sphere, 0.60 about 0.6), so a packing with about six contacts per sphere
+# needs a volume fraction above jamming.
+JAMMED_PHI = 0.66
+
+
+def jammed_packing(n=1_000_000, phi=JAMMED_PHI, seed=1012, rmin=0.4, rmax=0.6,
+                   relax_steps=4000, sigma_v=0.1, precision=P.PREC_FP64, tile=8000,
+                   system_factory=None):
+    """Polydisperse periodic packing above jamming (about six contacts per
+    sphere): a tile compressed to ``phi`` with overlaps and relaxed without
+    friction to mechanical equilibrium (restitution 0.1), replicated; the
+    measured contact parameters of the dense configurations (kn = 1e5,
+    e = 0.8, mu = 0.5) and seeded velocities N(0, sigma_v^2)."""
+    w = dense_packing(n=n, phi=phi, seed=seed, rmin=rmin, rmax=rmax, relax_steps=relax_steps,
+                      sigma_v=sigma_v, precision=precision, system_factory=system_factory,
+                      tile=tile)
+    w.name = "jammed_packing"
+    return w
 
 
 def max_overlap(pos, radius, L, sample=200_000):
