@@ -890,7 +890,11 @@ __global__ void __launch_bounds__(128, MINB) k_contact_fp64(PassArgs<double4, do
   __shared__ unsigned s_match[4][32];
   __shared__ double s_r[12][4][32];
   __shared__ double s_w[NWM][128];  // |FN| of each wall contact
-  if (A.cnt->abort) return;
+  __shared__ int s_abort;
+  // one decision for the whole block (it meets a block barrier later)
+  if (threadIdx.x == 0) s_abort = A.cnt->abort;
+  __syncthreads();
+  if (s_abort) return;
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int w = 0; w < A.nw_max; w++) s_w[w][threadIdx.x] = 0.0;
   const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
