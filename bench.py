@@ -50,9 +50,9 @@ WORKLOADS = {
     "bidisperse4m": dict(kind="bidisperse", n=4_000_000, seed=1004),
     "ensemble64": dict(kind="ensemble", n_systems=64, seed=1003),
     # above jamming (about six contacts per sphere): the contact-dense case
-    "jammed1m": dict(n=1_000_000, phi=0.66, seed=1012, tile=8000, relax=4000),
-    "jammed16m": dict(n=16_000_000, phi=0.66, seed=1012, tile=16000, relax=4000),
-    "jammed216k": dict(n=216_000, phi=0.66, seed=1012, tile=8000, relax=4000),
+    "jammed1m": dict(n=1_000_000, phi=0.65, seed=1012, tile=8000, relax=4000),
+    "jammed16m": dict(n=16_000_000, phi=0.65, seed=1012, tile=16000, relax=4000),
+    "jammed216k": dict(n=216_000, phi=0.65, seed=1012, tile=8000, relax=4000),
 }
 
 

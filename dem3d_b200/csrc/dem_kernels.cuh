@@ -1142,16 +1142,19 @@ __global__ void __launch_bounds__(128, MINB) k_contact_fp64(PassArgs<double4, do
     atomicExch(&A.cnt->in_overflow, 1);
     set_abort(A.cnt, A.tag);
   }
-  need_in = (int)__reduce_max_sync(0xffffffffu, (unsigned)need_in);
-  if (lane == 0 && need_in) atomicMax(&A.cnt->need_in, need_in);
-  publish_counts(A.cnt, A.update != 0, n_col, n_pc, n_wc, (unsigned)need);
+  publish_counts_block(A.cnt, A.update != 0, n_col, n_pc, n_wc, (unsigned)need,
+                       (unsigned)need_in);
 }
 
 // The fold kernel: Force and Torque of every particle in sweep order, a =
 // F/m, alpha = T/I (src/MForces.f90:330-333), then the integrator epilogue.
 template <bool PP, int EPI, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_fold_fp64(PassArgs<double4, double2> A) {
-  if (A.cnt->abort) return;
+  __shared__ int s_abort;
+  // one decision for the whole block (it meets a block barrier at the end)
+  if (threadIdx.x == 0) s_abort = A.cnt->abort;
+  __syncthreads();
+  if (s_abort) return;
   const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = p0 < A.n;
   const int p = valid ? p0 : 0;
@@ -1211,7 +1214,7 @@ __global__ void __launch_bounds__(128, MINB) k_fold_fp64(PassArgs<double4, doubl
     const double wp[3] = {pv4.w, pw2.x, pw2.y};
     epilogue<EPI>(A, P, p, xp, Rp, vp, wp, acc, alp, c, d2);
   }
-  if (EPI != EPI_STORE) publish_disp(A.cnt, d2);
+  if (EPI != EPI_STORE) publish_disp_block(A.cnt, d2);
 }
 
 }  // namespace dem

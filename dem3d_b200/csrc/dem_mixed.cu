@@ -481,16 +481,19 @@ __global__ void __launch_bounds__(128, MINB) k_contact_mixed(
     atomicExch(&A.cnt->in_overflow, 1);
     set_abort(A.cnt, A.tag);
   }
-  need_in = (int)__reduce_max_sync(0xffffffffu, (unsigned)need_in);
-  if (lane == 0 && need_in) atomicMax(&A.cnt->need_in, need_in);
-  publish_counts(A.cnt, A.update != 0, n_col, n_pc, n_wc, (unsigned)need);
+  publish_counts_block(A.cnt, A.update != 0, n_col, n_pc, n_wc, (unsigned)need,
+                       (unsigned)need_in);
 }
 
 // The fold kernel: Force and Torque in sweep order (FP32), a = F/m,
 // alpha = T/I, then the FP64 integrator epilogue.
 template <bool PP, int EPI>
 __global__ void __launch_bounds__(128, 4) k_fold_mixed(PassArgs<float4, float2> A) {
-  if (A.cnt->abort) return;
+  __shared__ int s_abort;
+  // one decision for the whole block (it meets a block barrier at the end)
+  if (threadIdx.x == 0) s_abort = A.cnt->abort;
+  __syncthreads();
+  if (s_abort) return;
   const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = p0 < A.n;
   const int p = valid ? p0 : 0;
@@ -548,7 +551,7 @@ __global__ void __launch_bounds__(128, 4) k_fold_mixed(PassArgs<float4, float2> 
     }
     epilogue<EPI>(A, P, p, xp, Rpd, vd, wd, acc, alp, c, d2);
   }
-  if (EPI != EPI_STORE) publish_disp(A.cnt, d2);
+  if (EPI != EPI_STORE) publish_disp_block(A.cnt, d2);
 }
 
 // FP64 records <-> FP32 records

@@ -80,6 +80,54 @@ __device__ __forceinline__ void publish_counts(Counters* cnt, bool update, unsig
   }
 }
 
+// The same statistics summed over the block first (one atomic per counter
+// per block of at most 256 threads), together with the largest number of
+// "j" records a particle received.  All threads of the block call.
+__device__ __forceinline__ void publish_counts_block(Counters* cnt, bool update, unsigned n_col,
+                                                     unsigned n_pc, unsigned n_wc,
+                                                     unsigned need, unsigned need_in) {
+  const unsigned FULL = 0xffffffffu;
+  __shared__ unsigned s_c[8][5];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned v[5] = {__reduce_add_sync(FULL, n_col), __reduce_add_sync(FULL, n_pc),
+                         __reduce_add_sync(FULL, n_wc), __reduce_max_sync(FULL, need),
+                         __reduce_max_sync(FULL, need_in)};
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < 5; k++) s_c[wid][k] = v[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned t[5] = {0u, 0u, 0u, 0u, 0u};
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+      t[0] += s_c[w][0];
+      t[1] += s_c[w][1];
+      t[2] += s_c[w][2];
+      t[3] = t[3] > s_c[w][3] ? t[3] : s_c[w][3];
+      t[4] = t[4] > s_c[w][4] ? t[4] : s_c[w][4];
+    }
+    if (t[0]) atomicAdd(update ? &cnt->ncol_pending : &cnt->ncol, (unsigned long long)t[0]);
+    if (t[1]) atomicAdd(&cnt->pair_contacts, (unsigned long long)t[1]);
+    if (t[2]) atomicAdd(&cnt->wall_contacts, (unsigned long long)t[2]);
+    if (t[3]) atomicMax(&cnt->need_capacity, (int)t[3]);
+    if (t[4]) atomicMax(&cnt->need_in, (int)t[4]);
+  }
+}
+
+// The largest displacement of the block into the pass maximum (one atomic
+// per block of at most 256 threads).  All threads of the block call.
+__device__ __forceinline__ void publish_disp_block(Counters* cnt, double d2) {
+  __shared__ unsigned s_d[8];
+  const unsigned bits = __float_as_uint(__double2float_ru(sqrt(d2)));
+  const unsigned m = __reduce_max_sync(0xffffffffu, bits);
+  if ((threadIdx.x & 31) == 0) s_d[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned t = 0u;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t = t > s_d[w] ? t : s_d[w];
+    if (t) atomicMax(&cnt->disp_max, t);
+  }
+}
+
 // Slot of partner `hi` among the records of `lo`; -1: no record.
 __device__ __forceinline__ int find_record(const History& H, int lo, int hi) {
   const int c = H.cnt[lo];

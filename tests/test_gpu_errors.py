@@ -55,7 +55,8 @@ def test_two_cells_on_a_periodic_axis_are_refused():
 
 def test_long_candidate_rows_grow():
     """Large spheres among small ones (d 3 and 1) with the widest row skin
-    (half of CutOff): a large sphere's row holds about 110 candidates."""
+    (half of CutOff): a large sphere's row (the partners it meets as "i")
+    holds about 55 candidates, past the initial capacity of 32."""
     w = configs.bidisperse_settling(n=3000, width=24.0, headroom=6.0, sigma_v=0.5,
                                     euler_intervals=10)
     g, o = DEMSystem(w.params), oracle_system(w.params)
@@ -65,7 +66,7 @@ def test_long_candidate_rows_grow():
     g.set_tuning(0.5, 0)
     for s in (g, o):
         s.run(1, 100)
-    assert g.row_stats()["row_capacity"] > 100
+    assert g.row_stats()["row_capacity"] > 48
     a, b = g.get_state(), o.get_state()
     for k in a:
         np.testing.assert_array_equal(a[k], b[k], err_msg=k)
