@@ -123,7 +123,7 @@ struct dem_ctx {
   int* rm_buf = nullptr;  // escaped list + status words of the removal kernel
   int rm_cap = 0;
   long long rm_stats[3] = {0, 0, 0};  // removals, swaps, records renamed or moved
-  int pass_variant = 0;  // pass kernel compiled for 4 (0) or 3 (1) blocks per SM
+  int pass_variant = 0;  // contact kernel compiled for 4 (0), 3 (1) or 5 (2) blocks per SM
   bool has_cone = false; // some wall of some system is a cone
   double skin_factor = 0.05;  // candidate-row skin / CutOff
   int par = 0;         // L.cell[par] is the assignment the lists hold
@@ -710,6 +710,9 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
   if (c->pass_variant == 1) {
     if (c->pp) CONTACT_CASE(true, 3);
     else CONTACT_CASE(false, 3);
+  } else if (c->pass_variant == 2) {
+    if (c->pp) CONTACT_CASE(true, 5);
+    else CONTACT_CASE(false, 5);
   } else {
     if (c->pp) CONTACT_CASE(true, 4);
     else CONTACT_CASE(false, 4);
@@ -2780,8 +2783,8 @@ int dem_get_pass_stats(dem_ctx* c, int64_t* pair_contacts, int64_t* wall_contact
 
 int dem_set_tuning(dem_ctx* c, double skin_factor, int32_t pass_variant) {
   if (!c) return DEM_ERR_INVALID;
-  if (!(skin_factor > 0.0 && skin_factor <= 0.5) || pass_variant < 0 || pass_variant > 1)
-    return fail(c, DEM_ERR_INVALID, "skin factor must lie in (0, 0.5], variant in {0, 1}");
+  if (!(skin_factor > 0.0 && skin_factor <= 0.5) || pass_variant < 0 || pass_variant > 2)
+    return fail(c, DEM_ERR_INVALID, "skin factor must lie in (0, 0.5], variant in {0, 1, 2}");
   CK(cudaStreamSynchronize(c->stream));
   if (skin_factor != c->skin_factor) {
     sync_host_walls(c);
@@ -2817,13 +2820,13 @@ int dem_autotune(dem_ctx* c, int32_t first_step, int32_t steps_per_trial, int32_
   int st = validate_ready(c);
   if (st) return st;
   const double skins[3] = {0.025, 0.05, 0.1};
-  const int trials = 6;
+  const int trials = 9;
   const int timed_steps = (steps_per_trial + 3) / 4 * 4;  // whole graph chunks
   int step = first_step;
   double best_ms = 1e300;
   int best = 0;
   for (int t = 0; t < trials; t++) {
-    st = dem_set_tuning(c, skins[t / 2], t % 2);
+    st = dem_set_tuning(c, skins[t / 3], t % 3);
     if (st) return st;
     // one untimed chunk takes the graph capture and the forced full rebuild
     st = dem_run(c, step, step + 3);
@@ -2839,7 +2842,7 @@ int dem_autotune(dem_ctx* c, int32_t first_step, int32_t steps_per_trial, int32_
       best = t;
     }
   }
-  st = dem_set_tuning(c, skins[best / 2], best % 2);
+  st = dem_set_tuning(c, skins[best / 3], best % 3);
   if (st) return st;
   if (last_step) *last_step = step - 1;
   return DEM_OK;

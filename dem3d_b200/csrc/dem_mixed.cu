@@ -730,6 +730,9 @@ void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant, bool cone,
     } else if (variant == 1) {
       if (pp) MCASE(true, 3, false);
       else MCASE(false, 3, false);
+    } else if (variant == 2) {
+      if (pp) MCASE(true, 5, false);
+      else MCASE(false, 5, false);
     } else {
       if (pp) MCASE(true, 4, false);
       else MCASE(false, 4, false);

@@ -31,9 +31,9 @@ bool mixed_regrow(MixedBuffers& M, int n, int stride, int newcap, int cur, const
 bool mixed_grow_walls(MixedBuffers& M, int n, int stride, int cur, cudaStream_t st);
 // One kernel of a force pass (FP32 contact arithmetic) on the context's
 // stream: part 0 = the contact kernel, 1 = the fold kernel with epilogue
-// `epi`.  variant: the contact kernel compiled for 4 (0) or 3 (1) resident
-// blocks per SM; cone: some wall is a cone (then the 3-block contact kernel
-// with the cone branch runs)
+// `epi`.  variant: the contact kernel compiled for 4 (0), 3 (1) or 5 (2)
+// resident blocks per SM; cone: some wall is a cone (then the 3-block
+// contact kernel with the cone branch runs)
 void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant, bool cone,
                 const PassArgs<float4, float2>& A, int cur, cudaStream_t st, int part);
 void mixed_import_history(MixedBuffers& M, const History& H, int n, int nw, int cur,

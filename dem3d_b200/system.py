@@ -421,10 +421,10 @@ class DEMSystem:
         return {"skin_factor": f.value, "pass_variant": v.value}
 
     def autotune(self, first_step: int, steps_per_trial: int = 20):
-        """Runs six timed trials on the live system (dem_autotune); returns
+        """Runs nine timed trials on the live system (dem_autotune); returns
         the last step advanced, the chosen setting and the trial times."""
         last = C.c_int32()
-        ms = (C.c_double * 6)()
+        ms = (C.c_double * 9)()
         self._call("autotune", C.c_int32(first_step), C.c_int32(steps_per_trial),
                    C.byref(last), ms)
         return {"last_step": last.value, **self.tuning(), "trial_ms": list(ms)}

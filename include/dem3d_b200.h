@@ -368,15 +368,17 @@ int dem_get_row_stats(dem_ctx* ctx, int64_t* candidates, int32_t* row_capacity);
 
 /* Tuning (no counterpart in the reference).  skin_factor: candidate-row skin
  * as a fraction of CutOff (0.05 by default; larger = longer rows, fewer full
- * row rebuilds); pass_variant: pass kernel compiled for 4 (0, default) or 3
- * (1) resident blocks per SM.  Neither changes any result: the rows stay
- * complete and in sweep order, and the arithmetic is the same code. */
+ * row rebuilds); pass_variant: the contact kernel's block budget, compiled
+ * for 4 (0, default), 3 (1) or 5 (2) resident blocks of 128 threads per SM
+ * (fewer registers per thread, more warps to hide memory latency).  Neither
+ * changes any result: the rows stay complete and in sweep order, and the
+ * arithmetic is the same code. */
 int dem_set_tuning(dem_ctx* ctx, double skin_factor, int32_t pass_variant);
 int dem_get_tuning(dem_ctx* ctx, double* skin_factor, int32_t* pass_variant);
-/* Autotuner: advances the run from first_step through six trials (skin
- * 0.025 / 0.05 / 0.1 x both variants), each one untimed 4-step chunk and
+/* Autotuner: advances the run from first_step through nine trials (skin
+ * 0.025 / 0.05 / 0.1 x the three variants), each one untimed 4-step chunk and
  * steps_per_trial timed steps (rounded up to whole 4-step chunks), keeps the
- * fastest setting and returns the last step advanced and the six trial times
+ * fastest setting and returns the last step advanced and the nine trial times
  * (trial_ms may be NULL).  The trajectory is the one dem_run would produce. */
 int dem_autotune(dem_ctx* ctx, int32_t first_step, int32_t steps_per_trial,
                  int32_t* last_step, double* trial_ms);

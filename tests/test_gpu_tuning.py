@@ -27,8 +27,8 @@ def test_autotune_keeps_the_trajectory(precision):
     a, b = _system(precision), _system(precision)
     a.run(1, 8)
     t = a.autotune(9, 4)
-    assert t["last_step"] == 8 + 6 * 8
-    assert t["skin_factor"] in (0.025, 0.05, 0.1) and t["pass_variant"] in (0, 1)
+    assert t["last_step"] == 8 + 9 * 8
+    assert t["skin_factor"] in (0.025, 0.05, 0.1) and t["pass_variant"] in (0, 1, 2)
     assert all(ms > 0 for ms in t["trial_ms"])
     b.run(1, t["last_step"])
     sa, sb = a.get_state(), b.get_state()
@@ -44,7 +44,7 @@ def test_tuning_settings_keep_the_trajectory():
     ref = _system(P.PREC_FP64)
     ref.run(1, 40)
     want = ref.get_state()
-    for skin, variant in ((0.01, 1), (0.2, 0), (0.1, 1)):
+    for skin, variant in ((0.01, 1), (0.2, 0), (0.1, 1), (0.05, 2)):
         s = _system(P.PREC_FP64)
         s.set_tuning(skin, variant)
         s.run(1, 40)
