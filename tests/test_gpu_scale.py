@@ -13,7 +13,7 @@ The CUDA path against the oracle on the states the benchmark runs on:
   - a bidisperse box closed by a floor and four side walls, run from rest
     past the impact on the floor.
 A mid-run state moves from the GPU to the oracle through the C-ABI's state,
-integration ring and contact records (the data a checkpoint holds); both
+integration ring, contact records and Ncol (the data a checkpoint holds); both
 sides then build their cell lists afresh from the positions
 (InitializeCellDistribution), so both continue from identical data.
 
@@ -34,7 +34,8 @@ FORCE_TOL = 1e-5
 
 def transfer(src, dst, radius=None, comp=None, lo=0, hi=None):
     """Particles [lo, hi) of `src` into `dst`, renumbered from 0: state, ring,
-    contact records; `dst` builds its cell lists from the positions."""
+    contact records (and Ncol for a whole system); `dst` builds its cell lists
+    from the positions."""
     st = src.get_state()
     hi = src.n if hi is None else hi
     sl = slice(lo, hi)
@@ -49,6 +50,8 @@ def transfer(src, dst, radius=None, comp=None, lo=0, hi=None):
     mw = (c["ip"] >= lo) & (c["ip"] < hi)
     dst.set_contacts(c["imin"][m] - lo, c["imax"][m] - lo, c["ft"][m], c["vt"][m],
                      c["ip"][mw] - lo, c["iw"][mw], c["ftw"][mw], c["vtw"][mw])
+    if lo == 0 and hi == src.n:
+        dst.set_ncol(src.ncol())
     dst.initialize_cell_distribution()
 
 
@@ -165,8 +168,10 @@ def test_ensemble_64_systems_against_oracle():
     s.run(1501, 1504)
     walls = 0
     for k, o in enumerate(oracles):
+        n0 = o.ncol()
         o.run(1501, 1504)
         compare(s, o, f"system {k}", lo=off[k], hi=off[k + 1])
+        assert o.ncol() >= n0
         walls += o.count_contacts()[1]
         o.close()
     assert walls > 0  # the beds are on the floor
@@ -175,8 +180,10 @@ def test_ensemble_64_systems_against_oracle():
 
 def test_bidisperse_walls_past_floor_impact():
     """Bidisperse spheres (d = 1 and 3, 20:1) in a box closed by a floor and
-    four side walls, from rest to well past the impact on the floor."""
-    w = configs.bidisperse_settling(n=4000, width=24.0, headroom=4.0, sigma_v=0.2)
+    four side walls, from rest to well past the impact on the floor (gravity
+    10: the lowest layer lands after about 1,300 of the 3,000 steps)."""
+    w = configs.bidisperse_settling(n=4000, width=24.0, headroom=4.0, sigma_v=0.2,
+                                    gravity=10.0)
     g = DEMSystem(w.params)
     o = oracle_system(w.params)
     for s in (g, o):
