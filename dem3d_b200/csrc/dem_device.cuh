@@ -90,6 +90,9 @@ struct Counters {
   int need_kc;       // longest candidate row requested
   int in_overflow;   // a particle received more "j" contact results than fit
   int need_in;       // most "j" contact results of one particle in the last step
+  int cl_overflow;   // the pass found more contacts than the contact list holds
+  int need_cl;       // most contacts of one pass in the last step
+  int n_contacts;    // length of this pass's contact list
   int list_error;    // a cell-list walk exceeded its bound (corrupt lists)
   int nonfinite;     // a particle position became NaN or infinite
   unsigned int disp_max;  // FP32 bits (rounded up) of the largest displacement of one pass
@@ -177,23 +180,23 @@ __device__ __forceinline__ unsigned long long sweep_key(int cell, int rank) {
   return ((unsigned long long)(unsigned)cell << 32) | (unsigned)rank;
 }
 
-// Contact results handed from the contact kernel to the fold kernel.
+// Contact results handed from the pair kernel to the fold kernel.
 //  - "j" side: what particle j adds for one contact that particle i
 //    evaluated (Force(j) - FN - FT, Torque(j) + Rj*(Nij x FT)), with i's sweep
 //    key; record s of particle j at s*stride + j.
-//  - "i" side: the particle's own block, iForce and iTorque after its loop
-//    over partners, its walls and its drag.
+//  - "i" side: what particle i adds for the same contact (iForce + FN + FT,
+//    iTorque + (Ri*Nij) x FT), at the contact's place in the contact list.
 struct alignas(16) InRec64 {
   double2 a, b, c, d, e;  // (key, FN.x) (FN.y, FN.z) (FT.x, FT.y) (FT.z, NxFT.x) (NxFT.y, NxFT.z)
 };
 struct alignas(16) InRec32 {
   float4 a, b, c;  // (key lo, key hi, FN.x, FN.y) (FN.z, FT.xyz) (NxFT.xyz, 0)
 };
-struct alignas(16) Own64 {
-  double2 a, b, c;  // (iF.x, iF.y) (iF.z, iT.x) (iT.y, iT.z)
+struct alignas(16) IRec64 {
+  double2 a, b, c, d, e;  // (FN.x, FN.y) (FN.z, FT.x) (FT.y, FT.z) (tq.x, tq.y) (tq.z, 0)
 };
-struct alignas(8) Own32 {
-  float2 a, b, c;   // (iF.x, iF.y) (iF.z, iT.x) (iT.y, iT.z)
+struct alignas(16) IRec32 {
+  float4 a, b, c;  // (FN.xyz, FT.x) (FT.yz, tq.xy) (tq.z, 0, 0, 0); FT = FT + FT remainder
 };
 
 // Arguments of the two kernels of a force pass (contact kernel, fold
@@ -234,15 +237,24 @@ struct PassArgs {
   // (src/MForces.f90:319-333) as amsum[3p+k], then amsum[3n+3p+k]; NULL: not
   // kept
   double* amsum;
-  // contact kernel -> fold kernel: "j" results of every particle (count,
-  // records: InRec64 / InRec32 [in_cap][in_stride]) and the "i" blocks
-  // (Own64 / Own32 [n]); the fold kernel resets the counts
   const int* rank;
+  // test kernel -> pair kernel -> fold kernel: the pass's contact list
+  // (pair (i, j) per contact, the contacts of each "i" together and in row
+  // order: clist[cstart[i] .. + ccount[i])), the "i" results of every
+  // contact (IRec64 / IRec32 [cl_cap]), the "j" results of every particle
+  // (count, records InRec64 / InRec32 [in_cap][in_stride]) and the records
+  // of each particle's table that a contact matched (bit r: record r); the
+  // fold kernel resets the counts and the matched bits
+  int2* clist;
+  int* cstart;
+  int* ccount;
+  void* irec;
+  int cl_cap;
   int* in_cnt;
   void* in_rec;
   int in_cap, in_stride;
-  void* own;
-  // normal force on each wall, summed per block of the contact kernel in a
+  unsigned* matched;
+  // normal force on each wall, summed per block of the fold kernel in a
   // fixed order ([block][DEM_MAX_WALLS]); nw_max: walls of the system with
   // the most
   double* wall_part;

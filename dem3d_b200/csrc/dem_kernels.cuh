@@ -554,11 +554,14 @@ __global__ void k_relink(const DevParams* __restrict__ PT, const int* __restrict
     }
     cnt->pair_contacts = 0ull;
     cnt->wall_contacts = 0ull;
+    cnt->n_contacts = 0;  // the contact list of this pass starts empty
     if (update) {
       cnt->need_capacity = 0;
       cnt->need_in = 0;
+      cnt->need_cl = 0;
+    } else {
+      cnt->escaped = 0ull;  // escapes are counted by the current step's corrector
     }
-    else cnt->escaped = 0ull;  // escapes are counted by the current step's corrector
     const double d = (double)__uint_as_float(cnt->disp_max);
     cnt->disp_max = 0u;
     const double acc = cnt->disp_acc + d;
@@ -853,157 +856,197 @@ __global__ void __launch_bounds__(256) k_screen(const DevParams* __restrict__ PT
 }
 
 // ---------------------------------------------------------------------------
-// K2+K4: the FP64 force pass (exact order), two kernels.
+// K2+K4: a force pass is three kernels.
 //
-// k_contact_fp64: one thread per particle p, as "i" of its row: the overlap
-//   test over the row, every contact evaluated once (one lane per contact),
-//   the "i" part folded by p in row order (iForce, iTorque), then p's walls
-//   and drag -- p's whole block of the sweep.  The "j" part of each contact
-//   (FN, FT, Nij x FT) goes to the partner's incoming records with p's sweep
-//   key.  The history record of the pair is looked up in p's table, then in
-//   the partner's, and rewritten into p's new table.
-// k_fold_fp64: one thread per particle: its incoming "j" results and its own
-//   block added in sweep order (Force(j) = Force(j) - FN - FT,
-//   Torque(j) = Torque(j) + Rj*Nij_x_FT, Force(i) = Force(i) + iForce,
-//   src/MForces.f90:254-259, 319-320), a = F/m, alpha = T/I, then the
-//   integrator epilogue.
+// k_test (both precisions): one thread per particle as "i" of its row
+//   applies the reference's overlap test DeltaDijSq = MinDijSq - DijSq > 0
+//   (src/MForces.f90:218-224, exact FP64) to its candidates and writes its
+//   contacts to the pass's contact list, together and in row order.
+// k_pair_fp64 / k_pair_mixed: one thread per contact of the list evaluates
+//   it once (src/MForces.f90:199-252, CommonCalculations :339-387) with the
+//   pair's history record (looked up in i's table, then j's), writes the "i"
+//   half at the contact's place in the list, the "j" half to j's incoming
+//   records with i's sweep key, and the updated record into i's new table at
+//   the contact's rank among i's contacts.
+// k_fold_fp64 / k_fold_mixed: one thread per particle p builds its block of
+//   the sweep (iForce = m_eff*g, the "i" halves of its contacts in row order,
+//   its walls, its drag; src/MForces.f90:190-316), keeps the records no
+//   contact visited, adds the block and the "j" halves it received in sweep
+//   order (Force(j) = Force(j) - FN - FT, Torque(j) + Rj*Nij_x_FT,
+//   Force(i) = Force(i) + iForce; :254-259, 319-320), forms a = F/m,
+//   alpha = T/I (:330-333) and runs the integrator epilogue.
 
-// record keys of the owner kept in shared memory by the contact kernels
-constexpr int KREG = 8;
-
-// Owner data handed to the lane that computes one of its contacts.
-struct OwnerF64 {
-  double x, y, z, R, vx, vy, vz, wx, wy, wz;
-  int p, cp, sys, pad;
-  unsigned long long key;
+// Arguments of the test kernel (the same for both precisions).
+struct TestArgs {
+  const DevParams* P;
+  const int* sysid;
+  int n;
+  const double4* X;
+  const int* comp;
+  const int* cand;
+  const int* meta;
+  int2* clist;
+  int* cstart;
+  int* ccount;
+  int cl_cap;
+  Counters* cnt;
+  int tag;
 };
 
-// MINB: resident blocks of 128 threads per SM the kernel is compiled for
-// (registers per thread <= 65536 / (128 * MINB)); the autotuner picks one.
-template <bool PP, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_contact_fp64(PassArgs<double4, double2> A) {
-  // per warp: the current 32 contacts (candidate index, owner lane), their
-  // "i" results FN, FT, VT, torque term (12 doubles), the owners' first
-  // record keys, record counts and the records their contacts matched
-  __shared__ int s_k[4][32], s_o[4][32], s_q[4][32];
-  __shared__ int s_hk[4][KREG][32], s_hc[4][32];
-  __shared__ unsigned s_match[4][32];
-  __shared__ double s_r[12][4][32];
-  __shared__ double s_w[NWM][128];  // |FN| of each wall contact
+template <bool PP>
+__global__ void __launch_bounds__(128) k_test(TestArgs A) {
   __shared__ int s_abort;
-  // one decision for the whole block (it meets a block barrier later)
   if (threadIdx.x == 0) s_abort = A.cnt->abort;
   __syncthreads();
   if (s_abort) return;
-  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int w = 0; w < A.nw_max; w++) s_w[w][threadIdx.x] = 0.0;
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
   const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = p0 < A.n;
   const int p = valid ? p0 : 0;
-  const DevParams& P = sys_params(A.P, A.sysid, p);  // this particle's system
-  const Box& B = P.box;
   const int n = A.n;
-  unsigned n_col = 0, n_pc = 0, n_wc = 0;
-  int need = 0, need_in = 0;
-  bool in_over = false;
-
-  const int c = A.cell_cur[p];
+  const DevParams& P = sys_params(A.P, A.sysid, p);
   const double4 p4 = A.X[p];
-  const double xp[3] = {p4.x, p4.y, p4.z};
-  const double Rp = p4.w;
-  const double4 pv4 = A.v4[p];
-  const double2 pw2 = A.w2[p];
-  const double vp[3] = {pv4.x, pv4.y, pv4.z};
-  const double wp[3] = {pv4.w, pw2.x, pw2.y};
   const int cp = PP ? 0 : A.comp[p];
-  double inv_m, inv_i, eff_m;
-  Material<PP>::self(P, cp, Rp, inv_m, inv_i, eff_m);
-  const int n1 = A.meta[p] & META_MASK;
-  const unsigned long long key_p = sweep_key(c, A.rank[p]);
-  const double half_dt = A.half_dt;
+  const int m = valid ? (A.meta[p] & META_MASK) : 0;
+  // contact bit masks of the row, 64 candidates per window (windows past
+  // the first only for rows longer than 64)
+  unsigned long long mask0 = 0ull;
+  unsigned long long more[(KC_MAX + 1) / 64 - 1];
+  int total = 0;
+  for (int base = 0; base < m; base += 64) {
+    unsigned long long mask = 0ull;
+    const int end = m < base + 64 ? m : base + 64;
+#pragma unroll 1
+    for (int b = base; b < end; b += 4) {
+      int q[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) q[u] = b + u < end ? __ldg(A.cand + (size_t)(b + u) * n + p) : -1;
+      double4 xq[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        xq[u] = q[u] >= 0 ? A.X[q[u]] : make_double4(0.0, 0.0, 0.0, 0.0);
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        if (q[u] < 0) continue;
+        double Rij[3] = {xq[u].x - p4.x, xq[u].y - p4.y, xq[u].z - p4.z};
+#pragma unroll
+        for (int k = 0; k < 3; k++) Rij[k] = min_image_exact(Rij[k], P.box, k);
+        const double DijSq = sumsq3(Rij);
+        const int cq = PP ? 0 : A.comp[q[u]];
+        if (Material<PP>::min_dij_sq(P, cp, p4.w, cq, xq[u].w) - DijSq > 0.0)
+          mask |= 1ull << (b + u - base);
+      }
+    }
+    total += __popcll(mask);
+    if (base == 0) mask0 = mask;
+    else more[base / 64 - 1] = mask;
+  }
+  // one allocation per warp; a particle's contacts are contiguous
+  int incl = total;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(FULL, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const int wsum = __shfl_sync(FULL, incl, 31);
+  int wbase = 0;
+  if (lane == 31 && wsum > 0) {
+    wbase = atomicAdd(&A.cnt->n_contacts, wsum);
+    atomicMax(&A.cnt->need_cl, wbase + wsum);
+  }
+  wbase = __shfl_sync(FULL, wbase, 31);
+  const int start = wbase + incl - total;
+  if (valid) {
+    A.cstart[p] = start;
+    A.ccount[p] = total;
+  }
+  if (start + total > A.cl_cap) {
+    // the list is grown and the pass launched again
+    atomicExch(&A.cnt->cl_overflow, 1);
+    set_abort(A.cnt, A.tag);
+  } else if (total > 0) {
+    int s = start;
+    for (int base = 0; base < m; base += 64) {
+      unsigned long long mask = base == 0 ? mask0 : more[base / 64 - 1];
+      while (mask) {
+        const int k = base + __ffsll((long long)mask) - 1;
+        mask &= mask - 1ull;
+        A.clist[s++] = make_int2(p, __ldg(A.cand + (size_t)k * n + p));
+      }
+    }
+  }
+  publish_counts_block(A.cnt, false, 0u, (unsigned)total, 0u, 0u, 0u);
+}
+
+// record keys read before the record count is known (speculatively, within
+// the table's capacity)
+constexpr int KSPEC = 2;
+
+// The pair kernel (FP64): one thread per contact, grid-stride over the list.
+template <bool PP, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_pair_fp64(PassArgs<double4, double2> A) {
+  __shared__ int s_abort;
+  if (threadIdx.x == 0) s_abort = A.cnt->abort;
+  __syncthreads();
+  if (s_abort) return;
+  const int total = A.cnt->n_contacts;
   const bool update = A.update != 0;
-  int hw_n = 0;
-  bool overflow = false;
-  const int hc = valid ? A.Hr.cnt[p] : 0;
-#pragma unroll
-  for (int r = 0; r < KREG; r++) s_hk[wid][r][lane] = r < hc ? A.Hr.key[hslot(A.Hr, p, r)] : -1;
-  s_hc[wid][lane] = hc;
-  s_match[wid][lane] = 0u;
-  __syncwarp();
-
-  double iF[3], iT[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-  for (int k = 0; k < 3; k++) iF[k] = eff_m * P.gravity[k];
-
-  auto record = [&](int partner, const double ft[3], const double vt[3]) {
-    if (hw_n < A.Hw.cap)
-      hist_write(A.Hw, p, hw_n, partner, ft, vt);
-    else
-      overflow = true;
-    hw_n++;
-  };
-  // Rij = x_j - x_i (minimum image, src/MForces.f90:209-217)
-  auto geometry = [&](const Box& Bx, const double xo[3], const double4& q4,
-                      double Rij[3]) -> double {
-    Rij[0] = q4.x - xo[0];
-    Rij[1] = q4.y - xo[1];
-    Rij[2] = q4.z - xo[2];
-#pragma unroll
-    for (int k = 0; k < 3; k++) Rij[k] = min_image_exact(Rij[k], Bx, k);
-    return sumsq3(Rij);
-  };
-  // the overlap test DeltaDijSq = MinDijSq - DijSq > 0 (src/MForces.f90:218-224)
-  auto test = [&](int, int q, const double4& q4) -> bool {
-    double Rij[3];
-    const double DijSq = geometry(B, xp, q4, Rij);
-    const int cq = PP ? 0 : A.comp[q];
-    return Material<PP>::min_dij_sq(P, cp, Rp, cq, q4.w) - DijSq > 0.0;
-  };
-  // one contact of owner `o` ("i") with candidate k ("j"), computed by this
-  // lane (src/MForces.f90:199-252)
-  auto compute = [&](const OwnerF64& o, int oo, int k, int slot) {
-    const int q = __ldg(A.cand + (size_t)k * n + o.p);
+  const double half_dt = A.half_dt;
+  unsigned n_col = 0;
+  int need = 0, need_in = 0;
+  bool overflow = false, in_over = false;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < total;
+       s += gridDim.x * blockDim.x) {
+    const int2 e = A.clist[s];
+    const int p = e.x, q = e.y;
     const int s_in = atomicAdd(&A.in_cnt[q], 1);  // q's "j" record (returns early)
-    const double4 q4 = A.X[q];
-    const double2 qw2 = A.w2[q];
-    const double4 qv4 = A.v4[q];
-    const double xo[3] = {o.x, o.y, o.z};
-    double Rij[3];
-    const DevParams& PO = A.P[o.sys];  // the owner's system (a warp may span two)
-    const double DijSq = geometry(PO.box, xo, q4, Rij);
-    const int cq = PP ? 0 : A.comp[q];
-    const double Delta = Material<PP>::min_dij_sq(PO, o.cp, o.R, cq, q4.w) - DijSq;
+    const int ord = s - A.cstart[p];
+    const int hc = A.Hr.cnt[p];
+    int kspec[KSPEC];
+#pragma unroll
+    for (int r = 0; r < KSPEC; r++) kspec[r] = r < A.Hr.cap ? A.Hr.key[hslot(A.Hr, p, r)] : -1;
+    const DevParams& P = sys_params(A.P, A.sysid, p);
+    const double4 p4 = A.X[p], q4 = A.X[q];
+    const double4 pv4 = A.v4[p], qv4 = A.v4[q];
+    const double2 pw2 = A.w2[p], qw2 = A.w2[q];
+    const int cp = PP ? 0 : A.comp[p], cq = PP ? 0 : A.comp[q];
+    // Rij = x_j - x_i (minimum image, src/MForces.f90:209-217)
+    double Rij[3] = {q4.x - p4.x, q4.y - p4.y, q4.z - p4.z};
+#pragma unroll
+    for (int k = 0; k < 3; k++) Rij[k] = min_image_exact(Rij[k], P.box, k);
+    const double DijSq = sumsq3(Rij);
+    const double Delta = Material<PP>::min_dij_sq(P, cp, p4.w, cq, q4.w) - DijSq;
     PairPar pp;
-    Material<PP>::pair(PO, o.cp, o.R, cq, q4.w, pp);
-    const double va[3] = {o.vx, o.vy, o.vz}, wa[3] = {o.wx, o.wy, o.wz};
+    Material<PP>::pair(P, cp, p4.w, cq, q4.w, pp);
+    const double va[3] = {pv4.x, pv4.y, pv4.z}, wa[3] = {pv4.w, pw2.x, pw2.y};
     const double vb[3] = {qv4.x, qv4.y, qv4.z}, wb[3] = {qv4.w, qw2.x, qw2.y};
-    // VerifyPairContact: the owner's records, then the partner's
-    double FT0[3] = {0.0, 0.0, 0.0}, VT0[3] = {0.0, 0.0, 0.0};
-    const int oc = s_hc[wid][oo];
+    // VerifyPairContact: i's records, then j's
     int r = -1;
 #pragma unroll
-    for (int rr = 0; rr < KREG; rr++)
-      if (rr < oc && s_hk[wid][rr][oo] == q) r = rr;
-    for (int rr = KREG; r < 0 && rr < oc; rr++)
-      if (A.Hr.key[hslot(A.Hr, o.p, rr)] == q) r = rr;
+    for (int rr = 0; rr < KSPEC; rr++)
+      if (r < 0 && rr < hc && kspec[rr] == q) r = rr;
+    for (int rr = KSPEC; r < 0 && rr < hc; rr++)
+      if (A.Hr.key[hslot(A.Hr, p, rr)] == q) r = rr;
+    double FT0[3] = {0.0, 0.0, 0.0}, VT0[3] = {0.0, 0.0, 0.0};
     bool contacting = r >= 0;
     if (contacting) {
-      hist_read(A.Hr, o.p, r, FT0, VT0);
-      if (r < 32) atomicOr(&s_match[wid][oo], 1u << r);
+      hist_read(A.Hr, p, r, FT0, VT0);
+      if (r < 32) atomicOr(&A.matched[p], 1u << r);
     } else {
-      const int r2 = find_record(A.Hr, q, o.p);
+      const int r2 = find_record(A.Hr, q, p);
       contacting = r2 >= 0;
       if (contacting) hist_read(A.Hr, q, r2, FT0, VT0);
     }
     if (!contacting) n_col++;
-    n_pc++;
     ContactOut out;
-    pair_contact(Rij, DijSq, Delta, pp, o.R, va, wa, q4.w, vb, wb, half_dt, contacting, FT0, VT0,
+    pair_contact(Rij, DijSq, Delta, pp, p4.w, va, wa, q4.w, vb, wb, half_dt, contacting, FT0, VT0,
                  out);
-    // "j" side into q's incoming records
+    // "j" half into q's incoming records
     if (s_in < A.in_cap) {
       InRec64* rec = (InRec64*)A.in_rec + (size_t)s_in * A.in_stride + q;
-      rec->a = make_double2(__longlong_as_double((long long)o.key), out.FN[0]);
+      rec->a = make_double2(__longlong_as_double((long long)sweep_key(A.cell_cur[p], A.rank[p])),
+                            out.FN[0]);
       rec->b = make_double2(out.FN[1], out.FN[2]);
       rec->c = make_double2(out.FT[0], out.FT[1]);
       rec->d = make_double2(out.FT[2], out.NxFT[0]);
@@ -1012,128 +1055,24 @@ __global__ void __launch_bounds__(128, MINB) k_contact_fp64(PassArgs<double4, do
       in_over = true;
     }
     need_in = need_in > s_in + 1 ? need_in : s_in + 1;
-    // "i" side to the owner (iTorque + (Ri*Nij) x FT)
+    // "i" half at the contact's place (iTorque + (Ri*Nij) x FT)
     double RN[3], tq[3];
 #pragma unroll
-    for (int d = 0; d < 3; d++) RN[d] = o.R * out.N[d];
+    for (int d = 0; d < 3; d++) RN[d] = p4.w * out.N[d];
     cross3(RN, out.FT, tq);
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      s_r[d][wid][slot] = out.FN[d];
-      s_r[3 + d][wid][slot] = out.FT[d];
-      s_r[6 + d][wid][slot] = out.VT[d];
-      s_r[9 + d][wid][slot] = tq[d];
-    }
-    s_q[wid][slot] = q;
-  };
-  // the owner adds one contact (iForce = iForce + FN + FT) and stores its record
-  auto accum = [&](int slot, int) {
-    double FN[3], FT[3], VT[3], tq[3];
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      FN[d] = s_r[d][wid][slot];
-      FT[d] = s_r[3 + d][wid][slot];
-      VT[d] = s_r[6 + d][wid][slot];
-      tq[d] = s_r[9 + d][wid][slot];
-    }
-#pragma unroll
-    for (int d = 0; d < 3; d++) iF[d] = iF[d] + FN[d] + FT[d];
-#pragma unroll
-    for (int d = 0; d < 3; d++) iT[d] = iT[d] + tq[d];
-    if (update) record(s_q[wid][slot], FT, VT);
-  };
-  const OwnerF64 me{xp[0], xp[1], xp[2], Rp, vp[0], vp[1], vp[2], wp[0], wp[1], wp[2],
-                    p, cp, A.sysid ? A.sysid[p] : 0, 0, key_p};
-  contact_loop(A.cand, A.X, n, p, valid, n1, me, s_k[wid], s_o[wid], test, compute, accum);
-
-  if (valid) {
-    // ---- walls (src/MForces.f90:274-314)
-    for (int w = 0; w < P.nw; w++) {
-      const dem_wall& W = P.walls[w];
-      const int wi = p * P.nw + w;
-      bool contacting = A.Hr.wflag[wi] != 0;
-      double FT0[3] = {0.0, 0.0, 0.0}, VT0[3] = {0.0, 0.0, 0.0};
-      if (contacting) {
-        const double2* v = A.Hr.wval + (size_t)wi * 3;
-        double2 a = v[0], b = v[1], d = v[2];
-        FT0[0] = a.x; FT0[1] = a.y; FT0[2] = b.x;
-        VT0[0] = b.y; VT0[1] = d.x; VT0[2] = d.y;
-      }
-      double Dij, Nij[3], Qji[3];
-      const bool ov = overlap_wall(P, W, xp, Rp, Dij, Nij, Qji);
-      if (ov) {
-        n_wc++;
-        const double Delta = Rp * Rp - Dij * Dij;
-        const double dn = Dij - Rp;
-        double DispN[3], wqv[3], Vij[3], ro[3], cr[3], VijC[3], Rw[3];
-#pragma unroll
-        for (int k = 0; k < 3; k++) DispN[k] = dn * Nij[k];
-        cross3(W.omega, Qji, wqv);
-#pragma unroll
-        for (int k = 0; k < 3; k++) Vij[k] = W.velocity[k] + wqv[k] - vp[k];
-#pragma unroll
-        for (int k = 0; k < 3; k++) ro[k] = Rp * wp[k];
-        cross3(ro, Nij, cr);
-#pragma unroll
-        for (int k = 0; k < 3; k++) VijC[k] = Vij[k] - cr[k];
-#pragma unroll
-        for (int k = 0; k < 3; k++) Rw[k] = W.position[k] + Qji[k] - xp[k];
-        PairPar pp;
-        Material<PP>::wall(P, cp, Rp, w, pp);
-        ContactOut o;
-        common_calc(Rw, Nij, DispN, Vij, VijC, Delta, half_dt, contacting, FT0, VT0, pp.kn, pp.yn,
-                    pp.kt, pp.yt, pp.mu_sq, o);
-#pragma unroll
-        for (int k = 0; k < 3; k++) iF[k] = iF[k] + o.FN[k] + o.FT[k];
-        double RN[3], tq[3];
-#pragma unroll
-        for (int k = 0; k < 3; k++) RN[k] = Rp * o.N[k];
-        cross3(RN, o.FT, tq);
-#pragma unroll
-        for (int k = 0; k < 3; k++) iT[k] = iT[k] + tq[k];
-        s_w[w][threadIdx.x] = sqrt(sumsq3(o.FN));
-        if (update) {
-          A.Hw.wflag[wi] = 1;
-          double2* v = A.Hw.wval + (size_t)wi * 3;
-          v[0] = make_double2(o.FT[0], o.FT[1]);
-          v[1] = make_double2(o.FT[2], o.VT[0]);
-          v[2] = make_double2(o.VT[1], o.VT[2]);
-        }
-      } else if (update) {
-        A.Hw.wflag[wi] = 0;
-      }
-    }
-    if (A.drag) {  // iForce = iForce + DragForce(iPart) (src/MForces.f90:316)
-#pragma unroll
-      for (int k = 0; k < 3; k++) iF[k] = iF[k] + A.drag[(size_t)3 * p + k];
-    }
-    Own64* ow = (Own64*)A.own + p;
-    ow->a = make_double2(iF[0], iF[1]);
-    ow->b = make_double2(iF[2], iT[0]);
-    ow->c = make_double2(iT[1], iT[2]);
-    // ---- the records this particle holds and no contact of the pass
-    // matched: kept if the sweep did not visit the pair (its cells are not
-    // neighbours, or the partner index lies past the last particle, a record
-    // that particle removal left behind), else the contact ended
-    // (RemovePairContact) or the other particle evaluated it
+    IRec64* ir = (IRec64*)A.irec + s;
+    ir->a = make_double2(out.FN[0], out.FN[1]);
+    ir->b = make_double2(out.FN[2], out.FT[0]);
+    ir->c = make_double2(out.FT[1], out.FT[2]);
+    ir->d = make_double2(tq[0], tq[1]);
+    ir->e = make_double2(tq[2], 0.0);
+    // UpdatePairContact: the record goes to i's new table, in row order
     if (update) {
-      const unsigned matched = s_match[wid][lane];
-      for (int r = 0; r < hc; r++) {
-        if (r < 32 && ((matched >> r) & 1u)) continue;
-        const int q2 = A.Hr.key[hslot(A.Hr, p, r)];
-        if (q2 >= A.n || !cells_adjacent(P, c, A.cell_cur[q2])) {
-          double ft[3], vt[3];
-          hist_read(A.Hr, p, r, ft, vt);
-          record(q2, ft, vt);
-        }
-      }
-      A.Hw.cnt[p] = hw_n < A.Hw.cap ? hw_n : A.Hw.cap;
-      need = hw_n;
+      if (ord < A.Hw.cap) hist_write(A.Hw, p, ord, q, out.FT, out.VT);
+      else overflow = true;
+      need = need > ord + 1 ? need : ord + 1;
     }
   }
-  if (A.nw_max > 0) wall_partials(s_w, A.nw_max, A.wall_part);
-  // a table that overflowed: the pass is launched again with larger tables;
-  // stop what follows
   if (overflow) {
     atomicExch(&A.cnt->overflow, 1);
     set_abort(A.cnt, A.tag);
@@ -1142,36 +1081,154 @@ __global__ void __launch_bounds__(128, MINB) k_contact_fp64(PassArgs<double4, do
     atomicExch(&A.cnt->in_overflow, 1);
     set_abort(A.cnt, A.tag);
   }
-  publish_counts_block(A.cnt, A.update != 0, n_col, n_pc, n_wc, (unsigned)need,
-                       (unsigned)need_in);
+  publish_counts_block(A.cnt, update, n_col, 0u, 0u, (unsigned)need, (unsigned)need_in);
 }
 
-// The fold kernel: Force and Torque of every particle in sweep order, a =
-// F/m, alpha = T/I (src/MForces.f90:330-333), then the integrator epilogue.
-template <bool PP, int EPI, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_fold_fp64(PassArgs<double4, double2> A) {
+// The fold kernel (FP64): p's block of the sweep, its Force and Torque in
+// sweep order, a = F/m, alpha = T/I, then the integrator epilogue.  WALLS:
+// some system has walls.
+template <bool PP, int EPI, bool WALLS>
+__global__ void __launch_bounds__(128, 4) k_fold_fp64(PassArgs<double4, double2> A) {
+  __shared__ double s_w[WALLS ? NWM : 1][128];  // |FN| of each wall contact
   __shared__ int s_abort;
-  // one decision for the whole block (it meets a block barrier at the end)
+  // one decision for the whole block (it meets block barriers later)
   if (threadIdx.x == 0) s_abort = A.cnt->abort;
   __syncthreads();
   if (s_abort) return;
+  if (WALLS)
+    for (int w = 0; w < A.nw_max; w++) s_w[w][threadIdx.x] = 0.0;
   const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = p0 < A.n;
   const int p = valid ? p0 : 0;
+  const bool update = A.update != 0;
+  unsigned n_wc = 0;
+  int need = 0;
+  bool overflow = false;
   double d2 = 0.0;
   if (valid) {
     const DevParams& P = sys_params(A.P, A.sysid, p);
     const int c = A.cell_cur[p];
     const unsigned long long key_p = sweep_key(c, A.rank[p]);
     const int ni = A.in_cnt[p];
-    A.in_cnt[p] = 0;  // for the next pass's contact kernel
+    if (ni) A.in_cnt[p] = 0;  // for the next pass's pair kernel
+    const unsigned matched = A.matched[p];
+    if (matched) A.matched[p] = 0u;
+    const int nc = A.ccount[p];
+    const int st0 = A.cstart[p];
     const double4 p4 = A.X[p];
     const double xp[3] = {p4.x, p4.y, p4.z};
     const double Rp = p4.w;
+    const double4 pv4 = A.v4[p];
+    const double2 pw2 = A.w2[p];
+    const double vp[3] = {pv4.x, pv4.y, pv4.z};
+    const double wp[3] = {pv4.w, pw2.x, pw2.y};
     const int cp = PP ? 0 : A.comp[p];
     double inv_m, inv_i, eff_m;
     Material<PP>::self(P, cp, Rp, inv_m, inv_i, eff_m);
-    const Own64 ow = ((const Own64*)A.own)[p];
+    // ---- p's block: gravity, its contacts as "i" in row order
+    double iF[3], iT[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < 3; k++) iF[k] = eff_m * P.gravity[k];
+    const IRec64* ir = (const IRec64*)A.irec + st0;
+    for (int k = 0; k < nc; k++) {
+      const IRec64 r = ir[k];
+      const double FN[3] = {r.a.x, r.a.y, r.b.x}, FT[3] = {r.b.y, r.c.x, r.c.y};
+      const double tq[3] = {r.d.x, r.d.y, r.e.x};
+#pragma unroll
+      for (int d = 0; d < 3; d++) iF[d] = iF[d] + FN[d] + FT[d];
+#pragma unroll
+      for (int d = 0; d < 3; d++) iT[d] = iT[d] + tq[d];
+    }
+    int hw_n = nc;  // the pair kernel wrote the records of the contacts
+    // ---- walls (src/MForces.f90:274-314)
+    if (WALLS) {
+      const double half_dt = A.half_dt;
+      for (int w = 0; w < P.nw; w++) {
+        const dem_wall& W = P.walls[w];
+        const int wi = p * P.nw + w;
+        bool contacting = A.Hr.wflag[wi] != 0;
+        double FT0[3] = {0.0, 0.0, 0.0}, VT0[3] = {0.0, 0.0, 0.0};
+        if (contacting) {
+          const double2* v = A.Hr.wval + (size_t)wi * 3;
+          double2 a = v[0], b = v[1], dd = v[2];
+          FT0[0] = a.x; FT0[1] = a.y; FT0[2] = b.x;
+          VT0[0] = b.y; VT0[1] = dd.x; VT0[2] = dd.y;
+        }
+        double Dij, Nij[3], Qji[3];
+        const bool ov = overlap_wall(P, W, xp, Rp, Dij, Nij, Qji);
+        if (ov) {
+          n_wc++;
+          const double Delta = Rp * Rp - Dij * Dij;
+          const double dn = Dij - Rp;
+          double DispN[3], wqv[3], Vij[3], ro[3], cr[3], VijC[3], Rw[3];
+#pragma unroll
+          for (int k = 0; k < 3; k++) DispN[k] = dn * Nij[k];
+          cross3(W.omega, Qji, wqv);
+#pragma unroll
+          for (int k = 0; k < 3; k++) Vij[k] = W.velocity[k] + wqv[k] - vp[k];
+#pragma unroll
+          for (int k = 0; k < 3; k++) ro[k] = Rp * wp[k];
+          cross3(ro, Nij, cr);
+#pragma unroll
+          for (int k = 0; k < 3; k++) VijC[k] = Vij[k] - cr[k];
+#pragma unroll
+          for (int k = 0; k < 3; k++) Rw[k] = W.position[k] + Qji[k] - xp[k];
+          PairPar pp;
+          Material<PP>::wall(P, cp, Rp, w, pp);
+          ContactOut o;
+          common_calc(Rw, Nij, DispN, Vij, VijC, Delta, half_dt, contacting, FT0, VT0, pp.kn,
+                      pp.yn, pp.kt, pp.yt, pp.mu_sq, o);
+#pragma unroll
+          for (int k = 0; k < 3; k++) iF[k] = iF[k] + o.FN[k] + o.FT[k];
+          double RN[3], tq[3];
+#pragma unroll
+          for (int k = 0; k < 3; k++) RN[k] = Rp * o.N[k];
+          cross3(RN, o.FT, tq);
+#pragma unroll
+          for (int k = 0; k < 3; k++) iT[k] = iT[k] + tq[k];
+          s_w[w][threadIdx.x] = sqrt(sumsq3(o.FN));
+          if (update) {
+            A.Hw.wflag[wi] = 1;
+            double2* v = A.Hw.wval + (size_t)wi * 3;
+            v[0] = make_double2(o.FT[0], o.FT[1]);
+            v[1] = make_double2(o.FT[2], o.VT[0]);
+            v[2] = make_double2(o.VT[1], o.VT[2]);
+          }
+        } else if (update) {
+          A.Hw.wflag[wi] = 0;
+        }
+      }
+    }
+    if (A.drag) {  // iForce = iForce + DragForce(iPart) (src/MForces.f90:316)
+#pragma unroll
+      for (int k = 0; k < 3; k++) iF[k] = iF[k] + A.drag[(size_t)3 * p + k];
+    }
+    // ---- the records p holds that no contact matched: kept if the sweep
+    // did not visit the pair (its cells are not neighbours, or the partner
+    // index lies past the last particle, a record that particle removal left
+    // behind), else the contact ended (RemovePairContact) or the other
+    // particle evaluated it
+    if (update) {
+      const int hc = A.Hr.cnt[p];
+      for (int r = 0; r < hc; r++) {
+        if (r < 32 && ((matched >> r) & 1u)) continue;
+        const int q2 = A.Hr.key[hslot(A.Hr, p, r)];
+        if (q2 >= A.n || !cells_adjacent(P, c, A.cell_cur[q2])) {
+          if (hw_n < A.Hw.cap) {
+            double ft[3], vt[3];
+            hist_read(A.Hr, p, r, ft, vt);
+            hist_write(A.Hw, p, hw_n, q2, ft, vt);
+          } else {
+            overflow = true;
+          }
+          hw_n++;
+        }
+      }
+      A.Hw.cnt[p] = hw_n < A.Hw.cap ? hw_n : A.Hw.cap;
+      if (hw_n > A.Hw.cap) overflow = true;
+      need = hw_n;
+    }
+    // ---- Force and Torque in sweep order
     const InRec64* in = (const InRec64*)A.in_rec + p;
     const size_t st = (size_t)A.in_stride;
     double F[3] = {0.0, 0.0, 0.0}, T[3] = {0.0, 0.0, 0.0};
@@ -1181,7 +1238,6 @@ __global__ void __launch_bounds__(128, MINB) k_fold_fp64(PassArgs<double4, doubl
           return (unsigned long long)__double_as_longlong(((const double*)(in + e * st))[0]);
         },
         [&]() {
-          const double iF[3] = {ow.a.x, ow.a.y, ow.b.x}, iT[3] = {ow.b.y, ow.c.x, ow.c.y};
 #pragma unroll
           for (int k = 0; k < 3; k++) F[k] = F[k] + iF[k];
 #pragma unroll
@@ -1208,12 +1264,14 @@ __global__ void __launch_bounds__(128, MINB) k_fold_fp64(PassArgs<double4, doubl
     for (int k = 0; k < 3; k++) acc[k] = F[k] * inv_m;
 #pragma unroll
     for (int k = 0; k < 3; k++) alp[k] = T[k] * inv_i;
-    const double4 pv4 = A.v4[p];
-    const double2 pw2 = A.w2[p];
-    const double vp[3] = {pv4.x, pv4.y, pv4.z};
-    const double wp[3] = {pv4.w, pw2.x, pw2.y};
     epilogue<EPI>(A, P, p, xp, Rp, vp, wp, acc, alp, c, d2);
   }
+  if (WALLS && A.nw_max > 0) wall_partials(s_w, A.nw_max, A.wall_part);
+  if (overflow) {
+    atomicExch(&A.cnt->overflow, 1);
+    set_abort(A.cnt, A.tag);
+  }
+  publish_counts_block(A.cnt, update, 0u, 0u, n_wc, (unsigned)need, 0u);
   if (EPI != EPI_STORE) publish_disp_block(A.cnt, d2);
 }
 

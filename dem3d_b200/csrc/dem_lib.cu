@@ -107,12 +107,18 @@ struct dem_ctx {
   int drag_cap = 0;
   double* amsum = nullptr;  // [9*ncap] corrector ring sums (predictor -> corrector)
   int amsum_cap = 0;
-  // contact kernel -> fold kernel of a pass: "j" results per particle
-  // (count, in_cap records of InRec64/InRec32 laid out for pass_cap rows) and
-  // the "i" block of every particle (Own64/Own32)
+  // test -> pair -> fold kernels of a pass: the contact list (cl_cap
+  // contacts, their "i" results IRec64/IRec32), each particle's place in
+  // it, the "j" results per particle (count, in_cap records of
+  // InRec64/InRec32 laid out for pass_cap rows) and the matched record bits
+  int2* clist = nullptr;
+  void* irec = nullptr;
+  int cl_cap = 0;
+  int* cstart = nullptr;
+  int* ccount = nullptr;
+  unsigned* matched = nullptr;
   int* in_cnt = nullptr;
   void* in_rec = nullptr;
-  void* own = nullptr;
   double* wall_part = nullptr;  // [contact-kernel blocks][NWM] wall normal forces
   int nw_max = 0;               // walls of the system with the most
   int in_cap = 8;
@@ -123,7 +129,7 @@ struct dem_ctx {
   int* rm_buf = nullptr;  // escaped list + status words of the removal kernel
   int rm_cap = 0;
   long long rm_stats[3] = {0, 0, 0};  // removals, swaps, records renamed or moved
-  int pass_variant = 0;  // contact kernel compiled for 4 (0), 3 (1) or 5 (2) blocks per SM
+  int pass_variant = 0;  // pair kernel compiled for 4 (0), 3 (1) or 5 (2) blocks per SM
   bool has_cone = false; // some wall of some system is a cone
   double skin_factor = 0.05;  // candidate-row skin / CutOff
   int par = 0;         // L.cell[par] is the assignment the lists hold
@@ -293,12 +299,21 @@ void free_lists(dem_ctx* c) {
   c->rows = Rows{};
   cudaFree(c->in_cnt);
   cudaFree(c->in_rec);
-  cudaFree(c->own);
   cudaFree(c->wall_part);
+  cudaFree(c->clist);
+  cudaFree(c->irec);
+  cudaFree(c->cstart);
+  cudaFree(c->ccount);
+  cudaFree(c->matched);
   c->in_cnt = nullptr;
   c->in_rec = nullptr;
-  c->own = nullptr;
   c->wall_part = nullptr;
+  c->clist = nullptr;
+  c->irec = nullptr;
+  c->cstart = nullptr;
+  c->ccount = nullptr;
+  c->matched = nullptr;
+  c->cl_cap = 0;
   c->pass_cap = 0;
   for (int b = 0; b < 2; b++) {
     cudaFree(c->X[b]);
@@ -594,11 +609,16 @@ PassArgs<V4, W2> pass_args(dem_ctx* c, int side, bool update, double dt, const R
   A.drag = c->fluid ? c->drag : nullptr;
   A.amsum = c->amsum;
   A.rank = c->rows.rank;
+  A.clist = c->clist;
+  A.cstart = c->cstart;
+  A.ccount = c->ccount;
+  A.irec = c->irec;
+  A.cl_cap = c->cl_cap;
   A.in_cnt = c->in_cnt;
   A.in_rec = c->in_rec;
   A.in_cap = c->in_cap;
   A.in_stride = c->pass_cap;
-  A.own = c->own;
+  A.matched = c->matched;
   A.wall_part = c->wall_part;
   A.nw_max = c->nw_max;
   return A;
@@ -614,6 +634,32 @@ int alloc_incoming(dem_ctx* c, int cap) {
   c->in_rec = nullptr;
   CK(cudaMalloc(&c->in_rec, in_rec_bytes(c) * (size_t)cap * (size_t)c->pass_cap));
   c->in_cap = cap;
+  return DEM_OK;
+}
+
+// the contact list of a pass and the "i" results of its contacts
+int alloc_contacts(dem_ctx* c, int cap) {
+  cudaFree(c->clist);
+  cudaFree(c->irec);
+  c->clist = nullptr;
+  c->irec = nullptr;
+  const size_t rb = c->precision == DEM_PREC_MIXED ? sizeof(IRec32) : sizeof(IRec64);
+  CK(cudaMalloc(&c->clist, sizeof(int2) * (size_t)std::max(cap, 1)));
+  CK(cudaMalloc(&c->irec, rb * (size_t)std::max(cap, 1)));
+  c->cl_cap = cap;
+  return DEM_OK;
+}
+
+// a longer contact list (it only lives within a pass)
+int grow_contacts(dem_ctx* c, int need) {
+  long long cap = std::max(c->cl_cap, 1024);
+  while (cap < need) cap = cap * 3 / 2;
+  if (cap > (1ll << 30)) return fail(c, DEM_ERR_CAPACITY, "contact list beyond 2^30 contacts");
+  if (cap == c->cl_cap) return DEM_OK;
+  CK(cudaStreamSynchronize(c->stream));
+  int st = alloc_contacts(c, (int)cap);
+  if (st) return st;
+  drop_graphs(c);
   return DEM_OK;
 }
 
@@ -635,16 +681,25 @@ int ensure_pass_buffers(dem_ctx* c) {
   if (c->pass_cap >= N) return DEM_OK;
   CK(cudaStreamSynchronize(c->stream));
   cudaFree(c->in_cnt);
-  cudaFree(c->own);
   cudaFree(c->wall_part);
+  cudaFree(c->cstart);
+  cudaFree(c->ccount);
+  cudaFree(c->matched);
   c->in_cnt = nullptr;
-  c->own = nullptr;
   c->wall_part = nullptr;
+  c->cstart = c->ccount = nullptr;
+  c->matched = nullptr;
   c->pass_cap = N;
   CK(cudaMalloc(&c->in_cnt, sizeof(int) * (size_t)N));
   CK(cudaMemset(c->in_cnt, 0, sizeof(int) * (size_t)N));
-  CK(cudaMalloc(&c->own, (c->precision == DEM_PREC_MIXED ? sizeof(Own32) : sizeof(Own64)) *
-                             (size_t)N));
+  CK(cudaMalloc(&c->matched, sizeof(unsigned) * (size_t)N));
+  CK(cudaMemset(c->matched, 0, sizeof(unsigned) * (size_t)N));
+  CK(cudaMalloc(&c->cstart, sizeof(int) * (size_t)N));
+  CK(cudaMalloc(&c->ccount, sizeof(int) * (size_t)N));
+  if (c->cl_cap < 2 * N) {
+    int st = alloc_contacts(c, 2 * N);
+    if (st) return st;
+  }
   const size_t parts = (size_t)blocks_for(N, 128) * NWM;
   CK(cudaMalloc(&c->wall_part, sizeof(double) * parts));
   CK(cudaMemset(c->wall_part, 0, sizeof(double) * parts));
@@ -692,12 +747,34 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
                         int tag) {
   if (c->n == 0) return;
   const StateArrays& tgt = side ? c->Pr : c->P;
+  // the test kernel: the contact list of the pass
+  TestArgs T;
+  T.P = c->dp;
+  T.sysid = c->sysid;
+  T.n = c->n;
+  T.X = c->X[side];
+  T.comp = c->comp;
+  T.cand = c->rows.cand;
+  T.meta = c->rows.meta;
+  T.clist = c->clist;
+  T.cstart = c->cstart;
+  T.ccount = c->ccount;
+  T.cl_cap = c->cl_cap;
+  T.cnt = c->cnt;
+  T.tag = tag;
+  const unsigned g = blocks_for(c->n, 128);
+  if (c->pp) launch(c, "test", k_test<true>, g, 128, T);
+  else launch(c, "test", k_test<false>, g, 128, T);
+  const int mb = c->pass_variant == 1 ? 3 : c->pass_variant == 2 ? 5 : 4;
+  const unsigned pair_blocks = (unsigned)(148 * mb);
+  const bool walls = c->nw_max > 0;
   if (c->precision == DEM_PREC_MIXED) {
     auto A = pass_args<float4, float2>(c, side, update, dt, rm, tag, tgt);
     if (epi == EPI_STORE) A.amsum = c->force_out;
     for (int part = 0; part < 2; part++) {
-      timed(c, part ? "fold_mixed" : "contact_mixed", [&]() {
-        mixed_pass(c->M, c->pp, epi, c->pass_variant, c->has_cone, A, c->hcur, c->stream, part);
+      timed(c, part ? "fold_mixed" : "pair_mixed", [&]() {
+        mixed_pass(c->M, c->pp, epi, c->pass_variant, walls, c->has_cone, A, c->hcur, c->stream,
+                   part, pair_blocks);
       });
       c->launches++;
     }
@@ -705,30 +782,35 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
   }
   auto A = pass_args<double4, double2>(c, side, update, dt, rm, tag, tgt);
   if (epi == EPI_STORE) A.amsum = c->force_out;
-  const unsigned g = blocks_for(c->n, 128);
-#define CONTACT_CASE(PPV, MB) launch(c, "contact_fp64", k_contact_fp64<PPV, MB>, g, 128, A)
-  if (c->pass_variant == 1) {
-    if (c->pp) CONTACT_CASE(true, 3);
-    else CONTACT_CASE(false, 3);
-  } else if (c->pass_variant == 2) {
-    if (c->pp) CONTACT_CASE(true, 5);
-    else CONTACT_CASE(false, 5);
+#define PAIR_CASE(PPV, MB) \
+  launch(c, "pair_fp64", k_pair_fp64<PPV, MB>, pair_blocks, 128, A)
+  if (mb == 3) {
+    if (c->pp) PAIR_CASE(true, 3);
+    else PAIR_CASE(false, 3);
+  } else if (mb == 5) {
+    if (c->pp) PAIR_CASE(true, 5);
+    else PAIR_CASE(false, 5);
   } else {
-    if (c->pp) CONTACT_CASE(true, 4);
-    else CONTACT_CASE(false, 4);
+    if (c->pp) PAIR_CASE(true, 4);
+    else PAIR_CASE(false, 4);
   }
-#undef CONTACT_CASE
-#define FOLD_CASE(PPV)                                                            \
+#undef PAIR_CASE
+#define FOLD_CASE(PPV, W)                                                         \
   do {                                                                            \
     if (epi == EPI_PREDICT)                                                       \
-      launch(c, "fold_fp64", k_fold_fp64<PPV, EPI_PREDICT, 4>, g, 128, A);        \
+      launch(c, "fold_fp64", k_fold_fp64<PPV, EPI_PREDICT, W>, g, 128, A);        \
     else if (epi == EPI_CORRECT)                                                  \
-      launch(c, "fold_fp64", k_fold_fp64<PPV, EPI_CORRECT, 4>, g, 128, A);        \
+      launch(c, "fold_fp64", k_fold_fp64<PPV, EPI_CORRECT, W>, g, 128, A);        \
     else                                                                          \
-      launch(c, "fold_fp64", k_fold_fp64<PPV, EPI_STORE, 4>, g, 128, A);          \
+      launch(c, "fold_fp64", k_fold_fp64<PPV, EPI_STORE, W>, g, 128, A);          \
   } while (0)
-  if (c->pp) FOLD_CASE(true);
-  else FOLD_CASE(false);
+  if (walls) {
+    if (c->pp) FOLD_CASE(true, true);
+    else FOLD_CASE(false, true);
+  } else {
+    if (c->pp) FOLD_CASE(true, false);
+    else FOLD_CASE(false, false);
+  }
 #undef FOLD_CASE
 }
 
@@ -814,10 +896,13 @@ int clear_abort(dem_ctx* c) {
   CK(cudaMemsetAsync(&d->ncol_pending, 0, sizeof(unsigned long long), c->stream));
   CK(cudaMemsetAsync(&d->pair_contacts, 0, 2 * sizeof(unsigned long long), c->stream));
   CK(cudaMemsetAsync(&d->overflow, 0, 4 * sizeof(int), c->stream));
-  CK(cudaMemsetAsync(&d->row_overflow, 0, 4 * sizeof(int), c->stream));  // .. in_overflow, need_in
-  // the stopped contact kernel may have counted "j" records
-  if (c->pass_cap > 0)
+  // row_overflow .. n_contacts
+  CK(cudaMemsetAsync(&d->row_overflow, 0, 7 * sizeof(int), c->stream));
+  // the stopped pair kernel may have counted "j" records and matched records
+  if (c->pass_cap > 0) {
     CK(cudaMemsetAsync(c->in_cnt, 0, sizeof(int) * (size_t)c->pass_cap, c->stream));
+    CK(cudaMemsetAsync(c->matched, 0, sizeof(unsigned) * (size_t)c->pass_cap, c->stream));
+  }
   return DEM_OK;
 }
 
@@ -858,6 +943,10 @@ int finish_pass(dem_ctx* c, int side, bool update, double dt, int epi, const Rin
     }
     if (h.in_overflow) {
       st = grow_incoming(c, std::max(h.need_in, c->in_cap + 1));
+      if (st) return st;
+    }
+    if (h.cl_overflow) {
+      st = grow_contacts(c, std::max(h.need_cl, c->cl_cap + 1));
       if (st) return st;
     }
     if (h.row_overflow) {
@@ -2319,6 +2408,10 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
     }
     if (c->hcnt->need_in + HEADROOM > c->in_cap) {
       st = grow_incoming(c, c->hcnt->need_in + HEADROOM);
+      if (st) return st;
+    }
+    if (c->hcnt->need_cl + c->hcnt->need_cl / 16 > c->cl_cap) {
+      st = grow_contacts(c, c->hcnt->need_cl + c->hcnt->need_cl / 8);
       if (st) return st;
     }
     // a graph starts from prepared Particle copies

@@ -233,246 +233,105 @@ __device__ __forceinline__ void rec_write(float4* a, float4* b, float* c, size_t
   c[i] = lo.z;
 }
 
-// The mixed-precision force pass: the FP64 kernels' structure (candidate
-// rows, exact FP64 overlap test, orientation, history semantics, each contact
-// evaluated once, summation order), FP32 contact arithmetic, FP64 integrator
-// epilogue.
+// The mixed-precision force pass: the FP64 pass's structure (the same test
+// kernel and contact list, exact FP64 overlap test, orientation, history
+// semantics, each contact evaluated once, summation order), FP32 contact
+// arithmetic, FP64 integrator epilogue.
 
-constexpr int KREG = 8;  // record keys of the owner kept in shared memory
+constexpr int KSPEC = 2;  // record keys read before the record count is known
 
-// Owner data handed to the lane that computes one of its contacts.
-struct OwnerMixed {
-  double x, y, z, R;
-  float vx, vy, vz, wx, wy, wz;
-  int p, cp, sys, pad;
-  unsigned long long key;
-};
-
-// MINB: resident blocks of 128 threads per SM the kernel is compiled for
-// (registers per thread <= 65536 / (128 * MINB)); the autotuner picks one.
-// CONE: cone walls compiled in (only with MINB = 3: the branch costs
-// registers, and systems without cone walls launch CONE = false kernels).
-template <bool PP, int MINB, bool CONE>
-__global__ void __launch_bounds__(128, MINB) k_contact_mixed(
-    PassArgs<float4, float2> A, MixedView V) {
-  // per warp: the current 32 contacts (candidate index, owner lane, partner),
-  // their "i" results FN, FT, FT remainder, VT, torque term (15 floats), the
-  // owners' first record keys, record counts and matched records
-  __shared__ int s_k[4][32], s_o[4][32], s_q[4][32];
-  __shared__ int s_hk[4][KREG][32], s_hc[4][32];
-  __shared__ unsigned s_match[4][32];
-  __shared__ float s_r[15][4][32];
-  __shared__ float s_w[NWM][128];  // |FN| of each wall contact
+// The pair kernel: one thread per contact, grid-stride over the list.
+template <bool PP, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_pair_mixed(PassArgs<float4, float2> A,
+                                                          MixedView V) {
   __shared__ int s_abort;
-  // one decision for the whole block (it meets a block barrier later)
   if (threadIdx.x == 0) s_abort = A.cnt->abort;
   __syncthreads();
   if (s_abort) return;
-  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int w = 0; w < A.nw_max; w++) s_w[w][threadIdx.x] = 0.f;
-  const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = p0 < A.n;
-  const int p = valid ? p0 : 0;
-  const DevParams& P = sys_params(A.P, A.sysid, p);  // this particle's system
-  const Box& B = P.box;
-  const int n = A.n;
-  unsigned n_col = 0, n_pc = 0, n_wc = 0;
-  int need = 0, need_in = 0;
-  bool in_over = false;
-
-  const int c = A.cell_cur[p];
-  const double4 p4 = A.X[p];
-  const double xp[3] = {p4.x, p4.y, p4.z};
-  const double Rpd = p4.w;
-  const float Rp = (float)Rpd;
-  const float4 pv4 = A.v4[p];
-  const float2 pw2 = A.w2[p];
-  const F3 vp = mk(pv4.x, pv4.y, pv4.z);
-  const F3 wp = mk(pv4.w, pw2.x, pw2.y);
-  const int cp = PP ? 0 : A.comp[p];
-  float inv_m, inv_i, eff_m;
-  MMat<PP>::self(P, cp, Rp, inv_m, inv_i, eff_m);
-  const int n1 = A.meta[p] & META_MASK;
-  const unsigned long long key_p = sweep_key(c, A.rank[p]);
-  const float half_dt = (float)A.half_dt;
+  const int total = A.cnt->n_contacts;
   const bool update = A.update != 0;
-  int hw_n = 0;
-  bool overflow = false;
+  const float half_dt = (float)A.half_dt;
   const History& Hr = A.Hr;
   const History& Hw = A.Hw;
-  const int hc = valid ? Hr.cnt[p] : 0;
-#pragma unroll
-  for (int r = 0; r < KREG; r++) s_hk[wid][r][lane] = r < hc ? Hr.key[hslot(Hr, p, r)] : -1;
-  s_hc[wid][lane] = hc;
-  s_match[wid][lane] = 0u;
-  __syncwarp();
-
-  F3 iF = mk(eff_m * (float)P.gravity[0], eff_m * (float)P.gravity[1],
-             eff_m * (float)P.gravity[2]);
-  F3 iT = mk(0.f, 0.f, 0.f);
-
-  auto record = [&](int partner, F3 ft, F3 lo, F3 vt) {
-    if (hw_n < Hw.cap) {
-      const size_t i = hslot(Hw, p, hw_n);
-      Hw.key[i] = partner;
-      rec_write(V.wa, V.wb, V.wc, i, ft, lo, vt);
-    } else {
-      overflow = true;
-    }
-    hw_n++;
-  };
-  // Rij = x_j - x_i (minimum image, FP64)
-  auto geometry = [&](const Box& Bx, const double xo[3], const double4& q4,
-                      double Rij[3]) -> double {
-    Rij[0] = q4.x - xo[0];
-    Rij[1] = q4.y - xo[1];
-    Rij[2] = q4.z - xo[2];
-#pragma unroll
-    for (int k = 0; k < 3; k++) Rij[k] = min_image_exact(Rij[k], Bx, k);
-    return sumsq3(Rij);
-  };
-  auto test = [&](int, int q, const double4& q4) -> bool {
-    double Rij[3];
-    const double DijSq = geometry(B, xp, q4, Rij);
-    const int cq = PP ? 0 : A.comp[q];
-    return MMat<PP>::min_dij_sq(P, cp, Rpd, cq, q4.w) - DijSq > 0.0;
-  };
-  auto compute = [&](const OwnerMixed& o, int oo, int k, int slot) {
-    const int q = __ldg(A.cand + (size_t)k * n + o.p);
+  unsigned n_col = 0;
+  int need = 0, need_in = 0;
+  bool overflow = false, in_over = false;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < total;
+       s += gridDim.x * blockDim.x) {
+    const int2 e = A.clist[s];
+    const int p = e.x, q = e.y;
     const int s_in = atomicAdd(&A.in_cnt[q], 1);  // q's "j" record (returns early)
-    const double4 q4 = A.X[q];
-    const float4 qv4 = A.v4[q];
-    const float2 qw2 = A.w2[q];
-    const double xo[3] = {o.x, o.y, o.z};
-    double Rij[3];
-    const DevParams& PO = A.P[o.sys];  // the owner's system (a warp may span two)
-    const double DijSq = geometry(PO.box, xo, q4, Rij);
-    const int cq = PP ? 0 : A.comp[q];
-    const double Delta = MMat<PP>::min_dij_sq(PO, o.cp, o.R, cq, q4.w) - DijSq;
-    const float Ra = (float)o.R, Rb = (float)q4.w;
+    const int ord = s - A.cstart[p];
+    const int hc = Hr.cnt[p];
+    int kspec[KSPEC];
+#pragma unroll
+    for (int r = 0; r < KSPEC; r++) kspec[r] = r < Hr.cap ? Hr.key[hslot(Hr, p, r)] : -1;
+    const DevParams& P = sys_params(A.P, A.sysid, p);
+    const double4 p4 = A.X[p], q4 = A.X[q];
+    const float4 pv4 = A.v4[p], qv4 = A.v4[q];
+    const float2 pw2 = A.w2[p], qw2 = A.w2[q];
+    const int cp = PP ? 0 : A.comp[p], cq = PP ? 0 : A.comp[q];
+    double Rij[3] = {q4.x - p4.x, q4.y - p4.y, q4.z - p4.z};
+#pragma unroll
+    for (int k = 0; k < 3; k++) Rij[k] = min_image_exact(Rij[k], P.box, k);
+    const double DijSq = sumsq3(Rij);
+    const double Delta = MMat<PP>::min_dij_sq(P, cp, p4.w, cq, q4.w) - DijSq;
+    const float Ra = (float)p4.w, Rb = (float)q4.w;
     MPair m;
-    MMat<PP>::pair(PO, o.cp, Ra, cq, Rb, m);
+    MMat<PP>::pair(P, cp, Ra, cq, Rb, m);
+    const F3 vo = mk(pv4.x, pv4.y, pv4.z), wo = mk(pv4.w, pw2.x, pw2.y);
     const F3 vq = mk(qv4.x, qv4.y, qv4.z), wq = mk(qv4.w, qw2.x, qw2.y);
-    const F3 vo = mk(o.vx, o.vy, o.vz), wo = mk(o.wx, o.wy, o.wz);
-    // the owner's records, then the partner's
-    F3 ft0 = mk(0.f, 0.f, 0.f), ft0lo = ft0, vt0 = ft0;
-    const int oc = s_hc[wid][oo];
+    // i's records, then j's
     int r = -1;
 #pragma unroll
-    for (int rr = 0; rr < KREG; rr++)
-      if (rr < oc && s_hk[wid][rr][oo] == q) r = rr;
-    for (int rr = KREG; r < 0 && rr < oc; rr++)
-      if (Hr.key[hslot(Hr, o.p, rr)] == q) r = rr;
+    for (int rr = 0; rr < KSPEC; rr++)
+      if (r < 0 && rr < hc && kspec[rr] == q) r = rr;
+    for (int rr = KSPEC; r < 0 && rr < hc; rr++)
+      if (Hr.key[hslot(Hr, p, rr)] == q) r = rr;
+    F3 ft0 = mk(0.f, 0.f, 0.f), ft0lo = ft0, vt0 = ft0;
     bool contacting = r >= 0;
     if (contacting) {
-      rec_read(V.ra, V.rb, V.rc, hslot(Hr, o.p, r), ft0, ft0lo, vt0);
-      if (r < 32) atomicOr(&s_match[wid][oo], 1u << r);
+      rec_read(V.ra, V.rb, V.rc, hslot(Hr, p, r), ft0, ft0lo, vt0);
+      if (r < 32) atomicOr(&A.matched[p], 1u << r);
     } else {
-      const int r2 = find_record(Hr, q, o.p);
+      const int r2 = find_record(Hr, q, p);
       contacting = r2 >= 0;
       if (contacting) rec_read(V.ra, V.rb, V.rc, hslot(Hr, q, r2), ft0, ft0lo, vt0);
     }
     if (!contacting) n_col++;
-    n_pc++;
     MOut out;
     mixed_pair(Rij, DijSq, Delta, m, Ra, vo, wo, Rb, vq, wq, half_dt, contacting, ft0, ft0lo,
                vt0, out);
-    // "j" side into q's incoming records
+    const F3 FTs = out.FT + out.FTlo;
+    // "j" half into q's incoming records
     if (s_in < A.in_cap) {
-      const F3 FTs = out.FT + out.FTlo;
+      const unsigned long long key = sweep_key(A.cell_cur[p], A.rank[p]);
       InRec32* rec = (InRec32*)A.in_rec + (size_t)s_in * A.in_stride + q;
-      rec->a = make_float4(__uint_as_float((unsigned)o.key),
-                           __uint_as_float((unsigned)(o.key >> 32)), out.FN.x, out.FN.y);
+      rec->a = make_float4(__uint_as_float((unsigned)key), __uint_as_float((unsigned)(key >> 32)),
+                           out.FN.x, out.FN.y);
       rec->b = make_float4(out.FN.z, FTs.x, FTs.y, FTs.z);
       rec->c = make_float4(out.NxFT.x, out.NxFT.y, out.NxFT.z, 0.f);
     } else {
       in_over = true;
     }
     need_in = need_in > s_in + 1 ? need_in : s_in + 1;
-    // "i" side to the owner
+    // "i" half at the contact's place
     const F3 tq = cross(Ra * out.N, out.FT);
-    const float vals[15] = {out.FN.x, out.FN.y, out.FN.z, out.FT.x, out.FT.y, out.FT.z,
-                            out.FTlo.x, out.FTlo.y, out.FTlo.z, out.VT.x, out.VT.y, out.VT.z,
-                            tq.x, tq.y, tq.z};
-#pragma unroll
-    for (int i = 0; i < 15; i++) s_r[i][wid][slot] = vals[i];
-    s_q[wid][slot] = q;
-  };
-  auto accum = [&](int slot, int) {
-    float v[15];
-#pragma unroll
-    for (int i = 0; i < 15; i++) v[i] = s_r[i][wid][slot];
-    const F3 FN = mk(v[0], v[1], v[2]), FT = mk(v[3], v[4], v[5]), FTlo = mk(v[6], v[7], v[8]);
-    const F3 VT = mk(v[9], v[10], v[11]), tq = mk(v[12], v[13], v[14]);
-    iF = iF + FN + (FT + FTlo);
-    iT = iT + tq;
-    if (update) record(s_q[wid][slot], FT, FTlo, VT);
-  };
-  const OwnerMixed me{xp[0], xp[1], xp[2], Rpd, vp.x, vp.y, vp.z, wp.x, wp.y, wp.z, p, cp,
-                      A.sysid ? A.sysid[p] : 0, 0, key_p};
-  contact_loop(A.cand, A.X, n, p, valid, n1, me, s_k[wid], s_o[wid], test, compute, accum);
-
-  if (valid) {
-    for (int w = 0; w < P.nw; w++) {
-      const dem_wall& W = P.walls[w];
-      const size_t wi = (size_t)p * P.nw + w;
-      const bool contacting = Hr.wflag[wi] != 0;
-      F3 ft0 = mk(0.f, 0.f, 0.f), ft0lo = ft0, vt0 = ft0;
-      if (contacting) rec_read(V.rwa, V.rwb, V.rwc, wi, ft0, ft0lo, vt0);
-      double Dij, Nij[3], Qji[3];
-      const bool ov = overlap_wall<CONE>(P, W, xp, Rpd, Dij, Nij, Qji);
-      if (ov) {
-        n_wc++;
-        const double Delta = Rpd * Rpd - Dij * Dij;
-        const float delta = (float)(Rpd - Dij);
-        F3 N = mk((float)Nij[0], (float)Nij[1], (float)Nij[2]);
-        F3 Q = mk((float)Qji[0], (float)Qji[1], (float)Qji[2]);
-        F3 wv = mk((float)W.velocity[0], (float)W.velocity[1], (float)W.velocity[2]);
-        F3 ww = mk((float)W.omega[0], (float)W.omega[1], (float)W.omega[2]);
-        F3 Vij = (wv + cross(ww, Q)) - vp;
-        F3 VijC = Vij - cross(Rp * wp, N);
-        F3 Rw = mk((float)(W.position[0] + Qji[0] - xp[0]), (float)(W.position[1] + Qji[1] - xp[1]),
-                   (float)(W.position[2] + Qji[2] - xp[2]));
-        MPair m;
-        MMat<PP>::wall(P, cp, Rp, w, m);
-        MOut o;
-        common_mixed(Rw, N, (-delta) * N, Vij, VijC, (float)Delta, half_dt, contacting, ft0,
-                     ft0lo, vt0, m, o);
-        iF = iF + o.FN + (o.FT + o.FTlo);
-        iT = iT + cross(Rp * o.N, o.FT);
-        s_w[w][threadIdx.x] = sqrtf(dot(o.FN, o.FN));
-        if (update) {
-          Hw.wflag[wi] = 1;
-          rec_write(V.wwa, V.wwb, V.wwc, wi, o.FT, o.FTlo, o.VT);
-        }
-      } else if (update) {
-        Hw.wflag[wi] = 0;
-      }
-    }
-    if (A.drag)  // iForce = iForce + DragForce(iPart) (src/MForces.f90:316)
-      iF = iF + mk((float)A.drag[(size_t)3 * p], (float)A.drag[(size_t)3 * p + 1],
-                   (float)A.drag[(size_t)3 * p + 2]);
-    Own32* ow = (Own32*)A.own + p;
-    ow->a = make_float2(iF.x, iF.y);
-    ow->b = make_float2(iF.z, iT.x);
-    ow->c = make_float2(iT.y, iT.z);
+    IRec32* ir = (IRec32*)A.irec + s;
+    ir->a = make_float4(out.FN.x, out.FN.y, out.FN.z, FTs.x);
+    ir->b = make_float4(FTs.y, FTs.z, tq.x, tq.y);
+    ir->c = make_float4(tq.z, 0.f, 0.f, 0.f);
     if (update) {
-      const unsigned matched = s_match[wid][lane];
-      for (int r = 0; r < hc; r++) {
-        if (r < 32 && ((matched >> r) & 1u)) continue;
-        const size_t i = hslot(Hr, p, r);
-        const int q2 = Hr.key[i];
-        if (q2 >= A.n || !cells_adjacent(P, c, A.cell_cur[q2])) {
-          F3 ft, lo, vt;
-          rec_read(V.ra, V.rb, V.rc, i, ft, lo, vt);
-          record(q2, ft, lo, vt);
-        }
+      if (ord < Hw.cap) {
+        const size_t i = hslot(Hw, p, ord);
+        Hw.key[i] = q;
+        rec_write(V.wa, V.wb, V.wc, i, out.FT, out.FTlo, out.VT);
+      } else {
+        overflow = true;
       }
-      Hw.cnt[p] = hw_n < Hw.cap ? hw_n : Hw.cap;
-      need = hw_n;
+      need = need > ord + 1 ? need : ord + 1;
     }
   }
-  if (A.nw_max > 0) wall_partials(s_w, A.nw_max, A.wall_part);
   if (overflow) {
     atomicExch(&A.cnt->overflow, 1);
     set_abort(A.cnt, A.tag);
@@ -481,29 +340,42 @@ __global__ void __launch_bounds__(128, MINB) k_contact_mixed(
     atomicExch(&A.cnt->in_overflow, 1);
     set_abort(A.cnt, A.tag);
   }
-  publish_counts_block(A.cnt, A.update != 0, n_col, n_pc, n_wc, (unsigned)need,
-                       (unsigned)need_in);
+  publish_counts_block(A.cnt, update, n_col, 0u, 0u, (unsigned)need, (unsigned)need_in);
 }
 
-// The fold kernel: Force and Torque in sweep order (FP32), a = F/m,
-// alpha = T/I, then the FP64 integrator epilogue.
-template <bool PP, int EPI>
-__global__ void __launch_bounds__(128, 4) k_fold_mixed(PassArgs<float4, float2> A) {
+// The fold kernel: p's block of the sweep, Force and Torque in sweep order
+// (FP32), a = F/m, alpha = T/I, then the FP64 integrator epilogue.  WALLS:
+// some system has walls; CONE: some wall is a cone.
+template <bool PP, int EPI, bool WALLS, bool CONE>
+__global__ void __launch_bounds__(128, 4) k_fold_mixed(PassArgs<float4, float2> A, MixedView V) {
+  __shared__ float s_w[WALLS ? NWM : 1][128];  // |FN| of each wall contact
   __shared__ int s_abort;
-  // one decision for the whole block (it meets a block barrier at the end)
+  // one decision for the whole block (it meets block barriers later)
   if (threadIdx.x == 0) s_abort = A.cnt->abort;
   __syncthreads();
   if (s_abort) return;
+  if (WALLS)
+    for (int w = 0; w < A.nw_max; w++) s_w[w][threadIdx.x] = 0.f;
   const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = p0 < A.n;
   const int p = valid ? p0 : 0;
+  const bool update = A.update != 0;
+  const History& Hr = A.Hr;
+  const History& Hw = A.Hw;
+  unsigned n_wc = 0;
+  int need = 0;
+  bool overflow = false;
   double d2 = 0.0;
   if (valid) {
     const DevParams& P = sys_params(A.P, A.sysid, p);
     const int c = A.cell_cur[p];
     const unsigned long long key_p = sweep_key(c, A.rank[p]);
     const int ni = A.in_cnt[p];
-    A.in_cnt[p] = 0;  // for the next pass's contact kernel
+    if (ni) A.in_cnt[p] = 0;  // for the next pass's pair kernel
+    const unsigned matched = A.matched[p];
+    if (matched) A.matched[p] = 0u;
+    const int nc = A.ccount[p];
+    const int st0 = A.cstart[p];
     const double4 p4 = A.X[p];
     const double xp[3] = {p4.x, p4.y, p4.z};
     const double Rpd = p4.w;
@@ -511,7 +383,88 @@ __global__ void __launch_bounds__(128, 4) k_fold_mixed(PassArgs<float4, float2> 
     const int cp = PP ? 0 : A.comp[p];
     float inv_m, inv_i, eff_m;
     MMat<PP>::self(P, cp, Rp, inv_m, inv_i, eff_m);
-    const Own32 ow = ((const Own32*)A.own)[p];
+    // ---- p's block: gravity, its contacts as "i" in row order
+    F3 iF = mk(eff_m * (float)P.gravity[0], eff_m * (float)P.gravity[1],
+               eff_m * (float)P.gravity[2]);
+    F3 iT = mk(0.f, 0.f, 0.f);
+    const IRec32* ir = (const IRec32*)A.irec + st0;
+    for (int k = 0; k < nc; k++) {
+      const IRec32 r = ir[k];
+      iF = iF + mk(r.a.x, r.a.y, r.a.z) + mk(r.a.w, r.b.x, r.b.y);
+      iT = iT + mk(r.b.z, r.b.w, r.c.x);
+    }
+    int hw_n = nc;  // the pair kernel wrote the records of the contacts
+    if (WALLS) {
+      const float4 pv4 = A.v4[p];
+      const float2 pw2 = A.w2[p];
+      const F3 vp = mk(pv4.x, pv4.y, pv4.z);
+      const F3 wp = mk(pv4.w, pw2.x, pw2.y);
+      const float half_dt = (float)A.half_dt;
+      for (int w = 0; w < P.nw; w++) {
+        const dem_wall& W = P.walls[w];
+        const size_t wi = (size_t)p * P.nw + w;
+        const bool contacting = Hr.wflag[wi] != 0;
+        F3 ft0 = mk(0.f, 0.f, 0.f), ft0lo = ft0, vt0 = ft0;
+        if (contacting) rec_read(V.rwa, V.rwb, V.rwc, wi, ft0, ft0lo, vt0);
+        double Dij, Nij[3], Qji[3];
+        const bool ov = overlap_wall<CONE>(P, W, xp, Rpd, Dij, Nij, Qji);
+        if (ov) {
+          n_wc++;
+          const double Delta = Rpd * Rpd - Dij * Dij;
+          const float delta = (float)(Rpd - Dij);
+          F3 N = mk((float)Nij[0], (float)Nij[1], (float)Nij[2]);
+          F3 Q = mk((float)Qji[0], (float)Qji[1], (float)Qji[2]);
+          F3 wv = mk((float)W.velocity[0], (float)W.velocity[1], (float)W.velocity[2]);
+          F3 ww = mk((float)W.omega[0], (float)W.omega[1], (float)W.omega[2]);
+          F3 Vij = (wv + cross(ww, Q)) - vp;
+          F3 VijC = Vij - cross(Rp * wp, N);
+          F3 Rw = mk((float)(W.position[0] + Qji[0] - xp[0]),
+                     (float)(W.position[1] + Qji[1] - xp[1]),
+                     (float)(W.position[2] + Qji[2] - xp[2]));
+          MPair m;
+          MMat<PP>::wall(P, cp, Rp, w, m);
+          MOut o;
+          common_mixed(Rw, N, (-delta) * N, Vij, VijC, (float)Delta, half_dt, contacting, ft0,
+                       ft0lo, vt0, m, o);
+          iF = iF + o.FN + (o.FT + o.FTlo);
+          iT = iT + cross(Rp * o.N, o.FT);
+          s_w[w][threadIdx.x] = sqrtf(dot(o.FN, o.FN));
+          if (update) {
+            Hw.wflag[wi] = 1;
+            rec_write(V.wwa, V.wwb, V.wwc, wi, o.FT, o.FTlo, o.VT);
+          }
+        } else if (update) {
+          Hw.wflag[wi] = 0;
+        }
+      }
+    }
+    if (A.drag)  // iForce = iForce + DragForce(iPart) (src/MForces.f90:316)
+      iF = iF + mk((float)A.drag[(size_t)3 * p], (float)A.drag[(size_t)3 * p + 1],
+                   (float)A.drag[(size_t)3 * p + 2]);
+    if (update) {
+      const int hc = Hr.cnt[p];
+      for (int r = 0; r < hc; r++) {
+        if (r < 32 && ((matched >> r) & 1u)) continue;
+        const size_t i = hslot(Hr, p, r);
+        const int q2 = Hr.key[i];
+        if (q2 >= A.n || !cells_adjacent(P, c, A.cell_cur[q2])) {
+          if (hw_n < Hw.cap) {
+            F3 ft, lo, vt;
+            rec_read(V.ra, V.rb, V.rc, i, ft, lo, vt);
+            const size_t o = hslot(Hw, p, hw_n);
+            Hw.key[o] = q2;
+            rec_write(V.wa, V.wb, V.wc, o, ft, lo, vt);
+          } else {
+            overflow = true;
+          }
+          hw_n++;
+        }
+      }
+      Hw.cnt[p] = hw_n < Hw.cap ? hw_n : Hw.cap;
+      if (hw_n > Hw.cap) overflow = true;
+      need = hw_n;
+    }
+    // ---- Force and Torque in sweep order
     const InRec32* in = (const InRec32*)A.in_rec + p;
     const size_t st = (size_t)A.in_stride;
     F3 F = mk(0.f, 0.f, 0.f), T = mk(0.f, 0.f, 0.f);
@@ -523,8 +476,8 @@ __global__ void __launch_bounds__(128, 4) k_fold_mixed(PassArgs<float4, float2> 
                  ((unsigned long long)__float_as_uint(k.y) << 32);
         },
         [&]() {
-          F = F + mk(ow.a.x, ow.a.y, ow.b.x);
-          T = T + mk(ow.b.y, ow.c.x, ow.c.y);
+          F = F + iF;
+          T = T + iT;
         },
         [&](int e) {
           const InRec32 r = in[e * st];
@@ -551,6 +504,12 @@ __global__ void __launch_bounds__(128, 4) k_fold_mixed(PassArgs<float4, float2> 
     }
     epilogue<EPI>(A, P, p, xp, Rpd, vd, wd, acc, alp, c, d2);
   }
+  if (WALLS && A.nw_max > 0) wall_partials(s_w, A.nw_max, A.wall_part);
+  if (overflow) {
+    atomicExch(&A.cnt->overflow, 1);
+    set_abort(A.cnt, A.tag);
+  }
+  publish_counts_block(A.cnt, update, 0u, 0u, n_wc, (unsigned)need, 0u);
   if (EPI != EPI_STORE) publish_disp_block(A.cnt, d2);
 }
 
@@ -705,8 +664,9 @@ bool mixed_grow_walls(MixedBuffers& M, int n, int stride, int cur, cudaStream_t 
   return true;
 }
 
-void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant, bool cone,
-                const PassArgs<float4, float2>& A, int cur, cudaStream_t st, int part) {
+void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant, bool walls, bool cone,
+                const PassArgs<float4, float2>& A, int cur, cudaStream_t st, int part,
+                unsigned pair_blocks) {
   if (A.n == 0) return;
   MixedView V;
   V.ra = M.ha[cur];
@@ -721,33 +681,38 @@ void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant, bool cone,
   V.wwa = M.wa[cur ^ 1];
   V.wwb = M.wb[cur ^ 1];
   V.wwc = M.wc[cur ^ 1];
-  const unsigned g = blocks(A.n, 128);
   if (part == 0) {
-#define MCASE(PPV, MB, CN) k_contact_mixed<PPV, MB, CN><<<g, 128, 0, st>>>(A, V)
-    if (cone) {
-      if (pp) MCASE(true, 3, true);
-      else MCASE(false, 3, true);
-    } else if (variant == 1) {
-      if (pp) MCASE(true, 3, false);
-      else MCASE(false, 3, false);
+#define PCASE(PPV, MB) k_pair_mixed<PPV, MB><<<pair_blocks, 128, 0, st>>>(A, V)
+    if (variant == 1) {
+      if (pp) PCASE(true, 3);
+      else PCASE(false, 3);
     } else if (variant == 2) {
-      if (pp) MCASE(true, 5, false);
-      else MCASE(false, 5, false);
+      if (pp) PCASE(true, 5);
+      else PCASE(false, 5);
     } else {
-      if (pp) MCASE(true, 4, false);
-      else MCASE(false, 4, false);
+      if (pp) PCASE(true, 4);
+      else PCASE(false, 4);
     }
-#undef MCASE
+#undef PCASE
     return;
   }
-#define FCASE(PPV)                                                                      \
-  do {                                                                                  \
-    if (epi == EPI_PREDICT) k_fold_mixed<PPV, EPI_PREDICT><<<g, 128, 0, st>>>(A);      \
-    else if (epi == EPI_CORRECT) k_fold_mixed<PPV, EPI_CORRECT><<<g, 128, 0, st>>>(A); \
-    else k_fold_mixed<PPV, EPI_STORE><<<g, 128, 0, st>>>(A);                            \
+  const unsigned g = blocks(A.n, 128);
+#define FCASE(PPV, W, CN)                                                                     \
+  do {                                                                                        \
+    if (epi == EPI_PREDICT) k_fold_mixed<PPV, EPI_PREDICT, W, CN><<<g, 128, 0, st>>>(A, V);  \
+    else if (epi == EPI_CORRECT) k_fold_mixed<PPV, EPI_CORRECT, W, CN><<<g, 128, 0, st>>>(A, V); \
+    else k_fold_mixed<PPV, EPI_STORE, W, CN><<<g, 128, 0, st>>>(A, V);                        \
   } while (0)
-  if (pp) FCASE(true);
-  else FCASE(false);
+  if (!walls) {
+    if (pp) FCASE(true, false, false);
+    else FCASE(false, false, false);
+  } else if (cone) {
+    if (pp) FCASE(true, true, true);
+    else FCASE(false, true, true);
+  } else {
+    if (pp) FCASE(true, true, false);
+    else FCASE(false, true, false);
+  }
 #undef FCASE
 }
 

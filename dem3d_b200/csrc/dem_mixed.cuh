@@ -30,12 +30,14 @@ bool mixed_regrow(MixedBuffers& M, int n, int stride, int newcap, int cur, const
 // the wall records of the first n particles into arrays for `stride` rows
 bool mixed_grow_walls(MixedBuffers& M, int n, int stride, int cur, cudaStream_t st);
 // One kernel of a force pass (FP32 contact arithmetic) on the context's
-// stream: part 0 = the contact kernel, 1 = the fold kernel with epilogue
-// `epi`.  variant: the contact kernel compiled for 4 (0), 3 (1) or 5 (2)
-// resident blocks per SM; cone: some wall is a cone (then the 3-block
-// contact kernel with the cone branch runs)
-void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant, bool cone,
-                const PassArgs<float4, float2>& A, int cur, cudaStream_t st, int part);
+// stream: part 0 = the pair kernel (pair_blocks blocks of 128 threads over
+// the contact list; variant: compiled for 4 (0), 3 (1) or 5 (2) resident
+// blocks per SM), 1 = the fold kernel with epilogue `epi` (walls: some
+// system has walls; cone: some wall is a cone).  The test kernel that builds
+// the contact list is shared with the FP64 path.
+void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant, bool walls, bool cone,
+                const PassArgs<float4, float2>& A, int cur, cudaStream_t st, int part,
+                unsigned pair_blocks);
 void mixed_import_history(MixedBuffers& M, const History& H, int n, int nw, int cur,
                           cudaStream_t st);
 void mixed_export_history(MixedBuffers& M, const History& H, int n, int nw, int cur,

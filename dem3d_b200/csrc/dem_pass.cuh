@@ -1,14 +1,16 @@
 // dem_pass.cuh -- device helpers shared by the FP64 and the mixed force
-// passes: the contact loop, the ordered fold, the AB/AM epilogues and the
+// passes: the per-block counters, the ordered fold, the AB/AM epilogues and the
 // cell transition (RedistributeParticles3D's bookkeeping) for the next pass.
 //
-// A force pass is two kernels, each one thread per particle in original
-// index order.  The contact kernel reads the particle's candidate row (the
-// partners it meets as "i"), applies the reference's overlap test, evaluates
-// every contact once and hands the "j" half of each contact to the partner.
-// The fold kernel adds the particle's received halves and its own block in
-// the sweep's order and finishes with the integrator step of the pass (AB
-// predictor or AM corrector).  Its epilogue also hashes the particle's next
+// A force pass is three kernels.  The test kernel (one thread per particle,
+// in original index order) applies the reference's overlap test to the
+// particle's candidate row (the partners it meets as "i") and lists its
+// contacts; the pair kernel evaluates every listed contact once and hands its
+// "i" half to the contact's place in the list and its "j" half to the
+// partner; the fold kernel (one thread per particle) builds the particle's
+// block of the sweep, adds the received halves and the block in the sweep's
+// order and finishes with the integrator step of the pass (AB predictor or
+// AM corrector).  Its epilogue also hashes the particle's next
 // position into its cell and, when the cell changes, records the move for
 // the next relink: the arrival list of the new cell and the dirty list of
 // both cells.  Every such side effect is idempotent, so a pass that was
@@ -134,91 +136,6 @@ __device__ __forceinline__ int find_record(const History& H, int lo, int hi) {
   for (int r = 0; r < c; r++)
     if (H.key[hslot(H, lo, r)] == hi) return r;
   return -1;
-}
-
-// Broadcast a small trivially copyable object from lane `src`.
-template <class T>
-__device__ __forceinline__ T shfl_obj(const T& v, int src) {
-  static_assert(sizeof(T) % 4 == 0, "shuffle in 4-byte words");
-  constexpr int W = (int)(sizeof(T) / 4);
-  unsigned w[W];
-  memcpy(w, &v, sizeof(T));
-#pragma unroll
-  for (int i = 0; i < W; i++) w[i] = __shfl_sync(0xffffffffu, w[i], src);
-  T r;
-  memcpy(&r, w, sizeof(T));
-  return r;
-}
-
-// The contacts of the warp's particles, each particle as "i" of its row, in
-// three steps per window of 64 candidates:
-//  1. every lane tests its own candidates (test(k, q, xq), four prefetched at
-//     a time) into a bit mask;
-//  2. the warp's contacts are laid out owner by owner in row order (prefix
-//     sum) and computed 32 at a time, one per lane: compute(owner, lane of the
-//     owner, k, slot) gets the owning particle's data by shuffle and leaves
-//     the owner's results in shared-memory slot `slot`;
-//  3. every owner folds its own results in row order, accum(slot, k): the
-//     order of the reference's loop over jj (src/MForces.f90:199-272).
-// s_k / s_o: 32 ints of shared memory per warp.  All 32 lanes must call
-// this; `valid` is false for lanes without a particle.
-template <class Owner, class Test, class Compute, class Accum>
-__device__ __forceinline__ void contact_loop(const int* __restrict__ cand,
-                                             const double4* __restrict__ X, int n, int p,
-                                             bool valid, int m, const Owner& me, int* s_k,
-                                             int* s_o, Test&& test, Compute&& compute,
-                                             Accum&& accum) {
-  const unsigned FULL = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  if (!valid) m = 0;
-  const int mmax = (int)__reduce_max_sync(FULL, (unsigned)m);
-  for (int base = 0; base < mmax; base += 64) {
-    unsigned long long mask = 0ull;
-    const int end = m < base + 64 ? m : base + 64;
-#pragma unroll 1
-    for (int b = base; b < end; b += 4) {
-      int q[4];
-#pragma unroll
-      for (int u = 0; u < 4; u++) q[u] = b + u < end ? __ldg(cand + (size_t)(b + u) * n + p) : -1;
-      double4 xq[4];
-#pragma unroll
-      for (int u = 0; u < 4; u++)
-        xq[u] = q[u] >= 0 ? X[q[u]] : make_double4(0.0, 0.0, 0.0, 0.0);
-#pragma unroll
-      for (int u = 0; u < 4; u++)
-        if (q[u] >= 0 && test(b + u, q[u], xq[u])) mask |= 1ull << (b + u - base);
-    }
-    const int cnt = __popcll(mask);
-    int incl = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(FULL, incl, o);
-      if (lane >= o) incl += y;
-    }
-    const int start = incl - cnt;
-    const int total = __shfl_sync(FULL, incl, 31);
-    unsigned long long rem = mask;
-    int e_pub = start;
-    for (int t0 = 0; t0 < total; t0 += 32) {
-      while (rem && e_pub < t0 + 32) {
-        s_k[e_pub - t0] = base + __ffsll((long long)rem) - 1;
-        s_o[e_pub - t0] = lane;
-        rem &= rem - 1ull;
-        e_pub++;
-      }
-      __syncwarp();
-      const bool has = t0 + lane < total;
-      const int kk = has ? s_k[lane] : 0;
-      const int oo = has ? s_o[lane] : lane;
-      const Owner ow = shfl_obj(me, oo);
-      if (has) compute(ow, oo, kk, lane);
-      __syncwarp();
-      const int e0 = start > t0 ? start : t0;
-      const int e1 = start + cnt < t0 + 32 ? start + cnt : t0 + 32;
-      for (int e = e0; e < e1; e++) accum(e - t0, s_k[e - t0]);
-      __syncwarp();
-    }
-  }
 }
 
 // The "j" results a particle received in this pass, in the order of the
