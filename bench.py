@@ -120,45 +120,51 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def contact_bytes_per_particle(mixed, update, z_pp, m_cand, z_pw=0.0, nw=0):
-    """Algorithmic DRAM bytes of one contact-kernel launch per particle (the
-    particle as "i" of its row): every input and output once; partner data
-    is other particles' own data (re-read from L1/L2) and adds nothing.
-      reads: position+R 32, velocities 24 (FP32) / 48 (FP64), row length 4,
-        rank 4, cell 4, record count 4, candidate row 4*m_cand (the row holds
-        the "i" partners only), the pair records (key 4 + 36 B FP32 / 48 B
-        FP64) once per pair (0.5*z_pp per particle), wall flags and records;
-      writes: the "i" block 24 (FP32) / 48 (FP64), one "j" record per pair
-        (48 B FP32 / 80 B FP64) and its count 4, and in the history-updating
-        pass the new tables (count 4, records, wall records)."""
-    vel = 24 if mixed else 48
+def test_bytes_per_particle(z_pp, m_cand):
+    """Algorithmic DRAM bytes of one test-kernel launch per particle: position
+    + R 32, row length 4, candidate row 4*m_cand (the "i" partners only) read;
+    the particle's place in the contact list 8 and one list entry (8 B) per
+    contact it evaluates (0.5*z_pp) written.  Partner positions are other
+    particles' own data (L1/L2) and add nothing."""
+    return 32 + 4 + 4 * m_cand + 8 + 0.5 * z_pp * 8
+
+
+def pair_bytes_per_particle(mixed, update, z_pp):
+    """Algorithmic DRAM bytes of one pair-kernel launch per particle (0.5*z_pp
+    contacts): per contact its list entry 8 and i's place 4 read, the pair's
+    history record (key 4 + 36 B FP32 / 48 B FP64) read, the "i" half
+    (48 / 80 B) and the "j" half (48 / 80 B + its count 4) written, and in
+    the history-updating pass the new record written.  The two particles'
+    positions and velocities are their own data (L1/L2)."""
     rec = 4 + (36 if mixed else 48)
-    jrec = (48 if mixed else 80) + 4
-    own = 32 + vel + 4 + 4 + 4 + 4 + 4 * m_cand
-    hist = 0.5 * z_pp * rec + nw * 4 + z_pw * (rec - 4)
-    out = (24 if mixed else 48) + 0.5 * z_pp * jrec
-    if update:
-        hist += 4 + 0.5 * z_pp * rec + nw * 4 + z_pw * (rec - 4)
-    return own + hist + out
+    half = 48 if mixed else 80
+    per = 8 + 4 + rec + half + half + 4 + (rec if update else 0)
+    return 0.5 * z_pp * per
 
 
-def fold_bytes_per_particle(mixed, epi, z_pp, nprev=3):
+def fold_bytes_per_particle(mixed, epi, z_pp, z_pw=0.0, nw=0, nprev=3):
     """Algorithmic DRAM bytes of one fold-kernel launch per particle:
-      reads: cell 4, rank 4, "j" count 4 (reset: written 4), the "i" block
-        24 / 48, the "j" records (0.5*z_pp per particle, 48 / 80 B), position
-        + R 32 (and the FP64 velocity copies 48 in FP64 mode);
-      epi "predict" (pass 1, src/MDEM.f90:296-331): ring nprev*72 read,
-        Particle v,w 48 read (mixed), a,alpha 48 + Predicted x,v,w 72 + ring
-        slot 72 + the corrector's ring sums 72 + next-pass copies (32 +
+      reads: cell 4, rank 4, "j" count 4 (reset), matched bits 4, place in
+        the contact list 8, position + R 32 (and the FP64 velocity copies 48
+        in FP64 mode, the FP32 ones 24 with walls), the "i" halves and the
+        "j" halves of its contacts (0.5*z_pp each, 48 / 80 B), wall flags and
+        records;
+      epi "predict" (pass 1, src/MDEM.f90:296-331, history-updating): the
+        record count 4 read and written, new wall records; ring nprev*72
+        read, Particle v,w 48 read (mixed), a,alpha 48 + Predicted x,v,w 72 +
+        ring slot 72 + the corrector's ring sums 72 + next-pass copies (32 +
         velocities) + cell 4 written;
       epi "correct" (pass 2, :340-367): the ring sums 72, Predicted v 24
         (mixed) read, Particle x,v,w 72 read and written, Predicted a,alpha
         48 + next-pass copies + cell 4 written."""
     vel = 24 if mixed else 48
-    base = 4 + 4 + 8 + (24 if mixed else 48) + 0.5 * z_pp * (48 if mixed else 80) + 32 + (
-        0 if mixed else 48)
+    half = 48 if mixed else 80
+    wrec = 4 + (36 if mixed else 48)
+    base = (4 + 4 + 4 + 4 + 8 + 32 + (0 if mixed else 48) + (24 if mixed and nw else 0)
+            + z_pp * half + nw * 4 + z_pw * (wrec - 4))
     sums = 72 if nprev else 0
     if epi == "predict":
+        base += 8 + nw * 4 + z_pw * (wrec - 4)
         epil = (nprev * 72 + (48 if mixed else 0) + 48 + 72 + (72 if nprev else 0) + sums + 32
                 + vel + 4)
     else:
@@ -167,14 +173,15 @@ def fold_bytes_per_particle(mixed, epi, z_pp, nprev=3):
 
 
 def step_bytes_per_particle(mixed, z_pp, m_cand, z_pw=0.0, nw=0, nprev=3):
-    """Bytes of one particle-update (MoveParticles: two passes of a contact
-    and a fold kernel) under the kernels' own model; the relink and
+    """Bytes of one particle-update (MoveParticles: two passes of a test, a
+    pair and a fold kernel) under the kernels' own model; the relink and
     candidate-row kernels touch only the few particles near cells that
     changed and are not counted."""
-    return (contact_bytes_per_particle(mixed, True, z_pp, m_cand, z_pw, nw) +
-            contact_bytes_per_particle(mixed, False, z_pp, m_cand, z_pw, nw) +
-            fold_bytes_per_particle(mixed, "predict", z_pp, nprev) +
-            fold_bytes_per_particle(mixed, "correct", z_pp, nprev))
+    return (2 * test_bytes_per_particle(z_pp, m_cand) +
+            pair_bytes_per_particle(mixed, True, z_pp) +
+            pair_bytes_per_particle(mixed, False, z_pp) +
+            fold_bytes_per_particle(mixed, "predict", z_pp, z_pw, nw, nprev) +
+            fold_bytes_per_particle(mixed, "correct", z_pp, z_pw, nw, nprev))
 
 
 def survey_bytes_per_particle(mixed, z_pp, z_pw=0.0):
@@ -412,12 +419,14 @@ def traffic_per_particle():
 def kernel_bytes(name, n, mixed, z_pp, m_cand, z_pw, nw):
     """Algorithmic bytes of one launch of a force-pass kernel (mean of the
     two passes of a step)."""
-    if name.startswith("contact"):
-        return n * 0.5 * (contact_bytes_per_particle(mixed, True, z_pp, m_cand, z_pw, nw) +
-                          contact_bytes_per_particle(mixed, False, z_pp, m_cand, z_pw, nw))
+    if name.startswith("test"):
+        return n * test_bytes_per_particle(z_pp, m_cand)
+    if name.startswith("pair"):
+        return n * 0.5 * (pair_bytes_per_particle(mixed, True, z_pp) +
+                          pair_bytes_per_particle(mixed, False, z_pp))
     if name.startswith("fold"):
-        return n * 0.5 * (fold_bytes_per_particle(mixed, "predict", z_pp) +
-                          fold_bytes_per_particle(mixed, "correct", z_pp))
+        return n * 0.5 * (fold_bytes_per_particle(mixed, "predict", z_pp, z_pw, nw) +
+                          fold_bytes_per_particle(mixed, "correct", z_pp, z_pw, nw))
     return None
 
 
@@ -617,6 +626,15 @@ def run_ours(args):
         # case of the same workload, scaled to this launch by the particles
         traffic = tr["bytes_per_particle"][dom] * n
         traffic_src = tr.get("state", "profiles/pass_traffic.json")
+    # every force-pass kernel against its own byte model
+    per_kernel = {}
+    for k, v in stats.items():
+        kb = kernel_bytes(k, n, mixed, z_pp, m_cand, z_pw, nw)
+        if kb and v[0]:
+            kms = v[1] / v[0]
+            per_kernel[k] = {"bytes_per_launch": kb, "avg_launch_ms": kms,
+                             "achieved_gbs": kb / (kms / 1000.0) / 1e9,
+                             "frac": kb / (kms / 1000.0) / 1e9 / peak}
     step_b = step_bytes_per_particle(mixed, z_pp, m_cand, z_pw, nw)
     step_ms = ms / res[headline]["steps"]
     step_gbs = step_b * n / (step_ms / 1000.0) / 1e9
@@ -624,7 +642,7 @@ def run_ours(args):
     # whole step (every kernel of it) and over the force-pass kernels alone
     surv_b = survey_bytes_per_particle(mixed, z_pp, z_pw)
     pass_ms = sum(v[1] for k, v in stats.items()
-                  if k.startswith(("contact", "fold"))) / nprof
+                  if k.startswith(("test", "pair", "fold"))) / nprof
     surv_step = surv_b * n / (step_ms / 1000.0) / 1e9
     surv_pass = surv_b * n / (pass_ms / 1000.0) / 1e9 if pass_ms > 0 else None
 
@@ -692,6 +710,7 @@ def run_ours(args):
                          "traffic_source": traffic_src,
                          "step_bytes_per_particle_update": step_b,
                          "step_achieved_gbs": step_gbs, "step_frac": step_gbs / peak,
+                         "kernels": per_kernel,
                          "survey_bytes_per_particle_update": surv_b,
                          "frac_survey": surv_step / peak,
                          "frac_survey_force_passes": surv_pass / peak if surv_pass else None,
