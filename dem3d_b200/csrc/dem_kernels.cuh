@@ -893,18 +893,23 @@ struct TestArgs {
   int tag;
 };
 
+// (No block barriers: every warp runs on its own.  The pass's contact count
+// and the list length it needs come from the pair kernel, or from here when
+// the list overflows.)
 template <bool PP>
 __global__ void __launch_bounds__(128) k_test(TestArgs A) {
-  __shared__ int s_abort;
-  if (threadIdx.x == 0) s_abort = A.cnt->abort;
-  __syncthreads();
-  if (s_abort) return;
+  if (A.cnt->abort) return;
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = p0 < A.n;
   const int p = valid ? p0 : 0;
   const int n = A.n;
+  // the first candidates are read before the row length is known (every
+  // row holds at least 4 entries' room)
+  int q0[4];
+#pragma unroll
+  for (int u = 0; u < 4; u++) q0[u] = __ldg(A.cand + (size_t)u * n + p);
   const DevParams& P = sys_params(A.P, A.sysid, p);
   const double4 p4 = A.X[p];
   const int cp = PP ? 0 : A.comp[p];
@@ -921,7 +926,8 @@ __global__ void __launch_bounds__(128) k_test(TestArgs A) {
     for (int b = base; b < end; b += 4) {
       int q[4];
 #pragma unroll
-      for (int u = 0; u < 4; u++) q[u] = b + u < end ? __ldg(A.cand + (size_t)(b + u) * n + p) : -1;
+      for (int u = 0; u < 4; u++)
+        q[u] = b + u < end ? (b == 0 ? q0[u] : __ldg(A.cand + (size_t)(b + u) * n + p)) : -1;
       double4 xq[4];
 #pragma unroll
       for (int u = 0; u < 4; u++)
@@ -951,10 +957,7 @@ __global__ void __launch_bounds__(128) k_test(TestArgs A) {
   }
   const int wsum = __shfl_sync(FULL, incl, 31);
   int wbase = 0;
-  if (lane == 31 && wsum > 0) {
-    wbase = atomicAdd(&A.cnt->n_contacts, wsum);
-    atomicMax(&A.cnt->need_cl, wbase + wsum);
-  }
+  if (lane == 31 && wsum > 0) wbase = atomicAdd(&A.cnt->n_contacts, wsum);
   wbase = __shfl_sync(FULL, wbase, 31);
   const int start = wbase + incl - total;
   if (valid) {
@@ -963,6 +966,7 @@ __global__ void __launch_bounds__(128) k_test(TestArgs A) {
   }
   if (start + total > A.cl_cap) {
     // the list is grown and the pass launched again
+    atomicMax(&A.cnt->need_cl, start + total);
     atomicExch(&A.cnt->cl_overflow, 1);
     set_abort(A.cnt, A.tag);
   } else if (total > 0) {
@@ -976,7 +980,6 @@ __global__ void __launch_bounds__(128) k_test(TestArgs A) {
       }
     }
   }
-  publish_counts_block(A.cnt, false, 0u, (unsigned)total, 0u, 0u, 0u);
 }
 
 // record keys read before the record count is known (speculatively, within
@@ -991,6 +994,11 @@ __global__ void __launch_bounds__(128, MINB) k_pair_fp64(PassArgs<double4, doubl
   __syncthreads();
   if (s_abort) return;
   const int total = A.cnt->n_contacts;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    // the pass's pair contacts: the length of its contact list
+    atomicAdd(&A.cnt->pair_contacts, (unsigned long long)total);
+    atomicMax(&A.cnt->need_cl, total);
+  }
   const bool update = A.update != 0;
   const double half_dt = A.half_dt;
   unsigned n_col = 0;
@@ -1107,6 +1115,7 @@ __global__ void __launch_bounds__(128, 4) k_fold_fp64(PassArgs<double4, double2>
   double d2 = 0.0;
   if (valid) {
     const DevParams& P = sys_params(A.P, A.sysid, p);
+    prefetch_epilogue<EPI>(A, P, p, false);
     const int c = A.cell_cur[p];
     const unsigned long long key_p = sweep_key(c, A.rank[p]);
     const int ni = A.in_cnt[p];

@@ -249,6 +249,11 @@ __global__ void __launch_bounds__(128, MINB) k_pair_mixed(PassArgs<float4, float
   __syncthreads();
   if (s_abort) return;
   const int total = A.cnt->n_contacts;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    // the pass's pair contacts: the length of its contact list
+    atomicAdd(&A.cnt->pair_contacts, (unsigned long long)total);
+    atomicMax(&A.cnt->need_cl, total);
+  }
   const bool update = A.update != 0;
   const float half_dt = (float)A.half_dt;
   const History& Hr = A.Hr;
@@ -368,6 +373,7 @@ __global__ void __launch_bounds__(128, 4) k_fold_mixed(PassArgs<float4, float2> 
   double d2 = 0.0;
   if (valid) {
     const DevParams& P = sys_params(A.P, A.sysid, p);
+    prefetch_epilogue<EPI>(A, P, p, true);
     const int c = A.cell_cur[p];
     const unsigned long long key_p = sweep_key(c, A.rank[p]);
     const int ni = A.in_cnt[p];

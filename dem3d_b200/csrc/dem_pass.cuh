@@ -199,6 +199,46 @@ __device__ __forceinline__ float2 mk_w2<float2>(double a, double b) {
   return make_float2((float)a, (float)b);
 }
 
+__device__ __forceinline__ void prefetch_l2(const void* ptr) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
+}
+
+// The state the integrator epilogue of particle p will read, requested into
+// L2 at the start of the fold kernel so that those reads overlap the fold
+// (they do not depend on it).  mixed: the FP64 velocities of Particle
+// (predictor) or Predicted (corrector) come from the state arrays.
+template <int EPI, class V4, class W2>
+__device__ __forceinline__ void prefetch_epilogue(const PassArgs<V4, W2>& A, const DevParams& P,
+                                                  int p, bool mixed) {
+  if (EPI == EPI_STORE) return;
+  const size_t n = (size_t)A.n;
+  if (EPI == EPI_PREDICT) {
+    for (int k = 0; k < P.nprev; k++) {
+      const double* rg = A.ring + (size_t)A.rm.phys[k] * 9 * n + p;
+#pragma unroll
+      for (int d = 0; d < 9; d++) prefetch_l2(rg + d * n);
+    }
+    if (mixed) {
+      const double* v[6] = {A.part.vx, A.part.vy, A.part.vz, A.part.wx, A.part.wy, A.part.wz};
+#pragma unroll
+      for (int d = 0; d < 6; d++) prefetch_l2(v[d] + p);
+    }
+  } else {
+    if (A.amsum)
+#pragma unroll
+      for (int d = 0; d < 9; d++) prefetch_l2(A.amsum + d * n + p);
+    const double* q[9] = {A.part.px, A.part.py, A.part.pz, A.part.vx, A.part.vy,
+                          A.part.vz, A.part.wx, A.part.wy, A.part.wz};
+#pragma unroll
+    for (int d = 0; d < 9; d++) prefetch_l2(q[d] + p);
+    if (mixed) {
+      prefetch_l2(A.pred.vx + p);
+      prefetch_l2(A.pred.vy + p);
+      prefetch_l2(A.pred.vz + p);
+    }
+  }
+}
+
 // The integrator part of a pass, after a = F/m and alpha = T/I
 // (src/MForces.f90:330-333):
 //  EPI_STORE   a, alpha -> tgt;
