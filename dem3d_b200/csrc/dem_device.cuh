@@ -98,6 +98,7 @@ struct Counters {
   unsigned int disp_max;  // FP32 bits (rounded up) of the largest displacement of one pass
   double disp_acc;   // sum of disp_max since the last full rebuild
   int escape_stop;   // a captured chunk stopped before a step: particles had left the box
+  int pass_id;       // force passes completed; a cell stamped pass_id + 1 has rows to rebuild
 };
 
 // Contact history, one table per buffer, stored slot major (record r of
@@ -150,9 +151,9 @@ struct CellLists {
   int* mflag;     // [n] particle already pushed as an arrival
   int* mnext;     // [n] a mover's successor in the list it leaves
   int* dflag;     // [ncell] cell already in a dirty list
-  int* rflag;     // [ncell] cell already in the repair list
+  int* rflag;     // [ncell] stamp: pass_id + 1 when the cell's rows are rebuilt in that pass
   int* dlist[2];  // [ncell] cells that gain or lose a particle on the way to assignment b
-  int* rlist;     // [ncell] cells whose particles' candidate rows are rebuilt
+  int* rlist;     // [ncell] (unused: the stamps replace a repair list)
 };
 
 // Candidate rows, column-major (cand[k*n + p]): the particles within

@@ -571,6 +571,7 @@ __global__ void k_relink(const DevParams* __restrict__ PT, const int* __restrict
     if (full) cnt->force_full = 0;
   }
   const int m = cnt->n_dirty[par];
+  const int stamp = cnt->pass_id + 1;  // fold kernels advance pass_id, not this one
   const int* __restrict__ cell_new = L.cell[par];
   for (int i = tid; i < m; i += gridDim.x * blockDim.x) {
     const int c = L.dlist[par][i];
@@ -626,31 +627,20 @@ __global__ void k_relink(const DevParams* __restrict__ PT, const int* __restrict
     }
     L.head[c] = first;
     L.dflag[c] = 0;
-    // 3. the rows of every particle around c are rebuilt in this pass: the
-    // 27 flag exchanges are issued together, then one append per cell
+    // 3. the rows of every particle around c are rebuilt in this pass (by
+    // the test kernel): the 27 cells are stamped with the pass
     const DevParams& P = sys_params(PT, cellsys, c);
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     const int cl = c - P.coff;
     const int cx = cl % nx, cy = (cl / nx) % ny, cz = cl / (nx * ny);
-    int jcs[27];
-    unsigned fresh = 0u;
 #pragma unroll
     for (int o = 0; o < 27; o++) {
       const int jx = cx + o % 3 - 1, jy = cy + (o / 3) % 3 - 1, jz = cz + o / 9 - 1;
       const bool ok = (P.pbc[0] || (jx >= 0 && jx < nx)) && (P.pbc[1] || (jy >= 0 && jy < ny)) &&
                       (P.pbc[2] || (jz >= 0 && jz < nz));
-      jcs[o] = ok ? P.coff + axis_wrap(jx, nx, P.pbc[0]) +
-                        nx * (axis_wrap(jy, ny, P.pbc[1]) + ny * axis_wrap(jz, nz, P.pbc[2]))
-                  : -1;
-    }
-#pragma unroll
-    for (int o = 0; o < 27; o++)
-      if (jcs[o] >= 0 && atomicExch(&L.rflag[jcs[o]], 1) == 0) fresh |= 1u << o;
-    if (fresh) {
-      int k = atomicAdd(&cnt->n_repair, __popc(fresh));
-#pragma unroll
-      for (int o = 0; o < 27; o++)
-        if ((fresh >> o) & 1u) L.rlist[k++] = jcs[o];
+      if (ok)
+        L.rflag[P.coff + axis_wrap(jx, nx, P.pbc[0]) +
+                nx * (axis_wrap(jy, ny, P.pbc[1]) + ny * axis_wrap(jz, nz, P.pbc[2]))] = stamp;
     }
   }
 }
@@ -812,49 +802,6 @@ __device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int 
   }
 }
 
-// Candidate rows of the pass: every row when the pass is due for a full
-// rebuild (one warp per particle), else the rows of the particles of every
-// repair cell (one warp per cell).  The repair flags of the listed cells are
-// cleared in every case (also when a stopped sequence skips the work).
-template <bool PP>
-__global__ void __launch_bounds__(256) k_screen(const DevParams* __restrict__ PT,
-                                                const int* __restrict__ sysid,
-                                                const int* __restrict__ cellsys, int n,
-                                                const double4* __restrict__ X,
-                                                const int* __restrict__ comp,
-                                                const int* __restrict__ cell_cur, CellLists L,
-                                                Rows R, Counters* cnt, int tag) {
-  const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  const bool skip = cnt->abort != 0;
-  const bool full = cnt->full_due != 0;
-  const int m = cnt->n_repair;
-  for (int r = warp; r < m; r += nwarps) {
-    const int c = L.rlist[r];
-    if (!skip && !full) {
-      int p = L.head[c], guard = 0;
-      while (p != -1) {
-        if (++guard > n) {
-          if (lane == 0) {
-            atomicExch(&cnt->list_error, 1);
-            set_abort(cnt, tag);
-          }
-          break;
-        }
-        build_row<PP>(sys_params(PT, cellsys, c), n, p, c, X, comp, L.head, L.next, R, cnt,
-                      tag);
-        p = L.next[p];
-      }
-    }
-    if (lane == 0) L.rflag[c] = 0;
-  }
-  if (!skip && full)
-    for (int p = warp; p < n; p += nwarps)
-      build_row<PP>(sys_params(PT, sysid, p), n, p, cell_cur[p], X, comp, L.head, L.next, R, cnt,
-                    tag);
-}
-
 // ---------------------------------------------------------------------------
 // K2+K4: a force pass is three kernels.
 //
@@ -881,6 +828,9 @@ struct TestArgs {
   const DevParams* P;
   const int* sysid;
   int n;
+  const int* cell_cur;  // cell of every particle in this pass
+  CellLists L;
+  Rows R;
   const double4* X;
   const int* comp;
   const int* cand;
@@ -893,9 +843,12 @@ struct TestArgs {
   int tag;
 };
 
-// (No block barriers: every warp runs on its own.  The pass's contact count
-// and the list length it needs come from the pair kernel, or from here when
-// the list overflows.)
+// First, the candidate rows of the warp's particles that this pass rebuilds
+// (every row on a full rebuild, else the rows of the particles whose cell the
+// relink stamped with this pass) are built, one particle at a time by the
+// whole warp (build_row).  (No block barriers: every warp runs on its own.
+// The pass's contact count and the list length it needs come from the pair
+// kernel, or from here when the list overflows.)
 template <bool PP>
 __global__ void __launch_bounds__(128) k_test(TestArgs A) {
   if (A.cnt->abort) return;
@@ -905,6 +858,21 @@ __global__ void __launch_bounds__(128) k_test(TestArgs A) {
   const bool valid = p0 < A.n;
   const int p = valid ? p0 : 0;
   const int n = A.n;
+  {
+    const bool full = A.cnt->full_due != 0;
+    const int stamp = A.cnt->pass_id + 1;
+    const int cp0 = A.cell_cur[p];
+    unsigned todo = __ballot_sync(FULL, valid && (full || A.L.rflag[cp0] == stamp));
+    while (todo) {
+      const int l = __ffs(todo) - 1;
+      todo &= todo - 1u;
+      const int pl = __shfl_sync(FULL, p, l);
+      const int cl = __shfl_sync(FULL, cp0, l);
+      build_row<PP>(sys_params(A.P, A.sysid, pl), n, pl, cl, A.X, A.comp, A.L.head, A.L.next,
+                    A.R, A.cnt, A.tag);
+    }
+    __syncwarp();  // the rows written by the warp are visible to their owners
+  }
   // the first candidates are read before the row length is known (every
   // row holds at least 4 entries' room)
   int q0[4];
@@ -1105,6 +1073,7 @@ __global__ void __launch_bounds__(128, 4) k_fold_fp64(PassArgs<double4, double2>
   if (s_abort) return;
   if (WALLS)
     for (int w = 0; w < A.nw_max; w++) s_w[w][threadIdx.x] = 0.0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.cnt->pass_id, 1);  // this pass is done
   const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = p0 < A.n;
   const int p = valid ? p0 : 0;

@@ -528,7 +528,6 @@ StateArrays make_state(double* base, size_t n) {
 // K1: initial distribution (DistributeParticles3D) of the Particle positions
 
 constexpr int LIST_BLOCKS = 148;      // relink / repair kernels (grid-stride)
-constexpr int FULL_BLOCKS = 148 * 8;  // full candidate-row rebuild (grid-stride)
 
 int init_cells(dem_ctx* c) {
   const int n = c->n;
@@ -752,6 +751,9 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
   T.P = c->dp;
   T.sysid = c->sysid;
   T.n = c->n;
+  T.cell_cur = c->L.cell[c->par];
+  T.L = c->L;
+  T.R = c->rows;
   T.X = c->X[side];
   T.comp = c->comp;
   T.cand = c->rows.cand;
@@ -766,7 +768,9 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
   if (c->pp) launch(c, "test", k_test<true>, g, 128, T);
   else launch(c, "test", k_test<false>, g, 128, T);
   const int mb = c->pass_variant == 1 ? 3 : c->pass_variant == 2 ? 5 : 4;
-  const unsigned pair_blocks = (unsigned)(148 * mb);
+  // the pair kernel loops over the list: two waves of the blocks its
+  // register budget lets an SM hold (at least mb per SM)
+  const unsigned pair_blocks = (unsigned)(148 * 2 * std::max(mb, 6));
   const bool walls = c->nw_max > 0;
   if (c->precision == DEM_PREC_MIXED) {
     auto A = pass_args<float4, float2>(c, side, update, dt, rm, tag, tgt);
@@ -838,30 +842,15 @@ int prepare_side(dem_ctx* c, int side) {
   return DEM_OK;
 }
 
-// candidate rows of the pass (repair or full rebuild, decided on the device)
-void launch_screen(dem_ctx* c, int side, int tag) {
-  if (c->n == 0) return;
-  const unsigned g = std::min(blocks_for((long long)c->n * 32, 256), (unsigned)FULL_BLOCKS);
-  if (c->pp)
-    launch(c, "screen", k_screen<true>, g, 256, (const DevParams*)c->dp, (const int*)c->sysid,
-           (const int*)c->cellsys, c->n,
-           (const double4*)c->X[side], (const int*)c->comp, (const int*)c->L.cell[c->par], c->L,
-           c->rows, c->cnt, tag);
-  else
-    launch(c, "screen", k_screen<false>, g, 256, (const DevParams*)c->dp, (const int*)c->sysid,
-           (const int*)c->cellsys, c->n,
-           (const double4*)c->X[side], (const int*)c->comp, (const int*)c->L.cell[c->par], c->L,
-           c->rows, c->cnt, tag);
-}
-
-// relink towards the prepared assignment, then the candidate rows
+// relink towards the prepared assignment (the candidate rows around the
+// relinked cells are rebuilt by the test kernel)
 void pass_lists(dem_ctx* c, int side, bool update, int tag) {
+  (void)side;
   const int b = c->par ^ 1;
   const int stop_tag = c->capturing && c->stop_on_escape && update ? tag : -1;
   launch(c, "relink", k_relink, (unsigned)LIST_BLOCKS, 256, (const DevParams*)c->dp,
          (const int*)c->cellsys, c->L, b, c->n, update ? 1 : 0, stop_tag, c->cnt);
   c->par = b;
-  launch_screen(c, side, tag);
 }
 
 RingMap current_map(dem_ctx* c) {
@@ -956,8 +945,6 @@ int finish_pass(dem_ctx* c, int side, bool update, double dt, int epi, const Rin
       CK(cudaMemcpyAsync(&c->cnt->full_due, &one, sizeof(int), cudaMemcpyHostToDevice,
                          c->stream));
       CK(cudaMemsetAsync(&c->cnt->disp_acc, 0, sizeof(double), c->stream));
-      CK(cudaMemsetAsync(&c->cnt->n_repair, 0, sizeof(int), c->stream));
-      launch_screen(c, side, tag);
     }
     launch_pass_kernel(c, side, update, dt, epi, rm, tag);
   }

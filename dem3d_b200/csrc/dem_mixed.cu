@@ -361,6 +361,7 @@ __global__ void __launch_bounds__(128, 4) k_fold_mixed(PassArgs<float4, float2> 
   if (s_abort) return;
   if (WALLS)
     for (int w = 0; w < A.nw_max; w++) s_w[w][threadIdx.x] = 0.f;
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.cnt->pass_id, 1);  // this pass is done
   const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = p0 < A.n;
   const int p = valid ? p0 : 0;
