@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(128, MINB) k_pair_mixed(PassArgs<float4, float
 // (FP32), a = F/m, alpha = T/I, then the FP64 integrator epilogue.  WALLS:
 // some system has walls; CONE: some wall is a cone.
 template <bool PP, int EPI, bool WALLS, bool CONE>
-__global__ void __launch_bounds__(128, 4) k_fold_mixed(PassArgs<float4, float2> A, MixedView V) {
+__global__ void __launch_bounds__(128, 5) k_fold_mixed(PassArgs<float4, float2> A, MixedView V) {
   __shared__ float s_w[WALLS ? NWM : 1][128];  // |FN| of each wall contact
   __shared__ int s_abort;
   // one decision for the whole block (it meets block barriers later)
