@@ -1090,7 +1090,7 @@ __global__ void __launch_bounds__(128, MINB) k_pair_fp64(PassArgs<double4, doubl
 // sweep order, a = F/m, alpha = T/I, then the integrator epilogue.  WALLS:
 // some system has walls.
 template <bool PP, int EPI, bool WALLS>
-__global__ void __launch_bounds__(128, 5) k_fold_fp64(PassArgs<double4, double2> A) {
+__global__ void __launch_bounds__(128, WALLS ? 4 : 5) k_fold_fp64(PassArgs<double4, double2> A) {
   __shared__ double s_w[WALLS ? NWM : 1][128];  // |FN| of each wall contact
   __shared__ int s_abort;
   // one decision for the whole block (it meets block barriers later)
