@@ -850,7 +850,7 @@ struct TestArgs {
 // The pass's contact count and the list length it needs come from the pair
 // kernel, or from here when the list overflows.)
 template <bool PP>
-__global__ void __launch_bounds__(128, 5) k_test(TestArgs A) {
+__global__ void __launch_bounds__(128) k_test(TestArgs A) {
   if (A.cnt->abort) return;
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
@@ -858,27 +858,11 @@ __global__ void __launch_bounds__(128, 5) k_test(TestArgs A) {
   const bool valid = p0 < A.n;
   const int p = valid ? p0 : 0;
   const int n = A.n;
-  // what the common path needs is requested at once: the cell (for the
-  // repair check), the row length, the position, the first 4 candidates and
-  // their positions (rows are valid unless a full rebuild is due)
-  const bool full = A.cnt->full_due != 0;
-  const int stamp = A.cnt->pass_id + 1;
-  const int cp0 = A.cell_cur[p];
-  int m = valid ? (A.meta[p] & META_MASK) : 0;
-  const double4 p4 = A.X[p];
-  int q0[4];
-  double4 x0[4];
-#pragma unroll
-  for (int u = 0; u < 4; u++) q0[u] = __ldg(A.cand + (size_t)u * n + p);
-#pragma unroll
-  for (int u = 0; u < 4; u++)
-    x0[u] = !full && u < m && (unsigned)q0[u] < (unsigned)n ? A.X[q0[u]]
-                                                            : make_double4(0.0, 0.0, 0.0, 0.0);
   {
-    // the rows this pass rebuilds (every row on a full rebuild, else those of
-    // the particles whose cell the relink stamped), one at a time by the warp
-    const unsigned todo0 = __ballot_sync(FULL, valid && (full || A.L.rflag[cp0] == stamp));
-    unsigned todo = todo0;
+    const bool full = A.cnt->full_due != 0;
+    const int stamp = A.cnt->pass_id + 1;
+    const int cp0 = A.cell_cur[p];
+    unsigned todo = __ballot_sync(FULL, valid && (full || A.L.rflag[cp0] == stamp));
     while (todo) {
       const int l = __ffs(todo) - 1;
       todo &= todo - 1u;
@@ -887,20 +871,17 @@ __global__ void __launch_bounds__(128, 5) k_test(TestArgs A) {
       build_row<PP>(sys_params(A.P, A.sysid, pl), n, pl, cl, A.X, A.comp, A.L.head, A.L.next,
                     A.R, A.cnt, A.tag);
     }
-    if (todo0) {
-      __syncwarp();  // the rows written by the warp are visible to their owners
-      if ((todo0 >> lane) & 1u) {
-        m = A.meta[p] & META_MASK;
-#pragma unroll
-        for (int u = 0; u < 4; u++) q0[u] = A.cand[(size_t)u * n + p];
-#pragma unroll
-        for (int u = 0; u < 4; u++)
-          x0[u] = u < m ? A.X[q0[u]] : make_double4(0.0, 0.0, 0.0, 0.0);
-      }
-    }
+    __syncwarp();  // the rows written by the warp are visible to their owners
   }
+  // the first candidates are read before the row length is known (every
+  // row holds at least 4 entries' room)
+  int q0[4];
+#pragma unroll
+  for (int u = 0; u < 4; u++) q0[u] = __ldg(A.cand + (size_t)u * n + p);
   const DevParams& P = sys_params(A.P, A.sysid, p);
+  const double4 p4 = A.X[p];
   const int cp = PP ? 0 : A.comp[p];
+  const int m = valid ? (A.meta[p] & META_MASK) : 0;
   // contact bit masks of the row, 64 candidates per window (windows past
   // the first only for rows longer than 64)
   unsigned long long mask0 = 0ull;
@@ -912,20 +893,13 @@ __global__ void __launch_bounds__(128, 5) k_test(TestArgs A) {
 #pragma unroll 1
     for (int b = base; b < end; b += 4) {
       int q[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        q[u] = b + u < end ? (b == 0 ? q0[u] : __ldg(A.cand + (size_t)(b + u) * n + p)) : -1;
       double4 xq[4];
-      if (b == 0) {
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-          q[u] = u < end ? q0[u] : -1;
-          xq[u] = x0[u];
-        }
-      } else {
-#pragma unroll
-        for (int u = 0; u < 4; u++) q[u] = b + u < end ? __ldg(A.cand + (size_t)(b + u) * n + p) : -1;
-#pragma unroll
-        for (int u = 0; u < 4; u++)
-          xq[u] = q[u] >= 0 ? A.X[q[u]] : make_double4(0.0, 0.0, 0.0, 0.0);
-      }
+      for (int u = 0; u < 4; u++)
+        xq[u] = q[u] >= 0 ? A.X[q[u]] : make_double4(0.0, 0.0, 0.0, 0.0);
 #pragma unroll
       for (int u = 0; u < 4; u++) {
         if (q[u] < 0) continue;
