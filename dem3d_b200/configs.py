@@ -464,7 +464,7 @@ def lattice_positions(n: int, L: float, rng, jitter=0.05, cutoff=1.2):
 
 def dense_packing_params(radius_max, L, *, e=0.8, mu=0.5, dt=1e-4, method_order=4,
                          euler_intervals=100, max_ncell=1 << 30, precision=P.PREC_FP64,
-                         hist_capacity=16):
+                         hist_capacity=4):
     return P.per_particle_params(
         density=DENSITY, kn=KN, kt=KT, en=e, et=e, mu=mu, rmax=radius_max, lbox=(L, L, L),
         pbc=(True, True, True), gravity=(0.0, 0.0, 0.0), time_step=dt,

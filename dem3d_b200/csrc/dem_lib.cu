@@ -121,7 +121,7 @@ struct dem_ctx {
   void* in_rec = nullptr;
   double* wall_part = nullptr;  // [contact-kernel blocks][NWM] wall normal forces
   int nw_max = 0;               // walls of the system with the most
-  int in_cap = 8;
+  int in_cap = 4;
   int pass_cap = 0;
   double2* pour_cand = nullptr;  // candidate points of one PourParticle call
   int* pour_fits = nullptr;
