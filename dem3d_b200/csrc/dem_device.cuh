@@ -264,9 +264,11 @@ struct PassArgs {
 
 // The |FN| of every wall contact of a block of 128 particles, summed in a
 // fixed order (lanes of warp 0 over the four warps, then a shuffle tree):
-// s_w[w][thread] holds each thread's value.  All threads of the block call.
+// s_w[w][thread] holds each thread's value; the sums go to row `block` of
+// out.  All threads of the block call.
 template <class T>
-__device__ __forceinline__ void wall_partials(const T (*s_w)[128], int nw_max, double* out) {
+__device__ __forceinline__ void wall_partials(const T (*s_w)[128], int nw_max, double* out,
+                                              int block) {
   __syncthreads();
   if (threadIdx.x < 32) {
     const int l = threadIdx.x;
@@ -277,7 +279,7 @@ __device__ __forceinline__ void wall_partials(const T (*s_w)[128], int nw_max, d
       v = v + (double)s_w[w][l + 96];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, o);
-      if (l == 0) out[(size_t)blockIdx.x * NWM + w] = v;
+      if (l == 0) out[(size_t)block * NWM + w] = v;
     }
   }
 }

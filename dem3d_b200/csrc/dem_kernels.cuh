@@ -527,21 +527,24 @@ __global__ void __launch_bounds__(256) k_prepare(const DevParams* __restrict__ P
 // moved (mnext), so no thread reads a link that another thread rewrites.
 // Thread 0 also closes the previous pass's bookkeeping and decides whether
 // this pass rebuilds every candidate row.
-__global__ void k_relink(const DevParams* __restrict__ PT, const int* __restrict__ cellsys,
-                         CellLists L, int par, int n, int update, int stop_tag, Counters* cnt) {
+// (The body of k_relink; tid / nthreads: this thread's index in the grid and
+// the grid's thread count, so that a persistent kernel can run it too.)
+__device__ __forceinline__ void relink_body(const DevParams* __restrict__ PT,
+                                            const int* __restrict__ cellsys, const CellLists& L,
+                                            int par, int n, int update, int stop_tag,
+                                            Counters* cnt, int tid, int nthreads) {
   if (cnt->abort) return;
   // inside a captured chunk, particles that left the box in the last step
   // stop the chunk before this step (the host runs UpdateParticleList); the
   // count is final here (written by the previous kernel), so every block
   // takes the same branch
   if (stop_tag >= 0 && cnt->escaped != 0ull) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (tid == 0) {
       cnt->escape_stop = 1;
       set_abort(cnt, stop_tag);
     }
     return;
   }
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   if (tid == 0) {
     const DevParams& P = PT[0];  // the integrator settings are shared
     cnt->n_repair = 0;
@@ -573,7 +576,7 @@ __global__ void k_relink(const DevParams* __restrict__ PT, const int* __restrict
   const int m = cnt->n_dirty[par];
   const int stamp = cnt->pass_id + 1;  // fold kernels advance pass_id, not this one
   const int* __restrict__ cell_new = L.cell[par];
-  for (int i = tid; i < m; i += gridDim.x * blockDim.x) {
+  for (int i = tid; i < m; i += nthreads) {
     const int c = L.dlist[par][i];
     // 1. unlink the leavers
     int prev = -1, first = -1, q = L.head[c];
@@ -643,6 +646,12 @@ __global__ void k_relink(const DevParams* __restrict__ PT, const int* __restrict
                 nx * (axis_wrap(jy, ny, P.pbc[1]) + ny * axis_wrap(jz, nz, P.pbc[2]))] = stamp;
     }
   }
+}
+
+__global__ void k_relink(const DevParams* __restrict__ PT, const int* __restrict__ cellsys,
+                         CellLists L, int par, int n, int update, int stop_tag, Counters* cnt) {
+  relink_body(PT, cellsys, L, par, n, update, stop_tag, cnt, blockIdx.x * blockDim.x + threadIdx.x,
+              gridDim.x * blockDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -849,12 +858,14 @@ struct TestArgs {
 // whole warp (build_row).  (No block barriers: every warp runs on its own.
 // The pass's contact count and the list length it needs come from the pair
 // kernel, or from here when the list overflows.)
+// (The body of k_test for block `vblock`, so that a persistent kernel can
+// run it too.)
 template <bool PP>
-__global__ void __launch_bounds__(128) k_test(TestArgs A) {
+__device__ __forceinline__ void test_body(const TestArgs& A, int vblock) {
   if (A.cnt->abort) return;
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
-  const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int p0 = vblock * blockDim.x + threadIdx.x;
   const bool valid = p0 < A.n;
   const int p = valid ? p0 : 0;
   const int n = A.n;
@@ -950,19 +961,26 @@ __global__ void __launch_bounds__(128) k_test(TestArgs A) {
   }
 }
 
+template <bool PP>
+__global__ void __launch_bounds__(128) k_test(TestArgs A) {
+  test_body<PP>(A, blockIdx.x);
+}
+
 // record keys read before the record count is known (speculatively, within
 // the table's capacity)
 constexpr int KSPEC = 2;
 
 // The pair kernel (FP64): one thread per contact, grid-stride over the list.
-template <bool PP, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_pair_fp64(PassArgs<double4, double2> A) {
+// (Body for block `vblock` of a grid of `vgrid` blocks.)
+template <bool PP>
+__device__ __forceinline__ void pair_fp64_body(const PassArgs<double4, double2>& A, int vblock,
+                                               int vgrid) {
   __shared__ int s_abort;
   if (threadIdx.x == 0) s_abort = A.cnt->abort;
   __syncthreads();
   if (s_abort) return;
   const int total = A.cnt->n_contacts;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (vblock == 0 && threadIdx.x == 0) {
     // the pass's pair contacts: the length of its contact list
     atomicAdd(&A.cnt->pair_contacts, (unsigned long long)total);
     atomicMax(&A.cnt->need_cl, total);
@@ -972,8 +990,7 @@ __global__ void __launch_bounds__(128, MINB) k_pair_fp64(PassArgs<double4, doubl
   unsigned n_col = 0;
   int need = 0, need_in = 0;
   bool overflow = false, in_over = false;
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < total;
-       s += gridDim.x * blockDim.x) {
+  for (int s = vblock * blockDim.x + threadIdx.x; s < total; s += vgrid * blockDim.x) {
     const int2 e = A.clist[s];
     const int p = e.x, q = e.y;
     const int s_in = atomicAdd(&A.in_cnt[q], 1);  // q's "j" record (returns early)
@@ -1060,11 +1077,16 @@ __global__ void __launch_bounds__(128, MINB) k_pair_fp64(PassArgs<double4, doubl
   publish_counts_block(A.cnt, update, n_col, 0u, 0u, (unsigned)need, (unsigned)need_in);
 }
 
+template <bool PP, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_pair_fp64(PassArgs<double4, double2> A) {
+  pair_fp64_body<PP>(A, blockIdx.x, gridDim.x);
+}
+
 // The fold kernel (FP64): p's block of the sweep, its Force and Torque in
 // sweep order, a = F/m, alpha = T/I, then the integrator epilogue.  WALLS:
 // some system has walls.
 template <bool PP, int EPI, bool WALLS>
-__global__ void __launch_bounds__(128, WALLS ? 4 : 5) k_fold_fp64(PassArgs<double4, double2> A) {
+__device__ __forceinline__ void fold_fp64_body(const PassArgs<double4, double2>& A, int vblock) {
   __shared__ double s_w[WALLS ? NWM : 1][128];  // |FN| of each wall contact
   __shared__ int s_abort;
   // one decision for the whole block (it meets block barriers later)
@@ -1073,8 +1095,8 @@ __global__ void __launch_bounds__(128, WALLS ? 4 : 5) k_fold_fp64(PassArgs<doubl
   if (s_abort) return;
   if (WALLS)
     for (int w = 0; w < A.nw_max; w++) s_w[w][threadIdx.x] = 0.0;
-  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.cnt->pass_id, 1);  // this pass is done
-  const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (vblock == 0 && threadIdx.x == 0) atomicAdd(&A.cnt->pass_id, 1);  // this pass is done
+  const int p0 = vblock * blockDim.x + threadIdx.x;
   const bool valid = p0 < A.n;
   const int p = valid ? p0 : 0;
   const bool update = A.update != 0;
@@ -1244,13 +1266,18 @@ __global__ void __launch_bounds__(128, WALLS ? 4 : 5) k_fold_fp64(PassArgs<doubl
     for (int k = 0; k < 3; k++) alp[k] = T[k] * inv_i;
     epilogue<EPI>(A, P, p, xp, Rp, vp, wp, acc, alp, c, d2);
   }
-  if (WALLS && A.nw_max > 0) wall_partials(s_w, A.nw_max, A.wall_part);
+  if (WALLS && A.nw_max > 0) wall_partials(s_w, A.nw_max, A.wall_part, vblock);
   if (overflow) {
     atomicExch(&A.cnt->overflow, 1);
     set_abort(A.cnt, A.tag);
   }
   publish_counts_block(A.cnt, update, 0u, 0u, n_wc, (unsigned)need, 0u);
   if (EPI != EPI_STORE) publish_disp_block(A.cnt, d2);
+}
+
+template <bool PP, int EPI, bool WALLS>
+__global__ void __launch_bounds__(128, WALLS ? 4 : 5) k_fold_fp64(PassArgs<double4, double2> A) {
+  fold_fp64_body<PP, EPI, WALLS>(A, blockIdx.x);
 }
 
 }  // namespace dem

@@ -511,7 +511,7 @@ __global__ void __launch_bounds__(128, 5) k_fold_mixed(PassArgs<float4, float2> 
     }
     epilogue<EPI>(A, P, p, xp, Rpd, vd, wd, acc, alp, c, d2);
   }
-  if (WALLS && A.nw_max > 0) wall_partials(s_w, A.nw_max, A.wall_part);
+  if (WALLS && A.nw_max > 0) wall_partials(s_w, A.nw_max, A.wall_part, blockIdx.x);
   if (overflow) {
     atomicExch(&A.cnt->overflow, 1);
     set_abort(A.cnt, A.tag);
