@@ -477,14 +477,20 @@ def measure(s, w, args, world, local, torch, dist, first_step=1):
             "steps": steps_done}
 
 
-def force_error(w_fp64, w_mixed, src):
+def snapshot(src):
+    """State, contact history and integration ring of a context, on the host."""
+    return {"state": src.get_state(), "contacts": src.get_contacts(),
+            "integration": src.get_integration()}
+
+
+def force_error(w_fp64, w_mixed, snap):
     """Per-step force error of the mixed path: one force pass from the same
-    state and contact history (taken from ``src``) in both precisions; the
-    error is normed by the largest |a| (net forces cancel in packings)."""
+    state and contact history (``snapshot`` of a context) in both precisions;
+    the error is normed by the largest |a| (net forces cancel in packings)."""
     from dem3d_b200.system import DEMSystem
-    st = src.get_state()
-    c = src.get_contacts()
-    prev, ipc = src.get_integration()
+    st = snap["state"]
+    c = snap["contacts"]
+    prev, ipc = snap["integration"]
     acc = {}
     for name, w in (("fp64", w_fp64), ("mixed", w_mixed)):
         t = DEMSystem(w.params)
@@ -564,10 +570,15 @@ def run_ours(args):
     ferr = None
     obs_cmp = None
     if "fp64" in systems and "mixed" in systems:
-        ferr = force_error(works["fp64"], works["mixed"], systems["fp64"])
         # both runs advanced the same steps from the same state: ensemble
         # observables of the mixed run against the FP64 run
         ob = {p: systems[p].observables() for p in ("fp64", "mixed")}
+        # the FP64 context closes before the two force-pass contexts open
+        # (three contexts of the 16M-sphere workload do not fit one GPU)
+        snap = snapshot(systems["fp64"])
+        systems.pop("fp64").close()
+        ferr = force_error(works["fp64"], works["mixed"], snap)
+        del snap
         keys = ("kinetic_energy", "mean_coordination", "packing_fraction", "bed_height")
         pick = {p: {k: ob[p][k] for k in keys} for p in ob}
         for p in ob:
