@@ -706,7 +706,9 @@ def run_ours(args):
             "dtype": "f64" if headline == "fp64" else "f32+f64", "data": "synthetic",
             "config": config_block(args.workload, w, world, headline),
             "gpu_launches": int(launches),
+            "launches_per_step": launches / res[headline]["steps"],
             "precisions": {p: {"value": r["value"], "ms_per_step": r["ms"] / r["steps"],
+                               "launches_per_step": r["launches"] / r["steps"],
                                "tuning": r["tuning"]}
                            for p, r in res.items()},
             "mixed_over_fp64": (res["mixed"]["value"] / res["fp64"]["value"]
@@ -858,6 +860,7 @@ def run_ensemble(args):
                                       f"{world}-th system per rank), no exchange"},
             "job_observables": job_obs,
             "gpu_launches": int(res["launches"]),
+            "launches_per_step": res["launches"] / res["steps"],
             "tuning": res["tuning"],
             "sequential_fp64_systems": seq,
             "ensemble_over_sequential_fp64": value / seq["value"] if seq else None,

@@ -185,6 +185,10 @@ GPU_ONLY = {
     "set_tuning": (C.c_int, [_P, C.c_double, C.c_int32]),
     "get_tuning": (C.c_int, [_P, _DP, _I32P]),
     "autotune": (C.c_int, [_P, C.c_int32, C.c_int32, _I32P, _DP]),
+    "set_launch_shape": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "get_launch_shape": (C.c_int, [_P, _I32P, _I32P, _I32P, _I32P]),
+    "set_persistent_barrier": (C.c_int, [_P, C.c_double, C.c_int32]),
+    "get_persistent_blocks": (C.c_int, [_P, _I32P]),
     # device pointers for positions and outputs; see the header
     "distribute_particles_noalloc": (C.c_int, [C.POINTER(DemParams), C.c_int32, _P, _P, _P, _P,
                                                _I32P, _P, C.c_char_p, C.c_int32]),

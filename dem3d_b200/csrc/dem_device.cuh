@@ -99,6 +99,7 @@ struct Counters {
   double disp_acc;   // sum of disp_max since the last full rebuild
   int escape_stop;   // a captured chunk stopped before a step: particles had left the box
   int pass_id;       // force passes completed; a cell stamped pass_id + 1 has rows to rebuild
+  int barrier_timeout;  // a grid-wide barrier of a persistent launch gave up waiting
 };
 
 // Contact history, one table per buffer, stored slot major (record r of

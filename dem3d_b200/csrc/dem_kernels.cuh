@@ -24,7 +24,7 @@
 //     them writes a fresh table (new/updated contacts + records of pairs that
 //     the sweep did not visit, as the reference keeps those untouched).
 #pragma once
-#include "dem_pass.cuh"
+#include "dem_test.cuh"
 
 namespace dem {
 
@@ -518,297 +518,10 @@ __global__ void __launch_bounds__(256) k_prepare(const DevParams* __restrict__ P
   publish_disp(cnt, d2);
 }
 
-// Relink (RedistributeParticles3D's list updates, src/MCells.f90:607-643):
-// one thread per dirty cell of list `par` drops the particles that left it
-// (TransferParticle's unlink, :747-774) and prepends its arrivals in
-// decreasing index (AddParticle, :684-698, applied in increasing index
-// order), then marks its 27-cell neighbourhood for candidate-row repair.
-// The walk over the old list follows a leaver's successor saved when it
-// moved (mnext), so no thread reads a link that another thread rewrites.
-// Thread 0 also closes the previous pass's bookkeeping and decides whether
-// this pass rebuilds every candidate row.
-// (The body of k_relink; tid / nthreads: this thread's index in the grid and
-// the grid's thread count, so that a persistent kernel can run it too.)
-__device__ __forceinline__ void relink_body(const DevParams* __restrict__ PT,
-                                            const int* __restrict__ cellsys, const CellLists& L,
-                                            int par, int n, int update, int stop_tag,
-                                            Counters* cnt, int tid, int nthreads) {
-  if (cnt->abort) return;
-  // inside a captured chunk, particles that left the box in the last step
-  // stop the chunk before this step (the host runs UpdateParticleList); the
-  // count is final here (written by the previous kernel), so every block
-  // takes the same branch
-  if (stop_tag >= 0 && cnt->escaped != 0ull) {
-    if (tid == 0) {
-      cnt->escape_stop = 1;
-      set_abort(cnt, stop_tag);
-    }
-    return;
-  }
-  if (tid == 0) {
-    const DevParams& P = PT[0];  // the integrator settings are shared
-    cnt->n_repair = 0;
-    cnt->n_dirty[par ^ 1] = 0;
-    cnt->movers = cnt->movers_pending;
-    cnt->movers_pending = 0ull;
-    if (cnt->ncol_pending) {  // the previous history-updating pass completed
-      cnt->ncol += cnt->ncol_pending;
-      cnt->ncol_pending = 0ull;
-    }
-    cnt->pair_contacts = 0ull;
-    cnt->wall_contacts = 0ull;
-    cnt->n_contacts = 0;  // the contact list of this pass starts empty
-    if (update) {
-      cnt->need_capacity = 0;
-      cnt->need_in = 0;
-      cnt->need_cl = 0;
-    } else {
-      cnt->escaped = 0ull;  // escapes are counted by the current step's corrector
-    }
-    const double d = (double)__uint_as_float(cnt->disp_max);
-    cnt->disp_max = 0u;
-    const double acc = cnt->disp_acc + d;
-    const int full = cnt->force_full != 0 || !(acc <= P.vl_thr);
-    cnt->full_due = full;
-    cnt->disp_acc = full ? 0.0 : acc;
-    if (full) cnt->force_full = 0;
-  }
-  const int m = cnt->n_dirty[par];
-  const int stamp = cnt->pass_id + 1;  // fold kernels advance pass_id, not this one
-  const int* __restrict__ cell_new = L.cell[par];
-  for (int i = tid; i < m; i += nthreads) {
-    const int c = L.dlist[par][i];
-    // 1. unlink the leavers
-    int prev = -1, first = -1, q = L.head[c];
-    int guard = 0;
-    while (q != -1) {
-      if (++guard > n) {
-        atomicExch(&cnt->list_error, 1);
-        atomicExch(&cnt->abort, 1);
-        return;
-      }
-      const bool stays = cell_new[q] == c;
-      const int nq = stays ? L.next[q] : L.mnext[q];
-      if (stays) {
-        if (prev == -1) first = q;
-        else L.next[prev] = q;
-        prev = q;
-      }
-      q = nq;
-    }
-    if (prev != -1) L.next[prev] = -1;
-    // 2. prepend the arrivals, highest index first
-    int sh = -1, tail = -1, a = L.arr_head[c];
-    guard = 0;
-    while (a != -1) {
-      if (++guard > n) {
-        atomicExch(&cnt->list_error, 1);
-        atomicExch(&cnt->abort, 1);
-        return;
-      }
-      const int an = L.arr_next[a];
-      L.mflag[a] = 0;
-      if (sh == -1) {
-        sh = tail = a;
-        L.next[a] = -1;
-      } else if (a > sh) {
-        L.next[a] = sh;
-        sh = a;
-      } else {
-        int q2 = sh;
-        for (int g2 = 0; L.next[q2] != -1 && L.next[q2] > a && g2 < guard; g2++) q2 = L.next[q2];
-        L.next[a] = L.next[q2];
-        L.next[q2] = a;
-        if (L.next[a] == -1) tail = a;
-      }
-      a = an;
-    }
-    L.arr_head[c] = -1;
-    if (sh != -1) {
-      L.next[tail] = first;
-      first = sh;
-    }
-    L.head[c] = first;
-    L.dflag[c] = 0;
-    // 3. the rows of every particle around c are rebuilt in this pass (by
-    // the test kernel): the 27 cells are stamped with the pass
-    const DevParams& P = sys_params(PT, cellsys, c);
-    const int nx = P.nx, ny = P.ny, nz = P.nz;
-    const int cl = c - P.coff;
-    const int cx = cl % nx, cy = (cl / nx) % ny, cz = cl / (nx * ny);
-#pragma unroll
-    for (int o = 0; o < 27; o++) {
-      const int jx = cx + o % 3 - 1, jy = cy + (o / 3) % 3 - 1, jz = cz + o / 9 - 1;
-      const bool ok = (P.pbc[0] || (jx >= 0 && jx < nx)) && (P.pbc[1] || (jy >= 0 && jy < ny)) &&
-                      (P.pbc[2] || (jz >= 0 && jz < nz));
-      if (ok)
-        L.rflag[P.coff + axis_wrap(jx, nx, P.pbc[0]) +
-                nx * (axis_wrap(jy, ny, P.pbc[1]) + ny * axis_wrap(jz, nz, P.pbc[2]))] = stamp;
-    }
-  }
-}
-
 __global__ void k_relink(const DevParams* __restrict__ PT, const int* __restrict__ cellsys,
                          CellLists L, int par, int n, int update, int stop_tag, Counters* cnt) {
   relink_body(PT, cellsys, L, par, n, update, stop_tag, cnt, blockIdx.x * blockDim.x + threadIdx.x,
               gridDim.x * blockDim.x);
-}
-
-// ---------------------------------------------------------------------------
-// K2: candidate rows
-
-// The row of particle p (cell c), built by one warp.  Lane L < 27 owns the
-// neighbour cell at offset (L%3-1, L/3%3-1, L/9-1); lane 13 (own cell) walks
-// the part of the list after p, lane 27 the part before p (p's rank).  The
-// row holds the partners the sweep meets with p as "i": the own cell after p,
-// then the half-shell cells (offset index kx + Nx*(ky + Ny*kz) > 0,
-// AddAllNeighbours3D src/MCells.f90:456) in FirstNeighbour order, i.e.
-// descending (kz, ky, kx) -- NeighbourParticles' list (src/MCells.f90:
-// 793-829) from p on.
-template <bool PP>
-__device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int c,
-                                          const double4* __restrict__ X,
-                                          const int* __restrict__ comp,
-                                          const int* __restrict__ head,
-                                          const int* __restrict__ next, const Rows& R,
-                                          Counters* cnt, int tag) {
-  const unsigned FULL = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  const int nx = P.nx, ny = P.ny, nz = P.nz;
-  const int cl = c - P.coff;
-  const int cx = cl % nx, cy = (cl / nx) % ny, cz = cl / (nx * ny);
-  const double4 p4 = X[p];
-  const int cp = PP ? 0 : comp[p];
-  int start = -1, order = 1 << 20;
-  bool walk = false;
-  if (lane < 27) {
-    const int d[3] = {lane % 3 - 1, (lane / 3) % 3 - 1, lane / 9 - 1};
-    const int cc[3] = {cx, cy, cz};
-    const int N[3] = {nx, ny, nz};
-    bool ok = true;
-    int w[3];
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-      int j = cc[k] + d[k];
-      if (P.pbc[k]) {
-        if (j == N[k]) j = 0;
-        if (j == -1) j = N[k] - 1;
-      } else if (j < 0 || j >= N[k]) {
-        ok = false;
-      }
-      w[k] = j;
-    }
-    const int lex = d[0] + 3 * d[1] + 9 * d[2];
-    if (lane == 13) {
-      start = next[p];
-      order = 0;
-      walk = true;
-    } else if (ok && lex > 0) {
-      start = head[P.coff + w[0] + nx * (w[1] + ny * w[2])];
-      order = 1 + (13 - lex);
-      walk = true;
-    }
-  }
-  const double skin = P.vl_skin;
-  auto is_cand = [&](int q) -> bool {
-    const double4 q4 = X[q];
-    double Rij[3] = {q4.x - p4.x, q4.y - p4.y, q4.z - p4.z};
-#pragma unroll
-    for (int k = 0; k < 3; k++) Rij[k] = min_image_exact(Rij[k], P.box, k);
-    const double DijSq = sumsq3(Rij);
-    double md;
-    if (PP) md = p4.w + q4.w;
-    else md = sqrt(Material<PP>::min_dij_sq(P, cp, p4.w, comp[q], q4.w));
-    md = md + skin;
-    return md * md - DijSq > 0.0;
-  };
-  // pass 1: walk and count; the first 8 list elements and their test
-  // results stay in registers for pass 2.  Lane 27 counts the list before p.
-  int count = 0, walked = 0;
-  unsigned hits = 0u;
-  int cache[8];
-  bool bad = false;
-  int q = start;
-#pragma unroll
-  for (int i = 0; i < 8; i++) cache[i] = -1;
-  if (walk) {
-#pragma unroll
-    for (int i = 0; i < 8; i++) {
-      if (q != -1) {
-        cache[i] = q;
-        walked = i + 1;
-        if (is_cand(q)) {
-          hits |= 1u << i;
-          count++;
-        }
-        q = next[q];
-      }
-    }
-  }
-  const int resume = q;  // first element not cached (-1: none)
-  {
-    int guard = 0;
-    if (walk) {
-      while (q != -1) {
-        if (++guard > n) {
-          bad = true;
-          break;
-        }
-        if (is_cand(q)) count++;
-        q = next[q];
-      }
-    } else if (lane == 27) {
-      q = head[c];
-      while (q != p) {
-        if (q == -1 || ++guard > n) {
-          bad = true;
-          break;
-        }
-        count++;
-        q = next[q];
-      }
-    }
-  }
-  if (__any_sync(FULL, bad)) {
-    if (lane == 0) {
-      atomicExch(&cnt->list_error, 1);
-      set_abort(cnt, tag);
-    }
-    return;
-  }
-  int off = 0, m = 0;
-  for (int l = 0; l < 27; l++) {
-    const int ol = __shfl_sync(FULL, order, l);
-    const int cl2 = __shfl_sync(FULL, walk ? count : 0, l);
-    if (ol < order) off += cl2;
-    m += cl2;
-  }
-  const int rank = __shfl_sync(FULL, count, 27);
-  if (m > R.kc) {
-    if (lane == 0) {
-      atomicMax(&cnt->need_kc, m);
-      atomicExch(&cnt->row_overflow, 1);
-      set_abort(cnt, tag);
-      R.meta[p] = 0;
-    }
-    return;
-  }
-  // pass 2: write (the cached part, then the rest of the list)
-  if (walk) {
-    int k = off;
-#pragma unroll
-    for (int i = 0; i < 8; i++)
-      if (i < walked && ((hits >> i) & 1u)) R.cand[(size_t)(k++) * n + p] = cache[i];
-    int q2 = resume;
-    while (q2 != -1) {
-      if (is_cand(q2)) R.cand[(size_t)(k++) * n + p] = q2;
-      q2 = next[q2];
-    }
-  }
-  if (lane == 0) {
-    R.meta[p] = m;
-    R.rank[p] = rank;
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -832,138 +545,17 @@ __device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int 
 //   Force(i) = Force(i) + iForce; :254-259, 319-320), forms a = F/m,
 //   alpha = T/I (:330-333) and runs the integrator epilogue.
 
-// Arguments of the test kernel (the same for both precisions).
-struct TestArgs {
-  const DevParams* P;
-  const int* sysid;
-  int n;
-  const int* cell_cur;  // cell of every particle in this pass
-  CellLists L;
-  Rows R;
-  const double4* X;
-  const int* comp;
-  const int* cand;
-  const int* meta;
-  int2* clist;
-  int* cstart;
-  int* ccount;
-  int cl_cap;
-  Counters* cnt;
-  int tag;
-};
-
-// First, the candidate rows of the warp's particles that this pass rebuilds
-// (every row on a full rebuild, else the rows of the particles whose cell the
-// relink stamped with this pass) are built, one particle at a time by the
-// whole warp (build_row).  (No block barriers: every warp runs on its own.
-// The pass's contact count and the list length it needs come from the pair
-// kernel, or from here when the list overflows.)
-// (The body of k_test for block `vblock`, so that a persistent kernel can
-// run it too.)
-template <bool PP>
-__device__ __forceinline__ void test_body(const TestArgs& A, int vblock) {
-  if (A.cnt->abort) return;
-  const unsigned FULL = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  const int p0 = vblock * blockDim.x + threadIdx.x;
-  const bool valid = p0 < A.n;
-  const int p = valid ? p0 : 0;
-  const int n = A.n;
-  {
-    const bool full = A.cnt->full_due != 0;
-    const int stamp = A.cnt->pass_id + 1;
-    const int cp0 = A.cell_cur[p];
-    unsigned todo = __ballot_sync(FULL, valid && (full || A.L.rflag[cp0] == stamp));
-    while (todo) {
-      const int l = __ffs(todo) - 1;
-      todo &= todo - 1u;
-      const int pl = __shfl_sync(FULL, p, l);
-      const int cl = __shfl_sync(FULL, cp0, l);
-      build_row<PP>(sys_params(A.P, A.sysid, pl), n, pl, cl, A.X, A.comp, A.L.head, A.L.next,
-                    A.R, A.cnt, A.tag);
-    }
-    __syncwarp();  // the rows written by the warp are visible to their owners
+// BS threads per block.  STRIDE: grid-stride over blocks of BS particles (a
+// grid smaller than the particle count gives each thread several particles);
+// else one block of particles per block.
+template <bool PP, int BS, bool STRIDE>
+__global__ void __launch_bounds__(BS) k_test(TestArgs A) {
+  if (!STRIDE) {
+    test_body<PP>(A, blockIdx.x);
+    return;
   }
-  // the first candidates are read before the row length is known (every
-  // row holds at least 4 entries' room)
-  int q0[4];
-#pragma unroll
-  for (int u = 0; u < 4; u++) q0[u] = __ldg(A.cand + (size_t)u * n + p);
-  const DevParams& P = sys_params(A.P, A.sysid, p);
-  const double4 p4 = A.X[p];
-  const int cp = PP ? 0 : A.comp[p];
-  const int m = valid ? (A.meta[p] & META_MASK) : 0;
-  // contact bit masks of the row, 64 candidates per window (windows past
-  // the first only for rows longer than 64)
-  unsigned long long mask0 = 0ull;
-  unsigned long long more[(KC_MAX + 1) / 64 - 1];
-  int total = 0;
-  for (int base = 0; base < m; base += 64) {
-    unsigned long long mask = 0ull;
-    const int end = m < base + 64 ? m : base + 64;
-#pragma unroll 1
-    for (int b = base; b < end; b += 4) {
-      int q[4];
-#pragma unroll
-      for (int u = 0; u < 4; u++)
-        q[u] = b + u < end ? (b == 0 ? q0[u] : __ldg(A.cand + (size_t)(b + u) * n + p)) : -1;
-      double4 xq[4];
-#pragma unroll
-      for (int u = 0; u < 4; u++)
-        xq[u] = q[u] >= 0 ? A.X[q[u]] : make_double4(0.0, 0.0, 0.0, 0.0);
-#pragma unroll
-      for (int u = 0; u < 4; u++) {
-        if (q[u] < 0) continue;
-        double Rij[3] = {xq[u].x - p4.x, xq[u].y - p4.y, xq[u].z - p4.z};
-#pragma unroll
-        for (int k = 0; k < 3; k++) Rij[k] = min_image_exact(Rij[k], P.box, k);
-        const double DijSq = sumsq3(Rij);
-        const int cq = PP ? 0 : A.comp[q[u]];
-        if (Material<PP>::min_dij_sq(P, cp, p4.w, cq, xq[u].w) - DijSq > 0.0)
-          mask |= 1ull << (b + u - base);
-      }
-    }
-    total += __popcll(mask);
-    if (base == 0) mask0 = mask;
-    else more[base / 64 - 1] = mask;
-  }
-  // one allocation per warp; a particle's contacts are contiguous
-  int incl = total;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(FULL, incl, o);
-    if (lane >= o) incl += y;
-  }
-  const int wsum = __shfl_sync(FULL, incl, 31);
-  int wbase = 0;
-  if (lane == 31 && wsum > 0) wbase = atomicAdd(&A.cnt->n_contacts, wsum);
-  wbase = __shfl_sync(FULL, wbase, 31);
-  const int start = wbase + incl - total;
-  if (valid) {
-    A.cstart[p] = start;
-    A.ccount[p] = total;
-  }
-  if (start + total > A.cl_cap) {
-    // the list is grown and the pass launched again
-    atomicMax(&A.cnt->need_cl, start + total);
-    atomicExch(&A.cnt->cl_overflow, 1);
-    set_abort(A.cnt, A.tag);
-  } else if (total > 0) {
-    int s = start;
-    for (int base = 0; base < m; base += 64) {
-      unsigned long long mask = base == 0 ? mask0 : more[base / 64 - 1];
-      while (mask) {
-        const int k = base + __ffsll((long long)mask) - 1;
-        mask &= mask - 1ull;
-        A.clist[s++] = make_int2(p, __ldg(A.cand + (size_t)k * n + p));
-      }
-    }
-  }
-}
-
-template <bool PP>
-__global__ void __launch_bounds__(128) k_test(TestArgs A) {
-  test_body<PP>(A, blockIdx.x);
+  const int nvb = (A.n + BS - 1) / BS;
+  for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) test_body<PP>(A, vb);
 }
 
 // record keys read before the record count is known (speculatively, within
@@ -1275,9 +867,55 @@ __device__ __forceinline__ void fold_fp64_body(const PassArgs<double4, double2>&
   if (EPI != EPI_STORE) publish_disp_block(A.cnt, d2);
 }
 
-template <bool PP, int EPI, bool WALLS>
+// (STRIDE: grid-stride over blocks of 128 particles, like k_test)
+template <bool PP, int EPI, bool WALLS, bool STRIDE>
 __global__ void __launch_bounds__(128, WALLS ? 4 : 5) k_fold_fp64(PassArgs<double4, double2> A) {
-  fold_fp64_body<PP, EPI, WALLS>(A, blockIdx.x);
+  if (!STRIDE) {
+    fold_fp64_body<PP, EPI, WALLS>(A, blockIdx.x);
+    return;
+  }
+  const int nvb = (A.n + 127) / 128;
+  for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
+    fold_fp64_body<PP, EPI, WALLS>(A, vb);
+    __syncthreads();  // the block's shared arrays are reused by the next block of particles
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The persistent chunk kernel (FP64): npass force passes (prog[0..npass))
+// in one cooperative launch of blocks of 128 threads, as many as fit on the
+// GPU at once.  Every pass runs its four phases in the order of the
+// separate kernels, each phase over the whole grid (the relink over all
+// threads, the test and fold over blocks of 128 particles grid-stride, the
+// pair kernel grid-stride over the contact list), with a grid-wide barrier
+// after each.  The results are those of the separate kernels: the same
+// bodies, the same contact list contents (its order is free), the same sums.
+// Rows are read coherently (written by earlier passes of the same launch).
+using ChunkPass64 = ChunkPass<double4, double2, NoView>;
+
+template <bool PP, bool WALLS>
+__global__ void __launch_bounds__(128, 4) k_chunk_fp64(const ChunkPass64* __restrict__ prog,
+                                                       int npass, GridSync g) {
+  __shared__ ChunkPass64 sp;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nthreads = gridDim.x * blockDim.x;
+  for (int k = 0; k < npass; k++) {
+    load_pass(sp, prog + k);
+    const RelinkArgs& R = sp.rl;
+    relink_body(R.PT, R.cellsys, R.L, R.par, R.n, R.update, R.stop_tag, R.cnt, tid, nthreads);
+    if (!grid_sync(g)) return;
+    const int nvb = (sp.t.n + 127) / 128;
+    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) test_body<PP, false>(sp.t, vb);
+    if (!grid_sync(g)) return;
+    pair_fp64_body<PP>(sp.a, blockIdx.x, gridDim.x);
+    if (!grid_sync(g)) return;
+    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
+      if (sp.epi == EPI_PREDICT) fold_fp64_body<PP, EPI_PREDICT, WALLS>(sp.a, vb);
+      else fold_fp64_body<PP, EPI_CORRECT, WALLS>(sp.a, vb);
+      __syncthreads();
+    }
+    if (!grid_sync(g)) return;  // (also: every block is done with sp)
+  }
 }
 
 }  // namespace dem

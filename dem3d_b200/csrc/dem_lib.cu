@@ -130,6 +130,29 @@ struct dem_ctx {
   int rm_cap = 0;
   long long rm_stats[3] = {0, 0, 0};  // removals, swaps, records renamed or moved
   int pass_variant = 0;  // pair kernel compiled for 4 (0), 3 (1) or 5 (2) blocks per SM
+  // launch shape (dem_set_launch_shape): threads per block of the test
+  // kernel, particles per thread of the test and fold kernels, the pair
+  // kernel's grid in waves of resident blocks, and 4-step chunks as one
+  // persistent launch (1) or replayed graphs (0)
+  int test_block = 128;
+  int ppt = 1;
+  int pair_waves = 2;
+  int launch_mode = 0;
+  // persistent chunks: while `recording`, the pass launchers append the
+  // passes of a chunk to rec (relink arguments wait in rec_rl for their
+  // pass) instead of launching; each rotation phase keeps its chunk's
+  // passes in device memory (prog[phase], prog_n passes)
+  bool recording = false;
+  RelinkArgs rec_rl{};
+  std::vector<unsigned char> rec;
+  int rec_n = 0;
+  void* prog[20] = {};
+  int prog_n[20] = {};
+  bool prog_valid = false;
+  unsigned* bar = nullptr;  // grid barrier: arrival count, generation
+  unsigned long long bar_limit_ns = 2000000000ull;
+  int bar_extra = 0;        // blocks a test adds to every barrier (0: none)
+  int chunk_blocks = 0;     // blocks of the last persistent launch
   bool has_cone = false; // some wall of some system is a cone
   double skin_factor = 0.05;  // candidate-row skin / CutOff
   int par = 0;         // L.cell[par] is the assignment the lists hold
@@ -365,6 +388,13 @@ void drop_graphs(dem_ctx* c) {
       g = nullptr;
     }
   c->graph_valid = false;
+  // the recorded chunks hold the same pointers and rotation phases
+  for (int k = 0; k < 20; k++) {
+    if (c->prog[k]) cudaFree(c->prog[k]);
+    c->prog[k] = nullptr;
+    c->prog_n[k] = 0;
+  }
+  c->prog_valid = false;
 }
 
 // tables laid out for the allocated capacity (record r of particle i at
@@ -764,21 +794,70 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
   T.cl_cap = c->cl_cap;
   T.cnt = c->cnt;
   T.tag = tag;
-  const unsigned g = blocks_for(c->n, 128);
-  if (c->pp) launch(c, "test", k_test<true>, g, 128, T);
-  else launch(c, "test", k_test<false>, g, 128, T);
-  const int mb = c->pass_variant == 1 ? 3 : c->pass_variant == 2 ? 5 : 4;
-  // the pair kernel loops over the list: two waves of the blocks its
-  // register budget lets an SM hold (at least mb per SM)
-  const unsigned pair_blocks = (unsigned)(148 * 2 * std::max(mb, 6));
   const bool walls = c->nw_max > 0;
+  if (c->recording) {
+    // a pass of a persistent chunk: appended, not launched
+    auto add = [&](const auto& cp) {
+      const size_t at = c->rec.size();
+      c->rec.resize(at + sizeof(cp));
+      std::memcpy(c->rec.data() + at, &cp, sizeof(cp));
+      c->rec_n++;
+    };
+    if (c->precision == DEM_PREC_MIXED) {
+      ChunkPass<float4, float2, MixedView> cp{};
+      cp.rl = c->rec_rl;
+      cp.t = T;
+      cp.a = pass_args<float4, float2>(c, side, update, dt, rm, tag, tgt);
+      cp.v = mixed_view(c->M, c->hcur);
+      cp.epi = epi;
+      add(cp);
+    } else {
+      ChunkPass<double4, double2, NoView> cp{};
+      cp.rl = c->rec_rl;
+      cp.t = T;
+      cp.a = pass_args<double4, double2>(c, side, update, dt, rm, tag, tgt);
+      cp.epi = epi;
+      add(cp);
+    }
+    return;
+  }
+  // test kernel: test_block threads per block; with ppt > 1 the grid holds
+  // 1/ppt of the blocks and strides over them
+  {
+    const int bs = c->test_block;
+    const unsigned nvb = blocks_for(c->n, bs);
+    const bool stride = c->ppt > 1;
+    const unsigned g = stride ? (nvb + c->ppt - 1) / c->ppt : nvb;
+#define TK(PPV, BS, S) launch(c, "test", k_test<PPV, BS, S>, g, BS, T)
+#define TCASE(PPV)                    \
+  do {                                \
+    if (bs == 64) {                   \
+      if (stride) TK(PPV, 64, true);  \
+      else TK(PPV, 64, false);        \
+    } else if (bs == 256) {           \
+      if (stride) TK(PPV, 256, true); \
+      else TK(PPV, 256, false);       \
+    } else {                          \
+      if (stride) TK(PPV, 128, true); \
+      else TK(PPV, 128, false);       \
+    }                                 \
+  } while (0)
+    if (c->pp) TCASE(true);
+    else TCASE(false);
+#undef TCASE
+#undef TK
+  }
+  const int mb = c->pass_variant == 1 ? 3 : c->pass_variant == 2 ? 5 : 4;
+  // the pair kernel loops over the list: pair_waves waves of the blocks its
+  // register budget lets an SM hold (at least mb per SM)
+  const unsigned pair_blocks = (unsigned)(148 * c->pair_waves * std::max(mb, 6));
   if (c->precision == DEM_PREC_MIXED) {
     auto A = pass_args<float4, float2>(c, side, update, dt, rm, tag, tgt);
     if (epi == EPI_STORE) A.amsum = c->force_out;
     for (int part = 0; part < 2; part++) {
       timed(c, part ? "fold_mixed" : "pair_mixed", [&]() {
         mixed_pass(c->M, c->pp, epi, c->pass_variant, walls, c->has_cone, A, c->hcur, c->stream,
-                   part, pair_blocks);
+                   part, pair_blocks, c->ppt);
       });
       c->launches++;
     }
@@ -799,14 +878,23 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
     else PAIR_CASE(false, 4);
   }
 #undef PAIR_CASE
-#define FOLD_CASE(PPV, W)                                                         \
-  do {                                                                            \
-    if (epi == EPI_PREDICT)                                                       \
-      launch(c, "fold_fp64", k_fold_fp64<PPV, EPI_PREDICT, W>, g, 128, A);        \
-    else if (epi == EPI_CORRECT)                                                  \
-      launch(c, "fold_fp64", k_fold_fp64<PPV, EPI_CORRECT, W>, g, 128, A);        \
-    else                                                                          \
-      launch(c, "fold_fp64", k_fold_fp64<PPV, EPI_STORE, W>, g, 128, A);          \
+  // fold kernel: blocks of 128 particles (ppt > 1: grid-stride, not for the
+  // Euler start-up's EPI_STORE)
+  const unsigned nvb = blocks_for(c->n, 128);
+  const bool stride = c->ppt > 1 && epi != EPI_STORE;
+  const unsigned g = stride ? (nvb + c->ppt - 1) / c->ppt : nvb;
+#define FK(PPV, E, W, S) launch(c, "fold_fp64", k_fold_fp64<PPV, E, W, S>, g, 128, A)
+#define FOLD_CASE(PPV, W)                     \
+  do {                                        \
+    if (epi == EPI_PREDICT) {                 \
+      if (stride) FK(PPV, EPI_PREDICT, W, true); \
+      else FK(PPV, EPI_PREDICT, W, false);    \
+    } else if (epi == EPI_CORRECT) {          \
+      if (stride) FK(PPV, EPI_CORRECT, W, true); \
+      else FK(PPV, EPI_CORRECT, W, false);    \
+    } else {                                  \
+      FK(PPV, EPI_STORE, W, false);           \
+    }                                         \
   } while (0)
   if (walls) {
     if (c->pp) FOLD_CASE(true, true);
@@ -816,6 +904,7 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
     else FOLD_CASE(false, false);
   }
 #undef FOLD_CASE
+#undef FK
 }
 
 // Copies of `side` for the pass kernel and the cell transition towards its
@@ -848,8 +937,12 @@ void pass_lists(dem_ctx* c, int side, bool update, int tag) {
   (void)side;
   const int b = c->par ^ 1;
   const int stop_tag = c->capturing && c->stop_on_escape && update ? tag : -1;
-  launch(c, "relink", k_relink, (unsigned)LIST_BLOCKS, 256, (const DevParams*)c->dp,
-         (const int*)c->cellsys, c->L, b, c->n, update ? 1 : 0, stop_tag, c->cnt);
+  if (c->recording) {
+    c->rec_rl = RelinkArgs{c->dp, c->cellsys, c->L, b, c->n, update ? 1 : 0, stop_tag, c->cnt};
+  } else {
+    launch(c, "relink", k_relink, (unsigned)LIST_BLOCKS, 256, (const DevParams*)c->dp,
+           (const int*)c->cellsys, c->L, b, c->n, update ? 1 : 0, stop_tag, c->cnt);
+  }
   c->par = b;
 }
 
@@ -1431,6 +1524,98 @@ int capture_steps(dem_ctx* c, int steps, cudaGraphExec_t* out) {
   return DEM_OK;
 }
 
+// A chunk runs as one persistent launch when its steps hold nothing but
+// force passes: no wall motion (a host copy per step), no fluid drag (two
+// more kernels per pass), no per-kernel event timing.
+bool chunk_persistent(const dem_ctx* c) {
+  return c->launch_mode == 1 && c->wm.empty() && !c->fluid && !c->prof;
+}
+
+// Record `steps` MoveParticles steps as the passes of one persistent chunk
+// into prog[phase] (the host bookkeeping is left as it was, as by
+// capture_steps).  Recording launches nothing.
+int record_chunk(dem_ctx* c, int steps, int phase) {
+  const long long l0 = c->launches;
+  int rm[5];
+  std::memcpy(rm, c->ringmap, sizeof(rm));
+  const int hc = c->hcur, par = c->par, prep = c->prepared, last = c->last_side;
+  const double t = c->time;
+  c->rec.clear();
+  c->rec_n = 0;
+  c->recording = true;
+  c->capturing = true;
+  int st = DEM_OK;
+  for (int k = 0; k < steps && !st; k++) st = move_particles_impl(c, 0, false, k);
+  c->recording = false;
+  c->capturing = false;
+  const bool clean = c->launches == l0;
+  c->launches = l0;
+  std::memcpy(c->ringmap, rm, sizeof(rm));
+  c->hcur = hc;
+  c->par = par;
+  c->prepared = prep;
+  c->last_side = last;
+  c->time = t;
+  if (st) return st;
+  if (!clean || c->rec_n != 2 * steps)
+    return fail(c, DEM_ERR_STATE, "a persistent chunk held work other than its force passes");
+  CK(cudaMalloc(&c->prog[phase], c->rec.size()));
+  CK(cudaMemcpy(c->prog[phase], c->rec.data(), c->rec.size(), cudaMemcpyHostToDevice));
+  c->prog_n[phase] = c->rec_n;
+  return DEM_OK;
+}
+
+// the FP64 chunk kernel for this context as a cooperative launch of at
+// most `want` blocks (as many as fit on the device at once)
+template <class K>
+cudaError_t coop_launch64(K k, const ChunkPass64* prog, int npass, GridSync g, int want,
+                          cudaStream_t st, int* blocks_out) {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, 128, 0);
+  const int nb = std::min(want, per * sms);
+  if (nb <= 0) return cudaErrorLaunchOutOfResources;
+  g.expected += (unsigned)nb;  // (on entry: the blocks a test adds to every barrier)
+  void* args[] = {(void*)&prog, (void*)&npass, (void*)&g};
+  if (blocks_out) *blocks_out = nb;
+  return cudaLaunchCooperativeKernel((const void*)k, dim3(nb), dim3(128), args, 0, st);
+}
+
+// Launch the recorded chunk of rotation phase `phase`.
+int launch_chunk(dem_ctx* c, int phase) {
+  if (!c->bar) {
+    CK(cudaMalloc(&c->bar, 2 * sizeof(unsigned)));
+    CK(cudaMemsetAsync(c->bar, 0, 2 * sizeof(unsigned), c->stream));
+  }
+  GridSync g{c->bar, c->bar + 1, c->cnt, c->bar_limit_ns, (unsigned)c->bar_extra};
+  const int want = std::max(1, (int)blocks_for(c->n, 128));
+  const bool walls = c->nw_max > 0;
+  cudaError_t e;
+  if (c->precision == DEM_PREC_MIXED) {
+    e = mixed_chunk(c->pp, walls, c->has_cone,
+                    (const ChunkPass<float4, float2, MixedView>*)c->prog[phase], c->prog_n[phase],
+                    g, want, c->stream, &c->chunk_blocks);
+  } else {
+    const ChunkPass64* prog = (const ChunkPass64*)c->prog[phase];
+    const int np = c->prog_n[phase];
+    if (walls) {
+      e = c->pp ? coop_launch64(k_chunk_fp64<true, true>, prog, np, g, want, c->stream,
+                                &c->chunk_blocks)
+                : coop_launch64(k_chunk_fp64<false, true>, prog, np, g, want, c->stream,
+                                &c->chunk_blocks);
+    } else {
+      e = c->pp ? coop_launch64(k_chunk_fp64<true, false>, prog, np, g, want, c->stream,
+                                &c->chunk_blocks)
+                : coop_launch64(k_chunk_fp64<false, false>, prog, np, g, want, c->stream,
+                                &c->chunk_blocks);
+    }
+  }
+  if (e != cudaSuccess) return cuda_fail(c, e, "persistent chunk launch");
+  c->launches += 1;
+  return DEM_OK;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -1724,6 +1909,7 @@ void dem_destroy(dem_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   drop_graphs(c);
   free_state(c);
+  cudaFree(c->bar);
   cudaFree(c->dp);
   cudaFree(c->rm_buf);
   cudaFree(c->pour_cand);
@@ -2406,21 +2592,44 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
       st = prepare_side(c, 0);
       if (st) return st;
     }
-    // one graph per rotation phase (ring spare slot, history parity, list parity)
+    // one graph (or recorded persistent chunk) per rotation phase (ring
+    // spare slot, history parity, list parity)
     int phase = (c->nprev > 0 ? c->ringmap[c->nprev] : 0) * 4 + c->hcur * 2 + c->par;
-    if (!c->graph_valid) {
-      for (auto& g : c->graph) g = nullptr;
-      c->graph_valid = true;
-    }
-    if (!c->graph[phase]) {
-      st = capture_steps(c, G, &c->graph[phase]);
+    if (chunk_persistent(c)) {
+      if (!c->prog[phase]) {
+        st = record_chunk(c, G, phase);
+        if (st) return st;
+      }
+      st = launch_chunk(c, phase);
       if (st) return st;
+    } else {
+      if (!c->graph_valid) {
+        for (auto& g : c->graph) g = nullptr;
+        c->graph_valid = true;
+      }
+      if (!c->graph[phase]) {
+        st = capture_steps(c, G, &c->graph[phase]);
+        if (st) return st;
+      }
+      fill_wall_slots(c, step, G);  // the previous replay has completed
+      CK(cudaGraphLaunch(c->graph[phase], c->stream));
+      c->launches += c->graph_kernels;
     }
-    fill_wall_slots(c, step, G);  // the previous replay has completed
-    CK(cudaGraphLaunch(c->graph[phase], c->stream));
-    c->launches += c->graph_kernels;
     st = read_counters(c);
     if (st) return st;
+    if (c->hcnt->barrier_timeout) {
+      // the chunk stopped part-way: the barrier words and flags are reset,
+      // the state is left as it is and must be set again
+      CK(cudaMemsetAsync(c->bar, 0, 2 * sizeof(unsigned), c->stream));
+      CK(cudaMemsetAsync(&c->cnt->barrier_timeout, 0, sizeof(int), c->stream));
+      CK(cudaMemsetAsync(&c->cnt->abort, 0, 2 * sizeof(int), c->stream));  // abort, abort_tag
+      CK(cudaStreamSynchronize(c->stream));
+      c->cells_ready = false;
+      drop_graphs(c);
+      return fail(c, DEM_ERR_STATE,
+                  "persistent chunk: a grid-wide barrier timed out; the state is part-way "
+                  "through the chunk (set it again)");
+    }
     int done = G, failed_pass = -1;
     bool escape_stop = false;
     if (c->hcnt->abort) {
@@ -2894,35 +3103,128 @@ int dem_get_tuning(dem_ctx* c, double* skin_factor, int32_t* pass_variant) {
   return DEM_OK;
 }
 
+int dem_set_launch_shape(dem_ctx* c, int32_t launch_mode, int32_t test_block,
+                         int32_t particles_per_thread, int32_t pair_waves) {
+  if (!c) return DEM_ERR_INVALID;
+  auto one_of = [](int v, int a, int b, int d) { return v == a || v == b || v == d; };
+  if ((launch_mode != 0 && launch_mode != 1) || !one_of(test_block, 64, 128, 256) ||
+      !one_of(particles_per_thread, 1, 2, 4) || !one_of(pair_waves, 1, 2, 4))
+    return fail(c, DEM_ERR_INVALID,
+                "launch shape: mode in {0, 1}, test_block in {64, 128, 256}, "
+                "particles_per_thread in {1, 2, 4}, pair_waves in {1, 2, 4}");
+  if (c->stream) CK(cudaStreamSynchronize(c->stream));
+  if (launch_mode != c->launch_mode || test_block != c->test_block ||
+      particles_per_thread != c->ppt || pair_waves != c->pair_waves)
+    drop_graphs(c);
+  c->launch_mode = launch_mode;
+  c->test_block = test_block;
+  c->ppt = particles_per_thread;
+  c->pair_waves = pair_waves;
+  return DEM_OK;
+}
+
+int dem_get_launch_shape(dem_ctx* c, int32_t* launch_mode, int32_t* test_block,
+                         int32_t* particles_per_thread, int32_t* pair_waves) {
+  if (!c) return DEM_ERR_INVALID;
+  if (launch_mode) *launch_mode = c->launch_mode;
+  if (test_block) *test_block = c->test_block;
+  if (particles_per_thread) *particles_per_thread = c->ppt;
+  if (pair_waves) *pair_waves = c->pair_waves;
+  return DEM_OK;
+}
+
+int dem_set_persistent_barrier(dem_ctx* c, double timeout_ms, int32_t extra_blocks) {
+  if (!c) return DEM_ERR_INVALID;
+  if (!(timeout_ms > 0.0 && timeout_ms <= 60000.0) || extra_blocks < 0 || extra_blocks > 1024)
+    return fail(c, DEM_ERR_INVALID, "barrier timeout in (0, 60000] ms, extra blocks in [0, 1024]");
+  c->bar_limit_ns = (unsigned long long)(timeout_ms * 1e6);
+  c->bar_extra = extra_blocks;
+  return DEM_OK;
+}
+
+int dem_get_persistent_blocks(dem_ctx* c, int32_t* blocks) {
+  if (!c) return DEM_ERR_INVALID;
+  if (blocks) *blocks = c->chunk_blocks;
+  return DEM_OK;
+}
+
 int dem_autotune(dem_ctx* c, int32_t first_step, int32_t steps_per_trial, int32_t* last_step,
                  double* trial_ms) {
   if (!c || steps_per_trial < 4) return DEM_ERR_INVALID;
   int st = validate_ready(c);
   if (st) return st;
   const double skins[3] = {0.025, 0.05, 0.1};
-  const int trials = 9;
-  const int timed_steps = (steps_per_trial + 3) / 4 * 4;  // whole graph chunks
+  const int timed_steps = (steps_per_trial + 3) / 4 * 4;  // whole chunks
   int step = first_step;
   double best_ms = 1e300;
-  int best = 0;
-  for (int t = 0; t < trials; t++) {
-    st = dem_set_tuning(c, skins[t / 3], t % 3);
-    if (st) return st;
-    // one untimed chunk takes the graph capture and the forced full rebuild
-    st = dem_run(c, step, step + 3);
-    if (st) return st;
+  // one trial: an untimed chunk takes the graph capture (or the chunk's
+  // recording) and the forced full rebuild, then the timed steps
+  auto trial = [&](int t, double& ms) -> int {
+    int s2 = dem_run(c, step, step + 3);
+    if (s2) return s2;
     step += 4;
-    double ms = 0.0;
-    st = dem_run_timed(c, step, step + timed_steps - 1, &ms);
-    if (st) return st;
+    s2 = dem_run_timed(c, step, step + timed_steps - 1, &ms);
+    if (s2) return s2;
     step += timed_steps;
     if (trial_ms) trial_ms[t] = ms;
+    return DEM_OK;
+  };
+  int mode = 0, tb = 128, ppt = 1, waves = 2;
+  st = dem_set_launch_shape(c, mode, tb, ppt, waves);
+  if (st) return st;
+  // skin x pair variant
+  int best = 0;
+  for (int t = 0; t < 9; t++) {
+    st = dem_set_tuning(c, skins[t / 3], t % 3);
+    if (st) return st;
+    double ms = 0.0;
+    st = trial(t, ms);
+    if (st) return st;
     if (ms < best_ms) {
       best_ms = ms;
       best = t;
     }
   }
   st = dem_set_tuning(c, skins[best / 3], best % 3);
+  if (st) return st;
+  // then one launch-shape knob at a time
+  struct Knob {
+    int* var;
+    int values[2];
+  } knobs[3] = {{&ppt, {2, 4}}, {&tb, {64, 256}}, {&waves, {1, 4}}};
+  int t = 9;
+  for (const Knob& k : knobs) {
+    const int keep = *k.var;
+    int chosen = keep;
+    for (int v : k.values) {
+      *k.var = v;
+      st = dem_set_launch_shape(c, mode, tb, ppt, waves);
+      if (st) return st;
+      double ms = 0.0;
+      st = trial(t++, ms);
+      if (st) return st;
+      if (ms < best_ms) {
+        best_ms = ms;
+        chosen = v;
+      }
+    }
+    *k.var = chosen;
+  }
+  // persistent chunks
+  st = dem_set_launch_shape(c, 1, tb, ppt, waves);
+  if (st) return st;
+  if (chunk_persistent(c)) {
+    double ms = 0.0;
+    st = trial(t, ms);
+    if (st) return st;
+    if (ms < best_ms) {
+      best_ms = ms;
+      mode = 1;
+    }
+  } else if (trial_ms) {
+    trial_ms[t] = -1.0;
+  }
+  st = dem_set_launch_shape(c, mode, tb, ppt, waves);
   if (st) return st;
   if (last_step) *last_step = step - 1;
   return DEM_OK;

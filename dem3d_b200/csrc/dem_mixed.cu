@@ -14,28 +14,11 @@
 //    the predictor/corrector stay FP64.
 // This translation unit may fuse multiply-adds.
 #include "dem_mixed.cuh"
-#include "dem_pass.cuh"
+#include "dem_test.cuh"
 
 namespace dem {
 
 namespace {
-
-struct MixedView {
-  // history values [n*cap]: a = (ft.xyz, vt.x) b = (vt.yz, lo.xy) c = lo.z
-  const float4* ra;
-  const float4* rb;
-  const float* rc;
-  float4* wa;
-  float4* wb;
-  float* wc;
-  // wall history values [n*nw], same packing
-  const float4* rwa;
-  const float4* rwb;
-  const float* rwc;
-  float4* wwa;
-  float4* wwb;
-  float* wwc;
-};
 
 struct F3 {
   float x, y, z;
@@ -241,15 +224,16 @@ __device__ __forceinline__ void rec_write(float4* a, float4* b, float* c, size_t
 constexpr int KSPEC = 2;  // record keys read before the record count is known
 
 // The pair kernel: one thread per contact, grid-stride over the list.
-template <bool PP, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_pair_mixed(PassArgs<float4, float2> A,
-                                                          MixedView V) {
+// (Body for block `vblock` of a grid of `vgrid` blocks.)
+template <bool PP>
+__device__ __forceinline__ void pair_mixed_body(const PassArgs<float4, float2>& A,
+                                                const MixedView& V, int vblock, int vgrid) {
   __shared__ int s_abort;
   if (threadIdx.x == 0) s_abort = A.cnt->abort;
   __syncthreads();
   if (s_abort) return;
   const int total = A.cnt->n_contacts;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (vblock == 0 && threadIdx.x == 0) {
     // the pass's pair contacts: the length of its contact list
     atomicAdd(&A.cnt->pair_contacts, (unsigned long long)total);
     atomicMax(&A.cnt->need_cl, total);
@@ -261,8 +245,7 @@ __global__ void __launch_bounds__(128, MINB) k_pair_mixed(PassArgs<float4, float
   unsigned n_col = 0;
   int need = 0, need_in = 0;
   bool overflow = false, in_over = false;
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < total;
-       s += gridDim.x * blockDim.x) {
+  for (int s = vblock * blockDim.x + threadIdx.x; s < total; s += vgrid * blockDim.x) {
     const int2 e = A.clist[s];
     const int p = e.x, q = e.y;
     const int s_in = atomicAdd(&A.in_cnt[q], 1);  // q's "j" record (returns early)
@@ -348,11 +331,19 @@ __global__ void __launch_bounds__(128, MINB) k_pair_mixed(PassArgs<float4, float
   publish_counts_block(A.cnt, update, n_col, 0u, 0u, (unsigned)need, (unsigned)need_in);
 }
 
+template <bool PP, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_pair_mixed(PassArgs<float4, float2> A,
+                                                          MixedView V) {
+  pair_mixed_body<PP>(A, V, blockIdx.x, gridDim.x);
+}
+
 // The fold kernel: p's block of the sweep, Force and Torque in sweep order
 // (FP32), a = F/m, alpha = T/I, then the FP64 integrator epilogue.  WALLS:
-// some system has walls; CONE: some wall is a cone.
+// some system has walls; CONE: some wall is a cone.  (Body for block
+// `vblock` of particles.)
 template <bool PP, int EPI, bool WALLS, bool CONE>
-__global__ void __launch_bounds__(128, 5) k_fold_mixed(PassArgs<float4, float2> A, MixedView V) {
+__device__ __forceinline__ void fold_mixed_body(const PassArgs<float4, float2>& A,
+                                                const MixedView& V, int vblock) {
   __shared__ float s_w[WALLS ? NWM : 1][128];  // |FN| of each wall contact
   __shared__ int s_abort;
   // one decision for the whole block (it meets block barriers later)
@@ -361,8 +352,8 @@ __global__ void __launch_bounds__(128, 5) k_fold_mixed(PassArgs<float4, float2> 
   if (s_abort) return;
   if (WALLS)
     for (int w = 0; w < A.nw_max; w++) s_w[w][threadIdx.x] = 0.f;
-  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.cnt->pass_id, 1);  // this pass is done
-  const int p0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (vblock == 0 && threadIdx.x == 0) atomicAdd(&A.cnt->pass_id, 1);  // this pass is done
+  const int p0 = vblock * blockDim.x + threadIdx.x;
   const bool valid = p0 < A.n;
   const int p = valid ? p0 : 0;
   const bool update = A.update != 0;
@@ -511,13 +502,58 @@ __global__ void __launch_bounds__(128, 5) k_fold_mixed(PassArgs<float4, float2> 
     }
     epilogue<EPI>(A, P, p, xp, Rpd, vd, wd, acc, alp, c, d2);
   }
-  if (WALLS && A.nw_max > 0) wall_partials(s_w, A.nw_max, A.wall_part, blockIdx.x);
+  if (WALLS && A.nw_max > 0) wall_partials(s_w, A.nw_max, A.wall_part, vblock);
   if (overflow) {
     atomicExch(&A.cnt->overflow, 1);
     set_abort(A.cnt, A.tag);
   }
   publish_counts_block(A.cnt, update, 0u, 0u, n_wc, (unsigned)need, 0u);
   if (EPI != EPI_STORE) publish_disp_block(A.cnt, d2);
+}
+
+// (STRIDE: grid-stride over blocks of 128 particles)
+template <bool PP, int EPI, bool WALLS, bool CONE, bool STRIDE>
+__global__ void __launch_bounds__(128, 5) k_fold_mixed(PassArgs<float4, float2> A, MixedView V) {
+  if (!STRIDE) {
+    fold_mixed_body<PP, EPI, WALLS, CONE>(A, V, blockIdx.x);
+    return;
+  }
+  const int nvb = (A.n + 127) / 128;
+  for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
+    fold_mixed_body<PP, EPI, WALLS, CONE>(A, V, vb);
+    __syncthreads();  // the block's shared arrays are reused by the next block of particles
+  }
+}
+
+// The persistent chunk kernel (mixed): k_chunk_fp64's structure with the
+// mixed pair and fold bodies.  The relink and test bodies are the FP64
+// unit's code, written with explicitly rounded operations, so this unit's
+// contraction and approximate division do not reach them.
+using ChunkPassMx = ChunkPass<float4, float2, MixedView>;
+
+template <bool PP, bool WALLS, bool CONE>
+__global__ void __launch_bounds__(128, 4) k_chunk_mixed(const ChunkPassMx* __restrict__ prog,
+                                                        int npass, GridSync g) {
+  __shared__ ChunkPassMx sp;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nthreads = gridDim.x * blockDim.x;
+  for (int k = 0; k < npass; k++) {
+    load_pass(sp, prog + k);
+    const RelinkArgs& R = sp.rl;
+    relink_body(R.PT, R.cellsys, R.L, R.par, R.n, R.update, R.stop_tag, R.cnt, tid, nthreads);
+    if (!grid_sync(g)) return;
+    const int nvb = (sp.t.n + 127) / 128;
+    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) test_body<PP, false>(sp.t, vb);
+    if (!grid_sync(g)) return;
+    pair_mixed_body<PP>(sp.a, sp.v, blockIdx.x, gridDim.x);
+    if (!grid_sync(g)) return;
+    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
+      if (sp.epi == EPI_PREDICT) fold_mixed_body<PP, EPI_PREDICT, WALLS, CONE>(sp.a, sp.v, vb);
+      else fold_mixed_body<PP, EPI_CORRECT, WALLS, CONE>(sp.a, sp.v, vb);
+      __syncthreads();
+    }
+    if (!grid_sync(g)) return;  // (also: every block is done with sp)
+  }
 }
 
 // FP64 records <-> FP32 records
@@ -578,6 +614,29 @@ __global__ void k_mixed_regrow(int n, int ns, int nd, const int* cnt, const floa
 }
 
 unsigned blocks(long long n, int b) { return (unsigned)((n + b - 1) / b); }
+
+// blocks of a cooperative launch of `k`: as many as fit on the device at
+// once (occupancy x SMs), at most `want`
+template <class K>
+int coop_blocks(K k, int want) {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, 128, 0);
+  const int most = per * sms;
+  return want < most ? want : most;
+}
+
+template <class K>
+cudaError_t launch_chunk(K k, const ChunkPassMx* prog, int npass, GridSync g, int want,
+                         cudaStream_t st, int* blocks_out) {
+  const int nb = coop_blocks(k, want);
+  if (nb <= 0) return cudaErrorLaunchOutOfResources;
+  g.expected += (unsigned)nb;  // (on entry: the blocks a test adds to every barrier)
+  void* args[] = {(void*)&prog, (void*)&npass, (void*)&g};
+  if (blocks_out) *blocks_out = nb;
+  return cudaLaunchCooperativeKernel((const void*)k, dim3(nb), dim3(128), args, 0, st);
+}
 
 }  // namespace
 
@@ -671,10 +730,7 @@ bool mixed_grow_walls(MixedBuffers& M, int n, int stride, int cur, cudaStream_t 
   return true;
 }
 
-void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant, bool walls, bool cone,
-                const PassArgs<float4, float2>& A, int cur, cudaStream_t st, int part,
-                unsigned pair_blocks) {
-  if (A.n == 0) return;
+MixedView mixed_view(const MixedBuffers& M, int cur) {
   MixedView V;
   V.ra = M.ha[cur];
   V.rb = M.hb[cur];
@@ -688,6 +744,14 @@ void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant, bool walls, bool
   V.wwa = M.wa[cur ^ 1];
   V.wwb = M.wb[cur ^ 1];
   V.wwc = M.wc[cur ^ 1];
+  return V;
+}
+
+void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant, bool walls, bool cone,
+                const PassArgs<float4, float2>& A, int cur, cudaStream_t st, int part,
+                unsigned pair_blocks, int ppt) {
+  if (A.n == 0) return;
+  const MixedView V = mixed_view(M, cur);
   if (part == 0) {
 #define PCASE(PPV, MB) k_pair_mixed<PPV, MB><<<pair_blocks, 128, 0, st>>>(A, V)
     if (variant == 1) {
@@ -703,12 +767,21 @@ void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant, bool walls, bool
 #undef PCASE
     return;
   }
-  const unsigned g = blocks(A.n, 128);
-#define FCASE(PPV, W, CN)                                                                     \
-  do {                                                                                        \
-    if (epi == EPI_PREDICT) k_fold_mixed<PPV, EPI_PREDICT, W, CN><<<g, 128, 0, st>>>(A, V);  \
-    else if (epi == EPI_CORRECT) k_fold_mixed<PPV, EPI_CORRECT, W, CN><<<g, 128, 0, st>>>(A, V); \
-    else k_fold_mixed<PPV, EPI_STORE, W, CN><<<g, 128, 0, st>>>(A, V);                        \
+  const unsigned nvb = blocks(A.n, 128);
+  const bool stride = ppt > 1 && epi != EPI_STORE;
+  const unsigned g = stride ? (nvb + ppt - 1) / ppt : nvb;
+#define FK(PPV, E, W, CN, S) k_fold_mixed<PPV, E, W, CN, S><<<g, 128, 0, st>>>(A, V)
+#define FCASE(PPV, W, CN)                          \
+  do {                                             \
+    if (epi == EPI_PREDICT) {                      \
+      if (stride) FK(PPV, EPI_PREDICT, W, CN, true); \
+      else FK(PPV, EPI_PREDICT, W, CN, false);     \
+    } else if (epi == EPI_CORRECT) {               \
+      if (stride) FK(PPV, EPI_CORRECT, W, CN, true); \
+      else FK(PPV, EPI_CORRECT, W, CN, false);     \
+    } else {                                       \
+      FK(PPV, EPI_STORE, W, CN, false);            \
+    }                                              \
   } while (0)
   if (!walls) {
     if (pp) FCASE(true, false, false);
@@ -721,6 +794,25 @@ void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant, bool walls, bool
     else FCASE(false, true, false);
   }
 #undef FCASE
+#undef FK
+}
+
+cudaError_t mixed_chunk(bool pp, bool walls, bool cone,
+                        const ChunkPass<float4, float2, MixedView>* prog, int npass, GridSync g,
+                        int want_blocks, cudaStream_t st, int* blocks_out) {
+#define CCASE(PPV, W, CN) \
+  return launch_chunk(k_chunk_mixed<PPV, W, CN>, prog, npass, g, want_blocks, st, blocks_out)
+  if (!walls) {
+    if (pp) CCASE(true, false, false);
+    CCASE(false, false, false);
+  }
+  if (cone) {
+    if (pp) CCASE(true, true, true);
+    CCASE(false, true, true);
+  }
+  if (pp) CCASE(true, true, false);
+  CCASE(false, true, false);
+#undef CCASE
 }
 
 void mixed_import_history(MixedBuffers& M, const History& H, int n, int nw, int cur,

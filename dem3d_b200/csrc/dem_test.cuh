@@ -1,0 +1,561 @@
+// dem_test.cuh -- the precision-independent parts of a force pass: the
+// relink of the cell lists, the candidate rows and the exact overlap test.
+// Both translation units include them (the FP64 one, compiled without
+// floating-point contraction, and the mixed one, compiled with it and with
+// approximate division and square root), so every floating-point operation
+// here is written with an explicitly rounded intrinsic (__dadd_rn,
+// __dsub_rn, __dmul_rn, __dsqrt_rn): the candidate rows and the contact
+// lists are the same bits in either unit, and equal to the reference's
+// (src/MForces.f90:218-224 tests DeltaDijSq = MinDijSq - DijSq > 0 in FP64).
+#pragma once
+#include "dem_pass.cuh"
+
+namespace dem {
+
+// min_image_exact, sumsq3 and the pair's MinDijSq with every operation
+// rounded on its own (no contraction into fused multiply-adds)
+__device__ __forceinline__ double min_image_rn(double r, const Box& B, int k) {
+  if (B.pbc[k] && !(fabs(r) < B.half_lim[k]))
+    r = __dsub_rn(r, __dmul_rn(B.lbox[k], (double)(int)round(__dmul_rn(r, B.inv_lbox[k]))));
+  return r;
+}
+__device__ __forceinline__ double sumsq3_rn(const double a[3]) {
+  double c = 0.0;
+  c = __dadd_rn(c, __dmul_rn(a[0], a[0]));
+  c = __dadd_rn(c, __dmul_rn(a[1], a[1]));
+  c = __dadd_rn(c, __dmul_rn(a[2], a[2]));
+  return c;
+}
+// MinDijSq of a pair: the material table (components ca, cb), or (Ra + Rb)^2
+// for per-particle radii (PP)
+template <bool PP>
+__device__ __forceinline__ double min_dij_sq_rn(const DevParams& P, int ca, double Ra, int cb,
+                                                double Rb) {
+  if (PP) {
+    const double d = __dadd_rn(Ra, Rb);
+    return __dmul_rn(d, d);
+  }
+  return P.min_dij_sq[ca * NCM + cb];
+}
+
+// Relink (RedistributeParticles3D's list updates, src/MCells.f90:607-643):
+// one thread per dirty cell of list `par` drops the particles that left it
+// (TransferParticle's unlink, :747-774) and prepends its arrivals in
+// decreasing index (AddParticle, :684-698, applied in increasing index
+// order), then marks its 27-cell neighbourhood for candidate-row repair.
+// The walk over the old list follows a leaver's successor saved when it
+// moved (mnext), so no thread reads a link that another thread rewrites.
+// Thread 0 also closes the previous pass's bookkeeping and decides whether
+// this pass rebuilds every candidate row.
+// (The body of k_relink; tid / nthreads: this thread's index in the grid and
+// the grid's thread count, so that a persistent kernel can run it too.)
+__device__ __forceinline__ void relink_body(const DevParams* __restrict__ PT,
+                                            const int* __restrict__ cellsys, const CellLists& L,
+                                            int par, int n, int update, int stop_tag,
+                                            Counters* cnt, int tid, int nthreads) {
+  if (cnt->abort) return;
+  // inside a captured chunk, particles that left the box in the last step
+  // stop the chunk before this step (the host runs UpdateParticleList); the
+  // count is final here (written by the previous kernel), so every block
+  // takes the same branch
+  if (stop_tag >= 0 && cnt->escaped != 0ull) {
+    if (tid == 0) {
+      cnt->escape_stop = 1;
+      set_abort(cnt, stop_tag);
+    }
+    return;
+  }
+  if (tid == 0) {
+    const DevParams& P = PT[0];  // the integrator settings are shared
+    cnt->n_repair = 0;
+    cnt->n_dirty[par ^ 1] = 0;
+    cnt->movers = cnt->movers_pending;
+    cnt->movers_pending = 0ull;
+    if (cnt->ncol_pending) {  // the previous history-updating pass completed
+      cnt->ncol += cnt->ncol_pending;
+      cnt->ncol_pending = 0ull;
+    }
+    cnt->pair_contacts = 0ull;
+    cnt->wall_contacts = 0ull;
+    cnt->n_contacts = 0;  // the contact list of this pass starts empty
+    if (update) {
+      cnt->need_capacity = 0;
+      cnt->need_in = 0;
+      cnt->need_cl = 0;
+    } else {
+      cnt->escaped = 0ull;  // escapes are counted by the current step's corrector
+    }
+    const double d = (double)__uint_as_float(cnt->disp_max);
+    cnt->disp_max = 0u;
+    const double acc = cnt->disp_acc + d;
+    const int full = cnt->force_full != 0 || !(acc <= P.vl_thr);
+    cnt->full_due = full;
+    cnt->disp_acc = full ? 0.0 : acc;
+    if (full) cnt->force_full = 0;
+  }
+  const int m = cnt->n_dirty[par];
+  const int stamp = cnt->pass_id + 1;  // fold kernels advance pass_id, not this one
+  const int* __restrict__ cell_new = L.cell[par];
+  for (int i = tid; i < m; i += nthreads) {
+    const int c = L.dlist[par][i];
+    // 1. unlink the leavers
+    int prev = -1, first = -1, q = L.head[c];
+    int guard = 0;
+    while (q != -1) {
+      if (++guard > n) {
+        atomicExch(&cnt->list_error, 1);
+        atomicExch(&cnt->abort, 1);
+        return;
+      }
+      const bool stays = cell_new[q] == c;
+      const int nq = stays ? L.next[q] : L.mnext[q];
+      if (stays) {
+        if (prev == -1) first = q;
+        else L.next[prev] = q;
+        prev = q;
+      }
+      q = nq;
+    }
+    if (prev != -1) L.next[prev] = -1;
+    // 2. prepend the arrivals, highest index first
+    int sh = -1, tail = -1, a = L.arr_head[c];
+    guard = 0;
+    while (a != -1) {
+      if (++guard > n) {
+        atomicExch(&cnt->list_error, 1);
+        atomicExch(&cnt->abort, 1);
+        return;
+      }
+      const int an = L.arr_next[a];
+      L.mflag[a] = 0;
+      if (sh == -1) {
+        sh = tail = a;
+        L.next[a] = -1;
+      } else if (a > sh) {
+        L.next[a] = sh;
+        sh = a;
+      } else {
+        int q2 = sh;
+        for (int g2 = 0; L.next[q2] != -1 && L.next[q2] > a && g2 < guard; g2++) q2 = L.next[q2];
+        L.next[a] = L.next[q2];
+        L.next[q2] = a;
+        if (L.next[a] == -1) tail = a;
+      }
+      a = an;
+    }
+    L.arr_head[c] = -1;
+    if (sh != -1) {
+      L.next[tail] = first;
+      first = sh;
+    }
+    L.head[c] = first;
+    L.dflag[c] = 0;
+    // 3. the rows of every particle around c are rebuilt in this pass (by
+    // the test kernel): the 27 cells are stamped with the pass
+    const DevParams& P = sys_params(PT, cellsys, c);
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const int cl = c - P.coff;
+    const int cx = cl % nx, cy = (cl / nx) % ny, cz = cl / (nx * ny);
+#pragma unroll
+    for (int o = 0; o < 27; o++) {
+      const int jx = cx + o % 3 - 1, jy = cy + (o / 3) % 3 - 1, jz = cz + o / 9 - 1;
+      const bool ok = (P.pbc[0] || (jx >= 0 && jx < nx)) && (P.pbc[1] || (jy >= 0 && jy < ny)) &&
+                      (P.pbc[2] || (jz >= 0 && jz < nz));
+      if (ok)
+        L.rflag[P.coff + axis_wrap(jx, nx, P.pbc[0]) +
+                nx * (axis_wrap(jy, ny, P.pbc[1]) + ny * axis_wrap(jz, nz, P.pbc[2]))] = stamp;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K2: candidate rows
+
+// The row of particle p (cell c), built by one warp.  Lane L < 27 owns the
+// neighbour cell at offset (L%3-1, L/3%3-1, L/9-1); lane 13 (own cell) walks
+// the part of the list after p, lane 27 the part before p (p's rank).  The
+// row holds the partners the sweep meets with p as "i": the own cell after p,
+// then the half-shell cells (offset index kx + Nx*(ky + Ny*kz) > 0,
+// AddAllNeighbours3D src/MCells.f90:456) in FirstNeighbour order, i.e.
+// descending (kz, ky, kx) -- NeighbourParticles' list (src/MCells.f90:
+// 793-829) from p on.
+template <bool PP>
+__device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int c,
+                                          const double4* __restrict__ X,
+                                          const int* __restrict__ comp,
+                                          const int* __restrict__ head,
+                                          const int* __restrict__ next, const Rows& R,
+                                          Counters* cnt, int tag) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  const int cl = c - P.coff;
+  const int cx = cl % nx, cy = (cl / nx) % ny, cz = cl / (nx * ny);
+  const double4 p4 = X[p];
+  const int cp = PP ? 0 : comp[p];
+  int start = -1, order = 1 << 20;
+  bool walk = false;
+  if (lane < 27) {
+    const int d[3] = {lane % 3 - 1, (lane / 3) % 3 - 1, lane / 9 - 1};
+    const int cc[3] = {cx, cy, cz};
+    const int N[3] = {nx, ny, nz};
+    bool ok = true;
+    int w[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      int j = cc[k] + d[k];
+      if (P.pbc[k]) {
+        if (j == N[k]) j = 0;
+        if (j == -1) j = N[k] - 1;
+      } else if (j < 0 || j >= N[k]) {
+        ok = false;
+      }
+      w[k] = j;
+    }
+    const int lex = d[0] + 3 * d[1] + 9 * d[2];
+    if (lane == 13) {
+      start = next[p];
+      order = 0;
+      walk = true;
+    } else if (ok && lex > 0) {
+      start = head[P.coff + w[0] + nx * (w[1] + ny * w[2])];
+      order = 1 + (13 - lex);
+      walk = true;
+    }
+  }
+  const double skin = P.vl_skin;
+  auto is_cand = [&](int q) -> bool {
+    const double4 q4 = X[q];
+    double Rij[3] = {__dsub_rn(q4.x, p4.x), __dsub_rn(q4.y, p4.y), __dsub_rn(q4.z, p4.z)};
+#pragma unroll
+    for (int k = 0; k < 3; k++) Rij[k] = min_image_rn(Rij[k], P.box, k);
+    const double DijSq = sumsq3_rn(Rij);
+    double md;
+    if (PP) md = __dadd_rn(p4.w, q4.w);
+    else md = __dsqrt_rn(min_dij_sq_rn<PP>(P, cp, p4.w, comp[q], q4.w));
+    md = __dadd_rn(md, skin);
+    return __dsub_rn(__dmul_rn(md, md), DijSq) > 0.0;
+  };
+  // pass 1: walk and count; the first 8 list elements and their test
+  // results stay in registers for pass 2.  Lane 27 counts the list before p.
+  int count = 0, walked = 0;
+  unsigned hits = 0u;
+  int cache[8];
+  bool bad = false;
+  int q = start;
+#pragma unroll
+  for (int i = 0; i < 8; i++) cache[i] = -1;
+  if (walk) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      if (q != -1) {
+        cache[i] = q;
+        walked = i + 1;
+        if (is_cand(q)) {
+          hits |= 1u << i;
+          count++;
+        }
+        q = next[q];
+      }
+    }
+  }
+  const int resume = q;  // first element not cached (-1: none)
+  {
+    int guard = 0;
+    if (walk) {
+      while (q != -1) {
+        if (++guard > n) {
+          bad = true;
+          break;
+        }
+        if (is_cand(q)) count++;
+        q = next[q];
+      }
+    } else if (lane == 27) {
+      q = head[c];
+      while (q != p) {
+        if (q == -1 || ++guard > n) {
+          bad = true;
+          break;
+        }
+        count++;
+        q = next[q];
+      }
+    }
+  }
+  if (__any_sync(FULL, bad)) {
+    if (lane == 0) {
+      atomicExch(&cnt->list_error, 1);
+      set_abort(cnt, tag);
+    }
+    return;
+  }
+  int off = 0, m = 0;
+  for (int l = 0; l < 27; l++) {
+    const int ol = __shfl_sync(FULL, order, l);
+    const int cl2 = __shfl_sync(FULL, walk ? count : 0, l);
+    if (ol < order) off += cl2;
+    m += cl2;
+  }
+  const int rank = __shfl_sync(FULL, count, 27);
+  if (m > R.kc) {
+    if (lane == 0) {
+      atomicMax(&cnt->need_kc, m);
+      atomicExch(&cnt->row_overflow, 1);
+      set_abort(cnt, tag);
+      R.meta[p] = 0;
+    }
+    return;
+  }
+  // pass 2: write (the cached part, then the rest of the list)
+  if (walk) {
+    int k = off;
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+      if (i < walked && ((hits >> i) & 1u)) R.cand[(size_t)(k++) * n + p] = cache[i];
+    int q2 = resume;
+    while (q2 != -1) {
+      if (is_cand(q2)) R.cand[(size_t)(k++) * n + p] = q2;
+      q2 = next[q2];
+    }
+  }
+  if (lane == 0) {
+    R.meta[p] = m;
+    R.rank[p] = rank;
+  }
+}
+
+
+// Arguments of the test kernel (the same for both precisions).
+struct TestArgs {
+  const DevParams* P;
+  const int* sysid;
+  int n;
+  const int* cell_cur;  // cell of every particle in this pass
+  CellLists L;
+  Rows R;
+  const double4* X;
+  const int* comp;
+  const int* cand;
+  const int* meta;
+  int2* clist;
+  int* cstart;
+  int* ccount;
+  int cl_cap;
+  Counters* cnt;
+  int tag;
+};
+
+// First, the candidate rows of the warp's particles that this pass rebuilds
+// (every row on a full rebuild, else the rows of the particles whose cell the
+// relink stamped with this pass) are built, one particle at a time by the
+// whole warp (build_row).  (No block barriers: every warp runs on its own.
+// The pass's contact count and the list length it needs come from the pair
+// kernel, or from here when the list overflows.)
+// (The body of k_test for block `vblock`, so that a persistent kernel can
+// run it too.  NC: candidates read through the non-coherent path, which
+// needs the rows unchanged for the whole launch except by the warp that
+// reads them; a kernel that runs several passes reads them coherently.)
+template <bool NC>
+__device__ __forceinline__ int ld_row(const int* a) {
+  return NC ? __ldg(a) : *a;
+}
+
+template <bool PP, bool NC = true>
+__device__ __forceinline__ void test_body(const TestArgs& A, int vblock) {
+  if (A.cnt->abort) return;
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int p0 = vblock * blockDim.x + threadIdx.x;
+  const bool valid = p0 < A.n;
+  const int p = valid ? p0 : 0;
+  const int n = A.n;
+  {
+    const bool full = A.cnt->full_due != 0;
+    const int stamp = A.cnt->pass_id + 1;
+    const int cp0 = A.cell_cur[p];
+    unsigned todo = __ballot_sync(FULL, valid && (full || A.L.rflag[cp0] == stamp));
+    while (todo) {
+      const int l = __ffs(todo) - 1;
+      todo &= todo - 1u;
+      const int pl = __shfl_sync(FULL, p, l);
+      const int cl = __shfl_sync(FULL, cp0, l);
+      build_row<PP>(sys_params(A.P, A.sysid, pl), n, pl, cl, A.X, A.comp, A.L.head, A.L.next,
+                    A.R, A.cnt, A.tag);
+    }
+    __syncwarp();  // the rows written by the warp are visible to their owners
+  }
+  // the first candidates are read before the row length is known (every
+  // row holds at least 4 entries' room)
+  int q0[4];
+#pragma unroll
+  for (int u = 0; u < 4; u++) q0[u] = ld_row<NC>(A.cand + (size_t)u * n + p);
+  const DevParams& P = sys_params(A.P, A.sysid, p);
+  const double4 p4 = A.X[p];
+  const int cp = PP ? 0 : A.comp[p];
+  const int m = valid ? (A.meta[p] & META_MASK) : 0;
+  // contact bit masks of the row, 64 candidates per window (windows past
+  // the first only for rows longer than 64)
+  unsigned long long mask0 = 0ull;
+  unsigned long long more[(KC_MAX + 1) / 64 - 1];
+  int total = 0;
+  for (int base = 0; base < m; base += 64) {
+    unsigned long long mask = 0ull;
+    const int end = m < base + 64 ? m : base + 64;
+#pragma unroll 1
+    for (int b = base; b < end; b += 4) {
+      int q[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        q[u] = b + u < end ? (b == 0 ? q0[u] : ld_row<NC>(A.cand + (size_t)(b + u) * n + p)) : -1;
+      double4 xq[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        xq[u] = q[u] >= 0 ? A.X[q[u]] : make_double4(0.0, 0.0, 0.0, 0.0);
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        if (q[u] < 0) continue;
+        double Rij[3] = {__dsub_rn(xq[u].x, p4.x), __dsub_rn(xq[u].y, p4.y),
+                         __dsub_rn(xq[u].z, p4.z)};
+#pragma unroll
+        for (int k = 0; k < 3; k++) Rij[k] = min_image_rn(Rij[k], P.box, k);
+        const double DijSq = sumsq3_rn(Rij);
+        const int cq = PP ? 0 : A.comp[q[u]];
+        if (__dsub_rn(min_dij_sq_rn<PP>(P, cp, p4.w, cq, xq[u].w), DijSq) > 0.0)
+          mask |= 1ull << (b + u - base);
+      }
+    }
+    total += __popcll(mask);
+    if (base == 0) mask0 = mask;
+    else more[base / 64 - 1] = mask;
+  }
+  // one allocation per warp; a particle's contacts are contiguous
+  int incl = total;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(FULL, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const int wsum = __shfl_sync(FULL, incl, 31);
+  int wbase = 0;
+  if (lane == 31 && wsum > 0) wbase = atomicAdd(&A.cnt->n_contacts, wsum);
+  wbase = __shfl_sync(FULL, wbase, 31);
+  const int start = wbase + incl - total;
+  if (valid) {
+    A.cstart[p] = start;
+    A.ccount[p] = total;
+  }
+  if (start + total > A.cl_cap) {
+    // the list is grown and the pass launched again
+    atomicMax(&A.cnt->need_cl, start + total);
+    atomicExch(&A.cnt->cl_overflow, 1);
+    set_abort(A.cnt, A.tag);
+  } else if (total > 0) {
+    int s = start;
+    for (int base = 0; base < m; base += 64) {
+      unsigned long long mask = base == 0 ? mask0 : more[base / 64 - 1];
+      while (mask) {
+        const int k = base + __ffsll((long long)mask) - 1;
+        mask &= mask - 1ull;
+        A.clist[s++] = make_int2(p, ld_row<NC>(A.cand + (size_t)k * n + p));
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Persistent launches: a 4-step chunk (8 force passes) as one cooperative
+// launch whose blocks step through every pass's phases (relink, test, pair,
+// fold), separated by grid-wide barriers.
+
+// Arguments of a relink (k_relink's parameters)
+struct RelinkArgs {
+  const DevParams* PT;
+  const int* cellsys;
+  CellLists L;
+  int par, n, update, stop_tag;
+  Counters* cnt;
+};
+
+// A grid-wide barrier over `expected` blocks (gridDim.x of a cooperative
+// launch, so that every block is resident): an arrival counter and a
+// generation word.  A block that waits longer than limit_ns nanoseconds
+// (%globaltimer) sets cnt->barrier_timeout and cnt->abort and reports
+// failure; its caller then returns, and the blocks still waiting give up in
+// turn, so the launch always ends.
+struct GridSync {
+  unsigned* count;
+  unsigned* gen;
+  Counters* cnt;
+  unsigned long long limit_ns;
+  unsigned expected;
+};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* a) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(a) : "memory");
+  return v;
+}
+
+// All threads of every block call; returns false after a timeout.
+__device__ __forceinline__ bool grid_sync(const GridSync& g) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned gen0 = ld_acquire_u32(g.gen);  // cannot advance before this block arrives
+    __threadfence();  // the block's writes before the arrival
+    if (atomicAdd(g.count, 1u) == g.expected - 1u) {
+      atomicExch(g.count, 0u);
+      __threadfence();
+      atomicAdd(g.gen, 1u);
+    } else {
+      const unsigned long long t0 = global_ns();
+      while (ld_acquire_u32(g.gen) == gen0) {
+        if (global_ns() - t0 > g.limit_ns) {
+          atomicExch(&g.cnt->barrier_timeout, 1);
+          atomicExch(&g.cnt->abort, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(100);
+      }
+    }
+    __threadfence();  // everything written before the other blocks arrived
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+struct NoView {};
+
+// One force pass of a chunk: its relink, test and pass arguments, the
+// integrator epilogue (EPI_PREDICT / EPI_CORRECT) and, for the mixed path,
+// the FP32 record arrays it reads and writes.  16-byte aligned: blocks copy
+// it into shared memory as int4.
+template <class V4, class W2, class View>
+struct alignas(16) ChunkPass {
+  RelinkArgs rl;
+  TestArgs t;
+  PassArgs<V4, W2> a;
+  View v;
+  int epi;
+};
+
+// the pass `src` into the block's shared copy `dst`
+template <class CP>
+__device__ __forceinline__ void load_pass(CP& dst, const CP* __restrict__ src) {
+  static_assert(sizeof(CP) % 16 == 0, "ChunkPass size");
+  const int4* a = reinterpret_cast<const int4*>(src);
+  int4* b = reinterpret_cast<int4*>(&dst);
+  for (int i = threadIdx.x; i < (int)(sizeof(CP) / 16); i += blockDim.x) b[i] = a[i];
+  __syncthreads();
+}
+
+}  // namespace dem

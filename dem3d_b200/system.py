@@ -420,14 +420,41 @@ class DEMSystem:
         self._call("get_tuning", C.byref(f), C.byref(v))
         return {"skin_factor": f.value, "pass_variant": v.value}
 
+    def set_launch_shape(self, launch_mode: int = 0, test_block: int = 128,
+                         particles_per_thread: int = 1, pair_waves: int = 2) -> None:
+        """dem_set_launch_shape: launch_mode 1 runs each 4-step chunk as one
+        persistent cooperative launch; the other knobs shape the test, fold
+        and pair kernels' grids.  No result depends on them."""
+        self._call("set_launch_shape", C.c_int32(launch_mode), C.c_int32(test_block),
+                   C.c_int32(particles_per_thread), C.c_int32(pair_waves))
+
+    def launch_shape(self):
+        v = [C.c_int32() for _ in range(4)]
+        self._call("get_launch_shape", *[C.byref(x) for x in v])
+        return dict(zip(("launch_mode", "test_block", "particles_per_thread", "pair_waves"),
+                        (x.value for x in v)))
+
+    def set_persistent_barrier(self, timeout_ms: float = 2000.0, extra_blocks: int = 0) -> None:
+        self._call("set_persistent_barrier", C.c_double(timeout_ms), C.c_int32(extra_blocks))
+
+    def persistent_blocks(self) -> int:
+        v = C.c_int32()
+        self._call("get_persistent_blocks", C.byref(v))
+        return v.value
+
+    AUTOTUNE_TRIALS = 16
+
     def autotune(self, first_step: int, steps_per_trial: int = 20):
-        """Runs nine timed trials on the live system (dem_autotune); returns
-        the last step advanced, the chosen setting and the trial times."""
+        """Runs the timed trials of dem_autotune on the live system; returns
+        the last step advanced, the chosen settings and the trial times
+        (skin x pair variant, then particles per thread, test block, pair
+        waves and the persistent launch)."""
         last = C.c_int32()
-        ms = (C.c_double * 9)()
+        ms = (C.c_double * self.AUTOTUNE_TRIALS)()
         self._call("autotune", C.c_int32(first_step), C.c_int32(steps_per_trial),
                    C.byref(last), ms)
-        return {"last_step": last.value, **self.tuning(), "trial_ms": list(ms)}
+        return {"last_step": last.value, **self.tuning(), **self.launch_shape(),
+                "trial_ms": list(ms)}
 
     def row_stats(self):
         """Candidate-row entries of the last pass and the row capacity."""

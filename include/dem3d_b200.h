@@ -375,11 +375,46 @@ int dem_get_row_stats(dem_ctx* ctx, int64_t* candidates, int32_t* row_capacity);
  * arithmetic is the same code. */
 int dem_set_tuning(dem_ctx* ctx, double skin_factor, int32_t pass_variant);
 int dem_get_tuning(dem_ctx* ctx, double* skin_factor, int32_t* pass_variant);
-/* Autotuner: advances the run from first_step through nine trials (skin
- * 0.025 / 0.05 / 0.1 x the three variants), each one untimed 4-step chunk and
- * steps_per_trial timed steps (rounded up to whole 4-step chunks), keeps the
- * fastest setting and returns the last step advanced and the nine trial times
- * (trial_ms may be NULL).  The trajectory is the one dem_run would produce. */
+/* Launch shape (no counterpart in the reference; changes no result: the
+ * same bodies run over the same particles and contacts, and every sum keeps
+ * its order).
+ *  - launch_mode: how dem_run issues its 4-step chunks.  0 (default): a
+ *    CUDA graph of the chunk's kernels (relink, test, pair, fold per force
+ *    pass: 8 launches per step).  1: one persistent cooperative launch per
+ *    chunk, as many blocks of 128 threads as fit on the GPU at once, which
+ *    step through the 8 passes' phases with grid-wide barriers between them
+ *    (every wait bounded: see dem_set_persistent_barrier).  Chunks with
+ *    moving walls, fluid drag or kernel profiling run as graphs.
+ *  - test_block: threads per block of the test kernel (64, 128 or 256).
+ *  - particles_per_thread: particles each thread of the test and fold
+ *    kernels takes in turn (1, 2 or 4): the grid holds 1/particles_per_thread
+ *    of the blocks and strides over them.
+ *  - pair_waves: the pair kernel's grid, in waves of the blocks an SM holds
+ *    (1, 2 or 4; contacts per thread = contacts / grid threads). */
+int dem_set_launch_shape(dem_ctx* ctx, int32_t launch_mode, int32_t test_block,
+                         int32_t particles_per_thread, int32_t pair_waves);
+int dem_get_launch_shape(dem_ctx* ctx, int32_t* launch_mode, int32_t* test_block,
+                         int32_t* particles_per_thread, int32_t* pair_waves);
+/* Grid-wide barriers of persistent chunks: every wait gives up after
+ * timeout_ms (default 2000), after which the chunk ends early, dem_run
+ * returns DEM_ERR_STATE and the state must be set again.  extra_blocks > 0
+ * is for tests only: every barrier then waits for that many blocks more
+ * than were launched, so the first wait runs out.  *blocks (may be NULL):
+ * blocks of the last persistent launch. */
+int dem_set_persistent_barrier(dem_ctx* ctx, double timeout_ms, int32_t extra_blocks);
+int dem_get_persistent_blocks(dem_ctx* ctx, int32_t* blocks);
+
+/* Autotuner: advances the run from first_step through DEM_AUTOTUNE_TRIALS
+ * trials, each one untimed 4-step chunk and steps_per_trial timed steps
+ * (rounded up to whole 4-step chunks), one knob at a time from the default
+ * launch shape: trials 0-8 the skin (0.025 / 0.05 / 0.1) x the three pair
+ * variants; from the best of those, 9-10 particles_per_thread 2 and 4,
+ * 11-12 test_block 64 and 256, 13-14 pair_waves 1 and 4, 15 launch_mode 1
+ * (trial time -1 where a chunk could not run persistent).  Each stage keeps
+ * a value only if it beat the best time so far.  Returns the last step
+ * advanced and the trial times (trial_ms may be NULL).  The trajectory is
+ * the one dem_run would produce. */
+#define DEM_AUTOTUNE_TRIALS 16
 int dem_autotune(dem_ctx* ctx, int32_t first_step, int32_t steps_per_trial,
                  int32_t* last_step, double* trial_ms);
 

@@ -2,7 +2,9 @@
 
 The candidate-row skin only changes which non-overlapping partners a row
 carries and how often rows are rebuilt; the pass-kernel variant only changes
-the register budget of the same code.  Trajectories must stay bit-identical."""
+the register budget of the same code; the launch shape (block size,
+particles per thread, pair grid, persistent chunks) only how the same code
+is launched.  Trajectories must stay bit-identical."""
 import numpy as np
 import pytest
 
@@ -27,9 +29,11 @@ def test_autotune_keeps_the_trajectory(precision):
     a, b = _system(precision), _system(precision)
     a.run(1, 8)
     t = a.autotune(9, 4)
-    assert t["last_step"] == 8 + 9 * 8
+    assert t["last_step"] == 8 + DEMSystem.AUTOTUNE_TRIALS * 8
     assert t["skin_factor"] in (0.025, 0.05, 0.1) and t["pass_variant"] in (0, 1, 2)
-    assert all(ms > 0 for ms in t["trial_ms"])
+    assert t["particles_per_thread"] in (1, 2, 4) and t["test_block"] in (64, 128, 256)
+    assert t["pair_waves"] in (1, 2, 4) and t["launch_mode"] in (0, 1)
+    assert all(ms > 0 for ms in t["trial_ms"])  # (the persistent trial ran too)
     b.run(1, t["last_step"])
     sa, sb = a.get_state(), b.get_state()
     for k in sa:
