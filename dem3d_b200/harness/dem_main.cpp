@@ -59,7 +59,8 @@ int main(int argc, char** argv) {
                pos.data(), vel.data(), omega.data());
     s.InitializeCellDistribution();
     if (pour_every > 0) s.SetPouring(pouring);
-    for (int step = 1; step <= p.method_order - 1 && step <= steps; step++) s.MoveParticlesEuler();
+    // MethodOrder-1 Euler steps whatever NumberOfSteps is (src/DEM.f90:88-90)
+    for (int step = 1; step <= p.method_order - 1; step++) s.MoveParticlesEuler();
     for (int step = p.method_order; step <= steps; step++) {
       if (pour_every > 0 && step % pour_every == 0) s.PourParticle();
       s.MoveParticles(step);

@@ -27,14 +27,16 @@ def build_main(out_dir):
     return exe
 
 
-def write_case(path, w, steps):
+def write_case(path, w, steps, pour=None):
     n = len(w.pos)
     with open(path, "wb") as f:
         f.write(bytes(w.params))
-        f.write(struct.pack("<4i", n, steps, 0, 0))
+        f.write(struct.pack("<4i", n, steps, pour.interval if pour is not None else 0, 0))
         f.write(np.ascontiguousarray(w.comp, dtype="<i4").tobytes())
         for a in (w.pos, w.vel, w.omega):
             f.write(np.ascontiguousarray(a, dtype="<f8").tobytes())
+        if pour is not None:
+            f.write(bytes(pour))
 
 
 def read_out(path):
@@ -84,3 +86,56 @@ def test_cpp_main_equals_the_oracle(tmp_path):
     np.testing.assert_array_equal(vel, st["vel"])
     np.testing.assert_array_equal(omega, st["omega"])
     assert ncol == o.ncol() > 0
+
+
+def _oracle_run(w, steps, pour=None):
+    from tests.oracle_lib import oracle_system
+    o = oracle_system(w.params)
+    o.set_state(w.pos, w.vel, w.omega, comp=w.comp)
+    o.initialize_cell_distribution()
+    if pour is not None:
+        o.set_pouring(pour)
+    o.run(1, steps)
+    return o
+
+
+@pytest.mark.gpu
+def test_cpp_main_fewer_steps_than_the_start_up(tmp_path):
+    """NumberOfSteps = 1 < MethodOrder - 1: the start-up still runs its
+    MethodOrder - 1 Euler steps (src/DEM.f90:88-90), as the oracle does."""
+    exe = build_main(str(tmp_path))
+    w = configs.settling(n=300, seed=2, sigma_v=0.5)
+    case, out = os.path.join(tmp_path, "case.bin"), os.path.join(tmp_path, "out.bin")
+    write_case(case, w, 1)
+    r = subprocess.run([exe, case, out], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    (pos, vel, omega), comp, ncol = read_out(out)
+    st = _oracle_run(w, 1).get_state()
+    np.testing.assert_array_equal(pos, st["pos"])
+    np.testing.assert_array_equal(vel, st["vel"])
+    assert not np.array_equal(pos, w.pos)
+
+
+@pytest.mark.gpu
+def test_cpp_main_pouring_equals_the_oracle(tmp_path):
+    """PouringAttempt before MoveParticles every IPouring steps, through the
+    C++ time loop: the same spheres go in at the same places."""
+    from types import SimpleNamespace
+    from tests.test_pouring import filling_box
+    exe = build_main(str(tmp_path))
+    prm, pos, comp, pour = filling_box(interval=4)
+    w = SimpleNamespace(params=prm, pos=pos, vel=np.zeros_like(pos), omega=np.zeros_like(pos),
+                        comp=comp)
+    case, out = os.path.join(tmp_path, "case.bin"), os.path.join(tmp_path, "out.bin")
+    write_case(case, w, 400, pour=pour)
+    r = subprocess.run([exe, case, out], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    (gpos, gvel, gomega), gcomp, ncol = read_out(out)
+    o = _oracle_run(w, 400, pour)
+    st = o.get_state()
+    assert len(gpos) == o.n > len(pos)
+    np.testing.assert_array_equal(gpos, st["pos"])
+    np.testing.assert_array_equal(gvel, st["vel"])
+    np.testing.assert_array_equal(gomega, st["omega"])
+    np.testing.assert_array_equal(gcomp, o.comp)
+    assert ncol == o.ncol()
