@@ -4,8 +4,11 @@ The library is compiled in-tree with nvcc (static CUDA runtime, so the .so
 only needs the driver at run time).  ``dem_lib.cu`` holds the FP64 path and is
 compiled with ``-fmad=false``: the exact path must not fuse multiply-adds,
 which is what makes it bit-identical to the reference arithmetic.  The
-mixed-precision kernels (``dem_mixed.cu``) may fuse multiply-adds and use the
-hardware's approximate FP32 division and square root.
+mixed-precision kernels (``dem_mixed.cu``) use the hardware's approximate FP32
+division and square root, and are compiled with ``-fmad=false`` too: with
+contraction left to the compiler, the same expression can be fused in one
+kernel and not in another that inlines the same code (the persistent chunk
+kernel), and the two launch modes would then differ in the last bits.
 """
 from __future__ import annotations
 
@@ -22,9 +25,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
           "-Xptxas", "-warn-spills"]
 # dem_mixed.cu: FP32 contact arithmetic within a stated 1e-5 tolerance, so
-# division and square root may use the hardware approximations (~1 ulp)
+# division and square root may use the hardware approximations (~1 ulp); no
+# contraction, so that every kernel that inlines the same code rounds alike
 SOURCES = [("dem_lib.cu", ["-fmad=false", "-Xcompiler", "-ffp-contract=off"]),
-           ("dem_mixed.cu", ["--prec-div=false", "--prec-sqrt=false"])]
+           ("dem_mixed.cu", ["-fmad=false", "--prec-div=false", "--prec-sqrt=false"])]
 
 
 def nvcc() -> str:

@@ -12,7 +12,9 @@
 //    increment is added with a compensated (Kahan/TwoSum) sum;
 //  - velocities are gathered as FP32 copies; positions, the ABM ring and
 //    the predictor/corrector stay FP64.
-// This translation unit may fuse multiply-adds.
+// This translation unit is compiled without multiply-add contraction (every
+// kernel that inlines the same code then rounds alike), with the hardware's
+// approximate FP32 division and square root.
 #include "dem_mixed.cuh"
 #include "dem_test.cuh"
 
@@ -528,7 +530,9 @@ __global__ void __launch_bounds__(128, 5) k_fold_mixed(PassArgs<float4, float2> 
 // The persistent chunk kernel (mixed): k_chunk_fp64's structure with the
 // mixed pair and fold bodies.  The relink and test bodies are the FP64
 // unit's code, written with explicitly rounded operations, so this unit's
-// contraction and approximate division do not reach them.
+// approximate division and square root do not reach them; this unit is
+// compiled without contraction, so the inlined pair and fold bodies round
+// exactly as in k_pair_mixed / k_fold_mixed.
 using ChunkPassMx = ChunkPass<float4, float2, MixedView>;
 
 template <bool PP, bool WALLS, bool CONE>

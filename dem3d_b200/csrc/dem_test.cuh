@@ -1,12 +1,13 @@
 // dem_test.cuh -- the precision-independent parts of a force pass: the
 // relink of the cell lists, the candidate rows and the exact overlap test.
-// Both translation units include them (the FP64 one, compiled without
-// floating-point contraction, and the mixed one, compiled with it and with
-// approximate division and square root), so every floating-point operation
-// here is written with an explicitly rounded intrinsic (__dadd_rn,
-// __dsub_rn, __dmul_rn, __dsqrt_rn): the candidate rows and the contact
-// lists are the same bits in either unit, and equal to the reference's
-// (src/MForces.f90:218-224 tests DeltaDijSq = MinDijSq - DijSq > 0 in FP64).
+// Both translation units include them (the FP64 one, compiled with IEEE
+// square root, and the mixed one, compiled with approximate division and
+// square root), so every floating-point operation here is written with an
+// explicitly rounded intrinsic (__dadd_rn, __dsub_rn, __dmul_rn,
+// __dsqrt_rn), which no compiler flag changes: the candidate rows and the
+// contact lists are the same bits in either unit, and equal to the
+// reference's (src/MForces.f90:218-224 tests DeltaDijSq = MinDijSq - DijSq
+// > 0 in FP64).
 #pragma once
 #include "dem_pass.cuh"
 
@@ -363,37 +364,47 @@ __device__ __forceinline__ int ld_row(const int* a) {
 
 template <bool PP, bool NC = true>
 __device__ __forceinline__ void test_body(const TestArgs& A, int vblock) {
-  if (A.cnt->abort) return;
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int p0 = vblock * blockDim.x + threadIdx.x;
   const bool valid = p0 < A.n;
   const int p = valid ? p0 : 0;
   const int n = A.n;
-  {
-    const bool full = A.cnt->full_due != 0;
-    const int stamp = A.cnt->pass_id + 1;
-    const int cp0 = A.cell_cur[p];
-    unsigned todo = __ballot_sync(FULL, valid && (full || A.L.rflag[cp0] == stamp));
-    while (todo) {
-      const int l = __ffs(todo) - 1;
-      todo &= todo - 1u;
-      const int pl = __shfl_sync(FULL, p, l);
-      const int cl = __shfl_sync(FULL, cp0, l);
-      build_row<PP>(sys_params(A.P, A.sysid, pl), n, pl, cl, A.X, A.comp, A.L.head, A.L.next,
-                    A.R, A.cnt, A.tag);
-    }
-    __syncwarp();  // the rows written by the warp are visible to their owners
-  }
-  // the first candidates are read before the row length is known (every
-  // row holds at least 4 entries' room)
+  // the abort word, the pass's rebuild decision, the particle's cell, own
+  // data, row length and first candidates are requested together (the first
+  // candidates before the row length is known: every row holds at least 4
+  // entries' room); nothing is written before the abort word is seen, and a
+  // warp whose rows were rebuilt reads them again
+  const int aborted = A.cnt->abort;
+  const bool full = A.cnt->full_due != 0;
+  const int stamp = A.cnt->pass_id + 1;
+  const int cp0 = A.cell_cur[p];
+  const double4 p4 = A.X[p];
+  const int cp = PP ? 0 : A.comp[p];
   int q0[4];
 #pragma unroll
   for (int u = 0; u < 4; u++) q0[u] = ld_row<NC>(A.cand + (size_t)u * n + p);
+  int meta = A.meta[p];
+  if (aborted) return;
+  {
+    unsigned todo = __ballot_sync(FULL, valid && (full || A.L.rflag[cp0] == stamp));
+    if (todo) {
+      while (todo) {
+        const int l = __ffs(todo) - 1;
+        todo &= todo - 1u;
+        const int pl = __shfl_sync(FULL, p, l);
+        const int cl = __shfl_sync(FULL, cp0, l);
+        build_row<PP>(sys_params(A.P, A.sysid, pl), n, pl, cl, A.X, A.comp, A.L.head, A.L.next,
+                      A.R, A.cnt, A.tag);
+      }
+      __syncwarp();  // the rows written by the warp are visible to their owners
+#pragma unroll
+      for (int u = 0; u < 4; u++) q0[u] = A.cand[(size_t)u * n + p];
+      meta = A.meta[p];
+    }
+  }
   const DevParams& P = sys_params(A.P, A.sysid, p);
-  const double4 p4 = A.X[p];
-  const int cp = PP ? 0 : A.comp[p];
-  const int m = valid ? (A.meta[p] & META_MASK) : 0;
+  const int m = valid ? (meta & META_MASK) : 0;
   // contact bit masks of the row, 64 candidates per window (windows past
   // the first only for rows longer than 64)
   unsigned long long mask0 = 0ull;
