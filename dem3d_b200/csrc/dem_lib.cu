@@ -858,8 +858,7 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
       timed(c, part ? "fold_mixed" : "pair_mixed", [&]() {
         mixed_pass(c->M, c->pp, epi, c->pass_variant, walls, c->has_cone, A, c->hcur, c->stream,
                    part, pair_blocks, c->ppt);
-      });
-      c->launches++;
+      });  // (timed counts the launch)
     }
     return;
   }
