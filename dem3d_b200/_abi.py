@@ -78,6 +78,10 @@ class DemWallMotion(C.Structure):
     ]
 
 
+# spatial decomposition: phases of a force pass and exchanges (dem3d_b200.h)
+SLAB_RELINK, SLAB_TEST_PAIR, SLAB_FOLD, SLAB_FINISH = 0, 1, 2, 3
+SLAB_GHOSTS, SLAB_LOWER, SLAB_JHALVES, SLAB_MIGRATE_UP, SLAB_MIGRATE_DOWN = 0, 1, 2, 3, 4
+
 POUR_RECTANGLE = 1
 POUR_CIRCLE = 2
 
@@ -189,6 +193,12 @@ GPU_ONLY = {
     "get_launch_shape": (C.c_int, [_P, _I32P, _I32P, _I32P, _I32P]),
     "set_persistent_barrier": (C.c_int, [_P, C.c_double, C.c_int32]),
     "get_persistent_blocks": (C.c_int, [_P, _I32P]),
+    "slab_set_range": (C.c_int, [_P, C.c_int32, C.c_int32]),
+    "slab_phase": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32]),
+    "slab_pack": (C.c_int, [_P, C.c_int32, _P, C.c_int64, _I64P]),
+    "slab_unpack": (C.c_int, [_P, C.c_int32, _P, C.c_int64]),
+    "slab_displacement": (C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "slab_owned": (C.c_int, [_P, _I32P]),
     # device pointers for positions and outputs; see the header
     "distribute_particles_noalloc": (C.c_int, [C.POINTER(DemParams), C.c_int32, _P, _P, _P, _P,
                                                _I32P, _P, C.c_char_p, C.c_int32]),

@@ -54,6 +54,10 @@ struct DevParams {
   Box box;                // lbox, inv_lbox, pbc again, with the minimum-image shortcut bound
   int coff, poff, np;     // first cell, first particle, particles of this system
   int sys;                // index of this system
+  // cells whose particles this context advances: [slab_c0, slab_c1), a
+  // range of whole z-layers (cells are numbered x + Nx*(y + Ny*z)); every
+  // cell of the system unless the context is one slab of a decomposition
+  int slab_c0, slab_c1;
   double comp_radius[NCM], comp_inv_mass[NCM], comp_inv_inertia[NCM], comp_eff_mass[NCM];
   double min_dij[NCM * NCM], min_dij_sq[NCM * NCM];
   double kn[NCM * NCM], yn[NCM * NCM], kt[NCM * NCM], yt[NCM * NCM], mu_sq[NCM * NCM];
@@ -261,7 +265,13 @@ struct PassArgs {
   // the most
   double* wall_part;
   int nw_max;
+  // a slab of a decomposition: the partner cells it knows this pass are its
+  // own slab's and those stamped gepoch in gstamp (the ghost layers it
+  // received); NULL: every cell is known
+  const int* gstamp;
+  int gepoch;
 };
+
 
 // The |FN| of every wall contact of a block of 128 particles, summed in a
 // fixed order (lanes of warp 0 over the four warps, then a shuffle tree):
@@ -624,6 +634,10 @@ __device__ __forceinline__ void cell_coords(const DevParams& P, int c, int& x, i
 // other's half-shell list)?  With >= 3 cells along every periodic axis this
 // is plain adjacency with wrap-around (VerifyPBC/ApplyPBC, src/MCells.f90:
 // 1030-1052).
+__device__ __forceinline__ bool in_slab(const DevParams& P, int c) {
+  return c >= P.slab_c0 && c < P.slab_c1;
+}
+
 __device__ __forceinline__ bool cells_adjacent(const DevParams& P, int a, int b) {
   int ax, ay, az, bx, by, bz;
   cell_coords(P, a, ax, ay, az);
@@ -636,6 +650,17 @@ __device__ __forceinline__ bool cells_adjacent(const DevParams& P, int a, int b)
     if (x > 1 && !(P.pbc[k] && x == N[k] - 1)) return false;
   }
   return true;
+}
+
+// Whether a history record's partner q sits in a cell adjacent to cell c
+// (the sweep visits the pair, src/MForces.f90:199-272), for records the
+// pass did not match.  A slab trusts only the cells it knows this pass; a
+// partner anywhere else is not adjacent to any of its cells.
+template <class PA>
+__device__ __forceinline__ bool partner_adjacent(const PA& A, const DevParams& P, int c, int q) {
+  const int cq = A.cell_cur[q];
+  if (A.gstamp && !in_slab(P, cq) && A.gstamp[q] != A.gepoch) return false;
+  return cells_adjacent(P, c, cq);
 }
 
 // axis helper: neighbour offsets of a cell coordinate, trimmed like VerifyPBC

@@ -548,8 +548,10 @@ __global__ void k_relink(const DevParams* __restrict__ PT, const int* __restrict
 // BS threads per block.  STRIDE: grid-stride over blocks of BS particles (a
 // grid smaller than the particle count gives each thread several particles);
 // else one block of particles per block.
+// (register budget: 7 blocks of 128 threads per SM, 28 warps, as the
+// kernel fits in 72 registers)
 template <bool PP, int BS, bool STRIDE>
-__global__ void __launch_bounds__(BS) k_test(TestArgs A) {
+__global__ void __launch_bounds__(BS, 7 * 128 / BS) k_test(TestArgs A) {
   if (!STRIDE) {
     test_body<PP>(A, blockIdx.x);
     return;
@@ -689,8 +691,9 @@ __device__ __forceinline__ void fold_fp64_body(const PassArgs<double4, double2>&
     for (int w = 0; w < A.nw_max; w++) s_w[w][threadIdx.x] = 0.0;
   if (vblock == 0 && threadIdx.x == 0) atomicAdd(&A.cnt->pass_id, 1);  // this pass is done
   const int p0 = vblock * blockDim.x + threadIdx.x;
-  const bool valid = p0 < A.n;
-  const int p = valid ? p0 : 0;
+  const int p = p0 < A.n ? p0 : 0;
+  // (a slab of a decomposition advances only its own particles)
+  const bool valid = p0 < A.n && in_slab(sys_params(A.P, A.sysid, p), A.cell_cur[p]);
   const bool update = A.update != 0;
   unsigned n_wc = 0;
   int need = 0;
@@ -805,7 +808,7 @@ __device__ __forceinline__ void fold_fp64_body(const PassArgs<double4, double2>&
       for (int r = 0; r < hc; r++) {
         if (r < 32 && ((matched >> r) & 1u)) continue;
         const int q2 = A.Hr.key[hslot(A.Hr, p, r)];
-        if (q2 >= A.n || !cells_adjacent(P, c, A.cell_cur[q2])) {
+        if (q2 >= A.n || !partner_adjacent(A, P, c, q2)) {
           if (hw_n < A.Hw.cap) {
             double ft[3], vt[3];
             hist_read(A.Hr, p, r, ft, vt);

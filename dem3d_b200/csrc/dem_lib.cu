@@ -17,6 +17,7 @@
 #include "dem_mixed.cuh"
 #include "dem_remove.cuh"
 #include "dem_fluid.cuh"
+#include "dem_slab.cuh"
 
 using namespace dem;
 
@@ -153,6 +154,18 @@ struct dem_ctx {
   unsigned long long bar_limit_ns = 2000000000ull;
   int bar_extra = 0;        // blocks a test adds to every barrier (0: none)
   int chunk_blocks = 0;     // blocks of the last persistent launch
+  // one slab of a spatial decomposition (dem_slab_set_range): the context
+  // holds every particle's arrays but advances only the particles of its
+  // cell layers; gstamp[p] == gepoch marks the ghosts it received this pass
+  bool slab = false;
+  int* gstamp = nullptr;
+  int gepoch = 0;
+  int slab_z0 = 0, slab_z1 = 0;
+  int* slab_list = nullptr;   // particles of a layer / migrants (scratch, [ncap])
+  int* slab_ghosts = nullptr; // the ghosts received this pass
+  int n_ghosts = 0;
+  int* slab_count = nullptr;  // device counters of the list kernels
+  RingMap slab_rm{};          // the ring map of the pass in progress
   bool has_cone = false; // some wall of some system is a cone
   double skin_factor = 0.05;  // candidate-row skin / CutOff
   int par = 0;         // L.cell[par] is the assignment the lists hold
@@ -650,6 +663,8 @@ PassArgs<V4, W2> pass_args(dem_ctx* c, int side, bool update, double dt, const R
   A.matched = c->matched;
   A.wall_part = c->wall_part;
   A.nw_max = c->nw_max;
+  A.gstamp = c->slab ? c->gstamp : nullptr;
+  A.gepoch = c->gepoch;
   return A;
 }
 
@@ -772,8 +787,10 @@ void fluid_prepare(dem_ctx* c, int side) {
          (const Counters*)c->cnt);
 }
 
+// part: 0 = the whole pass, 1 = the test and pair kernels, 2 = the fold
+// kernel (a slab of a decomposition exchanges data in between)
 void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, const RingMap& rm,
-                        int tag) {
+                        int tag, int part = 0) {
   if (c->n == 0) return;
   const StateArrays& tgt = side ? c->Pr : c->P;
   // the test kernel: the contact list of the pass
@@ -794,6 +811,8 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
   T.cl_cap = c->cl_cap;
   T.cnt = c->cnt;
   T.tag = tag;
+  T.slab_c0 = c->slab ? c->hsys[0].slab_c0 : 0;
+  T.slab_span = c->slab ? (unsigned)(c->hsys[0].slab_c1 - c->hsys[0].slab_c0) : 0xffffffffu;
   const bool walls = c->nw_max > 0;
   if (c->recording) {
     // a pass of a persistent chunk: appended, not launched
@@ -823,7 +842,7 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
   }
   // test kernel: test_block threads per block; with ppt > 1 the grid holds
   // 1/ppt of the blocks and strides over them
-  {
+  if (part != 2) {
     const int bs = c->test_block;
     const unsigned nvb = blocks_for(c->n, bs);
     const bool stride = c->ppt > 1;
@@ -854,10 +873,11 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
   if (c->precision == DEM_PREC_MIXED) {
     auto A = pass_args<float4, float2>(c, side, update, dt, rm, tag, tgt);
     if (epi == EPI_STORE) A.amsum = c->force_out;
-    for (int part = 0; part < 2; part++) {
-      timed(c, part ? "fold_mixed" : "pair_mixed", [&]() {
+    for (int k = 0; k < 2; k++) {
+      if ((k == 0 && part == 2) || (k == 1 && part == 1)) continue;
+      timed(c, k ? "fold_mixed" : "pair_mixed", [&]() {
         mixed_pass(c->M, c->pp, epi, c->pass_variant, walls, c->has_cone, A, c->hcur, c->stream,
-                   part, pair_blocks, c->ppt);
+                   k, pair_blocks, c->ppt);
       });  // (timed counts the launch)
     }
     return;
@@ -866,7 +886,8 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
   if (epi == EPI_STORE) A.amsum = c->force_out;
 #define PAIR_CASE(PPV, MB) \
   launch(c, "pair_fp64", k_pair_fp64<PPV, MB>, pair_blocks, 128, A)
-  if (mb == 3) {
+  if (part == 2) {
+  } else if (mb == 3) {
     if (c->pp) PAIR_CASE(true, 3);
     else PAIR_CASE(false, 3);
   } else if (mb == 5) {
@@ -877,6 +898,7 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
     else PAIR_CASE(false, 4);
   }
 #undef PAIR_CASE
+  if (part == 1) return;
   // fold kernel: blocks of 128 particles (ppt > 1: grid-stride, not for the
   // Euler start-up's EPI_STORE)
   const unsigned nvb = blocks_for(c->n, 128);
@@ -1615,6 +1637,153 @@ int launch_chunk(dem_ctx* c, int phase) {
   return DEM_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// Slabs of a spatial decomposition (dem_slab_*): column tables and layers.
+
+void slab_col(SlabCols& C, const void* base, int elem, int rows, long long stride) {
+  const int k = C.n++;
+  C.src[k] = (const char*)base;
+  C.dst[k] = (char*)base;
+  C.elem[k] = elem;
+  C.rows[k] = rows;
+  C.stride[k] = stride;
+  C.off[k] = C.rec;
+  C.rec += elem * rows;
+}
+
+SlabCols slab_cols_begin() {
+  SlabCols C{};
+  C.rec = SLAB_ID;
+  return C;
+}
+
+// the history rows of table b (counts, partners, values; FP32 values in
+// mixed mode), and with walls the wall rows
+void slab_hist_cols(const dem_ctx* c, SlabCols& C, int b, bool walls) {
+  const History& H = c->H[b];
+  const long long N = H.n;
+  const bool mixed = c->precision == DEM_PREC_MIXED;
+  slab_col(C, H.cnt, 4, 1, 0);
+  slab_col(C, H.key, 4, H.cap, N * 4);
+  if (mixed) {
+    slab_col(C, c->M.ha[b], 16, H.cap, N * 16);
+    slab_col(C, c->M.hb[b], 16, H.cap, N * 16);
+    slab_col(C, c->M.hc[b], 4, H.cap, N * 4);
+  } else {
+    slab_col(C, H.val, 48, H.cap, N * 48);
+  }
+  if (!walls) return;
+  const int nw = std::max(c->params.n_walls, 1);
+  slab_col(C, H.wflag, 4 * nw, 1, 0);
+  if (mixed) {
+    slab_col(C, c->M.wa[b], 16 * nw, 1, 0);
+    slab_col(C, c->M.wb[b], 16 * nw, 1, 0);
+    slab_col(C, c->M.wc[b], 4 * nw, 1, 0);
+  } else {
+    slab_col(C, H.wval, 48 * nw, 1, 0);
+  }
+}
+
+// what a slab needs of a ghost for the pass on `side`: list link, pass
+// copies, cell, current history rows
+SlabCols slab_ghost_cols(const dem_ctx* c, int side) {
+  const bool mixed = c->precision == DEM_PREC_MIXED;
+  SlabCols C = slab_cols_begin();
+  slab_col(C, c->L.next, 4, 1, 0);
+  slab_col(C, c->X[side], 32, 1, 0);
+  slab_col(C, c->v4[side], mixed ? 16 : 32, 1, 0);
+  slab_col(C, c->w2[side], mixed ? 8 : 16, 1, 0);
+  slab_col(C, c->L.cell[c->par], 4, 1, 0);
+  slab_hist_cols(c, C, c->hcur, false);
+  return C;
+}
+
+// everything a particle owns: state, Predicted, ABM ring, corrector sums,
+// pass copies of both sides, both cell entries, both history tables
+SlabCols slab_full_cols(const dem_ctx* c) {
+  const bool mixed = c->precision == DEM_PREC_MIXED;
+  const long long N = c->ncap, n = c->n;
+  SlabCols C = slab_cols_begin();
+  slab_col(C, c->state_block, 8, 30, N * 8);
+  if (c->nprev > 0) slab_col(C, c->ring, 8, 9 * (c->nprev + 1), n * 8);
+  if (c->amsum) slab_col(C, c->amsum, 8, 9, n * 8);
+  for (int b = 0; b < 2; b++) {
+    slab_col(C, c->X[b], 32, 1, 0);
+    slab_col(C, c->v4[b], mixed ? 16 : 32, 1, 0);
+    slab_col(C, c->w2[b], mixed ? 8 : 16, 1, 0);
+    slab_col(C, c->L.cell[b], 4, 1, 0);
+  }
+  for (int b = 0; b < 2; b++) slab_hist_cols(c, C, b, true);
+  return C;
+}
+
+int slab_nxy(const dem_ctx* c) { return c->hsys[0].nx * c->hsys[0].ny; }
+int slab_nz(const dem_ctx* c) { return c->hsys[0].nz; }
+// first cell of layer z (taken modulo Nz)
+int slab_layer(const dem_ctx* c, int z) {
+  const int nz = slab_nz(c);
+  return c->hsys[0].coff + ((z % nz + nz) % nz) * slab_nxy(c);
+}
+// whether the slab has a layer above / below it (periodic z: always)
+bool slab_has_up(const dem_ctx* c) { return c->hsys[0].pbc[2] || c->slab_z1 < slab_nz(c); }
+bool slab_has_down(const dem_ctx* c) { return c->hsys[0].pbc[2] || c->slab_z0 > 0; }
+
+// the particles of layer z into c->slab_list; returns their count
+int slab_list_layer(dem_ctx* c, int z, int* count) {
+  CK(cudaMemsetAsync(c->slab_count, 0, 2 * sizeof(int), c->stream));
+  const int nxy = slab_nxy(c);
+  launch(c, "slab_layer", k_slab_layer, blocks_for(nxy, 128), 128, (const int*)c->L.head,
+         (const int*)c->L.next, slab_layer(c, z), nxy, c->n, c->slab_list, c->slab_count, c->ncap,
+         c->slab_count + 1);
+  int h[2];
+  CK(cudaMemcpyAsync(h, c->slab_count, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (h[1]) return fail(c, DEM_ERR_STATE, "slab: a cell list of a boundary layer is inconsistent");
+  *count = h[0];
+  return DEM_OK;
+}
+
+// the header and records of a packed exchange
+int slab_write(dem_ctx* c, int what, const SlabCols& C, int count, const std::vector<int>& extra,
+               void* buf, int64_t cap, int64_t* bytes) {
+  const int64_t head = SLAB_HEAD + 4 * (int64_t)extra.size();
+  const int64_t body = (head + 15) / 16 * 16;
+  const int64_t total = body + (int64_t)count * C.rec;
+  *bytes = total;
+  if (total > cap) return fail(c, DEM_ERR_CAPACITY, "slab: the exchange buffer is too small");
+  std::vector<int> h(4 + extra.size());
+  h[0] = what;
+  h[1] = count;
+  h[2] = C.rec;
+  h[3] = (int)extra.size();
+  std::copy(extra.begin(), extra.end(), h.begin() + 4);
+  CK(cudaMemcpyAsync(buf, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  if (count > 0) {
+    const long long thr = (long long)count * (C.rec / 4);
+    launch(c, "slab_cols", k_slab_cols, (unsigned)((thr + 255) / 256), 256, C,
+           (const int*)c->slab_list, count, (char*)buf + body, (int*)nullptr, 0, (int*)nullptr);
+  }
+  CK(cudaStreamSynchronize(c->stream));  // the header's host copy is read
+  return DEM_OK;
+}
+
+// the header of a received exchange (host copy) and where its records start
+int slab_read_head(dem_ctx* c, const void* buf, int64_t bytes, int what, std::vector<int>& h,
+                   int64_t* body) {
+  int h4[4];
+  if (bytes < SLAB_HEAD) return fail(c, DEM_ERR_INVALID, "slab: short exchange buffer");
+  CK(cudaMemcpy(h4, buf, sizeof(h4), cudaMemcpyDeviceToHost));
+  if (h4[0] != what || h4[1] < 0 || h4[3] < 0)
+    return fail(c, DEM_ERR_INVALID, "slab: the buffer holds another exchange");
+  h.assign(4 + (size_t)h4[3], 0);
+  CK(cudaMemcpy(h.data(), buf, h.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  *body = (SLAB_HEAD + 4 * (int64_t)h4[3] + 15) / 16 * 16;
+  if (*body + (int64_t)h4[1] * h4[2] > bytes)
+    return fail(c, DEM_ERR_INVALID, "slab: truncated exchange buffer");
+  return DEM_OK;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -1828,6 +1997,8 @@ int dem_create_ensemble(const dem_params* ps, int32_t nsys, dem_ctx** out) {
     if (st) return st;
     hs[(size_t)s].coff = (int)ncell;
     hs[(size_t)s].sys = s;
+    hs[(size_t)s].slab_c0 = (int)ncell;
+    hs[(size_t)s].slab_c1 = (int)ncell + hs[(size_t)s].ncell;
     ncell += hs[(size_t)s].ncell;
     if (ncell >= (1LL << 30)) return DEM_ERR_INVALID;
   }
@@ -1909,6 +2080,10 @@ void dem_destroy(dem_ctx* c) {
   drop_graphs(c);
   free_state(c);
   cudaFree(c->bar);
+  cudaFree(c->gstamp);
+  cudaFree(c->slab_list);
+  cudaFree(c->slab_ghosts);
+  cudaFree(c->slab_count);
   cudaFree(c->dp);
   cudaFree(c->rm_buf);
   cudaFree(c->pour_cand);
@@ -3226,6 +3401,279 @@ int dem_autotune(dem_ctx* c, int32_t first_step, int32_t steps_per_trial, int32_
   st = dem_set_launch_shape(c, mode, tb, ppt, waves);
   if (st) return st;
   if (last_step) *last_step = step - 1;
+  return DEM_OK;
+}
+
+int dem_slab_set_range(dem_ctx* c, int32_t z0, int32_t z1) {
+  if (!c) return DEM_ERR_INVALID;
+  int st = validate_ready(c);
+  if (st) return st;
+  if (c->nsys != 1 || c->fluid || !c->wm.empty() || c->pouring)
+    return fail(c, DEM_ERR_INVALID,
+                "slab: one system without fluid drag, wall motion or pouring");
+  const int nz = slab_nz(c);
+  if (z0 < 0 || z1 > nz || z0 >= z1)
+    return fail(c, DEM_ERR_INVALID, "slab: the layers must satisfy 0 <= z0 < z1 <= Nz");
+  if (z1 - z0 < 2 && !(z0 == 0 && z1 == nz))
+    return fail(c, DEM_ERR_INVALID, "slab: a slab holds at least two cell layers");
+  CK(cudaStreamSynchronize(c->stream));
+  DevParams& h = c->hsys[0];
+  h.slab_c0 = h.coff + z0 * slab_nxy(c);
+  h.slab_c1 = h.coff + z1 * slab_nxy(c);
+  c->hp = h;
+  CK(cudaMemcpy(c->dp, c->hsys.data(), sizeof(DevParams), cudaMemcpyHostToDevice));
+  c->slab = !(z0 == 0 && z1 == nz);
+  c->slab_z0 = z0;
+  c->slab_z1 = z1;
+  c->removal = false;  // particles leave a slab for its neighbour, not the system
+  if (!c->gstamp) {
+    CK(cudaMalloc(&c->gstamp, sizeof(int) * (size_t)std::max(c->ncap, 1)));
+    CK(cudaMalloc(&c->slab_list, sizeof(int) * (size_t)std::max(c->ncap, slab_nxy(c))));
+    CK(cudaMalloc(&c->slab_ghosts, sizeof(int) * (size_t)std::max(c->ncap, 1)));
+    CK(cudaMalloc(&c->slab_count, sizeof(int) * 4));
+  }
+  CK(cudaMemset(c->gstamp, 0xFF, sizeof(int) * (size_t)std::max(c->ncap, 1)));
+  c->n_ghosts = 0;
+  drop_graphs(c);
+  // room for the "j" results a slab receives as well as its own: the
+  // exchange cannot grow it in the middle of a pass
+  return grow_incoming(c, 16);
+}
+
+int dem_slab_phase(dem_ctx* c, int32_t step, int32_t pass, int32_t phase) {
+  if (!c) return DEM_ERR_INVALID;
+  if (!c->slab && !(c->slab_z1 > c->slab_z0))
+    return fail(c, DEM_ERR_STATE, "slab: dem_slab_set_range first");
+  if (pass < 0 || pass > 1 || phase < 0 || phase > 3)
+    return fail(c, DEM_ERR_INVALID, "slab: pass in {0, 1}, phase in 0..3");
+  const int side = pass;
+  const bool update = pass == 0;
+  const int epi = pass == 0 ? EPI_PREDICT : EPI_CORRECT;
+  const double dt = c->params.time_step;
+  int st = DEM_OK;
+  switch (phase) {
+    case DEM_SLAB_RELINK:
+      st = ensure_drag(c);
+      if (st) return st;
+      c->slab_rm = current_map(c);
+      if (c->prepared != side) {
+        st = prepare_side(c, side);
+        if (st) return st;
+      }
+      c->gepoch++;
+      c->n_ghosts = 0;
+      pass_lists(c, side, update, pass);
+      break;
+    case DEM_SLAB_TEST_PAIR:
+      launch_pass_kernel(c, side, update, dt, epi, c->slab_rm, pass, 1);
+      break;
+    case DEM_SLAB_FOLD:
+      launch_pass_kernel(c, side, update, dt, epi, c->slab_rm, pass, 2);
+      break;
+    default: {  // DEM_SLAB_FINISH
+      st = read_counters(c);
+      if (st) return st;
+      const Counters& h = *c->hcnt;
+      if (h.abort) {
+        if (h.nonfinite) return fail(c, DEM_ERR_STATE, "a particle position is not finite");
+        if (h.list_error) return fail(c, DEM_ERR_STATE, "cell lists inconsistent");
+        return fail(c, DEM_ERR_CAPACITY,
+                    "slab: a table overflowed in the pass (reserve more room: history "
+                    "capacity, incoming results, rows)");
+      }
+      c->last_side = side;
+      c->prepared = epi == EPI_PREDICT ? 1 : 0;
+      if (update) c->hcur ^= 1;
+      if (pass == 0) {
+        rotate_ring(c);
+        c->time = (double)step * dt;
+        st = apply_walls(c, 0);
+        if (st) return st;
+      }
+    }
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(c, e, "slab phase");
+  return DEM_OK;
+}
+
+int dem_slab_pack(dem_ctx* c, int32_t what, void* buf, int64_t cap, int64_t* bytes) {
+  if (!c || !buf || !bytes) return DEM_ERR_INVALID;
+  if (!c->slab) return fail(c, DEM_ERR_STATE, "slab: dem_slab_set_range first");
+  int count = 0;
+  int st = DEM_OK;
+  std::vector<int> extra;
+  switch (what) {
+    case DEM_SLAB_GHOSTS: {
+      // this slab's bottom layer, for the slab below: its cells' lists,
+      // the stamps of the layer below it (the receiver's top layer), and
+      // its particles' pass data
+      if (!slab_has_down(c)) return slab_write(c, what, slab_cols_begin(), 0, {}, buf, cap, bytes);
+      const int nxy = slab_nxy(c);
+      const int cb = slab_layer(c, c->slab_z0), cr = slab_layer(c, c->slab_z0 - 1);
+      extra.resize(1 + 2 * (size_t)nxy);
+      extra[0] = cb;
+      CK(cudaMemcpyAsync(extra.data() + 1, c->L.head + cb, sizeof(int) * nxy,
+                         cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaMemcpyAsync(extra.data() + 1 + nxy, c->L.rflag + cr, sizeof(int) * nxy,
+                         cudaMemcpyDeviceToHost, c->stream));
+      st = slab_list_layer(c, c->slab_z0, &count);
+      if (st) return st;
+      return slab_write(c, what, slab_ghost_cols(c, c->prepared), count, extra, buf, cap,
+                        bytes);
+    }
+    case DEM_SLAB_LOWER: {
+      // the cells of this slab's top layer's particles, for the slab above
+      if (!slab_has_up(c)) return slab_write(c, what, slab_cols_begin(), 0, {}, buf, cap, bytes);
+      st = slab_list_layer(c, c->slab_z1 - 1, &count);
+      if (st) return st;
+      SlabCols C = slab_cols_begin();
+      slab_col(C, c->L.cell[c->par], 4, 1, 0);
+      extra.push_back(slab_layer(c, c->slab_z1 - 1));
+      return slab_write(c, what, C, count, extra, buf, cap, bytes);
+    }
+    case DEM_SLAB_JHALVES: {
+      // the "j" results and matched bits of the ghosts received this pass,
+      // for their owner (the slab above)
+      const int rec = (int)in_rec_bytes(c);
+      const int64_t item = SLAB_ID + (int64_t)c->in_cap * rec;
+      const int64_t total = SLAB_HEAD + 16 + (int64_t)c->n_ghosts * item;
+      *bytes = total;
+      if (total > cap) return fail(c, DEM_ERR_CAPACITY, "slab: the exchange buffer is too small");
+      int h[8] = {what, c->n_ghosts, (int)item, 4, c->in_cap, rec, 0, 0};
+      CK(cudaMemcpyAsync(buf, h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+      launch(c, "slab_jhalf_pack", k_slab_jhalf_pack, blocks_for(c->n_ghosts, 128), 128,
+             (const int*)c->slab_ghosts, c->n_ghosts, c->in_cnt, (const char*)c->in_rec,
+             c->in_cap, c->pass_cap, rec, c->matched, (char*)buf + SLAB_HEAD + 16);
+      CK(cudaStreamSynchronize(c->stream));
+      return DEM_OK;
+    }
+    case DEM_SLAB_MIGRATE_UP:
+    case DEM_SLAB_MIGRATE_DOWN: {
+      // the particles that entered the layer just above (below) this slab
+      const bool up = what == DEM_SLAB_MIGRATE_UP;
+      if (!(up ? slab_has_up(c) : slab_has_down(c)))
+        return slab_write(c, what, slab_cols_begin(), 0, {}, buf, cap, bytes);
+      const int nxy = slab_nxy(c);
+      const int tu = slab_layer(c, c->slab_z1), td = slab_layer(c, c->slab_z0 - 1);
+      const int t0 = up ? tu : td, u0 = up ? td : tu;
+      const int b = c->par ^ 1;  // the next assignment
+      CK(cudaMemsetAsync(c->slab_count, 0, 2 * sizeof(int), c->stream));
+      launch(c, "slab_leavers", k_slab_leavers, blocks_for(c->n, 256), 256, c->n,
+             (const int*)c->L.cell[c->par], (const int*)c->L.cell[b], c->hsys[0].slab_c0,
+             c->hsys[0].slab_c1, t0, t0 + nxy, (slab_has_up(c) && slab_has_down(c)) ? u0 : 0,
+             (slab_has_up(c) && slab_has_down(c)) ? u0 + nxy : 0, c->slab_list, c->slab_count,
+             c->ncap, c->slab_count + 1);
+      int hc[2];
+      CK(cudaMemcpyAsync(hc, c->slab_count, sizeof(hc), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      if (hc[1] == 2)
+        return fail(c, DEM_ERR_STATE, "slab: a particle moved more than one cell layer in a pass");
+      if (hc[1]) return fail(c, DEM_ERR_STATE, "slab: leaver list overflow");
+      count = hc[0];
+      st = slab_write(c, what, slab_full_cols(c), count, {}, buf, cap, bytes);
+      if (st) return st;
+      // handed on: both cell entries name the cell it entered
+      launch(c, "slab_depart", k_slab_depart, blocks_for(count, 128), 128,
+             (const int*)c->slab_list, count, c->L.cell[c->par], (const int*)c->L.cell[b]);
+      CK(cudaStreamSynchronize(c->stream));
+      return DEM_OK;
+    }
+    default:
+      return fail(c, DEM_ERR_INVALID, "slab: unknown exchange");
+  }
+}
+
+int dem_slab_unpack(dem_ctx* c, int32_t what, const void* buf, int64_t bytes) {
+  if (!c || !buf) return DEM_ERR_INVALID;
+  if (!c->slab) return fail(c, DEM_ERR_STATE, "slab: dem_slab_set_range first");
+  std::vector<int> h;
+  int64_t body = 0;
+  int st = slab_read_head(c, buf, bytes, what, h, &body);
+  if (st) return st;
+  const int count = h[1], rec = h[2];
+  const char* recs = (const char*)buf + body;
+  switch (what) {
+    case DEM_SLAB_GHOSTS: {
+      if (count == 0 && h[3] == 0) return DEM_OK;
+      const int nxy = slab_nxy(c);
+      const SlabCols C = slab_ghost_cols(c, c->prepared);
+      if (h[3] != 1 + 2 * nxy || h[4] != slab_layer(c, c->slab_z1) || rec != C.rec)
+        return fail(c, DEM_ERR_INVALID, "slab: ghosts from a slab that is not the one above");
+      const int* ex = h.data() + 4;
+      CK(cudaMemcpyAsync(c->L.head + ex[0], ex + 1, sizeof(int) * nxy, cudaMemcpyHostToDevice,
+                         c->stream));
+      // stamps: rows of this slab's top layer whose neighbourhood changed
+      CK(cudaMemcpyAsync(c->slab_list, ex + 1 + nxy, sizeof(int) * nxy, cudaMemcpyHostToDevice,
+                         c->stream));
+      launch(c, "slab_max", k_slab_max, blocks_for(nxy, 256), 256,
+             c->L.rflag + slab_layer(c, c->slab_z1 - 1), (const int*)c->slab_list, nxy);
+      if (count > 0) {
+        const long long thr = (long long)count * (rec / 4);
+        launch(c, "slab_cols", k_slab_cols, (unsigned)((thr + 255) / 256), 256, C,
+               (const int*)nullptr, count, (char*)recs, c->gstamp, c->gepoch, c->slab_ghosts);
+      }
+      c->n_ghosts = count;
+      break;
+    }
+    case DEM_SLAB_LOWER: {
+      if (count == 0) return DEM_OK;
+      SlabCols C = slab_cols_begin();
+      slab_col(C, c->L.cell[c->par], 4, 1, 0);
+      if (h[3] != 1 || h[4] != slab_layer(c, c->slab_z0 - 1) || rec != C.rec)
+        return fail(c, DEM_ERR_INVALID, "slab: cells from a slab that is not the one below");
+      const long long thr = (long long)count * (rec / 4);
+      launch(c, "slab_cols", k_slab_cols, (unsigned)((thr + 255) / 256), 256, C,
+             (const int*)nullptr, count, (char*)recs, c->gstamp, c->gepoch, (int*)nullptr);
+      break;
+    }
+    case DEM_SLAB_JHALVES: {
+      if (count == 0) return DEM_OK;
+      const int in_cap = h[4], r = h[5];
+      if (r != (int)in_rec_bytes(c) || in_cap != c->in_cap)
+        return fail(c, DEM_ERR_INVALID, "slab: results from a slab with another layout");
+      launch(c, "slab_jhalf_unpack", k_slab_jhalf_unpack, blocks_for(count, 128), 128, recs,
+             count, c->in_cnt, (char*)c->in_rec, c->in_cap, c->pass_cap, r, c->matched, c->cnt);
+      break;
+    }
+    case DEM_SLAB_MIGRATE_UP:
+    case DEM_SLAB_MIGRATE_DOWN: {
+      if (count == 0) return DEM_OK;
+      const SlabCols C = slab_full_cols(c);
+      if (rec != C.rec) return fail(c, DEM_ERR_INVALID, "slab: particles with another layout");
+      const long long thr = (long long)count * (rec / 4);
+      launch(c, "slab_cols", k_slab_cols, (unsigned)((thr + 255) / 256), 256, C,
+             (const int*)nullptr, count, (char*)recs, (int*)nullptr, 0, c->slab_list);
+      launch(c, "slab_arrive", k_slab_arrive, blocks_for(count, 128), 128,
+             (const int*)c->slab_list, count, c->L, c->cnt, c->par, c->par ^ 1);
+      break;
+    }
+    default:
+      return fail(c, DEM_ERR_INVALID, "slab: unknown exchange");
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(c, e, "slab unpack");
+  return DEM_OK;
+}
+
+int dem_slab_displacement(dem_ctx* c, uint32_t* bits_out, const uint32_t* bits_in) {
+  if (!c) return DEM_ERR_INVALID;
+  CK(cudaStreamSynchronize(c->stream));
+  if (bits_out) CK(cudaMemcpy(bits_out, &c->cnt->disp_max, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  if (bits_in) CK(cudaMemcpy(&c->cnt->disp_max, bits_in, sizeof(uint32_t), cudaMemcpyHostToDevice));
+  return DEM_OK;
+}
+
+int dem_slab_owned(dem_ctx* c, int32_t* owned) {
+  if (!c || !owned) return DEM_ERR_INVALID;
+  if (!c->cells_ready) return fail(c, DEM_ERR_STATE, "cell distribution not initialised");
+  std::vector<int> cell((size_t)c->n);
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpy(cell.data(), c->L.cell[c->par], sizeof(int) * (size_t)c->n,
+                cudaMemcpyDeviceToHost));
+  const int c0 = c->hsys[0].slab_c0, c1 = c->hsys[0].slab_c1;
+  for (int i = 0; i < c->n; i++) owned[i] = cell[(size_t)i] >= c0 && cell[(size_t)i] < c1;
   return DEM_OK;
 }
 

@@ -356,8 +356,9 @@ __device__ __forceinline__ void fold_mixed_body(const PassArgs<float4, float2>& 
     for (int w = 0; w < A.nw_max; w++) s_w[w][threadIdx.x] = 0.f;
   if (vblock == 0 && threadIdx.x == 0) atomicAdd(&A.cnt->pass_id, 1);  // this pass is done
   const int p0 = vblock * blockDim.x + threadIdx.x;
-  const bool valid = p0 < A.n;
-  const int p = valid ? p0 : 0;
+  const int p = p0 < A.n ? p0 : 0;
+  // (a slab of a decomposition advances only its own particles)
+  const bool valid = p0 < A.n && in_slab(sys_params(A.P, A.sysid, p), A.cell_cur[p]);
   const bool update = A.update != 0;
   const History& Hr = A.Hr;
   const History& Hw = A.Hw;
@@ -447,7 +448,7 @@ __device__ __forceinline__ void fold_mixed_body(const PassArgs<float4, float2>& 
         if (r < 32 && ((matched >> r) & 1u)) continue;
         const size_t i = hslot(Hr, p, r);
         const int q2 = Hr.key[i];
-        if (q2 >= A.n || !cells_adjacent(P, c, A.cell_cur[q2])) {
+        if (q2 >= A.n || !partner_adjacent(A, P, c, q2)) {
           if (hw_n < Hw.cap) {
             F3 ft, lo, vt;
             rec_read(V.ra, V.rb, V.rc, i, ft, lo, vt);

@@ -99,6 +99,16 @@ __device__ __forceinline__ void relink_body(const DevParams* __restrict__ PT,
   const int* __restrict__ cell_new = L.cell[par];
   for (int i = tid; i < m; i += nthreads) {
     const int c = L.dlist[par][i];
+    const DevParams& P = sys_params(PT, cellsys, c);
+    if (!in_slab(P, c)) {
+      // a cell another slab advances (a particle of this slab left for it):
+      // its list here is not kept; only the transition is forgotten
+      for (int a = L.arr_head[c], g2 = 0; a != -1 && g2 < n; a = L.arr_next[a], g2++)
+        L.mflag[a] = 0;
+      L.arr_head[c] = -1;
+      L.dflag[c] = 0;
+      continue;
+    }
     // 1. unlink the leavers
     int prev = -1, first = -1, q = L.head[c];
     int guard = 0;
@@ -153,7 +163,6 @@ __device__ __forceinline__ void relink_body(const DevParams* __restrict__ PT,
     L.dflag[c] = 0;
     // 3. the rows of every particle around c are rebuilt in this pass (by
     // the test kernel): the 27 cells are stamped with the pass
-    const DevParams& P = sys_params(PT, cellsys, c);
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     const int cl = c - P.coff;
     const int cx = cl % nx, cy = (cl / nx) % ny, cz = cl / (nx * ny);
@@ -345,6 +354,10 @@ struct TestArgs {
   int cl_cap;
   Counters* cnt;
   int tag;
+  // the cells whose particles are tested: [slab_c0, slab_c0 + slab_span)
+  // (a slab of a decomposition, or every cell)
+  int slab_c0;
+  unsigned slab_span;
 };
 
 // First, the candidate rows of the warp's particles that this pass rebuilds
@@ -367,8 +380,8 @@ __device__ __forceinline__ void test_body(const TestArgs& A, int vblock) {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int p0 = vblock * blockDim.x + threadIdx.x;
-  const bool valid = p0 < A.n;
-  const int p = valid ? p0 : 0;
+  const bool valid0 = p0 < A.n;
+  const int p = valid0 ? p0 : 0;
   const int n = A.n;
   // the abort word, the pass's rebuild decision, the particle's cell, own
   // data, row length and first candidates are requested together (the first
@@ -379,6 +392,8 @@ __device__ __forceinline__ void test_body(const TestArgs& A, int vblock) {
   const bool full = A.cnt->full_due != 0;
   const int stamp = A.cnt->pass_id + 1;
   const int cp0 = A.cell_cur[p];
+  // (a slab of a decomposition tests only its own particles)
+  const bool valid = valid0 && (unsigned)(cp0 - A.slab_c0) < A.slab_span;
   const double4 p4 = A.X[p];
   const int cp = PP ? 0 : A.comp[p];
   int q0[4];

@@ -442,6 +442,41 @@ class DEMSystem:
         self._call("get_persistent_blocks", C.byref(v))
         return v.value
 
+    # ---- one slab of a spatial decomposition (dem_slab_*; dem3d_b200.slab)
+    def slab_set_range(self, z0: int, z1: int) -> None:
+        self._call("slab_set_range", C.c_int32(z0), C.c_int32(z1))
+
+    def slab_phase(self, step: int, pass_: int, phase: int) -> None:
+        self._call("slab_phase", C.c_int32(step), C.c_int32(pass_), C.c_int32(phase))
+
+    def slab_pack(self, what: int, buf_ptr: int, cap: int) -> int:
+        """Packs exchange `what` into the device buffer at buf_ptr (cap
+        bytes); returns its size."""
+        n = C.c_int64()
+        self._call("slab_pack", C.c_int32(what), C.c_void_p(buf_ptr), C.c_int64(cap),
+                   C.byref(n))
+        return n.value
+
+    def slab_unpack(self, what: int, buf_ptr: int, nbytes: int) -> None:
+        self._call("slab_unpack", C.c_int32(what), C.c_void_p(buf_ptr), C.c_int64(nbytes))
+
+    def slab_displacement(self, set_bits=None) -> int:
+        """The last pass's largest displacement (FP32 bits) as read; with
+        set_bits, the context's value is then replaced by set_bits (the
+        maximum over all slabs)."""
+        out = C.c_uint32()
+        if set_bits is None:
+            self._call("slab_displacement", C.byref(out), None)
+        else:
+            v = C.c_uint32(set_bits)
+            self._call("slab_displacement", C.byref(out), C.byref(v))
+        return out.value
+
+    def slab_owned(self) -> np.ndarray:
+        out = np.zeros(self.n, dtype=np.int32)
+        self._call("slab_owned", _iptr(out))
+        return out.astype(bool)
+
     AUTOTUNE_TRIALS = 16
 
     def autotune(self, first_step: int, steps_per_trial: int = 20):

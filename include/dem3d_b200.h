@@ -418,6 +418,50 @@ int dem_get_persistent_blocks(dem_ctx* ctx, int32_t* blocks);
 int dem_autotune(dem_ctx* ctx, int32_t first_step, int32_t steps_per_trial,
                  int32_t* last_step, double* trial_ms);
 
+/* Spatial decomposition of one system into z-slabs (no counterpart in the
+ * reference; its thesis names spatial decomposition as the way to run it in
+ * parallel).  Each slab is a context holding every particle's arrays (the
+ * system's own particle numbers) that advances only the particles in its
+ * cell layers [z0, z1); it is set up from the whole state like any context
+ * (dem_set_state, dem_set_integration, dem_set_contacts, dem_set_ncol,
+ * dem_initialize_cell_distribution), then dem_slab_set_range.  A
+ * MoveParticles step is, for pass 0 (history update + AB predictor) and
+ * pass 1 (AM corrector), on every slab in turn:
+ *   - dem_slab_displacement: the largest displacement of the pass before,
+ *     read from every slab, their maximum written back to every slab;
+ *   - phase DEM_SLAB_RELINK; then from the slab above each slab
+ *     DEM_SLAB_GHOSTS (its bottom layer's lists, pass copies, cells and
+ *     history rows) and from the slab below DEM_SLAB_LOWER (its top layer's
+ *     cells);
+ *   - phase DEM_SLAB_TEST_PAIR; then to the slab above DEM_SLAB_JHALVES (the
+ *     results for its particles computed here, and its records matched);
+ *   - phase DEM_SLAB_FOLD; then DEM_SLAB_MIGRATE_UP / _DOWN to the slabs
+ *     above / below (the particles that entered their layers, with their
+ *     state, ABM ring and history);
+ *   - phase DEM_SLAB_FINISH.
+ * Every exchange is a device buffer written by dem_slab_pack on the sending
+ * slab (*bytes: its size; DEM_ERR_CAPACITY with *bytes set when cap is too
+ * small) and read by dem_slab_unpack on the receiving one; between them it
+ * travels by any device copy (cudaMemcpy on one GPU, a send/receive between
+ * GPUs).  The particles each slab advances at the end are dem_slab_owned's;
+ * their states equal the undivided system's bit for bit.  Slabs hold at
+ * least two layers; a pass whose tables overflow is an error. */
+#define DEM_SLAB_RELINK 0
+#define DEM_SLAB_TEST_PAIR 1
+#define DEM_SLAB_FOLD 2
+#define DEM_SLAB_FINISH 3
+#define DEM_SLAB_GHOSTS 0
+#define DEM_SLAB_LOWER 1
+#define DEM_SLAB_JHALVES 2
+#define DEM_SLAB_MIGRATE_UP 3
+#define DEM_SLAB_MIGRATE_DOWN 4
+int dem_slab_set_range(dem_ctx* ctx, int32_t z0, int32_t z1);
+int dem_slab_phase(dem_ctx* ctx, int32_t step, int32_t pass, int32_t phase);
+int dem_slab_pack(dem_ctx* ctx, int32_t what, void* buf, int64_t cap, int64_t* bytes);
+int dem_slab_unpack(dem_ctx* ctx, int32_t what, const void* buf, int64_t bytes);
+int dem_slab_displacement(dem_ctx* ctx, uint32_t* bits_out, const uint32_t* bits_in);
+int dem_slab_owned(dem_ctx* ctx, int32_t* owned);
+
 /* Allocation-free cell distribution.  No counterpart in the reference: it
  * serves callers that may not allocate device memory while they run: a host
  * application whose device memory is all handed out by its own pool or
