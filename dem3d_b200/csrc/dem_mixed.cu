@@ -29,9 +29,35 @@ __device__ __forceinline__ F3 mk(float x, float y, float z) { return F3{x, y, z}
 __device__ __forceinline__ F3 operator+(F3 a, F3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
 __device__ __forceinline__ F3 operator-(F3 a, F3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
 __device__ __forceinline__ F3 operator*(float s, F3 a) { return mk(s * a.x, s * a.y, s * a.z); }
-__device__ __forceinline__ float dot(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+// (dot and cross products and the two-term combinations below use explicit
+// fused multiply-adds: one rounding per term, whatever kernel inlines them)
+__device__ __forceinline__ float dot(F3 a, F3 b) {
+  return __fmaf_rn(a.z, b.z, __fmaf_rn(a.y, b.y, __fmul_rn(a.x, b.x)));
+}
 __device__ __forceinline__ F3 cross(F3 a, F3 b) {
-  return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+  return mk(__fmaf_rn(a.y, b.z, -__fmul_rn(a.z, b.y)), __fmaf_rn(a.z, b.x, -__fmul_rn(a.x, b.z)),
+            __fmaf_rn(a.x, b.y, -__fmul_rn(a.y, b.x)));
+}
+// s*a + t*b
+__device__ __forceinline__ F3 comb(float s, F3 a, float t, F3 b) {
+  return mk(__fmaf_rn(s, a.x, __fmul_rn(t, b.x)), __fmaf_rn(s, a.y, __fmul_rn(t, b.y)),
+            __fmaf_rn(s, a.z, __fmul_rn(t, b.z)));
+}
+// a - s*b
+__device__ __forceinline__ F3 sub_scaled(F3 a, float s, F3 b) {
+  return mk(__fmaf_rn(-s, b.x, a.x), __fmaf_rn(-s, b.y, a.y), __fmaf_rn(-s, b.z, a.z));
+}
+// FP64 sums of a particle's FP32 contributions (exact terms, one rounding
+// per addition at FP64: the net force of a packing, where contact forces
+// nearly cancel, keeps the contact forces' own accuracy)
+struct D3 {
+  double x, y, z;
+};
+__device__ __forceinline__ D3 operator+(D3 a, F3 b) {
+  return D3{a.x + (double)b.x, a.y + (double)b.y, a.z + (double)b.z};
+}
+__device__ __forceinline__ D3 operator-(D3 a, F3 b) {
+  return D3{a.x - (double)b.x, a.y - (double)b.y, a.z - (double)b.z};
 }
 
 struct MPair {
@@ -112,7 +138,7 @@ struct MMat<true> {
 };
 
 __device__ __forceinline__ F3 change_plane_f(F3 V, F3 N) {
-  F3 P = V - dot(V, N) * N;
+  F3 P = sub_scaled(V, dot(V, N), N);
   float ns = dot(P, P);
   if (ns != 0.0f) return sqrtf(dot(V, V) / ns) * P;
   return mk(0.f, 0.f, 0.f);
@@ -135,14 +161,14 @@ __device__ __forceinline__ void common_mixed(F3 Rij, F3 N, F3 DispN, F3 Vij, F3 
                                              F3 ft0, F3 ft0lo, F3 vt0, const MPair& m, MOut& o) {
   F3 VijN = dot(VijC, N) * N;
   o.VT = VijC - VijN;
-  o.FN = m.kn * DispN + m.yn * VijN;
+  o.FN = comb(m.kn, DispN, m.yn, VijN);
   if (contacting) {
     F3 VT0 = change_plane_f(vt0, N);
     F3 dD = half_dt * (VT0 + o.VT);
     F3 dV = o.VT - VT0;
     // rotate the compensated spring (hi + lo) onto the new contact plane
-    F3 ph = ft0 - dot(ft0, N) * N;
-    F3 pl = ft0lo - dot(ft0lo, N) * N;
+    F3 ph = sub_scaled(ft0, dot(ft0, N), N);
+    F3 pl = sub_scaled(ft0lo, dot(ft0lo, N), N);
     float ns = dot(ph, ph);
     F3 hi = mk(0.f, 0.f, 0.f), lo = mk(0.f, 0.f, 0.f);
     if (ns != 0.0f) {
@@ -150,7 +176,7 @@ __device__ __forceinline__ void common_mixed(F3 Rij, F3 N, F3 DispN, F3 Vij, F3 
       hi = f * ph;
       lo = f * pl;
     }
-    F3 inc = m.kt * dD + m.yt * dV;
+    F3 inc = comb(m.kt, dD, m.yt, dV);
     float e;
     two_sum(hi.x, inc.x, o.FT.x, e);
     o.FTlo.x = lo.x + e;
@@ -468,7 +494,7 @@ __device__ __forceinline__ void fold_mixed_body(const PassArgs<float4, float2>& 
     // ---- Force and Torque in sweep order
     const InRec32* in = (const InRec32*)A.in_rec + p;
     const size_t st = (size_t)A.in_stride;
-    F3 F = mk(0.f, 0.f, 0.f), T = mk(0.f, 0.f, 0.f);
+    D3 F = D3{0.0, 0.0, 0.0}, T = D3{0.0, 0.0, 0.0};
     fold_in_order(
         ni, key_p,
         [&](int e) {
@@ -492,8 +518,8 @@ __device__ __forceinline__ void fold_mixed_body(const PassArgs<float4, float2>& 
       A.amsum[q] = F.x; A.amsum[q + 1] = F.y; A.amsum[q + 2] = F.z;
       A.amsum[n3 + q] = T.x; A.amsum[n3 + q + 1] = T.y; A.amsum[n3 + q + 2] = T.z;
     }
-    const double acc[3] = {(double)(F.x * inv_m), (double)(F.y * inv_m), (double)(F.z * inv_m)};
-    const double alp[3] = {(double)(T.x * inv_i), (double)(T.y * inv_i), (double)(T.z * inv_i)};
+    const double acc[3] = {F.x * (double)inv_m, F.y * (double)inv_m, F.z * (double)inv_m};
+    const double alp[3] = {T.x * (double)inv_i, T.y * (double)inv_i, T.z * (double)inv_i};
     // the integrator runs on FP64 velocities: Particle's for the predictor,
     // Predicted's for the corrector (the pass copies are FP32)
     double vd[3] = {0.0, 0.0, 0.0}, wd[3] = {0.0, 0.0, 0.0};
