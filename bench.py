@@ -477,6 +477,29 @@ def measure(s, w, args, world, local, torch, dist, first_step=1):
             "steps": steps_done}
 
 
+def window_observables(s, first, window, every):
+    """Observables averaged over `window` further steps of a run, sampled
+    after every `every` steps (the instantaneous wall force of a settling
+    bed fluctuates; its time average is what compares between runs).
+    Returns (averages, last step, samples)."""
+    every = max(1, min(every, window))
+    samples = []
+    step = first
+    while step - first < window:
+        last = min(step + every - 1, first + window - 1)
+        s.run(step, last)
+        step = last + 1
+        samples.append(s.observables())
+    avg = {}
+    for k, v in samples[0].items():
+        if isinstance(v, (int, float)):
+            avg[k] = float(np.mean([x[k] for x in samples]))
+        elif isinstance(v, (list, tuple, np.ndarray)):
+            avg[k] = [float(y) for y in np.mean([np.asarray(x[k], dtype=float)
+                                                 for x in samples], axis=0)]
+    return avg, step - 1, len(samples)
+
+
 def snapshot(src):
     """State, contact history and integration ring of a context, on the host."""
     return {"state": src.get_state(), "contacts": src.get_contacts(),
@@ -571,8 +594,17 @@ def run_ours(args):
     obs_cmp = None
     if "fp64" in systems and "mixed" in systems:
         # both runs advanced the same steps from the same state: ensemble
-        # observables of the mixed run against the FP64 run
-        ob = {p: systems[p].observables() for p in ("fp64", "mixed")}
+        # observables of the mixed run against the FP64 run (with
+        # --obs-window, time averages over that many further steps)
+        window = None
+        if args.obs_window > 0:
+            avg = {p: window_observables(systems[p], res[p]["last"] + 1, args.obs_window,
+                                         args.obs_every) for p in ("fp64", "mixed")}
+            ob = {p: avg[p][0] for p in avg}
+            window = {"from_step": res["fp64"]["last"] + 1, "to_step": avg["fp64"][1],
+                      "samples": avg["fp64"][2]}
+        else:
+            ob = {p: systems[p].observables() for p in ("fp64", "mixed")}
         # the FP64 context closes before the two force-pass contexts open
         # (three contexts of the 16M-sphere workload do not fit one GPU)
         snap = snapshot(systems["fp64"])
@@ -586,7 +618,8 @@ def run_ours(args):
             pick[p]["floor_pressure"] = ob[p]["wall_pressure"][0]
         rel = {k: (abs(pick["mixed"][k] - pick["fp64"][k]) / abs(pick["fp64"][k])
                    if pick["fp64"][k] else None) for k in pick["fp64"]}
-        obs_cmp = {"after_step": res["fp64"]["last"], **pick, "rel_diff": rel}
+        obs_cmp = {"after_step": res["fp64"]["last"], **pick, "rel_diff": rel,
+                   "time_average": window}
     cell_occ = None
     if WORKLOADS[args.workload].get("kind") == "bidisperse":
         # cell-cost imbalance: cells are sized by the large spheres, so a cell
@@ -893,6 +926,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--retune-every", type=int, default=0,
                     help="run the autotuner's trials again every N timed steps (0: never)")
+    ap.add_argument("--obs-window", type=int, default=0,
+                    help="after the timed steps, compare the two precisions' observables "
+                         "averaged over this many further steps (0: the values at the end)")
+    ap.add_argument("--obs-every", type=int, default=500,
+                    help="steps between the samples of --obs-window")
     ap.add_argument("--no-autotune", action="store_true",
                     help="skip the autotuner's trials (default settings)")
     ap.add_argument("--skip-steps", type=int, default=-1,
