@@ -363,9 +363,11 @@ struct TestArgs {
 // First, the candidate rows of the warp's particles that this pass rebuilds
 // (every row on a full rebuild, else the rows of the particles whose cell the
 // relink stamped with this pass) are built, one particle at a time by the
-// whole warp (build_row).  (No block barriers: every warp runs on its own.
-// The pass's contact count and the list length it needs come from the pair
-// kernel, or from here when the list overflows.)
+// whole warp (build_row).  Then every particle tests its row, and the block
+// takes room for its contacts in the list with one atomic (two block
+// barriers, which every thread of the block meets).  (The pass's contact
+// count and the list length it needs come from the pair kernel, or from
+// here when the list overflows.)
 // (The body of k_test for block `vblock`, so that a persistent kernel can
 // run it too.  NC: candidates read through the non-coherent path, which
 // needs the rows unchanged for the whole launch except by the warp that
@@ -386,9 +388,10 @@ __device__ __forceinline__ void test_body(const TestArgs& A, int vblock) {
   // the abort word, the pass's rebuild decision, the particle's cell, own
   // data, row length and first candidates are requested together (the first
   // candidates before the row length is known: every row holds at least 4
-  // entries' room); nothing is written before the abort word is seen, and a
-  // warp whose rows were rebuilt reads them again
-  const int aborted = A.cnt->abort;
+  // entries' room); nothing is written once the abort word is seen (the
+  // block still meets its barrier), and a warp whose rows were rebuilt reads
+  // them again
+  const bool live = A.cnt->abort == 0;
   const bool full = A.cnt->full_due != 0;
   const int stamp = A.cnt->pass_id + 1;
   const int cp0 = A.cell_cur[p];
@@ -400,9 +403,8 @@ __device__ __forceinline__ void test_body(const TestArgs& A, int vblock) {
 #pragma unroll
   for (int u = 0; u < 4; u++) q0[u] = ld_row<NC>(A.cand + (size_t)u * n + p);
   int meta = A.meta[p];
-  if (aborted) return;
   {
-    unsigned todo = __ballot_sync(FULL, valid && (full || A.L.rflag[cp0] == stamp));
+    unsigned todo = __ballot_sync(FULL, live && valid && (full || A.L.rflag[cp0] == stamp));
     if (todo) {
       while (todo) {
         const int l = __ffs(todo) - 1;
@@ -419,7 +421,7 @@ __device__ __forceinline__ void test_body(const TestArgs& A, int vblock) {
     }
   }
   const DevParams& P = sys_params(A.P, A.sysid, p);
-  const int m = valid ? (meta & META_MASK) : 0;
+  const int m = live && valid ? (meta & META_MASK) : 0;
   // contact bit masks of the row, 64 candidates per window (windows past
   // the first only for rows longer than 64)
   unsigned long long mask0 = 0ull;
@@ -455,22 +457,35 @@ __device__ __forceinline__ void test_body(const TestArgs& A, int vblock) {
     if (base == 0) mask0 = mask;
     else more[base / 64 - 1] = mask;
   }
-  // one allocation per warp; a particle's contacts are contiguous
+  // one allocation per block (the warps' sums through shared memory, one
+  // atomic on the pass's list length); a particle's contacts are contiguous
   int incl = total;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     const int y = __shfl_up_sync(FULL, incl, o);
     if (lane >= o) incl += y;
   }
-  const int wsum = __shfl_sync(FULL, incl, 31);
-  int wbase = 0;
-  if (lane == 31 && wsum > 0) wbase = atomicAdd(&A.cnt->n_contacts, wsum);
-  wbase = __shfl_sync(FULL, wbase, 31);
-  const int start = wbase + incl - total;
-  if (valid) {
+  __shared__ int s_wsum[8];  // blocks of at most 256 threads
+  __shared__ int s_base;
+  const int warp = threadIdx.x >> 5;
+  if (lane == 31) s_wsum[warp] = incl;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+      const int t = s_wsum[w];
+      s_wsum[w] = acc;
+      acc += t;
+    }
+    s_base = acc > 0 ? atomicAdd(&A.cnt->n_contacts, acc) : 0;
+  }
+  __syncthreads();
+  const int start = s_base + s_wsum[warp] + incl - total;
+  if (live && valid) {
     A.cstart[p] = start;
     A.ccount[p] = total;
   }
+  if (!live) return;
   if (start + total > A.cl_cap) {
     // the list is grown and the pass launched again
     atomicMax(&A.cnt->need_cl, start + total);

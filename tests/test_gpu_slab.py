@@ -100,3 +100,41 @@ def test_slab_range_is_checked():
     for z0, z1 in ((0, 0), (-1, 3), (0, nz + 1), (2, 3)):
         with pytest.raises(DEMError):
             g.slab_set_range(z0, z1)
+
+
+def test_slabs_over_a_floor_equal_the_whole_system():
+    """A bed over a floor wall (z not periodic: the slabs form a chain, the
+    bottom slab holds the wall contacts and their records), spheres moving
+    fast enough (σ_v = 5, dt = 5e-4) to cross slab boundaries with their
+    wall records."""
+    w = configs.settling(n=4096, layer_side=16, seed=1024, dt=5e-4, sigma_v=5.0, gravity=10.0,
+                         headroom=8.0, euler_intervals=10)
+    w.params.hist_capacity = 16
+    g = DEMSystem(w.params)
+    g.set_state(w.pos, w.vel, w.omega, comp=w.comp)
+    g.initialize_cell_distribution()
+    g.run(1, 12)
+    nz = g.grid()[2]
+    nslabs = 3 if nz >= 6 else 2
+    ref = DEMSystem(w.params)
+    transfer(g, ref, comp=w.comp)
+    slabs = []
+    for z0, z1 in S.slab_ranges(nz, nslabs):
+        s = DEMSystem(w.params)
+        transfer(g, s, comp=w.comp)
+        s.slab_set_range(z0, z1)
+        slabs.append(s)
+    before = [s.slab_owned() for s in slabs]
+    tr = S.LocalTransport(slabs, periodic=False, cap_bytes=64 << 20)
+    for step in range(13, 413):
+        S.move_particles(tr, step)
+    ref.run(13, 412)
+    want = ref.get_state()
+    got = S.compose_state(slabs)
+    for k in want:
+        np.testing.assert_array_equal(got[k], want[k], err_msg=k)
+    ncol0 = g.ncol()
+    assert ncol0 + sum(s.ncol() - ncol0 for s in slabs) == ref.ncol()
+    assert ref.count_contacts()[1] > 0  # spheres on the floor
+    after = [s.slab_owned() for s in slabs]
+    assert int(np.count_nonzero(before[0] != after[0])) > 20
