@@ -540,9 +540,12 @@ __device__ __forceinline__ void fold_mixed_body(const PassArgs<float4, float2>& 
   if (EPI != EPI_STORE) publish_disp_block(A.cnt, d2);
 }
 
-// (STRIDE: grid-stride over blocks of 128 particles)
+// (STRIDE: grid-stride over blocks of 128 particles.  Register budget: 5
+// blocks of 128 per SM; the corrector without walls fits in 80 registers,
+// 6 blocks.)
 template <bool PP, int EPI, bool WALLS, bool CONE, bool STRIDE>
-__global__ void __launch_bounds__(128, 5) k_fold_mixed(PassArgs<float4, float2> A, MixedView V) {
+__global__ void __launch_bounds__(128, (!WALLS && EPI == EPI_CORRECT) ? 6 : 5)
+    k_fold_mixed(PassArgs<float4, float2> A, MixedView V) {
   if (!STRIDE) {
     fold_mixed_body<PP, EPI, WALLS, CONE>(A, V, blockIdx.x);
     return;
