@@ -914,6 +914,75 @@ def run_ensemble(args):
     return 0
 
 
+def run_slabs(args):
+    """One system cut into --slabs z-slabs, all on this GPU (every slab its
+    own context, the exchanges as device copies between them): the cost of
+    the decomposition's exchanges against the undivided context, and the
+    composed state checked against it bit for bit.  Not a multi-GPU number."""
+    import torch
+
+    from dem3d_b200 import _abi
+    from dem3d_b200 import slab as S
+    from dem3d_b200.system import DEMSystem
+    lib = _abi.load_library()
+    lib.dem_select_device(0)
+    prec = "mixed" if args.precision == "mixed" else "fp64"
+    w = make_workload(args.workload, prec, 0)
+    w.params.hist_capacity = max(w.params.hist_capacity, 16)
+    g = DEMSystem(w.params)
+    g.set_state(w.pos, w.vel, w.omega, comp=w.comp, radius=w.radius)
+    g.initialize_cell_distribution()
+    first = 4 + args.warmup
+    g.run(1, first - 1)
+
+    def copy_of(src):
+        d = DEMSystem(w.params)
+        st = src.get_state()
+        d.set_state(st["pos"], st["vel"], st["omega"], comp=w.comp, radius=w.radius,
+                    acc=st["acc"], alpha=st["alpha"])
+        prev, ipc = src.get_integration()
+        d.set_integration(prev, ipc)
+        c = src.get_contacts()
+        d.set_contacts(c["imin"], c["imax"], c["ft"], c["vt"], c["ip"], c["iw"], c["ftw"],
+                       c["vtw"])
+        d.set_ncol(src.ncol())
+        d.initialize_cell_distribution()
+        return d
+
+    ref = copy_of(g)
+    nz = g.grid()[2]
+    slabs = []
+    for z0, z1 in S.slab_ranges(nz, args.slabs):
+        sl = copy_of(g)
+        sl.slab_set_range(z0, z1)
+        slabs.append(sl)
+    periodic = bool(w.params.pbc[2])
+    tr = S.LocalTransport(slabs, periodic=periodic, cap_bytes=256 << 20)
+    last = first + args.steps - 1
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for step in range(first, last + 1):
+        S.move_particles(tr, step)
+    torch.cuda.synchronize()
+    ms_slab = (time.perf_counter() - t0) * 1000.0
+    ms_whole = ref.run_timed(first, last)
+    want = ref.get_state()
+    got = S.compose_state(slabs)
+    exact = all(np.array_equal(got[k], want[k]) for k in want)
+    line = {"metric": f"particle-updates/s, one system in {args.slabs} z-slabs on one GPU "
+                      "(decomposition emulated: slab contexts, exchanges as device copies)",
+            "value": w.n * args.steps / (ms_slab / 1000.0), "unit": "particle-updates/s",
+            "n_gpus": 1, "steps": args.steps, "ms_per_step": ms_slab / args.steps,
+            "undivided_ms_per_step": ms_whole / args.steps,
+            "exchange_bytes_per_step": tr.bytes_moved / args.steps,
+            "bit_exact_vs_undivided": bool(exact), "slabs": args.slabs, "grid_layers": nz,
+            "timing": "host clock around device-synchronised steps (the exchanges are host "
+                      "driven)", "dtype": "f64" if prec == "fp64" else "f32+f64",
+            "data": "synthetic", "config": {"workload": args.workload, "particles": w.n}}
+    print(json.dumps(line), flush=True)
+    return 0 if exact else 1
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -933,6 +1002,9 @@ def main():
                     help="steps between the samples of --obs-window")
     ap.add_argument("--no-autotune", action="store_true",
                     help="skip the autotuner's trials (default settings)")
+    ap.add_argument("--slabs", type=int, default=0,
+                    help="cut the system into this many z-slabs on one GPU (the spatial "
+                         "decomposition, emulated) and report its cost and bit-exactness")
     ap.add_argument("--skip-steps", type=int, default=-1,
                     help="untimed steps before the warm-up (ensembles: the beds start to "
                          "form; default: the workload's own)")
@@ -947,6 +1019,8 @@ def main():
         return 2
     if args.impl == "reference":
         return run_reference(args)
+    if args.slabs > 1:
+        return run_slabs(args)
     if WORKLOADS[args.workload].get("kind") == "ensemble":
         return run_ensemble(args)
     return run_ours(args)
