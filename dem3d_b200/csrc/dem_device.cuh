@@ -159,7 +159,14 @@ struct CellLists {
   int* rflag;     // [ncell] stamp: pass_id + 1 when the cell's rows are rebuilt in that pass
   int* dlist[2];  // [ncell] cells that gain or lose a particle on the way to assignment b
   int* rlist;     // [ncell] (unused: the stamps replace a repair list)
+  // each cell's list copied in order into SLOT_CAP slots ([cell*SLOT_CAP +
+  // k]) and its length (slot_n > SLOT_CAP: only the first SLOT_CAP are
+  // copied; -1: not current): the candidate rows read a neighbour cell with
+  // independent loads instead of walking its links one after the other
+  int* slot;
+  int* slot_n;
 };
+constexpr int SLOT_CAP = 32;
 
 // Candidate rows, column-major (cand[k*n + p]): the particles within
 // MinDij + skin of particle p that the sweep visits with p as "i" (loop jj

@@ -518,6 +518,13 @@ __global__ void __launch_bounds__(256) k_prepare(const DevParams* __restrict__ P
   publish_disp(cnt, d2);
 }
 
+// The slots of cells [c_begin, c_begin + ncells) from their lists (after
+// the lists were built or changed outside the relink).
+__global__ void k_cell_slots(CellLists L, int c_begin, int ncells, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < ncells) copy_slots(L, c_begin + i, L.head[c_begin + i], n);
+}
+
 __global__ void k_relink(const DevParams* __restrict__ PT, const int* __restrict__ cellsys,
                          CellLists L, int par, int n, int update, int stop_tag, Counters* cnt) {
   relink_body(PT, cellsys, L, par, n, update, stop_tag, cnt, blockIdx.x * blockDim.x + threadIdx.x,

@@ -324,7 +324,8 @@ unsigned blocks_for(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 void free_lists(dem_ctx* c) {
   CellLists& L = c->L;
   int** f[] = {&L.head,  &L.next,  &L.cell[0], &L.cell[1], &L.arr_head, &L.arr_next, &L.mflag,
-               &L.mnext, &L.dflag, &L.rflag,   &L.dlist[0], &L.dlist[1],  &L.rlist};
+               &L.mnext, &L.dflag, &L.rflag,   &L.dlist[0], &L.dlist[1],  &L.rlist,
+               &L.slot,  &L.slot_n};
   for (int** q : f) {
     cudaFree(*q);
     *q = nullptr;
@@ -572,6 +573,14 @@ StateArrays make_state(double* base, size_t n) {
 
 constexpr int LIST_BLOCKS = 148;      // relink / repair kernels (grid-stride)
 
+// the slots of every cell from its list (after the lists were built or
+// changed outside the relink: initial distribution, imported lists, removal,
+// insertion)
+void refresh_slots(dem_ctx* c) {
+  launch(c, "cell_slots", k_cell_slots, blocks_for(c->ncell_total, 256), 256, c->L, 0,
+         c->ncell_total, c->n);
+}
+
 int init_cells(dem_ctx* c) {
   const int n = c->n;
   const int ncell = c->ncell_total;
@@ -602,6 +611,7 @@ int init_cells(dem_ctx* c) {
     launch(c, "link_init", k_link_init, blocks_for(n, 256), 256, n, (const int*)c->S.orig,
            (const int*)c->S.cell, (const int*)c->cell_start, L.head, L.next, L.cell[c->par]);
   }
+  refresh_slots(c);
   // no transition pending; the first pass builds every candidate row
   CK(cudaMemsetAsync(&c->cnt->n_dirty[0], 0, 3 * sizeof(int), c->stream));
   CK(cudaMemsetAsync(&c->cnt->movers_pending, 0, sizeof(unsigned long long), c->stream));
@@ -1228,6 +1238,7 @@ int update_particle_list_impl(dem_ctx* c, int64_t* removed) {
   CK(cudaMemsetAsync(&c->cnt->escaped, 0, sizeof(unsigned long long), c->stream));
   const int one = 1;
   CK(cudaMemcpyAsync(&c->cnt->force_full, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  refresh_slots(c);
   // the cell transition towards the current positions, for the new numbering
   c->last_side = -1;
   int st = prepare_side(c, 0);
@@ -1392,6 +1403,7 @@ int pour_particle_impl(dem_ctx* c, int32_t* inserted) {
   launch(c, "insert", k_insert, 1u, 32u, A);  // (in mixed mode too: the wall flags and
                                               // record counts live in the key tables)
   c->n = n0 + 1;
+  refresh_slots(c);
   c->comp_count[(size_t)comp]++;
   const int one = 1;
   CK(cudaMemcpyAsync(&c->cnt->force_full, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
@@ -2189,6 +2201,9 @@ int dem_set_state(dem_ctx* c, int32_t n, const int32_t* comp, const double* radi
     CK(cudaMalloc(&L.dlist[0], sizeof(int) * NC));
     CK(cudaMalloc(&L.dlist[1], sizeof(int) * NC));
     CK(cudaMalloc(&L.rlist, sizeof(int) * NC));
+    CK(cudaMalloc(&L.slot, sizeof(int) * NC * SLOT_CAP));
+    CK(cudaMalloc(&L.slot_n, sizeof(int) * NC));
+    CK(cudaMemsetAsync(L.slot_n, 0xFF, sizeof(int) * NC, c->stream));
     CK(cudaMalloc(&c->rows.cand, sizeof(int) * N * (size_t)c->kc));
     CK(cudaMalloc(&c->rows.meta, sizeof(int) * N));
     CK(cudaMemsetAsync(c->rows.meta, 0, sizeof(int) * N, c->stream));
@@ -2610,6 +2625,7 @@ int dem_set_cells(dem_ctx* c, const int32_t* traversal, const int32_t* cell_star
     CK(cudaMemcpyAsync(c->L.next, next.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice,
                        c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  refresh_slots(c);
   c->cells_ready = true;
   return DEM_OK;
 }
@@ -3613,6 +3629,8 @@ int dem_slab_unpack(dem_ctx* c, int32_t what, const void* buf, int64_t bytes) {
         launch(c, "slab_cols", k_slab_cols, (unsigned)((thr + 255) / 256), 256, C,
                (const int*)nullptr, count, (char*)recs, c->gstamp, c->gepoch, c->slab_ghosts);
       }
+      // the ghost cells' slots from the lists just received
+      launch(c, "cell_slots", k_cell_slots, blocks_for(nxy, 256), 256, c->L, ex[0], nxy, c->n);
       c->n_ghosts = count;
       break;
     }

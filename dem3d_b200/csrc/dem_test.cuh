@@ -39,6 +39,21 @@ __device__ __forceinline__ double min_dij_sq_rn(const DevParams& P, int ca, doub
   return P.min_dij_sq[ca * NCM + cb];
 }
 
+// Copy cell c's list into its slots (the first SLOT_CAP entries) and record
+// its length; a walk longer than n (corrupt links) records -1.
+__device__ __forceinline__ void copy_slots(const CellLists& L, int c, int first, int n) {
+  int k = 0;
+  for (int q = first; q != -1; q = L.next[q]) {
+    if (k >= n) {
+      k = -1;
+      break;
+    }
+    if (k < SLOT_CAP) L.slot[(size_t)c * SLOT_CAP + k] = q;
+    k++;
+  }
+  L.slot_n[c] = k;
+}
+
 // Relink (RedistributeParticles3D's list updates, src/MCells.f90:607-643):
 // one thread per dirty cell of list `par` drops the particles that left it
 // (TransferParticle's unlink, :747-774) and prepends its arrivals in
@@ -161,13 +176,17 @@ __device__ __forceinline__ void relink_body(const DevParams* __restrict__ PT,
     }
     L.head[c] = first;
     L.dflag[c] = 0;
-    // 3. the rows of every particle around c are rebuilt in this pass (by
-    // the test kernel): the 27 cells are stamped with the pass
+    copy_slots(L, c, first, n);
+    // 3. the rows that read c are rebuilt in this pass (by the test
+    // kernel): a row of a particle in cell b holds the rest of b's list and
+    // the half-shell cells b + o, kx + Nx*(ky + Ny*kz) > 0, so c is read by
+    // the rows of c itself and of c + o' for the 13 offsets o' with
+    // kx + Nx*(ky + Ny*kz) < 0; those 14 cells are stamped with the pass
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     const int cl = c - P.coff;
     const int cx = cl % nx, cy = (cl / nx) % ny, cz = cl / (nx * ny);
 #pragma unroll
-    for (int o = 0; o < 27; o++) {
+    for (int o = 0; o < 14; o++) {
       const int jx = cx + o % 3 - 1, jy = cy + (o / 3) % 3 - 1, jz = cz + o / 9 - 1;
       const bool ok = (P.pbc[0] || (jx >= 0 && jx < nx)) && (P.pbc[1] || (jy >= 0 && jy < ny)) &&
                       (P.pbc[2] || (jz >= 0 && jz < nz));
@@ -192,10 +211,8 @@ __device__ __forceinline__ void relink_body(const DevParams* __restrict__ PT,
 template <bool PP>
 __device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int c,
                                           const double4* __restrict__ X,
-                                          const int* __restrict__ comp,
-                                          const int* __restrict__ head,
-                                          const int* __restrict__ next, const Rows& R,
-                                          Counters* cnt, int tag) {
+                                          const int* __restrict__ comp, const CellLists& L,
+                                          const Rows& R, Counters* cnt, int tag) {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int nx = P.nx, ny = P.ny, nz = P.nz;
@@ -203,7 +220,7 @@ __device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int 
   const int cx = cl % nx, cy = (cl / nx) % ny, cz = cl / (nx * ny);
   const double4 p4 = X[p];
   const int cp = PP ? 0 : comp[p];
-  int start = -1, order = 1 << 20;
+  int cw = -1, order = 1 << 20;  // the lane's cell, its place in the row
   bool walk = false;
   if (lane < 27) {
     const int d[3] = {lane % 3 - 1, (lane / 3) % 3 - 1, lane / 9 - 1};
@@ -224,14 +241,16 @@ __device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int 
     }
     const int lex = d[0] + 3 * d[1] + 9 * d[2];
     if (lane == 13) {
-      start = next[p];
+      cw = c;
       order = 0;
       walk = true;
     } else if (ok && lex > 0) {
-      start = head[P.coff + w[0] + nx * (w[1] + ny * w[2])];
+      cw = P.coff + w[0] + nx * (w[1] + ny * w[2]);
       order = 1 + (13 - lex);
       walk = true;
     }
+  } else if (lane == 27) {
+    cw = c;
   }
   const double skin = P.vl_skin;
   auto is_cand = [&](int q) -> bool {
@@ -246,31 +265,58 @@ __device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int 
     md = __dadd_rn(md, skin);
     return __dsub_rn(__dmul_rn(md, md), DijSq) > 0.0;
   };
-  // pass 1: walk and count; the first 8 list elements and their test
-  // results stay in registers for pass 2.  Lane 27 counts the list before p.
+  // the lane's cell read from its slots when its whole list is there
+  // (independent loads), else by walking its links
+  const int len = cw >= 0 ? L.slot_n[cw] : -1;
+  const bool arr = len >= 0 && len <= SLOT_CAP;
+  const int* sl = L.slot + (size_t)(cw >= 0 ? cw : 0) * SLOT_CAP;
+  // pass 1: count the candidates; lane 13 (own cell after p) and lane 27
+  // (p's rank: the list before p) first find p in its cell.  Slots: the hits
+  // are a bit mask for pass 2; links: the first 8 elements and their test
+  // results stay in registers for pass 2.
   int count = 0, walked = 0;
   unsigned hits = 0u;
   int cache[8];
   bool bad = false;
-  int q = start;
+  int q = -1;
 #pragma unroll
   for (int i = 0; i < 8; i++) cache[i] = -1;
-  if (walk) {
-#pragma unroll
-    for (int i = 0; i < 8; i++) {
-      if (q != -1) {
-        cache[i] = q;
-        walked = i + 1;
-        if (is_cand(q)) {
-          hits |= 1u << i;
+  if (arr) {
+    int k0 = 0;
+    if (lane == 13 || lane == 27) {
+      int r = 0;
+      while (r < len && sl[r] != p) r++;
+      if (r == len) bad = true;
+      if (lane == 27) count = r;
+      k0 = r + 1;
+    }
+    if (walk && !bad) {
+#pragma unroll 4
+      for (int k = k0; k < len; k++)
+        if (is_cand(sl[k])) {
+          hits |= 1u << k;
           count++;
         }
-        q = next[q];
+    }
+  } else if (cw >= 0) {
+    q = lane == 13 ? L.next[p] : L.head[cw];
+    if (walk) {
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        if (q != -1) {
+          cache[i] = q;
+          walked = i + 1;
+          if (is_cand(q)) {
+            hits |= 1u << i;
+            count++;
+          }
+          q = L.next[q];
+        }
       }
     }
   }
-  const int resume = q;  // first element not cached (-1: none)
-  {
+  const int resume = q;  // (links) first element not cached (-1: none)
+  if (!arr && cw >= 0) {
     int guard = 0;
     if (walk) {
       while (q != -1) {
@@ -279,17 +325,16 @@ __device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int 
           break;
         }
         if (is_cand(q)) count++;
-        q = next[q];
+        q = L.next[q];
       }
     } else if (lane == 27) {
-      q = head[c];
       while (q != p) {
         if (q == -1 || ++guard > n) {
           bad = true;
           break;
         }
         count++;
-        q = next[q];
+        q = L.next[q];
       }
     }
   }
@@ -317,16 +362,25 @@ __device__ __forceinline__ void build_row(const DevParams& P, int n, int p, int 
     }
     return;
   }
-  // pass 2: write (the cached part, then the rest of the list)
+  // pass 2: write (slots: the hits; links: the cached part, then the rest)
   if (walk) {
     int k = off;
+    if (arr) {
+      unsigned h = hits;
+      while (h) {
+        const int j = __ffs(h) - 1;
+        h &= h - 1u;
+        R.cand[(size_t)(k++) * n + p] = sl[j];
+      }
+    } else {
 #pragma unroll
-    for (int i = 0; i < 8; i++)
-      if (i < walked && ((hits >> i) & 1u)) R.cand[(size_t)(k++) * n + p] = cache[i];
-    int q2 = resume;
-    while (q2 != -1) {
-      if (is_cand(q2)) R.cand[(size_t)(k++) * n + p] = q2;
-      q2 = next[q2];
+      for (int i = 0; i < 8; i++)
+        if (i < walked && ((hits >> i) & 1u)) R.cand[(size_t)(k++) * n + p] = cache[i];
+      int q2 = resume;
+      while (q2 != -1) {
+        if (is_cand(q2)) R.cand[(size_t)(k++) * n + p] = q2;
+        q2 = L.next[q2];
+      }
     }
   }
   if (lane == 0) {
@@ -411,8 +465,8 @@ __device__ __forceinline__ void test_body(const TestArgs& A, int vblock) {
         todo &= todo - 1u;
         const int pl = __shfl_sync(FULL, p, l);
         const int cl = __shfl_sync(FULL, cp0, l);
-        build_row<PP>(sys_params(A.P, A.sysid, pl), n, pl, cl, A.X, A.comp, A.L.head, A.L.next,
-                      A.R, A.cnt, A.tag);
+        build_row<PP>(sys_params(A.P, A.sysid, pl), n, pl, cl, A.X, A.comp, A.L, A.R, A.cnt,
+                      A.tag);
       }
       __syncwarp();  // the rows written by the warp are visible to their owners
 #pragma unroll
