@@ -49,6 +49,9 @@ WORKLOADS = {
     "ensemble4096": dict(kind="ensemble", n_systems=4096, seed=1003, skip=3000),
     "bidisperse4m": dict(kind="bidisperse", n=4_000_000, seed=1004),
     "ensemble64": dict(kind="ensemble", n_systems=64, seed=1003),
+    # small systems (200-2,000 spheres), where a step is a few microseconds of
+    # work per kernel: the case for one persistent launch per 4-step chunk
+    "ensemble16small": dict(kind="ensemble", n_systems=16, seed=1003, nmin=200, nmax=2000),
     # above jamming (about six contacts per sphere): the contact-dense case
     "jammed1m": dict(n=1_000_000, phi=0.65, seed=1012, tile=8000, relax=4000),
     "jammed16m": dict(n=16_000_000, phi=0.65, seed=1012, tile=16000, relax=4000),
@@ -807,6 +810,7 @@ def run_ensemble(args):
     # one ensemble for the whole job; rank r advances every world-th system
     # (no exchange between ranks: the systems are independent)
     e_all = configs.settling_ensemble(n_systems=spec["n_systems"], seed=spec["seed"],
+                                      nmin=spec.get("nmin", 200), nmax=spec.get("nmax", 20000),
                                       precision=P.PREC_MIXED if prec == "mixed" else P.PREC_FP64)
     e = e_all.shard(rank, world)
     t_gen = time.perf_counter() - t0
@@ -883,7 +887,8 @@ def run_ensemble(args):
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "f32+f64" if prec == "mixed" else "f64", "data": "synthetic",
             "config": {"workload": (f"{len(e.counts)} gravity-settling systems, sizes log-uniform "
-                                    f"in [200, 20000] ({n:,} spheres), R~U[0.45,0.55], per-system "
+                                    f"in [{spec.get('nmin', 200)}, {spec.get('nmax', 20000)}] "
+                                    f"({n:,} spheres), R~U[0.45,0.55], per-system "
                                     "mu~U[0.2,0.8], e~U[0.5,0.95], 10x10 x-y periodic box with "
                                     "floor, dt=1e-4, ABM4, one context"),
                        "particles_per_gpu": n, "global_particles": e_all.n,
