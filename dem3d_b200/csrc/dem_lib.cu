@@ -1672,18 +1672,23 @@ SlabCols slab_cols_begin() {
 
 // the history rows of table b (counts, partners, values; FP32 values in
 // mixed mode), and with walls the wall rows
-void slab_hist_cols(const dem_ctx* c, SlabCols& C, int b, bool walls) {
+// (rows: the record slots carried, at most the capacity; a particle's
+// records past its count are not read)
+void slab_hist_cols(const dem_ctx* c, SlabCols& C, int b, bool walls, int rows) {
   const History& H = c->H[b];
   const long long N = H.n;
   const bool mixed = c->precision == DEM_PREC_MIXED;
+  rows = std::min(rows, H.cap);
   slab_col(C, H.cnt, 4, 1, 0);
-  slab_col(C, H.key, 4, H.cap, N * 4);
-  if (mixed) {
-    slab_col(C, c->M.ha[b], 16, H.cap, N * 16);
-    slab_col(C, c->M.hb[b], 16, H.cap, N * 16);
-    slab_col(C, c->M.hc[b], 4, H.cap, N * 4);
-  } else {
-    slab_col(C, H.val, 48, H.cap, N * 48);
+  if (rows > 0) {
+    slab_col(C, H.key, 4, rows, N * 4);
+    if (mixed) {
+      slab_col(C, c->M.ha[b], 16, rows, N * 16);
+      slab_col(C, c->M.hb[b], 16, rows, N * 16);
+      slab_col(C, c->M.hc[b], 4, rows, N * 4);
+    } else {
+      slab_col(C, H.val, 48, rows, N * 48);
+    }
   }
   if (!walls) return;
   const int nw = std::max(c->params.n_walls, 1);
@@ -1699,7 +1704,7 @@ void slab_hist_cols(const dem_ctx* c, SlabCols& C, int b, bool walls) {
 
 // what a slab needs of a ghost for the pass on `side`: list link, pass
 // copies, cell, current history rows
-SlabCols slab_ghost_cols(const dem_ctx* c, int side) {
+SlabCols slab_ghost_cols(const dem_ctx* c, int side, int hrows) {
   const bool mixed = c->precision == DEM_PREC_MIXED;
   SlabCols C = slab_cols_begin();
   slab_col(C, c->L.next, 4, 1, 0);
@@ -1707,7 +1712,7 @@ SlabCols slab_ghost_cols(const dem_ctx* c, int side) {
   slab_col(C, c->v4[side], mixed ? 16 : 32, 1, 0);
   slab_col(C, c->w2[side], mixed ? 8 : 16, 1, 0);
   slab_col(C, c->L.cell[c->par], 4, 1, 0);
-  slab_hist_cols(c, C, c->hcur, false);
+  slab_hist_cols(c, C, c->hcur, false, hrows);
   return C;
 }
 
@@ -1726,7 +1731,7 @@ SlabCols slab_full_cols(const dem_ctx* c) {
     slab_col(C, c->w2[b], mixed ? 8 : 16, 1, 0);
     slab_col(C, c->L.cell[b], 4, 1, 0);
   }
-  for (int b = 0; b < 2; b++) slab_hist_cols(c, C, b, true);
+  for (int b = 0; b < 2; b++) slab_hist_cols(c, C, b, true, c->H[b].cap);
   return C;
 }
 
@@ -1753,6 +1758,18 @@ int slab_list_layer(dem_ctx* c, int z, int* count) {
   CK(cudaStreamSynchronize(c->stream));
   if (h[1]) return fail(c, DEM_ERR_STATE, "slab: a cell list of a boundary layer is inconsistent");
   *count = h[0];
+  return DEM_OK;
+}
+
+// the largest v[p] over the particles of c->slab_list[0..count)
+int slab_max_over(dem_ctx* c, int count, const int* v, int* out) {
+  *out = 0;
+  if (count == 0) return DEM_OK;
+  CK(cudaMemsetAsync(c->slab_count + 2, 0, sizeof(int), c->stream));
+  launch(c, "slab_max_of", k_slab_max_of, blocks_for(count, 256), 256, (const int*)c->slab_list,
+         count, v, c->slab_count + 2);
+  CK(cudaMemcpyAsync(out, c->slab_count + 2, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   return DEM_OK;
 }
 
@@ -3527,15 +3544,20 @@ int dem_slab_pack(dem_ctx* c, int32_t what, void* buf, int64_t cap, int64_t* byt
       if (!slab_has_down(c)) return slab_write(c, what, slab_cols_begin(), 0, {}, buf, cap, bytes);
       const int nxy = slab_nxy(c);
       const int cb = slab_layer(c, c->slab_z0), cr = slab_layer(c, c->slab_z0 - 1);
-      extra.resize(1 + 2 * (size_t)nxy);
+      extra.resize(2 + 2 * (size_t)nxy);
       extra[0] = cb;
-      CK(cudaMemcpyAsync(extra.data() + 1, c->L.head + cb, sizeof(int) * nxy,
+      CK(cudaMemcpyAsync(extra.data() + 2, c->L.head + cb, sizeof(int) * nxy,
                          cudaMemcpyDeviceToHost, c->stream));
-      CK(cudaMemcpyAsync(extra.data() + 1 + nxy, c->L.rflag + cr, sizeof(int) * nxy,
+      CK(cudaMemcpyAsync(extra.data() + 2 + nxy, c->L.rflag + cr, sizeof(int) * nxy,
                          cudaMemcpyDeviceToHost, c->stream));
       st = slab_list_layer(c, c->slab_z0, &count);
       if (st) return st;
-      return slab_write(c, what, slab_ghost_cols(c, c->prepared), count, extra, buf, cap,
+      // the records carry as many history slots as the fullest table needs
+      int hrows = 0;
+      st = slab_max_over(c, count, c->H[c->hcur].cnt, &hrows);
+      if (st) return st;
+      extra[1] = hrows;
+      return slab_write(c, what, slab_ghost_cols(c, c->prepared, hrows), count, extra, buf, cap,
                         bytes);
     }
     case DEM_SLAB_LOWER: {
@@ -3552,15 +3574,24 @@ int dem_slab_pack(dem_ctx* c, int32_t what, void* buf, int64_t cap, int64_t* byt
       // the "j" results and matched bits of the ghosts received this pass,
       // for their owner (the slab above)
       const int rec = (int)in_rec_bytes(c);
-      const int64_t item = SLAB_ID + (int64_t)c->in_cap * rec;
+      // as many result slots as the ghost with the most results
+      int slots = 0;
+      if (c->n_ghosts > 0) {
+        CK(cudaMemcpyAsync(c->slab_list, c->slab_ghosts, sizeof(int) * (size_t)c->n_ghosts,
+                           cudaMemcpyDeviceToDevice, c->stream));
+        int st2 = slab_max_over(c, c->n_ghosts, c->in_cnt, &slots);
+        if (st2) return st2;
+        slots = std::min(slots, c->in_cap);
+      }
+      const int64_t item = SLAB_ID + (int64_t)slots * rec;
       const int64_t total = SLAB_HEAD + 16 + (int64_t)c->n_ghosts * item;
       *bytes = total;
       if (total > cap) return fail(c, DEM_ERR_CAPACITY, "slab: the exchange buffer is too small");
-      int h[8] = {what, c->n_ghosts, (int)item, 4, c->in_cap, rec, 0, 0};
+      int h[8] = {what, c->n_ghosts, (int)item, 4, slots, rec, 0, 0};
       CK(cudaMemcpyAsync(buf, h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
       launch(c, "slab_jhalf_pack", k_slab_jhalf_pack, blocks_for(c->n_ghosts, 128), 128,
              (const int*)c->slab_ghosts, c->n_ghosts, c->in_cnt, (const char*)c->in_rec,
-             c->in_cap, c->pass_cap, rec, c->matched, (char*)buf + SLAB_HEAD + 16);
+             slots, c->pass_cap, rec, c->matched, (char*)buf + SLAB_HEAD + 16);
       CK(cudaStreamSynchronize(c->stream));
       return DEM_OK;
     }
@@ -3613,14 +3644,15 @@ int dem_slab_unpack(dem_ctx* c, int32_t what, const void* buf, int64_t bytes) {
     case DEM_SLAB_GHOSTS: {
       if (count == 0 && h[3] == 0) return DEM_OK;
       const int nxy = slab_nxy(c);
-      const SlabCols C = slab_ghost_cols(c, c->prepared);
-      if (h[3] != 1 + 2 * nxy || h[4] != slab_layer(c, c->slab_z1) || rec != C.rec)
+      if (h[3] != 2 + 2 * nxy || h[4] != slab_layer(c, c->slab_z1))
         return fail(c, DEM_ERR_INVALID, "slab: ghosts from a slab that is not the one above");
       const int* ex = h.data() + 4;
-      CK(cudaMemcpyAsync(c->L.head + ex[0], ex + 1, sizeof(int) * nxy, cudaMemcpyHostToDevice,
+      const SlabCols C = slab_ghost_cols(c, c->prepared, ex[1]);
+      if (rec != C.rec) return fail(c, DEM_ERR_INVALID, "slab: ghosts with another layout");
+      CK(cudaMemcpyAsync(c->L.head + ex[0], ex + 2, sizeof(int) * nxy, cudaMemcpyHostToDevice,
                          c->stream));
       // stamps: rows of this slab's top layer whose neighbourhood changed
-      CK(cudaMemcpyAsync(c->slab_list, ex + 1 + nxy, sizeof(int) * nxy, cudaMemcpyHostToDevice,
+      CK(cudaMemcpyAsync(c->slab_list, ex + 2 + nxy, sizeof(int) * nxy, cudaMemcpyHostToDevice,
                          c->stream));
       launch(c, "slab_max", k_slab_max, blocks_for(nxy, 256), 256,
              c->L.rflag + slab_layer(c, c->slab_z1 - 1), (const int*)c->slab_list, nxy);
@@ -3647,11 +3679,12 @@ int dem_slab_unpack(dem_ctx* c, int32_t what, const void* buf, int64_t bytes) {
     }
     case DEM_SLAB_JHALVES: {
       if (count == 0) return DEM_OK;
-      const int in_cap = h[4], r = h[5];
-      if (r != (int)in_rec_bytes(c) || in_cap != c->in_cap)
+      const int slots = h[4], r = h[5];
+      if (r != (int)in_rec_bytes(c) || slots > c->in_cap || rec != SLAB_ID + slots * r)
         return fail(c, DEM_ERR_INVALID, "slab: results from a slab with another layout");
       launch(c, "slab_jhalf_unpack", k_slab_jhalf_unpack, blocks_for(count, 128), 128, recs,
-             count, c->in_cnt, (char*)c->in_rec, c->in_cap, c->pass_cap, r, c->matched, c->cnt);
+             count, c->in_cnt, (char*)c->in_rec, c->in_cap, slots, c->pass_cap, r, c->matched,
+             c->cnt);
       break;
     }
     case DEM_SLAB_MIGRATE_UP:

@@ -97,6 +97,14 @@ __global__ void k_slab_cols(SlabCols C, const int* __restrict__ list, int count,
   else *(int*)(C.dst[k] + at) = *(const int*)(rec + byte);
 }
 
+// *out = max(*out, v[ids[i]]) over the items (the fullest history table or
+// result list of an exchange: the records carry that many slots)
+__global__ void k_slab_max_of(const int* __restrict__ ids, int count, const int* __restrict__ v,
+                              int* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) atomicMax(out, v[ids[i]]);
+}
+
 // dst[i] = max(dst[i], src[i]) (rebuild stamps of a layer)
 __global__ void k_slab_max(int* __restrict__ dst, const int* __restrict__ src, int m) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -108,13 +116,13 @@ __global__ void k_slab_max(int* __restrict__ dst, const int* __restrict__ src, i
 // {q, count, matched, 0, slots...}; the ghosts' counts and bits are reset
 // here (their owner folds them).
 __global__ void k_slab_jhalf_pack(const int* __restrict__ ids, int count, int* __restrict__ in_cnt,
-                                  const char* __restrict__ in_rec, int in_cap, int stride, int rec,
+                                  const char* __restrict__ in_rec, int slots, int stride, int rec,
                                   unsigned* __restrict__ matched, char* __restrict__ buf) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   const int q = ids[i];
-  const int m = min(in_cnt[q], in_cap);
-  int* h = (int*)(buf + (size_t)i * (SLAB_ID + (size_t)in_cap * rec));
+  const int m = min(in_cnt[q], slots);
+  int* h = (int*)(buf + (size_t)i * (SLAB_ID + (size_t)slots * rec));
   h[0] = q;
   h[1] = m;
   h[2] = (int)matched[q];
@@ -132,11 +140,11 @@ __global__ void k_slab_jhalf_pack(const int* __restrict__ ids, int count, int* _
 // sweep key) and OR the matched bits in; too many for the room sets the
 // incoming overflow (the pass is then an error of the decomposition).
 __global__ void k_slab_jhalf_unpack(const char* __restrict__ buf, int count, int* __restrict__ in_cnt,
-                                    char* __restrict__ in_rec, int in_cap, int stride, int rec,
-                                    unsigned* __restrict__ matched, Counters* cnt) {
+                                    char* __restrict__ in_rec, int in_cap, int slots, int stride,
+                                    int rec, unsigned* __restrict__ matched, Counters* cnt) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
-  const int* h = (const int*)(buf + (size_t)i * (SLAB_ID + (size_t)in_cap * rec));
+  const int* h = (const int*)(buf + (size_t)i * (SLAB_ID + (size_t)slots * rec));
   const int q = h[0], m = h[1];
   matched[q] |= (unsigned)h[2];
   const int base = in_cnt[q];
