@@ -597,18 +597,25 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* a) {
   return v;
 }
 
-// All threads of every block call; returns false after a timeout.
+// All threads of every block call; returns false after a timeout.  The
+// block's thread 0 arrives with an acquire-release add (after the block
+// barrier, so it releases the whole block's writes); the last to arrive
+// resets the count and publishes the next generation with a release add;
+// the others poll the generation with acquire loads.
 __device__ __forceinline__ bool grid_sync(const GridSync& g) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
     const unsigned gen0 = ld_acquire_u32(g.gen);  // cannot advance before this block arrives
-    __threadfence();  // the block's writes before the arrival
-    if (atomicAdd(g.count, 1u) == g.expected - 1u) {
-      atomicExch(g.count, 0u);
-      __threadfence();
-      atomicAdd(g.gen, 1u);
+    unsigned prev;
+    asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;"
+                 : "=r"(prev)
+                 : "l"(g.count)
+                 : "memory");
+    if (prev == g.expected - 1u) {
+      *(volatile unsigned*)g.count = 0u;
+      asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(g.gen) : "memory");
     } else {
       const unsigned long long t0 = global_ns();
       while (ld_acquire_u32(g.gen) == gen0) {
@@ -618,10 +625,9 @@ __device__ __forceinline__ bool grid_sync(const GridSync& g) {
           ok = 0;
           break;
         }
-        __nanosleep(100);
+        __nanosleep(32);
       }
     }
-    __threadfence();  // everything written before the other blocks arrived
     s_ok = ok;
   }
   __syncthreads();
