@@ -273,9 +273,21 @@ __device__ __forceinline__ void pair_mixed_body(const PassArgs<float4, float2>& 
   unsigned n_col = 0;
   int need = 0, need_in = 0;
   bool overflow = false, in_over = false;
-  for (int s = vblock * blockDim.x + threadIdx.x; s < total; s += vgrid * blockDim.x) {
+  const int stride = vgrid * blockDim.x;
+  for (int s = vblock * blockDim.x + threadIdx.x; s < total; s += stride) {
     const int2 e = A.clist[s];
     const int p = e.x, q = e.y;
+    // the next contact of this thread: its pair's data requested into L2
+    // now, so that the next iteration's gathers overlap this one's work
+    if (s + stride < total) {
+      const int2 e2 = A.clist[s + stride];
+      prefetch_l2(A.X + e2.x);
+      prefetch_l2(A.X + e2.y);
+      prefetch_l2(A.v4 + e2.x);
+      prefetch_l2(A.v4 + e2.y);
+      prefetch_l2(Hr.key + e2.x);
+      prefetch_l2(A.in_cnt + e2.y);
+    }
     const int s_in = atomicAdd(&A.in_cnt[q], 1);  // q's "j" record (returns early)
     const int ord = s - A.cstart[p];
     const int hc = Hr.cnt[p];
