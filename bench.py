@@ -583,6 +583,8 @@ def run_ours(args):
         s = DEMSystem(w.params)
         s.set_state(w.pos, w.vel, w.omega, comp=w.comp, radius=w.radius)
         s.initialize_cell_distribution()
+        if args.reorder_every > 0:
+            s.set_reorder(args.reorder_every)
         res[prec] = measure(s, w, args, world, local, torch, dist)
         systems[prec] = s
     s = systems[headline]
@@ -740,7 +742,8 @@ def run_ours(args):
             "ms_per_step": ms / res[headline]["steps"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if headline == "fp64" else "f32+f64", "data": "synthetic",
-            "config": config_block(args.workload, w, world, headline),
+            "config": dict(config_block(args.workload, w, world, headline),
+                           storage_reorder_every=args.reorder_every),
             "gpu_launches": int(launches),
             "launches_per_step": launches / res[headline]["steps"],
             "precisions": {p: {"value": r["value"], "ms_per_step": r["ms"] / r["steps"],
@@ -1007,6 +1010,9 @@ def main():
                     help="steps between the samples of --obs-window")
     ap.add_argument("--no-autotune", action="store_true",
                     help="skip the autotuner's trials (default settings)")
+    ap.add_argument("--reorder-every", type=int, default=0,
+                    help="keep the particle storage in cell order, permuting it every N steps "
+                         "of the run (0: never)")
     ap.add_argument("--slabs", type=int, default=0,
                     help="cut the system into this many z-slabs on one GPU (the spatial "
                          "decomposition, emulated) and report its cost and bit-exactness")

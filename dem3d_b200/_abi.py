@@ -193,6 +193,8 @@ GPU_ONLY = {
     "get_launch_shape": (C.c_int, [_P, _I32P, _I32P, _I32P, _I32P]),
     "set_persistent_barrier": (C.c_int, [_P, C.c_double, C.c_int32]),
     "get_persistent_blocks": (C.c_int, [_P, _I32P]),
+    "set_reorder": (C.c_int, [_P, C.c_int32]),
+    "get_reorder": (C.c_int, [_P, _I32P, _I64P]),
     "slab_set_range": (C.c_int, [_P, C.c_int32, C.c_int32]),
     "slab_phase": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32]),
     "slab_pack": (C.c_int, [_P, C.c_int32, _P, C.c_int64, _I64P]),

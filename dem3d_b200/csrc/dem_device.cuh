@@ -165,6 +165,10 @@ struct CellLists {
   // independent loads instead of walking its links one after the other
   int* slot;
   int* slot_n;
+  // the reference's index of the particle stored at each place, when the
+  // storage is kept in cell order (the relink orders arrivals by it); NULL:
+  // stored in the reference's order
+  const int* gid;
 };
 constexpr int SLOT_CAP = 32;
 

@@ -518,6 +518,80 @@ __global__ void __launch_bounds__(256) k_prepare(const DevParams* __restrict__ P
   publish_disp(cnt, d2);
 }
 
+// ---------------------------------------------------------------------------
+// Storage in cell order (dem_set_reorder): the permutation pi (new place s
+// holds the particle stored at pi[s]) is the cells' lists in cell order.
+
+// pi[cell_start[c] + k] = the k-th particle of cell c's list
+__global__ void k_reorder_fill(CellLists L, int ncell, const int* __restrict__ cell_start,
+                               int* __restrict__ pi, int n, int* __restrict__ err) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  int k = cell_start[c];
+  const int end = cell_start[c + 1];
+  for (int q = L.head[c]; q != -1; q = L.next[q]) {
+    if (k >= end || q < 0 || q >= n) {
+      atomicExch(err, 1);
+      return;
+    }
+    pi[k++] = q;
+  }
+  if (k != end) atomicExch(err, 1);
+}
+
+// the list length of every cell (the slots record it)
+__global__ void k_reorder_counts(const CellLists L, int ncell, int* __restrict__ cnt,
+                                 int* __restrict__ err) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  const int m = L.slot_n[c];
+  if (m < 0) atomicExch(err, 1);
+  cnt[c] = m < 0 ? 0 : m;
+}
+
+__global__ void k_iota(int n, int* __restrict__ a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = i;
+}
+
+__global__ void k_inverse(int n, const int* __restrict__ pi, int* __restrict__ inv) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) inv[pi[s]] = s;
+}
+
+// dst row r, place s <- base row r, place pi[s] (elem bytes, a multiple of 4)
+__global__ void k_gather_col(const char* __restrict__ base, int elem, int rows, long long stride,
+                             int n, const int* __restrict__ pi, char* __restrict__ dst) {
+  const long long words = (long long)elem / 4;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= words * n * rows) return;
+  const int w = (int)(t % words);
+  const long long rs = t / words;
+  const int s = (int)(rs % n), r = (int)(rs / n);
+  ((int*)(dst + ((long long)r * n + s) * elem))[w] =
+      ((const int*)(base + (long long)r * stride + (long long)pi[s] * elem))[w];
+}
+
+__global__ void k_scatter_col(char* __restrict__ base, int elem, int rows, long long stride, int n,
+                              const char* __restrict__ src) {
+  const long long words = (long long)elem / 4;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= words * n * rows) return;
+  const int w = (int)(t % words);
+  const long long rs = t / words;
+  const int s = (int)(rs % n), r = (int)(rs / n);
+  ((int*)(base + (long long)r * stride + (long long)s * elem))[w] =
+      ((const int*)(src + ((long long)r * n + s) * elem))[w];
+}
+
+// stored particle numbers in a[0..m) renamed by inv (other values kept)
+__global__ void k_remap(int* __restrict__ a, long long m, const int* __restrict__ inv, int n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int v = a[i];
+  if (v >= 0 && v < n) a[i] = inv[v];
+}
+
 // The slots of cells [c_begin, c_begin + ncells) from their lists (after
 // the lists were built or changed outside the relink).
 __global__ void k_cell_slots(CellLists L, int c_begin, int ncells, int n) {

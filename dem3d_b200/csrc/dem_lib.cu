@@ -166,6 +166,16 @@ struct dem_ctx {
   int n_ghosts = 0;
   int* slab_count = nullptr;  // device counters of the list kernels
   RingMap slab_rm{};          // the ring map of the pass in progress
+  // storage in cell order (dem_set_reorder): every reorder_every steps of
+  // dem_run the particle arrays are permuted into the cells' list order;
+  // gid[s] is the reference's index of the particle stored at s (L.gid);
+  // calls that read or write particle data restore the reference's order
+  int reorder_every = 0;
+  long long since_reorder = 0;
+  long long reorders = 0;
+  bool permuted = false;
+  int* gid = nullptr;
+  int gid_cap = 0;
   bool has_cone = false; // some wall of some system is a cone
   double skin_factor = 0.05;  // candidate-row skin / CutOff
   int par = 0;         // L.cell[par] is the assignment the lists hold
@@ -221,6 +231,15 @@ int cuda_fail(dem_ctx* c, cudaError_t e, const char* where) {
   do {                                                        \
     cudaError_t e_ = (call);                                  \
     if (e_ != cudaSuccess) return cuda_fail(c, e_, #call);    \
+  } while (0)
+
+int restore_order(dem_ctx* c);
+
+// calls that read or write particle data see the reference's order
+#define RESTORE_ORDER                \
+  do {                               \
+    int st_ = restore_order(c);      \
+    if (st_) return st_;             \
   } while (0)
 
 int stat_index(dem_ctx* c, const char* name) {
@@ -364,6 +383,11 @@ void free_lists(dem_ctx* c) {
 void free_state(dem_ctx* c) {
   cudaFree(c->sysid);
   c->sysid = nullptr;
+  cudaFree(c->gid);
+  c->gid = nullptr;
+  c->gid_cap = 0;
+  c->L.gid = nullptr;
+  c->permuted = false;
   cudaFree(c->staging);
   c->staging = nullptr;
   cudaFree(c->state_block);
@@ -474,6 +498,12 @@ int grow_capacity(dem_ctx* c, int newcap) {
   if (newcap <= c->ncap) return DEM_OK;
   CK(cudaStreamSynchronize(c->stream));
   drop_graphs(c);
+  // (called in the reference's order: gid is the identity and is made again
+  // for the new capacity at the next reorder)
+  cudaFree(c->gid);
+  c->gid = nullptr;
+  c->gid_cap = 0;
+  c->L.gid = nullptr;
   const size_t n = (size_t)c->n, N = (size_t)newcap;
   auto fresh = [&](auto*& p, size_t elems, size_t keep) -> cudaError_t {
     using T = std::remove_reference_t<decltype(*p)>;
@@ -1154,6 +1184,7 @@ int canonical_history(dem_ctx* c) {
 // pass rebuilds every candidate row.
 int update_particle_list_impl(dem_ctx* c, int64_t* removed) {
   if (removed) *removed = 0;
+  RESTORE_ORDER;
   if (c->nsys > 1) return fail(c, DEM_ERR_UNSUPPORTED, "particle removal needs one system");
   const int n0 = c->n;
   if (n0 == 0) return DEM_OK;
@@ -1312,6 +1343,7 @@ bool pour_active(const dem_ctx* c) {
 // that fits), and the sphere goes in at index n.
 int pour_particle_impl(dem_ctx* c, int32_t* inserted) {
   if (inserted) *inserted = 0;
+  RESTORE_ORDER;
   if (!pour_active(c)) return DEM_OK;
   const dem_pouring& Pp = c->pour;
   const int NC = c->params.n_components;
@@ -1813,6 +1845,138 @@ int slab_read_head(dem_ctx* c, const void* buf, int64_t bytes, int what, std::ve
   return DEM_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Storage in cell order (dem_set_reorder).
+
+// Permute every particle array: place s takes the particle stored at pi[s]
+// (pi a device array of n places); the stored particle numbers (cell
+// lists, slots, arrival lists, history partners) are renamed, and the next
+// pass rebuilds every candidate row.
+int permute_particles(dem_ctx* c, const int* pi) {
+  const int n = c->n;
+  if (n == 0) return DEM_OK;
+  SlabCols C = slab_full_cols(c);
+  auto col = [&](const void* base, int elem) { slab_col(C, base, elem, 1, 0); };
+  col(c->comp, 4);
+  col(c->radius, 8);
+  col(c->gid, 4);
+  if (c->sysid) col(c->sysid, 4);
+  col(c->L.next, 4);
+  col(c->L.arr_next, 4);
+  col(c->L.mflag, 4);
+  col(c->L.mnext, 4);
+  col(c->rows.meta, 4);
+  col(c->rows.rank, 4);
+  col(c->in_cnt, 4);
+  col(c->matched, 4);
+  size_t most = 0;
+  for (int k = 0; k < C.n; k++) most = std::max(most, (size_t)C.elem[k] * C.rows[k] * (size_t)n);
+  char* tmp = nullptr;
+  int* inv = nullptr;
+  CK(cudaMalloc(&tmp, most));
+  CK(cudaMalloc(&inv, sizeof(int) * (size_t)n));
+  for (int k = 0; k < C.n; k++) {
+    const long long thr = (long long)C.elem[k] / 4 * n * C.rows[k];
+    const unsigned g = (unsigned)((thr + 255) / 256);
+    launch(c, "reorder_gather", k_gather_col, g, 256u, C.src[k], C.elem[k], C.rows[k],
+           C.stride[k], n, pi, tmp);
+    launch(c, "reorder_scatter", k_scatter_col, g, 256u, C.dst[k], C.elem[k], C.rows[k],
+           C.stride[k], n, (const char*)tmp);
+  }
+  launch(c, "inverse", k_inverse, blocks_for(n, 256), 256, n, pi, inv);
+  auto remap = [&](int* a, long long m) {
+    if (m > 0)
+      launch(c, "remap", k_remap, (unsigned)((m + 255) / 256), 256u, a, m, (const int*)inv, n);
+  };
+  const long long nc = c->ncell_total;
+  remap(c->L.next, n);
+  remap(c->L.arr_next, n);
+  remap(c->L.mnext, n);
+  remap(c->L.head, nc);
+  remap(c->L.arr_head, nc);
+  remap(c->L.slot, nc * SLOT_CAP);
+  for (int b = 0; b < 2; b++) remap(c->H[b].key, (long long)c->H[b].cap * c->H[b].n);
+  const int one = 1;
+  CK(cudaMemcpyAsync(&c->cnt->force_full, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  cudaFree(tmp);
+  cudaFree(inv);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(c, e, "reorder");
+  return DEM_OK;
+}
+
+// gid for the whole capacity, the identity while the storage is in the
+// reference's order (the relink reads it through L.gid, so a new array
+// means new graphs)
+int ensure_gid(dem_ctx* c) {
+  if (c->gid && c->gid_cap >= c->ncap) return DEM_OK;
+  if (c->permuted) return fail(c, DEM_ERR_STATE, "reorder: capacity changed while permuted");
+  cudaFree(c->gid);
+  c->gid = nullptr;
+  const int cap = std::max(c->ncap, 1);
+  CK(cudaMalloc(&c->gid, sizeof(int) * (size_t)cap));
+  launch(c, "iota", k_iota, blocks_for(cap, 256), 256, cap, c->gid);
+  c->gid_cap = cap;
+  c->L.gid = c->gid;
+  drop_graphs(c);
+  return DEM_OK;
+}
+
+// the particles into the cells' list order (cell by cell, each list in
+// order): gathers from one cell's particles then read neighbouring memory
+int reorder_by_cell(dem_ctx* c) {
+  const int n = c->n, nc = c->ncell_total;
+  if (n == 0) return DEM_OK;
+  {
+    int st = ensure_gid(c);
+    if (st) return st;
+  }
+  int* pi = nullptr;
+  CK(cudaMalloc(&pi, sizeof(int) * (size_t)n));
+  int* dev_err = nullptr;
+  CK(cudaMalloc(&dev_err, sizeof(int)));
+  CK(cudaMemsetAsync(dev_err, 0, sizeof(int), c->stream));
+  launch(c, "reorder_counts", k_reorder_counts, blocks_for(nc, 256), 256, c->L, nc, c->cell_cnt,
+         dev_err);
+  launch(c, "scan_tiles", k_scan_tiles, (unsigned)c->n_tiles, SCAN_THREADS,
+         (const int*)c->cell_cnt, nc, c->cell_start, c->scan_bsum, (const Counters*)c->cnt);
+  launch(c, "scan_bsums", k_scan_bsums, 1u, SCAN_THREADS, c->scan_bsum, c->n_tiles,
+         c->cell_start, nc, (const Counters*)c->cnt);
+  launch(c, "scan_add", k_scan_add, blocks_for(nc, 256), 256, c->cell_start, nc,
+         (const int*)c->scan_bsum, (const Counters*)c->cnt);
+  launch(c, "reorder_fill", k_reorder_fill, blocks_for(nc, 256), 256, c->L, nc,
+         (const int*)c->cell_start, pi, n, dev_err);
+  int h_err = 0, total = 0;
+  CK(cudaMemcpyAsync(&h_err, dev_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(&total, c->cell_start + nc, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  cudaFree(dev_err);
+  int st = DEM_OK;
+  if (h_err || total != n) st = fail(c, DEM_ERR_STATE, "reorder: cell lists inconsistent");
+  else st = permute_particles(c, pi);
+  cudaFree(pi);
+  if (st) return st;
+  c->permuted = true;
+  c->reorders++;
+  return DEM_OK;
+}
+
+// back to the reference's order (place g holds the particle numbered g)
+int restore_order(dem_ctx* c) {
+  if (!c->permuted) return DEM_OK;
+  const int n = c->n;
+  int* pi = nullptr;
+  CK(cudaMalloc(&pi, sizeof(int) * (size_t)std::max(n, 1)));
+  if (n > 0) launch(c, "inverse", k_inverse, blocks_for(n, 256), 256, n, (const int*)c->gid, pi);
+  int st = permute_particles(c, pi);
+  cudaFree(pi);
+  if (st) return st;
+  c->permuted = false;
+  return DEM_OK;
+}
+
+
 }  // namespace
 
 // ===========================================================================
@@ -2086,6 +2250,7 @@ int dem_create_ensemble(const dem_params* ps, int32_t nsys, dem_ctx** out) {
 
 int dem_set_system_counts(dem_ctx* c, const int32_t* counts) {
   if (!c || !counts) return DEM_ERR_INVALID;
+  RESTORE_ORDER;
   long long off = 0;
   for (int s = 0; s < c->nsys; s++) {
     if (counts[s] < 0) return fail(c, DEM_ERR_INVALID, "negative system size");
@@ -2109,6 +2274,7 @@ void dem_destroy(dem_ctx* c) {
   drop_graphs(c);
   free_state(c);
   cudaFree(c->bar);
+  cudaFree(c->gid);
   cudaFree(c->gstamp);
   cudaFree(c->slab_list);
   cudaFree(c->slab_ghosts);
@@ -2147,6 +2313,7 @@ int dem_set_state(dem_ctx* c, int32_t n, const int32_t* comp, const double* radi
                   const double* pos, const double* vel, const double* omega, const double* acc,
                   const double* alpha) {
   if (!c) return DEM_ERR_INVALID;
+  RESTORE_ORDER;
   if (n < 0 || !pos || !vel || !omega) return fail(c, DEM_ERR_INVALID, "bad state arrays");
   if (!c->pp && !comp) return fail(c, DEM_ERR_INVALID, "component indices required");
   if (c->pp && !radius) return fail(c, DEM_ERR_INVALID, "per-particle radii required");
@@ -2316,6 +2483,7 @@ static int put_state_arrays(dem_ctx* c, const StateArrays& s, const double* pos,
 int dem_update_state(dem_ctx* c, const double* pos, const double* vel, const double* omega,
                      const double* acc, const double* alpha) {
   if (!c) return DEM_ERR_INVALID;
+  RESTORE_ORDER;
   if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
   // the Particle copies of the pass kernel are stale from here on
   if (c->prepared == 0) c->prepared = -1;
@@ -2343,12 +2511,14 @@ int dem_timer_stop(dem_ctx* c, double* ms) {
 int dem_get_state(dem_ctx* c, double* pos, double* vel, double* omega, double* acc,
                   double* alpha) {
   if (!c) return DEM_ERR_INVALID;
+  RESTORE_ORDER;
   return get_state_arrays(c, c->P, pos, vel, omega, acc, alpha);
 }
 
 int dem_get_predicted(dem_ctx* c, double* pos, double* vel, double* omega, double* acc,
                       double* alpha) {
   if (!c) return DEM_ERR_INVALID;
+  RESTORE_ORDER;
   return get_state_arrays(c, c->Pr, pos, vel, omega, acc, alpha);
 }
 
@@ -2360,6 +2530,7 @@ int dem_get_n(dem_ctx* c, int32_t* n) {
 
 int dem_set_integration(dem_ctx* c, const double* previous, const int32_t* ipc) {
   if (!c || !previous || !ipc) return DEM_ERR_INVALID;
+  RESTORE_ORDER;
   if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
   size_t N = (size_t)std::max(c->n, 1);
   // logical slot k (ipc(k+1)) -> physical slot k; spare = nprev
@@ -2380,6 +2551,7 @@ int dem_set_integration(dem_ctx* c, const double* previous, const int32_t* ipc) 
 
 int dem_get_integration(dem_ctx* c, double* previous, int32_t* ipc) {
   if (!c) return DEM_ERR_INVALID;
+  RESTORE_ORDER;
   if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
   size_t N = (size_t)std::max(c->n, 1);
   std::vector<double> tmp(9 * N * (c->nprev + 1));
@@ -2402,6 +2574,7 @@ int dem_set_contacts(dem_ctx* c, int64_t m, const int32_t* imin, const int32_t* 
                      const double* ft, const double* vt, int64_t mw, const int32_t* ip,
                      const int32_t* iw, const double* ftw, const double* vtw) {
   if (!c) return DEM_ERR_INVALID;
+  RESTORE_ORDER;
   if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
   const int n = c->n;
   size_t N = (size_t)std::max(n, 1);
@@ -2510,6 +2683,7 @@ int dem_get_contacts(dem_ctx* c, int64_t cap, int32_t* imin, int32_t* imax, doub
                      double* vt, int64_t capw, int32_t* ip, int32_t* iw, double* ftw,
                      double* vtw) {
   if (!c) return DEM_ERR_INVALID;
+  RESTORE_ORDER;
   if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
   HostHist h;
   int st = download_history(c, h);
@@ -2557,6 +2731,7 @@ int dem_get_contacts(dem_ctx* c, int64_t cap, int32_t* imin, int32_t* imax, doub
 
 int dem_initialize_cell_distribution(dem_ctx* c) {
   if (!c) return DEM_ERR_INVALID;
+  RESTORE_ORDER;
   if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
   int st = init_cells(c);
   if (st) return st;
@@ -2576,6 +2751,7 @@ int dem_get_grid(dem_ctx* c, int32_t* nxyz) {
 
 int dem_get_cells(dem_ctx* c, int32_t* cell_index, int32_t* traversal, int32_t* cell_start) {
   if (!c) return DEM_ERR_INVALID;
+  RESTORE_ORDER;
   int st = validate_ready(c);
   if (st) return st;
   CK(cudaStreamSynchronize(c->stream));
@@ -2609,6 +2785,7 @@ int dem_get_cells(dem_ctx* c, int32_t* cell_index, int32_t* traversal, int32_t* 
 // would have.  The lists must hold every particle once, in its own cell.
 int dem_set_cells(dem_ctx* c, const int32_t* traversal, const int32_t* cell_start) {
   if (!c || !traversal || !cell_start) return DEM_ERR_INVALID;
+  RESTORE_ORDER;
   if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
   const int n = c->n, ncell = c->ncell_total;
   if (cell_start[0] != 0 || cell_start[ncell] != n)
@@ -2678,6 +2855,7 @@ int dem_compute_accelerations(dem_ctx* c, int32_t use_predicted, double time_ste
 int dem_compute_forces(dem_ctx* c, int32_t use_predicted, double time_step, int32_t update,
                        double* force, double* torque) {
   if (!c || !force || !torque) return DEM_ERR_INVALID;
+  RESTORE_ORDER;
   int st = validate_ready(c);
   if (st) return st;
   c->force_out = c->staging;
@@ -2772,12 +2950,19 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
         if ((step + k) % c->pour.interval == 0) pour_inside = true;
     }
     poured_step = step;
+    // the storage back into cell order every reorder_every steps
+    if (c->reorder_every > 0 && !c->slab && c->since_reorder >= c->reorder_every) {
+      st = reorder_by_cell(c);
+      if (st) return st;
+      c->since_reorder = 0;
+    }
     if (remaining < G || c->prof || pour_inside) {
       st = move_particles_impl(c, step, true, 0);
       if (st) return st;
       st = remove_escaped();
       if (st) return st;
       step++;
+      c->since_reorder++;
       continue;
     }
     st = read_counters(c);
@@ -2858,6 +3043,7 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
       c->last_side = 1;
     }
     step += done;
+    c->since_reorder += done;
     c->time = (double)(step - 1) * dt;
     if (escape_stop) {
       // the replay's later wall copies ran: back to the walls of step-1
@@ -2944,6 +3130,7 @@ int dem_get_ncol(dem_ctx* c, int64_t* ncol) {
 
 int dem_set_fluid(dem_ctx* c, const dem_fluid* f) {
   if (!c) return DEM_ERR_INVALID;
+  RESTORE_ORDER;
   drop_graphs(c);
   if (!f) {
     c->fluid = false;
@@ -2975,6 +3162,7 @@ int dem_set_fluid(dem_ctx* c, const dem_fluid* f) {
 
 int dem_set_pouring(dem_ctx* c, const dem_pouring* p) {
   if (!c) return DEM_ERR_INVALID;
+  RESTORE_ORDER;
   if (!p) {
     c->pouring = false;
     drop_graphs(c);
@@ -3034,6 +3222,7 @@ int dem_set_particle_removal(dem_ctx* c, int32_t enable) {
 
 int dem_get_components(dem_ctx* c, int32_t* comp) {
   if (!c || !comp) return DEM_ERR_INVALID;
+  RESTORE_ORDER;
   if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
   CK(cudaStreamSynchronize(c->stream));
   if (c->n > 0) CK(cudaMemcpy(comp, c->comp, sizeof(int) * (size_t)c->n, cudaMemcpyDeviceToHost));
@@ -3439,6 +3628,7 @@ int dem_autotune(dem_ctx* c, int32_t first_step, int32_t steps_per_trial, int32_
 
 int dem_slab_set_range(dem_ctx* c, int32_t z0, int32_t z1) {
   if (!c) return DEM_ERR_INVALID;
+  RESTORE_ORDER;
   int st = validate_ready(c);
   if (st) return st;
   if (c->nsys != 1 || c->fluid || !c->wm.empty() || c->pouring)
@@ -3725,6 +3915,24 @@ int dem_slab_owned(dem_ctx* c, int32_t* owned) {
                 cudaMemcpyDeviceToHost));
   const int c0 = c->hsys[0].slab_c0, c1 = c->hsys[0].slab_c1;
   for (int i = 0; i < c->n; i++) owned[i] = cell[(size_t)i] >= c0 && cell[(size_t)i] < c1;
+  return DEM_OK;
+}
+
+int dem_set_reorder(dem_ctx* c, int32_t every_steps) {
+  if (!c) return DEM_ERR_INVALID;
+  if (every_steps < 0) return fail(c, DEM_ERR_INVALID, "reorder: steps must be >= 0");
+  if (every_steps > 0 && c->slab)
+    return fail(c, DEM_ERR_INVALID, "reorder: a slab keeps the system's own order");
+  RESTORE_ORDER;
+  c->reorder_every = every_steps;
+  c->since_reorder = every_steps;  // the next dem_run starts with a reorder
+  return DEM_OK;
+}
+
+int dem_get_reorder(dem_ctx* c, int32_t* every_steps, int64_t* reorders) {
+  if (!c) return DEM_ERR_INVALID;
+  if (every_steps) *every_steps = c->reorder_every;
+  if (reorders) *reorders = c->reorders;
   return DEM_OK;
 }
 

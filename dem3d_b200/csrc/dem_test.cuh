@@ -143,7 +143,9 @@ __device__ __forceinline__ void relink_body(const DevParams* __restrict__ PT,
       q = nq;
     }
     if (prev != -1) L.next[prev] = -1;
-    // 2. prepend the arrivals, highest index first
+    // 2. prepend the arrivals, highest index first (the reference's index:
+    // gid when the storage is in cell order)
+    auto G = [&](int x) { return L.gid ? L.gid[x] : x; };
     int sh = -1, tail = -1, a = L.arr_head[c];
     guard = 0;
     while (a != -1) {
@@ -157,12 +159,13 @@ __device__ __forceinline__ void relink_body(const DevParams* __restrict__ PT,
       if (sh == -1) {
         sh = tail = a;
         L.next[a] = -1;
-      } else if (a > sh) {
+      } else if (G(a) > G(sh)) {
         L.next[a] = sh;
         sh = a;
       } else {
         int q2 = sh;
-        for (int g2 = 0; L.next[q2] != -1 && L.next[q2] > a && g2 < guard; g2++) q2 = L.next[q2];
+        for (int g2 = 0; L.next[q2] != -1 && G(L.next[q2]) > G(a) && g2 < guard; g2++)
+          q2 = L.next[q2];
         L.next[a] = L.next[q2];
         L.next[q2] = a;
         if (L.next[a] == -1) tail = a;

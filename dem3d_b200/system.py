@@ -442,6 +442,18 @@ class DEMSystem:
         self._call("get_persistent_blocks", C.byref(v))
         return v.value
 
+    def set_reorder(self, every_steps: int) -> None:
+        """dem_set_reorder: dem_run keeps the particle storage in cell order,
+        permuting it every `every_steps` steps (0: never).  No result
+        changes; every call that reads particle data sees the reference's
+        order."""
+        self._call("set_reorder", C.c_int32(every_steps))
+
+    def reorder(self):
+        e, k = C.c_int32(), C.c_int64()
+        self._call("get_reorder", C.byref(e), C.byref(k))
+        return {"every_steps": e.value, "reorders": k.value}
+
     # ---- one slab of a spatial decomposition (dem_slab_*; dem3d_b200.slab)
     def slab_set_range(self, z0: int, z1: int) -> None:
         self._call("slab_set_range", C.c_int32(z0), C.c_int32(z1))

@@ -418,6 +418,21 @@ int dem_get_persistent_blocks(dem_ctx* ctx, int32_t* blocks);
 int dem_autotune(dem_ctx* ctx, int32_t first_step, int32_t steps_per_trial,
                  int32_t* last_step, double* trial_ms);
 
+/* Storage in cell order (no counterpart in the reference; changes no
+ * result).  With every_steps > 0, dem_run permutes the particles' arrays
+ * into the cells' list order before its first step and then every
+ * every_steps steps (state, Predicted, ABM ring, pass copies, history
+ * tables, cell lists, with every stored particle number renamed), so that
+ * the gathers of neighbouring spheres read neighbouring memory again after
+ * the spheres have moved.  The reference's numbering is kept alongside for
+ * the one rule of the step that depends on it (a cell's arrivals enter its
+ * list in decreasing index) and is restored before any call that reads or
+ * writes particle data or renumbers particles (states, contacts, cells,
+ * forces, removal, pouring).  0 (default): never.  *reorders: permutations
+ * done so far. */
+int dem_set_reorder(dem_ctx* ctx, int32_t every_steps);
+int dem_get_reorder(dem_ctx* ctx, int32_t* every_steps, int64_t* reorders);
+
 /* Spatial decomposition of one system into z-slabs (no counterpart in the
  * reference; its thesis names spatial decomposition as the way to run it in
  * parallel).  Each slab is a context holding every particle's arrays (the
