@@ -530,7 +530,7 @@ __global__ void k_reorder_fill(CellLists L, int ncell, const int* __restrict__ c
   int k = cell_start[c];
   const int end = cell_start[c + 1];
   for (int q = L.head[c]; q != -1; q = L.next[q]) {
-    if (k >= end || q < 0 || q >= n) {
+    if (k >= end || k >= n || q < 0 || q >= n) {
       atomicExch(err, 1);
       return;
     }
