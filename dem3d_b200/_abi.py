@@ -146,6 +146,7 @@ SIGNATURES = {
                                _DP, _DP]),
     "initialize_cell_distribution": (C.c_int, [_P]),
     "get_grid": (C.c_int, [_P, _I32P]),
+    "get_cell_count": (C.c_int, [_P, _I32P]),
     "get_cells": (C.c_int, [_P, _I32P, _I32P, _I32P]),
     "set_cells": (C.c_int, [_P, _I32P, _I32P]),
     "compute_accelerations": (C.c_int, [_P, C.c_int32, C.c_double, C.c_int32]),

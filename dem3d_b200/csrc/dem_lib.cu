@@ -2749,6 +2749,12 @@ int dem_get_grid(dem_ctx* c, int32_t* nxyz) {
   return DEM_OK;
 }
 
+int dem_get_cell_count(dem_ctx* c, int32_t* ncell) {
+  if (!c || !ncell) return DEM_ERR_INVALID;
+  *ncell = c->ncell_total;
+  return DEM_OK;
+}
+
 int dem_get_cells(dem_ctx* c, int32_t* cell_index, int32_t* traversal, int32_t* cell_start) {
   if (!c) return DEM_ERR_INVALID;
   RESTORE_ORDER;

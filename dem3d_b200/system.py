@@ -215,10 +215,11 @@ class DEMSystem:
         return tuple(int(x) for x in g)
 
     def get_cells(self):
-        nx, ny, nz = self.grid()
+        nc = C.c_int32()
+        self._call("get_cell_count", C.byref(nc))  # every system's cells
         ci = np.empty(self.n, np.int32)
         tr = np.empty(self.n, np.int32)
-        cs = np.empty(nx * ny * nz + 1, np.int32)
+        cs = np.empty(nc.value + 1, np.int32)
         self._call("get_cells", _iptr(ci), _iptr(tr), _iptr(cs))
         return ci, tr, cs
 

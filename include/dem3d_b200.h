@@ -260,9 +260,11 @@ int dem_get_contacts(dem_ctx* ctx, int64_t cap, int32_t* imin, int32_t* imax,
 int dem_initialize_cell_distribution(dem_ctx* ctx);
 /* Cell grid: Nx,Ny,Nz (InitCellStructure3D src/MCells.f90:155-227). */
 int dem_get_grid(dem_ctx* ctx, int32_t* nxyz);
+/* Cells of the context: Nx*Ny*Nz, summed over the systems of an ensemble. */
+int dem_get_cell_count(dem_ctx* ctx, int32_t* ncell);
 /* CellIndex(1:n) (0-based cells) and the particles of every cell in list
  * order (the traversal order of ComputeAccelerations): traversal[n],
- * cell_start[ncell+1]. */
+ * cell_start[ncell+1], ncell from dem_get_cell_count. */
 int dem_get_cells(dem_ctx* ctx, int32_t* cell_index, int32_t* traversal,
                   int32_t* cell_start);
 /* ReadCellDistribution (src/MForces.f90:121-131, ReadCellStructure

@@ -1684,6 +1684,11 @@ int orc_get_grid(orc_ctx* c, int32_t* nxyz) {
   return DEM_OK;
 }
 
+int orc_get_cell_count(orc_ctx* c, int32_t* ncell) {
+  *ncell = c->Nt;
+  return DEM_OK;
+}
+
 int orc_get_cells(orc_ctx* c, int32_t* cell_index, int32_t* traversal, int32_t* cell_start) {
   if (cell_index) memcpy(cell_index, c->cell_index, sizeof(int32_t) * (size_t)c->n);
   int32_t k = 0;
