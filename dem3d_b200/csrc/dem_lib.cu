@@ -1686,6 +1686,10 @@ int launch_chunk(dem_ctx* c, int phase) {
 // Slabs of a spatial decomposition (dem_slab_*): column tables and layers.
 
 void slab_col(SlabCols& C, const void* base, int elem, int rows, long long stride) {
+  if (C.n >= SLAB_MAXC) {
+    C.overflow = 1;
+    return;
+  }
   const int k = C.n++;
   C.src[k] = (const char*)base;
   C.dst[k] = (char*)base;
@@ -1808,6 +1812,7 @@ int slab_max_over(dem_ctx* c, int count, const int* v, int* out) {
 // the header and records of a packed exchange
 int slab_write(dem_ctx* c, int what, const SlabCols& C, int count, const std::vector<int>& extra,
                void* buf, int64_t cap, int64_t* bytes) {
+  if (C.overflow) return fail(c, DEM_ERR_STATE, "slab: too many particle arrays");
   const int64_t head = SLAB_HEAD + 4 * (int64_t)extra.size();
   const int64_t body = (head + 15) / 16 * 16;
   const int64_t total = body + (int64_t)count * C.rec;
@@ -1850,8 +1855,8 @@ int slab_read_head(dem_ctx* c, const void* buf, int64_t bytes, int what, std::ve
 
 // Permute every particle array: place s takes the particle stored at pi[s]
 // (pi a device array of n places); the stored particle numbers (cell
-// lists, slots, arrival lists, history partners) are renamed, and the next
-// pass rebuilds every candidate row.
+// lists, slots, arrival lists, history partners, candidate rows) are
+// renamed.
 int permute_particles(dem_ctx* c, const int* pi) {
   const int n = c->n;
   if (n == 0) return DEM_OK;
@@ -1867,8 +1872,12 @@ int permute_particles(dem_ctx* c, const int* pi) {
   col(c->L.mnext, 4);
   col(c->rows.meta, 4);
   col(c->rows.rank, 4);
+  // the candidate rows move with their particles and are renamed below:
+  // the same partners in the same order, so no row is rebuilt
+  slab_col(C, c->rows.cand, 4, c->rows.kc, (long long)n * 4);
   col(c->in_cnt, 4);
   col(c->matched, 4);
+  if (C.overflow) return fail(c, DEM_ERR_STATE, "reorder: too many particle arrays");
   size_t most = 0;
   for (int k = 0; k < C.n; k++) most = std::max(most, (size_t)C.elem[k] * C.rows[k] * (size_t)n);
   char* tmp = nullptr;
@@ -1896,8 +1905,7 @@ int permute_particles(dem_ctx* c, const int* pi) {
   remap(c->L.arr_head, nc);
   remap(c->L.slot, nc * SLOT_CAP);
   for (int b = 0; b < 2; b++) remap(c->H[b].key, (long long)c->H[b].cap * c->H[b].n);
-  const int one = 1;
-  CK(cudaMemcpyAsync(&c->cnt->force_full, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  remap(c->rows.cand, (long long)c->rows.kc * n);
   CK(cudaStreamSynchronize(c->stream));
   cudaFree(tmp);
   cudaFree(inv);

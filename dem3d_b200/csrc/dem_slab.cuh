@@ -32,8 +32,9 @@ constexpr int SLAB_HEAD = 16;  // bytes of the buffer header
 constexpr int SLAB_ID = 16;    // bytes of a record's particle field
 
 struct SlabCols {
-  int n;    // columns
-  int rec;  // bytes per record (SLAB_ID + the columns)
+  int n;         // columns
+  int rec;       // bytes per record (SLAB_ID + the columns)
+  int overflow;  // more than SLAB_MAXC columns were asked for
   const char* src[SLAB_MAXC];
   char* dst[SLAB_MAXC];
   long long stride[SLAB_MAXC];
