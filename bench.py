@@ -585,6 +585,8 @@ def run_ours(args):
         s.initialize_cell_distribution()
         if args.reorder_every > 0:
             s.set_reorder(args.reorder_every)
+        if args.no_early_launch:
+            s.set_early_launch(False)
         res[prec] = measure(s, w, args, world, local, torch, dist)
         systems[prec] = s
     s = systems[headline]
@@ -743,7 +745,8 @@ def run_ours(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if headline == "fp64" else "f32+f64", "data": "synthetic",
             "config": dict(config_block(args.workload, w, world, headline),
-                           storage_reorder_every=args.reorder_every),
+                           storage_reorder_every=args.reorder_every,
+                           early_launch=not args.no_early_launch),
             "gpu_launches": int(launches),
             "launches_per_step": launches / res[headline]["steps"],
             "precisions": {p: {"value": r["value"], "ms_per_step": r["ms"] / r["steps"],
@@ -821,6 +824,8 @@ def run_ensemble(args):
     s = DEMSystem.ensemble(e.params, e.counts)
     s.set_state(e.pos, e.vel, e.omega, radius=e.radius)
     s.initialize_cell_distribution()
+    if args.no_early_launch:
+        s.set_early_launch(False)
     skip = args.skip_steps if args.skip_steps >= 0 else spec.get("skip", 0)
     if skip > 0:
         # the beds start to form: untimed steps before the warm-up
@@ -1010,6 +1015,8 @@ def main():
                     help="steps between the samples of --obs-window")
     ap.add_argument("--no-autotune", action="store_true",
                     help="skip the autotuner's trials (default settings)")
+    ap.add_argument("--no-early-launch", action="store_true",
+                    help="launch the pass kernels in plain stream order (dem_set_early_launch 0)")
     ap.add_argument("--reorder-every", type=int, default=0,
                     help="keep the particle storage in cell order, permuting it every N steps "
                          "of the run (0: never)")

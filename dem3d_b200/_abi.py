@@ -192,6 +192,8 @@ GPU_ONLY = {
     "autotune": (C.c_int, [_P, C.c_int32, C.c_int32, _I32P, _DP]),
     "set_launch_shape": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     "get_launch_shape": (C.c_int, [_P, _I32P, _I32P, _I32P, _I32P]),
+    "set_early_launch": (C.c_int, [_P, C.c_int32]),
+    "get_early_launch": (C.c_int, [_P, _I32P]),
     "set_persistent_barrier": (C.c_int, [_P, C.c_double, C.c_int32]),
     "get_persistent_blocks": (C.c_int, [_P, _I32P]),
     "set_reorder": (C.c_int, [_P, C.c_int32]),

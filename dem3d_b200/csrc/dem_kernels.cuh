@@ -601,6 +601,7 @@ __global__ void k_cell_slots(CellLists L, int c_begin, int ncells, int n) {
 
 __global__ void k_relink(const DevParams* __restrict__ PT, const int* __restrict__ cellsys,
                          CellLists L, int par, int n, int update, int stop_tag, Counters* cnt) {
+  pass_kernel_entry();
   relink_body(PT, cellsys, L, par, n, update, stop_tag, cnt, blockIdx.x * blockDim.x + threadIdx.x,
               gridDim.x * blockDim.x);
 }
@@ -633,6 +634,7 @@ __global__ void k_relink(const DevParams* __restrict__ PT, const int* __restrict
 // kernel fits in 72 registers)
 template <bool PP, int BS, bool STRIDE>
 __global__ void __launch_bounds__(BS, 7 * 128 / BS) k_test(TestArgs A) {
+  pass_kernel_entry();
   if (!STRIDE) {
     test_body<PP>(A, blockIdx.x);
     return;
@@ -754,6 +756,7 @@ __device__ __forceinline__ void pair_fp64_body(const PassArgs<double4, double2>&
 
 template <bool PP, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_pair_fp64(PassArgs<double4, double2> A) {
+  pass_kernel_entry();
   pair_fp64_body<PP>(A, blockIdx.x, gridDim.x);
 }
 
@@ -951,9 +954,13 @@ __device__ __forceinline__ void fold_fp64_body(const PassArgs<double4, double2>&
   if (EPI != EPI_STORE) publish_disp_block(A.cnt, d2);
 }
 
-// (STRIDE: grid-stride over blocks of 128 particles, like k_test)
+// (STRIDE: grid-stride over blocks of 128 particles, like k_test.  Register
+// budget without walls: 6 blocks of 128 per SM, 80 registers; the predictor
+// spills a little there and still runs faster than at 5 blocks, 135 against
+// 146 us per launch at 1M spheres.)
 template <bool PP, int EPI, bool WALLS, bool STRIDE>
-__global__ void __launch_bounds__(128, WALLS ? 4 : 5) k_fold_fp64(PassArgs<double4, double2> A) {
+__global__ void __launch_bounds__(128, WALLS ? 4 : 6) k_fold_fp64(PassArgs<double4, double2> A) {
+  pass_kernel_entry();
   if (!STRIDE) {
     fold_fp64_body<PP, EPI, WALLS>(A, blockIdx.x);
     return;

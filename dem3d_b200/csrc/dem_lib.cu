@@ -139,6 +139,10 @@ struct dem_ctx {
   int ppt = 1;
   int pair_waves = 2;
   int launch_mode = 0;
+  // the test, pair and fold kernels of a pass launched with programmatic
+  // stream serialization (dem_set_early_launch), so that each is scheduled
+  // while the kernel ahead of it finishes
+  int early_launch = 1;
   // persistent chunks: while `recording`, the pass launchers append the
   // passes of a chunk to rec (relink arguments wait in rec_rl for their
   // pass) instead of launching; each rotation phase keeps its chunk's
@@ -277,6 +281,21 @@ void launch(dem_ctx* c, const char* name, void (*kernel)(KArgs...), unsigned gri
   } else {
     kernel<<<grid, block, 0, c->stream>>>(args...);
   }
+  c->launches++;
+}
+
+// launch of a test, pair or fold kernel: early (programmatic stream
+// serialization) when the context allows it and no kernel is being timed
+// on its own
+template <typename... KArgs, typename... Args>
+void launch_early(dem_ctx* c, bool early, const char* name, void (*kernel)(KArgs...),
+                  unsigned grid, unsigned block, Args... args) {
+  if (grid == 0) return;
+  if (c->prof || !early) {
+    launch(c, name, kernel, grid, block, args...);
+    return;
+  }
+  launch_pass(true, kernel, grid, block, c->stream, args...);
   c->launches++;
 }
 
@@ -829,9 +848,14 @@ void fluid_prepare(dem_ctx* c, int side) {
 
 // part: 0 = the whole pass, 1 = the test and pair kernels, 2 = the fold
 // kernel (a slab of a decomposition exchanges data in between)
+// early_ok: the operation ahead of this pass's test kernel in the stream is
+// the pass's relink (or a fluid kernel after it), so the test, pair and fold
+// kernels may be launched early; not after the status resets of a repeated
+// pass, nor between the exchanges of a slab
 void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, const RingMap& rm,
-                        int tag, int part = 0) {
+                        int tag, int part = 0, bool early_ok = true) {
   if (c->n == 0) return;
+  const bool early = early_ok && c->early_launch && !c->slab && part == 0;
   const StateArrays& tgt = side ? c->Pr : c->P;
   // the test kernel: the contact list of the pass
   TestArgs T;
@@ -887,7 +911,7 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
     const unsigned nvb = blocks_for(c->n, bs);
     const bool stride = c->ppt > 1;
     const unsigned g = stride ? (nvb + c->ppt - 1) / c->ppt : nvb;
-#define TK(PPV, BS, S) launch(c, "test", k_test<PPV, BS, S>, g, BS, T)
+#define TK(PPV, BS, S) launch_early(c, early, "test", k_test<PPV, BS, S>, g, BS, T)
 #define TCASE(PPV)                    \
   do {                                \
     if (bs == 64) {                   \
@@ -917,7 +941,7 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
       if ((k == 0 && part == 2) || (k == 1 && part == 1)) continue;
       timed(c, k ? "fold_mixed" : "pair_mixed", [&]() {
         mixed_pass(c->M, c->pp, epi, c->pass_variant, walls, c->has_cone, A, c->hcur, c->stream,
-                   k, pair_blocks, c->ppt);
+                   k, pair_blocks, c->ppt, early && !c->prof);
       });  // (timed counts the launch)
     }
     return;
@@ -925,7 +949,7 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
   auto A = pass_args<double4, double2>(c, side, update, dt, rm, tag, tgt);
   if (epi == EPI_STORE) A.amsum = c->force_out;
 #define PAIR_CASE(PPV, MB) \
-  launch(c, "pair_fp64", k_pair_fp64<PPV, MB>, pair_blocks, 128, A)
+  launch_early(c, early, "pair_fp64", k_pair_fp64<PPV, MB>, pair_blocks, 128, A)
   if (part == 2) {
   } else if (mb == 3) {
     if (c->pp) PAIR_CASE(true, 3);
@@ -944,7 +968,8 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
   const unsigned nvb = blocks_for(c->n, 128);
   const bool stride = c->ppt > 1 && epi != EPI_STORE;
   const unsigned g = stride ? (nvb + c->ppt - 1) / c->ppt : nvb;
-#define FK(PPV, E, W, S) launch(c, "fold_fp64", k_fold_fp64<PPV, E, W, S>, g, 128, A)
+#define FK(PPV, E, W, S) \
+  launch_early(c, early, "fold_fp64", k_fold_fp64<PPV, E, W, S>, g, 128, A)
 #define FOLD_CASE(PPV, W)                     \
   do {                                        \
     if (epi == EPI_PREDICT) {                 \
@@ -1100,7 +1125,7 @@ int finish_pass(dem_ctx* c, int side, bool update, double dt, int epi, const Rin
                          c->stream));
       CK(cudaMemsetAsync(&c->cnt->disp_acc, 0, sizeof(double), c->stream));
     }
-    launch_pass_kernel(c, side, update, dt, epi, rm, tag);
+    launch_pass_kernel(c, side, update, dt, epi, rm, tag, 0, false);
   }
 }
 
@@ -3530,6 +3555,20 @@ int dem_set_launch_shape(dem_ctx* c, int32_t launch_mode, int32_t test_block,
   c->test_block = test_block;
   c->ppt = particles_per_thread;
   c->pair_waves = pair_waves;
+  return DEM_OK;
+}
+
+int dem_set_early_launch(dem_ctx* c, int32_t on) {
+  if (!c) return DEM_ERR_INVALID;
+  if (c->stream) CK(cudaStreamSynchronize(c->stream));
+  if ((on != 0) != (c->early_launch != 0)) drop_graphs(c);
+  c->early_launch = on != 0;
+  return DEM_OK;
+}
+
+int dem_get_early_launch(dem_ctx* c, int32_t* on) {
+  if (!c) return DEM_ERR_INVALID;
+  if (on) *on = c->early_launch;
   return DEM_OK;
 }
 

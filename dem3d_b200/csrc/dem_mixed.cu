@@ -374,6 +374,7 @@ __device__ __forceinline__ void pair_mixed_body(const PassArgs<float4, float2>& 
 template <bool PP, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_pair_mixed(PassArgs<float4, float2> A,
                                                           MixedView V) {
+  pass_kernel_entry();
   pair_mixed_body<PP>(A, V, blockIdx.x, gridDim.x);
 }
 
@@ -552,12 +553,14 @@ __device__ __forceinline__ void fold_mixed_body(const PassArgs<float4, float2>& 
   if (EPI != EPI_STORE) publish_disp_block(A.cnt, d2);
 }
 
-// (STRIDE: grid-stride over blocks of 128 particles.  Register budget: 5
-// blocks of 128 per SM; the corrector without walls fits in 80 registers,
-// 6 blocks.)
+// (STRIDE: grid-stride over blocks of 128 particles.  Register budget: 6
+// blocks of 128 per SM, 80 registers.  The predictor spills a few registers
+// at that budget and still runs faster than at 5 blocks: 127.6 against
+// 137.9 us per launch at 1M spheres, 611 against 695 us with walls at 4M.)
 template <bool PP, int EPI, bool WALLS, bool CONE, bool STRIDE>
-__global__ void __launch_bounds__(128, (!WALLS && EPI == EPI_CORRECT) ? 6 : 5)
+__global__ void __launch_bounds__(128, 6)
     k_fold_mixed(PassArgs<float4, float2> A, MixedView V) {
+  pass_kernel_entry();
   if (!STRIDE) {
     fold_mixed_body<PP, EPI, WALLS, CONE>(A, V, blockIdx.x);
     return;
@@ -795,11 +798,11 @@ MixedView mixed_view(const MixedBuffers& M, int cur) {
 
 void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant, bool walls, bool cone,
                 const PassArgs<float4, float2>& A, int cur, cudaStream_t st, int part,
-                unsigned pair_blocks, int ppt) {
+                unsigned pair_blocks, int ppt, bool early) {
   if (A.n == 0) return;
   const MixedView V = mixed_view(M, cur);
   if (part == 0) {
-#define PCASE(PPV, MB) k_pair_mixed<PPV, MB><<<pair_blocks, 128, 0, st>>>(A, V)
+#define PCASE(PPV, MB) launch_pass(early, k_pair_mixed<PPV, MB>, pair_blocks, 128, st, A, V)
     if (variant == 1) {
       if (pp) PCASE(true, 3);
       else PCASE(false, 3);
@@ -816,7 +819,7 @@ void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant, bool walls, bool
   const unsigned nvb = blocks(A.n, 128);
   const bool stride = ppt > 1 && epi != EPI_STORE;
   const unsigned g = stride ? (nvb + ppt - 1) / ppt : nvb;
-#define FK(PPV, E, W, CN, S) k_fold_mixed<PPV, E, W, CN, S><<<g, 128, 0, st>>>(A, V)
+#define FK(PPV, E, W, CN, S) launch_pass(early, k_fold_mixed<PPV, E, W, CN, S>, g, 128, st, A, V)
 #define FCASE(PPV, W, CN)                          \
   do {                                             \
     if (epi == EPI_PREDICT) {                      \

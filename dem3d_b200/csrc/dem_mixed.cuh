@@ -54,11 +54,12 @@ bool mixed_grow_walls(MixedBuffers& M, int n, int stride, int cur, cudaStream_t 
 // the contact list; variant: compiled for 4 (0), 3 (1) or 5 (2) resident
 // blocks per SM), 1 = the fold kernel with epilogue `epi` (walls: some
 // system has walls; cone: some wall is a cone; ppt > 1: the fold grid holds
-// 1/ppt of the blocks of 128 particles and strides over them).  The test
-// kernel that builds the contact list is shared with the FP64 path.
+// 1/ppt of the blocks of 128 particles and strides over them; early: launched
+// with programmatic stream serialization).  The test kernel that builds the
+// contact list is shared with the FP64 path.
 void mixed_pass(MixedBuffers& M, bool pp, int epi, int variant, bool walls, bool cone,
                 const PassArgs<float4, float2>& A, int cur, cudaStream_t st, int part,
-                unsigned pair_blocks, int ppt);
+                unsigned pair_blocks, int ppt, bool early);
 // One persistent chunk (npass passes of prog, a device array) as a
 // cooperative launch of at most want_blocks blocks of 128 threads (fewer if
 // fewer fit on the device at once; the count in *blocks_out).  g.expected

@@ -384,6 +384,37 @@ __device__ __forceinline__ void epilogue(const PassArgs<V4, W2>& A, const DevPar
   }
 }
 
+// First statement of every kernel of a force pass (relink, test, pair,
+// fold).  A kernel launched with programmatic stream serialization may be
+// scheduled while the kernel before it in the stream is still running; it
+// waits here until that kernel has completed and its writes are visible, and
+// then allows the next kernel of the pass to be scheduled (whose blocks take
+// the SM slots this kernel's last blocks free, and wait in turn).  Without
+// that launch attribute both instructions return at once.  Nothing a pass
+// kernel reads or writes is touched before the wait.
+__device__ __forceinline__ void pass_kernel_entry() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Host side: launch a pass kernel on `st`, with programmatic stream
+// serialization when `early` (the kernel must begin with pass_kernel_entry).
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pass(bool early, void (*kernel)(KArgs...), unsigned grid, unsigned block,
+                               cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = early ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 __device__ __forceinline__ void set_abort(Counters* cnt, int tag) {
   atomicCAS(&cnt->abort_tag, 0, tag + 1);
   atomicExch(&cnt->abort, 1);

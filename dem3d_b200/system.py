@@ -435,6 +435,17 @@ class DEMSystem:
         return dict(zip(("launch_mode", "test_block", "particles_per_thread", "pair_waves"),
                         (x.value for x in v)))
 
+    def set_early_launch(self, on: bool = True) -> None:
+        """dem_set_early_launch: the test, pair and fold kernels of a pass
+        launched with programmatic stream serialization (default on).  No
+        result depends on it."""
+        self._call("set_early_launch", C.c_int32(1 if on else 0))
+
+    def early_launch(self) -> bool:
+        v = C.c_int32()
+        self._call("get_early_launch", C.byref(v))
+        return bool(v.value)
+
     def set_persistent_barrier(self, timeout_ms: float = 2000.0, extra_blocks: int = 0) -> None:
         self._call("set_persistent_barrier", C.c_double(timeout_ms), C.c_int32(extra_blocks))
 

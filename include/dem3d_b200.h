@@ -397,6 +397,13 @@ int dem_set_launch_shape(dem_ctx* ctx, int32_t launch_mode, int32_t test_block,
                          int32_t particles_per_thread, int32_t pair_waves);
 int dem_get_launch_shape(dem_ctx* ctx, int32_t* launch_mode, int32_t* test_block,
                          int32_t* particles_per_thread, int32_t* pair_waves);
+/* Early launch (no counterpart in the reference; changes no result): with
+ * on != 0 (the default) the test, pair and fold kernels of a force pass are
+ * launched with programmatic stream serialization, so that each is
+ * scheduled while the kernel ahead of it finishes and starts its work the
+ * moment that kernel's writes are visible.  *on (get) may be NULL. */
+int dem_set_early_launch(dem_ctx* ctx, int32_t on);
+int dem_get_early_launch(dem_ctx* ctx, int32_t* on);
 /* Grid-wide barriers of persistent chunks: every wait gives up after
  * timeout_ms (default 2000), after which the chunk ends early, dem_run
  * returns DEM_ERR_STATE and the state must be set again.  extra_blocks > 0

@@ -55,3 +55,25 @@ def test_tuning_settings_keep_the_trajectory():
         got = s.get_state()
         for k in want:
             np.testing.assert_array_equal(got[k], want[k], err_msg=f"{skin} {variant} {k}")
+
+
+@pytest.mark.parametrize("precision", [P.PREC_FP64, P.PREC_MIXED])
+def test_early_launch_keeps_the_trajectory(precision):
+    """Test, pair and fold kernels launched with programmatic stream
+    serialization (the default) against plain stream order: the same bits,
+    in graph-replayed chunks and in passes launched one by one."""
+    a, b = _system(precision), _system(precision)
+    assert a.early_launch()
+    b.set_early_launch(False)
+    assert not b.early_launch()
+    for s in (a, b):
+        s.run(1, 60)
+        for k in range(61, 66):
+            s.move_particles(k)
+    sa, sb = a.get_state(), b.get_state()
+    for k in sa:
+        np.testing.assert_array_equal(sa[k], sb[k], err_msg=k)
+    ca, cb = a.get_contacts(), b.get_contacts()
+    for k in ca:
+        np.testing.assert_array_equal(ca[k], cb[k], err_msg=k)
+    assert a.ncol() == b.ncol()
