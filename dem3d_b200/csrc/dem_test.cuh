@@ -69,12 +69,18 @@ __device__ __forceinline__ void relink_body(const DevParams* __restrict__ PT,
                                             const int* __restrict__ cellsys, const CellLists& L,
                                             int par, int n, int update, int stop_tag,
                                             Counters* cnt, int tid, int nthreads) {
-  if (cnt->abort) return;
+  // (the status words, the dirty-cell count and the pass number requested
+  // together)
+  const int abort0 = cnt->abort;
+  const unsigned long long escaped = cnt->escaped;
+  const int m = cnt->n_dirty[par];
+  const int stamp = cnt->pass_id + 1;  // fold kernels advance pass_id, not this one
+  if (abort0) return;
   // inside a captured chunk, particles that left the box in the last step
   // stop the chunk before this step (the host runs UpdateParticleList); the
   // count is final here (written by the previous kernel), so every block
   // takes the same branch
-  if (stop_tag >= 0 && cnt->escaped != 0ull) {
+  if (stop_tag >= 0 && escaped != 0ull) {
     if (tid == 0) {
       cnt->escape_stop = 1;
       set_abort(cnt, stop_tag);
@@ -109,8 +115,6 @@ __device__ __forceinline__ void relink_body(const DevParams* __restrict__ PT,
     cnt->disp_acc = full ? 0.0 : acc;
     if (full) cnt->force_full = 0;
   }
-  const int m = cnt->n_dirty[par];
-  const int stamp = cnt->pass_id + 1;  // fold kernels advance pass_id, not this one
   const int* __restrict__ cell_new = L.cell[par];
   for (int i = tid; i < m; i += nthreads) {
     const int c = L.dlist[par][i];
@@ -124,23 +128,46 @@ __device__ __forceinline__ void relink_body(const DevParams* __restrict__ PT,
       L.dflag[c] = 0;
       continue;
     }
-    // 1. unlink the leavers
-    int prev = -1, first = -1, q = L.head[c];
+    // 1. unlink the leavers.  The old list is in the cell's slots when it
+    // fits there (independent loads); else it is walked link by link (a
+    // leaver's successor saved when it moved: its own link may be rewritten
+    // by the thread of the cell it entered)
+    int prev = -1, first = -1;
     int guard = 0;
-    while (q != -1) {
-      if (++guard > n) {
-        atomicExch(&cnt->list_error, 1);
-        atomicExch(&cnt->abort, 1);
-        return;
+    const int len = L.slot_n[c];
+    const bool from_slots = len >= 0 && len <= SLOT_CAP;
+    int old[SLOT_CAP];
+    unsigned stay = 0u;  // bit k: old element k stays
+    if (from_slots) {
+      const int* sl = L.slot + (size_t)c * SLOT_CAP;
+#pragma unroll 4
+      for (int k = 0; k < len; k++) old[k] = sl[k];
+#pragma unroll 4
+      for (int k = 0; k < len; k++)
+        if (cell_new[old[k]] == c) stay |= 1u << k;
+      for (int k = 0; k < len; k++) {
+        if (!((stay >> k) & 1u)) continue;
+        if (prev == -1) first = old[k];
+        else L.next[prev] = old[k];
+        prev = old[k];
       }
-      const bool stays = cell_new[q] == c;
-      const int nq = stays ? L.next[q] : L.mnext[q];
-      if (stays) {
-        if (prev == -1) first = q;
-        else L.next[prev] = q;
-        prev = q;
+    } else {
+      int q = L.head[c];
+      while (q != -1) {
+        if (++guard > n) {
+          atomicExch(&cnt->list_error, 1);
+          atomicExch(&cnt->abort, 1);
+          return;
+        }
+        const bool stays = cell_new[q] == c;
+        const int nq = stays ? L.next[q] : L.mnext[q];
+        if (stays) {
+          if (prev == -1) first = q;
+          else L.next[prev] = q;
+          prev = q;
+        }
+        q = nq;
       }
-      q = nq;
     }
     if (prev != -1) L.next[prev] = -1;
     // 2. prepend the arrivals, highest index first (the reference's index:
@@ -154,7 +181,7 @@ __device__ __forceinline__ void relink_body(const DevParams* __restrict__ PT,
         atomicExch(&cnt->abort, 1);
         return;
       }
-      const int an = L.arr_next[a];
+      const int an = L.arr_next[a];  // (guard: arrivals so far)
       L.mflag[a] = 0;
       if (sh == -1) {
         sh = tail = a;
@@ -179,7 +206,25 @@ __device__ __forceinline__ void relink_body(const DevParams* __restrict__ PT,
     }
     L.head[c] = first;
     L.dflag[c] = 0;
-    copy_slots(L, c, first, n);
+    if (from_slots) {
+      // the new list's slots: the arrivals (this thread linked them), then
+      // the stayers in their old order
+      int k = 0;
+      int x = sh;
+      for (int t = 0; t < guard; t++) {
+        if (k < SLOT_CAP) L.slot[(size_t)c * SLOT_CAP + k] = x;
+        k++;
+        x = L.next[x];
+      }
+      for (int j = 0; j < len; j++)
+        if ((stay >> j) & 1u) {
+          if (k < SLOT_CAP) L.slot[(size_t)c * SLOT_CAP + k] = old[j];
+          k++;
+        }
+      L.slot_n[c] = k;
+    } else {
+      copy_slots(L, c, first, n);
+    }
     // 3. the rows that read c are rebuilt in this pass (by the test
     // kernel): a row of a particle in cell b holds the rest of b's list and
     // the half-shell cells b + o, kx + Nx*(ky + Ny*kz) > 0, so c is read by
