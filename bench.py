@@ -730,7 +730,7 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         lib_path, flags = _oracle_variant()
-        v, k, dt = cpu_time_steps(base, max_steps=3, budget_s=25.0, lib_path=lib_path, core=0)
+        v, k, dt = cpu_time_steps(base, max_steps=30, budget_s=10.0, lib_path=lib_path, core=0)
         cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
                "sample": f"{k} MoveParticles steps (after 1 untimed; the GPU arm times "
                          f"{res[headline]['steps']}) of the same {n:,}-sphere "
