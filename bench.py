@@ -154,9 +154,11 @@ def fold_bytes_per_particle(mixed, epi, z_pp, z_pw=0.0, nw=0, nprev=3):
         records;
       epi "predict" (pass 1, src/MDEM.f90:296-331, history-updating): the
         record count 4 read and written, new wall records; ring nprev*72
-        read, Particle v,w 48 read (mixed), a,alpha 48 + Predicted x,v,w 72 +
-        ring slot 72 + the corrector's ring sums 72 + next-pass copies (32 +
-        velocities) + cell 4 written;
+        read, Particle v,w 48 read (mixed), ring slot 72 + the corrector's
+        ring sums 72 + next-pass copies (32 + velocities) + cell 4 written,
+        and of Particle a,alpha and Predicted x,v,w only what no other array
+        holds: a,alpha 48 only without a ring (nprev = 0), Predicted v,w 48
+        only in mixed mode (its velocity copies are FP32);
       epi "correct" (pass 2, :340-367): the ring sums 72, Predicted v 24
         (mixed) read, Particle x,v,w 72 read and written, Predicted a,alpha
         48 + next-pass copies + cell 4 written."""
@@ -168,8 +170,8 @@ def fold_bytes_per_particle(mixed, epi, z_pp, z_pw=0.0, nw=0, nprev=3):
     sums = 72 if nprev else 0
     if epi == "predict":
         base += 8 + nw * 4 + z_pw * (wrec - 4)
-        epil = (nprev * 72 + (48 if mixed else 0) + 48 + 72 + (72 if nprev else 0) + sums + 32
-                + vel + 4)
+        epil = (nprev * 72 + (48 if mixed else 0) + (0 if nprev else 48) + (48 if mixed else 0)
+                + (72 if nprev else 0) + sums + 32 + vel + 4)
     else:
         epil = sums + (24 if mixed else 0) + 72 + 72 + 48 + 32 + vel + 4
     return base + epil

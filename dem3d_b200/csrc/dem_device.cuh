@@ -247,6 +247,12 @@ struct PassArgs {
   Counters* cnt;
   int tag;  // 2*(step within a captured chunk) + pass
   const double* drag;  // [3n] fluid drag of every sphere (NULL: no fluid)
+  // 1: the AB predictor leaves out the values that only export calls read
+  // and that other arrays of the step already hold: Particle a, alpha (the
+  // ring slot it writes holds them), Predicted x (the next pass's position
+  // copy) and, with FP64 velocity copies, Predicted v, w.  The host writes
+  // them back (k_settle_state) before a call reads or changes particle data.
+  int lazy;
   // EPI_PREDICT/EPI_CORRECT: the corrector's ring sums sum_k AM(k)*
   // Previous(ipc(k)) (v, a, alpha: [9][n]), formed by the predictor pass,
   // which holds every term of them.  EPI_STORE: ComputeAccelerations'

@@ -310,6 +310,32 @@ __global__ void k_ring_store(int n, StateArrays Q, double* __restrict__ ring, in
   rg[6 * (size_t)n] = Q.lx[i]; rg[7 * (size_t)n] = Q.ly[i]; rg[8 * (size_t)n] = Q.lz[i];
 }
 
+// The values the predictor passes leave out (PassArgs::lazy) written back:
+// Particle a, alpha from the ring slot ipc(1) (nprev > 0), Predicted x from
+// the Predicted side's position copy and, with FP64 copies (EXACT),
+// Predicted v, w from its velocity copies.  Plain copies: the bits are the
+// ones the predictor computed.
+template <bool EXACT, class V4, class W2>
+__global__ void k_settle_state(int n, StateArrays Q, StateArrays R, const double* __restrict__ ring,
+                               int slot0, int nprev, const double4* __restrict__ X1,
+                               const V4* __restrict__ v41, const W2* __restrict__ w21) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (nprev > 0) {
+    const double* rg = ring + (size_t)slot0 * 9 * n + i;
+    Q.ax[i] = rg[3 * (size_t)n]; Q.ay[i] = rg[4 * (size_t)n]; Q.az[i] = rg[5 * (size_t)n];
+    Q.lx[i] = rg[6 * (size_t)n]; Q.ly[i] = rg[7 * (size_t)n]; Q.lz[i] = rg[8 * (size_t)n];
+  }
+  const double4 x = X1[i];
+  R.px[i] = x.x; R.py[i] = x.y; R.pz[i] = x.z;
+  if (EXACT) {
+    const V4 v = v41[i];
+    const W2 w = w21[i];
+    R.vx[i] = (double)v.x; R.vy[i] = (double)v.y; R.vz[i] = (double)v.z;
+    R.wx[i] = (double)v.w; R.wy[i] = (double)w.x; R.wz[i] = (double)w.y;
+  }
+}
+
 // explicit Euler update (src/MDEM.f90:240-252)
 __global__ void k_euler_update(int n, StateArrays Q, double dt, const Counters* __restrict__ cnt) {
   if (cnt->abort) return;

@@ -178,6 +178,10 @@ struct dem_ctx {
   long long since_reorder = 0;
   long long reorders = 0;
   bool permuted = false;
+  // the passes' predictors left Particle a, alpha in the ring slot ipc(1)
+  // and Predicted x (v, w: FP64) in the Predicted side's pass copies
+  // (PassArgs::lazy); settle_state writes them back
+  bool lazy_state = false;
   int* gid = nullptr;
   int gid_cap = 0;
   bool has_cone = false; // some wall of some system is a cone
@@ -237,7 +241,9 @@ int cuda_fail(dem_ctx* c, cudaError_t e, const char* where) {
     if (e_ != cudaSuccess) return cuda_fail(c, e_, #call);    \
   } while (0)
 
-int restore_order(dem_ctx* c);
+// settle: write back what the predictors left out (settle_state) first
+int restore_order(dem_ctx* c, bool settle = true);
+int settle_state(dem_ctx* c);
 
 // calls that read or write particle data see the reference's order
 #define RESTORE_ORDER                \
@@ -407,6 +413,7 @@ void free_state(dem_ctx* c) {
   c->gid_cap = 0;
   c->L.gid = nullptr;
   c->permuted = false;
+  c->lazy_state = false;
   cudaFree(c->staging);
   c->staging = nullptr;
   cudaFree(c->state_block);
@@ -515,6 +522,10 @@ int ensure_drag(dem_ctx* c);
 // the prepared cell transition are rebuilt by the next pass).
 int grow_capacity(dem_ctx* c, int newcap) {
   if (newcap <= c->ncap) return DEM_OK;
+  {
+    int st = settle_state(c);  // (the ring and the copies are not kept)
+    if (st) return st;
+  }
   CK(cudaStreamSynchronize(c->stream));
   drop_graphs(c);
   // (called in the reference's order: gid is the identity and is made again
@@ -677,6 +688,12 @@ int init_cells(dem_ctx* c) {
 // one pass: copies of the side (if not prepared), relink, candidate rows,
 // pass kernel
 
+// The predictors leave out Particle a, alpha and Predicted x (v, w with FP64
+// copies) where other arrays hold them (PassArgs::lazy): not with fluid drag
+// (its kernels read Predicted z and v) nor in a slab of a decomposition
+// (ghost and result exchanges).
+bool lazy_now(const dem_ctx* c) { return !c->fluid && !c->slab; }
+
 template <class V4, class W2>
 PassArgs<V4, W2> pass_args(dem_ctx* c, int side, bool update, double dt, const RingMap& rm,
                            int tag, const StateArrays& tgt) {
@@ -708,6 +725,7 @@ PassArgs<V4, W2> pass_args(dem_ctx* c, int side, bool update, double dt, const R
   A.cnt = c->cnt;
   A.tag = tag;
   A.drag = c->fluid ? c->drag : nullptr;
+  A.lazy = lazy_now(c) ? 1 : 0;
   A.amsum = c->amsum;
   A.rank = c->rows.rank;
   A.clist = c->clist;
@@ -996,6 +1014,10 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
 // Copies of `side` for the pass kernel and the cell transition towards its
 // positions (after forgetting a transition prepared for the other side).
 int prepare_side(dem_ctx* c, int side) {
+  if (side == 1) {  // Predicted's copies are made from Predicted
+    int st = settle_state(c);
+    if (st) return st;
+  }
   const int nxt = c->par ^ 1;
   launch(c, "discard", k_discard, (unsigned)LIST_BLOCKS, 256, c->L, nxt, (const Counters*)c->cnt);
   CK(cudaMemsetAsync(&c->cnt->n_dirty[nxt], 0, sizeof(int), c->stream));
@@ -1047,6 +1069,38 @@ void rotate_ring(dem_ctx* c) {
   for (int k = np - 1; k > 0; k--) c->ringmap[k] = c->ringmap[k - 1];
   c->ringmap[0] = spare;
   c->ringmap[np] = oldest;
+}
+
+// the rotation after a step's predictor pass: its ring slot becomes ipc(1),
+// and a lazy predictor (PassArgs::lazy) left a, alpha there
+void abm_rotate(dem_ctx* c) {
+  rotate_ring(c);
+  if (lazy_now(c)) c->lazy_state = true;
+}
+
+// Particle a, alpha and Predicted x (v, w: FP64) written back from the
+// arrays the lazy predictors left them in; before anything reads or changes
+// particle data, grows or renumbers it, or runs an Euler step
+int settle_state(dem_ctx* c) {
+  if (!c->lazy_state) return DEM_OK;
+  if (c->capturing || c->recording)
+    return fail(c, DEM_ERR_STATE, "state written back inside a captured chunk");
+  const int n = c->n;
+  if (n > 0) {
+    const int slot0 = c->nprev > 0 ? c->ringmap[0] : 0;
+    if (c->precision == DEM_PREC_MIXED)
+      launch(c, "settle_state", k_settle_state<false, float4, float2>, blocks_for(n, 256), 256, n,
+             c->P, c->Pr, (const double*)c->ring, slot0, c->nprev, (const double4*)c->X[1],
+             (const float4*)c->v4[1], (const float2*)c->w2[1]);
+    else
+      launch(c, "settle_state", k_settle_state<true, double4, double2>, blocks_for(n, 256), 256,
+             n, c->P, c->Pr, (const double*)c->ring, slot0, c->nprev, (const double4*)c->X[1],
+             (const double4*)c->v4[1], (const double2*)c->w2[1]);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "settle_state");
+  }
+  c->lazy_state = false;
+  return DEM_OK;
 }
 
 int read_counters(dem_ctx* c) {
@@ -1541,7 +1595,7 @@ int move_particles_impl(dem_ctx* c, int step, bool check, int k) {
   // force pass @ x(t) with history update, a(t) -> Particle, AB predictor
   int st = force_pass(c, 0, true, c->params.time_step, EPI_PREDICT, rm, check, 2 * k);
   if (st) return st;
-  rotate_ring(c);
+  abm_rotate(c);
   c->time = (double)step * c->params.time_step;
   st = apply_walls(c, k);
   if (st) return st;
@@ -1552,6 +1606,8 @@ int move_particles_impl(dem_ctx* c, int step, bool check, int k) {
 
 // MoveParticlesEuler (src/MDEM.f90:258-281)
 int move_particles_euler_impl(dem_ctx* c) {
+  int st0 = settle_state(c);  // the ring store reads Particle a, alpha
+  if (st0) return st0;
   const int n = c->n;
   const double dt = c->params.time_step / (double)c->params.euler_intervals;
   if (c->nprev > 0) {
@@ -1591,6 +1647,7 @@ int capture_steps(dem_ctx* c, int steps, cudaGraphExec_t* out) {
   std::memcpy(rm, c->ringmap, sizeof(rm));
   const int hc = c->hcur, par = c->par, prep = c->prepared, last = c->last_side;
   const double t = c->time;
+  const bool lazy = c->lazy_state;
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
   int st = DEM_OK;
   c->capturing = true;
@@ -1606,6 +1663,7 @@ int capture_steps(dem_ctx* c, int steps, cudaGraphExec_t* out) {
   c->prepared = prep;
   c->last_side = last;
   c->time = t;
+  c->lazy_state = lazy;
   if (st) return st;
   if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
   e = cudaGraphInstantiate(out, g, 0);
@@ -1630,6 +1688,7 @@ int record_chunk(dem_ctx* c, int steps, int phase) {
   std::memcpy(rm, c->ringmap, sizeof(rm));
   const int hc = c->hcur, par = c->par, prep = c->prepared, last = c->last_side;
   const double t = c->time;
+  const bool lazy = c->lazy_state;
   c->rec.clear();
   c->rec_n = 0;
   c->recording = true;
@@ -1646,6 +1705,7 @@ int record_chunk(dem_ctx* c, int steps, int phase) {
   c->prepared = prep;
   c->last_side = last;
   c->time = t;
+  c->lazy_state = lazy;
   if (st) return st;
   if (!clean || c->rec_n != 2 * steps)
     return fail(c, DEM_ERR_STATE, "a persistent chunk held work other than its force passes");
@@ -1996,7 +2056,11 @@ int reorder_by_cell(dem_ctx* c) {
 }
 
 // back to the reference's order (place g holds the particle numbered g)
-int restore_order(dem_ctx* c) {
+int restore_order(dem_ctx* c, bool settle) {
+  if (settle) {
+    int st = settle_state(c);
+    if (st) return st;
+  }
   if (!c->permuted) return DEM_OK;
   const int n = c->n;
   int* pi = nullptr;
@@ -2516,7 +2580,12 @@ static int put_state_arrays(dem_ctx* c, const StateArrays& s, const double* pos,
 int dem_update_state(dem_ctx* c, const double* pos, const double* vel, const double* omega,
                      const double* acc, const double* alpha) {
   if (!c) return DEM_ERR_INVALID;
-  RESTORE_ORDER;
+  {
+    // positions and velocities only: a and alpha may stay where the
+    // predictor left them
+    int st_ = restore_order(c, acc || alpha);
+    if (st_) return st_;
+  }
   if (!c->state_set) return fail(c, DEM_ERR_STATE, "no state");
   // the Particle copies of the pass kernel are stale from here on
   if (c->prepared == 0) c->prepared = -1;
@@ -2544,7 +2613,10 @@ int dem_timer_stop(dem_ctx* c, double* ms) {
 int dem_get_state(dem_ctx* c, double* pos, double* vel, double* omega, double* acc,
                   double* alpha) {
   if (!c) return DEM_ERR_INVALID;
-  RESTORE_ORDER;
+  {
+    int st_ = restore_order(c, acc || alpha);
+    if (st_) return st_;
+  }
   return get_state_arrays(c, c->P, pos, vel, omega, acc, alpha);
 }
 
@@ -3074,7 +3146,7 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
       failed_pass = escape_stop ? -1 : tag % 2;
     }
     for (int k = 0; k < done; k++) {
-      rotate_ring(c);
+      abm_rotate(c);
       c->hcur ^= 1;
     }
     if (done > 0) {
@@ -3108,7 +3180,7 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
         c->last_side = 0;
         c->prepared = 1;
         c->hcur ^= 1;
-        rotate_ring(c);
+        abm_rotate(c);
         c->time = (double)step * dt;
         st = apply_walls(c, 0);
         if (st) return st;
@@ -3119,7 +3191,7 @@ int dem_run(dem_ctx* c, int32_t first_step, int32_t last_step) {
         c->last_side = 0;
         c->prepared = 1;
         c->hcur ^= 1;
-        rotate_ring(c);
+        abm_rotate(c);
         c->time = (double)step * dt;
         st = apply_walls(c, 0);
         if (st) return st;
@@ -3761,7 +3833,7 @@ int dem_slab_phase(dem_ctx* c, int32_t step, int32_t pass, int32_t phase) {
       c->prepared = epi == EPI_PREDICT ? 1 : 0;
       if (update) c->hcur ^= 1;
       if (pass == 0) {
-        rotate_ring(c);
+        abm_rotate(c);
         c->time = (double)step * dt;
         st = apply_walls(c, 0);
         if (st) return st;

@@ -320,8 +320,11 @@ __device__ __forceinline__ void epilogue(const PassArgs<V4, W2>& A, const DevPar
   if (EPI == EPI_PREDICT) {
     const StateArrays& Q = A.part;
     const StateArrays& R = A.pred;
-    Q.ax[p] = acc[0]; Q.ay[p] = acc[1]; Q.az[p] = acc[2];
-    Q.lx[p] = alp[0]; Q.ly[p] = alp[1]; Q.lz[p] = alp[2];
+    // (with A.lazy, a and alpha stay in the new ring slot only)
+    if (!A.lazy || P.nprev == 0) {
+      Q.ax[p] = acc[0]; Q.ay[p] = acc[1]; Q.az[p] = acc[2];
+      Q.lx[p] = alp[0]; Q.ly[p] = alp[1]; Q.lz[p] = alp[2];
+    }
 #pragma unroll
     for (int d = 0; d < 3; d++) x[d] = xp[d] + P.ab0 * vp[d] + sv[d];
 #pragma unroll
@@ -331,9 +334,16 @@ __device__ __forceinline__ void epilogue(const PassArgs<V4, W2>& A, const DevPar
 #pragma unroll
     for (int d = 0; d < 3; d++)
       if (B.pbc[d]) x[d] = x[d] - B.lbox[d] * fnint(x[d] * B.inv_lbox[d]);
-    R.px[p] = x[0]; R.py[p] = x[1]; R.pz[p] = x[2];
-    R.vx[p] = v[0]; R.vy[p] = v[1]; R.vz[p] = v[2];
-    R.wx[p] = w[0]; R.wy[p] = w[1]; R.wz[p] = w[2];
+    // (with A.lazy, Predicted x stays in the position copy Xn, and with
+    // FP64 copies Predicted v, w stay in v4n, w2n; the mixed corrector reads
+    // Predicted v, and its FP32 copies do not hold v, w exactly)
+    if (!A.lazy) {
+      R.px[p] = x[0]; R.py[p] = x[1]; R.pz[p] = x[2];
+    }
+    if (!A.lazy || sizeof(V4) != sizeof(double4)) {
+      R.vx[p] = v[0]; R.vy[p] = v[1]; R.vz[p] = v[2];
+      R.wx[p] = w[0]; R.wy[p] = w[1]; R.wz[p] = w[2];
+    }
     if (P.nprev > 0) {
       double* rg = A.ring + (size_t)A.rm.phys[P.nprev] * 9 * n + p;
 #pragma unroll
