@@ -529,6 +529,11 @@ __device__ __forceinline__ void test_body(const TestArgs& A, int vblock) {
   unsigned long long mask0 = 0ull;
   unsigned long long more[(KC_MAX + 1) / 64 - 1];
   int total = 0;
+  // the next group's candidates are requested with this group's positions:
+  // one round trip per group of 4 after the first
+  int qn[4];
+#pragma unroll
+  for (int u = 0; u < 4; u++) qn[u] = q0[u];
   for (int base = 0; base < m; base += 64) {
     unsigned long long mask = 0ull;
     const int end = m < base + 64 ? m : base + 64;
@@ -536,8 +541,10 @@ __device__ __forceinline__ void test_body(const TestArgs& A, int vblock) {
     for (int b = base; b < end; b += 4) {
       int q[4];
 #pragma unroll
+      for (int u = 0; u < 4; u++) q[u] = b + u < end ? qn[u] : -1;
+#pragma unroll
       for (int u = 0; u < 4; u++)
-        q[u] = b + u < end ? (b == 0 ? q0[u] : ld_row<NC>(A.cand + (size_t)(b + u) * n + p)) : -1;
+        qn[u] = b + 4 + u < m ? ld_row<NC>(A.cand + (size_t)(b + 4 + u) * n + p) : -1;
       double4 xq[4];
 #pragma unroll
       for (int u = 0; u < 4; u++)
