@@ -7,7 +7,10 @@ linear spring-dashpot collision restore the requested restitution coefficient
 after a contact time pi/omega_d (MinCollisionTime, src/DEM.f90:330-331);
 the Coulomb cap (src/MForces.f90:372-378); the rectangle closest-point
 geometry (src/MConfig.f90:717-749); CurrentCell3D (src/MCells.f90:498-513);
-Newton's third law of the pair loop (src/MForces.f90:254-259)."""
+Newton's third law of the pair loop (src/MForces.f90:254-259); free flight,
+which the Euler start-up and the Adams-Bashforth-Moulton steps integrate
+exactly; and a sphere resting on the floor, a damped linear oscillator that
+the fourth-order integrator follows at fourth order."""
 import math
 
 import numpy as np
