@@ -104,6 +104,7 @@ struct Counters {
   int escape_stop;   // a captured chunk stopped before a step: particles had left the box
   int pass_id;       // force passes completed; a cell stamped pass_id + 1 has rows to rebuild
   int barrier_timeout;  // a grid-wide barrier of a persistent launch gave up waiting
+  int n_mlist[2];  // entries of CellLists::mlist recorded by the relinks of even / odd stamps
 };
 
 // Contact history, one table per buffer, stored slot major (record r of
@@ -159,6 +160,13 @@ struct CellLists {
   int* rflag;     // [ncell] stamp: pass_id + 1 when the cell's rows are rebuilt in that pass
   int* dlist[2];  // [ncell] cells that gain or lose a particle on the way to assignment b
   int* rlist;     // [ncell] (unused: the stamps replace a repair list)
+  // the particles that left or entered a cell in the relink of the pass
+  // with stamp s: mlist[(s & 1) * mcap + k], k < Counters::n_mlist[s & 1]
+  // (more than mcap: not all recorded); dstamp[c] = s when that relink
+  // rewrote cell c's list
+  int* mlist;
+  int* dstamp;
+  int mcap;
   // each cell's list copied in order into SLOT_CAP slots ([cell*SLOT_CAP +
   // k]) and its length (slot_n > SLOT_CAP: only the first SLOT_CAP are
   // copied; -1: not current): the candidate rows read a neighbour cell with
@@ -171,6 +179,9 @@ struct CellLists {
   const int* gid;
 };
 constexpr int SLOT_CAP = 32;
+// movers one relink records for the test kernel's row check (more: every
+// stamped row is rebuilt)
+constexpr int MLIST_CAP = 4096;
 
 // Candidate rows, column-major (cand[k*n + p]): the particles within
 // MinDij + skin of particle p that the sweep visits with p as "i" (loop jj

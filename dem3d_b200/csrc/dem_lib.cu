@@ -369,7 +369,7 @@ void free_lists(dem_ctx* c) {
   CellLists& L = c->L;
   int** f[] = {&L.head,  &L.next,  &L.cell[0], &L.cell[1], &L.arr_head, &L.arr_next, &L.mflag,
                &L.mnext, &L.dflag, &L.rflag,   &L.dlist[0], &L.dlist[1],  &L.rlist,
-               &L.slot,  &L.slot_n};
+               &L.slot,  &L.slot_n, &L.mlist, &L.dstamp};
   for (int** q : f) {
     cudaFree(*q);
     *q = nullptr;
@@ -649,6 +649,7 @@ int init_cells(dem_ctx* c) {
   CK(cudaMemsetAsync(L.arr_head, 0xFF, sizeof(int) * (size_t)ncell, c->stream));
   CK(cudaMemsetAsync(L.dflag, 0, sizeof(int) * (size_t)ncell, c->stream));
   CK(cudaMemsetAsync(L.rflag, 0, sizeof(int) * (size_t)ncell, c->stream));
+  CK(cudaMemsetAsync(L.dstamp, 0, sizeof(int) * (size_t)ncell, c->stream));
   if (n > 0) CK(cudaMemsetAsync(L.mflag, 0, sizeof(int) * (size_t)n, c->stream));
   CK(cudaMemsetAsync(c->cell_cnt, 0, sizeof(int) * (size_t)ncell, c->stream));
   if (n > 0) {
@@ -895,6 +896,7 @@ void launch_pass_kernel(dem_ctx* c, int side, bool update, double dt, int epi, c
   T.tag = tag;
   T.slab_c0 = c->slab ? c->hsys[0].slab_c0 : 0;
   T.slab_span = c->slab ? (unsigned)(c->hsys[0].slab_c1 - c->hsys[0].slab_c0) : 0xffffffffu;
+  T.fine = c->slab ? 0 : 1;  // (a slab's stamps of its ghost layer come by exchange)
   const bool walls = c->nw_max > 0;
   if (c->recording) {
     // a pass of a persistent chunk: appended, not launched
@@ -2485,6 +2487,10 @@ int dem_set_state(dem_ctx* c, int32_t n, const int32_t* comp, const double* radi
     CK(cudaMalloc(&L.slot, sizeof(int) * NC * SLOT_CAP));
     CK(cudaMalloc(&L.slot_n, sizeof(int) * NC));
     CK(cudaMemsetAsync(L.slot_n, 0xFF, sizeof(int) * NC, c->stream));
+    L.mcap = MLIST_CAP;
+    CK(cudaMalloc(&L.mlist, sizeof(int) * 2 * (size_t)MLIST_CAP));
+    CK(cudaMalloc(&L.dstamp, sizeof(int) * NC));
+    CK(cudaMemsetAsync(L.dstamp, 0, sizeof(int) * NC, c->stream));
     CK(cudaMalloc(&c->rows.cand, sizeof(int) * N * (size_t)c->kc));
     CK(cudaMalloc(&c->rows.meta, sizeof(int) * N));
     CK(cudaMemsetAsync(c->rows.meta, 0, sizeof(int) * N, c->stream));

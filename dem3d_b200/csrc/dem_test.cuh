@@ -90,6 +90,7 @@ __device__ __forceinline__ void relink_body(const DevParams* __restrict__ PT,
   if (tid == 0) {
     const DevParams& P = PT[0];  // the integrator settings are shared
     cnt->n_repair = 0;
+    cnt->n_mlist[(stamp & 1) ^ 1] = 0;  // for the next pass's relink
     cnt->n_dirty[par ^ 1] = 0;
     cnt->movers = cnt->movers_pending;
     cnt->movers_pending = 0ull;
@@ -116,6 +117,11 @@ __device__ __forceinline__ void relink_body(const DevParams* __restrict__ PT,
     if (full) cnt->force_full = 0;
   }
   const int* __restrict__ cell_new = L.cell[par];
+  // a particle that leaves or enters a cell, for the test kernel's row check
+  auto record = [&](int x) {
+    const int k = atomicAdd(&cnt->n_mlist[stamp & 1], 1);
+    if (k < L.mcap) L.mlist[(size_t)(stamp & 1) * L.mcap + k] = x;
+  };
   for (int i = tid; i < m; i += nthreads) {
     const int c = L.dlist[par][i];
     const DevParams& P = sys_params(PT, cellsys, c);
@@ -146,7 +152,10 @@ __device__ __forceinline__ void relink_body(const DevParams* __restrict__ PT,
       for (int k = 0; k < len; k++)
         if (cell_new[old[k]] == c) stay |= 1u << k;
       for (int k = 0; k < len; k++) {
-        if (!((stay >> k) & 1u)) continue;
+        if (!((stay >> k) & 1u)) {
+          record(old[k]);
+          continue;
+        }
         if (prev == -1) first = old[k];
         else L.next[prev] = old[k];
         prev = old[k];
@@ -161,6 +170,7 @@ __device__ __forceinline__ void relink_body(const DevParams* __restrict__ PT,
         }
         const bool stays = cell_new[q] == c;
         const int nq = stays ? L.next[q] : L.mnext[q];
+        if (!stays) record(q);
         if (stays) {
           if (prev == -1) first = q;
           else L.next[prev] = q;
@@ -183,6 +193,7 @@ __device__ __forceinline__ void relink_body(const DevParams* __restrict__ PT,
       }
       const int an = L.arr_next[a];  // (guard: arrivals so far)
       L.mflag[a] = 0;
+      record(a);
       if (sh == -1) {
         sh = tail = a;
         L.next[a] = -1;
@@ -206,6 +217,7 @@ __device__ __forceinline__ void relink_body(const DevParams* __restrict__ PT,
     }
     L.head[c] = first;
     L.dflag[c] = 0;
+    L.dstamp[c] = stamp;
     if (from_slots) {
       // the new list's slots: the arrivals (this thread linked them), then
       // the stayers in their old order
@@ -460,7 +472,61 @@ struct TestArgs {
   // (a slab of a decomposition, or every cell)
   int slab_c0;
   unsigned slab_span;
+  // 1: a stamped row is rebuilt only when a particle that changed cell is
+  // near it (row_stays); 0: every stamped row is rebuilt
+  int fine;
 };
+
+// Whether the row of particle pl (cell cl), stamped because a cell it reads
+// was relinked, can stay as it is; called by the whole warp together.  A
+// relink keeps the stayers of a list in their order and puts the arrivals
+// first, so the row changes only if a particle that left or entered one of
+// those cells is within MinDij + skin of pl; one farther than that can come
+// no closer than MinDij + 0.2 skin before the next full rebuild (every
+// particle moves at most 0.4 skin in between), so a stale entry for it in
+// the row is tested and rejected, and its absence changes no contact.  The
+// lanes check the pass's movers 32 at a time (a margin errs towards
+// rebuilding); when none is near, the row stays, and if pl's own cell was
+// relinked its rank (its place in the list) is rewritten from the slots.
+template <bool PP>
+__device__ __forceinline__ bool row_stays(const TestArgs& A, int pl, int cl, const double4& p4,
+                                          int cp, int stamp, int n, int lane) {
+  const unsigned FULL = 0xffffffffu;
+  const int b = stamp & 1;
+  const int nm = A.cnt->n_mlist[b];
+  if (nm > A.L.mcap) return false;
+  const DevParams& P = sys_params(A.P, A.sysid, pl);
+  const double skin = P.vl_skin;
+  const int* ml = A.L.mlist + (size_t)b * A.L.mcap;
+  bool near = false;
+  for (int k = lane; k < nm && !near; k += 32) {
+    const int q = ml[k];
+    if ((unsigned)q >= (unsigned)n) {
+      near = true;
+      break;
+    }
+    const double4 q4 = A.X[q];
+    double Rij[3] = {__dsub_rn(q4.x, p4.x), __dsub_rn(q4.y, p4.y), __dsub_rn(q4.z, p4.z)};
+#pragma unroll
+    for (int d = 0; d < 3; d++) Rij[d] = min_image_rn(Rij[d], P.box, d);
+    const double DijSq = sumsq3_rn(Rij);
+    double md;
+    if (PP) md = __dadd_rn(p4.w, q4.w);
+    else md = __dsqrt_rn(min_dij_sq_rn<PP>(P, cp, p4.w, A.comp[q], q4.w));
+    md = __dadd_rn(__dadd_rn(md, skin), __dadd_rn(1.0e-9, __dmul_rn(1.0e-9, md)));
+    if (!(__dsub_rn(__dmul_rn(md, md), DijSq) < 0.0)) near = true;
+  }
+  if (__any_sync(FULL, near)) return false;
+  if (A.L.dstamp[cl] == stamp) {
+    const int len = A.L.slot_n[cl];
+    if (len < 0 || len > SLOT_CAP) return false;
+    const bool hit = lane < len && A.L.slot[(size_t)cl * SLOT_CAP + lane] == pl;
+    const unsigned h = __ballot_sync(FULL, hit);
+    if (!h) return false;
+    if (lane == 0) A.R.rank[pl] = __ffs(h) - 1;
+  }
+  return true;
+}
 
 // First, the candidate rows of the warp's particles that this pass rebuilds
 // (every row on a full rebuild, else the rows of the particles whose cell the
@@ -506,7 +572,24 @@ __device__ __forceinline__ void test_body(const TestArgs& A, int vblock) {
   for (int u = 0; u < 4; u++) q0[u] = ld_row<NC>(A.cand + (size_t)u * n + p);
   int meta = A.meta[p];
   {
-    unsigned todo = __ballot_sync(FULL, live && valid && (full || A.L.rflag[cp0] == stamp));
+    bool stale = live && valid && (full || A.L.rflag[cp0] == stamp);
+    if (!full && A.fine) {
+      // the stamped rows checked against the pass's movers, one at a time
+      // by the whole warp
+      unsigned chk = __ballot_sync(FULL, stale);
+      while (chk) {
+        const int l = __ffs(chk) - 1;
+        chk &= chk - 1u;
+        const int pl = __shfl_sync(FULL, p, l);
+        const int cl = __shfl_sync(FULL, cp0, l);
+        const int cpl = __shfl_sync(FULL, cp, l);
+        const double4 pl4 = make_double4(__shfl_sync(FULL, p4.x, l), __shfl_sync(FULL, p4.y, l),
+                                         __shfl_sync(FULL, p4.z, l), __shfl_sync(FULL, p4.w, l));
+        const bool keep = row_stays<PP>(A, pl, cl, pl4, cpl, stamp, n, lane);
+        if (lane == l && keep) stale = false;
+      }
+    }
+    unsigned todo = __ballot_sync(FULL, stale);
     if (todo) {
       while (todo) {
         const int l = __ffs(todo) - 1;
